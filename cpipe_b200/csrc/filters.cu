@@ -1,0 +1,832 @@
+// The filter seam: one extern "C" function per reference aot_id, with the
+// reference's HalideParamFilterEntry / HalideFilterEntry signatures
+// (src/cpipe/runtime/HalideFilterRegistry.hpp:18-21), so a reference runtime can
+// register them in place of the Halide/C++ CPU filters
+// (ComputeContext::register_halide_param_filter, ComputeContext.cpp:16-23).
+//
+// Buffers: a halide_buffer_t with device != 0 is CUDA device memory and is
+// processed in place, asynchronously, on the calling thread's current stream
+// (cpipe_cuda_set_stream).  Otherwise its host pointer is staged through device
+// memory and the call returns only after the result is back in host memory,
+// which is what a CPU-filter caller expects.  There is no CPU code path: if no
+// CUDA device is usable, every filter returns CPIPE_INTERNAL_ERROR.
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/cpipe_b200.h"
+#include "filters_impl.h"
+#include "kernels.h"
+
+namespace cpb {
+
+// ------------------------------------------------------------ thread state
+namespace {
+thread_local cudaStream_t g_stream = nullptr;
+thread_local char g_err[512] = {0};
+}  // namespace
+
+void set_error(const char* fmt, const char* detail) {
+    std::snprintf(g_err, sizeof(g_err), fmt, detail ? detail : "");
+}
+cudaStream_t current_stream() { return g_stream; }
+
+int cuda_status(cudaError_t e, const char* where) {
+    if (e == cudaSuccess) return CPIPE_OK;
+    std::snprintf(g_err, sizeof(g_err), "%s: %s", where, cudaGetErrorString(e));
+    return CPIPE_INTERNAL_ERROR;
+}
+
+// ---------------------------------------------------------------- binding
+int Call::bind(halide_buffer_t* hb, Kind kind, bool is_output, Bound* out) {
+    if (hb == nullptr) return CPIPE_BAD_INDEX;
+    const int code = hb->type.code, bits = hb->type.bits;
+    int elem = bits / 8, ch = 1;
+    switch (kind) {
+        case Kind::BayerU16:
+            if (code != halide_type_uint || bits != 16) return CPIPE_BAD_PRECISION;
+            if (hb->dimensions != 2) return CPIPE_BAD_INDEX;
+            break;
+        case Kind::BayerF32:
+            if (code != halide_type_float || bits != 32) return CPIPE_BAD_PRECISION;
+            if (hb->dimensions != 2) return CPIPE_BAD_INDEX;
+            break;
+        case Kind::Rgba:
+            if (code != halide_type_float || (bits != 16 && bits != 32)) return CPIPE_BAD_PRECISION;
+            if (hb->dimensions != 3 || hb->dim[2].extent != 4 || hb->dim[2].stride != 1) return CPIPE_BAD_INDEX;
+            ch = 4;
+            break;
+        case Kind::RgbaU8:
+            if (code != halide_type_uint || bits != 8) return CPIPE_BAD_PRECISION;
+            if (hb->dimensions != 3 || hb->dim[2].extent != 4 || hb->dim[2].stride != 1) return CPIPE_BAD_INDEX;
+            ch = 4;
+            break;
+        case Kind::RgbaU16:
+            if (code != halide_type_uint || bits != 16) return CPIPE_BAD_PRECISION;
+            if (hb->dimensions != 3 || hb->dim[2].extent != 4 || hb->dim[2].stride != 1) return CPIPE_BAD_INDEX;
+            ch = 4;
+            break;
+        case Kind::Any:
+            if (bits % 8 != 0 || bits == 0) return CPIPE_BAD_PRECISION;
+            if (hb->dimensions == 3) {
+                if (hb->dim[2].stride != 1) return CPIPE_BAD_INDEX;
+                ch = hb->dim[2].extent;
+            } else if (hb->dimensions != 2) {
+                return CPIPE_BAD_INDEX;
+            }
+            break;
+    }
+    const int w = hb->dim[0].extent, h = hb->dim[1].extent;
+    if (w <= 0 || h <= 0) return CPIPE_BAD_INDEX;
+    if (hb->dim[0].stride != ch) {
+        set_error("%s", "interleaved pixels with pixel stride == channel count are required");
+        return CPIPE_UNSUPPORTED;
+    }
+    const long long row_stride = hb->dim[1].stride;
+    if (row_stride < (long long)w * ch) return CPIPE_BAD_INDEX;
+    // Vector loads need 8-byte (RGBA f16) / 16-byte (RGBA f32) aligned pixels.
+    const int align = (ch == 4 && kind != Kind::Any) ? elem * 4 : elem;
+    Bound b;
+    b.hb = hb;
+    b.elem = elem;
+    b.ch = ch;
+    b.is_output = is_output;
+    const bool on_device = hb->device != 0 && !(hb->flags & halide_buffer_flag_host_dirty && hb->host);
+    if (on_device) {
+        if ((hb->device % align) != 0 || ((row_stride * elem) % align) != 0) {
+            set_error("%s", "device buffer rows are not aligned for vector access");
+            return CPIPE_UNSUPPORTED;
+        }
+        b.img = Img{reinterpret_cast<void*>(hb->device), w, h, row_stride, ch};
+        b.staged = false;
+    } else {
+        if (hb->host == nullptr) return CPIPE_BAD_INDEX;
+        const size_t bytes = (size_t)w * h * ch * elem;
+        void* d = nullptr;
+        int st = alloc(bytes, &d);
+        if (st != CPIPE_OK) return st;
+        b.img = Img{d, w, h, (long long)w * ch, ch};
+        b.staged = true;
+        if (!is_output) {
+            st = cuda_status(cudaMemcpy2DAsync(d, (size_t)w * ch * elem, hb->host, (size_t)row_stride * elem,
+                                               (size_t)w * ch * elem, (size_t)h, cudaMemcpyHostToDevice, stream),
+                             "stage in");
+            if (st != CPIPE_OK) return st;
+        }
+        staged_any = true;
+    }
+    bounds.push_back(b);
+    *out = b;
+    return CPIPE_OK;
+}
+
+int Call::alloc(size_t bytes, void** out) {
+    void* d = nullptr;
+    const cudaError_t e = cudaMallocAsync(&d, bytes < 256 ? 256 : bytes, stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        std::snprintf(g_err, sizeof(g_err), "device allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
+        return CPIPE_OOM;
+    }
+    scratch.push_back(d);
+    *out = d;
+    return CPIPE_OK;
+}
+
+int Call::upload(const void* host, size_t bytes, void** out) {
+    int st = alloc(bytes, out);
+    if (st != CPIPE_OK) return st;
+    return cuda_status(cudaMemcpyAsync(*out, host, bytes, cudaMemcpyHostToDevice, stream), "upload params");
+}
+
+int Call::finish(int status) {
+    if (status == CPIPE_OK) {
+        status = cuda_status(cudaGetLastError(), "kernel launch");
+    }
+    for (const Bound& b : bounds) {
+        if (!b.is_output) continue;
+        if (b.staged) {
+            if (status == CPIPE_OK) {
+                const halide_buffer_t* hb = b.hb;
+                status = cuda_status(cudaMemcpy2DAsync(hb->host, (size_t)hb->dim[1].stride * b.elem, b.img.data,
+                                                       (size_t)b.img.w * b.ch * b.elem, (size_t)b.img.w * b.ch * b.elem,
+                                                       (size_t)b.img.h, cudaMemcpyDeviceToHost, stream),
+                                     "stage out");
+            }
+        } else if (status == CPIPE_OK) {
+            b.hb->flags |= halide_buffer_flag_device_dirty;
+        }
+    }
+    for (void* p : scratch) cudaFreeAsync(p, stream);
+    scratch.clear();
+    if (staged_any) {
+        const int st = cuda_status(cudaStreamSynchronize(stream), "synchronize");
+        if (status == CPIPE_OK) status = st;
+    }
+    return status;
+}
+
+Call::Call() : stream(current_stream()) {}
+Call::~Call() {
+    for (void* p : scratch) cudaFreeAsync(p, stream);
+}
+
+bool device_ready() {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        set_error("%s", "no CUDA device is available; the cpipe B200 filters have no CPU path");
+        return false;
+    }
+    return true;
+}
+
+static bool same_extent(const Bound& a, const Bound& b) { return a.img.w == b.img.w && a.img.h == b.img.h; }
+
+// float-float split of a double.
+ff split(double v) {
+    const float hi = (float)v;
+    return ff{hi, (float)(v - (double)hi)};
+}
+
+}  // namespace cpb
+
+using namespace cpb;
+
+#define CHECK_ARITY(nin, nout)                                                                     \
+    if (n_in != (nin) || n_out != (nout) || inputs == nullptr || outputs == nullptr ||             \
+        inputs[0] == nullptr || outputs[0] == nullptr)                                             \
+        return CPIPE_BAD_INDEX;
+#define BIND(idx, arr, kind, is_out, var)                                                          \
+    Bound var;                                                                                     \
+    {                                                                                              \
+        const int s_ = call.bind(arr[idx], kind, is_out, &var);                                    \
+        if (s_ != CPIPE_OK) return call.finish(s_);                                                \
+    }
+#define REQUIRE_SAME_EXTENT(a, b) \
+    if (!same_extent(a, b)) return call.finish(CPIPE_BAD_INDEX);
+
+extern "C" {
+
+// ----------------------------------------------------------------- stream API
+int cpipe_cuda_set_stream(void* stream) {
+    g_stream = static_cast<cudaStream_t>(stream);
+    return CPIPE_OK;
+}
+void* cpipe_cuda_get_stream(void) { return g_stream; }
+const char* cpipe_cuda_last_error(void) { return g_err; }
+int cpipe_cuda_synchronize(void) { return cuda_status(cudaStreamSynchronize(g_stream), "synchronize"); }
+int cpipe_cuda_device_count(void) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        return 0;
+    }
+    return n;
+}
+
+// ------------------------------------------------------ a1 precision_convert
+// precision_convert_generator.cpp:31-124; plain (input, output) filters
+// registered with CPIPE_REGISTER_HALIDE_FILTER (precision_convert_dispatch.cpp).
+int cpipe_cuda_precision_convert_r16u_to_f32(halide_buffer_t* input, halide_buffer_t* output) {
+    if (!device_ready()) return CPIPE_INTERNAL_ERROR;
+    Call call;
+    halide_buffer_t* ins[1] = {input};
+    halide_buffer_t* outs[1] = {output};
+    BIND(0, ins, Kind::BayerU16, false, in);
+    BIND(0, outs, Kind::BayerF32, true, out);
+    REQUIRE_SAME_EXTENT(in, out);
+    return call.finish(cuda_status(launch_r16u_to_f32(in.img, out.img, call.stream), "r16u_to_f32"));
+}
+int cpipe_cuda_precision_convert_f32_to_rgba16f(halide_buffer_t* input, halide_buffer_t* output) {
+    if (!device_ready()) return CPIPE_INTERNAL_ERROR;
+    Call call;
+    halide_buffer_t* ins[1] = {input};
+    halide_buffer_t* outs[1] = {output};
+    BIND(0, ins, Kind::BayerF32, false, in);
+    BIND(0, outs, Kind::Rgba, true, out);
+    if (out.elem != 2) return call.finish(CPIPE_BAD_PRECISION);
+    REQUIRE_SAME_EXTENT(in, out);
+    return call.finish(cuda_status(launch_f32_to_rgba16f(in.img, out.img, call.stream), "f32_to_rgba16f"));
+}
+static int rgba16f_to_unorm(halide_buffer_t* input, halide_buffer_t* output, int bits8) {
+    if (!device_ready()) return CPIPE_INTERNAL_ERROR;
+    Call call;
+    halide_buffer_t* ins[1] = {input};
+    halide_buffer_t* outs[1] = {output};
+    BIND(0, ins, Kind::Rgba, false, in);
+    if (in.elem != 2) return call.finish(CPIPE_BAD_PRECISION);
+    BIND(0, outs, bits8 ? Kind::RgbaU8 : Kind::RgbaU16, true, out);
+    REQUIRE_SAME_EXTENT(in, out);
+    return call.finish(cuda_status(launch_rgba16f_to_unorm(in.img, out.img, bits8, call.stream), "to_unorm"));
+}
+int cpipe_cuda_precision_convert_rgba16f_to_rgba8(halide_buffer_t* input, halide_buffer_t* output) {
+    return rgba16f_to_unorm(input, output, 1);
+}
+int cpipe_cuda_precision_convert_rgba16f_to_rgba16u(halide_buffer_t* input, halide_buffer_t* output) {
+    return rgba16f_to_unorm(input, output, 0);
+}
+
+// --------------------------------------------------------------- a2 linearize
+// linearize_dng_lut_dispatch.cpp:17-51
+int cpipe_cuda_linearize_dng_lut(halide_buffer_t* const* inputs, size_t n_in, halide_buffer_t* const* outputs,
+                                 size_t n_out, const void* blob, size_t blob_size) {
+    CHECK_ARITY(1, 1);
+    if (blob == nullptr || blob_size < sizeof(cpipe_LinearizeParamsHeader)) return CPIPE_BAD_INDEX;
+    const auto* hd = static_cast<const cpipe_LinearizeParamsHeader*>(blob);
+    const size_t expected = sizeof(*hd) + (size_t)hd->table_size * sizeof(uint16_t);
+    if (hd->table_size == 0 || blob_size < expected) return CPIPE_NEED_METADATA;
+    if (!device_ready()) return CPIPE_INTERNAL_ERROR;
+    Call call;
+    BIND(0, inputs, Kind::BayerU16, false, in);
+    BIND(0, outputs, Kind::BayerF32, true, out);
+    REQUIRE_SAME_EXTENT(in, out);
+    void* d_table = nullptr;
+    int st = call.upload(static_cast<const char*>(blob) + sizeof(*hd), hd->table_size * sizeof(uint16_t), &d_table);
+    if (st != CPIPE_OK) return call.finish(st);
+    return call.finish(cuda_status(
+        launch_linearize(in.img, out.img, static_cast<const uint16_t*>(d_table), (int)hd->table_size, call.stream),
+        "linearize"));
+}
+
+// -------------------------------------------------------------- a3 blacklevel
+// blacklevel_dng_levels_dispatch.cpp:16-47
+int cpb_blacklevel_dev(const cpipe_BlacklevelParams* p, int w, int h, BlackDev* out) {
+    for (int i = 0; i < 4; ++i) {
+        const unsigned ch = p->cfa_pattern[i] < 3 ? p->cfa_pattern[i] : 3;
+        out->black[i] = p->black_level[ch];
+        out->denom[i] = (float)p->white_level - p->black_level[ch];
+        const bool used = ((i & 1) == 0 || w > 1) && ((i >> 1) == 0 || h > 1);
+        if (used && out->denom[i] <= 0.0F) return CPIPE_NEED_METADATA;
+    }
+    return CPIPE_OK;
+}
+int cpipe_cuda_blacklevel_dng_levels(halide_buffer_t* const* inputs, size_t n_in, halide_buffer_t* const* outputs,
+                                     size_t n_out, const void* blob, size_t blob_size) {
+    CHECK_ARITY(1, 1);
+    if (blob == nullptr || blob_size < sizeof(cpipe_BlacklevelParams)) return CPIPE_BAD_INDEX;
+    if (!device_ready()) return CPIPE_INTERNAL_ERROR;
+    Call call;
+    BIND(0, inputs, Kind::BayerF32, false, in);
+    BIND(0, outputs, Kind::BayerF32, true, out);
+    REQUIRE_SAME_EXTENT(in, out);
+    BlackDev p;
+    const int st = cpb_blacklevel_dev(static_cast<const cpipe_BlacklevelParams*>(blob), in.img.w, in.img.h, &p);
+    if (st != CPIPE_OK) return call.finish(st);
+    return call.finish(cuda_status(launch_blacklevel(in.img, out.img, p, call.stream), "blacklevel"));
+}
+
+// ----------------------------------------------------------------- a4 gainmap
+// shading_gainmap_dispatch.cpp:23-133.  The double-precision axis sampling is
+// done here on the host, once per row and column.
+static AxisSample host_sample_axis(double coord, uint32_t points) {
+    AxisSample a{0, 0, 0.0F};
+    if (points <= 1U || coord <= 0.0) return a;
+    const double last = (double)(points - 1U);
+    if (coord >= last) {
+        a.low = a.high = points - 1U;
+        return a;
+    }
+    a.low = (uint32_t)std::floor(coord);
+    a.high = a.low + 1U;
+    a.weight = (float)(coord - (double)a.low);
+    return a;
+}
+int cpb_gainmap_prepare(const void* blob, size_t blob_size, int w, int h, std::vector<char>* table,
+                        GainMapDev* g, size_t offsets[3][4]) {
+    if (blob == nullptr || blob_size < sizeof(cpipe_GainMapDispatchHeader)) return CPIPE_BAD_INDEX;
+    const auto* hd = static_cast<const cpipe_GainMapDispatchHeader*>(blob);
+    if (hd->map_count == 0U || hd->map_count > 4U) return CPIPE_NEED_METADATA;
+    const size_t map_bytes = hd->map_count * sizeof(cpipe_GainMapDispatchPlane);
+    if (blob_size < sizeof(*hd) + map_bytes) return CPIPE_BAD_INDEX;
+    const auto* maps = reinterpret_cast<const cpipe_GainMapDispatchPlane*>(static_cast<const char*>(blob) + sizeof(*hd));
+    const char* gains = static_cast<const char*>(blob) + sizeof(*hd) + map_bytes;
+    const size_t gain_bytes = blob_size - sizeof(*hd) - map_bytes;
+    for (uint32_t i = 0; i < hd->map_count; ++i) {
+        const uint64_t req = ((uint64_t)maps[i].gain_offset + maps[i].gain_count) * sizeof(float);
+        if (maps[i].map_points_v == 0U || maps[i].map_points_h == 0U || maps[i].gain_count == 0U || req > gain_bytes)
+            return CPIPE_BAD_INDEX;
+        // the sampler reads up to (points_v-1)*points_h + points_h-1 from the map's offset
+        if ((uint64_t)maps[i].map_points_v * maps[i].map_points_h > maps[i].gain_count) return CPIPE_BAD_INDEX;
+    }
+    g->map_count = (int)hd->map_count;
+    g->qbc = hd->cfa_repeat[0] == 4U && hd->cfa_repeat[1] == 4U;
+    for (int p = 0; p < 4; ++p) {
+        g->plane_to_map[p] = -1;
+        for (uint32_t i = 0; i < hd->map_count; ++i)
+            if (maps[i].plane == (uint32_t)p) {
+                g->plane_to_map[p] = (int)i;
+                break;
+            }
+    }
+    if (hd->map_count > 1) {
+        // select_map returns nullptr -> CPIPE_NEED_METADATA for any pixel whose plane has no map
+        for (int p = 0; p < 4; ++p) {
+            const bool used = g->qbc ? (((p & 1) == 0 || w > 2) && ((p >> 1) == 0 || h > 2))
+                                     : (((p & 1) == 0 || w > 1) && ((p >> 1) == 0 || h > 1));
+            if (used && g->plane_to_map[p] < 0) return CPIPE_NEED_METADATA;
+        }
+    }
+    // layout: gains | cols (w per map) | rows (h per map)
+    size_t off = 0;
+    table->clear();
+    for (uint32_t i = 0; i < hd->map_count; ++i) {
+        offsets[0][i] = off;
+        const size_t n = (size_t)maps[i].map_points_v * maps[i].map_points_h * sizeof(float);
+        table->resize(off + n);
+        std::memcpy(table->data() + off, gains + (size_t)maps[i].gain_offset * sizeof(float), n);
+        off += (n + 15) & ~size_t(15);
+        g->points_h[i] = (int)maps[i].map_points_h;
+    }
+    for (uint32_t i = 0; i < hd->map_count; ++i) {
+        offsets[1][i] = off;
+        table->resize(off + (size_t)w * sizeof(AxisSample));
+        auto* cols = reinterpret_cast<AxisSample*>(table->data() + off);
+        for (int x = 0; x < w; ++x)
+            cols[x] = host_sample_axis(((double)x - maps[i].map_origin_h) / maps[i].map_spacing_h, maps[i].map_points_h);
+        off += ((size_t)w * sizeof(AxisSample) + 15) & ~size_t(15);
+    }
+    for (uint32_t i = 0; i < hd->map_count; ++i) {
+        offsets[2][i] = off;
+        table->resize(off + (size_t)h * sizeof(AxisSample));
+        auto* rows = reinterpret_cast<AxisSample*>(table->data() + off);
+        for (int y = 0; y < h; ++y)
+            rows[y] = host_sample_axis(((double)y - maps[i].map_origin_v) / maps[i].map_spacing_v, maps[i].map_points_v);
+        off += ((size_t)h * sizeof(AxisSample) + 15) & ~size_t(15);
+    }
+    table->resize(off);
+    return CPIPE_OK;
+}
+void cpb_gainmap_bind(GainMapDev* g, const char* d_table, size_t offsets[3][4]) {
+    for (int i = 0; i < g->map_count; ++i) {
+        g->gains[i] = reinterpret_cast<const float*>(d_table + offsets[0][i]);
+        g->cols[i] = reinterpret_cast<const AxisSample*>(d_table + offsets[1][i]);
+        g->rows[i] = reinterpret_cast<const AxisSample*>(d_table + offsets[2][i]);
+    }
+}
+int cpipe_cuda_lens_shading_gainmap(halide_buffer_t* const* inputs, size_t n_in, halide_buffer_t* const* outputs,
+                                    size_t n_out, const void* blob, size_t blob_size) {
+    CHECK_ARITY(1, 1);
+    if (blob == nullptr || blob_size < sizeof(cpipe_GainMapDispatchHeader)) return CPIPE_BAD_INDEX;
+    if (!device_ready()) return CPIPE_INTERNAL_ERROR;
+    Call call;
+    BIND(0, inputs, Kind::BayerF32, false, in);
+    BIND(0, outputs, Kind::BayerF32, true, out);
+    REQUIRE_SAME_EXTENT(in, out);
+    std::vector<char> table;
+    GainMapDev g{};
+    size_t offsets[3][4] = {};
+    int st = cpb_gainmap_prepare(blob, blob_size, in.img.w, in.img.h, &table, &g, offsets);
+    if (st != CPIPE_OK) return call.finish(st);
+    void* d_table = nullptr;
+    st = call.upload(table.data(), table.size(), &d_table);
+    if (st != CPIPE_OK) return call.finish(st);
+    cpb_gainmap_bind(&g, static_cast<const char*>(d_table), offsets);
+    return call.finish(cuda_status(launch_gainmap(in.img, out.img, g, call.stream), "gainmap"));
+}
+
+// ---------------------------------------------------------------- a5-a7 demosaic
+static int demosaic_filter(int algo, halide_buffer_t* const* inputs, size_t n_in, halide_buffer_t* const* outputs,
+                           size_t n_out, const void* blob, size_t blob_size) {
+    CHECK_ARITY(1, 1);
+    if (blob == nullptr || blob_size < sizeof(cpipe_DemosaicParams)) return CPIPE_BAD_INDEX;
+    if (!device_ready()) return CPIPE_INTERNAL_ERROR;
+    Call call;
+    BIND(0, inputs, Kind::BayerF32, false, in);
+    BIND(0, outputs, Kind::Rgba, true, out);
+    REQUIRE_SAME_EXTENT(in, out);
+    const auto* p = static_cast<const cpipe_DemosaicParams*>(blob);
+    const int cfa[4] = {p->cfa_pattern[0], p->cfa_pattern[1], p->cfa_pattern[2], p->cfa_pattern[3]};
+    return call.finish(cuda_status(launch_demosaic(algo, in.img, out.img, out.elem == 2, cfa, call.stream), "demosaic"));
+}
+int cpipe_cuda_demosaic_bilinear(halide_buffer_t* const* i, size_t ni, halide_buffer_t* const* o, size_t no,
+                                 const void* b, size_t bs) {
+    return demosaic_filter(0, i, ni, o, no, b, bs);
+}
+int cpipe_cuda_demosaic_rcd(halide_buffer_t* const* i, size_t ni, halide_buffer_t* const* o, size_t no, const void* b,
+                            size_t bs) {
+    return demosaic_filter(1, i, ni, o, no, b, bs);
+}
+int cpipe_cuda_demosaic_amaze(halide_buffer_t* const* i, size_t ni, halide_buffer_t* const* o, size_t no,
+                              const void* b, size_t bs) {
+    return demosaic_filter(2, i, ni, o, no, b, bs);
+}
+
+// ------------------------------------------------------------ a8 QBC remosaic
+int cpipe_cuda_demosaic_quad_bayer_remosaic(halide_buffer_t* input, halide_buffer_t* output) {
+    if (!device_ready()) return CPIPE_INTERNAL_ERROR;
+    Call call;
+    halide_buffer_t* ins[1] = {input};
+    halide_buffer_t* outs[1] = {output};
+    BIND(0, ins, Kind::BayerU16, false, in);
+    BIND(0, outs, Kind::BayerU16, true, out);
+    REQUIRE_SAME_EXTENT(in, out);
+    return call.finish(cuda_status(launch_qbc_remosaic(in.img, out.img, call.stream), "qbc_remosaic"));
+}
+
+// -------------------------------------------------------- a9/a10 WB, colormatrix
+int cpipe_cuda_wb_dual_illuminant(halide_buffer_t* const* inputs, size_t n_in, halide_buffer_t* const* outputs,
+                                  size_t n_out, const void* blob, size_t blob_size) {
+    CHECK_ARITY(1, 1);
+    if (blob == nullptr || blob_size < sizeof(cpipe_WbParams)) return CPIPE_BAD_INDEX;
+    if (!device_ready()) return CPIPE_INTERNAL_ERROR;
+    Call call;
+    BIND(0, inputs, Kind::Rgba, false, in);
+    BIND(0, outputs, Kind::Rgba, true, out);
+    REQUIRE_SAME_EXTENT(in, out);
+    if (in.elem != out.elem) return call.finish(CPIPE_BAD_PRECISION);
+    const auto* p = static_cast<const cpipe_WbParams*>(blob);
+    return call.finish(cuda_status(launch_wb(in.img, out.img, in.elem == 2, p->as_shot_neutral, call.stream), "wb"));
+}
+int cpipe_cuda_colormatrix_dng_to_working(halide_buffer_t* const* inputs, size_t n_in, halide_buffer_t* const* outputs,
+                                          size_t n_out, const void* blob, size_t blob_size) {
+    CHECK_ARITY(1, 1);
+    if (blob == nullptr || blob_size < sizeof(cpipe_ColormatrixParams)) return CPIPE_BAD_INDEX;
+    if (!device_ready()) return CPIPE_INTERNAL_ERROR;
+    Call call;
+    BIND(0, inputs, Kind::Rgba, false, in);
+    BIND(0, outputs, Kind::Rgba, true, out);
+    REQUIRE_SAME_EXTENT(in, out);
+    if (in.elem != out.elem) return call.finish(CPIPE_BAD_PRECISION);
+    const auto* p = static_cast<const cpipe_ColormatrixParams*>(blob);
+    return call.finish(cuda_status(launch_colormatrix(in.img, out.img, in.elem == 2, p->transform, call.stream), "cm"));
+}
+
+// ---------------------------------------------------------- a11-a13 denoise
+static int rgba_pair(Call& call, halide_buffer_t* const* inputs, halide_buffer_t* const* outputs, Bound* in, Bound* out) {
+    int st = call.bind(inputs[0], Kind::Rgba, false, in);
+    if (st != CPIPE_OK) return st;
+    st = call.bind(outputs[0], Kind::Rgba, true, out);
+    if (st != CPIPE_OK) return st;
+    if (!same_extent(*in, *out)) return CPIPE_BAD_INDEX;
+    if (in->elem != out->elem) return CPIPE_BAD_PRECISION;
+    return CPIPE_OK;
+}
+int cpipe_cuda_denoise_bm3d_step1(halide_buffer_t* const* inputs, size_t n_in, halide_buffer_t* const* outputs,
+                                  size_t n_out, const void* blob, size_t blob_size) {
+    CHECK_ARITY(1, 1);
+    if (blob == nullptr || blob_size < sizeof(cpipe_Bm3dParams)) return CPIPE_BAD_INDEX;
+    if (!device_ready()) return CPIPE_INTERNAL_ERROR;
+    Call call;
+    Bound in, out;
+    const int st = rgba_pair(call, inputs, outputs, &in, &out);
+    if (st != CPIPE_OK) return call.finish(st);
+    const float sigma = static_cast<const cpipe_Bm3dParams*>(blob)->sigma;
+    return call.finish(cuda_status(launch_bm3d_parity(in.img, out.img, in.elem == 2, sigma, call.stream), "bm3d"));
+}
+// bm3d_step2_generator.cpp:33-42: a sigma-aware identity.
+int cpipe_cuda_denoise_bm3d_step2(halide_buffer_t* const* inputs, size_t n_in, halide_buffer_t* const* outputs,
+                                  size_t n_out, const void* blob, size_t blob_size) {
+    CHECK_ARITY(1, 1);
+    if (blob == nullptr || blob_size < sizeof(cpipe_Bm3dParams)) return CPIPE_BAD_INDEX;
+    if (!device_ready()) return CPIPE_INTERNAL_ERROR;
+    Call call;
+    Bound in, out;
+    const int st = rgba_pair(call, inputs, outputs, &in, &out);
+    if (st != CPIPE_OK) return call.finish(st);
+    return call.finish(cuda_status(launch_copy(in.img.data, in.img.row_stride * in.elem, out.img.data,
+                                               out.img.row_stride * out.elem, (long long)in.img.w * 4 * in.elem,
+                                               in.img.h, call.stream),
+                                   "bm3d_step2"));
+}
+int cpipe_cuda_denoise_guided_filter(halide_buffer_t* const* inputs, size_t n_in, halide_buffer_t* const* outputs,
+                                     size_t n_out, const void* blob, size_t blob_size) {
+    CHECK_ARITY(1, 1);
+    if (blob == nullptr || blob_size < sizeof(cpipe_GuidedFilterParams)) return CPIPE_BAD_INDEX;
+    if (!device_ready()) return CPIPE_INTERNAL_ERROR;
+    Call call;
+    Bound in, out;
+    const int st = rgba_pair(call, inputs, outputs, &in, &out);
+    if (st != CPIPE_OK) return call.finish(st);
+    const auto* p = static_cast<const cpipe_GuidedFilterParams*>(blob);
+    return call.finish(
+        cuda_status(launch_guided(in.img, out.img, in.elem == 2, p->radius, p->eps, call.stream), "guided"));
+}
+int cpipe_cuda_denoise_wavelet_bayes_shrink(halide_buffer_t* const* inputs, size_t n_in,
+                                            halide_buffer_t* const* outputs, size_t n_out, const void* blob,
+                                            size_t blob_size) {
+    CHECK_ARITY(1, 1);
+    if (blob == nullptr || blob_size < sizeof(cpipe_WaveletBayesShrinkParams)) return CPIPE_BAD_INDEX;
+    if (!device_ready()) return CPIPE_INTERNAL_ERROR;
+    Call call;
+    Bound in, out;
+    const int st = rgba_pair(call, inputs, outputs, &in, &out);
+    if (st != CPIPE_OK) return call.finish(st);
+    const float strength = static_cast<const cpipe_WaveletBayesShrinkParams*>(blob)->chroma_strength;
+    return call.finish(cuda_status(launch_wavelet(in.img, out.img, in.elem == 2, strength, call.stream), "wavelet"));
+}
+
+// -------------------------------------------------------------- a15 3D LUT
+int cpb_lut_prepare(const void* blob, size_t blob_size, std::vector<float4>* cells, int* S, int* interp) {
+    if (blob == nullptr || blob_size < sizeof(cpipe_Lut3dParamHeader)) return CPIPE_BAD_INDEX;
+    cpipe_Lut3dParamHeader hd;
+    std::memcpy(&hd, blob, sizeof(hd));
+    if (hd.size < 2U || hd.value_count == 0U || (hd.value_count % 3U) != 0U) return CPIPE_BAD_INDEX;
+    if (blob_size != sizeof(hd) + (size_t)hd.value_count * sizeof(float) || hd.size > 256U) return CPIPE_BAD_INDEX;
+    const size_t ncell = (size_t)hd.size * hd.size * hd.size;
+    if ((size_t)hd.value_count / 3U < ncell) return CPIPE_BAD_INDEX;
+    const float* v = reinterpret_cast<const float*>(static_cast<const char*>(blob) + sizeof(hd));
+    cells->resize(ncell);
+    for (size_t i = 0; i < ncell; ++i) (*cells)[i] = make_float4(v[3 * i], v[3 * i + 1], v[3 * i + 2], 0.0F);
+    *S = (int)hd.size;
+    *interp = hd.interpolation == 1U ? 1 : 0;
+    return CPIPE_OK;
+}
+int cpipe_cuda_color_3d_lut(halide_buffer_t* const* inputs, size_t n_in, halide_buffer_t* const* outputs,
+                            size_t n_out, const void* blob, size_t blob_size) {
+    CHECK_ARITY(1, 1);
+    std::vector<float4> cells;
+    int S = 0, interp = 0;
+    const int pst = cpb_lut_prepare(blob, blob_size, &cells, &S, &interp);
+    if (pst != CPIPE_OK) return pst;
+    if (!device_ready()) return CPIPE_INTERNAL_ERROR;
+    Call call;
+    Bound in, out;
+    int st = rgba_pair(call, inputs, outputs, &in, &out);
+    if (st != CPIPE_OK) return call.finish(st);
+    void* d_lut = nullptr;
+    st = call.upload(cells.data(), cells.size() * sizeof(float4), &d_lut);
+    if (st != CPIPE_OK) return call.finish(st);
+    return call.finish(cuda_status(
+        launch_lut3d(in.img, out.img, in.elem == 2, static_cast<const float4*>(d_lut), S, interp, call.stream), "lut"));
+}
+
+// ----------------------------------------------------------------- a16 filmic
+FilmicDev cpb_filmic_dev(const cpipe_FilmicRgbParams* p) {
+    FilmicDev f;
+    f.exposure = std::pow(2.0F, p->ev);
+    f.inv_contrast = 1.0F / p->contrast;
+    f.saturation = p->saturation;
+    f.highlights = p->highlights;
+    f.shadows = p->shadows;
+    f.log_white = (float)std::log(109.0);  // log(1 + 6 * 18), folded by the generator
+    return f;
+}
+int cpipe_cuda_tone_filmic_rgb(halide_buffer_t* const* inputs, size_t n_in, halide_buffer_t* const* outputs,
+                               size_t n_out, const void* blob, size_t blob_size) {
+    CHECK_ARITY(1, 1);
+    if (blob == nullptr || blob_size < sizeof(cpipe_FilmicRgbParams)) return CPIPE_BAD_INDEX;
+    if (!device_ready()) return CPIPE_INTERNAL_ERROR;
+    Call call;
+    Bound in, out;
+    const int st = rgba_pair(call, inputs, outputs, &in, &out);
+    if (st != CPIPE_OK) return call.finish(st);
+    const FilmicDev f = cpb_filmic_dev(static_cast<const cpipe_FilmicRgbParams*>(blob));
+    return call.finish(cuda_status(launch_filmic(in.img, out.img, in.elem == 2, f, call.stream), "filmic"));
+}
+
+// ------------------------------------------------------------ a14 OpcodeList3
+// dng_opcode_list_3_dispatch.cpp:254-398.  Records run in order, each from the
+// previous result; two device scratch images ping-pong between them.
+static double max_corner_distance(double cx, double cy, int w, int h) {
+    const double x1 = (double)(w - 1), y1 = (double)(h - 1);
+    const double d00 = (cx * cx) + (cy * cy), d10 = ((x1 - cx) * (x1 - cx)) + (cy * cy);
+    const double d01 = (cx * cx) + ((y1 - cy) * (y1 - cy)), d11 = ((x1 - cx) * (x1 - cx)) + ((y1 - cy) * (y1 - cy));
+    double m = d00;
+    if (d10 > m) m = d10;
+    if (d01 > m) m = d01;
+    if (d11 > m) m = d11;
+    return std::sqrt(m);
+}
+int cpb_warp_dev(const cpipe_Opcode3DispatchRecord* r, int w, int h, WarpDev* out) {
+    // returns CPIPE_OK when a warp applies, CPIPE_REPLY_DEFAULT for the copy cases
+    if (r->coefficient_count == 0U || w <= 1 || h <= 1) return CPIPE_REPLY_DEFAULT;
+    const double cx = r->cx_hat * (double)(w - 1), cy = r->cy_hat * (double)(h - 1);
+    const double m = max_corner_distance(cx, cy, w, h);
+    if (m <= 2.220446049250313e-16) return CPIPE_REPLY_DEFAULT;
+    out->count = (int)(r->coefficient_count < 4U ? r->coefficient_count : 4U);
+    for (int i = 0; i < out->count; ++i) {
+        const cpipe_Opcode3WarpCoefficient& k = r->coefficients[i];
+        out->k[i] = WarpCoefDev{split(k.kr0), split(k.kr1), split(k.kr2), split(k.kr3), split(k.kt0), split(k.kt1)};
+    }
+    out->cx = split(cx);
+    out->cy = split(cy);
+    out->m = split(m);
+    out->inv_m = split(1.0 / m);
+    out->xmax = (float)(w - 1);
+    out->ymax = (float)(h - 1);
+    return CPIPE_OK;
+}
+int cpb_opcode3_parse(const void* blob, size_t blob_size, Opcode3View* v) {
+    if (blob == nullptr || blob_size < sizeof(cpipe_Opcode3DispatchHeader)) return CPIPE_BAD_INDEX;
+    const char* base = static_cast<const char*>(blob);
+    const auto* hd = reinterpret_cast<const cpipe_Opcode3DispatchHeader*>(base);
+    const size_t rec_bytes = (size_t)hd->opcode_count * sizeof(cpipe_Opcode3DispatchRecord);
+    if (blob_size < sizeof(*hd) + rec_bytes) return CPIPE_BAD_INDEX;
+    const auto* recs = reinterpret_cast<const cpipe_Opcode3DispatchRecord*>(base + sizeof(*hd));
+    size_t npt = 0, nrc = 0;
+    for (uint32_t i = 0; i < hd->opcode_count; ++i) {
+        npt = std::max(npt, (size_t)recs[i].point_offset + recs[i].point_count);
+        nrc = std::max(nrc, (size_t)recs[i].rect_offset + recs[i].rect_count);
+    }
+    const size_t pts_off = sizeof(*hd) + rec_bytes;
+    const size_t rc_off = pts_off + npt * sizeof(cpipe_Opcode3BadPoint);
+    if (blob_size < rc_off + nrc * sizeof(cpipe_Opcode3BadRect)) return CPIPE_BAD_INDEX;
+    v->count = hd->opcode_count;
+    v->records = recs;
+    v->points = reinterpret_cast<const cpipe_Opcode3BadPoint*>(base + pts_off);
+    v->rects = reinterpret_cast<const cpipe_Opcode3BadRect*>(base + rc_off);
+    v->npoints = npt;
+    v->nrects = nrc;
+    return CPIPE_OK;
+}
+int cpb_opcode3_run(Call& call, const Opcode3View& v, const Img& in, const Img& out, int elem) {
+    const bool f16 = elem == 2;
+    const int w = in.w, h = in.h;
+    for (uint32_t i = 0; i < v.count; ++i)
+        if (v.records[i].id != CPIPE_OPCODE3_UNKNOWN && v.records[i].id != CPIPE_OPCODE3_WARP_RECTILINEAR &&
+            v.records[i].id != CPIPE_OPCODE3_FIX_VIGNETTE_RADIAL && v.records[i].id != CPIPE_OPCODE3_FIX_BAD_PIXELS_CONSTANT &&
+            v.records[i].id != CPIPE_OPCODE3_FIX_BAD_PIXELS_LIST && v.records[i].id != CPIPE_OPCODE3_TRIM_BOUNDS)
+            return CPIPE_UNSUPPORTED;
+        else if (v.records[i].id == CPIPE_OPCODE3_UNKNOWN && v.records[i].optional == 0U)
+            return CPIPE_UNSUPPORTED;
+    // Device copies of the point / rect lists.
+    void* d_pts = nullptr;
+    void* d_rects = nullptr;
+    int st = CPIPE_OK;
+    if (v.npoints) st = call.upload(v.points, v.npoints * sizeof(cpipe_Opcode3BadPoint), &d_pts);
+    if (st == CPIPE_OK && v.nrects) st = call.upload(v.rects, v.nrects * sizeof(cpipe_Opcode3BadRect), &d_rects);
+    if (st != CPIPE_OK) return st;
+    // Ping-pong: the working image starts as `in`; every applied opcode writes a
+    // scratch image (or `out` for the last applied one).
+    int last = -1;
+    for (uint32_t i = 0; i < v.count; ++i)
+        if (v.records[i].id != CPIPE_OPCODE3_UNKNOWN) last = (int)i;
+    const long long row_bytes = (long long)w * 4 * elem;
+    if (last < 0) return cuda_status(launch_copy(in.data, in.row_stride * elem, out.data, out.row_stride * elem,
+                                                 row_bytes, h, call.stream), "opcode3 copy");
+    void* tmp[2] = {nullptr, nullptr};
+    Img work = in;
+    int slot = 0;
+    for (uint32_t i = 0; i < v.count; ++i) {
+        const cpipe_Opcode3DispatchRecord& r = v.records[i];
+        if (r.id == CPIPE_OPCODE3_UNKNOWN) continue;
+        Img dst = out;
+        if ((int)i != last) {
+            if (tmp[slot] == nullptr) {
+                st = call.alloc((size_t)w * h * 4 * elem, &tmp[slot]);
+                if (st != CPIPE_OK) return st;
+            }
+            dst = Img{tmp[slot], w, h, (long long)w * 4, 4};
+            slot ^= 1;
+        }
+        cudaError_t e = cudaSuccess;
+        switch (r.id) {
+            case CPIPE_OPCODE3_WARP_RECTILINEAR: {
+                WarpDev wd;
+                if (cpb_warp_dev(&r, w, h, &wd) == CPIPE_OK) e = launch_warp(work, dst, f16, wd, call.stream);
+                else e = launch_copy(work.data, work.row_stride * elem, dst.data, dst.row_stride * elem, row_bytes, h, call.stream);
+                break;
+            }
+            case CPIPE_OPCODE3_FIX_VIGNETTE_RADIAL: {
+                const double cx = r.vignette_cx_hat * (double)(w - 1), cy = r.vignette_cy_hat * (double)(h - 1);
+                const double m = (w <= 1 || h <= 1) ? 0.0 : max_corner_distance(cx, cy, w, h);
+                if (w <= 1 || h <= 1 || m <= 2.220446049250313e-16) {
+                    e = launch_copy(work.data, work.row_stride * elem, dst.data, dst.row_stride * elem, row_bytes, h, call.stream);
+                } else {
+                    VignetteParams vp;
+                    vp.cx = split(cx);
+                    vp.cy = split(cy);
+                    vp.inv_m = split(1.0 / m);
+                    for (int k = 0; k < 5; ++k) vp.k[k] = split(r.vignette_k[k]);
+                    e = launch_vignette(work, dst, f16, vp, call.stream);
+                }
+                break;
+            }
+            case CPIPE_OPCODE3_FIX_BAD_PIXELS_CONSTANT:
+                e = launch_bad_constant(work, dst, f16, (float)r.constant, call.stream);
+                break;
+            case CPIPE_OPCODE3_FIX_BAD_PIXELS_LIST:
+                e = launch_copy(work.data, work.row_stride * elem, dst.data, dst.row_stride * elem, row_bytes, h, call.stream);
+                if (e == cudaSuccess && (r.point_count || r.rect_count))
+                    e = launch_bad_list(work, dst, f16,
+                                        static_cast<const uint32_t*>(d_pts) + 2 * (size_t)r.point_offset, (int)r.point_count,
+                                        static_cast<const uint32_t*>(d_rects) + 4 * (size_t)r.rect_offset, (int)r.rect_count,
+                                        call.stream);
+                break;
+            case CPIPE_OPCODE3_TRIM_BOUNDS:
+                e = launch_trim(work, dst, f16, r.top, r.left, r.bottom, r.right, call.stream);
+                break;
+            default:
+                return CPIPE_UNSUPPORTED;
+        }
+        st = cuda_status(e, "opcode3");
+        if (st != CPIPE_OK) return st;
+        work = dst;
+    }
+    return CPIPE_OK;
+}
+int cpipe_cuda_lens_dng_opcode_list_3(halide_buffer_t* const* inputs, size_t n_in, halide_buffer_t* const* outputs,
+                                      size_t n_out, const void* blob, size_t blob_size) {
+    CHECK_ARITY(1, 1);
+    Opcode3View v;
+    const int pst = cpb_opcode3_parse(blob, blob_size, &v);
+    if (pst != CPIPE_OK) return pst;
+    if (!device_ready()) return CPIPE_INTERNAL_ERROR;
+    Call call;
+    Bound in, out;
+    int st = rgba_pair(call, inputs, outputs, &in, &out);
+    if (st != CPIPE_OK) return call.finish(st);
+    return call.finish(cpb_opcode3_run(call, v, in.img, out.img, in.elem));
+}
+
+// ----------------------------------------------------------- pass-through
+// Device copy used by the node plugins for their pass-through cases (no GainMap,
+// no OpcodeList3, Bayer input to the Quad-Bayer remosaic), in place of the
+// reference's lock_cpu + memcpy.  The blob is ignored.
+int cpipe_cuda_copy(halide_buffer_t* const* inputs, size_t n_in, halide_buffer_t* const* outputs, size_t n_out,
+                    const void* blob, size_t blob_size) {
+    (void)blob;
+    (void)blob_size;
+    CHECK_ARITY(1, 1);
+    if (!device_ready()) return CPIPE_INTERNAL_ERROR;
+    Call call;
+    BIND(0, inputs, Kind::Any, false, in);
+    BIND(0, outputs, Kind::Any, true, out);
+    REQUIRE_SAME_EXTENT(in, out);
+    if (in.elem != out.elem || in.ch != out.ch) return call.finish(CPIPE_BAD_PRECISION);
+    return call.finish(cuda_status(launch_copy(in.img.data, in.img.row_stride * in.elem, out.img.data,
+                                               out.img.row_stride * out.elem, (long long)in.img.w * in.ch * in.elem,
+                                               in.img.h, call.stream),
+                                   "copy"));
+}
+
+// -------------------------------------------------------------- filter table
+static const cpipe_cuda_filter_desc kFilters[] = {
+    {"precision_convert_r16u_to_f32", (void*)&cpipe_cuda_precision_convert_r16u_to_f32, 0},
+    {"precision_convert_f32_to_rgba16f", (void*)&cpipe_cuda_precision_convert_f32_to_rgba16f, 0},
+    {"precision_convert_rgba16f_to_rgba8", (void*)&cpipe_cuda_precision_convert_rgba16f_to_rgba8, 0},
+    {"precision_convert_rgba16f_to_rgba16u", (void*)&cpipe_cuda_precision_convert_rgba16f_to_rgba16u, 0},
+    {"demosaic_quad_bayer_remosaic", (void*)&cpipe_cuda_demosaic_quad_bayer_remosaic, 0},
+    {"linearize_dng_lut", (void*)&cpipe_cuda_linearize_dng_lut, 1},
+    {"blacklevel_dng_levels", (void*)&cpipe_cuda_blacklevel_dng_levels, 1},
+    {"lens_shading_gainmap", (void*)&cpipe_cuda_lens_shading_gainmap, 1},
+    {"demosaic_bilinear", (void*)&cpipe_cuda_demosaic_bilinear, 1},
+    {"demosaic_rcd", (void*)&cpipe_cuda_demosaic_rcd, 1},
+    {"demosaic_amaze", (void*)&cpipe_cuda_demosaic_amaze, 1},
+    {"wb_dual_illuminant", (void*)&cpipe_cuda_wb_dual_illuminant, 1},
+    {"colormatrix_dng_to_working", (void*)&cpipe_cuda_colormatrix_dng_to_working, 1},
+    {"denoise_bm3d_step1", (void*)&cpipe_cuda_denoise_bm3d_step1, 1},
+    {"denoise_bm3d_step2", (void*)&cpipe_cuda_denoise_bm3d_step2, 1},
+    {"denoise_guided_filter", (void*)&cpipe_cuda_denoise_guided_filter, 1},
+    {"denoise_wavelet_bayes_shrink", (void*)&cpipe_cuda_denoise_wavelet_bayes_shrink, 1},
+    {"lens_dng_opcode_list_3", (void*)&cpipe_cuda_lens_dng_opcode_list_3, 1},
+    {"color_3d_lut", (void*)&cpipe_cuda_color_3d_lut, 1},
+    {"tone_filmic_rgb", (void*)&cpipe_cuda_tone_filmic_rgb, 1},
+    {"cpipe_copy", (void*)&cpipe_cuda_copy, 1},
+};
+
+const cpipe_cuda_filter_desc* cpipe_cuda_filters(size_t* count) {
+    if (count) *count = sizeof(kFilters) / sizeof(kFilters[0]);
+    return kFilters;
+}
+const cpipe_cuda_filter_desc* cpipe_cuda_find_filter(const char* aot_id) {
+    if (aot_id == nullptr) return nullptr;
+    for (const auto& f : kFilters)
+        if (std::strcmp(f.aot_id, aot_id) == 0) return &f;
+    return nullptr;
+}
+
+}  // extern "C"

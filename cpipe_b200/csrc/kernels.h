@@ -1,0 +1,43 @@
+// Host-side launch functions of the per-node kernels (kernels_nodes.cu).  These
+// are internal C++ entry points; the public C ABI is in include/cpipe_b200.h.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "common.cuh"
+#include "nodes.cuh"
+
+namespace cpb {
+
+struct VignetteParams {
+    ff cx, cy, inv_m, k[5];
+};
+
+cudaError_t launch_r16u_to_f32(const Img& in, const Img& out, cudaStream_t st);
+cudaError_t launch_linearize(const Img& in, const Img& out, const uint16_t* d_table, int n, cudaStream_t st);
+cudaError_t launch_blacklevel(const Img& in, const Img& out, const BlackDev& p, cudaStream_t st);
+cudaError_t launch_gainmap(const Img& in, const Img& out, const GainMapDev& g, cudaStream_t st);
+cudaError_t launch_copy(const void* src, long long src_pitch, void* dst, long long dst_pitch, long long row_bytes,
+                        int rows, cudaStream_t st);
+cudaError_t launch_demosaic(int algo, const Img& in, const Img& out, bool out_f16, const int cfa[4], cudaStream_t st);
+cudaError_t launch_qbc_remosaic(const Img& in, const Img& out, cudaStream_t st);
+cudaError_t launch_f32_to_rgba16f(const Img& in, const Img& out, cudaStream_t st);
+cudaError_t launch_rgba16f_to_unorm(const Img& in, const Img& out, int bits8, cudaStream_t st);
+cudaError_t launch_wb(const Img& in, const Img& out, bool f16, const float n[3], cudaStream_t st);
+cudaError_t launch_colormatrix(const Img& in, const Img& out, bool f16, const float t[9], cudaStream_t st);
+cudaError_t launch_filmic(const Img& in, const Img& out, bool f16, const FilmicDev& p, cudaStream_t st);
+cudaError_t launch_lut3d(const Img& in, const Img& out, bool f16, const float4* d_lut, int S, int interp,
+                         cudaStream_t st);
+cudaError_t launch_bm3d_parity(const Img& in, const Img& out, bool f16, float sigma, cudaStream_t st);
+cudaError_t launch_wavelet(const Img& in, const Img& out, bool f16, float strength, cudaStream_t st);
+cudaError_t launch_guided(const Img& in, const Img& out, bool f16, int radius, float eps, cudaStream_t st);
+cudaError_t launch_warp(const Img& in, const Img& out, bool f16, const WarpDev& w, cudaStream_t st);
+cudaError_t launch_vignette(const Img& in, const Img& out, bool f16, const VignetteParams& p, cudaStream_t st);
+cudaError_t launch_bad_constant(const Img& in, const Img& out, bool f16, float k, cudaStream_t st);
+cudaError_t launch_bad_list(const Img& in, const Img& out, bool f16, const uint32_t* d_pts, int npts,
+                            const uint32_t* d_rects, int nrects, cudaStream_t st);
+cudaError_t launch_trim(const Img& in, const Img& out, bool f16, uint32_t top, uint32_t left, uint32_t bottom,
+                        uint32_t right, cudaStream_t st);
+
+}  // namespace cpb

@@ -1,0 +1,262 @@
+// Device-side math for every node of the raw->linear chain.  Each function
+// keeps the reference's floating-point operation order (cited per function) so
+// that, with -fmad=false, a kernel built from it reproduces the reference
+// arithmetic; the per-node kernels (kernels_nodes.cu) and the fused chain
+// kernels (chain.cu) share these definitions.
+#pragma once
+
+#include "common.cuh"
+
+namespace cpb {
+
+// ---------------------------------------------------------------- raw domain
+// Black/white scaling with the per-CFA-index constants precomputed on the host
+// exactly as the reference does per pixel (blacklevel_dng_levels_dispatch.cpp:31-45).
+struct BlackDev {
+    float black[4];  // indexed by (y&1)*2 + (x&1)
+    float denom[4];  // float(white_level) - black
+};
+__device__ __forceinline__ float blacklevel_px(float v, int x, int y, const BlackDev& p) {
+    const int i = ((y & 1) * 2) + (x & 1);
+    return clampf((v - p.black[i]) / p.denom[i], 0.0F, 1.0F);
+}
+
+// GainMap: axis samples are evaluated on the host in double, exactly as
+// sample_axis (shading_gainmap_dispatch.cpp:23-36), and stored per column / row.
+struct AxisSample {
+    uint32_t low, high;
+    float weight;
+};
+struct GainMapDev {
+    int map_count;
+    int qbc;                   // 4x4 CFA repeat: plane from (y%4)/2, (x%4)/2
+    int plane_to_map[4];       // -1 when no map covers that plane
+    const float* gains[4];     // per map, row-major map_points_v x map_points_h
+    int points_h[4];
+    const AxisSample* cols[4]; // per map, w entries
+    const AxisSample* rows[4]; // per map, h entries
+};
+__device__ __forceinline__ float lerpf(float a, float b, float t) { return a + ((b - a) * t); }
+__device__ __forceinline__ int gain_map_index(int x, int y, const GainMapDev& g) {
+    if (g.map_count == 1) return 0;
+    int plane = ((y & 1) * 2) + (x & 1);
+    if (g.qbc) plane = (((y % 4) / 2) * 2) + ((x % 4) / 2);
+    return g.plane_to_map[plane];
+}
+__device__ __forceinline__ float gain_px(int m, int x, int y, const GainMapDev& g) {
+    const AxisSample sy = g.rows[m][y];
+    const AxisSample sx = g.cols[m][x];
+    const float* gm = g.gains[m];
+    const int rs = g.points_h[m];
+    const float g00 = __ldg(gm + sy.low * rs + sx.low), g10 = __ldg(gm + sy.low * rs + sx.high);
+    const float g01 = __ldg(gm + sy.high * rs + sx.low), g11 = __ldg(gm + sy.high * rs + sx.high);
+    return lerpf(lerpf(g00, g10, sx.weight), lerpf(g01, g11, sx.weight), sy.weight);
+}
+
+// ----------------------------------------------------------------- demosaic
+// The three demosaics read a shared-memory tile `t` holding the clamped input
+// (repeat_edge) with a fixed halo; `T(dx,dy)` addresses it relative to the
+// pixel being evaluated.  cfa_at uses unclamped coordinates, as the generator's
+// cfa_at(x, y) = cfa_pattern((y & 1) * 2 + (x & 1)) does.
+struct Cfa {
+    int p[4];
+    __device__ __forceinline__ int at(int x, int y) const { return p[((y & 1) * 2) + (x & 1)]; }
+};
+
+// demosaic_rcd_generator.cpp:28-35
+template <class Tap>
+__device__ __forceinline__ float rcd_green(const Tap& T, int x, int y, const Cfa& cfa) {
+    const float c = T(0, 0);
+    const float gh = 0.5F * (T(-1, 0) + T(1, 0));
+    const float gv = 0.5F * (T(0, -1) + T(0, 1));
+    const float dh = fabsf(T(-2, 0) - T(2, 0));
+    const float dv = fabsf(T(0, -2) - T(0, 2));
+    if (cfa.at(x, y) == 1) return c;
+    if (dh < dv) return gh;
+    if (dv < dh) return gv;
+    return 0.5F * (gh + gv);
+}
+// demosaic_amaze_generator.cpp:24-46
+template <class Tap>
+__device__ __forceinline__ float amaze_green(const Tap& T, int x, int y, const Cfa& cfa) {
+    const float c = T(0, 0);
+    if (cfa.at(x, y) == 1) return c;
+    const float ct = 2.0F * c;
+    const float ghn = T(-1, 0) + T(1, 0);
+    const float gvn = T(0, -1) + T(0, 1);
+    const float ghs = ct - T(-2, 0) - T(2, 0);
+    const float gvs = ct - T(0, -2) - T(0, 2);
+    const float gh = (0.5F * ghn) + (0.25F * ghs);
+    const float gv = (0.5F * gvn) + (0.25F * gvs);
+    const float grh = fabsf(T(-1, 0) - T(1, 0)) + fabsf(T(-2, 0) - c) + fabsf(T(2, 0) - c);
+    const float grv = fabsf(T(0, -1) - T(0, 1)) + fabsf(T(0, -2) - c) + fabsf(T(0, 2) - c);
+    if (grh < grv) return gh;
+    if (grv < grh) return gv;
+    return 0.5F * (gh + gv);
+}
+
+// ------------------------------------------------------------ RGBA pixel ops
+// wb_dual_illuminant_dispatch.cpp:31-45: rgb / AsShotNeutral, alpha copied.
+__device__ __forceinline__ Rgba wb_px(Rgba v, const float n[3]) {
+    return Rgba{v.r / n[0], v.g / n[1], v.b / n[2], v.a};
+}
+// colormatrix_dng_to_working_dispatch.cpp:33-50
+__device__ __forceinline__ Rgba cm_px(Rgba v, const float t[9]) {
+    return Rgba{t[0] * v.r + t[1] * v.g + t[2] * v.b, t[3] * v.r + t[4] * v.g + t[5] * v.b,
+                t[6] * v.r + t[7] * v.g + t[8] * v.b, v.a};
+}
+
+// filmic_rgb_generator.cpp:22-36,57-70.  exposure = pow(2, ev) and
+// inv_contrast = 1/contrast are computed once per launch on the host with the
+// same float operations; log_white = log(109) is the generator's constant.
+struct FilmicDev {
+    float exposure, inv_contrast, saturation, highlights, shadows, log_white;
+};
+__device__ __forceinline__ float filmic_tone(float value, const FilmicDev& p) {
+    const float e = max0(value * p.exposure);
+    const float curved = clampf(logf(1.0F + (6.0F * e)) / p.log_white, 0.0F, 1.0F);
+    const float v = powf(max0(curved), p.inv_contrast);
+    const float sd = (p.shadows - 1.0F) * 0.08F * (1.0F - v) * (1.0F - v);
+    const float hd = (p.highlights - 1.0F) * 0.08F * v * v;
+    return clampf(v + sd + hd, 0.0F, 1.0F);
+}
+__device__ __forceinline__ Rgba filmic_px(Rgba v, const FilmicDev& p) {
+    const float t0 = filmic_tone(v.r, p), t1 = filmic_tone(v.g, p), t2 = filmic_tone(v.b, p);
+    const float luma = (0.2126F * t0) + (0.7152F * t1) + (0.0722F * t2);
+    return Rgba{clampf(luma + ((t0 - luma) * p.saturation), 0.0F, 1.0F),
+                clampf(luma + ((t1 - luma) * p.saturation), 0.0F, 1.0F),
+                clampf(luma + ((t2 - luma) * p.saturation), 0.0F, 1.0F), v.a};
+}
+
+// lut3d_generator.cpp:49-138.  The LUT is stored as float4 (r,g,b,0) per cell,
+// cell index ((r*S + g)*S + b), blue fastest (reference color/lut3d_generator.cpp:83-86).
+__device__ __forceinline__ float add_delta(float base, float from, float to, float w) {
+    return base + ((to - from) * w);
+}
+__device__ __forceinline__ float4 add_delta4(float4 base, float4 from, float4 to, float w) {
+    return make_float4(add_delta(base.x, from.x, to.x, w), add_delta(base.y, from.y, to.y, w),
+                       add_delta(base.z, from.z, to.z, w), 0.0F);
+}
+__device__ __forceinline__ float4 lerp4(float4 a, float4 b, float t) {
+    return make_float4(a.x + ((b.x - a.x) * t), a.y + ((b.y - a.y) * t), a.z + ((b.z - a.z) * t), 0.0F);
+}
+__device__ __forceinline__ Rgba lut_px(Rgba v, const float4* __restrict__ lut, int S, int interp) {
+    const float mi = (float)(S - 1);
+    const float rs = clampf(v.r, 0.0F, 1.0F) * mi;
+    const float gs = clampf(v.g, 0.0F, 1.0F) * mi;
+    const float bs = clampf(v.b, 0.0F, 1.0F) * mi;
+    const int r0 = clampi((int)floorf(rs), 0, S - 2);
+    const int g0 = clampi((int)floorf(gs), 0, S - 2);
+    const int b0 = clampi((int)floorf(bs), 0, S - 2);
+    const float dr = rs - (float)r0, dg = gs - (float)g0, db = bs - (float)b0;
+    const int base = (r0 * S + g0) * S + b0;
+    const int sr = S * S, sg = S;
+    const float4 c000 = __ldg(lut + base);
+    const float4 c111 = __ldg(lut + base + sr + sg + 1);
+    float4 o;
+    if (interp == 1) {
+        const float4 c100 = __ldg(lut + base + sr), c010 = __ldg(lut + base + sg);
+        const float4 c001 = __ldg(lut + base + 1), c110 = __ldg(lut + base + sr + sg);
+        const float4 c101 = __ldg(lut + base + sr + 1), c011 = __ldg(lut + base + sg + 1);
+        const float4 c00 = lerp4(c000, c100, dr), c10 = lerp4(c010, c110, dr);
+        const float4 c01 = lerp4(c001, c101, dr), c11 = lerp4(c011, c111, dr);
+        const float4 c0 = lerp4(c00, c10, dg), c1 = lerp4(c01, c11, dg);
+        o = lerp4(c0, c1, db);
+    } else {
+        // Tetrahedral: the first matching branch of the generator's select chain;
+        // each branch reads only the two intermediate corners it walks through.
+        int s1, s2;
+        float w1, w2, w3;
+        if (dr >= dg && dg >= db) { s1 = sr; s2 = sr + sg; w1 = dr; w2 = dg; w3 = db; }
+        else if (dr >= db && db >= dg) { s1 = sr; s2 = sr + 1; w1 = dr; w2 = db; w3 = dg; }
+        else if (db >= dr && dr >= dg) { s1 = 1; s2 = sr + 1; w1 = db; w2 = dr; w3 = dg; }
+        else if (dg >= dr && dr >= db) { s1 = sg; s2 = sr + sg; w1 = dg; w2 = dr; w3 = db; }
+        else if (dg >= db && db >= dr) { s1 = sg; s2 = sg + 1; w1 = dg; w2 = db; w3 = dr; }
+        else { s1 = 1; s2 = sg + 1; w1 = db; w2 = dg; w3 = dr; }
+        const float4 ca = __ldg(lut + base + s1), cb = __ldg(lut + base + s2);
+        o = add_delta4(add_delta4(add_delta4(c000, c000, ca, w1), ca, cb, w2), cb, c111, w3);
+    }
+    return Rgba{clampf(o.x, 0.0F, 1.0F), clampf(o.y, 0.0F, 1.0F), clampf(o.z, 0.0F, 1.0F), v.a};
+}
+
+// bm3d_step1_generator.cpp:42-56 (parity form): blend toward the aligned 2x2 mean.
+__device__ __forceinline__ float bm3d_blend(float v, float p00, float p10, float p01, float p11, float s) {
+    const float basic = (p00 + p10 + p01 + p11) * 0.25F;
+    return max0((v * (1.0F - s)) + (basic * s));
+}
+
+// wavelet_bayes_shrink_generator.cpp:9-31,63-85
+__device__ __forceinline__ float soft_th(float v, float t) {
+    return v > t ? v - t : (v < -t ? v + t : 0.0F);
+}
+struct HaarBand { float ll, h, v, d; };
+__device__ __forceinline__ HaarBand haar_shrink(float p00, float p10, float p01, float p11, float th) {
+    HaarBand b;
+    b.ll = 0.25F * (p00 + p10 + p01 + p11);
+    b.h = soft_th(0.25F * (p00 - p10 + p01 - p11), th);
+    b.v = soft_th(0.25F * (p00 + p10 - p01 - p11), th);
+    b.d = soft_th(0.25F * (p00 - p10 - p01 + p11), th);
+    return b;
+}
+__device__ __forceinline__ float haar_pick(const HaarBand& b, int ox, int oy) {
+    if (ox == 0 && oy == 0) return b.ll + b.h + b.v + b.d;
+    if (ox == 1 && oy == 0) return b.ll - b.h + b.v - b.d;
+    if (ox == 0 && oy == 1) return b.ll + b.h - b.v - b.d;
+    return b.ll - b.h - b.v + b.d;
+}
+__device__ __forceinline__ float wv_co(Rgba p) { return p.r - p.b; }
+__device__ __forceinline__ float wv_cg(Rgba p) { return p.g - ((p.r + p.b) * 0.5F); }
+// Output for pixel (ox, oy) of the aligned 2x2 block q[0..3] = (0,0),(1,0),(0,1),(1,1).
+__device__ __forceinline__ Rgba wavelet_px(const Rgba q[4], int ox, int oy, float th) {
+    const HaarBand bco = haar_shrink(wv_co(q[0]), wv_co(q[1]), wv_co(q[2]), wv_co(q[3]), th);
+    const HaarBand bcg = haar_shrink(wv_cg(q[0]), wv_cg(q[1]), wv_cg(q[2]), wv_cg(q[3]), th);
+    const Rgba p = q[oy * 2 + ox];
+    const float luma = (p.r + (2.0F * p.g) + p.b) * 0.25F;
+    const float co = haar_pick(bco, ox, oy), cg = haar_pick(bcg, ox, oy);
+    const float t = luma - (0.5F * cg);
+    return Rgba{max0(t + (0.5F * co)), max0(t + cg), max0(t - (0.5F * co)), max0(p.a)};
+}
+
+// --------------------------------------------------------------- OpcodeList3
+// Catmull-Rom cubic (dng_opcode_list_3_dispatch.cpp:48-53).
+__device__ __forceinline__ float cubic(float p0, float p1, float p2, float p3, float t) {
+    const float a0 = (-0.5F * p0) + (1.5F * p1) - (1.5F * p2) + (0.5F * p3);
+    const float a1 = p0 - (2.5F * p1) + (2.0F * p2) - (0.5F * p3);
+    const float a2 = (-0.5F * p0) + (0.5F * p2);
+    return (((a0 * t) + a1) * t + a2) * t + p1;
+}
+__device__ __forceinline__ Rgba cubic4(Rgba p0, Rgba p1, Rgba p2, Rgba p3, float t) {
+    return Rgba{cubic(p0.r, p1.r, p2.r, p3.r, t), cubic(p0.g, p1.g, p2.g, p3.g, t),
+                cubic(p0.b, p1.b, p2.b, p3.b, t), cubic(p0.a, p1.a, p2.a, p3.a, t)};
+}
+
+// Warp coefficients converted to float-float on the host.
+struct WarpCoefDev {
+    ff kr0, kr1, kr2, kr3, kt0, kt1;
+};
+struct WarpDev {
+    int count;  // 1..4 coefficient sets; channel c uses min(c, count-1)
+    WarpCoefDev k[4];
+    ff cx, cy, m, inv_m;
+    float xmax, ymax;  // w-1, h-1
+};
+// Source coordinate of output pixel (x, y) for coefficient set k
+// (dng_opcode_list_3_dispatch.cpp:103-115), in float-float.
+__device__ __forceinline__ void warp_src(const WarpDev& w, const WarpCoefDev& k, ff dx, ff dy, ff r2,
+                                         ff r4, ff r6, ff* sx, ff* sy) {
+    const ff f = ff_add(ff_add(ff_add(k.kr0, ff_mul(k.kr1, r2)), ff_mul(k.kr2, r4)), ff_mul(k.kr3, r6));
+    const ff two = ff_from(2.0F);
+    const ff dxdy = ff_mul(dx, dy);
+    const ff tx = ff_add(ff_mul(ff_mul(two, k.kt0), dxdy), ff_mul(k.kt1, ff_add(r2, ff_mul(ff_mul(two, dx), dx))));
+    const ff ty = ff_add(ff_mul(k.kt0, ff_add(r2, ff_mul(ff_mul(two, dy), dy))), ff_mul(ff_mul(two, k.kt1), dxdy));
+    *sx = ff_add(w.cx, ff_mul(w.m, ff_add(ff_mul(f, dx), tx)));
+    *sy = ff_add(w.cy, ff_mul(w.m, ff_add(ff_mul(f, dy), ty)));
+}
+// Clamp a float-float coordinate to [0, maxv] (sample_bicubic :57-58).
+__device__ __forceinline__ ff ff_clamp0(ff v, float maxv) {
+    if (v.hi < 0.0F || (v.hi == 0.0F && v.lo < 0.0F)) return ff_from(0.0F);
+    if (v.hi > maxv || (v.hi == maxv && v.lo > 0.0F)) return ff_from(maxv);
+    return v;
+}
+
+}  // namespace cpb

@@ -1,0 +1,173 @@
+/* libcpipe_b200: B200 (sm_100a) CUDA implementation of the cpipe raw->linear
+ * node chain, behind the reference's own plugin and filter interfaces.
+ *
+ * Three layers, each a drop-in at the boundary a reference integration binds:
+ *
+ *  1. Filter seam -- one function per reference aot_id with the reference's
+ *     filter signatures (src/cpipe/runtime/HalideFilterRegistry.hpp:18-21):
+ *       HalideParamFilterEntry  int(halide_buffer_t* const*, size_t,
+ *                                   halide_buffer_t* const*, size_t,
+ *                                   const void* param_blob, size_t blob_size)
+ *       HalideFilterEntry       int(halide_buffer_t* input, halide_buffer_t* output)
+ *     A reference runtime registers them per aot_id with
+ *     ComputeContext::register_halide_[param_]filter (ComputeContext.cpp:16-23).
+ *     Param blobs are the reference PODs (cpipe_b200_params.h).  A buffer whose
+ *     `device` field is non-zero is CUDA device memory processed in place,
+ *     asynchronously on the thread's current stream; any other buffer is staged
+ *     through device memory and the call returns when the host buffer holds the
+ *     result.  Return values are cpipe_status_t codes with the reference's
+ *     meaning; CUDA failures are CPIPE_INTERNAL_ERROR (message in
+ *     cpipe_cuda_last_error()).  There is no CPU path.
+ *
+ *  2. Node plugins -- one cpipe_plugin_desc_t per reference node id, placed in
+ *     the ELF section `cpipe_registry` (reference include/cpipe/sdk/registry.hpp:17-32)
+ *     and also listed by cpipe_b200_node_descs().  Their main_entry does the
+ *     reference node's host-side work (metadata checks, WB CCT search,
+ *     colormatrix composition, OpcodeList2/3 parsing, .cube loading) and submits
+ *     the CUDA filter through the host's compute suite.
+ *
+ *  3. A small host runtime (cpipe_b200_host_*) implementing the reference host
+ *     suites over device-resident buffers, used by tests, benchmarks and hosts
+ *     without their own runtime; and the fused chain (cpipe_cuda_chain_*).
+ */
+#ifndef CPIPE_B200_H
+#define CPIPE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "cpipe_b200_params.h"
+#include "cpipe_halide_abi.h"
+#include "cpipe_node_abi.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------- stream / status */
+/* Stream used by filter calls made from this thread (a cudaStream_t; NULL = legacy default stream). */
+int cpipe_cuda_set_stream(void* cuda_stream);
+void* cpipe_cuda_get_stream(void);
+int cpipe_cuda_synchronize(void);
+const char* cpipe_cuda_last_error(void);
+int cpipe_cuda_device_count(void);
+
+/* ------------------------------------------------------------------ filter seam */
+/* precision_convert_generator.cpp:31-124, registered in precision_convert_dispatch.cpp */
+int cpipe_cuda_precision_convert_r16u_to_f32(halide_buffer_t* input, halide_buffer_t* output);
+int cpipe_cuda_precision_convert_f32_to_rgba16f(halide_buffer_t* input, halide_buffer_t* output);
+int cpipe_cuda_precision_convert_rgba16f_to_rgba8(halide_buffer_t* input, halide_buffer_t* output);
+int cpipe_cuda_precision_convert_rgba16f_to_rgba16u(halide_buffer_t* input, halide_buffer_t* output);
+/* demosaic_quad_bayer_remosaic_dispatch.cpp:6-8 */
+int cpipe_cuda_demosaic_quad_bayer_remosaic(halide_buffer_t* input, halide_buffer_t* output);
+
+#define CPIPE_CUDA_PARAM_FILTER(name)                                                         \
+    int name(halide_buffer_t* const* inputs, size_t n_inputs, halide_buffer_t* const* outputs, \
+             size_t n_outputs, const void* param_blob, size_t param_blob_size)
+CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_linearize_dng_lut);          /* linearize_dng_lut_dispatch.cpp:17-51 */
+CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_blacklevel_dng_levels);      /* blacklevel_dng_levels_dispatch.cpp:16-47 */
+CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_lens_shading_gainmap);       /* shading_gainmap_dispatch.cpp:73-133 */
+CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_demosaic_bilinear);          /* demosaic_bilinear_dispatch.cpp */
+CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_demosaic_rcd);               /* demosaic_rcd_dispatch.cpp:19-38 */
+CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_demosaic_amaze);             /* demosaic_amaze_dispatch.cpp */
+CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_wb_dual_illuminant);         /* wb_dual_illuminant_dispatch.cpp:16-48 */
+CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_colormatrix_dng_to_working); /* colormatrix_dng_to_working_dispatch.cpp:17-62 */
+CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_denoise_bm3d_step1);         /* bm3d_dispatch.cpp:19-30 */
+CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_denoise_bm3d_step2);         /* bm3d_dispatch.cpp:32-43 */
+CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_denoise_guided_filter);      /* guided_filter_dispatch.cpp */
+CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_denoise_wavelet_bayes_shrink); /* wavelet_bayes_shrink_dispatch.cpp */
+CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_lens_dng_opcode_list_3);     /* dng_opcode_list_3_dispatch.cpp:333-398 */
+CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_color_3d_lut);               /* lut3d_dispatch.cpp:20-60 */
+CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_tone_filmic_rgb);            /* filmic_rgb_dispatch.cpp:22-36 */
+/* Device copy for pass-through cases (aot_id "cpipe_copy"); replaces the lock_cpu
+ * memcpy of e.g. shading_gainmap.cpp:50-75.  No reference filter counterpart. */
+CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_copy);
+
+/* Registration table: entry is a HalideParamFilterEntry when takes_params != 0,
+ * else a HalideFilterEntry. */
+typedef struct {
+    const char* aot_id;
+    void* entry;
+    int takes_params;
+} cpipe_cuda_filter_desc;
+const cpipe_cuda_filter_desc* cpipe_cuda_filters(size_t* count);
+const cpipe_cuda_filter_desc* cpipe_cuda_find_filter(const char* aot_id);
+
+/* ----------------------------------------------------------------- node plugins */
+/* Every node descriptor of this library (the same records are in `cpipe_registry`). */
+const cpipe_plugin_desc_t* cpipe_b200_node_descs(size_t* count);
+const cpipe_plugin_desc_t* cpipe_b200_find_node(const char* node_id);
+
+/* ---------------------------------------------------- host-side parameter prep */
+/* Dual-illuminant WB: CCT search + matrix blend (wb_dual_illuminant.cpp:79-282,352-367).
+ * fm1/fm2 may be NULL (ColorMatrix blend inverted instead). */
+int cpipe_b200_wb_prepare(const float neutral[3], const float cm1[9], const float cm2[9], const float* fm1,
+                          const float* fm2, uint16_t illuminant1, uint16_t illuminant2, cpipe_WbParams* out,
+                          double* scene_cct);
+/* XYZ(D65)->Rec.2020 * Bradford D50->D65 * camera->XYZ(D50) (colormatrix_dng_to_working.cpp:20-28,125). */
+int cpipe_b200_colormatrix_compose(const float camera_to_xyz_d50[9], float out[9]);
+/* OpcodeList2 GainMap parse + pack (OpcodeList2.cpp:94-176, shading_gainmap.cpp:80-137).
+ * *blob_size: capacity in, bytes needed out. */
+int cpipe_b200_pack_gain_maps(const void* opcode_list_2, size_t n, const uint8_t cfa_repeat[2],
+                              const uint8_t cfa_pattern[16], void* blob, size_t* blob_size);
+/* OpcodeList3 parse + pack (OpcodeList3.cpp:83-296, dng_opcode_list_3.cpp:75-168). */
+int cpipe_b200_pack_opcode_list_3(const void* opcode_list_3, size_t n, void* blob, size_t* blob_size,
+                                  uint32_t* opcode_count);
+/* .cube / .spi3d loader (Cube3dLutLoader.cpp:57-204); values NULL queries *size. */
+int cpipe_b200_load_lut(const char* path, uint32_t* size, float* values, size_t capacity);
+
+/* ----------------------------------------------------------------- host runtime */
+typedef struct cpipe_b200_host cpipe_b200_host;
+typedef struct cpipe_b200_buffer cpipe_b200_buffer;
+typedef struct cpipe_b200_params cpipe_b200_params;
+
+cpipe_b200_host* cpipe_b200_host_create(void);
+void cpipe_b200_host_destroy(cpipe_b200_host* host);
+cpipe_host_t* cpipe_b200_host_abi(cpipe_b200_host* host);
+/* Device allocation cap for buffers and scratch of this host (0 = none);
+ * allocations past it fail with CPIPE_OOM (reference Pipeline.cpp:587-592). */
+int cpipe_b200_host_set_memory_cap(cpipe_b200_host* host, uint64_t bytes);
+
+/* Image2D buffer in device memory; format is a CPIPE_FMT_* value. */
+cpipe_b200_buffer* cpipe_b200_buffer_create(cpipe_b200_host* host, int format, uint32_t width, uint32_t height);
+void cpipe_b200_buffer_destroy(cpipe_b200_buffer* buffer);
+int cpipe_b200_buffer_upload(cpipe_b200_buffer* buffer, const void* host_data, size_t bytes);
+int cpipe_b200_buffer_download(cpipe_b200_buffer* buffer, void* host_data, size_t bytes);
+void* cpipe_b200_buffer_device_ptr(cpipe_b200_buffer* buffer);
+const cpipe_buffer_t* cpipe_b200_buffer_abi(cpipe_b200_buffer* buffer);
+
+/* Buffer metadata (what the reference BufferMetadata carries for this path). */
+int cpipe_b200_buffer_set_cfa(cpipe_b200_buffer* b, const uint8_t repeat[2], const uint8_t pattern[16]);
+int cpipe_b200_buffer_set_levels(cpipe_b200_buffer* b, const float black[4], uint32_t white);
+int cpipe_b200_buffer_set_matrix(cpipe_b200_buffer* b, int which, const float m[9]); /* 1,2 color; 3,4 forward */
+int cpipe_b200_buffer_set_illuminants(cpipe_b200_buffer* b, uint16_t illuminant1, uint16_t illuminant2);
+int cpipe_b200_buffer_set_linearization_table(cpipe_b200_buffer* b, const uint16_t* values, size_t n);
+int cpipe_b200_buffer_set_noise_profile(cpipe_b200_buffer* b, const float* beta, const float* lambda, size_t n);
+int cpipe_b200_buffer_set_as_shot_neutral(cpipe_b200_buffer* b, const float rgb[3]);
+int cpipe_b200_buffer_set_cs_role(cpipe_b200_buffer* b, const char* role);
+int cpipe_b200_buffer_add_applied_step(cpipe_b200_buffer* b, const char* step);
+int cpipe_b200_buffer_set_blob(cpipe_b200_buffer* b, const char* key, const void* data, size_t size);
+int cpipe_b200_buffer_has_applied_step(cpipe_b200_buffer* b, const char* step);
+const char* cpipe_b200_buffer_cs_role(cpipe_b200_buffer* b);
+int cpipe_b200_buffer_get_blob(cpipe_b200_buffer* b, const char* key, const void** data, size_t* size);
+int cpipe_b200_buffer_get_cfa(cpipe_b200_buffer* b, int* has_cfa, uint8_t repeat[2], uint8_t pattern[16]);
+
+cpipe_b200_params* cpipe_b200_params_create(void);
+void cpipe_b200_params_destroy(cpipe_b200_params* p);
+int cpipe_b200_params_set_double(cpipe_b200_params* p, const char* key, double value);
+int cpipe_b200_params_set_string(cpipe_b200_params* p, const char* key, const char* value);
+int cpipe_b200_params_set_bool(cpipe_b200_params* p, const char* key, int value);
+
+/* create -> process -> destroy one node on the host's stream, then freeze the
+ * metadata builder into each output (reference Pipeline.cpp:704-787 per node).
+ * Synchronises before returning. */
+int cpipe_b200_run_node(cpipe_b200_host* host, const char* node_id, const cpipe_b200_params* params,
+                        cpipe_b200_buffer* const* inputs, size_t n_in, cpipe_b200_buffer* const* outputs,
+                        size_t n_out);
+const char* cpipe_b200_host_last_error(cpipe_b200_host* host);
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* CPIPE_B200_H */

@@ -1,0 +1,172 @@
+/* Parameter blobs passed through `submit_halide_with_params` to each filter.
+ *
+ * Every struct is byte-compatible with the POD the reference node packs for its
+ * filter, so a reference host can hand the same blob to the CUDA filter:
+ *   LinearizeParamsHeader .. Opcode3BadRect  src/cpipe/nodes/detail/P1ParamDispatch.hpp:10-104
+ *   Lut3dParamHeader                          src/cpipe/nodes/color/Lut3dParams.hpp:10-14
+ *   Bm3dParams                                src/cpipe/nodes/denoise/bm3d_dispatch.cpp:12-14
+ *   GuidedFilterParams                        src/cpipe/nodes/denoise/guided_filter_dispatch.cpp:13-16
+ *   WaveletBayesShrinkParams                  src/cpipe/nodes/denoise/wavelet_bayes_shrink_dispatch.cpp:12-14
+ *   FilmicRgbParams                           src/cpipe/nodes/tone/filmic_rgb_dispatch.cpp:12-18
+ * The static size checks at the end pin the layouts (x86-64 / aarch64 LP64).
+ */
+#ifndef CPIPE_B200_PARAMS_H
+#define CPIPE_B200_PARAMS_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+    uint32_t table_size; /* followed by table_size uint16 entries */
+} cpipe_LinearizeParamsHeader;
+
+typedef struct {
+    float black_level[4];
+    uint32_t white_level;
+    uint8_t cfa_pattern[4];
+} cpipe_BlacklevelParams;
+
+typedef struct {
+    uint8_t cfa_pattern[4];
+} cpipe_DemosaicParams;
+
+typedef struct {
+    float as_shot_neutral[3];
+    float camera_to_xyz_d50[9];
+    float scene_cct;
+    float dual_illuminant_weight;
+} cpipe_WbParams;
+
+typedef struct {
+    float transform[9];
+} cpipe_ColormatrixParams;
+
+typedef struct {
+    uint32_t map_count;
+    uint8_t cfa_repeat[2];
+    uint8_t cfa_pattern[16];
+} cpipe_GainMapDispatchHeader;
+
+typedef struct {
+    uint32_t top;
+    uint32_t left;
+    uint32_t bottom;
+    uint32_t right;
+    uint32_t plane;
+    uint32_t planes;
+    uint32_t map_points_v;
+    uint32_t map_points_h;
+    double map_spacing_v;
+    double map_spacing_h;
+    double map_origin_v;
+    double map_origin_h;
+    uint32_t gain_offset;
+    uint32_t gain_count;
+} cpipe_GainMapDispatchPlane;
+
+typedef struct {
+    uint32_t opcode_count;
+    uint32_t reserved;
+} cpipe_Opcode3DispatchHeader;
+
+typedef struct {
+    double kr0;
+    double kr1;
+    double kr2;
+    double kr3;
+    double kt0;
+    double kt1;
+} cpipe_Opcode3WarpCoefficient;
+
+typedef struct {
+    uint32_t id;
+    uint32_t optional;
+    uint32_t coefficient_count;
+    cpipe_Opcode3WarpCoefficient coefficients[4];
+    double cx_hat;
+    double cy_hat;
+    double vignette_k[5];
+    double vignette_cx_hat;
+    double vignette_cy_hat;
+    uint32_t constant;
+    uint32_t bayer_phase;
+    uint32_t point_offset;
+    uint32_t point_count;
+    uint32_t rect_offset;
+    uint32_t rect_count;
+    uint32_t top;
+    uint32_t left;
+    uint32_t bottom;
+    uint32_t right;
+} cpipe_Opcode3DispatchRecord;
+
+typedef struct {
+    uint32_t row;
+    uint32_t column;
+} cpipe_Opcode3BadPoint;
+
+typedef struct {
+    uint32_t top;
+    uint32_t left;
+    uint32_t bottom;
+    uint32_t right;
+} cpipe_Opcode3BadRect;
+
+/* Opcode ids as packed into cpipe_Opcode3DispatchRecord::id
+ * (reference src/cpipe/nodes/lens/dng_opcode_list_3_dispatch.cpp:26-31). */
+enum {
+    CPIPE_OPCODE3_UNKNOWN = 0,
+    CPIPE_OPCODE3_WARP_RECTILINEAR = 1,
+    CPIPE_OPCODE3_FIX_VIGNETTE_RADIAL = 3,
+    CPIPE_OPCODE3_FIX_BAD_PIXELS_CONSTANT = 4,
+    CPIPE_OPCODE3_FIX_BAD_PIXELS_LIST = 5,
+    CPIPE_OPCODE3_TRIM_BOUNDS = 6
+};
+
+typedef struct {
+    uint32_t size;
+    uint32_t value_count;
+    uint32_t interpolation; /* 0 tetrahedral, 1 trilinear */
+} cpipe_Lut3dParamHeader;
+
+typedef struct {
+    float sigma;
+} cpipe_Bm3dParams;
+
+typedef struct {
+    int32_t radius;
+    float eps;
+} cpipe_GuidedFilterParams;
+
+typedef struct {
+    float chroma_strength;
+} cpipe_WaveletBayesShrinkParams;
+
+typedef struct {
+    float ev;
+    float contrast;
+    float saturation;
+    float highlights;
+    float shadows;
+} cpipe_FilmicRgbParams;
+
+#if defined(__cplusplus)
+#define CPIPE_STATIC_ASSERT static_assert
+#else
+#define CPIPE_STATIC_ASSERT _Static_assert
+#endif
+CPIPE_STATIC_ASSERT(sizeof(cpipe_BlacklevelParams) == 24, "BlacklevelParams layout");
+CPIPE_STATIC_ASSERT(sizeof(cpipe_WbParams) == 56, "WbParams layout");
+CPIPE_STATIC_ASSERT(sizeof(cpipe_GainMapDispatchHeader) == 24, "GainMapDispatchHeader layout");
+CPIPE_STATIC_ASSERT(sizeof(cpipe_GainMapDispatchPlane) == 72, "GainMapDispatchPlane layout");
+CPIPE_STATIC_ASSERT(sizeof(cpipe_Opcode3DispatchRecord) == 320, "Opcode3DispatchRecord layout");
+CPIPE_STATIC_ASSERT(sizeof(cpipe_Lut3dParamHeader) == 12, "Lut3dParamHeader layout");
+
+#ifdef __cplusplus
+} /* extern "C" */
+#endif
+
+#endif /* CPIPE_B200_PARAMS_H */
