@@ -1,0 +1,301 @@
+"""Benchmark: 12 MP ms/frame of the classic raw->linear chain on B200.
+
+One step = the fused chain (convert, black level, GainMap, RCD, OpcodeList3
+warp, WB, colormatrix, BM3D, guided, wavelet, filmic, 3D LUT) over one
+4032x3024 10-bit RGGB frame already resident in HBM.  Frames rotate through a
+ring of 8 raw inputs (195 MB) and 2 outputs (195 MB), so no step reads its
+input from L2.  Timing: CUDA events on the chain's stream around exactly K
+steps, bracketed by a barrier and a stream synchronize; max over ranks.  The
+`e2e` figure runs the same chain through the C-ABI host entry point
+(cpipe_cuda_chain_run_host: pinned raw frame H2D, chain, RGBA16F D2H).
+
+Multi-GPU: frames are independent, so N GPUs run N replicas on their own
+frames (no collective on the data path); `value` = whole-job ms per frame.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+"""
+import argparse
+import ctypes as C
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "12MP ms/frame, classic raw->linear chain (parity form)"
+BYTES_PER_PX = {"raw_to_rgba": 10, "warp_wb_cm": 16, "denoise_tone": 16}  # algorithmic HBM bytes
+KERNELS = ["raw_to_rgba", "warp_wb_cm", "denoise_tone"]
+
+
+def measured_peak_gbs():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def traffic_per_launch(kernel):
+    """DRAM bytes per launch from the committed ncu summary, or None."""
+    path = os.path.join(ROOT, "profiles", "traffic_full_chain_12mp.json")
+    try:
+        with open(path) as f:
+            return json.load(f)["dram_bytes_per_launch"].get(kernel)
+    except Exception:
+        return None
+
+
+class ClockSampler:
+    """nvidia-smi samples of SM clock and throttle reasons during the timed region."""
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device):
+        self.device = device
+        self.proc = None
+        self.out = tempfile.NamedTemporaryFile("w+", suffix=".csv", delete=False)
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}",
+                                          "--format=csv,noheader,nounits", "-lms", "100"],
+                                         stdout=self.out, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.2)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        self.out.flush()
+        rows = []
+        with open(self.out.name) as f:
+            for line in f:
+                parts = [p.strip() for p in line.split(",")]
+                if len(parts) == 7:
+                    rows.append(parts)
+        os.unlink(self.out.name)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[0]) for r in rows if r[0].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[3 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": float(rows[0][1]) if rows[0][1].replace(".", "").isdigit() else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+def cpu_chain_ms(cfg_small, scale, repeats=1):
+    """Time the CPU chain (oracle restatement of the reference nodes) on a
+    sample frame; returns ms per 12 MP frame (area-scaled) and the sample."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    from chain_oracle import run_chain_oracle
+    raw = cfg_small.make_raw()
+    b = cfg_small.blobs()
+    times = []
+    for _ in range(repeats):
+        t0 = time.perf_counter()
+        run_chain_oracle(cfg_small, raw, blobs=b)
+        times.append(time.perf_counter() - t0)
+    return 1000.0 * min(times) * scale
+
+
+def reference_arm(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    from cpipe_b200.chain import ChainConfig
+    cores = os.cpu_count()
+    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
+    full = ChainConfig.full_12mp()
+    sample = ChainConfig.full_12mp(width=1008, height=756, name="sample_1008x756")
+    scale = (full.width * full.height) / (sample.width * sample.height)
+    for _ in range(args.warmup):
+        cpu_chain_ms(sample, scale)
+    vals = [cpu_chain_ms(sample, scale) for _ in range(args.steps)]
+    v = statistics.median(vals)
+    line = {"impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "ms/frame", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(v, 3), "higher_is_better": False,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Philox scene)",
+            "config": {"workload": full.name, "sample": sample.name},
+            "cpu_baseline": {"value": round(v, 3), "unit": "ms/frame", "cores": cores, "kind": "port",
+                             "sample": f"one {sample.width}x{sample.height} frame of the same chain per step, "
+                                       f"scaled x{scale:.0f} by area; C restatement of the reference nodes "
+                                       "(plain-C++ filters single-threaded as in the reference, Halide "
+                                       "restatements OpenMP over rows)"},
+            "e2e": {"value": round(v, 3), "unit": "ms/frame", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def b200_arm(args):
+    import numpy as np
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    dist = None
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    from cpipe_b200 import _abi as A
+    from cpipe_b200.chain import Chain, ChainConfig
+    L = A.lib()
+    assert L.cpipe_cuda_set_device(local) == 0, "no CUDA device"
+
+    def barrier():
+        if dist is not None:
+            import torch
+            dist.barrier(device_ids=[local])
+            torch.cuda.synchronize()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        import torch
+        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    cfg = ChainConfig.full_12mp(seed=0x5EED0002 + 1000 * rank)
+    w, h = cfg.width, cfg.height
+    base = cfg.make_raw()
+    ring = [np.ascontiguousarray(np.roll(base, (2 * k, 4 * k), axis=(0, 1))) for k in range(8)]
+    raw_bytes = base.nbytes
+    out_bytes = w * h * 8
+    d_raw, d_out = [], []
+    for fr in ring:
+        p = C.c_void_p()
+        assert L.cpipe_cuda_device_alloc(raw_bytes, C.byref(p)) == 0
+        assert L.cpipe_cuda_memcpy_h2d(p, fr.ctypes.data, raw_bytes) == 0
+        d_raw.append(p.value)
+    for _ in range(2):
+        p = C.c_void_p()
+        assert L.cpipe_cuda_device_alloc(out_bytes, C.byref(p)) == 0
+        d_out.append(p.value)
+    stream = C.c_void_p()
+    assert L.cpipe_cuda_stream_create(C.byref(stream)) == 0
+    chain = Chain(cfg)
+    ev0, ev1 = C.c_void_p(), C.c_void_p()
+    L.cpipe_cuda_event_create(C.byref(ev0))
+    L.cpipe_cuda_event_create(C.byref(ev1))
+
+    for i in range(args.warmup):
+        chain.run(d_raw[i % 8], d_out[i % 2], stream)
+    L.cpipe_cuda_stream_synchronize(stream)
+    L.cpipe_cuda_chain_set_profiling(chain._h, 1)
+
+    with ClockSampler(local) as clocks:
+        # keep the GPU busy while the sampler starts, then time exactly K steps
+        for i in range(max(args.warmup, 3)):
+            chain.run(d_raw[i % 8], d_out[i % 2], stream)
+        L.cpipe_cuda_stream_synchronize(stream)
+        ms_k = (C.c_double * 3)()
+        nfr = C.c_int32()
+        L.cpipe_cuda_chain_profile(chain._h, ms_k, C.byref(nfr))  # discard the extra warm-up frames
+        barrier()
+        L.cpipe_cuda_stream_synchronize(stream)
+        L.cpipe_cuda_event_record(ev0, stream)
+        for i in range(args.steps):
+            chain.run(d_raw[i % 8], d_out[i % 2], stream)
+        L.cpipe_cuda_event_record(ev1, stream)
+        L.cpipe_cuda_stream_synchronize(stream)
+        barrier()
+        ms = C.c_float()
+        L.cpipe_cuda_event_elapsed_ms(ev0, ev1, C.byref(ms))
+        L.cpipe_cuda_chain_profile(chain._h, ms_k, C.byref(nfr))
+        # end-to-end through the host entry point: pinned frames in and out
+        L.cpipe_cuda_chain_set_profiling(chain._h, 0)
+        e2e_steps = max(3, min(args.steps, 20))
+        h_raw = C.c_void_p()
+        h_out = C.c_void_p()
+        assert L.cpipe_cuda_pinned_alloc(raw_bytes, C.byref(h_raw)) == 0
+        assert L.cpipe_cuda_pinned_alloc(out_bytes, C.byref(h_out)) == 0
+        C.memmove(h_raw, ring[0].ctypes.data, raw_bytes)
+        st = L.cpipe_cuda_chain_run_host(chain._h, h_raw, h_out, stream)
+        assert st == 0, st
+        barrier()
+        t0 = time.perf_counter()
+        for i in range(e2e_steps):
+            L.cpipe_cuda_chain_run_host(chain._h, h_raw, h_out, stream)
+        e2e_s = time.perf_counter() - t0
+        barrier()
+    clk = clocks.summary()
+
+    total_ms = max_over_ranks(float(ms.value))
+    e2e_ms = max_over_ranks(e2e_s * 1000.0)
+    per_kernel = {k: ms_k[i] / max(1, nfr.value) for i, k in enumerate(KERNELS)}
+    value = total_ms / (args.steps * world)
+    dominant = max(per_kernel, key=per_kernel.get)
+    peak, peak_kind = measured_peak_gbs()
+    alg_bytes = BYTES_PER_PX[dominant] * w * h
+    achieved = alg_bytes / (per_kernel[dominant] * 1e-3) / 1e9
+    traffic = traffic_per_launch(dominant)
+    line = {
+        "metric": METRIC, "value": round(value, 4), "unit": "ms/frame", "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": False,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Philox scene)",
+        "config": {"workload": cfg.name, "frame": f"{w}x{h} RGGB 10-bit", "mode": "parity (RGBA16F between nodes)",
+                   "nodes": ["precision_convert", "blacklevel", "gainmap 17x13", "demosaic.rcd",
+                             "opcode_list_3 warp", "wb.dual_illuminant", "colormatrix", "bm3d", "guided r8",
+                             "wavelet", "filmic", "3d_lut 33^3"],
+                   "l2": "inputs larger than L2: ring of 8 raw frames (195 MB) and 2 output frames",
+                   "parallelism": f"replicas x{world}"},
+        "per_kernel_ms": {k: round(v, 4) for k, v in per_kernel.items()},
+        "roofline": {"bound": "hbm", "kernel": dominant, "achieved": round(achieved, 1), "peak": peak,
+                     "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                     "algorithmic_bytes": alg_bytes, "traffic": traffic},
+        "chain_roofline": {"achieved": round(sum(BYTES_PER_PX.values()) * w * h / (total_ms / args.steps * 1e-3) / 1e9,
+                                             1), "unit": "GB/s", "bytes_per_px": sum(BYTES_PER_PX.values())},
+        "e2e": {"value": round(e2e_ms / (e2e_steps * world), 4), "unit": "ms/frame", "h2d_bytes_per_step": raw_bytes,
+                "d2h_bytes_per_step": out_bytes},
+        "clocks": clk,
+        "gpu_launches": 3 * args.steps,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        sample = ChainConfig.full_12mp(width=2016, height=1512, name="sample_2016x1512")
+        scale = (w * h) / (sample.width * sample.height)
+        os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
+        v = cpu_chain_ms(sample, scale)
+        line["cpu_baseline"] = {"value": round(v, 1), "unit": "ms/frame", "cores": os.cpu_count(), "kind": "port",
+                                "sample": "one 2016x1512 frame of the same chain, scaled x4 by area; C "
+                                          "restatement of the reference nodes (plain-C++ filters single-threaded "
+                                          "as in the reference, Halide restatements OpenMP over rows)"}
+    chain.close()
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return reference_arm(args)
+    return b200_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

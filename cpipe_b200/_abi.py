@@ -105,6 +105,16 @@ class FilmicRgbParams(C.Structure):
     _fields_ = [(n, C.c_float) for n in ("ev", "contrast", "saturation", "highlights", "shadows")]
 
 
+class ChainConfig(C.Structure):
+    _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("black", BlacklevelParams),
+                ("gainmap_blob", C.c_void_p), ("gainmap_blob_size", C.c_size_t), ("demosaic", C.c_int32),
+                ("opcode3_blob", C.c_void_p), ("opcode3_blob_size", C.c_size_t),
+                ("as_shot_neutral", C.c_float * 3), ("colormatrix", C.c_float * 9), ("bm3d_sigma", C.c_float),
+                ("guided_radius", C.c_int32), ("guided_eps", C.c_float), ("wavelet_strength", C.c_float),
+                ("filmic", FilmicRgbParams), ("lut_blob", C.c_void_p), ("lut_blob_size", C.c_size_t),
+                ("plain_f32", C.c_int32), ("use_graph", C.c_int32)]
+
+
 MAIN_ENTRY = C.CFUNCTYPE(C.c_int, C.c_char_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p)
 
 
@@ -147,6 +157,12 @@ EXPORTS = [
     "cpipe_b200_params_create", "cpipe_b200_params_destroy", "cpipe_b200_params_set_double",
     "cpipe_b200_params_set_string", "cpipe_b200_params_set_bool", "cpipe_b200_run_node",
     "cpipe_b200_host_last_error",
+    "cpipe_cuda_chain_create", "cpipe_cuda_chain_destroy", "cpipe_cuda_chain_output_bytes", "cpipe_cuda_chain_run",
+    "cpipe_cuda_chain_run_host", "cpipe_cuda_pinned_alloc", "cpipe_cuda_pinned_free",
+    "cpipe_cuda_chain_set_profiling", "cpipe_cuda_chain_profile", "cpipe_cuda_set_device", "cpipe_cuda_device_alloc",
+    "cpipe_cuda_device_free", "cpipe_cuda_memcpy_h2d", "cpipe_cuda_memcpy_d2h", "cpipe_cuda_stream_create",
+    "cpipe_cuda_stream_destroy", "cpipe_cuda_stream_synchronize", "cpipe_cuda_event_create",
+    "cpipe_cuda_event_destroy", "cpipe_cuda_event_record", "cpipe_cuda_event_elapsed_ms",
 ]
 
 _lib = None
@@ -196,6 +212,19 @@ def lib():
         "cpipe_b200_pack_gain_maps": (i32, [vp, sz, vp, vp, vp, C.POINTER(sz)]),
         "cpipe_b200_pack_opcode_list_3": (i32, [vp, sz, vp, C.POINTER(sz), C.POINTER(u32)]),
         "cpipe_b200_load_lut": (i32, [cp, C.POINTER(u32), vp, sz]),
+        "cpipe_cuda_chain_create": (vp, [C.POINTER(ChainConfig), C.POINTER(i32)]),
+        "cpipe_cuda_chain_destroy": (None, [vp]), "cpipe_cuda_chain_output_bytes": (sz, [vp]),
+        "cpipe_cuda_chain_run": (i32, [vp, vp, vp, vp]), "cpipe_cuda_chain_run_host": (i32, [vp, vp, vp, vp]),
+        "cpipe_cuda_pinned_alloc": (i32, [sz, C.POINTER(vp)]), "cpipe_cuda_pinned_free": (None, [vp]),
+        "cpipe_cuda_chain_set_profiling": (i32, [vp, i32]),
+        "cpipe_cuda_chain_profile": (i32, [vp, C.POINTER(C.c_double), C.POINTER(i32)]),
+        "cpipe_cuda_set_device": (i32, [i32]), "cpipe_cuda_device_alloc": (i32, [sz, C.POINTER(vp)]),
+        "cpipe_cuda_device_free": (None, [vp]), "cpipe_cuda_memcpy_h2d": (i32, [vp, vp, sz]),
+        "cpipe_cuda_memcpy_d2h": (i32, [vp, vp, sz]), "cpipe_cuda_stream_create": (i32, [C.POINTER(vp)]),
+        "cpipe_cuda_stream_destroy": (None, [vp]), "cpipe_cuda_stream_synchronize": (i32, [vp]),
+        "cpipe_cuda_event_create": (i32, [C.POINTER(vp)]), "cpipe_cuda_event_destroy": (None, [vp]),
+        "cpipe_cuda_event_record": (i32, [vp, vp]),
+        "cpipe_cuda_event_elapsed_ms": (i32, [vp, vp, C.POINTER(C.c_float)]),
     }
     for name, (res, args) in sigs.items():
         f = getattr(L, name)

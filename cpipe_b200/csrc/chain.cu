@@ -1,0 +1,672 @@
+// The fused raw->linear chain: the reference node sequence
+//   precision_convert(r16u->f32) -> blacklevel -> GainMap -> demosaic ->
+//   OpcodeList3 -> WB -> colormatrix -> BM3D -> guided -> wavelet -> filmic -> 3D LUT
+// in three kernels instead of twelve launches and eleven intermediate frames:
+//
+//   K1 raw_to_rgba   u16 Bayer tile (+3 halo) -> convert/black/gain in shared
+//                    memory -> demosaic -> RGBA            (2 B/px in, 8 B/px out)
+//   K2 warp_wb_cm    OpcodeList3 warp (bicubic gather from K1's frame) -> WB ->
+//                    colormatrix, per pixel               (8 B/px in, 8 B/px out)
+//   K3 denoise_tone  BM3D (parity form) -> guided -> wavelet -> filmic -> LUT on a
+//                    shared-memory tile with the halo the guided box-of-boxes
+//                    and the 2x2 blocks need             (8 B/px in, 8 B/px out)
+//
+// Every node boundary keeps the reference storage rounding (binary16 for the
+// RGBA nodes; none in the FP32 plain form), so the fused result equals running
+// the nodes one by one.  OpcodeList3 lists other than a single WarpRectilinear
+// run through the per-node OpcodeList3 path between K1 and a WB+colormatrix K2.
+#include <cstring>
+#include <vector>
+
+#include "../../include/cpipe_b200.h"
+#include "filters_impl.h"
+#include "kernels.h"
+#include "nodes.cuh"
+
+namespace cpb {
+namespace {
+
+// ------------------------------------------------------------------ K1
+constexpr int kATW = 64, kATH = 16, kAHalo = 3;
+constexpr int kAIW = kATW + 2 * kAHalo, kAIH = kATH + 2 * kAHalo;
+constexpr int kAGW = kATW + 2, kAGH = kATH + 2;
+
+struct RawParams {
+    BlackDev black;
+    GainMapDev gain;
+    int has_gain;
+    Cfa cfa;
+};
+
+struct TapA {
+    const float* base;
+    __device__ __forceinline__ float operator()(int dx, int dy) const { return base[dy * kAIW + dx]; }
+};
+
+template <int ALGO, class TOut>
+__global__ void __launch_bounds__(256) raw_to_rgba_kernel(Img raw, Img out, RawParams p) {
+    __shared__ float s_in[kAIH * kAIW];
+    __shared__ float s_g[kAGH * kAGW];
+    const int x0 = blockIdx.x * kATW, y0 = blockIdx.y * kATH;
+    // precision_convert -> blacklevel -> GainMap at each clamped coordinate
+    for (int i = threadIdx.x; i < kAIH * kAIW; i += blockDim.x) {
+        const int ty = i / kAIW, tx = i - ty * kAIW;
+        const int gx = clampi(x0 - kAHalo + tx, 0, raw.w - 1), gy = clampi(y0 - kAHalo + ty, 0, raw.h - 1);
+        float v = (float)*px<const uint16_t>(raw, gx, gy);
+        v = blacklevel_px(v, gx, gy, p.black);
+        if (p.has_gain) v = v * gain_px(gain_map_index(gx, gy, p.gain), gx, gy, p.gain);
+        s_in[i] = v;
+    }
+    __syncthreads();
+    if (ALGO != 0) {
+        for (int i = threadIdx.x; i < kAGH * kAGW; i += blockDim.x) {
+            const int ty = i / kAGW, tx = i - ty * kAGW;
+            const TapA T{s_in + (ty + kAHalo - 1) * kAIW + (tx + kAHalo - 1)};
+            s_g[i] = ALGO == 1 ? rcd_green(T, x0 - 1 + tx, y0 - 1 + ty, p.cfa) : amaze_green(T, x0 - 1 + tx, y0 - 1 + ty, p.cfa);
+        }
+        __syncthreads();
+    }
+    for (int i = threadIdx.x; i < kATH * kATW; i += blockDim.x) {
+        const int ty = i / kATW, tx = i - ty * kATW;
+        const int x = x0 + tx, y = y0 + ty;
+        if (x >= out.w || y >= out.h) continue;
+        const float* c = s_in + (ty + kAHalo) * kAIW + (tx + kAHalo);
+        const TapA T{c};
+        const float ctr = c[0];
+        const int site = p.cfa.at(x, y);
+        const bool red = site == 0, blue = site == 2;
+        const bool hred = p.cfa.at(x - 1, y) == 0, hblue = p.cfa.at(x - 1, y) == 2;
+        float r, g, b;
+        if (ALGO == 0) {
+            const float hz = 0.5F * (T(-1, 0) + T(1, 0));
+            const float vt = 0.5F * (T(0, -1) + T(0, 1));
+            const float cross = 0.25F * (T(-1, 0) + T(1, 0) + T(0, -1) + T(0, 1));
+            const float diag = 0.25F * (T(-1, -1) + T(1, -1) + T(-1, 1) + T(1, 1));
+            r = red ? ctr : blue ? diag : hred ? hz : vt;
+            g = (red || blue) ? cross : ctr;
+            b = blue ? ctr : red ? diag : hred ? vt : hz;
+        } else {
+            const float* G = s_g + (ty + 1) * kAGW + (tx + 1);
+#define GG(dx, dy) G[(dy) * kAGW + (dx)]
+            const float gc = GG(0, 0);
+            if (ALGO == 1) {
+#define RT(dx, dy) (T(dx, dy) / maxf(GG(dx, dy), 0.000001F))
+                const float rh = gc * 0.5F * (RT(-1, 0) + RT(1, 0));
+                const float rv = gc * 0.5F * (RT(0, -1) + RT(0, 1));
+                const float rd = gc * 0.25F * (RT(-1, -1) + RT(1, -1) + RT(-1, 1) + RT(1, 1));
+#undef RT
+                r = max0(red ? ctr : blue ? rd : hred ? rh : rv);
+                g = max0(gc);
+                b = max0(blue ? ctr : red ? rd : hblue ? rh : rv);
+            } else {
+#define CH(dx, dy) (T(dx, dy) - GG(dx, dy))
+                const float chh = 0.5F * (CH(-1, 0) + CH(1, 0));
+                const float chv = 0.5F * (CH(0, -1) + CH(0, 1));
+                const float chd = 0.25F * (CH(-1, -1) + CH(1, -1) + CH(-1, 1) + CH(1, 1));
+#undef CH
+                const float rh = gc + chh, rv = gc + chv, rd = gc + chd;
+                r = max0(red ? ctr : (blue ? rd : hred ? rh : rv));
+                g = max0(gc);
+                b = max0(blue ? ctr : (red ? rd : hblue ? rh : rv));
+            }
+#undef GG
+        }
+        store_rgba(px<TOut>(out, x, y), Rgba{r, g, b, 1.0F});
+    }
+}
+
+// ------------------------------------------------------------------ K2
+struct ColorParams {
+    float neutral[3];
+    float cm[9];
+};
+
+template <class T, bool F16, bool WARP>
+__global__ void __launch_bounds__(128) warp_wb_cm_kernel(Img in, Img out, WarpDev w, ColorParams cp) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= out.w) return;
+    Rgba v;
+    if (WARP) {
+        const ff dx = ff_mul(ff_sub(ff_from((float)x), w.cx), w.inv_m);
+        const ff dy = ff_mul(ff_sub(ff_from((float)y), w.cy), w.inv_m);
+        const ff r2 = ff_add(ff_mul(dx, dx), ff_mul(dy, dy));
+        const ff r4 = ff_mul(r2, r2), r6 = ff_mul(r4, r2);
+        float res[4];
+        int done_for = -1;
+        Rgba last{};
+        for (int c = 0; c < 4; ++c) {
+            const int ci = c < w.count - 1 ? c : w.count - 1;
+            if (ci != done_for) {
+                ff sx, sy;
+                warp_src(w, w.k[ci], dx, dy, r2, r4, r6, &sx, &sy);
+                sx = ff_clamp0(sx, w.xmax);
+                sy = ff_clamp0(sy, w.ymax);
+                const int ix = ff_floor(sx), iy = ff_floor(sy);
+                const float tx = ff_frac(sx, ix), ty = ff_frac(sy, iy);
+                Rgba rows[4];
+#pragma unroll
+                for (int r = 0; r < 4; ++r) {
+                    const int yy = iy + r - 1;
+                    rows[r] = cubic4(load_clamped<T>(in, ix - 1, yy), load_clamped<T>(in, ix, yy),
+                                     load_clamped<T>(in, ix + 1, yy), load_clamped<T>(in, ix + 2, yy), tx);
+                }
+                last = cubic4(rows[0], rows[1], rows[2], rows[3], ty);
+                done_for = ci;
+            }
+            res[c] = c == 0 ? last.r : c == 1 ? last.g : c == 2 ? last.b : last.a;
+        }
+        v = Rgba{rnd<F16>(res[0]), rnd<F16>(res[1]), rnd<F16>(res[2]), rnd<F16>(res[3])};
+    } else {
+        v = load_rgba(px<const T>(in, x, y));
+    }
+    Rgba b = wb_px(v, cp.neutral);
+    b = Rgba{rnd<F16>(b.r), rnd<F16>(b.g), rnd<F16>(b.b), v.a};
+    const Rgba c = cm_px(b, cp.cm);
+    store_rgba(px<T>(out, x, y), Rgba{c.r, c.g, c.b, v.a});
+}
+
+// ------------------------------------------------------------------ K3
+// Tile TW x TH; R = guided box radius (1 or 2).  Shared-memory planes (3 colour
+// channels each), indexed by unclamped coordinate relative to the tile origin:
+//   s_cm : colormatrix output at clamp(coord), coords [x0-2R, x0+TW+2R)
+//   s_bm : BM3D output at clamp(coord), same extent
+//   s_a/s_b : guided a, b at coords [x0-R, x0+TW+R)
+//   s_gf : guided output for the tile (needed whole for the wavelet 2x2 blocks)
+// The BM3D 2x2 block of a clamped coordinate xc is (xc & ~1, min(xc|1, w-1)),
+// always inside the s_cm extent because x0 and 2R are even.
+constexpr int kCTW = 32, kCTH = 16;
+
+template <class S>
+struct Plane;
+template <>
+struct Plane<__half> {
+    __device__ static float get(const __half* p, int i) { return __half2float(p[i]); }
+    __device__ static void put(__half* p, int i, float v) { p[i] = __float2half_rn(v); }
+};
+template <>
+struct Plane<float> {
+    __device__ static float get(const float* p, int i) { return p[i]; }
+    __device__ static void put(float* p, int i, float v) { p[i] = v; }
+};
+
+struct ToneParams {
+    int has_wavelet;
+    float bm3d_strength;
+    float eps;
+    float wavelet_th;
+    FilmicDev filmic;
+    const float4* lut;
+    int lut_size, lut_interp;
+    int has_lut;
+};
+
+template <class T, bool F16, int R>
+__global__ void __launch_bounds__(256) denoise_tone_kernel(Img in, Img out, ToneParams p) {
+    using S = typename std::conditional<F16, __half, float>::type;  // storage of rounded planes
+    constexpr int H = 2 * R;
+    constexpr int CW = kCTW + 2 * H, CH = kCTH + 2 * H;  // cm / bm3d extent
+    constexpr int AW = kCTW + 2 * R, AH = kCTH + 2 * R;  // a / b extent (unused when R == 0)
+    extern __shared__ __align__(16) unsigned char smem[];
+    S* s_cm = reinterpret_cast<S*>(smem);
+    S* s_bm = s_cm + 3 * CW * CH;
+    float* s_a = reinterpret_cast<float*>(s_bm + 3 * CW * CH);
+    float* s_b = s_a + 3 * AW * AH;
+    S* s_gf = reinterpret_cast<S*>(s_b + 3 * AW * AH);
+    const int x0 = blockIdx.x * kCTW, y0 = blockIdx.y * kCTH;
+    const int cx0 = x0 - H, cy0 = y0 - H;
+    // 1) colormatrix output at clamped coordinates
+    for (int i = threadIdx.x; i < CW * CH; i += blockDim.x) {
+        const int ty = i / CW, tx = i - ty * CW;
+        const Rgba v = load_clamped<T>(in, cx0 + tx, cy0 + ty);
+        Plane<S>::put(s_cm, i, v.r);
+        Plane<S>::put(s_cm, CW * CH + i, v.g);
+        Plane<S>::put(s_cm, 2 * CW * CH + i, v.b);
+    }
+    __syncthreads();
+    // 2) BM3D parity form at clamped coordinates
+    for (int i = threadIdx.x; i < CW * CH; i += blockDim.x) {
+        const int ty = i / CW, tx = i - ty * CW;
+        const int xc = clampi(cx0 + tx, 0, in.w - 1), yc = clampi(cy0 + ty, 0, in.h - 1);
+        const int bx = xc & ~1, by = yc & ~1;
+        const int bx1 = min(bx + 1, in.w - 1), by1 = min(by + 1, in.h - 1);
+        const int l00 = (by - cy0) * CW + (bx - cx0), l10 = (by - cy0) * CW + (bx1 - cx0);
+        const int l01 = (by1 - cy0) * CW + (bx - cx0), l11 = (by1 - cy0) * CW + (bx1 - cx0);
+        const int lc = (yc - cy0) * CW + (xc - cx0);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const S* P = s_cm + c * CW * CH;
+            const float o = bm3d_blend(Plane<S>::get(P, lc), Plane<S>::get(P, l00), Plane<S>::get(P, l10),
+                                       Plane<S>::get(P, l01), Plane<S>::get(P, l11), p.bm3d_strength);
+            Plane<S>::put(s_bm, c * CW * CH + i, o);
+        }
+    }
+    __syncthreads();
+    // 3) guided a, b at unclamped coordinates [x0-R, x0+TW+R)
+    constexpr float N = (float)((2 * R + 1) * (2 * R + 1));
+    if (R == 0) {  // no guided node: the wavelet reads the BM3D output
+        for (int i = threadIdx.x; i < 3 * kCTW * kCTH; i += blockDim.x) {
+            const int c = i / (kCTW * kCTH);
+            const int j = i - c * kCTW * kCTH;
+            const int ty = j / kCTW, tx = j - ty * kCTW;
+            Plane<S>::put(s_gf, i, Plane<S>::get(s_bm, c * CW * CH + ty * CW + tx));
+        }
+    }
+    for (int i = threadIdx.x; R > 0 && i < 3 * AW * AH; i += blockDim.x) {
+        const int c = i / (AW * AH);
+        const int j = i - c * AW * AH;
+        const int ty = j / AW, tx = j - ty * AW;
+        const S* V = s_bm + c * CW * CH + (ty + R) * CW + (tx + R);
+        float sm = 0.0F, sq = 0.0F;
+        bool first = true;
+#pragma unroll
+        for (int dy = -R; dy <= R; ++dy)
+#pragma unroll
+            for (int dx = -R; dx <= R; ++dx) {
+                const float t = Plane<S>::get(V, dy * CW + dx);
+                if (R == 1 && first) { sm = t; sq = t * t; first = false; }
+                else { sm = sm + t; sq = sq + (t * t); }
+            }
+        const float m = sm / N, corr = sq / N;
+        const float var = max0(corr - (m * m));
+        const float a = var / (var + p.eps);
+        s_a[i] = a;
+        s_b[i] = m - (a * m);
+    }
+    __syncthreads();
+    // 4) guided output for the tile
+    for (int i = threadIdx.x; R > 0 && i < 3 * kCTW * kCTH; i += blockDim.x) {
+        const int c = i / (kCTW * kCTH);
+        const int j = i - c * kCTW * kCTH;
+        const int ty = j / kCTW, tx = j - ty * kCTW;
+        const float* A = s_a + c * AW * AH + (ty + R) * AW + (tx + R);
+        const float* B = s_b + c * AW * AH + (ty + R) * AW + (tx + R);
+        float sa = 0.0F, sb = 0.0F;
+        bool first = true;
+#pragma unroll
+        for (int dy = -R; dy <= R; ++dy)
+#pragma unroll
+            for (int dx = -R; dx <= R; ++dx) {
+                if (R == 1 && first) { sa = A[dy * AW + dx]; sb = B[dy * AW + dx]; first = false; }
+                else { sa = sa + A[dy * AW + dx]; sb = sb + B[dy * AW + dx]; }
+            }
+        const float v = Plane<S>::get(s_bm, c * CW * CH + (ty + H) * CW + (tx + H));
+        Plane<S>::put(s_gf, c * kCTW * kCTH + j, max0(((sa / N) * v) + (sb / N)));
+    }
+    __syncthreads();
+    // 5) wavelet on the aligned 2x2 block, filmic, LUT; one thread per pixel
+    for (int j = threadIdx.x; j < kCTW * kCTH; j += blockDim.x) {
+        const int ty = j / kCTW, tx = j - ty * kCTW;
+        const int x = x0 + tx, y = y0 + ty;
+        if (x >= out.w || y >= out.h) continue;
+        const int bx = x & ~1, by = y & ~1;
+        const int xs[2] = {bx - x0, min(bx + 1, out.w - 1) - x0};
+        const int ys[2] = {by - y0, min(by + 1, out.h - 1) - y0};
+        Rgba q[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int l = ys[k >> 1] * kCTW + xs[k & 1];
+            q[k] = Rgba{Plane<S>::get(s_gf, l), Plane<S>::get(s_gf, kCTW * kCTH + l),
+                        Plane<S>::get(s_gf, 2 * kCTW * kCTH + l), 0.0F};
+        }
+        // alpha runs through unchanged except the wavelet's max(0, .)
+        const float alpha = load_rgba(px<const T>(in, x, y)).a;
+        q[(y & 1) * 2 + (x & 1)].a = alpha;
+        Rgba v = q[(y & 1) * 2 + (x & 1)];
+        if (p.has_wavelet) {
+            v = wavelet_px(q, x & 1, y & 1, p.wavelet_th);
+            v = Rgba{rnd<F16>(v.r), rnd<F16>(v.g), rnd<F16>(v.b), rnd<F16>(v.a)};
+        }
+        v = filmic_px(v, p.filmic);
+        if (p.has_lut) {
+            v = Rgba{rnd<F16>(v.r), rnd<F16>(v.g), rnd<F16>(v.b), v.a};
+            v = lut_px(v, p.lut, p.lut_size, p.lut_interp);
+        }
+        store_rgba(px<T>(out, x, y), v);
+    }
+}
+
+template <class T, bool F16, int R>
+size_t denoise_tone_smem() {
+    using S = typename std::conditional<F16, __half, float>::type;
+    constexpr int H = 2 * R;
+    constexpr int CW = kCTW + 2 * H, CH = kCTH + 2 * H;
+    constexpr int AW = kCTW + 2 * R, AH = kCTH + 2 * R;
+    size_t s = 2 * 3 * CW * CH * sizeof(S);
+    s = (s + 15) & ~size_t(15);
+    return s + (R > 0 ? 2 * 3 * AW * AH * sizeof(float) : 0) + 3 * kCTW * kCTH * sizeof(S);
+}
+
+}  // namespace
+}  // namespace cpb
+
+using namespace cpb;
+
+struct cpipe_cuda_chain {
+    cpipe_cuda_chain_config cfg{};
+    bool f16 = true;
+    int algo = 1;
+    RawParams raw{};
+    ColorParams color{};
+    ToneParams tone{};
+    WarpDev warp{};
+    int warp_mode = 0;  // 0 none, 1 fused single warp, 2 general OpcodeList3 list
+    std::vector<unsigned char> opcode3_blob;
+    Opcode3View opcode3{};
+    int radius = 2;
+    void* d_tables = nullptr;   // gain tables + LUT cells
+    void* d_mid[2] = {nullptr, nullptr};  // K1 output, K2 output (scratch frames)
+    void* d_io[2] = {nullptr, nullptr};   // device staging for run_host
+    size_t frame_bytes = 0;
+    // profiling: 4 events per frame (start, after K1, after K2, after K3)
+    bool profiling = false;
+    std::vector<cudaEvent_t> events;
+    size_t profiled = 0;
+    cudaGraphExec_t graph = nullptr;
+    const void* graph_in = nullptr;
+    void* graph_out = nullptr;
+    cudaStream_t graph_stream = nullptr;
+};
+
+namespace {
+
+cudaEvent_t* profile_slot(cpipe_cuda_chain* c) {
+    if (!c->profiling) return nullptr;
+    const size_t need = (c->profiled + 1) * 4;
+    while (c->events.size() < need) {
+        cudaEvent_t e;
+        if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
+        c->events.push_back(e);
+    }
+    return &c->events[c->profiled++ * 4];
+}
+
+int launch_chain(cpipe_cuda_chain* c, const void* d_raw, size_t raw_pitch, void* d_out, size_t out_pitch,
+                 cudaStream_t st) {
+    cudaEvent_t* ev = profile_slot(c);
+    if (ev) cudaEventRecord(ev[0], st);
+    const int w = c->cfg.width, h = c->cfg.height;
+    const int elem = c->f16 ? 2 : 4;
+    const Img raw{const_cast<void*>(d_raw), w, h, (long long)(raw_pitch ? raw_pitch / 2 : (size_t)w), 1};
+    const Img mid0{c->d_mid[0], w, h, (long long)w * 4, 4};
+    const Img mid1{c->d_mid[1], w, h, (long long)w * 4, 4};
+    const Img out{d_out, w, h, (long long)(out_pitch ? out_pitch / elem : (size_t)w * 4), 4};
+    const dim3 ga((unsigned)((w + kATW - 1) / kATW), (unsigned)((h + kATH - 1) / kATH));
+#define K1(A)                                                                                        \
+    if (c->f16) raw_to_rgba_kernel<A, __half><<<ga, 256, 0, st>>>(raw, mid0, c->raw);                \
+    else raw_to_rgba_kernel<A, float><<<ga, 256, 0, st>>>(raw, mid0, c->raw);
+    if (c->algo == 0) { K1(0) } else if (c->algo == 1) { K1(1) } else { K1(2) }
+#undef K1
+    if (ev) cudaEventRecord(ev[1], st);
+    Img k2_in = mid0;
+    if (c->warp_mode == 2) {
+        // General OpcodeList3 list through the per-node path (its scratch is stream-ordered).
+        Call call;
+        call.stream = st;
+        int s = cpb_opcode3_run(call, c->opcode3, mid0, mid1, elem);
+        if (s != CPIPE_OK) return s;
+        s = call.finish(CPIPE_OK);
+        if (s != CPIPE_OK) return s;
+        k2_in = mid1;
+    }
+    const dim3 gb((unsigned)((w + 127) / 128), (unsigned)h);
+    Img k2_out = (c->warp_mode == 2) ? mid0 : mid1;
+    if (c->warp_mode == 1) {
+        if (c->f16) warp_wb_cm_kernel<__half, true, true><<<gb, 128, 0, st>>>(k2_in, k2_out, c->warp, c->color);
+        else warp_wb_cm_kernel<float, false, true><<<gb, 128, 0, st>>>(k2_in, k2_out, c->warp, c->color);
+    } else {
+        if (c->f16) warp_wb_cm_kernel<__half, true, false><<<gb, 128, 0, st>>>(k2_in, k2_out, c->warp, c->color);
+        else warp_wb_cm_kernel<float, false, false><<<gb, 128, 0, st>>>(k2_in, k2_out, c->warp, c->color);
+    }
+    if (ev) cudaEventRecord(ev[2], st);
+    const dim3 gc((unsigned)((w + kCTW - 1) / kCTW), (unsigned)((h + kCTH - 1) / kCTH));
+#define K3(TT, F, R)                                                                                       \
+    denoise_tone_kernel<TT, F, R><<<gc, 256, denoise_tone_smem<TT, F, R>(), st>>>(k2_out, out, c->tone);
+    if (c->f16) {
+        if (c->radius == 0) { K3(__half, true, 0) } else if (c->radius == 1) { K3(__half, true, 1) } else { K3(__half, true, 2) }
+    } else {
+        if (c->radius == 0) { K3(float, false, 0) } else if (c->radius == 1) { K3(float, false, 1) } else { K3(float, false, 2) }
+    }
+#undef K3
+    if (ev) cudaEventRecord(ev[3], st);
+    return cuda_status(cudaGetLastError(), "chain launch");
+}
+
+template <class T, bool F, int R>
+cudaError_t allow_smem() {
+    return cudaFuncSetAttribute(denoise_tone_kernel<T, F, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)denoise_tone_smem<T, F, R>());
+}
+
+}  // namespace
+
+extern "C" {
+
+cpipe_cuda_chain* cpipe_cuda_chain_create(const cpipe_cuda_chain_config* cfg, int* status) {
+    auto fail = [&](int st, cpipe_cuda_chain* c) -> cpipe_cuda_chain* {
+        if (status) *status = st;
+        if (c) cpipe_cuda_chain_destroy(c);
+        return nullptr;
+    };
+    if (!cfg || cfg->width <= 0 || cfg->height <= 0) return fail(CPIPE_BAD_INDEX, nullptr);
+    if (!device_ready()) return fail(CPIPE_INTERNAL_ERROR, nullptr);
+    auto* c = new (std::nothrow) cpipe_cuda_chain();
+    if (!c) return fail(CPIPE_OOM, nullptr);
+    c->cfg = *cfg;
+    c->f16 = cfg->plain_f32 == 0;
+    c->algo = cfg->demosaic < 0 || cfg->demosaic > 2 ? 1 : cfg->demosaic;
+    const int w = cfg->width, h = cfg->height;
+    // raw stage
+    int st = cpb_blacklevel_dev(&cfg->black, w, h, &c->raw.black);
+    if (st != CPIPE_OK) return fail(st, c);
+    for (int i = 0; i < 4; ++i) c->raw.cfa.p[i] = cfg->black.cfa_pattern[i];
+    std::vector<char> table;
+    size_t offsets[3][4] = {};
+    if (cfg->gainmap_blob && cfg->gainmap_blob_size) {
+        st = cpb_gainmap_prepare(cfg->gainmap_blob, cfg->gainmap_blob_size, w, h, &table, &c->raw.gain, offsets);
+        if (st != CPIPE_OK) return fail(st, c);
+        c->raw.has_gain = 1;
+    }
+    // LUT cells after the gain tables
+    std::vector<float4> cells;
+    size_t lut_off = (table.size() + 15) & ~size_t(15);
+    if (cfg->lut_blob && cfg->lut_blob_size) {
+        st = cpb_lut_prepare(cfg->lut_blob, cfg->lut_blob_size, &cells, &c->tone.lut_size, &c->tone.lut_interp);
+        if (st != CPIPE_OK) return fail(st, c);
+        c->tone.has_lut = 1;
+    }
+    const size_t total = lut_off + cells.size() * sizeof(float4);
+    if (total) {
+        if (cudaMalloc(&c->d_tables, total) != cudaSuccess) return fail(CPIPE_OOM, c);
+        std::vector<char> host(total, 0);
+        if (!table.empty()) std::memcpy(host.data(), table.data(), table.size());
+        if (!cells.empty()) std::memcpy(host.data() + lut_off, cells.data(), cells.size() * sizeof(float4));
+        if (cudaMemcpy(c->d_tables, host.data(), total, cudaMemcpyHostToDevice) != cudaSuccess)
+            return fail(CPIPE_INTERNAL_ERROR, c);
+        if (c->raw.has_gain) cpb_gainmap_bind(&c->raw.gain, static_cast<const char*>(c->d_tables), offsets);
+        if (c->tone.has_lut) c->tone.lut = reinterpret_cast<const float4*>(static_cast<char*>(c->d_tables) + lut_off);
+    }
+    // OpcodeList3
+    if (cfg->opcode3_blob && cfg->opcode3_blob_size) {
+        c->opcode3_blob.assign(static_cast<const unsigned char*>(cfg->opcode3_blob),
+                               static_cast<const unsigned char*>(cfg->opcode3_blob) + cfg->opcode3_blob_size);
+        st = cpb_opcode3_parse(c->opcode3_blob.data(), c->opcode3_blob.size(), &c->opcode3);
+        if (st != CPIPE_OK) return fail(st, c);
+        int applied = 0, warps = 0;
+        const cpipe_Opcode3DispatchRecord* warp_rec = nullptr;
+        for (uint32_t i = 0; i < c->opcode3.count; ++i) {
+            const auto& r = c->opcode3.records[i];
+            if (r.id == CPIPE_OPCODE3_UNKNOWN) {
+                if (!r.optional) return fail(CPIPE_UNSUPPORTED, c);
+                continue;
+            }
+            ++applied;
+            if (r.id == CPIPE_OPCODE3_WARP_RECTILINEAR) {
+                ++warps;
+                warp_rec = &r;
+            }
+        }
+        if (applied == 1 && warps == 1) c->warp_mode = cpb_warp_dev(warp_rec, w, h, &c->warp) == CPIPE_OK ? 1 : 0;
+        else if (applied > 0) c->warp_mode = 2;
+    }
+    // colour, denoise, tone
+    std::memcpy(c->color.neutral, cfg->as_shot_neutral, sizeof(c->color.neutral));
+    std::memcpy(c->color.cm, cfg->colormatrix, sizeof(c->color.cm));
+    c->tone.bm3d_strength = fminf(1.0F, fmaxf(0.0F, cfg->bm3d_sigma / 0.03F));
+    // guided_radius 0 leaves the guided node out; otherwise the reference box
+    // is 3x3 for radius <= 1 and 5x5 above (guided_filter_generator.cpp:66-70).
+    c->radius = cfg->guided_radius <= 0 ? 0 : (cfg->guided_radius == 1 ? 1 : 2);
+    c->tone.has_wavelet = cfg->wavelet_strength >= 0.0F;
+    c->tone.eps = cfg->guided_eps;
+    c->tone.wavelet_th = 0.035F * cfg->wavelet_strength;
+    c->tone.filmic = cpb_filmic_dev(&cfg->filmic);
+    // scratch frames
+    c->frame_bytes = (size_t)w * h * 4 * (c->f16 ? 2 : 4);
+    for (void*& p : c->d_mid)
+        if (cudaMalloc(&p, c->frame_bytes) != cudaSuccess) return fail(CPIPE_OOM, c);
+    cudaError_t e = cudaSuccess;
+    if (c->f16) e = c->radius == 0 ? allow_smem<__half, true, 0>() : c->radius == 1 ? allow_smem<__half, true, 1>() : allow_smem<__half, true, 2>();
+    else e = c->radius == 0 ? allow_smem<float, false, 0>() : c->radius == 1 ? allow_smem<float, false, 1>() : allow_smem<float, false, 2>();
+    if (e != cudaSuccess) return fail(cuda_status(e, "chain smem"), c);
+    if (status) *status = CPIPE_OK;
+    return c;
+}
+
+void cpipe_cuda_chain_destroy(cpipe_cuda_chain* c) {
+    if (!c) return;
+    for (cudaEvent_t e : c->events) cudaEventDestroy(e);
+    if (c->graph) cudaGraphExecDestroy(c->graph);
+    cudaFree(c->d_tables);
+    for (void* p : c->d_mid) cudaFree(p);
+    for (void* p : c->d_io) cudaFree(p);
+    delete c;
+}
+
+size_t cpipe_cuda_chain_output_bytes(const cpipe_cuda_chain* c) { return c ? c->frame_bytes : 0; }
+
+int cpipe_cuda_chain_run(cpipe_cuda_chain* c, const void* d_raw, void* d_out, void* stream) {
+    if (!c || !d_raw || !d_out) return CPIPE_BAD_INDEX;
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    if (c->cfg.use_graph && c->warp_mode != 2 && !c->profiling) {
+        if (!c->graph || c->graph_in != d_raw || c->graph_out != d_out || c->graph_stream != st) {
+            if (c->graph) cudaGraphExecDestroy(c->graph);
+            c->graph = nullptr;
+            cudaGraph_t g;
+            cudaStream_t cap = st;
+            cudaStream_t own = nullptr;
+            if (cap == nullptr) {  // the legacy stream cannot be captured
+                if (cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking) != cudaSuccess) return CPIPE_INTERNAL_ERROR;
+                cap = own;
+            }
+            int s = cuda_status(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal), "begin capture");
+            if (s == CPIPE_OK) {
+                const int ls = launch_chain(c, d_raw, 0, d_out, 0, cap);
+                s = cuda_status(cudaStreamEndCapture(cap, &g), "end capture");
+                if (ls != CPIPE_OK) s = ls;
+            }
+            if (s == CPIPE_OK) {
+                s = cuda_status(cudaGraphInstantiate(&c->graph, g, 0), "instantiate");
+                cudaGraphDestroy(g);
+            }
+            if (own) cudaStreamDestroy(own);
+            if (s != CPIPE_OK) return s;
+            c->graph_in = d_raw;
+            c->graph_out = d_out;
+            c->graph_stream = st;
+        }
+        return cuda_status(cudaGraphLaunch(c->graph, st), "graph launch");
+    }
+    return launch_chain(c, d_raw, 0, d_out, 0, st);
+}
+
+int cpipe_cuda_chain_run_host(cpipe_cuda_chain* c, const uint16_t* h_raw, void* h_out, void* stream) {
+    if (!c || !h_raw || !h_out) return CPIPE_BAD_INDEX;
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t raw_bytes = (size_t)c->cfg.width * c->cfg.height * sizeof(uint16_t);
+    if (!c->d_io[0] && cudaMalloc(&c->d_io[0], raw_bytes) != cudaSuccess) return CPIPE_OOM;
+    if (!c->d_io[1] && cudaMalloc(&c->d_io[1], c->frame_bytes) != cudaSuccess) return CPIPE_OOM;
+    int s = cuda_status(cudaMemcpyAsync(c->d_io[0], h_raw, raw_bytes, cudaMemcpyHostToDevice, st), "chain H2D");
+    if (s == CPIPE_OK) s = cpipe_cuda_chain_run(c, c->d_io[0], c->d_io[1], stream);
+    if (s == CPIPE_OK)
+        s = cuda_status(cudaMemcpyAsync(h_out, c->d_io[1], c->frame_bytes, cudaMemcpyDeviceToHost, st), "chain D2H");
+    const int ss = cuda_status(cudaStreamSynchronize(st), "chain sync");
+    return s != CPIPE_OK ? s : ss;
+}
+
+int cpipe_cuda_chain_set_profiling(cpipe_cuda_chain* c, int enable) {
+    if (!c) return CPIPE_BAD_INDEX;
+    c->profiling = enable != 0;
+    c->profiled = 0;
+    return CPIPE_OK;
+}
+
+int cpipe_cuda_chain_profile(cpipe_cuda_chain* c, double ms_per_kernel[3], int* frames) {
+    if (!c || !ms_per_kernel || !frames) return CPIPE_BAD_INDEX;
+    ms_per_kernel[0] = ms_per_kernel[1] = ms_per_kernel[2] = 0.0;
+    for (size_t f = 0; f < c->profiled; ++f) {
+        cudaEvent_t* ev = &c->events[f * 4];
+        const int st = cuda_status(cudaEventSynchronize(ev[3]), "profile sync");
+        if (st != CPIPE_OK) return st;
+        for (int k = 0; k < 3; ++k) {
+            float ms = 0.0F;
+            cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
+            ms_per_kernel[k] += ms;
+        }
+    }
+    *frames = (int)c->profiled;
+    c->profiled = 0;
+    return CPIPE_OK;
+}
+
+int cpipe_cuda_stream_create(void** out) {
+    if (!out) return CPIPE_BAD_INDEX;
+    cudaStream_t s;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess) return CPIPE_INTERNAL_ERROR;
+    *out = s;
+    return CPIPE_OK;
+}
+void cpipe_cuda_stream_destroy(void* s) { cudaStreamDestroy(static_cast<cudaStream_t>(s)); }
+int cpipe_cuda_stream_synchronize(void* s) {
+    return cuda_status(cudaStreamSynchronize(static_cast<cudaStream_t>(s)), "stream sync");
+}
+int cpipe_cuda_event_create(void** out) {
+    if (!out) return CPIPE_BAD_INDEX;
+    cudaEvent_t e;
+    if (cudaEventCreate(&e) != cudaSuccess) return CPIPE_INTERNAL_ERROR;
+    *out = e;
+    return CPIPE_OK;
+}
+void cpipe_cuda_event_destroy(void* e) { cudaEventDestroy(static_cast<cudaEvent_t>(e)); }
+int cpipe_cuda_event_record(void* e, void* stream) {
+    return cuda_status(cudaEventRecord(static_cast<cudaEvent_t>(e), static_cast<cudaStream_t>(stream)), "event record");
+}
+int cpipe_cuda_event_elapsed_ms(void* start, void* stop, float* ms) {
+    if (!ms) return CPIPE_BAD_INDEX;
+    int st = cuda_status(cudaEventSynchronize(static_cast<cudaEvent_t>(stop)), "event sync");
+    if (st == CPIPE_OK)
+        st = cuda_status(cudaEventElapsedTime(ms, static_cast<cudaEvent_t>(start), static_cast<cudaEvent_t>(stop)), "elapsed");
+    return st;
+}
+int cpipe_cuda_device_alloc(size_t bytes, void** out) {
+    if (!out) return CPIPE_BAD_INDEX;
+    if (cudaMalloc(out, bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return CPIPE_OOM;
+    }
+    return CPIPE_OK;
+}
+void cpipe_cuda_device_free(void* p) { cudaFree(p); }
+int cpipe_cuda_memcpy_h2d(void* dst, const void* src, size_t bytes) {
+    return cuda_status(cudaMemcpy(dst, src, bytes, cudaMemcpyHostToDevice), "h2d");
+}
+int cpipe_cuda_memcpy_d2h(void* dst, const void* src, size_t bytes) {
+    return cuda_status(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost), "d2h");
+}
+int cpipe_cuda_set_device(int device) { return cuda_status(cudaSetDevice(device), "set device"); }
+
+int cpipe_cuda_pinned_alloc(size_t bytes, void** out) {
+    if (!out) return CPIPE_BAD_INDEX;
+    return cudaHostAlloc(out, bytes, cudaHostAllocDefault) == cudaSuccess ? CPIPE_OK : CPIPE_OOM;
+}
+void cpipe_cuda_pinned_free(void* p) { cudaFreeHost(p); }
+
+}  // extern "C"

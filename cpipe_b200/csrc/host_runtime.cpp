@@ -19,6 +19,7 @@
 #include <map>
 #include <memory>
 #include <optional>
+#include <set>
 #include <string>
 #include <vector>
 
@@ -86,6 +87,7 @@ struct cpipe_b200_host {
     cudaStream_t stream = nullptr;
     uint64_t cap = 0, allocated = 0;
     std::string error;
+    std::set<cpipe_b200_buffer*> live;  // buffers still holding device memory
 };
 
 struct cpipe_b200_buffer {
@@ -532,9 +534,17 @@ cpipe_b200_host* cpipe_b200_host_create(void) {
     }
     return h;
 }
+// Destroying the host releases the device memory of every buffer still alive;
+// those buffer handles stay valid for cpipe_b200_buffer_destroy (which then only
+// frees the handle), whatever order the caller releases things in.
 void cpipe_b200_host_destroy(cpipe_b200_host* h) {
     if (!h) return;
     cudaStreamSynchronize(h->stream);
+    for (cpipe_b200_buffer* b : h->live) {
+        cudaFree(b->dev);
+        b->dev = nullptr;
+        b->host = nullptr;
+    }
     cudaStreamDestroy(h->stream);
     delete h;
 }
@@ -562,6 +572,7 @@ cpipe_b200_buffer* cpipe_b200_buffer_create(cpipe_b200_host* h, int format, uint
         return nullptr;
     }
     b->host = h;
+    h->live.insert(b);
     b->format = format;
     b->w = w;
     b->h = hgt;
@@ -571,20 +582,23 @@ cpipe_b200_buffer* cpipe_b200_buffer_create(cpipe_b200_host* h, int format, uint
 }
 void cpipe_b200_buffer_destroy(cpipe_b200_buffer* b) {
     if (!b) return;
-    cudaStreamSynchronize(b->host->stream);
-    cudaFree(b->dev);
-    b->host->allocated -= b->bytes;
+    if (b->host) {
+        cudaStreamSynchronize(b->host->stream);
+        cudaFree(b->dev);
+        b->host->allocated -= b->bytes;
+        b->host->live.erase(b);
+    }
     delete b;
 }
 int cpipe_b200_buffer_upload(cpipe_b200_buffer* b, const void* data, size_t bytes) {
-    if (!b || !data || bytes != b->bytes) return CPIPE_BAD_INDEX;
+    if (!b || !b->host || !data || bytes != b->bytes) return CPIPE_BAD_INDEX;
     if (cudaMemcpyAsync(b->dev, data, bytes, cudaMemcpyHostToDevice, b->host->stream) != cudaSuccess ||
         cudaStreamSynchronize(b->host->stream) != cudaSuccess)
         return CPIPE_INTERNAL_ERROR;
     return CPIPE_OK;
 }
 int cpipe_b200_buffer_download(cpipe_b200_buffer* b, void* data, size_t bytes) {
-    if (!b || !data || bytes != b->bytes) return CPIPE_BAD_INDEX;
+    if (!b || !b->host || !data || bytes != b->bytes) return CPIPE_BAD_INDEX;
     if (cudaMemcpyAsync(data, b->dev, bytes, cudaMemcpyDeviceToHost, b->host->stream) != cudaSuccess ||
         cudaStreamSynchronize(b->host->stream) != cudaSuccess)
         return CPIPE_INTERNAL_ERROR;

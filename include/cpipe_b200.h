@@ -166,6 +166,66 @@ int cpipe_b200_run_node(cpipe_b200_host* host, const char* node_id, const cpipe_
                         size_t n_out);
 const char* cpipe_b200_host_last_error(cpipe_b200_host* host);
 
+/* ---------------------------------------------------------------- fused chain */
+/* The raw->linear node sequence of the reference's classic pipeline
+ * (examples/pipelines/full-classic-pipeline.cpipe.json, nodes lin..lut):
+ *   precision_convert(r16u->f32) -> blacklevel -> GainMap -> demosaic ->
+ *   OpcodeList3 -> WB -> colormatrix -> BM3D -> guided -> wavelet -> filmic -> 3D LUT
+ * with every parameter already resolved by the nodes' host-side preparation
+ * (the same blobs the filters take).  Output: RGBA16F (or RGBA f32 when
+ * plain_f32), identical to running the nodes one by one. */
+typedef struct {
+    int32_t width, height;
+    cpipe_BlacklevelParams black;       /* levels and the 2x2 CFA pattern */
+    const void* gainmap_blob;           /* GainMap dispatch blob, or NULL for none */
+    size_t gainmap_blob_size;
+    int32_t demosaic;                   /* 0 bilinear, 1 RCD, 2 AMaZE */
+    const void* opcode3_blob;           /* OpcodeList3 dispatch blob, or NULL */
+    size_t opcode3_blob_size;
+    float as_shot_neutral[3];           /* WB divisor */
+    float colormatrix[9];               /* camera -> Rec.2020 */
+    float bm3d_sigma;
+    int32_t guided_radius;              /* 0: no guided node */
+    float guided_eps;
+    float wavelet_strength;             /* < 0: no wavelet node */
+    cpipe_FilmicRgbParams filmic;
+    const void* lut_blob;               /* Lut3dParamHeader + values, or NULL */
+    size_t lut_blob_size;
+    int32_t plain_f32;                  /* 1: FP32 plain form (no f16 rounding between nodes) */
+    int32_t use_graph;                  /* 1: replay a captured CUDA graph per (input, output) pair */
+} cpipe_cuda_chain_config;
+
+typedef struct cpipe_cuda_chain cpipe_cuda_chain;
+/* Allocates the chain's device tables and two intermediate frames. */
+cpipe_cuda_chain* cpipe_cuda_chain_create(const cpipe_cuda_chain_config* cfg, int* status);
+void cpipe_cuda_chain_destroy(cpipe_cuda_chain* chain);
+size_t cpipe_cuda_chain_output_bytes(const cpipe_cuda_chain* chain);
+/* Device pointers (dense rows); asynchronous on `stream` (a cudaStream_t). */
+int cpipe_cuda_chain_run(cpipe_cuda_chain* chain, const void* d_raw_u16, void* d_out, void* stream);
+/* Host pointers: H2D of the raw frame, the chain, D2H of the result; returns after the copy-out. */
+int cpipe_cuda_chain_run_host(cpipe_cuda_chain* chain, const uint16_t* h_raw, void* h_out, void* stream);
+/* Per-kernel timing: while enabled, each run records CUDA events around its
+ * three kernels (and bypasses the graph); chain_profile sums the kernel times
+ * of the runs recorded since the last call. */
+int cpipe_cuda_chain_set_profiling(cpipe_cuda_chain* chain, int enable);
+int cpipe_cuda_chain_profile(cpipe_cuda_chain* chain, double ms_per_kernel[3], int* frames);
+/* Device memory, streams and events for callers without their own CUDA runtime. */
+int cpipe_cuda_set_device(int device);
+int cpipe_cuda_device_alloc(size_t bytes, void** out);
+void cpipe_cuda_device_free(void* p);
+int cpipe_cuda_memcpy_h2d(void* dst, const void* src, size_t bytes);
+int cpipe_cuda_memcpy_d2h(void* dst, const void* src, size_t bytes);
+int cpipe_cuda_stream_create(void** out);
+void cpipe_cuda_stream_destroy(void* stream);
+int cpipe_cuda_stream_synchronize(void* stream);
+int cpipe_cuda_event_create(void** out);
+void cpipe_cuda_event_destroy(void* event);
+int cpipe_cuda_event_record(void* event, void* stream);
+int cpipe_cuda_event_elapsed_ms(void* start, void* stop, float* ms);
+/* Page-locked host memory for run_host callers. */
+int cpipe_cuda_pinned_alloc(size_t bytes, void** out);
+void cpipe_cuda_pinned_free(void* p);
+
 #ifdef __cplusplus
 } /* extern "C" */
 #endif

@@ -596,7 +596,7 @@ int oracle_opcode3(const float* in, float* out, float* work, float* next, int w,
                 const double cx = r->cx_hat * (double)(w - 1), cy = r->cy_hat * (double)(h - 1);
                 const double m = max_corner(cx, cy, w, h);
                 if (m <= 2.220446049250313e-16) break;
-#pragma omp parallel for schedule(static)
+                /* single-threaded, as the reference's plain-C++ filter */
                 for (int y = 0; y < h; ++y)
                     for (int x = 0; x < w; ++x) {
                         const double dx = ((double)x - cx) / m, dy = ((double)y - cy) / m;

@@ -1,0 +1,160 @@
+"""The fused chain on the GPU against (a) the CPU oracle run node by node and
+(b) the same nodes run one by one on the GPU through their plugins.  Small
+frames (including odd sizes) are compared element by element; the full 12 MP
+workload is compared with the oracle and checked for the size-independent
+properties: fused == unfused bit for bit, deterministic, graph replay equal to
+direct launch, finite and in [0, 1]."""
+import numpy as np
+import pytest
+from chain_oracle import run_chain_oracle
+from cpipe_b200 import _abi as A
+from cpipe_b200.chain import Chain, ChainConfig
+from parity import assert_f16_parity, assert_f32_parity, f16_ulp_distance
+
+pytestmark = pytest.mark.gpu
+
+
+def run_nodes_on_gpu(host, cfg, raw):
+    """The chain as a sequence of plugin nodes on device buffers (reference
+    node order), returning the RGBA16F result."""
+    b = cfg.blobs()
+    w, h = cfg.width, cfg.height
+    F32, F16, U16 = A.FMT_R32_SFLOAT, A.FMT_R16G16B16A16_SFLOAT, A.FMT_R16_UINT
+    cur = host.buffer(U16, w, h).upload(raw)
+    meta = dict(cfa=cfg.cfa, black_level=[cfg.black] * 4, white_level=cfg.white, cs_role="raw_camera",
+                illuminants=(17, 21), as_shot_neutral=list(cfg.neutral),
+                noise_profile=[(cfg.noise_b, cfg.noise_a)])
+    from cpipe_b200.chain import CAMERA_TO_XYZ, COLOR_MATRIX1, COLOR_MATRIX2
+    meta.update(color_matrix1=COLOR_MATRIX1, color_matrix2=COLOR_MATRIX2, forward_matrix1=CAMERA_TO_XYZ,
+                forward_matrix2=CAMERA_TO_XYZ)
+    blob_meta = {}
+    if "opcode_list_2" in b:
+        blob_meta["com.cpipe.dng.opcode_list_2_bytes"] = b["opcode_list_2"]
+    if "opcode_list_3" in b:
+        blob_meta["com.cpipe.dng.opcode_list_3_bytes"] = b["opcode_list_3"]
+    cur.set_metadata(blobs=blob_meta, **meta)
+    import tempfile, os
+    from cpipe_b200 import blobs as BL
+    steps = [("com.cpipe.precision_convert", F32, {"target_format": "R32_SFLOAT"}),
+             ("com.cpipe.blacklevel.dng_levels", F32, {})]
+    if cfg.gainmap:
+        steps.append(("com.cpipe.lens.shading_gainmap", F32, {}))
+    steps.append((f"com.cpipe.demosaic.{cfg.demosaic}", F16, {}))
+    if cfg.warp is not None:
+        steps.append(("com.cpipe.lens.dng_opcode_list_3", F16, {}))
+    steps += [("com.cpipe.wb.dual_illuminant", F16, {}), ("com.cpipe.colormatrix.dng_to_working", F16, {}),
+              ("com.cpipe.denoise.bm3d", F16, {})]
+    if cfg.guided_radius > 0:
+        steps.append(("com.cpipe.denoise.guided_filter", F16, {"radius": cfg.guided_radius, "eps": cfg.guided_eps}))
+    if cfg.wavelet_strength >= 0:
+        steps.append(("com.cpipe.denoise.wavelet_bayes_shrink", F16, {"chroma_strength": cfg.wavelet_strength}))
+    steps.append(("com.cpipe.tone.filmic_rgb", F16, {}))
+    tmp = None
+    if "lut" in b:
+        tmp = tempfile.NamedTemporaryFile(suffix=".cube", delete=False)
+        tmp.close()
+        BL.write_cube(tmp.name, 33, b["lut_values"])
+        steps.append(("com.cpipe.color.3d_lut", F16, {"lut_path": tmp.name}))
+    try:
+        for node_id, fmt, params in steps:
+            nxt = host.buffer(fmt, w, h)
+            st = host.run_node(node_id, [cur], [nxt], params)
+            assert st == 0, f"{node_id}: {A.STATUS_NAMES.get(st)} {host.last_error()}"
+            cur = nxt
+    finally:
+        if tmp:
+            os.unlink(tmp.name)
+    return cur.download()
+
+
+SMALL = [(96, 64), (97, 63), (33, 17), (2, 2), (1, 1), (130, 70)]
+
+
+@pytest.mark.parametrize("w,h", SMALL)
+def test_chain_matches_oracle_small(cuda_device, w, h):
+    cfg = ChainConfig.small(w, h)
+    raw = cfg.make_raw()
+    chain = Chain(cfg)
+    got = chain.run_host(raw)
+    want = run_chain_oracle(cfg, raw)
+    assert_f16_parity(got, want, what=f"chain {w}x{h}")
+    chain.close()
+
+
+@pytest.mark.parametrize("variant", [
+    dict(demosaic="amaze"), dict(demosaic="bilinear"), dict(gainmap=False), dict(warp=None),
+    dict(guided_radius=1, guided_eps=0.015), dict(guided_radius=0), dict(wavelet_strength=-1.0),
+    dict(lut="identity_gamma"), dict(lut="none"), dict(filmic=dict(ev=0.5, contrast=1.3, saturation=1.2)),
+    dict(cfa=(2, 1, 1, 0)), dict(cfa=(1, 0, 2, 1)), dict(use_graph=False),
+])
+def test_chain_variants_match_oracle(cuda_device, variant):
+    cfg = ChainConfig.small(120, 90, **variant)
+    raw = cfg.make_raw()
+    chain = Chain(cfg)
+    got = chain.run_host(raw)
+    assert_f16_parity(got, run_chain_oracle(cfg, raw), what=str(variant))
+    chain.close()
+
+
+def test_chain_plain_f32_form(cuda_device):
+    cfg = ChainConfig.small(128, 96, plain_f32=True)
+    raw = cfg.make_raw()
+    chain = Chain(cfg)
+    got = chain.run_host(raw)
+    assert got.dtype == np.float32
+    assert_f32_parity(got, run_chain_oracle(cfg, raw), what="chain f32")
+    chain.close()
+
+
+def test_chain_equals_nodes_on_gpu(cuda_device, host):
+    """Fusing the nodes changes no arithmetic: bit-identical to the plugins run one by one."""
+    cfg = ChainConfig.small(160, 120)
+    raw = cfg.make_raw()
+    chain = Chain(cfg)
+    fused = chain.run_host(raw)
+    nodes = run_nodes_on_gpu(host, cfg, raw)
+    assert f16_ulp_distance(fused, nodes).max() == 0
+    chain.close()
+
+
+def test_chain_general_opcode_list(cuda_device):
+    """OpcodeList3 lists other than a single warp take the per-node path inside the chain."""
+    import ctypes as C
+    from cpipe_b200 import blobs as BL
+    cfg = ChainConfig.small(100, 80)
+    raw = cfg.make_raw()
+    b = cfg.blobs()
+    vig = BL.vignette_record([0.3])
+    warp = BL.warp_record([cfg.warp])
+    b["opcode3"] = BL.opcode3_dispatch([vig, warp])
+    c_cfg, keep = cfg.c_config()
+    buf = C.create_string_buffer(b["opcode3"], len(b["opcode3"]))
+    c_cfg.opcode3_blob, c_cfg.opcode3_blob_size = C.cast(buf, C.c_void_p), len(b["opcode3"])
+    st = C.c_int32()
+    h = A.lib().cpipe_cuda_chain_create(C.byref(c_cfg), C.byref(st))
+    assert h, st.value
+    out = np.empty((80, 100, 4), np.float16)
+    assert A.lib().cpipe_cuda_chain_run_host(h, raw.ctypes.data, out.ctypes.data, None) == 0
+    A.lib().cpipe_cuda_chain_destroy(h)
+    assert_f16_parity(out, run_chain_oracle(cfg, raw, blobs=b), what="general opcode list")
+
+
+def test_chain_full_12mp(cuda_device, host):
+    cfg = ChainConfig.full_12mp()
+    raw = cfg.make_raw()
+    chain = Chain(cfg)
+    a = chain.run_host(raw)
+    b = chain.run_host(raw)
+    assert np.array_equal(a.view(np.uint16), b.view(np.uint16)), "non-deterministic"
+    af = a.astype(np.float32)
+    assert np.isfinite(af).all() and af.min() >= 0.0 and af.max() <= 1.0
+    cfg_ng = ChainConfig.full_12mp(use_graph=False)
+    chain_ng = Chain(cfg_ng)
+    c = chain_ng.run_host(raw)
+    assert np.array_equal(a.view(np.uint16), c.view(np.uint16)), "graph replay differs"
+    nodes = run_nodes_on_gpu(host, cfg, raw)
+    assert f16_ulp_distance(a, nodes).max() == 0, "fused differs from node-by-node"
+    want = run_chain_oracle(cfg, raw)
+    ulps, n_off = assert_f16_parity(a, want, what="12MP chain vs oracle")
+    chain.close()
+    chain_ng.close()
