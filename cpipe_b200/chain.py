@@ -145,7 +145,7 @@ class ChainConfig:
                "demosaic": B.demosaic(self.cfa)}
         if self.gainmap:
             stream = B.opcode_list_2_with_gain_maps([B.gain_map_params(
-                17, 13, 0, 1, (self.height - 1) / 12.0, (self.width - 1) / 16.0, radial_gains())])
+                17, 13, 0, 1, max(self.height - 1, 1) / 12.0, max(self.width - 1, 1) / 16.0, radial_gains())])
             n = C.c_size_t(0)
             rep, pat = (C.c_uint8 * 2)(2, 2), (C.c_uint8 * 16)(*self.cfa)
             st = L.cpipe_b200_pack_gain_maps(stream, len(stream), rep, pat, None, C.byref(n))
@@ -259,3 +259,35 @@ class Chain:
         if st:
             raise CpipeError(st, "chain_run_host " + A.lib().cpipe_cuda_last_error().decode())
         return out
+
+
+def _main():
+    """Run the 12 MP chain a few times on the GPU (used for profiler captures):
+    python -m cpipe_b200.chain [--frames N] [--width W --height H] [--demosaic rcd|amaze|bilinear]"""
+    import argparse
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--frames", type=int, default=3)
+    ap.add_argument("--width", type=int, default=4032)
+    ap.add_argument("--height", type=int, default=3024)
+    ap.add_argument("--demosaic", default="rcd")
+    args = ap.parse_args()
+    L = A.lib()
+    assert L.cpipe_cuda_device_count() > 0, "no CUDA device"
+    cfg = ChainConfig.full_12mp(width=args.width, height=args.height, demosaic=args.demosaic, use_graph=False)
+    raw = cfg.make_raw()
+    chain = Chain(cfg)
+    d_raw, d_out = C.c_void_p(), C.c_void_p()
+    assert L.cpipe_cuda_device_alloc(raw.nbytes, C.byref(d_raw)) == 0
+    assert L.cpipe_cuda_device_alloc(cfg.width * cfg.height * 8, C.byref(d_out)) == 0
+    assert L.cpipe_cuda_memcpy_h2d(d_raw, raw.ctypes.data, raw.nbytes) == 0
+    for _ in range(args.frames):
+        chain.run(d_raw.value, d_out.value, None)
+    assert L.cpipe_cuda_synchronize() == 0
+    chain.close()
+    L.cpipe_cuda_device_free(d_raw)
+    L.cpipe_cuda_device_free(d_out)
+    print("ran", args.frames, "frames of", cfg.name)
+
+
+if __name__ == "__main__":
+    _main()

@@ -21,16 +21,13 @@
 #include "../../include/cpipe_b200.h"
 #include "filters_impl.h"
 #include "kernels.h"
+#include "demosaic.cuh"
 #include "nodes.cuh"
 
 namespace cpb {
 namespace {
 
 // ------------------------------------------------------------------ K1
-constexpr int kATW = 64, kATH = 16, kAHalo = 3;
-constexpr int kAIW = kATW + 2 * kAHalo, kAIH = kATH + 2 * kAHalo;
-constexpr int kAGW = kATW + 2, kAGH = kATH + 2;
-
 struct RawParams {
     BlackDev black;
     GainMapDev gain;
@@ -38,81 +35,21 @@ struct RawParams {
     Cfa cfa;
 };
 
-struct TapA {
-    const float* base;
-    __device__ __forceinline__ float operator()(int dx, int dy) const { return base[dy * kAIW + dx]; }
+// precision_convert -> blacklevel -> GainMap at a clamped coordinate
+struct RawLoader {
+    Img raw;
+    const RawParams* p;
+    __device__ __forceinline__ float operator()(int gx, int gy) const {
+        float v = (float)*px<const uint16_t>(raw, gx, gy);
+        v = blacklevel_px(v, gx, gy, p->black);
+        if (p->has_gain) v = v * gain_px(gain_map_index(gx, gy, p->gain), gx, gy, p->gain);
+        return v;
+    }
 };
 
 template <int ALGO, class TOut>
 __global__ void __launch_bounds__(256) raw_to_rgba_kernel(Img raw, Img out, RawParams p) {
-    __shared__ float s_in[kAIH * kAIW];
-    __shared__ float s_g[kAGH * kAGW];
-    const int x0 = blockIdx.x * kATW, y0 = blockIdx.y * kATH;
-    // precision_convert -> blacklevel -> GainMap at each clamped coordinate
-    for (int i = threadIdx.x; i < kAIH * kAIW; i += blockDim.x) {
-        const int ty = i / kAIW, tx = i - ty * kAIW;
-        const int gx = clampi(x0 - kAHalo + tx, 0, raw.w - 1), gy = clampi(y0 - kAHalo + ty, 0, raw.h - 1);
-        float v = (float)*px<const uint16_t>(raw, gx, gy);
-        v = blacklevel_px(v, gx, gy, p.black);
-        if (p.has_gain) v = v * gain_px(gain_map_index(gx, gy, p.gain), gx, gy, p.gain);
-        s_in[i] = v;
-    }
-    __syncthreads();
-    if (ALGO != 0) {
-        for (int i = threadIdx.x; i < kAGH * kAGW; i += blockDim.x) {
-            const int ty = i / kAGW, tx = i - ty * kAGW;
-            const TapA T{s_in + (ty + kAHalo - 1) * kAIW + (tx + kAHalo - 1)};
-            s_g[i] = ALGO == 1 ? rcd_green(T, x0 - 1 + tx, y0 - 1 + ty, p.cfa) : amaze_green(T, x0 - 1 + tx, y0 - 1 + ty, p.cfa);
-        }
-        __syncthreads();
-    }
-    for (int i = threadIdx.x; i < kATH * kATW; i += blockDim.x) {
-        const int ty = i / kATW, tx = i - ty * kATW;
-        const int x = x0 + tx, y = y0 + ty;
-        if (x >= out.w || y >= out.h) continue;
-        const float* c = s_in + (ty + kAHalo) * kAIW + (tx + kAHalo);
-        const TapA T{c};
-        const float ctr = c[0];
-        const int site = p.cfa.at(x, y);
-        const bool red = site == 0, blue = site == 2;
-        const bool hred = p.cfa.at(x - 1, y) == 0, hblue = p.cfa.at(x - 1, y) == 2;
-        float r, g, b;
-        if (ALGO == 0) {
-            const float hz = 0.5F * (T(-1, 0) + T(1, 0));
-            const float vt = 0.5F * (T(0, -1) + T(0, 1));
-            const float cross = 0.25F * (T(-1, 0) + T(1, 0) + T(0, -1) + T(0, 1));
-            const float diag = 0.25F * (T(-1, -1) + T(1, -1) + T(-1, 1) + T(1, 1));
-            r = red ? ctr : blue ? diag : hred ? hz : vt;
-            g = (red || blue) ? cross : ctr;
-            b = blue ? ctr : red ? diag : hred ? vt : hz;
-        } else {
-            const float* G = s_g + (ty + 1) * kAGW + (tx + 1);
-#define GG(dx, dy) G[(dy) * kAGW + (dx)]
-            const float gc = GG(0, 0);
-            if (ALGO == 1) {
-#define RT(dx, dy) (T(dx, dy) / maxf(GG(dx, dy), 0.000001F))
-                const float rh = gc * 0.5F * (RT(-1, 0) + RT(1, 0));
-                const float rv = gc * 0.5F * (RT(0, -1) + RT(0, 1));
-                const float rd = gc * 0.25F * (RT(-1, -1) + RT(1, -1) + RT(-1, 1) + RT(1, 1));
-#undef RT
-                r = max0(red ? ctr : blue ? rd : hred ? rh : rv);
-                g = max0(gc);
-                b = max0(blue ? ctr : red ? rd : hblue ? rh : rv);
-            } else {
-#define CH(dx, dy) (T(dx, dy) - GG(dx, dy))
-                const float chh = 0.5F * (CH(-1, 0) + CH(1, 0));
-                const float chv = 0.5F * (CH(0, -1) + CH(0, 1));
-                const float chd = 0.25F * (CH(-1, -1) + CH(1, -1) + CH(-1, 1) + CH(1, 1));
-#undef CH
-                const float rh = gc + chh, rv = gc + chv, rd = gc + chd;
-                r = max0(red ? ctr : (blue ? rd : hred ? rh : rv));
-                g = max0(gc);
-                b = max0(blue ? ctr : (red ? rd : hblue ? rh : rv));
-            }
-#undef GG
-        }
-        store_rgba(px<TOut>(out, x, y), Rgba{r, g, b, 1.0F});
-    }
+    demosaic_tile<ALGO, TOut>(RawLoader{raw, &p}, raw.w, raw.h, out, p.cfa);
 }
 
 // ------------------------------------------------------------------ K2
@@ -127,35 +64,8 @@ __global__ void __launch_bounds__(128) warp_wb_cm_kernel(Img in, Img out, WarpDe
     if (x >= out.w) return;
     Rgba v;
     if (WARP) {
-        const ff dx = ff_mul(ff_sub(ff_from((float)x), w.cx), w.inv_m);
-        const ff dy = ff_mul(ff_sub(ff_from((float)y), w.cy), w.inv_m);
-        const ff r2 = ff_add(ff_mul(dx, dx), ff_mul(dy, dy));
-        const ff r4 = ff_mul(r2, r2), r6 = ff_mul(r4, r2);
-        float res[4];
-        int done_for = -1;
-        Rgba last{};
-        for (int c = 0; c < 4; ++c) {
-            const int ci = c < w.count - 1 ? c : w.count - 1;
-            if (ci != done_for) {
-                ff sx, sy;
-                warp_src(w, w.k[ci], dx, dy, r2, r4, r6, &sx, &sy);
-                sx = ff_clamp0(sx, w.xmax);
-                sy = ff_clamp0(sy, w.ymax);
-                const int ix = ff_floor(sx), iy = ff_floor(sy);
-                const float tx = ff_frac(sx, ix), ty = ff_frac(sy, iy);
-                Rgba rows[4];
-#pragma unroll
-                for (int r = 0; r < 4; ++r) {
-                    const int yy = iy + r - 1;
-                    rows[r] = cubic4(load_clamped<T>(in, ix - 1, yy), load_clamped<T>(in, ix, yy),
-                                     load_clamped<T>(in, ix + 1, yy), load_clamped<T>(in, ix + 2, yy), tx);
-                }
-                last = cubic4(rows[0], rows[1], rows[2], rows[3], ty);
-                done_for = ci;
-            }
-            res[c] = c == 0 ? last.r : c == 1 ? last.g : c == 2 ? last.b : last.a;
-        }
-        v = Rgba{rnd<F16>(res[0]), rnd<F16>(res[1]), rnd<F16>(res[2]), rnd<F16>(res[3])};
+        const Rgba wv = warp_px<T>(in, w, x, y);
+        v = Rgba{rnd<F16>(wv.r), rnd<F16>(wv.g), rnd<F16>(wv.b), rnd<F16>(wv.a)};
     } else {
         v = load_rgba(px<const T>(in, x, y));
     }
@@ -166,28 +76,19 @@ __global__ void __launch_bounds__(128) warp_wb_cm_kernel(Img in, Img out, WarpDe
 }
 
 // ------------------------------------------------------------------ K3
-// Tile TW x TH; R = guided box radius (1 or 2).  Shared-memory planes (3 colour
-// channels each), indexed by unclamped coordinate relative to the tile origin:
+// Tile TW x TH; R = guided box radius (0: no guided node, 1: 3x3, 2: 5x5).
+// Shared-memory planes (3 colour channels each, float: every value stored is
+// either an f16 node output or an f32 intermediate, so no precision is lost),
+// indexed by unclamped coordinate relative to the tile origin:
 //   s_cm : colormatrix output at clamp(coord), coords [x0-2R, x0+TW+2R)
 //   s_bm : BM3D output at clamp(coord), same extent
 //   s_a/s_b : guided a, b at coords [x0-R, x0+TW+R)
 //   s_gf : guided output for the tile (needed whole for the wavelet 2x2 blocks)
 // The BM3D 2x2 block of a clamped coordinate xc is (xc & ~1, min(xc|1, w-1)),
 // always inside the s_cm extent because x0 and 2R are even.
-constexpr int kCTW = 32, kCTH = 16;
-
-template <class S>
-struct Plane;
-template <>
-struct Plane<__half> {
-    __device__ static float get(const __half* p, int i) { return __half2float(p[i]); }
-    __device__ static void put(__half* p, int i, float v) { p[i] = __float2half_rn(v); }
-};
-template <>
-struct Plane<float> {
-    __device__ static float get(const float* p, int i) { return p[i]; }
-    __device__ static void put(float* p, int i, float v) { p[i] = v; }
-};
+// Box sums keep the generator's row-major left-to-right order; a thread loads
+// one (G+2R) x (2R+1) window into registers and produces G outputs from it.
+constexpr int kCTW = 32, kCTH = 16, kCG = 4;
 
 struct ToneParams {
     int has_wavelet;
@@ -200,30 +101,52 @@ struct ToneParams {
     int has_lut;
 };
 
+template <int R>
+struct ToneGeom {
+    static constexpr int H = 2 * R;
+    static constexpr int CW = kCTW + 2 * H, CH = kCTH + 2 * H;  // cm / bm3d extent
+    static constexpr int AW = kCTW + 2 * R, AH = kCTH + 2 * R;  // a / b extent
+    static constexpr int AB = R > 0 ? AW * AH : 0;
+    static constexpr int D = 2 * R + 1;
+    static constexpr size_t bytes() {
+        return sizeof(float) * (size_t)(2 * 3 * CW * CH + 2 * 3 * AB + 3 * kCTW * kCTH);
+    }
+};
+
+// Sum of a D x D window (rows k..k+D-1 of `win`) in row-major order.
+template <int D, int ROWS>
+__device__ __forceinline__ float box_chain(const float (&win)[ROWS][D], int k) {
+    float s = win[k][0];
+#pragma unroll
+    for (int dy = 0; dy < D; ++dy)
+#pragma unroll
+        for (int dx = 0; dx < D; ++dx)
+            if (dy != 0 || dx != 0) s = s + win[k + dy][dx];
+    return s;
+}
+
 template <class T, bool F16, int R>
 __global__ void __launch_bounds__(256) denoise_tone_kernel(Img in, Img out, ToneParams p) {
-    using S = typename std::conditional<F16, __half, float>::type;  // storage of rounded planes
-    constexpr int H = 2 * R;
-    constexpr int CW = kCTW + 2 * H, CH = kCTH + 2 * H;  // cm / bm3d extent
-    constexpr int AW = kCTW + 2 * R, AH = kCTH + 2 * R;  // a / b extent (unused when R == 0)
-    extern __shared__ __align__(16) unsigned char smem[];
-    S* s_cm = reinterpret_cast<S*>(smem);
-    S* s_bm = s_cm + 3 * CW * CH;
-    float* s_a = reinterpret_cast<float*>(s_bm + 3 * CW * CH);
-    float* s_b = s_a + 3 * AW * AH;
-    S* s_gf = reinterpret_cast<S*>(s_b + 3 * AW * AH);
+    using Gm = ToneGeom<R>;
+    constexpr int H = Gm::H, CW = Gm::CW, CH = Gm::CH, AW = Gm::AW, AH = Gm::AH, AB = Gm::AB, D = Gm::D;
+    extern __shared__ __align__(16) float smem_f[];
+    float* s_cm = smem_f;
+    float* s_bm = s_cm + 3 * CW * CH;
+    float* s_a = s_bm + 3 * CW * CH;
+    float* s_b = s_a + 3 * AB;
+    float* s_gf = s_b + 3 * AB;
     const int x0 = blockIdx.x * kCTW, y0 = blockIdx.y * kCTH;
     const int cx0 = x0 - H, cy0 = y0 - H;
     // 1) colormatrix output at clamped coordinates
     for (int i = threadIdx.x; i < CW * CH; i += blockDim.x) {
         const int ty = i / CW, tx = i - ty * CW;
         const Rgba v = load_clamped<T>(in, cx0 + tx, cy0 + ty);
-        Plane<S>::put(s_cm, i, v.r);
-        Plane<S>::put(s_cm, CW * CH + i, v.g);
-        Plane<S>::put(s_cm, 2 * CW * CH + i, v.b);
+        s_cm[i] = v.r;
+        s_cm[CW * CH + i] = v.g;
+        s_cm[2 * CW * CH + i] = v.b;
     }
     __syncthreads();
-    // 2) BM3D parity form at clamped coordinates
+    // 2) BM3D parity form at clamped coordinates (rounded like the node's output)
     for (int i = threadIdx.x; i < CW * CH; i += blockDim.x) {
         const int ty = i / CW, tx = i - ty * CW;
         const int xc = clampi(cx0 + tx, 0, in.w - 1), yc = clampi(cy0 + ty, 0, in.h - 1);
@@ -234,63 +157,83 @@ __global__ void __launch_bounds__(256) denoise_tone_kernel(Img in, Img out, Tone
         const int lc = (yc - cy0) * CW + (xc - cx0);
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            const S* P = s_cm + c * CW * CH;
-            const float o = bm3d_blend(Plane<S>::get(P, lc), Plane<S>::get(P, l00), Plane<S>::get(P, l10),
-                                       Plane<S>::get(P, l01), Plane<S>::get(P, l11), p.bm3d_strength);
-            Plane<S>::put(s_bm, c * CW * CH + i, o);
+            const float* P = s_cm + c * CW * CH;
+            s_bm[c * CW * CH + i] = rnd<F16>(bm3d_blend(P[lc], P[l00], P[l10], P[l01], P[l11], p.bm3d_strength));
         }
     }
     __syncthreads();
-    // 3) guided a, b at unclamped coordinates [x0-R, x0+TW+R)
-    constexpr float N = (float)((2 * R + 1) * (2 * R + 1));
+    constexpr float N = (float)(D * D);
     if (R == 0) {  // no guided node: the wavelet reads the BM3D output
         for (int i = threadIdx.x; i < 3 * kCTW * kCTH; i += blockDim.x) {
             const int c = i / (kCTW * kCTH);
             const int j = i - c * kCTW * kCTH;
             const int ty = j / kCTW, tx = j - ty * kCTW;
-            Plane<S>::put(s_gf, i, Plane<S>::get(s_bm, c * CW * CH + ty * CW + tx));
+            s_gf[i] = s_bm[c * CW * CH + ty * CW + tx];
         }
-    }
-    for (int i = threadIdx.x; R > 0 && i < 3 * AW * AH; i += blockDim.x) {
-        const int c = i / (AW * AH);
-        const int j = i - c * AW * AH;
-        const int ty = j / AW, tx = j - ty * AW;
-        const S* V = s_bm + c * CW * CH + (ty + R) * CW + (tx + R);
-        float sm = 0.0F, sq = 0.0F;
-        bool first = true;
+    } else {
+        // 3) guided a, b at unclamped coordinates [x0-R, x0+TW+R), G rows per thread
+        constexpr int AG = (AH + kCG - 1) / kCG;
+        for (int item = threadIdx.x; item < 3 * AW * AG; item += blockDim.x) {
+            const int c = item / (AW * AG);
+            const int rem = item - c * AW * AG;
+            const int g = rem / AW, tx = rem - g * AW;
+            const int ty0 = g * kCG;
+            const float* V = s_bm + c * CW * CH + ty0 * CW + tx;  // window origin of output (ty0, tx)
+            float win[kCG + 2 * R][D], sq[kCG + 2 * R][D];
 #pragma unroll
-        for (int dy = -R; dy <= R; ++dy)
+            for (int r = 0; r < kCG + 2 * R; ++r)
 #pragma unroll
-            for (int dx = -R; dx <= R; ++dx) {
-                const float t = Plane<S>::get(V, dy * CW + dx);
-                if (R == 1 && first) { sm = t; sq = t * t; first = false; }
-                else { sm = sm + t; sq = sq + (t * t); }
+                for (int dx = 0; dx < D; ++dx) {
+                    win[r][dx] = (ty0 + r < CH) ? V[r * CW + dx] : 0.0F;
+                    sq[r][dx] = win[r][dx] * win[r][dx];
+                }
+#pragma unroll
+            for (int k = 0; k < kCG; ++k) {
+                if (ty0 + k >= AH) break;
+                const float m = box_chain<D>(win, k) / N, corr = box_chain<D>(sq, k) / N;
+                const float var = max0(corr - (m * m));
+                const float a = var / (var + p.eps);
+                const int j = c * AB + (ty0 + k) * AW + tx;
+                s_a[j] = a;
+                s_b[j] = m - (a * m);
             }
-        const float m = sm / N, corr = sq / N;
-        const float var = max0(corr - (m * m));
-        const float a = var / (var + p.eps);
-        s_a[i] = a;
-        s_b[i] = m - (a * m);
-    }
-    __syncthreads();
-    // 4) guided output for the tile
-    for (int i = threadIdx.x; R > 0 && i < 3 * kCTW * kCTH; i += blockDim.x) {
-        const int c = i / (kCTW * kCTH);
-        const int j = i - c * kCTW * kCTH;
-        const int ty = j / kCTW, tx = j - ty * kCTW;
-        const float* A = s_a + c * AW * AH + (ty + R) * AW + (tx + R);
-        const float* B = s_b + c * AW * AH + (ty + R) * AW + (tx + R);
-        float sa = 0.0F, sb = 0.0F;
-        bool first = true;
+        }
+        __syncthreads();
+        // 4) guided output for the tile: box of a and b
+        constexpr int TG = kCTH / kCG;
+        for (int item = threadIdx.x; item < 3 * kCTW * TG; item += blockDim.x) {
+            const int c = item / (kCTW * TG);
+            const int rem = item - c * kCTW * TG;
+            const int g = rem / kCTW, tx = rem - g * kCTW;
+            const int ty0 = g * kCG;
+            float sa[kCG], sb[kCG];
+            {
+                float win[kCG + 2 * R][D];
+                const float* A = s_a + c * AB + ty0 * AW + tx;
 #pragma unroll
-        for (int dy = -R; dy <= R; ++dy)
+                for (int r = 0; r < kCG + 2 * R; ++r)
 #pragma unroll
-            for (int dx = -R; dx <= R; ++dx) {
-                if (R == 1 && first) { sa = A[dy * AW + dx]; sb = B[dy * AW + dx]; first = false; }
-                else { sa = sa + A[dy * AW + dx]; sb = sb + B[dy * AW + dx]; }
+                    for (int dx = 0; dx < D; ++dx) win[r][dx] = A[r * AW + dx];
+#pragma unroll
+                for (int k = 0; k < kCG; ++k) sa[k] = box_chain<D>(win, k);
             }
-        const float v = Plane<S>::get(s_bm, c * CW * CH + (ty + H) * CW + (tx + H));
-        Plane<S>::put(s_gf, c * kCTW * kCTH + j, max0(((sa / N) * v) + (sb / N)));
+            {
+                float win[kCG + 2 * R][D];
+                const float* B = s_b + c * AB + ty0 * AW + tx;
+#pragma unroll
+                for (int r = 0; r < kCG + 2 * R; ++r)
+#pragma unroll
+                    for (int dx = 0; dx < D; ++dx) win[r][dx] = B[r * AW + dx];
+#pragma unroll
+                for (int k = 0; k < kCG; ++k) sb[k] = box_chain<D>(win, k);
+            }
+#pragma unroll
+            for (int k = 0; k < kCG; ++k) {
+                const int ty = ty0 + k;
+                const float v = s_bm[c * CW * CH + (ty + H) * CW + (tx + H)];
+                s_gf[c * kCTW * kCTH + ty * kCTW + tx] = rnd<F16>(max0(((sa[k] / N) * v) + (sb[k] / N)));
+            }
+        }
     }
     __syncthreads();
     // 5) wavelet on the aligned 2x2 block, filmic, LUT; one thread per pixel
@@ -305,8 +248,7 @@ __global__ void __launch_bounds__(256) denoise_tone_kernel(Img in, Img out, Tone
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
             const int l = ys[k >> 1] * kCTW + xs[k & 1];
-            q[k] = Rgba{Plane<S>::get(s_gf, l), Plane<S>::get(s_gf, kCTW * kCTH + l),
-                        Plane<S>::get(s_gf, 2 * kCTW * kCTH + l), 0.0F};
+            q[k] = Rgba{s_gf[l], s_gf[kCTW * kCTH + l], s_gf[2 * kCTW * kCTH + l], 0.0F};
         }
         // alpha runs through unchanged except the wavelet's max(0, .)
         const float alpha = load_rgba(px<const T>(in, x, y)).a;
@@ -327,13 +269,7 @@ __global__ void __launch_bounds__(256) denoise_tone_kernel(Img in, Img out, Tone
 
 template <class T, bool F16, int R>
 size_t denoise_tone_smem() {
-    using S = typename std::conditional<F16, __half, float>::type;
-    constexpr int H = 2 * R;
-    constexpr int CW = kCTW + 2 * H, CH = kCTH + 2 * H;
-    constexpr int AW = kCTW + 2 * R, AH = kCTH + 2 * R;
-    size_t s = 2 * 3 * CW * CH * sizeof(S);
-    s = (s + 15) & ~size_t(15);
-    return s + (R > 0 ? 2 * 3 * AW * AH * sizeof(float) : 0) + 3 * kCTW * kCTH * sizeof(S);
+    return ToneGeom<R>::bytes();
 }
 
 }  // namespace
@@ -390,7 +326,7 @@ int launch_chain(cpipe_cuda_chain* c, const void* d_raw, size_t raw_pitch, void*
     const Img mid0{c->d_mid[0], w, h, (long long)w * 4, 4};
     const Img mid1{c->d_mid[1], w, h, (long long)w * 4, 4};
     const Img out{d_out, w, h, (long long)(out_pitch ? out_pitch / elem : (size_t)w * 4), 4};
-    const dim3 ga((unsigned)((w + kATW - 1) / kATW), (unsigned)((h + kATH - 1) / kATH));
+    const dim3 ga((unsigned)((w + kDmTW - 1) / kDmTW), (unsigned)((h + kDmTH - 1) / kDmTH));
 #define K1(A)                                                                                        \
     if (c->f16) raw_to_rgba_kernel<A, __half><<<ga, 256, 0, st>>>(raw, mid0, c->raw);                \
     else raw_to_rgba_kernel<A, float><<<ga, 256, 0, st>>>(raw, mid0, c->raw);

@@ -639,12 +639,19 @@ int cpb_warp_dev(const cpipe_Opcode3DispatchRecord* r, int w, int h, WarpDev* ou
     out->count = (int)(r->coefficient_count < 4U ? r->coefficient_count : 4U);
     for (int i = 0; i < out->count; ++i) {
         const cpipe_Opcode3WarpCoefficient& k = r->coefficients[i];
-        out->k[i] = WarpCoefDev{split(k.kr0), split(k.kr1), split(k.kr2), split(k.kr3), split(k.kt0), split(k.kt1)};
+        WarpCoefDev& d = out->k[i];
+        d.kr0m1 = split(k.kr0 - 1.0);
+        d.kr1 = split(k.kr1);
+        d.kr2 = split(k.kr2);
+        d.kr3 = split(k.kr3);
+        d.t0 = split(k.kt0 / m);
+        d.t1 = split(k.kt1 / m);
+        d.has_kr3 = k.kr3 != 0.0;
+        d.has_tan = k.kt0 != 0.0 || k.kt1 != 0.0;
     }
     out->cx = split(cx);
     out->cy = split(cy);
-    out->m = split(m);
-    out->inv_m = split(1.0 / m);
+    out->inv_m2 = split(1.0 / (m * m));
     out->xmax = (float)(w - 1);
     out->ymax = (float)(h - 1);
     return CPIPE_OK;

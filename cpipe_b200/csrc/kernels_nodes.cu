@@ -6,6 +6,7 @@
 // shared-memory halo tiles for the stencil nodes.
 #include <type_traits>
 
+#include "demosaic.cuh"
 #include "kernels.h"
 #include "nodes.cuh"
 
@@ -92,86 +93,13 @@ __global__ void copy_rows_kernel(const char* src, long long src_pitch, char* dst
 }
 
 // ---------------------------------------------------------------- demosaic
-// Tile of TW x TH outputs; shared memory holds the clamped input with a halo
-// of 3 (RCD/AMaZE read green/chroma at +-1 whose stencils reach +-2) and the
-// green plane for the tile plus a halo of 1.
-constexpr int kDmTW = 64, kDmTH = 16, kDmHalo = 3;
-constexpr int kDmIW = kDmTW + 2 * kDmHalo, kDmIH = kDmTH + 2 * kDmHalo;
-constexpr int kDmGW = kDmTW + 2, kDmGH = kDmTH + 2;
-
-struct SmemTap {
-    const float* base;  // points at the pixel being evaluated
-    __device__ __forceinline__ float operator()(int dx, int dy) const { return base[dy * kDmIW + dx]; }
+struct F32Loader {
+    Img in;
+    __device__ __forceinline__ float operator()(int gx, int gy) const { return *px<const float>(in, gx, gy); }
 };
-
 template <int ALGO, class TOut>
 __global__ void __launch_bounds__(256) demosaic_kernel(Img in, Img out, Cfa cfa) {
-    __shared__ float s_in[kDmIH * kDmIW];
-    __shared__ float s_g[kDmGH * kDmGW];
-    const int x0 = blockIdx.x * kDmTW, y0 = blockIdx.y * kDmTH;
-    const int tid = threadIdx.x;
-    for (int i = tid; i < kDmIH * kDmIW; i += blockDim.x) {
-        const int ty = i / kDmIW, tx = i - ty * kDmIW;
-        const int gx = clampi(x0 - kDmHalo + tx, 0, in.w - 1), gy = clampi(y0 - kDmHalo + ty, 0, in.h - 1);
-        s_in[i] = *px<const float>(in, gx, gy);
-    }
-    __syncthreads();
-    if (ALGO != 0) {
-        for (int i = tid; i < kDmGH * kDmGW; i += blockDim.x) {
-            const int ty = i / kDmGW, tx = i - ty * kDmGW;
-            const int x = x0 - 1 + tx, y = y0 - 1 + ty;
-            const SmemTap T{s_in + (ty + kDmHalo - 1) * kDmIW + (tx + kDmHalo - 1)};
-            s_g[i] = ALGO == 1 ? rcd_green(T, x, y, cfa) : amaze_green(T, x, y, cfa);
-        }
-        __syncthreads();
-    }
-    for (int i = tid; i < kDmTH * kDmTW; i += blockDim.x) {
-        const int ty = i / kDmTW, tx = i - ty * kDmTW;
-        const int x = x0 + tx, y = y0 + ty;
-        if (x >= out.w || y >= out.h) continue;
-        const float* c = s_in + (ty + kDmHalo) * kDmIW + (tx + kDmHalo);
-        const SmemTap T{c};
-        const float ctr = c[0];
-        const int site = cfa.at(x, y);
-        const bool red = site == 0, blue = site == 2;
-        const bool hred = cfa.at(x - 1, y) == 0, hblue = cfa.at(x - 1, y) == 2;
-        float r, g, b;
-        if (ALGO == 0) {  // demosaic_bilinear_generator.cpp:23-41
-            const float hz = 0.5F * (T(-1, 0) + T(1, 0));
-            const float vt = 0.5F * (T(0, -1) + T(0, 1));
-            const float cross = 0.25F * (T(-1, 0) + T(1, 0) + T(0, -1) + T(0, 1));
-            const float diag = 0.25F * (T(-1, -1) + T(1, -1) + T(-1, 1) + T(1, 1));
-            r = red ? ctr : blue ? diag : hred ? hz : vt;
-            g = (red || blue) ? cross : ctr;
-            b = blue ? ctr : red ? diag : hred ? vt : hz;
-        } else {
-            const float* G = s_g + (ty + 1) * kDmGW + (tx + 1);
-#define GG(dx, dy) G[(dy) * kDmGW + (dx)]
-            const float gc = GG(0, 0);
-            if (ALGO == 1) {  // demosaic_rcd_generator.cpp:37-63
-#define RT(dx, dy) (T(dx, dy) / maxf(GG(dx, dy), 0.000001F))
-                const float rh = gc * 0.5F * (RT(-1, 0) + RT(1, 0));
-                const float rv = gc * 0.5F * (RT(0, -1) + RT(0, 1));
-                const float rd = gc * 0.25F * (RT(-1, -1) + RT(1, -1) + RT(-1, 1) + RT(1, 1));
-#undef RT
-                r = max0(red ? ctr : blue ? rd : hred ? rh : rv);
-                g = max0(gc);
-                b = max0(blue ? ctr : red ? rd : hblue ? rh : rv);
-            } else {  // demosaic_amaze_generator.cpp:48-66
-#define CH(dx, dy) (T(dx, dy) - GG(dx, dy))
-                const float chh = 0.5F * (CH(-1, 0) + CH(1, 0));
-                const float chv = 0.5F * (CH(0, -1) + CH(0, 1));
-                const float chd = 0.25F * (CH(-1, -1) + CH(1, -1) + CH(-1, 1) + CH(1, 1));
-#undef CH
-                const float rh = gc + chh, rv = gc + chv, rd = gc + chd;
-                r = max0(red ? ctr : (blue ? rd : hred ? rh : rv));
-                g = max0(gc);
-                b = max0(blue ? ctr : (red ? rd : hblue ? rh : rv));
-            }
-#undef GG
-        }
-        store_rgba(px<TOut>(out, x, y), Rgba{r, g, b, 1.0F});
-    }
+    demosaic_tile<ALGO, TOut>(F32Loader{in}, in.w, in.h, out, cfa);
 }
 
 // ---------------------------------------------------------------- QBC remosaic
@@ -393,37 +321,7 @@ template <class T, bool F16>
 __global__ void __launch_bounds__(128) warp_kernel(Img in, Img out, WarpDev w) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     if (x >= out.w) return;
-    const ff dx = ff_mul(ff_sub(ff_from((float)x), w.cx), w.inv_m);
-    const ff dy = ff_mul(ff_sub(ff_from((float)y), w.cy), w.inv_m);
-    const ff r2 = ff_add(ff_mul(dx, dx), ff_mul(dy, dy));
-    const ff r4 = ff_mul(r2, r2), r6 = ff_mul(r4, r2);
-    float res[4];
-    int done_for = -1;
-    Rgba shared_val{};
-    for (int c = 0; c < 4; ++c) {
-        const int ci = c < w.count - 1 ? c : w.count - 1;
-        if (ci == done_for) {  // same coefficient set as the previous channel
-            res[c] = c == 1 ? shared_val.g : c == 2 ? shared_val.b : shared_val.a;
-            continue;
-        }
-        ff sx, sy;
-        warp_src(w, w.k[ci], dx, dy, r2, r4, r6, &sx, &sy);
-        sx = ff_clamp0(sx, w.xmax);
-        sy = ff_clamp0(sy, w.ymax);
-        const int ix = ff_floor(sx), iy = ff_floor(sy);
-        const float tx = ff_frac(sx, ix), ty = ff_frac(sy, iy);
-        Rgba rows[4];
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-            const int yy = iy + r - 1;
-            rows[r] = cubic4(load_clamped<T>(in, ix - 1, yy), load_clamped<T>(in, ix, yy),
-                             load_clamped<T>(in, ix + 1, yy), load_clamped<T>(in, ix + 2, yy), tx);
-        }
-        shared_val = cubic4(rows[0], rows[1], rows[2], rows[3], ty);
-        done_for = ci;
-        res[c] = c == 0 ? shared_val.r : c == 1 ? shared_val.g : c == 2 ? shared_val.b : shared_val.a;
-    }
-    store_rgba(px<T>(out, x, y), Rgba{res[0], res[1], res[2], res[3]});
+    store_rgba(px<T>(out, x, y), warp_px<T>(in, w, x, y));
 }
 
 // FixVignetteRadial (:126-158): gain evaluated in float-float, value*gain rounded to float.

@@ -112,10 +112,14 @@ __device__ __forceinline__ Rgba cm_px(Rgba v, const float t[9]) {
 struct FilmicDev {
     float exposure, inv_contrast, saturation, highlights, shadows, log_white;
 };
+// Two exact shortcuts for the default parameters: pow(x, 1) == x for x >= 0
+// (the reference's libm powf returns x exactly), and with shadows == highlights
+// == 1 both range terms are +0, so v + sd + hd == v.
 __device__ __forceinline__ float filmic_tone(float value, const FilmicDev& p) {
     const float e = max0(value * p.exposure);
     const float curved = clampf(logf(1.0F + (6.0F * e)) / p.log_white, 0.0F, 1.0F);
-    const float v = powf(max0(curved), p.inv_contrast);
+    const float v = p.inv_contrast == 1.0F ? max0(curved) : powf(max0(curved), p.inv_contrast);
+    if (p.shadows == 1.0F && p.highlights == 1.0F) return clampf(v, 0.0F, 1.0F);
     const float sd = (p.shadows - 1.0F) * 0.08F * (1.0F - v) * (1.0F - v);
     const float hd = (p.highlights - 1.0F) * 0.08F * v * v;
     return clampf(v + sd + hd, 0.0F, 1.0F);
@@ -230,32 +234,100 @@ __device__ __forceinline__ Rgba cubic4(Rgba p0, Rgba p1, Rgba p2, Rgba p3, float
                 cubic(p0.b, p1.b, p2.b, p3.b, t), cubic(p0.a, p1.a, p2.a, p3.a, t)};
 }
 
-// Warp coefficients converted to float-float on the host.
+// Warp coefficients converted to float-float on the host, in pixel units.
+// The reference evaluates, in double (dng_opcode_list_3_dispatch.cpp:103-115),
+//   dx = X/m, dy = Y/m, r2 = dx^2 + dy^2, f = kr0 + kr1 r2 + kr2 r2^2 + kr3 r2^3
+//   sx = cx + m (f dx + 2 kt0 dx dy + kt1 (r2 + 2 dx^2))           (sy alike)
+// with X = x - cx, Y = y - cy.  Multiplying the m through gives the same real
+// number as
+//   sx = x + (f - 1) X + 2 t0 X Y + t1 (q + 2 X^2),  q = X^2 + Y^2, r2 = q / m^2,
+//   t0 = kt0 / m, t1 = kt1 / m,
+// which needs far fewer float-float operations; its float-float error (~1e-12 px)
+// is far below the binary32 spacing of the bicubic weight it feeds.
 struct WarpCoefDev {
-    ff kr0, kr1, kr2, kr3, kt0, kt1;
+    ff kr0m1, kr1, kr2, kr3, t0, t1;  // kr0 - 1, kr1..kr3, kt0 / m, kt1 / m
+    int has_kr3, has_tan;
 };
 struct WarpDev {
     int count;  // 1..4 coefficient sets; channel c uses min(c, count-1)
     WarpCoefDev k[4];
-    ff cx, cy, m, inv_m;
-    float xmax, ymax;  // w-1, h-1
+    ff cx, cy, inv_m2;  // inv_m2 = 1 / m^2
+    float xmax, ymax;   // w-1, h-1
 };
-// Source coordinate of output pixel (x, y) for coefficient set k
-// (dng_opcode_list_3_dispatch.cpp:103-115), in float-float.
-__device__ __forceinline__ void warp_src(const WarpDev& w, const WarpCoefDev& k, ff dx, ff dy, ff r2,
-                                         ff r4, ff r6, ff* sx, ff* sy) {
-    const ff f = ff_add(ff_add(ff_add(k.kr0, ff_mul(k.kr1, r2)), ff_mul(k.kr2, r4)), ff_mul(k.kr3, r6));
-    const ff two = ff_from(2.0F);
-    const ff dxdy = ff_mul(dx, dy);
-    const ff tx = ff_add(ff_mul(ff_mul(two, k.kt0), dxdy), ff_mul(k.kt1, ff_add(r2, ff_mul(ff_mul(two, dx), dx))));
-    const ff ty = ff_add(ff_mul(k.kt0, ff_add(r2, ff_mul(ff_mul(two, dy), dy))), ff_mul(ff_mul(two, k.kt1), dxdy));
-    *sx = ff_add(w.cx, ff_mul(w.m, ff_add(ff_mul(f, dx), tx)));
-    *sy = ff_add(w.cy, ff_mul(w.m, ff_add(ff_mul(f, dy), ty)));
+__device__ __forceinline__ ff ff_add_f(ff a, float b) {
+    ff s = two_sum(a.hi, b);
+    s.lo = __fadd_rn(s.lo, a.lo);
+    return quick_two_sum(s.hi, s.lo);
 }
+__device__ __forceinline__ ff ff_scale2(ff a) { return ff{a.hi * 2.0F, a.lo * 2.0F}; }
+// Source coordinate of output pixel (x, y) for coefficient set k.
+__device__ __forceinline__ void warp_src(const WarpCoefDev& k, float x, float y, ff X, ff Y, ff q, ff r2, ff* sx,
+                                         ff* sy) {
+    // (f - 1) by Horner in r2
+    ff p = k.has_kr3 ? ff_add(k.kr2, ff_mul(r2, k.kr3)) : k.kr2;
+    p = ff_add(k.kr1, ff_mul(r2, p));
+    const ff fm1 = ff_add(k.kr0m1, ff_mul(r2, p));
+    ff dx = ff_mul(fm1, X), dy = ff_mul(fm1, Y);
+    if (k.has_tan) {
+        const ff xy2 = ff_scale2(ff_mul(X, Y));
+        dx = ff_add(dx, ff_add(ff_mul(k.t0, xy2), ff_mul(k.t1, ff_add(q, ff_scale2(ff_mul(X, X))))));
+        dy = ff_add(dy, ff_add(ff_mul(k.t0, ff_add(q, ff_scale2(ff_mul(Y, Y)))), ff_mul(k.t1, xy2)));
+    }
+    *sx = ff_add_f(dx, x);
+    *sy = ff_add_f(dy, y);
+}
+// Bicubic sample (all four channels) of the warp output pixel (x, y) for
+// coefficient set k: source coordinate clamped to the frame, Catmull-Rom taps
+// with clamped reads (sample_bicubic :55-73).
+template <class T>
+__device__ __forceinline__ Rgba warp_sample(const Img& in, const WarpDev& w, const WarpCoefDev& k, float x, float y,
+                                            ff X, ff Y, ff q, ff r2);
 // Clamp a float-float coordinate to [0, maxv] (sample_bicubic :57-58).
 __device__ __forceinline__ ff ff_clamp0(ff v, float maxv) {
     if (v.hi < 0.0F || (v.hi == 0.0F && v.lo < 0.0F)) return ff_from(0.0F);
     if (v.hi > maxv || (v.hi == maxv && v.lo > 0.0F)) return ff_from(maxv);
+    return v;
+}
+
+template <class T>
+__device__ __forceinline__ Rgba warp_sample(const Img& in, const WarpDev& w, const WarpCoefDev& k, float x, float y,
+                                            ff X, ff Y, ff q, ff r2) {
+    ff sx, sy;
+    warp_src(k, x, y, X, Y, q, r2, &sx, &sy);
+    sx = ff_clamp0(sx, w.xmax);
+    sy = ff_clamp0(sy, w.ymax);
+    const int ix = ff_floor(sx), iy = ff_floor(sy);
+    const float tx = ff_frac(sx, ix), ty = ff_frac(sy, iy);
+    Rgba rows[4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+        const int yy = iy + r - 1;
+        rows[r] = cubic4(load_clamped<T>(in, ix - 1, yy), load_clamped<T>(in, ix, yy), load_clamped<T>(in, ix + 1, yy),
+                         load_clamped<T>(in, ix + 2, yy), tx);
+    }
+    return cubic4(rows[0], rows[1], rows[2], rows[3], ty);
+}
+
+// Warp output pixel (x, y), all channels (channel c uses coefficient set min(c, count-1)).
+template <class T>
+__device__ __forceinline__ Rgba warp_px(const Img& in, const WarpDev& w, int x, int y) {
+    const float fx = (float)x, fy = (float)y;
+    const ff X = ff_add_f(ff_neg(w.cx), fx), Y = ff_add_f(ff_neg(w.cy), fy);
+    const ff q = ff_add(ff_mul(X, X), ff_mul(Y, Y));
+    const ff r2 = ff_mul(q, w.inv_m2);
+    Rgba v = warp_sample<T>(in, w, w.k[0], fx, fy, X, Y, q, r2);
+    if (w.count > 1) {
+        const Rgba g = warp_sample<T>(in, w, w.k[1], fx, fy, X, Y, q, r2);
+        v.g = g.g;
+        v.b = g.b;
+        v.a = g.a;
+        if (w.count > 2) {
+            const Rgba b = warp_sample<T>(in, w, w.k[2], fx, fy, X, Y, q, r2);
+            v.b = b.b;
+            v.a = b.a;
+            if (w.count > 3) v.a = warp_sample<T>(in, w, w.k[3], fx, fy, X, Y, q, r2).a;
+        }
+    }
     return v;
 }
 
