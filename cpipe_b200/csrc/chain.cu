@@ -80,15 +80,16 @@ __global__ void __launch_bounds__(128) warp_wb_cm_kernel(Img in, Img out, WarpDe
 // Shared-memory planes (3 colour channels each, float: every value stored is
 // either an f16 node output or an f32 intermediate, so no precision is lost),
 // indexed by unclamped coordinate relative to the tile origin:
-//   s_cm : colormatrix output at clamp(coord), coords [x0-2R, x0+TW+2R)
-//   s_bm : BM3D output at clamp(coord), same extent
+//   s_bm : BM3D output at clamp(coord), coords [x0-2R, x0+TW+2R)
 //   s_a/s_b : guided a, b at coords [x0-R, x0+TW+R)
 //   s_gf : guided output for the tile (needed whole for the wavelet 2x2 blocks)
-// The BM3D 2x2 block of a clamped coordinate xc is (xc & ~1, min(xc|1, w-1)),
-// always inside the s_cm extent because x0 and 2R are even.
+// BM3D is evaluated per 2x2 block of the extent (x0 and 2R are even, so the
+// extent is made of whole blocks): an interior block reads its four input
+// pixels with two 16-byte loads and yields four outputs; a block that overlaps
+// the frame border evaluates each cell at its clamped coordinate.
 // Box sums keep the generator's row-major left-to-right order; a thread loads
 // one (G+2R) x (2R+1) window into registers and produces G outputs from it.
-constexpr int kCTW = 32, kCTH = 16, kCG = 4;
+constexpr int kCTW = 64, kCTH = 16, kCG = 4;
 
 struct ToneParams {
     int has_wavelet;
@@ -104,13 +105,13 @@ struct ToneParams {
 template <int R>
 struct ToneGeom {
     static constexpr int H = 2 * R;
-    static constexpr int CW = kCTW + 2 * H, CH = kCTH + 2 * H;  // cm / bm3d extent
+    static constexpr int CW = kCTW + 2 * H, CH = kCTH + 2 * H;  // bm3d extent
+    static constexpr int CP = CW + 1;                           // padded row pitch
     static constexpr int AW = kCTW + 2 * R, AH = kCTH + 2 * R;  // a / b extent
-    static constexpr int AB = R > 0 ? AW * AH : 0;
+    static constexpr int AP = AW + 1;
+    static constexpr int AB = R > 0 ? AP * AH : 0;
     static constexpr int D = 2 * R + 1;
-    static constexpr size_t bytes() {
-        return sizeof(float) * (size_t)(2 * 3 * CW * CH + 2 * 3 * AB + 3 * kCTW * kCTH);
-    }
+    static constexpr size_t bytes() { return sizeof(float) * (size_t)(3 * CP * CH + 2 * 3 * AB + 3 * kCTW * kCTH); }
 };
 
 // Sum of a D x D window (rows k..k+D-1 of `win`) in row-major order.
@@ -125,40 +126,74 @@ __device__ __forceinline__ float box_chain(const float (&win)[ROWS][D], int k) {
     return s;
 }
 
+template <class T>
+__device__ __forceinline__ void load_pair(const Img& in, int x, int y, Rgba* a, Rgba* b);
+// Two adjacent RGBA16F pixels; one 16-byte load when the pair is 16-byte
+// aligned (always for even x when the row pitch is a multiple of 16 bytes),
+// else two 8-byte loads.
+template <>
+__device__ __forceinline__ void load_pair<__half>(const Img& in, int x, int y, Rgba* a, Rgba* b) {
+    const __half* p0 = px<const __half>(in, x, y);
+    if ((reinterpret_cast<uintptr_t>(p0) & 15) != 0) {
+        *a = load_rgba(p0);
+        *b = load_rgba(p0 + in.pix_stride);
+        return;
+    }
+    const uint4 u = *reinterpret_cast<const uint4*>(p0);
+    const __half2 h0 = *reinterpret_cast<const __half2*>(&u.x), h1 = *reinterpret_cast<const __half2*>(&u.y);
+    const __half2 h2 = *reinterpret_cast<const __half2*>(&u.z), h3 = *reinterpret_cast<const __half2*>(&u.w);
+    *a = Rgba{__low2float(h0), __high2float(h0), __low2float(h1), __high2float(h1)};
+    *b = Rgba{__low2float(h2), __high2float(h2), __low2float(h3), __high2float(h3)};
+}
+template <>
+__device__ __forceinline__ void load_pair<float>(const Img& in, int x, int y, Rgba* a, Rgba* b) {
+    *a = load_rgba(px<const float>(in, x, y));
+    *b = load_rgba(px<const float>(in, x + 1, y));
+}
+
 template <class T, bool F16, int R>
-__global__ void __launch_bounds__(256) denoise_tone_kernel(Img in, Img out, ToneParams p) {
+__global__ void __launch_bounds__(256, 3) denoise_tone_kernel(Img in, Img out, ToneParams p) {
     using Gm = ToneGeom<R>;
-    constexpr int H = Gm::H, CW = Gm::CW, CH = Gm::CH, AW = Gm::AW, AH = Gm::AH, AB = Gm::AB, D = Gm::D;
+    constexpr int H = Gm::H, CW = Gm::CW, CH = Gm::CH, CP = Gm::CP, AW = Gm::AW, AH = Gm::AH, AP = Gm::AP;
+    constexpr int AB = Gm::AB, D = Gm::D;
     extern __shared__ __align__(16) float smem_f[];
-    float* s_cm = smem_f;
-    float* s_bm = s_cm + 3 * CW * CH;
-    float* s_a = s_bm + 3 * CW * CH;
+    float* s_bm = smem_f;
+    float* s_a = s_bm + 3 * CP * CH;
     float* s_b = s_a + 3 * AB;
     float* s_gf = s_b + 3 * AB;
     const int x0 = blockIdx.x * kCTW, y0 = blockIdx.y * kCTH;
     const int cx0 = x0 - H, cy0 = y0 - H;
-    // 1) colormatrix output at clamped coordinates
-    for (int i = threadIdx.x; i < CW * CH; i += blockDim.x) {
-        const int ty = i / CW, tx = i - ty * CW;
-        const Rgba v = load_clamped<T>(in, cx0 + tx, cy0 + ty);
-        s_cm[i] = v.r;
-        s_cm[CW * CH + i] = v.g;
-        s_cm[2 * CW * CH + i] = v.b;
-    }
-    __syncthreads();
-    // 2) BM3D parity form at clamped coordinates (rounded like the node's output)
-    for (int i = threadIdx.x; i < CW * CH; i += blockDim.x) {
-        const int ty = i / CW, tx = i - ty * CW;
-        const int xc = clampi(cx0 + tx, 0, in.w - 1), yc = clampi(cy0 + ty, 0, in.h - 1);
-        const int bx = xc & ~1, by = yc & ~1;
-        const int bx1 = min(bx + 1, in.w - 1), by1 = min(by + 1, in.h - 1);
-        const int l00 = (by - cy0) * CW + (bx - cx0), l10 = (by - cy0) * CW + (bx1 - cx0);
-        const int l01 = (by1 - cy0) * CW + (bx - cx0), l11 = (by1 - cy0) * CW + (bx1 - cx0);
-        const int lc = (yc - cy0) * CW + (xc - cx0);
+    const float s = p.bm3d_strength;
+    // 1) BM3D parity form (bm3d_step1_generator.cpp:42-56) per 2x2 block of the extent
+    for (int item = threadIdx.x; item < (CW / 2) * (CH / 2); item += blockDim.x) {
+        const int by2 = item / (CW / 2), bx2 = item - by2 * (CW / 2);
+        const int u = cx0 + 2 * bx2, v = cy0 + 2 * by2;  // unclamped block origin
+        const int l = (2 * by2) * CP + 2 * bx2;
+        if (u >= 0 && u + 1 < in.w && v >= 0 && v + 1 < in.h) {
+            Rgba q[4];
+            load_pair<T>(in, u, v, &q[0], &q[1]);
+            load_pair<T>(in, u, v + 1, &q[2], &q[3]);
 #pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            const float* P = s_cm + c * CW * CH;
-            s_bm[c * CW * CH + i] = rnd<F16>(bm3d_blend(P[lc], P[l00], P[l10], P[l01], P[l11], p.bm3d_strength));
+            for (int k = 0; k < 4; ++k) {
+                const int o = l + (k >> 1) * CP + (k & 1);
+                s_bm[o] = rnd<F16>(bm3d_blend(q[k].r, q[0].r, q[1].r, q[2].r, q[3].r, s));
+                s_bm[CP * CH + o] = rnd<F16>(bm3d_blend(q[k].g, q[0].g, q[1].g, q[2].g, q[3].g, s));
+                s_bm[2 * CP * CH + o] = rnd<F16>(bm3d_blend(q[k].b, q[0].b, q[1].b, q[2].b, q[3].b, s));
+            }
+        } else {
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                const int xc = clampi(u + (k & 1), 0, in.w - 1), yc = clampi(v + (k >> 1), 0, in.h - 1);
+                const int bx = xc & ~1, by = yc & ~1;
+                const int bx1 = min(bx + 1, in.w - 1), by1 = min(by + 1, in.h - 1);
+                const Rgba q0 = load_rgba(px<const T>(in, bx, by)), q1 = load_rgba(px<const T>(in, bx1, by));
+                const Rgba q2 = load_rgba(px<const T>(in, bx, by1)), q3 = load_rgba(px<const T>(in, bx1, by1));
+                const Rgba c = load_rgba(px<const T>(in, xc, yc));
+                const int o = l + (k >> 1) * CP + (k & 1);
+                s_bm[o] = rnd<F16>(bm3d_blend(c.r, q0.r, q1.r, q2.r, q3.r, s));
+                s_bm[CP * CH + o] = rnd<F16>(bm3d_blend(c.g, q0.g, q1.g, q2.g, q3.g, s));
+                s_bm[2 * CP * CH + o] = rnd<F16>(bm3d_blend(c.b, q0.b, q1.b, q2.b, q3.b, s));
+            }
         }
     }
     __syncthreads();
@@ -168,23 +203,24 @@ __global__ void __launch_bounds__(256) denoise_tone_kernel(Img in, Img out, Tone
             const int c = i / (kCTW * kCTH);
             const int j = i - c * kCTW * kCTH;
             const int ty = j / kCTW, tx = j - ty * kCTW;
-            s_gf[i] = s_bm[c * CW * CH + ty * CW + tx];
+            s_gf[i] = s_bm[c * CP * CH + ty * CP + tx];
         }
     } else {
-        // 3) guided a, b at unclamped coordinates [x0-R, x0+TW+R), G rows per thread
+        // 2) guided a, b (guided_filter_generator.cpp:60-76) at unclamped
+        //    coordinates [x0-R, x0+TW+R), kCG rows per thread
         constexpr int AG = (AH + kCG - 1) / kCG;
         for (int item = threadIdx.x; item < 3 * AW * AG; item += blockDim.x) {
             const int c = item / (AW * AG);
             const int rem = item - c * AW * AG;
             const int g = rem / AW, tx = rem - g * AW;
             const int ty0 = g * kCG;
-            const float* V = s_bm + c * CW * CH + ty0 * CW + tx;  // window origin of output (ty0, tx)
+            const float* V = s_bm + c * CP * CH + ty0 * CP + tx;  // window origin of output (ty0, tx)
             float win[kCG + 2 * R][D], sq[kCG + 2 * R][D];
 #pragma unroll
             for (int r = 0; r < kCG + 2 * R; ++r)
 #pragma unroll
                 for (int dx = 0; dx < D; ++dx) {
-                    win[r][dx] = (ty0 + r < CH) ? V[r * CW + dx] : 0.0F;
+                    win[r][dx] = (ty0 + r < CH) ? V[r * CP + dx] : 0.0F;
                     sq[r][dx] = win[r][dx] * win[r][dx];
                 }
 #pragma unroll
@@ -193,13 +229,13 @@ __global__ void __launch_bounds__(256) denoise_tone_kernel(Img in, Img out, Tone
                 const float m = box_chain<D>(win, k) / N, corr = box_chain<D>(sq, k) / N;
                 const float var = max0(corr - (m * m));
                 const float a = var / (var + p.eps);
-                const int j = c * AB + (ty0 + k) * AW + tx;
+                const int j = c * AB + (ty0 + k) * AP + tx;
                 s_a[j] = a;
                 s_b[j] = m - (a * m);
             }
         }
         __syncthreads();
-        // 4) guided output for the tile: box of a and b
+        // 3) guided output for the tile: mean(a) * v + mean(b)
         constexpr int TG = kCTH / kCG;
         for (int item = threadIdx.x; item < 3 * kCTW * TG; item += blockDim.x) {
             const int c = item / (kCTW * TG);
@@ -209,53 +245,53 @@ __global__ void __launch_bounds__(256) denoise_tone_kernel(Img in, Img out, Tone
             float sa[kCG], sb[kCG];
             {
                 float win[kCG + 2 * R][D];
-                const float* A = s_a + c * AB + ty0 * AW + tx;
+                const float* A = s_a + c * AB + ty0 * AP + tx;
 #pragma unroll
                 for (int r = 0; r < kCG + 2 * R; ++r)
 #pragma unroll
-                    for (int dx = 0; dx < D; ++dx) win[r][dx] = A[r * AW + dx];
+                    for (int dx = 0; dx < D; ++dx) win[r][dx] = A[r * AP + dx];
 #pragma unroll
                 for (int k = 0; k < kCG; ++k) sa[k] = box_chain<D>(win, k);
             }
             {
                 float win[kCG + 2 * R][D];
-                const float* B = s_b + c * AB + ty0 * AW + tx;
+                const float* B = s_b + c * AB + ty0 * AP + tx;
 #pragma unroll
                 for (int r = 0; r < kCG + 2 * R; ++r)
 #pragma unroll
-                    for (int dx = 0; dx < D; ++dx) win[r][dx] = B[r * AW + dx];
+                    for (int dx = 0; dx < D; ++dx) win[r][dx] = B[r * AP + dx];
 #pragma unroll
                 for (int k = 0; k < kCG; ++k) sb[k] = box_chain<D>(win, k);
             }
 #pragma unroll
             for (int k = 0; k < kCG; ++k) {
                 const int ty = ty0 + k;
-                const float v = s_bm[c * CW * CH + (ty + H) * CW + (tx + H)];
+                const float v = s_bm[c * CP * CH + (ty + H) * CP + (tx + H)];
                 s_gf[c * kCTW * kCTH + ty * kCTW + tx] = rnd<F16>(max0(((sa[k] / N) * v) + (sb[k] / N)));
             }
         }
     }
     __syncthreads();
-    // 5) wavelet on the aligned 2x2 block, filmic, LUT; one thread per pixel
+    // 4) wavelet on the aligned 2x2 block, filmic, LUT; one thread per pixel
     for (int j = threadIdx.x; j < kCTW * kCTH; j += blockDim.x) {
         const int ty = j / kCTW, tx = j - ty * kCTW;
         const int x = x0 + tx, y = y0 + ty;
         if (x >= out.w || y >= out.h) continue;
         const int bx = x & ~1, by = y & ~1;
-        const int xs[2] = {bx - x0, min(bx + 1, out.w - 1) - x0};
-        const int ys[2] = {by - y0, min(by + 1, out.h - 1) - y0};
+        const int xs0 = bx - x0, xs1 = min(bx + 1, out.w - 1) - x0;
+        const int ys0 = by - y0, ys1 = min(by + 1, out.h - 1) - y0;
         Rgba q[4];
 #pragma unroll
         for (int k = 0; k < 4; ++k) {
-            const int l = ys[k >> 1] * kCTW + xs[k & 1];
+            const int l = ((k >> 1) ? ys1 : ys0) * kCTW + ((k & 1) ? xs1 : xs0);
             q[k] = Rgba{s_gf[l], s_gf[kCTW * kCTH + l], s_gf[2 * kCTW * kCTH + l], 0.0F};
         }
         // alpha runs through unchanged except the wavelet's max(0, .)
-        const float alpha = load_rgba(px<const T>(in, x, y)).a;
-        q[(y & 1) * 2 + (x & 1)].a = alpha;
-        Rgba v = q[(y & 1) * 2 + (x & 1)];
+        const int ox = x & 1, oy = y & 1;
+        const Rgba own = oy ? (ox ? q[3] : q[2]) : (ox ? q[1] : q[0]);
+        Rgba v{own.r, own.g, own.b, load_rgba(px<const T>(in, x, y)).a};
         if (p.has_wavelet) {
-            v = wavelet_px(q, x & 1, y & 1, p.wavelet_th);
+            v = wavelet_px(q, v, ox, oy, p.wavelet_th);
             v = Rgba{rnd<F16>(v.r), rnd<F16>(v.g), rnd<F16>(v.b), rnd<F16>(v.a)};
         }
         v = filmic_px(v, p.filmic);
@@ -369,8 +405,12 @@ int launch_chain(cpipe_cuda_chain* c, const void* d_raw, size_t raw_pitch, void*
 
 template <class T, bool F, int R>
 cudaError_t allow_smem() {
-    return cudaFuncSetAttribute(denoise_tone_kernel<T, F, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)denoise_tone_smem<T, F, R>());
+    cudaError_t e = cudaFuncSetAttribute(denoise_tone_kernel<T, F, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)denoise_tone_smem<T, F, R>());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(denoise_tone_kernel<T, F, R>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared);
+    return e;
 }
 
 }  // namespace

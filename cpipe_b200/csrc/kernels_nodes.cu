@@ -241,7 +241,7 @@ __global__ void __launch_bounds__(256) wavelet_kernel(Img in, Img out, float th)
     for (int k = 0; k < 4; ++k) {
         const int x = bx + (k & 1), y = by + (k >> 1);
         if (x >= out.w || y >= out.h) continue;
-        store_rgba(px<T>(out, x, y), wavelet_px(q, k & 1, k >> 1, th));
+        store_rgba(px<T>(out, x, y), wavelet_px(q, q[k], k & 1, k >> 1, th));
     }
 }
 

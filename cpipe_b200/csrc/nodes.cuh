@@ -210,11 +210,11 @@ __device__ __forceinline__ float haar_pick(const HaarBand& b, int ox, int oy) {
 }
 __device__ __forceinline__ float wv_co(Rgba p) { return p.r - p.b; }
 __device__ __forceinline__ float wv_cg(Rgba p) { return p.g - ((p.r + p.b) * 0.5F); }
-// Output for pixel (ox, oy) of the aligned 2x2 block q[0..3] = (0,0),(1,0),(0,1),(1,1).
-__device__ __forceinline__ Rgba wavelet_px(const Rgba q[4], int ox, int oy, float th) {
+// Output for pixel (ox, oy) of the aligned 2x2 block q[0..3] = (0,0),(1,0),(0,1),(1,1);
+// `p` is that pixel (q[oy*2+ox], passed separately so q is never indexed at run time).
+__device__ __forceinline__ Rgba wavelet_px(const Rgba q[4], const Rgba& p, int ox, int oy, float th) {
     const HaarBand bco = haar_shrink(wv_co(q[0]), wv_co(q[1]), wv_co(q[2]), wv_co(q[3]), th);
     const HaarBand bcg = haar_shrink(wv_cg(q[0]), wv_cg(q[1]), wv_cg(q[2]), wv_cg(q[3]), th);
-    const Rgba p = q[oy * 2 + ox];
     const float luma = (p.r + (2.0F * p.g) + p.b) * 0.25F;
     const float co = haar_pick(bco, ox, oy), cg = haar_pick(bcg, ox, oy);
     const float t = luma - (0.5F * cg);
