@@ -114,6 +114,32 @@ def cpu_chain_ms(cfg_small, scale, repeats=1):
     return 1000.0 * min(times) * scale
 
 
+# ------------------------------------------------------------ rank helpers
+def rank_env(default_world=1):
+    return (int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", str(default_world))),
+            int(os.environ.get("LOCAL_RANK", "0")))
+
+
+def frame_seed(rank):
+    """Replica r processes its own frames (seeded per rank): no data is shared."""
+    return 0x5EED0002 + 1000 * rank
+
+
+def max_over_ranks(x, dist=None, device=None):
+    """Max of a per-rank scalar over the process group (CPU tensor for gloo)."""
+    if dist is None:
+        return float(x)
+    import torch
+    t = torch.tensor([float(x)], dtype=torch.float64, device=device or "cpu")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_ms_per_frame(max_ms, steps, world):
+    """Every rank ran `steps` frames; the job's time is the slowest rank's."""
+    return max_ms / (steps * world)
+
+
 def reference_arm(args):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
@@ -144,9 +170,7 @@ def reference_arm(args):
 
 def b200_arm(args):
     import numpy as np
-    rank = int(os.environ.get("RANK", "0"))
-    world = int(os.environ.get("WORLD_SIZE", str(args.gpus)))
-    local = int(os.environ.get("LOCAL_RANK", "0"))
+    rank, world, local = rank_env(args.gpus)
     dist = None
     if world > 1:
         import torch
@@ -164,15 +188,7 @@ def b200_arm(args):
             dist.barrier(device_ids=[local])
             torch.cuda.synchronize()
 
-    def max_over_ranks(x):
-        if dist is None:
-            return x
-        import torch
-        t = torch.tensor([x], dtype=torch.float64, device=f"cuda:{local}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
-
-    cfg = ChainConfig.full_12mp(seed=0x5EED0002 + 1000 * rank)
+    cfg = ChainConfig.full_12mp(seed=frame_seed(rank))
     w, h = cfg.width, cfg.height
     base = cfg.make_raw()
     ring = [np.ascontiguousarray(np.roll(base, (2 * k, 4 * k), axis=(0, 1))) for k in range(8)]
@@ -237,10 +253,10 @@ def b200_arm(args):
         barrier()
     clk = clocks.summary()
 
-    total_ms = max_over_ranks(float(ms.value))
-    e2e_ms = max_over_ranks(e2e_s * 1000.0)
+    total_ms = max_over_ranks(float(ms.value), dist, f"cuda:{local}")
+    e2e_ms = max_over_ranks(e2e_s * 1000.0, dist, f"cuda:{local}")
     per_kernel = {k: ms_k[i] / max(1, nfr.value) for i, k in enumerate(KERNELS)}
-    value = total_ms / (args.steps * world)
+    value = whole_job_ms_per_frame(total_ms, args.steps, world)
     dominant = max(per_kernel, key=per_kernel.get)
     peak, peak_kind = measured_peak_gbs()
     alg_bytes = BYTES_PER_PX[dominant] * w * h
@@ -262,7 +278,7 @@ def b200_arm(args):
                      "algorithmic_bytes": alg_bytes, "traffic": traffic},
         "chain_roofline": {"achieved": round(sum(BYTES_PER_PX.values()) * w * h / (total_ms / args.steps * 1e-3) / 1e9,
                                              1), "unit": "GB/s", "bytes_per_px": sum(BYTES_PER_PX.values())},
-        "e2e": {"value": round(e2e_ms / (e2e_steps * world), 4), "unit": "ms/frame", "h2d_bytes_per_step": raw_bytes,
+        "e2e": {"value": round(whole_job_ms_per_frame(e2e_ms, e2e_steps, world), 4), "unit": "ms/frame", "h2d_bytes_per_step": raw_bytes,
                 "d2h_bytes_per_step": out_bytes},
         "clocks": clk,
         "gpu_launches": 3 * args.steps,
