@@ -143,6 +143,7 @@ EXPORTS = [
     "cpipe_cuda_denoise_bm3d_step1", "cpipe_cuda_denoise_bm3d_step2", "cpipe_cuda_denoise_guided_filter",
     "cpipe_cuda_denoise_wavelet_bayes_shrink", "cpipe_cuda_lens_dng_opcode_list_3", "cpipe_cuda_color_3d_lut",
     "cpipe_cuda_tone_filmic_rgb", "cpipe_cuda_copy", "cpipe_cuda_filters", "cpipe_cuda_find_filter",
+    "cpipe_cuda_color_3d_lut_noalloc",
     "cpipe_b200_node_descs", "cpipe_b200_find_node",
     "cpipe_b200_wb_prepare", "cpipe_b200_colormatrix_compose", "cpipe_b200_pack_gain_maps",
     "cpipe_b200_pack_opcode_list_3", "cpipe_b200_load_lut",

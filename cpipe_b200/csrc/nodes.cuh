@@ -183,6 +183,47 @@ __device__ __forceinline__ Rgba lut_px(Rgba v, const float4* __restrict__ lut, i
     return Rgba{clampf(o.x, 0.0F, 1.0F), clampf(o.y, 0.0F, 1.0F), clampf(o.z, 0.0F, 1.0F), v.a};
 }
 
+// The same interpolation as lut_px with the cells read through `fetch(i)`
+// (cell i as float4 r, g, b, -), for LUTs stored in another layout.
+template <class Fetch>
+__device__ __forceinline__ Rgba lut_px_cells(Rgba v, const Fetch& fetch, int S, int interp) {
+    const float mi = (float)(S - 1);
+    const float rs = clampf(v.r, 0.0F, 1.0F) * mi;
+    const float gs = clampf(v.g, 0.0F, 1.0F) * mi;
+    const float bs = clampf(v.b, 0.0F, 1.0F) * mi;
+    const int r0 = clampi((int)floorf(rs), 0, S - 2);
+    const int g0 = clampi((int)floorf(gs), 0, S - 2);
+    const int b0 = clampi((int)floorf(bs), 0, S - 2);
+    const float dr = rs - (float)r0, dg = gs - (float)g0, db = bs - (float)b0;
+    const int base = (r0 * S + g0) * S + b0;
+    const int sr = S * S, sg = S;
+    const float4 c000 = fetch(base);
+    const float4 c111 = fetch(base + sr + sg + 1);
+    float4 o;
+    if (interp == 1) {
+        const float4 c100 = fetch(base + sr), c010 = fetch(base + sg);
+        const float4 c001 = fetch(base + 1), c110 = fetch(base + sr + sg);
+        const float4 c101 = fetch(base + sr + 1), c011 = fetch(base + sg + 1);
+        const float4 c00 = lerp4(c000, c100, dr), c10 = lerp4(c010, c110, dr);
+        const float4 c01 = lerp4(c001, c101, dr), c11 = lerp4(c011, c111, dr);
+        const float4 c0 = lerp4(c00, c10, dg), c1 = lerp4(c01, c11, dg);
+        o = lerp4(c0, c1, db);
+    } else {
+        // Tetrahedral: the first matching branch of the generator's select chain;
+        // each branch reads only the two intermediate corners it walks through.
+        int s1, s2;
+        float w1, w2, w3;
+        if (dr >= dg && dg >= db) { s1 = sr; s2 = sr + sg; w1 = dr; w2 = dg; w3 = db; }
+        else if (dr >= db && db >= dg) { s1 = sr; s2 = sr + 1; w1 = dr; w2 = db; w3 = dg; }
+        else if (db >= dr && dr >= dg) { s1 = 1; s2 = sr + 1; w1 = db; w2 = dr; w3 = dg; }
+        else if (dg >= dr && dr >= db) { s1 = sg; s2 = sr + sg; w1 = dg; w2 = dr; w3 = db; }
+        else if (dg >= db && db >= dr) { s1 = sg; s2 = sg + 1; w1 = dg; w2 = db; w3 = dr; }
+        else { s1 = 1; s2 = sg + 1; w1 = db; w2 = dg; w3 = dr; }
+        const float4 ca = fetch(base + s1), cb = fetch(base + s2);
+        o = add_delta4(add_delta4(add_delta4(c000, c000, ca, w1), ca, cb, w2), cb, c111, w3);
+    }
+    return Rgba{clampf(o.x, 0.0F, 1.0F), clampf(o.y, 0.0F, 1.0F), clampf(o.z, 0.0F, 1.0F), v.a};
+}
 // bm3d_step1_generator.cpp:42-56 (parity form): blend toward the aligned 2x2 mean.
 __device__ __forceinline__ float bm3d_blend(float v, float p00, float p10, float p01, float p11, float s) {
     const float basic = (p00 + p10 + p01 + p11) * 0.25F;

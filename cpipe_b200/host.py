@@ -131,6 +131,26 @@ def call_filter(aot_id, inputs, outputs, blob=None):
     return fn(C.pointer(ins[0]), C.pointer(outs[0]))
 
 
+def call_entry(symbol, inputs, outputs, blob=None):
+    """Call an exported HalideParamFilterEntry-shaped function of the library by
+    its symbol name (for entry points outside the aot_id table), with the same
+    buffer and blob conventions as call_filter."""
+    fn = getattr(A.lib(), symbol)
+    keep = []
+    ins = [_halide(a, keep) for a in inputs]
+    outs = [_halide(a, keep) for a in outputs]
+    if blob is None:
+        bptr, bsize = None, 0
+    else:
+        raw = bytes(blob)
+        keep.append(C.create_string_buffer(raw, len(raw)))
+        bptr, bsize = C.cast(keep[-1], C.c_void_p), len(raw)
+    pin = (C.POINTER(A.HalideBuffer) * max(1, len(ins)))(*[C.pointer(b) for b in ins])
+    pout = (C.POINTER(A.HalideBuffer) * max(1, len(outs)))(*[C.pointer(b) for b in outs])
+    entry = A.PARAM_FILTER(C.cast(fn, C.c_void_p).value)
+    return entry(pin, len(ins), pout, len(outs), bptr, bsize)
+
+
 def last_error():
     return A.lib().cpipe_cuda_last_error().decode()
 

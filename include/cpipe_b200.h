@@ -83,6 +83,19 @@ CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_tone_filmic_rgb);            /* filmic_rgb_di
  * memcpy of e.g. shading_gainmap.cpp:50-75.  No reference filter counterpart. */
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_copy);
 
+/* Allocation-free 3D LUT filter: the same arguments and result as
+ * cpipe_cuda_color_3d_lut, for callers that cannot allocate device memory while
+ * they run (a frame loop with a fixed latency budget, where an allocator call
+ * may block on the device, or a host that fixes each plugin's device memory at
+ * start-up).  It has no counterpart in the reference: the LUT goes into a fixed
+ * 3.3 MB device array every GPU holds while the library is loaded, so the LUT
+ * edge length is at most 65 (larger: CPIPE_BAD_INDEX with a message), input and
+ * output must be device buffers (host buffers: CPIPE_UNSUPPORTED), and calls
+ * that overlap on the GPU race on that one array (calls in order on one stream
+ * are safe).  The first call on a device looks up the array's device address;
+ * make it before any stream capture on that device. */
+CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_color_3d_lut_noalloc);
+
 /* Registration table: entry is a HalideParamFilterEntry when takes_params != 0,
  * else a HalideFilterEntry. */
 typedef struct {
