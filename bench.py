@@ -29,7 +29,7 @@ sys.path.insert(0, ROOT)
 
 METRIC = "12MP ms/frame, classic raw->linear chain (parity form)"
 BYTES_PER_PX = {"raw_to_rgba": 10, "warp_wb_cm": 16, "denoise_tone": 16}  # algorithmic HBM bytes
-KERNELS = ["raw_to_rgba", "warp_wb_cm", "denoise_tone"]
+KERNELS = ["raw_to_rgba", "warp_wb_cm", "denoise", "denoise_tone"]
 
 
 def measured_peak_gbs():
@@ -221,7 +221,7 @@ def b200_arm(args):
         for i in range(max(args.warmup, 3)):
             chain.run(d_raw[i % 8], d_out[i % 2], stream)
         L.cpipe_cuda_stream_synchronize(stream)
-        ms_k = (C.c_double * 3)()
+        ms_k = (C.c_double * 4)()
         nfr = C.c_int32()
         L.cpipe_cuda_chain_profile(chain._h, ms_k, C.byref(nfr))  # discard the extra warm-up frames
         barrier()
@@ -255,7 +255,7 @@ def b200_arm(args):
 
     total_ms = max_over_ranks(float(ms.value), dist, f"cuda:{local}")
     e2e_ms = max_over_ranks(e2e_s * 1000.0, dist, f"cuda:{local}")
-    per_kernel = {k: ms_k[i] / max(1, nfr.value) for i, k in enumerate(KERNELS)}
+    per_kernel = {k: ms_k[i] / max(1, nfr.value) for i, k in enumerate(KERNELS) if k != "denoise" or ms_k[i] > 0}
     value = whole_job_ms_per_frame(total_ms, args.steps, world)
     dominant = max(per_kernel, key=per_kernel.get)
     peak, peak_kind = measured_peak_gbs()

@@ -93,6 +93,13 @@ class Bm3dParams(C.Structure):
     _fields_ = [("sigma", C.c_float)]
 
 
+class Bm3dSpecParams(C.Structure):
+    """cpipe_Bm3dSpecParams (two-stage colour BM3D, aot_id denoise_bm3d_spec)."""
+    _fields_ = [("sigma", C.c_float), ("lambda3d", C.c_float), ("tau_match1", C.c_float),
+                ("tau_match2", C.c_float), ("n2", C.c_int32), ("ns", C.c_int32), ("nstep", C.c_int32),
+                ("kaiser_beta", C.c_float), ("stages", C.c_int32), ("reserved", C.c_int32)]
+
+
 class GuidedFilterParams(C.Structure):
     _fields_ = [("radius", C.c_int32), ("eps", C.c_float)]
 
@@ -112,7 +119,8 @@ class ChainConfig(C.Structure):
                 ("as_shot_neutral", C.c_float * 3), ("colormatrix", C.c_float * 9), ("bm3d_sigma", C.c_float),
                 ("guided_radius", C.c_int32), ("guided_eps", C.c_float), ("wavelet_strength", C.c_float),
                 ("filmic", FilmicRgbParams), ("lut_blob", C.c_void_p), ("lut_blob_size", C.c_size_t),
-                ("plain_f32", C.c_int32), ("use_graph", C.c_int32)]
+                ("plain_f32", C.c_int32), ("use_graph", C.c_int32), ("denoise_mode", C.c_int32),
+                ("bm3d_spec", Bm3dSpecParams), ("surrogate_blob", C.c_void_p), ("surrogate_blob_size", C.c_size_t)]
 
 
 MAIN_ENTRY = C.CFUNCTYPE(C.c_int, C.c_char_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p)
@@ -140,7 +148,8 @@ EXPORTS = [
     "cpipe_cuda_demosaic_quad_bayer_remosaic", "cpipe_cuda_linearize_dng_lut", "cpipe_cuda_blacklevel_dng_levels",
     "cpipe_cuda_lens_shading_gainmap", "cpipe_cuda_demosaic_bilinear", "cpipe_cuda_demosaic_rcd",
     "cpipe_cuda_demosaic_amaze", "cpipe_cuda_wb_dual_illuminant", "cpipe_cuda_colormatrix_dng_to_working",
-    "cpipe_cuda_denoise_bm3d_step1", "cpipe_cuda_denoise_bm3d_step2", "cpipe_cuda_denoise_guided_filter",
+    "cpipe_cuda_denoise_bm3d_step1", "cpipe_cuda_denoise_bm3d_step2", "cpipe_cuda_denoise_bm3d_spec",
+    "cpipe_cuda_denoise_guided_filter",
     "cpipe_cuda_denoise_wavelet_bayes_shrink", "cpipe_cuda_lens_dng_opcode_list_3", "cpipe_cuda_color_3d_lut",
     "cpipe_cuda_tone_filmic_rgb", "cpipe_cuda_copy", "cpipe_cuda_filters", "cpipe_cuda_find_filter",
     "cpipe_cuda_color_3d_lut_noalloc",

@@ -52,6 +52,14 @@ def bm3d(sigma):
     return raw(A.Bm3dParams(sigma))
 
 
+def bm3d_spec(sigma, lambda3d=2.7, tau_match1=2500.0, tau_match2=400.0, n2=16, ns=39, nstep=3,
+              kaiser_beta=2.0, stages=2):
+    """Two-stage BM3D parameters; defaults are the published values (8x8 blocks,
+    16-block groups, 39x39 search, step 3, hard threshold then Wiener)."""
+    return raw(A.Bm3dSpecParams(float(sigma), float(lambda3d), float(tau_match1), float(tau_match2), int(n2),
+                                int(ns), int(nstep), float(kaiser_beta), int(stages), 0))
+
+
 def guided(radius, eps):
     return raw(A.GuidedFilterParams(int(radius), float(eps)))
 

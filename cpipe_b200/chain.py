@@ -81,6 +81,9 @@ class ChainConfig:
     lut: str = "identity_gamma"    # identity_gamma | smooth | none
     plain_f32: bool = False
     use_graph: bool = True
+    denoise: str = "box2x2"        # box2x2 (the reference's bm3d node) | bm3d (two-stage) | surrogate
+    bm3d_stages: int = 2
+    surrogate_blob: bytes = None   # trained network (cpipe_b200.surrogate) for denoise="surrogate"
 
     # ------------------------------------------------------------ workloads
     @classmethod
@@ -216,6 +219,11 @@ class ChainConfig:
             cfg.lut_blob, cfg.lut_blob_size = ptr(b["lut"])
         cfg.plain_f32 = int(self.plain_f32)
         cfg.use_graph = int(self.use_graph)
+        cfg.denoise_mode = {"box2x2": 0, "bm3d": 1, "surrogate": 2}[self.denoise]
+        C.memmove(C.addressof(cfg.bm3d_spec), B.bm3d_spec(self.bm3d_sigma, stages=self.bm3d_stages),
+                  C.sizeof(A.Bm3dSpecParams))
+        if self.surrogate_blob:
+            cfg.surrogate_blob, cfg.surrogate_blob_size = ptr(bytes(self.surrogate_blob))
         return cfg, keep
 
 
@@ -270,10 +278,12 @@ def _main():
     ap.add_argument("--width", type=int, default=4032)
     ap.add_argument("--height", type=int, default=3024)
     ap.add_argument("--demosaic", default="rcd")
+    ap.add_argument("--denoise", default="box2x2", choices=["box2x2", "bm3d", "surrogate"])
     args = ap.parse_args()
     L = A.lib()
     assert L.cpipe_cuda_device_count() > 0, "no CUDA device"
-    cfg = ChainConfig.full_12mp(width=args.width, height=args.height, demosaic=args.demosaic, use_graph=False)
+    cfg = ChainConfig.full_12mp(width=args.width, height=args.height, demosaic=args.demosaic, use_graph=False,
+                                denoise=args.denoise)
     raw = cfg.make_raw()
     chain = Chain(cfg)
     d_raw, d_out = C.c_void_p(), C.c_void_p()

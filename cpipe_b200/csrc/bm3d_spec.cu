@@ -1,0 +1,596 @@
+// Two-stage colour BM3D on sm_100a (aot_id denoise_bm3d_spec).
+//
+// The algorithm is the published one (Dabov et al., IEEE TIP 2007; colour
+// grouping on luminance; parameters of Lebrun, IPOL 2012).  The reference's
+// denoise.bm3d node computes a 2x2 box blend instead
+// (src/cpipe/nodes/denoise/bm3d_step1_generator.cpp:33-61); that form lives in
+// kernels_nodes.cu and the fused chain.  The exact definition shared with the
+// FP64 CPU oracle:
+//   colour    orthonormal opponent Y=(R+G+B)/sqrt3, U=(R-B)/sqrt2, V=(R-2G+B)/sqrt6
+//   refs      8x8 blocks at min(i*nstep, W-8), same in y
+//   matching  integer sum of squared differences of q = rint(clamp(L,0,1)*255)
+//             (L = ((R+G)+B)*(1/3) for step 1, Y_basic*(1/sqrt3) for step 2)
+//             over all positions within +-(ns-1)/2, d <= floor(64*tau);
+//             group = reference + best (d, raster) candidates, at most n2,
+//             truncated to a power of two
+//   transform orthonormal 8x8 DCT-II, then orthonormal Haar along the group
+//   step 1    hard threshold |c| > lambda3d*sigma, weight 1/(sigma^2*kept)
+//   step 2    Wiener W = B^2/(B^2+sigma^2) from the basic estimate's group,
+//             weight 1/(sigma^2*sum W^2)
+//   aggregate weight x Kaiser(beta) 8x8 window; estimate = num / den
+//
+// Kernels (all FP32 on the CUDA cores; the transforms use explicit fused
+// multiply-adds, the library being built without contraction):
+//   bm3d_prep_kernel    RGBA -> Y,U,V planes + 8-bit matching luminance
+//   bm3d_match_kernel   one thread per reference block; the search region of a
+//                       16x16 tile of references is staged in shared memory as
+//                       four byte-shifted word copies so every 4-pixel chunk is
+//                       one aligned 32-bit load; distances with byte-SIMD
+//                       |a-b| and dp4a (exact integers); a sorted register list
+//                       keeps the 15 best (d << 11 | window index) keys
+//   bm3d_filter_kernel  one warp per group and channel: lane = (block, row
+//                       half); row DCT in registers, column DCT through a warp
+//                       shared buffer, Haar along the group with warp shuffles;
+//                       aggregation into a shared-memory footprint of the 8x8
+//                       reference tile, then added to the frame accumulators.
+//                       Tiles are launched in P x P phases so that tiles of one
+//                       launch have disjoint footprints: the flush is a plain
+//                       read-modify-write, no global atomics.
+//   bm3d_basic_kernel   step-1 num/den -> basic estimate + step-2 luminance
+//   bm3d_final_kernel   num/den -> RGB, alpha copied
+#include "bm3d_spec.h"
+
+#include <math.h>
+
+#include "../../include/cpipe_node_abi.h"
+#include "kernels.h"
+
+namespace cpb {
+namespace {
+
+constexpr float kInvS3 = 0.57735026918962576451F;
+constexpr float kInvS2 = 0.70710678118654752440F;
+constexpr float kInvS6 = 0.40824829046386301637F;
+
+// cos(m * pi / 16) for any integer m.
+__host__ __device__ constexpr float cos16(int m) {
+    m = ((m % 32) + 32) % 32;
+    if (m > 16) m = 32 - m;
+    float sgn = 1.0F;
+    if (m > 8) {
+        m = 16 - m;
+        sgn = -1.0F;
+    }
+    return sgn * (m == 0   ? 1.0F
+                  : m == 1 ? 0.98078528040323044913F
+                  : m == 2 ? 0.92387953251128675613F
+                  : m == 3 ? 0.83146961230254523708F
+                  : m == 4 ? 0.70710678118654752440F
+                  : m == 5 ? 0.55557023301960222474F
+                  : m == 6 ? 0.38268343236508977173F
+                  : m == 7 ? 0.19509032201612826785F
+                           : 0.0F);
+}
+// Orthonormal DCT-II basis: dctc(k, n) = a(k) cos((2n+1) k pi / 16).
+__host__ __device__ constexpr float dctc(int k, int n) {
+    return (k == 0 ? 0.35355339059327376220F : 0.5F) * cos16((2 * n + 1) * k);
+}
+
+__device__ __forceinline__ int refpos(int i, int n, int nstep) { return min(i * nstep, n - 8); }
+
+__device__ __forceinline__ uint8_t quantise(float l) {
+    l = l > 0.0F ? l : 0.0F;
+    l = fminf(l, 1.0F);
+    return (uint8_t)__float2int_rn(l * 255.0F);
+}
+
+// ------------------------------------------------------------------- prep
+template <class T>
+__global__ void bm3d_prep_kernel(Img in, float* __restrict__ yuv, uint8_t* __restrict__ q, long long npx) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= in.w) return;
+    const Rgba p = load_rgba(px<const T>(in, x, y));
+    const float s = (p.r + p.g) + p.b;
+    const long long o = (long long)y * in.w + x;
+    yuv[o] = s * kInvS3;
+    yuv[npx + o] = (p.r - p.b) * kInvS2;
+    yuv[2 * npx + o] = ((p.r + p.b) - 2.0F * p.g) * kInvS6;
+    q[o] = quantise(s * (1.0F / 3.0F));
+}
+
+// ------------------------------------------------------------------ match
+struct MatchArgs {
+    int w, h, nrx, nry, nstep, R, ns, n2, wpr, rows;
+    uint32_t dthr;
+    const uint8_t* q;
+    uint32_t* list;
+    uint8_t* cnt;
+};
+
+constexpr int kMatchTile = 16;  // reference blocks per CTA edge (one thread each)
+
+__global__ void __launch_bounds__(256) bm3d_match_kernel(MatchArgs a) {
+    extern __shared__ uint32_t s_w[];
+    const int i0 = blockIdx.x * kMatchTile, j0 = blockIdx.y * kMatchTile;
+    const int iL = min(i0 + kMatchTile - 1, a.nrx - 1), jL = min(j0 + kMatchTile - 1, a.nry - 1);
+    const int rx0 = max(0, refpos(i0, a.w, a.nstep) - a.R);
+    const int rx1 = min(a.w, refpos(iL, a.w, a.nstep) + a.R + 8);
+    const int ry0 = max(0, refpos(j0, a.h, a.nstep) - a.R);
+    const int ry1 = min(a.h, refpos(jL, a.h, a.nstep) + a.R + 8);
+    const int RW = rx1 - rx0, RH = ry1 - ry0;
+    const int plane = a.rows * a.wpr;  // words per shifted copy
+    // Copy s, row r, word k holds region bytes 4k+s .. 4k+s+3 (little endian).
+    for (int idx = threadIdx.x; idx < 4 * RH * a.wpr; idx += blockDim.x) {
+        const int s = idx / (RH * a.wpr), rem = idx - s * RH * a.wpr;
+        const int r = rem / a.wpr, k = rem - r * a.wpr;
+        const uint8_t* row = a.q + (size_t)(ry0 + r) * a.w + rx0;
+        const int c0 = 4 * k + s;
+        uint32_t word = 0;
+#pragma unroll
+        for (int b = 0; b < 4; ++b) {
+            const int cc = c0 + b;
+            word |= (cc < RW ? (uint32_t)row[cc] : 0U) << (8 * b);
+        }
+        s_w[s * plane + r * a.wpr + k] = word;
+    }
+    __syncthreads();
+    const int i = i0 + (int)(threadIdx.x % kMatchTile), j = j0 + (int)(threadIdx.x / kMatchTile);
+    if (i >= a.nrx || j >= a.nry) return;
+    const int x = refpos(i, a.w, a.nstep), y = refpos(j, a.h, a.nstep);
+    uint32_t rw[16];
+    {
+        const int c = x - rx0;
+        const uint32_t* p = s_w + (c & 3) * plane + (y - ry0) * a.wpr + (c >> 2);
+#pragma unroll
+        for (int r = 0; r < 8; ++r) {
+            rw[2 * r] = p[r * a.wpr];
+            rw[2 * r + 1] = p[r * a.wpr + 1];
+        }
+    }
+    uint32_t keys[15];
+#pragma unroll
+    for (int m = 0; m < 15; ++m) keys[m] = 0xFFFFFFFFU;
+    const int ylo = max(0, y - a.R), yhi = min(a.h - 8, y + a.R);
+    const int xlo = max(0, x - a.R), xhi = min(a.w - 8, x + a.R);
+    if (a.n2 > 1) {
+        for (int yy = ylo; yy <= yhi; ++yy) {
+            const uint32_t wrow = (uint32_t)((yy - y + a.R) * a.ns + a.R - x);
+            const uint32_t* rowp = s_w + (yy - ry0) * a.wpr;
+            for (int xx = xlo; xx <= xhi; ++xx) {
+                const int c = xx - rx0;
+                const uint32_t* p = rowp + (c & 3) * plane + (c >> 2);
+                uint32_t d = 0;
+#pragma unroll
+                for (int r = 0; r < 8; ++r) {
+                    const uint32_t a0 = __vabsdiffu4(rw[2 * r], p[r * a.wpr]);
+                    d = __dp4a(a0, a0, d);
+                    const uint32_t a1 = __vabsdiffu4(rw[2 * r + 1], p[r * a.wpr + 1]);
+                    d = __dp4a(a1, a1, d);
+                }
+                if (d <= a.dthr && (xx != x || yy != y)) {
+                    uint32_t key = (d << 11) | (wrow + (uint32_t)xx);
+                    if (key < keys[14]) {
+#pragma unroll
+                        for (int m = 0; m < 15; ++m) {
+                            const uint32_t lo = min(keys[m], key);
+                            key = max(keys[m], key);
+                            keys[m] = lo;
+                        }
+                    }
+                }
+            }
+        }
+    }
+    const long long ref = (long long)j * a.nrx + i;
+    uint32_t* out = a.list + ref * 16;
+    out[0] = ((uint32_t)y << 16) | (uint32_t)x;
+    int n = 1;
+#pragma unroll
+    for (int m = 0; m < 15; ++m) {
+        if (m < a.n2 - 1 && keys[m] != 0xFFFFFFFFU) {
+            const int widx = (int)(keys[m] & 2047U);
+            const int dy = widx / a.ns - a.R, dx = widx % a.ns - a.R;
+            out[1 + m] = ((uint32_t)(y + dy) << 16) | (uint32_t)(x + dx);
+            ++n;
+        }
+    }
+    a.cnt[ref] = (uint8_t)n;
+}
+
+// ----------------------------------------------------------------- filter
+struct FilterArgs {
+    int w, h, nrx, nry, nstep, R, ntx, nty, phases, fw;
+    float sigma2, thr;
+    long long npx;
+    const uint32_t* list;
+    const uint8_t* cnt;
+    const float* noisy;
+    const float* basic;
+    float* acc;  // num of channel c at c*npx, den at (3+c)*npx
+    float kaiser[64];
+};
+
+constexpr int kBufStride = 65;                 // floats per block in a warp buffer
+constexpr int kWarpBuf = 16 * kBufStride;      // one group of 16 blocks
+constexpr int kFilterWarps = 8;
+constexpr int kRefTile = 8;                    // reference blocks per tile edge
+
+__device__ __forceinline__ void haar_forward(float (&Z)[32], int N, int b, bool act) {
+    for (int s = 1; s < N; s <<= 1) {
+        const bool part = act && (b & (s - 1)) == 0;
+        const bool odd = (b & s) != 0;
+#pragma unroll
+        for (int e = 0; e < 32; ++e) {
+            const float p = __shfl_xor_sync(0xFFFFFFFFU, Z[e], 2 * s);
+            if (part) Z[e] = odd ? (p - Z[e]) * kInvS2 : (Z[e] + p) * kInvS2;
+        }
+    }
+}
+__device__ __forceinline__ void haar_inverse(float (&Z)[32], int N, int b, bool act) {
+    for (int s = N >> 1; s >= 1; s >>= 1) {
+        const bool part = act && (b & (s - 1)) == 0;
+        const bool odd = (b & s) != 0;
+#pragma unroll
+        for (int e = 0; e < 32; ++e) {
+            const float p = __shfl_xor_sync(0xFFFFFFFFU, Z[e], 2 * s);
+            if (part) Z[e] = odd ? (p - Z[e]) * kInvS2 : (Z[e] + p) * kInvS2;
+        }
+    }
+}
+
+// 3D transform of the group held by one warp.  Lane (b, hh) loads rows
+// 4hh..4hh+3 of block b; on return it holds frequency rows 0..7 of frequency
+// columns 4hh..4hh+3 (Z[kr*4 + jj]) after the Haar transform along the group.
+__device__ __forceinline__ void forward3d(const float* img, int fw, int bx, int by, int hh, int b, bool act, int N,
+                                          float* buf, float (&Z)[32]) {
+    if (act) {
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const float* row = img + (by + 4 * hh + r) * fw + bx;
+            float v[8];
+#pragma unroll
+            for (int n = 0; n < 8; ++n) v[n] = row[n];
+#pragma unroll
+            for (int k = 0; k < 8; ++k) {
+                float s = dctc(k, 0) * v[0];
+#pragma unroll
+                for (int n = 1; n < 8; ++n) s = __fmaf_rn(dctc(k, n), v[n], s);
+                buf[b * kBufStride + (4 * hh + r) * 8 + k] = s;
+            }
+        }
+    }
+    __syncwarp();
+    float z[8][4];
+#pragma unroll
+    for (int r = 0; r < 8; ++r)
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) z[r][jj] = act ? buf[b * kBufStride + r * 8 + 4 * hh + jj] : 0.0F;
+    __syncwarp();
+#pragma unroll
+    for (int kr = 0; kr < 8; ++kr)
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+            float s = dctc(kr, 0) * z[0][jj];
+#pragma unroll
+            for (int r = 1; r < 8; ++r) s = __fmaf_rn(dctc(kr, r), z[r][jj], s);
+            Z[kr * 4 + jj] = s;
+        }
+    haar_forward(Z, N, b, act);
+}
+
+template <int STAGE>
+__global__ void __launch_bounds__(256, 2) bm3d_filter_kernel(FilterArgs a, int phx, int phy) {
+    extern __shared__ float sm[];
+    const int c = blockIdx.z;
+    const int tx = blockIdx.x * a.phases + phx, ty = blockIdx.y * a.phases + phy;
+    if (tx >= a.ntx || ty >= a.nty) return;
+    const int i0 = tx * kRefTile, j0 = ty * kRefTile;
+    const int i1 = min(i0 + kRefTile, a.nrx), j1 = min(j0 + kRefTile, a.nry);
+    const int fx0 = max(0, refpos(i0, a.w, a.nstep) - a.R);
+    const int fx1 = min(a.w, refpos(i1 - 1, a.w, a.nstep) + a.R + 8);
+    const int fy0 = max(0, refpos(j0, a.h, a.nstep) - a.R);
+    const int fy1 = min(a.h, refpos(j1 - 1, a.h, a.nstep) + a.R + 8);
+    const int fw = fx1 - fx0, fn = fw * (fy1 - fy0);
+    const int FN = a.fw * a.fw;
+    float* s_num = sm;
+    float* s_den = sm + FN;
+    float* s_img = sm + 2 * FN;
+    float* s_bas = sm + 3 * FN;
+    float* s_buf = sm + (STAGE == 2 ? 4 : 3) * FN;
+    float* s_k = s_buf + kFilterWarps * kWarpBuf;
+    const float* gz = a.noisy + (long long)c * a.npx;
+    const float* gb = STAGE == 2 ? a.basic + (long long)c * a.npx : nullptr;
+    for (int idx = threadIdx.x; idx < fn; idx += blockDim.x) {
+        const int yy = idx / fw, xx = idx - yy * fw;
+        const long long o = (long long)(fy0 + yy) * a.w + fx0 + xx;
+        s_num[idx] = 0.0F;
+        s_den[idx] = 0.0F;
+        s_img[idx] = gz[o];
+        if (STAGE == 2) s_bas[idx] = gb[o];
+    }
+    if (threadIdx.x < 64) s_k[threadIdx.x] = a.kaiser[threadIdx.x];
+    __syncthreads();
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, b = lane >> 1, hh = lane & 1;
+    float* buf = s_buf + warp * kWarpBuf;
+    const int nti = i1 - i0, nref = nti * (j1 - j0);
+    for (int k = warp; k < nref; k += kFilterWarps) {
+        const long long ref = (long long)(j0 + k / nti) * a.nrx + i0 + k % nti;
+        const int cnt = a.cnt[ref];
+        const int N = cnt >= 16 ? 16 : cnt >= 8 ? 8 : cnt >= 4 ? 4 : cnt >= 2 ? 2 : 1;
+        const bool act = b < N;
+        int bx = 0, by = 0;
+        if (act) {
+            const uint32_t p = a.list[ref * 16 + b];
+            bx = (int)(p & 0xFFFFU) - fx0;
+            by = (int)(p >> 16) - fy0;
+        }
+        float Z[32];
+        forward3d(s_img, fw, bx, by, hh, b, act, N, buf, Z);
+        float wgt;
+        if (STAGE == 1) {
+            unsigned kept = 0;
+#pragma unroll
+            for (int e = 0; e < 32; ++e) {
+                const bool keep = fabsf(Z[e]) > a.thr;
+                Z[e] = keep ? Z[e] : 0.0F;
+                kept += keep ? 1U : 0U;
+            }
+            kept = __reduce_add_sync(0xFFFFFFFFU, kept);
+            wgt = kept > 0U ? 1.0F / (a.sigma2 * (float)kept) : 1.0F;
+        } else {
+            float B[32];
+            forward3d(s_bas, fw, bx, by, hh, b, act, N, buf, B);
+            float sw2 = 0.0F;
+#pragma unroll
+            for (int e = 0; e < 32; ++e) {
+                const float b2 = B[e] * B[e];
+                const float W = b2 / (b2 + a.sigma2);
+                Z[e] = Z[e] * W;
+                sw2 = __fmaf_rn(W, W, sw2);
+            }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) sw2 += __shfl_xor_sync(0xFFFFFFFFU, sw2, off);
+            wgt = sw2 > 0.0F ? 1.0F / (a.sigma2 * sw2) : 1.0F;
+        }
+        haar_inverse(Z, N, b, act);
+        if (act) {
+#pragma unroll
+            for (int r = 0; r < 8; ++r)
+#pragma unroll
+                for (int jj = 0; jj < 4; ++jj) {
+                    float s = dctc(0, r) * Z[jj];
+#pragma unroll
+                    for (int kr = 1; kr < 8; ++kr) s = __fmaf_rn(dctc(kr, r), Z[kr * 4 + jj], s);
+                    buf[b * kBufStride + r * 8 + 4 * hh + jj] = s;
+                }
+        }
+        __syncwarp();
+        if (act) {
+#pragma unroll
+            for (int r = 0; r < 4; ++r) {
+                const int row = 4 * hh + r;
+                float v[8];
+#pragma unroll
+                for (int kk = 0; kk < 8; ++kk) v[kk] = buf[b * kBufStride + row * 8 + kk];
+                float* dn = s_num + (by + row) * fw + bx;
+                float* dd = s_den + (by + row) * fw + bx;
+#pragma unroll
+                for (int n = 0; n < 8; ++n) {
+                    float s = dctc(0, n) * v[0];
+#pragma unroll
+                    for (int kk = 1; kk < 8; ++kk) s = __fmaf_rn(dctc(kk, n), v[kk], s);
+                    const float kw = wgt * s_k[row * 8 + n];
+                    atomicAdd(dn + n, kw * s);
+                    atomicAdd(dd + n, kw);
+                }
+            }
+        }
+        __syncwarp();
+    }
+    __syncthreads();
+    float* gn = a.acc + (long long)c * a.npx;
+    float* gd = a.acc + (long long)(3 + c) * a.npx;
+    for (int idx = threadIdx.x; idx < fn; idx += blockDim.x) {
+        const int yy = idx / fw, xx = idx - yy * fw;
+        const long long o = (long long)(fy0 + yy) * a.w + fx0 + xx;
+        gn[o] += s_num[idx];
+        gd[o] += s_den[idx];
+    }
+}
+
+// --------------------------------------------------------- basic / final
+__global__ void bm3d_basic_kernel(const float* __restrict__ acc, float* __restrict__ basic, uint8_t* __restrict__ q,
+                                  long long npx) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= npx) return;
+    float y = 0.0F;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const float v = acc[c * npx + i] / acc[(3 + c) * npx + i];
+        basic[c * npx + i] = v;
+        if (c == 0) y = v;
+    }
+    q[i] = quantise(y * kInvS3);
+}
+
+template <class T>
+__global__ void bm3d_final_kernel(const float* __restrict__ acc, Img in, Img out, long long npx) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= in.w) return;
+    const long long i = (long long)y * in.w + x;
+    const float Y = acc[i] / acc[3 * npx + i];
+    const float U = acc[npx + i] / acc[4 * npx + i];
+    const float V = acc[2 * npx + i] / acc[5 * npx + i];
+    const float yy = Y * kInvS3, uu = U * kInvS2, vv = V * kInvS6;
+    const Rgba o{(yy + uu) + vv, yy - 2.0F * vv, (yy - uu) + vv, 0.0F};
+    store_rgb_keep_alpha(px<T>(out, x, y), o, px<const T>(in, x, y));
+}
+
+double bessel_i0(double x) {
+    double sum = 1.0, term = 1.0;
+    const double hx = 0.5 * x;
+    for (int k = 1; k < 64; ++k) {
+        term *= (hx / k) * (hx / k);
+        sum += term;
+        if (term < 1e-18 * sum) break;
+    }
+    return sum;
+}
+
+int ref_count(int n, int nstep) {
+    if (n < 8) return 0;
+    int m = (n - 8) / nstep + 1;
+    if ((n - 8) % nstep) ++m;
+    return m;
+}
+
+size_t align256(size_t v) { return (v + 255U) & ~(size_t)255U; }
+
+size_t filter_smem(const Bm3dPlan& p, int stage) {
+    return sizeof(float) * ((size_t)(stage == 2 ? 4 : 3) * p.fw * p.fw + (size_t)kFilterWarps * kWarpBuf + 64);
+}
+size_t match_smem(const Bm3dPlan& p) { return sizeof(uint32_t) * 4 * (size_t)p.mwin * p.mwpr; }
+
+}  // namespace
+
+int bm3d_plan(const cpipe_Bm3dSpecParams* p, int w, int h, Bm3dPlan* out) {
+    if (p == nullptr || out == nullptr) return CPIPE_BAD_INDEX;
+    const int n2 = p->n2;
+    if (!(n2 == 1 || n2 == 2 || n2 == 4 || n2 == 8 || n2 == 16)) return CPIPE_BAD_INDEX;
+    if (p->ns < 1 || p->ns > 45 || (p->ns & 1) == 0) return CPIPE_BAD_INDEX;
+    if (p->nstep < 1 || p->nstep > 8) return CPIPE_BAD_INDEX;
+    if (!(p->tau_match1 >= 0.0F && p->tau_match1 <= 16000.0F)) return CPIPE_BAD_INDEX;
+    if (!(p->tau_match2 >= 0.0F && p->tau_match2 <= 16000.0F)) return CPIPE_BAD_INDEX;
+    if (p->stages != 1 && p->stages != 2) return CPIPE_BAD_INDEX;
+    if (!(p->lambda3d >= 0.0F) || !(p->kaiser_beta >= 0.0F)) return CPIPE_BAD_INDEX;
+    if (w <= 0 || h <= 0 || w > 65535 || h > 65535) return CPIPE_BAD_INDEX;
+    Bm3dPlan& q = *out;
+    q = Bm3dPlan{};
+    q.w = w;
+    q.h = h;
+    q.ns = p->ns;
+    q.R = (p->ns - 1) / 2;
+    q.n2 = n2;
+    q.nstep = p->nstep;
+    q.stages = p->stages;
+    q.sigma = p->sigma;
+    q.sigma2 = p->sigma * p->sigma;
+    q.thr = p->lambda3d * p->sigma;
+    q.dthr[0] = (uint32_t)floor(64.0 * (double)p->tau_match1);
+    q.dthr[1] = (uint32_t)floor(64.0 * (double)p->tau_match2);
+    q.copy = w < 8 || h < 8 || !(p->sigma > 0.0F) || !(q.sigma2 > 0.0F);
+    if (q.copy) return CPIPE_OK;
+    double k1[8];
+    const double i0b = bessel_i0(p->kaiser_beta);
+    for (int n = 0; n < 8; ++n) {
+        const double t = (2.0 * n - 7.0) / 7.0;
+        k1[n] = bessel_i0(p->kaiser_beta * sqrt(1.0 - t * t)) / i0b;
+    }
+    for (int v = 0; v < 8; ++v)
+        for (int u = 0; u < 8; ++u) q.kaiser[v * 8 + u] = (float)(k1[v] * k1[u]);
+    q.nrx = ref_count(w, q.nstep);
+    q.nry = ref_count(h, q.nstep);
+    q.fw = (kRefTile - 1) * q.nstep + 2 * q.R + 8;
+    const int span = kRefTile * q.nstep;
+    q.phases = (span + 2 * q.R + 8 + span - 1) / span;
+    q.ntx = (q.nrx + kRefTile - 1) / kRefTile;
+    q.nty = (q.nry + kRefTile - 1) / kRefTile;
+    q.mwin = (kMatchTile - 1) * q.nstep + 2 * q.R + 8;
+    q.mwpr = (q.mwin + 3) / 4 + 1;
+    const size_t npx = (size_t)w * h, nref = (size_t)q.nrx * q.nry;
+    size_t o = 0;
+    q.off_yuv = o;
+    o = align256(o + 3 * npx * sizeof(float));
+    q.off_basic = o;
+    if (q.stages == 2) o = align256(o + 3 * npx * sizeof(float));
+    q.off_acc = o;
+    o = align256(o + 6 * npx * sizeof(float));
+    q.off_q = o;
+    o = align256(o + npx);
+    q.off_list = o;
+    o = align256(o + nref * 16 * sizeof(uint32_t));
+    q.off_cnt = o;
+    o = align256(o + nref);
+    q.bytes = o;
+    return CPIPE_OK;
+}
+
+cudaError_t bm3d_setup(const Bm3dPlan& p) {
+    if (p.copy) return cudaSuccess;
+    static const size_t kSmemOptIn = 227 * 1024;
+    const size_t ms = match_smem(p), fs1 = filter_smem(p, 1), fs2 = filter_smem(p, 2);
+    if (ms > kSmemOptIn || fs2 > kSmemOptIn) return cudaErrorInvalidConfiguration;
+    cudaError_t e = cudaFuncSetAttribute(bm3d_match_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ms);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(bm3d_filter_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fs1);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(bm3d_filter_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fs2);
+    return e;
+}
+
+cudaError_t bm3d_run(const Bm3dPlan& p, const Img& in, const Img& out, bool f16, void* scratch, cudaStream_t st,
+                     bool setup) {
+    if (p.copy) {
+        const int elem = f16 ? 2 : 4;
+        return launch_copy(in.data, in.row_stride * elem, out.data, out.row_stride * elem, (long long)in.w * 4 * elem,
+                           in.h, st);
+    }
+    char* base = static_cast<char*>(scratch);
+    float* yuv = reinterpret_cast<float*>(base + p.off_yuv);
+    float* basic = reinterpret_cast<float*>(base + p.off_basic);
+    float* acc = reinterpret_cast<float*>(base + p.off_acc);
+    uint8_t* q = reinterpret_cast<uint8_t*>(base + p.off_q);
+    uint32_t* list = reinterpret_cast<uint32_t*>(base + p.off_list);
+    uint8_t* cnt = reinterpret_cast<uint8_t*>(base + p.off_cnt);
+    const long long npx = (long long)p.w * p.h;
+    cudaError_t e;
+    if (setup && (e = bm3d_setup(p)) != cudaSuccess) return e;
+    const size_t ms = match_smem(p), fs1 = filter_smem(p, 1), fs2 = filter_smem(p, 2);
+
+    const dim3 pgrid((p.w + 255) / 256, p.h);
+    if (f16) bm3d_prep_kernel<__half><<<pgrid, 256, 0, st>>>(in, yuv, q, npx);
+    else bm3d_prep_kernel<float><<<pgrid, 256, 0, st>>>(in, yuv, q, npx);
+
+    MatchArgs ma{p.w, p.h, p.nrx, p.nry, p.nstep, p.R, p.ns, p.n2, p.mwpr, p.mwin, p.dthr[0], q, list, cnt};
+    const dim3 mgrid((p.nrx + kMatchTile - 1) / kMatchTile, (p.nry + kMatchTile - 1) / kMatchTile);
+    FilterArgs fa{};
+    fa.w = p.w;
+    fa.h = p.h;
+    fa.nrx = p.nrx;
+    fa.nry = p.nry;
+    fa.nstep = p.nstep;
+    fa.R = p.R;
+    fa.ntx = p.ntx;
+    fa.nty = p.nty;
+    fa.phases = p.phases;
+    fa.fw = p.fw;
+    fa.sigma2 = p.sigma2;
+    fa.thr = p.thr;
+    fa.npx = npx;
+    fa.list = list;
+    fa.cnt = cnt;
+    fa.noisy = yuv;
+    fa.basic = basic;
+    fa.acc = acc;
+    for (int i = 0; i < 64; ++i) fa.kaiser[i] = p.kaiser[i];
+    const dim3 fgrid((p.ntx + p.phases - 1) / p.phases, (p.nty + p.phases - 1) / p.phases, 3);
+
+    for (int stage = 1; stage <= p.stages; ++stage) {
+        if ((e = cudaMemsetAsync(acc, 0, 6 * (size_t)npx * sizeof(float), st)) != cudaSuccess) return e;
+        ma.dthr = p.dthr[stage - 1];
+        bm3d_match_kernel<<<mgrid, kMatchTile * kMatchTile, ms, st>>>(ma);
+        for (int py = 0; py < p.phases; ++py)
+            for (int pxh = 0; pxh < p.phases; ++pxh) {
+                if (stage == 1) bm3d_filter_kernel<1><<<fgrid, 32 * kFilterWarps, fs1, st>>>(fa, pxh, py);
+                else bm3d_filter_kernel<2><<<fgrid, 32 * kFilterWarps, fs2, st>>>(fa, pxh, py);
+            }
+        if (stage == 1 && p.stages == 2)
+            bm3d_basic_kernel<<<(unsigned)((npx + 255) / 256), 256, 0, st>>>(acc, basic, q, npx);
+    }
+    if (f16) bm3d_final_kernel<__half><<<pgrid, 256, 0, st>>>(acc, in, out, npx);
+    else bm3d_final_kernel<float><<<pgrid, 256, 0, st>>>(acc, in, out, npx);
+    return cudaGetLastError();
+}
+
+}  // namespace cpb

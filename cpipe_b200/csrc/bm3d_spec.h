@@ -1,0 +1,43 @@
+// Two-stage colour BM3D ("spec mode", aot_id denoise_bm3d_spec): host plan
+// and launcher shared by the filter entry and the fused chain.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+#include <stdint.h>
+
+#include "../../include/cpipe_b200_params.h"
+#include "common.cuh"
+
+namespace cpb {
+
+struct Bm3dPlan {
+    int w = 0, h = 0;
+    int nrx = 0, nry = 0;  // reference blocks per axis
+    int ns = 0, R = 0, n2 = 0, nstep = 0, stages = 0;
+    float sigma = 0.0F, sigma2 = 0.0F, thr = 0.0F;
+    uint32_t dthr[2] = {0, 0};  // integer match thresholds (64 * tau)
+    float kaiser[64] = {};
+    int fw = 0;            // filter footprint edge bound (pixels)
+    int phases = 0;        // filter launch phases per axis
+    int ntx = 0, nty = 0;  // filter tiles (8x8 reference blocks each)
+    int mwin = 0, mwpr = 0;  // match tile region edge bound, words per smem row
+    bool copy = false;       // image below 8x8 or sigma <= 0: output = input
+    size_t off_yuv = 0, off_basic = 0, off_acc = 0, off_q = 0, off_list = 0, off_cnt = 0, bytes = 0;
+};
+
+// Validates the parameters (CPIPE_BAD_INDEX when out of range) and sizes the
+// scratch buffer for a w x h frame.
+int bm3d_plan(const cpipe_Bm3dSpecParams* p, int w, int h, Bm3dPlan* out);
+
+// Sets the kernels' shared-memory limits for the plan (host-side; call
+// before capturing bm3d_run into a graph).
+cudaError_t bm3d_setup(const Bm3dPlan& plan);
+
+// RGBA in -> RGBA out (both binary16 when f16, else float32; alpha copied).
+// scratch: plan.bytes of device memory, 256-byte aligned.  setup = true runs
+// bm3d_setup first.
+cudaError_t bm3d_run(const Bm3dPlan& plan, const Img& in, const Img& out, bool f16, void* scratch,
+                     cudaStream_t stream, bool setup = true);
+
+}  // namespace cpb

@@ -21,6 +21,7 @@
 #include "../../include/cpipe_b200.h"
 #include "filters_impl.h"
 #include "kernels.h"
+#include "bm3d_spec.h"
 #include "demosaic.cuh"
 #include "nodes.cuh"
 
@@ -327,9 +328,12 @@ struct cpipe_cuda_chain {
     int radius = 2;
     void* d_tables = nullptr;   // gain tables + LUT cells
     void* d_mid[2] = {nullptr, nullptr};  // K1 output, K2 output (scratch frames)
+    int denoise_mode = 0;
+    Bm3dPlan bm3d{};
+    void* d_denoise = nullptr;            // scratch of the mode-1/2 denoiser
     void* d_io[2] = {nullptr, nullptr};   // device staging for run_host
     size_t frame_bytes = 0;
-    // profiling: 4 events per frame (start, after K1, after K2, after K3)
+    // profiling: 5 events per frame (start, after K1, after K2, after the denoiser, after K3)
     bool profiling = false;
     std::vector<cudaEvent_t> events;
     size_t profiled = 0;
@@ -341,15 +345,17 @@ struct cpipe_cuda_chain {
 
 namespace {
 
+constexpr int kProfileEvents = 5;
+
 cudaEvent_t* profile_slot(cpipe_cuda_chain* c) {
     if (!c->profiling) return nullptr;
-    const size_t need = (c->profiled + 1) * 4;
+    const size_t need = (c->profiled + 1) * kProfileEvents;
     while (c->events.size() < need) {
         cudaEvent_t e;
         if (cudaEventCreate(&e) != cudaSuccess) return nullptr;
         c->events.push_back(e);
     }
-    return &c->events[c->profiled++ * 4];
+    return &c->events[c->profiled++ * kProfileEvents];
 }
 
 int launch_chain(cpipe_cuda_chain* c, const void* d_raw, size_t raw_pitch, void* d_out, size_t out_pitch,
@@ -390,6 +396,13 @@ int launch_chain(cpipe_cuda_chain* c, const void* d_raw, size_t raw_pitch, void*
         else warp_wb_cm_kernel<float, false, false><<<gb, 128, 0, st>>>(k2_in, k2_out, c->warp, c->color);
     }
     if (ev) cudaEventRecord(ev[2], st);
+    if (c->denoise_mode == 1) {
+        const Img dn_out = (k2_out.data == mid1.data) ? mid0 : mid1;
+        const cudaError_t e = bm3d_run(c->bm3d, k2_out, dn_out, c->f16, c->d_denoise, st, false);
+        if (e != cudaSuccess) return cuda_status(e, "chain bm3d");
+        k2_out = dn_out;
+    }
+    if (ev) cudaEventRecord(ev[3], st);
     const dim3 gc((unsigned)((w + kCTW - 1) / kCTW), (unsigned)((h + kCTH - 1) / kCTH));
 #define K3(TT, F, R)                                                                                       \
     denoise_tone_kernel<TT, F, R><<<gc, 256, denoise_tone_smem<TT, F, R>(), st>>>(k2_out, out, c->tone);
@@ -399,7 +412,7 @@ int launch_chain(cpipe_cuda_chain* c, const void* d_raw, size_t raw_pitch, void*
         if (c->radius == 0) { K3(float, false, 0) } else if (c->radius == 1) { K3(float, false, 1) } else { K3(float, false, 2) }
     }
 #undef K3
-    if (ev) cudaEventRecord(ev[3], st);
+    if (ev) cudaEventRecord(ev[4], st);
     return cuda_status(cudaGetLastError(), "chain launch");
 }
 
@@ -487,7 +500,16 @@ cpipe_cuda_chain* cpipe_cuda_chain_create(const cpipe_cuda_chain_config* cfg, in
     // colour, denoise, tone
     std::memcpy(c->color.neutral, cfg->as_shot_neutral, sizeof(c->color.neutral));
     std::memcpy(c->color.cm, cfg->colormatrix, sizeof(c->color.cm));
-    c->tone.bm3d_strength = fminf(1.0F, fmaxf(0.0F, cfg->bm3d_sigma / 0.03F));
+    c->denoise_mode = cfg->denoise_mode;
+    if (c->denoise_mode < 0 || c->denoise_mode > 1) return fail(CPIPE_UNSUPPORTED, c);
+    c->tone.bm3d_strength = c->denoise_mode == 0 ? fminf(1.0F, fmaxf(0.0F, cfg->bm3d_sigma / 0.03F)) : 0.0F;
+    if (c->denoise_mode == 1) {
+        cpipe_Bm3dSpecParams sp = cfg->bm3d_spec;
+        if (!(sp.sigma > 0.0F)) sp.sigma = cfg->bm3d_sigma;
+        if ((st = bm3d_plan(&sp, w, h, &c->bm3d)) != CPIPE_OK) return fail(st, c);
+        if (!c->bm3d.copy && cudaMalloc(&c->d_denoise, c->bm3d.bytes) != cudaSuccess) return fail(CPIPE_OOM, c);
+        if (cudaError_t e = bm3d_setup(c->bm3d); e != cudaSuccess) return fail(cuda_status(e, "bm3d setup"), c);
+    }
     // guided_radius 0 leaves the guided node out; otherwise the reference box
     // is 3x3 for radius <= 1 and 5x5 above (guided_filter_generator.cpp:66-70).
     c->radius = cfg->guided_radius <= 0 ? 0 : (cfg->guided_radius == 1 ? 1 : 2);
@@ -512,6 +534,7 @@ void cpipe_cuda_chain_destroy(cpipe_cuda_chain* c) {
     for (cudaEvent_t e : c->events) cudaEventDestroy(e);
     if (c->graph) cudaGraphExecDestroy(c->graph);
     cudaFree(c->d_tables);
+    cudaFree(c->d_denoise);
     for (void* p : c->d_mid) cudaFree(p);
     for (void* p : c->d_io) cudaFree(p);
     delete c;
@@ -575,17 +598,17 @@ int cpipe_cuda_chain_set_profiling(cpipe_cuda_chain* c, int enable) {
     return CPIPE_OK;
 }
 
-int cpipe_cuda_chain_profile(cpipe_cuda_chain* c, double ms_per_kernel[3], int* frames) {
-    if (!c || !ms_per_kernel || !frames) return CPIPE_BAD_INDEX;
-    ms_per_kernel[0] = ms_per_kernel[1] = ms_per_kernel[2] = 0.0;
+int cpipe_cuda_chain_profile(cpipe_cuda_chain* c, double ms_per_stage[4], int* frames) {
+    if (!c || !ms_per_stage || !frames) return CPIPE_BAD_INDEX;
+    for (int k = 0; k < kProfileEvents - 1; ++k) ms_per_stage[k] = 0.0;
     for (size_t f = 0; f < c->profiled; ++f) {
-        cudaEvent_t* ev = &c->events[f * 4];
-        const int st = cuda_status(cudaEventSynchronize(ev[3]), "profile sync");
+        cudaEvent_t* ev = &c->events[f * kProfileEvents];
+        const int st = cuda_status(cudaEventSynchronize(ev[kProfileEvents - 1]), "profile sync");
         if (st != CPIPE_OK) return st;
-        for (int k = 0; k < 3; ++k) {
+        for (int k = 0; k < kProfileEvents - 1; ++k) {
             float ms = 0.0F;
             cudaEventElapsedTime(&ms, ev[k], ev[k + 1]);
-            ms_per_kernel[k] += ms;
+            ms_per_stage[k] += ms;
         }
     }
     *frames = (int)c->profiled;

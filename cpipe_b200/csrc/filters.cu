@@ -17,6 +17,7 @@
 #include <vector>
 
 #include "../../include/cpipe_b200.h"
+#include "bm3d_spec.h"
 #include "filters_impl.h"
 #include "kernels.h"
 
@@ -531,6 +532,27 @@ int cpipe_cuda_denoise_bm3d_step2(halide_buffer_t* const* inputs, size_t n_in, h
                                                in.img.h, call.stream),
                                    "bm3d_step2"));
 }
+// Two-stage colour BM3D (bm3d_spec.cu); no reference counterpart.
+int cpipe_cuda_denoise_bm3d_spec(halide_buffer_t* const* inputs, size_t n_in, halide_buffer_t* const* outputs,
+                                 size_t n_out, const void* blob, size_t blob_size) {
+    CHECK_ARITY(1, 1);
+    if (blob == nullptr || blob_size < sizeof(cpipe_Bm3dSpecParams)) return CPIPE_BAD_INDEX;
+    if (!device_ready()) return CPIPE_INTERNAL_ERROR;
+    cpipe_Bm3dSpecParams prm;
+    std::memcpy(&prm, blob, sizeof(prm));
+    Call call;
+    Bound in, out;
+    int st = rgba_pair(call, inputs, outputs, &in, &out);
+    if (st != CPIPE_OK) return call.finish(st);
+    Bm3dPlan plan;
+    if ((st = bm3d_plan(&prm, in.img.w, in.img.h, &plan)) != CPIPE_OK) {
+        set_error("bm3d_spec: %s", "parameters out of range");
+        return call.finish(st);
+    }
+    void* scratch = nullptr;
+    if (!plan.copy && (st = call.alloc(plan.bytes, &scratch)) != CPIPE_OK) return call.finish(st);
+    return call.finish(cuda_status(bm3d_run(plan, in.img, out.img, in.elem == 2, scratch, call.stream), "bm3d_spec"));
+}
 int cpipe_cuda_denoise_guided_filter(halide_buffer_t* const* inputs, size_t n_in, halide_buffer_t* const* outputs,
                                      size_t n_out, const void* blob, size_t blob_size) {
     CHECK_ARITY(1, 1);
@@ -817,6 +839,7 @@ static const cpipe_cuda_filter_desc kFilters[] = {
     {"colormatrix_dng_to_working", (void*)&cpipe_cuda_colormatrix_dng_to_working, 1},
     {"denoise_bm3d_step1", (void*)&cpipe_cuda_denoise_bm3d_step1, 1},
     {"denoise_bm3d_step2", (void*)&cpipe_cuda_denoise_bm3d_step2, 1},
+    {"denoise_bm3d_spec", (void*)&cpipe_cuda_denoise_bm3d_spec, 1},
     {"denoise_guided_filter", (void*)&cpipe_cuda_denoise_guided_filter, 1},
     {"denoise_wavelet_bayes_shrink", (void*)&cpipe_cuda_denoise_wavelet_bayes_shrink, 1},
     {"lens_dng_opcode_list_3", (void*)&cpipe_cuda_lens_dng_opcode_list_3, 1},

@@ -366,6 +366,17 @@ int node_bm3d(Ctx& c) {
             }
         }
     }
+    std::string algorithm = "box2x2";
+    c.get_string("algorithm", &algorithm);
+    if (algorithm == "bm3d") {
+        // Extension: the published two-stage BM3D (aot_id denoise_bm3d_spec);
+        // "box2x2" (default) is the reference's computation.
+        cpipe_Bm3dSpecParams sp{sigma, 2.7F, 2500.0F, 400.0F, 16, 39, 3, 2.0F, 2, 0};
+        if (c.get_double("stages", &v)) sp.stages = v < 1.5 ? 1 : 2;
+        if ((st = c.submit("denoise_bm3d_spec", &sp, sizeof(sp))) != CPIPE_OK) return st;
+        return c.step("denoise.bm3d");
+    }
+    if (algorithm != "box2x2") return CPIPE_BAD_INDEX;
     const cpipe_Bm3dParams p{sigma};
     if ((st = c.submit("denoise_bm3d_step1", &p, sizeof(p))) != CPIPE_OK) return st;
     return c.step("denoise.bm3d");
@@ -533,8 +544,10 @@ const char kCm[] = MANIFEST("com.cpipe.colormatrix.dng_to_working", "DNG Color M
 const char kBm3d[] = MANIFEST("com.cpipe.denoise.bm3d", "BM3D Denoise", "denoise",
     RGBA_IN("rgb", "\"requires_steps_applied\":[\"color_matrix\"],\"requires_fields\":[\"calibration.noise_profile\"]"),
     RGBA_OUT("rgb", "denoise.bm3d", ""),
-    "{\"name\":\"sigma\",\"type\":\"number\",\"range\":{\"min\":0,\"max\":0.2}},{\"name\":\"sigma_override\",\"type\":\"number\",\"range\":{\"min\":0},\"default\":0}",
-    "scene_linear_rec2020", "scene_linear_rec2020", "true", "\"bm3d_parity_kernel\"");
+    "{\"name\":\"sigma\",\"type\":\"number\",\"range\":{\"min\":0,\"max\":0.2}},{\"name\":\"sigma_override\",\"type\":\"number\",\"range\":{\"min\":0},\"default\":0},"
+    "{\"name\":\"algorithm\",\"type\":\"enum\",\"values\":[\"box2x2\",\"bm3d\"],\"default\":\"box2x2\"},"
+    NUM("stages", "1", "2", "2"),
+    "scene_linear_rec2020", "scene_linear_rec2020", "true", "\"bm3d_parity_kernel\",\"bm3d_match_kernel\",\"bm3d_filter_kernel\"");
 const char kGuided[] = MANIFEST("com.cpipe.denoise.guided_filter", "Guided Filter Denoise", "denoise",
     RGBA_IN("rgb", "\"requires_steps_applied\":[\"color_matrix\"]"), RGBA_OUT("rgb", "denoise.guided_filter", ""),
     NUM("radius", "1", "32", "1") "," NUM("eps", "1e-05", "0.1", "0.015"), "scene_linear_rec2020",

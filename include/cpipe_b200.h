@@ -74,6 +74,11 @@ CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_wb_dual_illuminant);         /* wb_dual_illum
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_colormatrix_dng_to_working); /* colormatrix_dng_to_working_dispatch.cpp:17-62 */
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_denoise_bm3d_step1);         /* bm3d_dispatch.cpp:19-30 */
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_denoise_bm3d_step2);         /* bm3d_dispatch.cpp:32-43 */
+/* Two-stage colour BM3D (aot_id "denoise_bm3d_spec", blob cpipe_Bm3dSpecParams):
+ * the published algorithm the reference's denoise.bm3d node is named after; the
+ * node selects it with param algorithm = "bm3d".  No reference filter
+ * counterpart (the reference's bm3d_step1 is a 2x2 box blend). */
+CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_denoise_bm3d_spec);
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_denoise_guided_filter);      /* guided_filter_dispatch.cpp */
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_denoise_wavelet_bayes_shrink); /* wavelet_bayes_shrink_dispatch.cpp */
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_lens_dng_opcode_list_3);     /* dng_opcode_list_3_dispatch.cpp:333-398 */
@@ -206,6 +211,13 @@ typedef struct {
     size_t lut_blob_size;
     int32_t plain_f32;                  /* 1: FP32 plain form (no f16 rounding between nodes) */
     int32_t use_graph;                  /* 1: replay a captured CUDA graph per (input, output) pair */
+    /* Denoiser in the BM3D slot: 0 = the reference's denoise.bm3d computation
+     * (2x2 box blend, bm3d_sigma); 1 = two-stage BM3D (bm3d_spec; its sigma 0
+     * means bm3d_sigma); 2 = learned surrogate (surrogate_blob). */
+    int32_t denoise_mode;
+    cpipe_Bm3dSpecParams bm3d_spec;
+    const void* surrogate_blob;
+    size_t surrogate_blob_size;
 } cpipe_cuda_chain_config;
 
 typedef struct cpipe_cuda_chain cpipe_cuda_chain;
@@ -217,11 +229,12 @@ size_t cpipe_cuda_chain_output_bytes(const cpipe_cuda_chain* chain);
 int cpipe_cuda_chain_run(cpipe_cuda_chain* chain, const void* d_raw_u16, void* d_out, void* stream);
 /* Host pointers: H2D of the raw frame, the chain, D2H of the result; returns after the copy-out. */
 int cpipe_cuda_chain_run_host(cpipe_cuda_chain* chain, const uint16_t* h_raw, void* h_out, void* stream);
-/* Per-kernel timing: while enabled, each run records CUDA events around its
- * three kernels (and bypasses the graph); chain_profile sums the kernel times
- * of the runs recorded since the last call. */
+/* Per-stage timing: while enabled, each run records CUDA events around its
+ * stages (and bypasses the graph); chain_profile sums the stage times of the
+ * runs recorded since the last call: [0] raw_to_rgba, [1] warp_wb_cm,
+ * [2] the denoiser of denoise_mode 1 or 2 (0 in mode 0), [3] denoise_tone. */
 int cpipe_cuda_chain_set_profiling(cpipe_cuda_chain* chain, int enable);
-int cpipe_cuda_chain_profile(cpipe_cuda_chain* chain, double ms_per_kernel[3], int* frames);
+int cpipe_cuda_chain_profile(cpipe_cuda_chain* chain, double ms_per_stage[4], int* frames);
 /* Device memory, streams and events for callers without their own CUDA runtime. */
 int cpipe_cuda_set_device(int device);
 int cpipe_cuda_device_alloc(size_t bytes, void** out);

@@ -153,6 +153,29 @@ typedef struct {
     float shadows;
 } cpipe_FilmicRgbParams;
 
+/* Two-stage colour BM3D ("spec mode"; aot_id denoise_bm3d_spec).  The
+ * reference's denoise.bm3d node computes a 2x2 box blend
+ * (nodes/denoise/bm3d_step1_generator.cpp:33-61); this is the published
+ * algorithm it is named after: Dabov, Foi, Katkovnik, Egiazarian, "Image
+ * denoising by sparse 3D transform-domain collaborative filtering", IEEE TIP
+ * 16(8), 2007, in its colour form (grouping on luminance, ICIP 2007), with
+ * the parameter values of Lebrun, "An analysis and implementation of the BM3D
+ * image denoising method", IPOL 2012.  Blocks are 8x8; matching uses the
+ * 8-bit-quantised luminance mean; thresholds are mean squared 8-bit
+ * differences per pixel.  There is no reference counterpart. */
+typedef struct {
+    float sigma;        /* noise standard deviation per RGB channel (linear units); <= 0 copies */
+    float lambda3d;     /* hard-threshold factor (2.7) */
+    float tau_match1;   /* step-1 match threshold, mean squared 8-bit difference (2500, <= 16000) */
+    float tau_match2;   /* step-2 match threshold (400, <= 16000) */
+    int32_t n2;         /* maximum blocks per stack: 1, 2, 4, 8 or 16 */
+    int32_t ns;         /* search window edge, odd, 1..45 (39) */
+    int32_t nstep;      /* reference-block step, 1..8 (3) */
+    float kaiser_beta;  /* aggregation window parameter (2.0) */
+    int32_t stages;     /* 1 = hard threshold only, 2 = hard threshold then Wiener */
+    int32_t reserved;   /* 0 */
+} cpipe_Bm3dSpecParams;
+
 #if defined(__cplusplus)
 #define CPIPE_STATIC_ASSERT static_assert
 #else
@@ -164,6 +187,7 @@ CPIPE_STATIC_ASSERT(sizeof(cpipe_GainMapDispatchHeader) == 24, "GainMapDispatchH
 CPIPE_STATIC_ASSERT(sizeof(cpipe_GainMapDispatchPlane) == 72, "GainMapDispatchPlane layout");
 CPIPE_STATIC_ASSERT(sizeof(cpipe_Opcode3DispatchRecord) == 320, "Opcode3DispatchRecord layout");
 CPIPE_STATIC_ASSERT(sizeof(cpipe_Lut3dParamHeader) == 12, "Lut3dParamHeader layout");
+CPIPE_STATIC_ASSERT(sizeof(cpipe_Bm3dSpecParams) == 40, "Bm3dSpecParams layout");
 
 #ifdef __cplusplus
 } /* extern "C" */

@@ -24,7 +24,16 @@ def run_chain_oracle(cfg, raw, blobs=None):
         assert st == 0
     x = oracle.wb(x, cfg.neutral, f16)
     x = oracle.colormatrix(x, b["colormatrix_t"], f16)
-    x = oracle.bm3d_parity(x, cfg.bm3d_sigma, f16)
+    denoise = getattr(cfg, "denoise", "box2x2")
+    if denoise == "bm3d":
+        from cpipe_b200 import blobs as B
+        x = oracle.bm3d_spec(x, B.bm3d_spec(cfg.bm3d_sigma, stages=cfg.bm3d_stages)).astype(np.float32)
+        if f16:
+            x = oracle.h16(x)
+    elif denoise == "box2x2":
+        x = oracle.bm3d_parity(x, cfg.bm3d_sigma, f16)
+    else:
+        raise ValueError(f"no oracle for denoise={denoise}")
     if cfg.guided_radius > 0:
         x = oracle.guided(x, cfg.guided_radius, cfg.guided_eps, f16)
     if cfg.wavelet_strength >= 0:

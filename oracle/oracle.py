@@ -147,6 +147,40 @@ def bm3d_parity(x, sigma, f16=True):
     return out
 
 
+def bm3d_spec(x, blob, basic=False):
+    """Two-stage colour BM3D in FP64 (oracle_bm3d.c).  x: HxWx4 float32 (the
+    RGBA16F input as float).  Returns the HxWx4 float64 estimate, and with
+    basic=True also the step-1 estimate as 3xHxW opponent (Y, U, V) planes."""
+    x = _f32(x)
+    h, w = x.shape[:2]
+    out = np.empty((h, w, 4), np.float64)
+    b3 = np.empty((3, h, w), np.float64) if basic else None
+    pb, _ = _blob(blob)
+    st = lib().oracle_bm3d_spec(_p(x), w, h, pb, _p(out), _p(b3) if basic else None)
+    if st != 0:
+        raise ValueError(f"oracle_bm3d_spec status {st}")
+    return (out, b3) if basic else out
+
+
+def bm3d_quantise_rgb(x):
+    x = _f32(x)
+    q = np.empty(x.shape[:2], np.uint8)
+    lib().oracle_bm3d_quantise_rgb(_p(x), x.shape[1], x.shape[0], _p(q))
+    return q
+
+
+def bm3d_match(q, x, y, ns=39, n2=16, tau=2500.0):
+    """Group of the reference block at (x, y): list of (x, y) block positions."""
+    q = np.ascontiguousarray(q, np.uint8)
+    pos = (C.c_uint32 * 16)()
+    scratch = (C.c_uint64 * (ns * ns))()
+    L = lib()
+    L.oracle_bm3d_dthr.restype = C.c_uint32
+    n = L.oracle_bm3d_match(_p(q), q.shape[1], q.shape[0], int(x), int(y), int(ns), int(n2),
+                            C.c_uint32(L.oracle_bm3d_dthr(C.c_float(tau))), pos, scratch)
+    return [(pos[i] & 0xFFFF, pos[i] >> 16) for i in range(n)]
+
+
 def guided(x, radius, eps, f16=True):
     x = _f32(x)
     out = np.empty_like(x)

@@ -61,7 +61,9 @@ EXPECTED_NODES = {
     "com.cpipe.demosaic.quad_bayer_remosaic": ("qbc", "bayer", []),
     "com.cpipe.wb.dual_illuminant": ("rgb", "rgb", []),
     "com.cpipe.colormatrix.dng_to_working": ("rgb", "rgb", []),
-    "com.cpipe.denoise.bm3d": ("rgb", "rgb", ["sigma", "sigma_override"]),
+    # sigma, sigma_override as the reference; algorithm and stages select the
+    # two-stage BM3D extension (default "box2x2" is the reference computation).
+    "com.cpipe.denoise.bm3d": ("rgb", "rgb", ["sigma", "sigma_override", "algorithm", "stages"]),
     "com.cpipe.denoise.guided_filter": ("rgb", "rgb", ["radius", "eps"]),
     "com.cpipe.denoise.wavelet_bayes_shrink": ("rgb", "rgb", ["chroma_strength"]),
     "com.cpipe.lens.dng_opcode_list_3": ("scene_rgb", "corrected_rgb", []),

@@ -9,7 +9,7 @@ import pytest
 from chain_oracle import run_chain_oracle
 from cpipe_b200 import _abi as A
 from cpipe_b200.chain import Chain, ChainConfig
-from parity import assert_f16_parity, assert_f32_parity, f16_ulp_distance
+from parity import assert_f16_parity, assert_f32_parity, f16_ulp_distance, psnr
 
 pytestmark = pytest.mark.gpu
 
@@ -43,7 +43,8 @@ def run_nodes_on_gpu(host, cfg, raw):
     if cfg.warp is not None:
         steps.append(("com.cpipe.lens.dng_opcode_list_3", F16, {}))
     steps += [("com.cpipe.wb.dual_illuminant", F16, {}), ("com.cpipe.colormatrix.dng_to_working", F16, {}),
-              ("com.cpipe.denoise.bm3d", F16, {})]
+              ("com.cpipe.denoise.bm3d", F16, {"algorithm": "bm3d", "stages": cfg.bm3d_stages}
+               if cfg.denoise == "bm3d" else {})]
     if cfg.guided_radius > 0:
         steps.append(("com.cpipe.denoise.guided_filter", F16, {"radius": cfg.guided_radius, "eps": cfg.guided_eps}))
     if cfg.wavelet_strength >= 0:
@@ -158,3 +159,21 @@ def test_chain_full_12mp(cuda_device, host):
     ulps, n_off = assert_f16_parity(a, want, what="12MP chain vs oracle")
     chain.close()
     chain_ng.close()
+
+
+@pytest.mark.parametrize("demosaic", ["rcd", "amaze"])
+def test_chain_with_two_stage_bm3d(host, demosaic):
+    """denoise_mode 1: the two-stage BM3D between colormatrix and guided.  The
+    BM3D aggregation order is not fixed on the GPU (shared-memory atomics), so
+    the chain is compared with the nodes one by one, and with the oracle chain
+    (FP64 BM3D), within tolerances: PSNR >= 60 dB against the nodes, >= 50 dB
+    against the oracle."""
+    cfg = ChainConfig.full_12mp(width=200, height=136, demosaic=demosaic, denoise="bm3d")
+    raw = cfg.make_raw()
+    got = Chain(cfg).run_host(raw).astype(np.float32)
+    nodes = run_nodes_on_gpu(host, cfg, raw).astype(np.float32)
+    want = run_chain_oracle(cfg, raw)
+    p_nodes, p_oracle = psnr(got[..., :3], nodes[..., :3]), psnr(got[..., :3], want[..., :3])
+    print(f"bm3d chain {demosaic}: vs nodes {p_nodes:.1f} dB, vs oracle {p_oracle:.1f} dB")
+    assert p_nodes >= 60.0 and p_oracle >= 50.0
+    np.testing.assert_array_equal(got[..., 3], want[..., 3])
