@@ -120,7 +120,8 @@ class ChainConfig(C.Structure):
                 ("guided_radius", C.c_int32), ("guided_eps", C.c_float), ("wavelet_strength", C.c_float),
                 ("filmic", FilmicRgbParams), ("lut_blob", C.c_void_p), ("lut_blob_size", C.c_size_t),
                 ("plain_f32", C.c_int32), ("use_graph", C.c_int32), ("denoise_mode", C.c_int32),
-                ("bm3d_spec", Bm3dSpecParams), ("surrogate_blob", C.c_void_p), ("surrogate_blob_size", C.c_size_t)]
+                ("bm3d_spec", Bm3dSpecParams), ("surrogate_blob", C.c_void_p), ("surrogate_blob_size", C.c_size_t),
+                ("noise_a", C.c_float), ("noise_b", C.c_float), ("stop_after", C.c_int32)]
 
 
 MAIN_ENTRY = C.CFUNCTYPE(C.c_int, C.c_char_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p)
@@ -154,6 +155,8 @@ EXPORTS = [
     "cpipe_cuda_tone_filmic_rgb", "cpipe_cuda_copy", "cpipe_cuda_filters", "cpipe_cuda_find_filter",
     "cpipe_cuda_color_3d_lut_noalloc",
     "cpipe_b200_node_descs", "cpipe_b200_find_node",
+    "cpipe_cuda_scene_raw", "cpipe_surrogate_blob_size", "cpipe_surrogate_create", "cpipe_surrogate_destroy", "cpipe_surrogate_export",
+    "cpipe_surrogate_denoise", "cpipe_surrogate_train_step", "cpipe_surrogate_gradients",
     "cpipe_b200_wb_prepare", "cpipe_b200_colormatrix_compose", "cpipe_b200_pack_gain_maps",
     "cpipe_b200_pack_opcode_list_3", "cpipe_b200_load_lut",
     "cpipe_b200_host_create", "cpipe_b200_host_destroy", "cpipe_b200_host_abi", "cpipe_b200_host_set_memory_cap",
@@ -170,7 +173,8 @@ EXPORTS = [
     "cpipe_cuda_chain_create", "cpipe_cuda_chain_destroy", "cpipe_cuda_chain_output_bytes", "cpipe_cuda_chain_run",
     "cpipe_cuda_chain_run_host", "cpipe_cuda_pinned_alloc", "cpipe_cuda_pinned_free",
     "cpipe_cuda_chain_set_profiling", "cpipe_cuda_chain_profile", "cpipe_cuda_set_device", "cpipe_cuda_device_alloc",
-    "cpipe_cuda_device_free", "cpipe_cuda_memcpy_h2d", "cpipe_cuda_memcpy_d2h", "cpipe_cuda_stream_create",
+    "cpipe_cuda_device_free", "cpipe_cuda_memcpy_h2d", "cpipe_cuda_memcpy_d2h", "cpipe_cuda_memcpy_d2d_async", "cpipe_cuda_count_nonfinite",
+    "cpipe_cuda_stream_create",
     "cpipe_cuda_stream_destroy", "cpipe_cuda_stream_synchronize", "cpipe_cuda_event_create",
     "cpipe_cuda_event_destroy", "cpipe_cuda_event_record", "cpipe_cuda_event_elapsed_ms",
 ]
@@ -230,11 +234,19 @@ def lib():
         "cpipe_cuda_chain_profile": (i32, [vp, C.POINTER(C.c_double), C.POINTER(i32)]),
         "cpipe_cuda_set_device": (i32, [i32]), "cpipe_cuda_device_alloc": (i32, [sz, C.POINTER(vp)]),
         "cpipe_cuda_device_free": (None, [vp]), "cpipe_cuda_memcpy_h2d": (i32, [vp, vp, sz]),
-        "cpipe_cuda_memcpy_d2h": (i32, [vp, vp, sz]), "cpipe_cuda_stream_create": (i32, [C.POINTER(vp)]),
+        "cpipe_cuda_memcpy_d2h": (i32, [vp, vp, sz]), "cpipe_cuda_memcpy_d2d_async": (i32, [vp, vp, sz, vp]),
+        "cpipe_cuda_count_nonfinite": (i32, [vp, sz, i32, C.POINTER(C.c_uint64), vp]), "cpipe_cuda_stream_create": (i32, [C.POINTER(vp)]),
         "cpipe_cuda_stream_destroy": (None, [vp]), "cpipe_cuda_stream_synchronize": (i32, [vp]),
         "cpipe_cuda_event_create": (i32, [C.POINTER(vp)]), "cpipe_cuda_event_destroy": (None, [vp]),
         "cpipe_cuda_event_record": (i32, [vp, vp]),
         "cpipe_cuda_event_elapsed_ms": (i32, [vp, vp, C.POINTER(C.c_float)]),
+        "cpipe_cuda_scene_raw": (i32, [vp, i32, i32, C.c_uint64, i32, i32, C.c_float, C.c_float, vp, i32, vp]),
+        "cpipe_surrogate_blob_size": (sz, []), "cpipe_surrogate_create": (vp, [vp, sz, C.POINTER(i32)]),
+        "cpipe_surrogate_destroy": (None, [vp]), "cpipe_surrogate_export": (i32, [vp, vp, sz]),
+        "cpipe_surrogate_denoise": (i32, [vp, vp, vp, i32, i32, i32, i32, vp, vp]),
+        "cpipe_surrogate_train_step": (i32, [vp, vp, vp, vp, i32, i32, i32, C.c_float, i32, C.POINTER(C.c_float),
+                                             vp]),
+        "cpipe_surrogate_gradients": (i32, [vp, vp, sz]),
     }
     for name, (res, args) in sigs.items():
         f = getattr(L, name)

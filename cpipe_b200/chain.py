@@ -84,6 +84,7 @@ class ChainConfig:
     denoise: str = "box2x2"        # box2x2 (the reference's bm3d node) | bm3d (two-stage) | surrogate
     bm3d_stages: int = 2
     surrogate_blob: bytes = None   # trained network (cpipe_b200.surrogate) for denoise="surrogate"
+    stop_after: int = 0            # 1: output the denoiser's input; 2: the denoiser's output
 
     # ------------------------------------------------------------ workloads
     @classmethod
@@ -224,6 +225,8 @@ class ChainConfig:
                   C.sizeof(A.Bm3dSpecParams))
         if self.surrogate_blob:
             cfg.surrogate_blob, cfg.surrogate_blob_size = ptr(bytes(self.surrogate_blob))
+        cfg.noise_a, cfg.noise_b = self.noise_a, self.noise_b
+        cfg.stop_after = int(self.stop_after)
         return cfg, keep
 
 

@@ -16,7 +16,9 @@
 //   transform orthonormal 8x8 DCT-II, then orthonormal Haar along the group
 //   step 1    hard threshold |c| > lambda3d*sigma, weight 1/(sigma^2*kept)
 //   step 2    Wiener W = B^2/(B^2+sigma^2) from the basic estimate's group,
-//             weight 1/(sigma^2*sum W^2)
+//             weight 1/(sigma^2*max(sum W^2, 1e-20)) (1 when the sum is 0);
+//             the kernels use the weights times sigma^2, which cancels in
+//             num / den and keeps FP32 from overflowing
 //   aggregate weight x Kaiser(beta) 8x8 window; estimate = num / den
 //
 // Kernels (all FP32 on the CUDA cores; the transforms use explicit fused
@@ -51,6 +53,7 @@ namespace {
 constexpr float kInvS3 = 0.57735026918962576451F;
 constexpr float kInvS2 = 0.70710678118654752440F;
 constexpr float kInvS6 = 0.40824829046386301637F;
+constexpr float kMinWienerEnergy = 1e-20F;  // floor of sum W^2 in the step-2 weight
 
 // cos(m * pi / 16) for any integer m.
 __host__ __device__ constexpr float cos16(int m) {
@@ -337,7 +340,8 @@ __global__ void __launch_bounds__(256, 2) bm3d_filter_kernel(FilterArgs a, int p
                 kept += keep ? 1U : 0U;
             }
             kept = __reduce_add_sync(0xFFFFFFFFU, kept);
-            wgt = kept > 0U ? 1.0F / (a.sigma2 * (float)kept) : 1.0F;
+            // weight x sigma^2 (the factor cancels in num / den): 1/kept, or sigma^2
+            wgt = kept > 0U ? 1.0F / (float)kept : a.sigma2;
         } else {
             float B[32];
             forward3d(s_bas, fw, bx, by, hh, b, act, N, buf, B);
@@ -351,7 +355,7 @@ __global__ void __launch_bounds__(256, 2) bm3d_filter_kernel(FilterArgs a, int p
             }
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1) sw2 += __shfl_xor_sync(0xFFFFFFFFU, sw2, off);
-            wgt = sw2 > 0.0F ? 1.0F / (a.sigma2 * sw2) : 1.0F;
+            wgt = sw2 > 0.0F ? 1.0F / fmaxf(sw2, kMinWienerEnergy) : a.sigma2;
         }
         haar_inverse(Z, N, b, act);
         if (act) {

@@ -22,6 +22,7 @@
 #include "filters_impl.h"
 #include "kernels.h"
 #include "bm3d_spec.h"
+#include "surrogate.h"
 #include "demosaic.cuh"
 #include "nodes.cuh"
 
@@ -329,8 +330,11 @@ struct cpipe_cuda_chain {
     void* d_tables = nullptr;   // gain tables + LUT cells
     void* d_mid[2] = {nullptr, nullptr};  // K1 output, K2 output (scratch frames)
     int denoise_mode = 0;
+    int stop_after = 0;
     Bm3dPlan bm3d{};
-    void* d_denoise = nullptr;            // scratch of the mode-1/2 denoiser
+    void* d_denoise = nullptr;            // scratch of the mode-1 denoiser
+    SurrogateNet* sg = nullptr;           // mode-2 network
+    float* d_ab = nullptr;                // its noise model (a, b) on the device
     void* d_io[2] = {nullptr, nullptr};   // device staging for run_host
     size_t frame_bytes = 0;
     // profiling: 5 events per frame (start, after K1, after K2, after the denoiser, after K3)
@@ -387,7 +391,7 @@ int launch_chain(cpipe_cuda_chain* c, const void* d_raw, size_t raw_pitch, void*
         k2_in = mid1;
     }
     const dim3 gb((unsigned)((w + 127) / 128), (unsigned)h);
-    Img k2_out = (c->warp_mode == 2) ? mid0 : mid1;
+    Img k2_out = c->stop_after == 1 ? out : (c->warp_mode == 2) ? mid0 : mid1;
     if (c->warp_mode == 1) {
         if (c->f16) warp_wb_cm_kernel<__half, true, true><<<gb, 128, 0, st>>>(k2_in, k2_out, c->warp, c->color);
         else warp_wb_cm_kernel<float, false, true><<<gb, 128, 0, st>>>(k2_in, k2_out, c->warp, c->color);
@@ -396,13 +400,24 @@ int launch_chain(cpipe_cuda_chain* c, const void* d_raw, size_t raw_pitch, void*
         else warp_wb_cm_kernel<float, false, false><<<gb, 128, 0, st>>>(k2_in, k2_out, c->warp, c->color);
     }
     if (ev) cudaEventRecord(ev[2], st);
-    if (c->denoise_mode == 1) {
-        const Img dn_out = (k2_out.data == mid1.data) ? mid0 : mid1;
-        const cudaError_t e = bm3d_run(c->bm3d, k2_out, dn_out, c->f16, c->d_denoise, st, false);
-        if (e != cudaSuccess) return cuda_status(e, "chain bm3d");
+    if (c->stop_after == 1) {
+        if (ev) cudaEventRecord(ev[3], st);
+        if (ev) cudaEventRecord(ev[4], st);
+        return cuda_status(cudaGetLastError(), "chain launch");
+    }
+    if (c->denoise_mode != 0) {
+        const Img dn_out = c->stop_after == 2 ? out : (k2_out.data == mid1.data) ? mid0 : mid1;
+        const cudaError_t e =
+            c->denoise_mode == 1 ? bm3d_run(c->bm3d, k2_out, dn_out, c->f16, c->d_denoise, st, false)
+                                 : surrogate_infer(c->sg, k2_out.data, dn_out.data, 1, h, w, c->f16, c->d_ab, st);
+        if (e != cudaSuccess) return cuda_status(e, "chain denoise");
         k2_out = dn_out;
     }
     if (ev) cudaEventRecord(ev[3], st);
+    if (c->stop_after == 2) {
+        if (ev) cudaEventRecord(ev[4], st);
+        return cuda_status(cudaGetLastError(), "chain launch");
+    }
     const dim3 gc((unsigned)((w + kCTW - 1) / kCTW), (unsigned)((h + kCTH - 1) / kCTH));
 #define K3(TT, F, R)                                                                                       \
     denoise_tone_kernel<TT, F, R><<<gc, 256, denoise_tone_smem<TT, F, R>(), st>>>(k2_out, out, c->tone);
@@ -501,7 +516,19 @@ cpipe_cuda_chain* cpipe_cuda_chain_create(const cpipe_cuda_chain_config* cfg, in
     std::memcpy(c->color.neutral, cfg->as_shot_neutral, sizeof(c->color.neutral));
     std::memcpy(c->color.cm, cfg->colormatrix, sizeof(c->color.cm));
     c->denoise_mode = cfg->denoise_mode;
-    if (c->denoise_mode < 0 || c->denoise_mode > 1) return fail(CPIPE_UNSUPPORTED, c);
+    c->stop_after = cfg->stop_after;
+    if (c->denoise_mode < 0 || c->denoise_mode > 2) return fail(CPIPE_UNSUPPORTED, c);
+    if (c->stop_after < 0 || c->stop_after > 2 || (c->stop_after == 2 && c->denoise_mode == 0))
+        return fail(CPIPE_UNSUPPORTED, c);
+    if (c->denoise_mode == 2) {
+        c->sg = surrogate_new(cfg->surrogate_blob, cfg->surrogate_blob_size, &st);
+        if (!c->sg) return fail(st, c);
+        const float ab[2] = {cfg->noise_a, cfg->noise_b};
+        if (cudaMalloc(&c->d_ab, sizeof(ab)) != cudaSuccess) return fail(CPIPE_OOM, c);
+        if (cudaMemcpy(c->d_ab, ab, sizeof(ab), cudaMemcpyHostToDevice) != cudaSuccess)
+            return fail(CPIPE_INTERNAL_ERROR, c);
+        if (surrogate_reserve(c->sg, (long long)w * h) != cudaSuccess) return fail(CPIPE_OOM, c);
+    }
     c->tone.bm3d_strength = c->denoise_mode == 0 ? fminf(1.0F, fmaxf(0.0F, cfg->bm3d_sigma / 0.03F)) : 0.0F;
     if (c->denoise_mode == 1) {
         cpipe_Bm3dSpecParams sp = cfg->bm3d_spec;
@@ -535,6 +562,8 @@ void cpipe_cuda_chain_destroy(cpipe_cuda_chain* c) {
     if (c->graph) cudaGraphExecDestroy(c->graph);
     cudaFree(c->d_tables);
     cudaFree(c->d_denoise);
+    cudaFree(c->d_ab);
+    surrogate_free(c->sg);
     for (void* p : c->d_mid) cudaFree(p);
     for (void* p : c->d_io) cudaFree(p);
     delete c;
@@ -659,6 +688,43 @@ int cpipe_cuda_memcpy_h2d(void* dst, const void* src, size_t bytes) {
 }
 int cpipe_cuda_memcpy_d2h(void* dst, const void* src, size_t bytes) {
     return cuda_status(cudaMemcpy(dst, src, bytes, cudaMemcpyDeviceToHost), "d2h");
+}
+}  // extern "C"
+
+namespace {
+__global__ void count_nonfinite_kernel(const void* d, size_t n, int f16, unsigned long long* out) {
+    unsigned long long c = 0;
+    for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
+        const float v = f16 ? __half2float(static_cast<const __half*>(d)[i]) : static_cast<const float*>(d)[i];
+        c += isfinite(v) ? 0ULL : 1ULL;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) c += __shfl_xor_sync(0xFFFFFFFFU, c, off);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
+}
+}  // namespace
+
+extern "C" {
+
+int cpipe_cuda_count_nonfinite(const void* d, size_t count, int f16, uint64_t* out, void* stream) {
+    if (!d || !out) return CPIPE_BAD_INDEX;
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    unsigned long long* dc = nullptr;
+    int s = cuda_status(cudaMallocAsync(&dc, sizeof(*dc), st), "count alloc");
+    if (s != CPIPE_OK) return s;
+    unsigned long long h = 0;
+    cudaMemsetAsync(dc, 0, sizeof(*dc), st);
+    count_nonfinite_kernel<<<kSmCount * 4, 256, 0, st>>>(d, count, f16, dc);
+    s = cuda_status(cudaMemcpyAsync(&h, dc, sizeof(h), cudaMemcpyDeviceToHost, st), "count copy");
+    cudaFreeAsync(dc, st);
+    const int ss = cuda_status(cudaStreamSynchronize(st), "count sync");
+    *out = h;
+    return s != CPIPE_OK ? s : ss;
+}
+
+int cpipe_cuda_memcpy_d2d_async(void* dst, const void* src, size_t bytes, void* stream) {
+    return cuda_status(cudaMemcpyAsync(dst, src, bytes, cudaMemcpyDeviceToDevice, static_cast<cudaStream_t>(stream)),
+                       "d2d");
 }
 int cpipe_cuda_set_device(int device) { return cuda_status(cudaSetDevice(device), "set device"); }
 

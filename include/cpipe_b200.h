@@ -218,6 +218,9 @@ typedef struct {
     cpipe_Bm3dSpecParams bm3d_spec;
     const void* surrogate_blob;
     size_t surrogate_blob_size;
+    float noise_a, noise_b;             /* noise model var = a*x + b (the surrogate's noise-map input) */
+    int32_t stop_after;                 /* 0: whole chain; 1: output the colormatrix result (the
+                                           denoiser's input); 2: output the denoiser's result */
 } cpipe_cuda_chain_config;
 
 typedef struct cpipe_cuda_chain cpipe_cuda_chain;
@@ -235,12 +238,48 @@ int cpipe_cuda_chain_run_host(cpipe_cuda_chain* chain, const uint16_t* h_raw, vo
  * [2] the denoiser of denoise_mode 1 or 2 (0 in mode 0), [3] denoise_tone. */
 int cpipe_cuda_chain_set_profiling(cpipe_cuda_chain* chain, int enable);
 int cpipe_cuda_chain_profile(cpipe_cuda_chain* chain, double ms_per_stage[4], int* frames);
+/* Seeded synthetic raw frame on the device (uint16, width x height): linear
+ * gradients, `rects` (<= 64) rectangles of uniform reflectance, a zone plate,
+ * 2x2 CFA mosaic, Gaussian-form noise var = a*x + b, `bits`-bit values above
+ * `black`.  Counter-based (Philox4x32-10), so a seed gives the same frame on
+ * every launch.  No reference counterpart (training data and benchmarks). */
+int cpipe_cuda_scene_raw(void* d_out, int width, int height, uint64_t seed, int bits, int black, float noise_a,
+                         float noise_b, const uint8_t cfa[4], int rects, void* stream);
+
+/* ---------------------------------------------------------- learned surrogate */
+/* A residual convolutional denoiser that stands in for BM3D (weights:
+ * cpipe_SurrogateHeader + FP32 parameters, see cpipe_b200_params.h), with its
+ * own forward and training kernels.  No reference counterpart: the reference's
+ * AI denoise node is planned but not implemented.  Frames are dense RGBA
+ * device buffers [n][height][width][4] (binary16 when f16, training: binary16);
+ * noise_ab holds n host-side (a, b) pairs of the noise model var = a*x + b that
+ * the network's noise-map input is computed from. */
+typedef struct cpipe_surrogate cpipe_surrogate;
+size_t cpipe_surrogate_blob_size(void);
+cpipe_surrogate* cpipe_surrogate_create(const void* blob, size_t blob_size, int* status);
+void cpipe_surrogate_destroy(cpipe_surrogate* s);
+/* Current (trained) weights in the blob format. */
+int cpipe_surrogate_export(const cpipe_surrogate* s, void* blob, size_t blob_size);
+int cpipe_surrogate_denoise(cpipe_surrogate* s, const void* d_in, void* d_out, int n, int width, int height, int f16,
+                            const float* noise_ab, void* stream);
+/* One step on a batch: forward, mean-squared-error loss against the target,
+ * backward; with update != 0 also an Adam step (lr).  *loss (optional) gets
+ * the batch loss (the call then waits for the stream). */
+int cpipe_surrogate_train_step(cpipe_surrogate* s, const void* d_noisy, const void* d_target, const float* noise_ab,
+                               int n, int width, int height, float lr, int update, float* loss, void* stream);
+/* Gradients of the last train_step, in blob parameter order. */
+int cpipe_surrogate_gradients(const cpipe_surrogate* s, float* grad, size_t count);
+
 /* Device memory, streams and events for callers without their own CUDA runtime. */
 int cpipe_cuda_set_device(int device);
 int cpipe_cuda_device_alloc(size_t bytes, void** out);
 void cpipe_cuda_device_free(void* p);
 int cpipe_cuda_memcpy_h2d(void* dst, const void* src, size_t bytes);
 int cpipe_cuda_memcpy_d2h(void* dst, const void* src, size_t bytes);
+int cpipe_cuda_memcpy_d2d_async(void* dst, const void* src, size_t bytes, void* stream);
+/* Number of non-finite values among `count` binary16 (f16 != 0) or float32
+ * values on the device; waits for the stream. */
+int cpipe_cuda_count_nonfinite(const void* d, size_t count, int f16, uint64_t* out, void* stream);
 int cpipe_cuda_stream_create(void** out);
 void cpipe_cuda_stream_destroy(void* stream);
 int cpipe_cuda_stream_synchronize(void* stream);

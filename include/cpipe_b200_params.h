@@ -176,6 +176,25 @@ typedef struct {
     int32_t reserved;   /* 0 */
 } cpipe_Bm3dSpecParams;
 
+/* Learned surrogate denoiser weights (no reference counterpart: the
+ * reference's AI denoise node is planned but not implemented).  A residual
+ * network of `layers` 3x3 convolutions, zero padded, ReLU after every layer but
+ * the last; input = R, G, B and the noise map sigma/0.03 with
+ * sigma = sqrt(max(0, noise_b + noise_a * max(L, 0))), L = (R+G+B)/3; output =
+ * input RGB + the last layer's 3 channels.  The blob is this header followed,
+ * per layer l, by float weights[cout][cin][3][3] then float bias[cout]
+ * (cin = in_channels for l = 0 else channels; cout = out_channels for the last
+ * layer else channels), little endian. */
+typedef struct {
+    char magic[4];          /* "CPSN" */
+    uint32_t version;       /* 1 */
+    uint32_t layers;        /* 8 */
+    uint32_t channels;      /* 32 */
+    uint32_t in_channels;   /* 4 */
+    uint32_t out_channels;  /* 3 */
+    uint32_t reserved[2];   /* 0 */
+} cpipe_SurrogateHeader;
+
 #if defined(__cplusplus)
 #define CPIPE_STATIC_ASSERT static_assert
 #else
@@ -188,6 +207,7 @@ CPIPE_STATIC_ASSERT(sizeof(cpipe_GainMapDispatchPlane) == 72, "GainMapDispatchPl
 CPIPE_STATIC_ASSERT(sizeof(cpipe_Opcode3DispatchRecord) == 320, "Opcode3DispatchRecord layout");
 CPIPE_STATIC_ASSERT(sizeof(cpipe_Lut3dParamHeader) == 12, "Lut3dParamHeader layout");
 CPIPE_STATIC_ASSERT(sizeof(cpipe_Bm3dSpecParams) == 40, "Bm3dSpecParams layout");
+CPIPE_STATIC_ASSERT(sizeof(cpipe_SurrogateHeader) == 32, "SurrogateHeader layout");
 
 #ifdef __cplusplus
 } /* extern "C" */

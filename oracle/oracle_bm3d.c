@@ -34,7 +34,7 @@
  *    (1 when nothing is kept);
  *  - step 2: groups of the basic estimate and of the noisy image at the same
  *    positions; Wiener shrink W = B^2/(B^2+sigma^2) of the noisy coefficients,
- *    weight 1/(sigma^2*sum W^2) (1 when the sum is 0);
+ *    weight 1/(sigma^2*max(sum W^2, 1e-20)) (1 when the sum is 0);
  *  - aggregation: weight x 8x8 Kaiser window (beta) per block, numerator and
  *    denominator per channel; estimate = numerator / denominator;
  *  - alpha is copied; images smaller than 8x8, sigma <= 0 or a sigma whose
@@ -281,7 +281,7 @@ static void run_stage(const Geo* g, const double* noisy, const double* basic, co
                             gz[k] *= W;
                             sw2 += W * W;
                         }
-                        wgt = sw2 > 0.0 ? 1.0 / (s2 * sw2) : 1.0;
+                        wgt = sw2 > 0.0 ? 1.0 / (s2 * (sw2 > 1e-20 ? sw2 : 1e-20)) : 1.0;
                     }
                     haar(gz, N, 1);
                     for (int b = 0; b < N; ++b) {
