@@ -691,7 +691,8 @@ int cpipe_cuda_memcpy_d2h(void* dst, const void* src, size_t bytes) {
 }
 }  // extern "C"
 
-namespace {
+namespace cpb {
+namespace util {
 __global__ void count_nonfinite_kernel(const void* d, size_t n, int f16, unsigned long long* out) {
     unsigned long long c = 0;
     for (size_t i = (size_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (size_t)gridDim.x * blockDim.x) {
@@ -702,7 +703,8 @@ __global__ void count_nonfinite_kernel(const void* d, size_t n, int f16, unsigne
     for (int off = 16; off > 0; off >>= 1) c += __shfl_xor_sync(0xFFFFFFFFU, c, off);
     if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
 }
-}  // namespace
+}  // namespace util
+}  // namespace cpb
 
 extern "C" {
 
@@ -714,7 +716,7 @@ int cpipe_cuda_count_nonfinite(const void* d, size_t count, int f16, uint64_t* o
     if (s != CPIPE_OK) return s;
     unsigned long long h = 0;
     cudaMemsetAsync(dc, 0, sizeof(*dc), st);
-    count_nonfinite_kernel<<<kSmCount * 4, 256, 0, st>>>(d, count, f16, dc);
+    cpb::util::count_nonfinite_kernel<<<kSmCount * 4, 256, 0, st>>>(d, count, f16, dc);
     s = cuda_status(cudaMemcpyAsync(&h, dc, sizeof(h), cudaMemcpyDeviceToHost, st), "count copy");
     cudaFreeAsync(dc, st);
     const int ss = cuda_status(cudaStreamSynchronize(st), "count sync");
