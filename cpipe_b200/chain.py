@@ -285,8 +285,12 @@ def _main():
     args = ap.parse_args()
     L = A.lib()
     assert L.cpipe_cuda_device_count() > 0, "no CUDA device"
+    blob = None
+    if args.denoise == "surrogate":
+        from .surrogate import load_weights
+        blob = load_weights()
     cfg = ChainConfig.full_12mp(width=args.width, height=args.height, demosaic=args.demosaic, use_graph=False,
-                                denoise=args.denoise)
+                                denoise=args.denoise, surrogate_blob=blob)
     raw = cfg.make_raw()
     chain = Chain(cfg)
     d_raw, d_out = C.c_void_p(), C.c_void_p()
