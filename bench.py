@@ -1,12 +1,17 @@
-"""Benchmark: 12 MP ms/frame of the classic raw->linear chain on B200.
+"""Benchmark: 12 MP ms/frame of the raw->linear chain with the learned
+surrogate denoiser, against the same chain with the two-stage BM3D, on B200.
 
 One step = the fused chain (convert, black level, GainMap, RCD, OpcodeList3
-warp, WB, colormatrix, BM3D, guided, wavelet, filmic, 3D LUT) over one
+warp, WB, colormatrix, denoiser, guided, wavelet, filmic, 3D LUT) over one
 4032x3024 10-bit RGGB frame already resident in HBM.  Frames rotate through a
 ring of 8 raw inputs (195 MB) and 2 outputs (195 MB), so no step reads its
 input from L2.  Timing: CUDA events on the chain's stream around exactly K
 steps, bracketed by a barrier and a stream synchronize; max over ranks.  The
-`e2e` figure runs the same chain through the C-ABI host entry point
+same is measured for the BM3D chain (fewer steps; it is the slow arm) and for
+the chain with the reference's own denoise.bm3d computation (2x2 box blend).
+Quality: PSNR of the surrogate chain's output against the BM3D chain's output
+on the same frame (and of the two denoisers' outputs).  The `e2e` figure runs
+the surrogate chain through the C-ABI host entry point
 (cpipe_cuda_chain_run_host: pinned raw frame H2D, chain, RGBA16F D2H).
 
 Multi-GPU: frames are independent, so N GPUs run N replicas on their own
@@ -27,7 +32,7 @@ import time
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
-METRIC = "12MP ms/frame, classic raw->linear chain (parity form)"
+METRIC = "12MP ms/frame: surrogate vs plain BM3D chain on B200 at >=40 dB; % HBM roofline"
 BYTES_PER_PX = {"raw_to_rgba": 10, "warp_wb_cm": 16, "denoise_tone": 16}  # algorithmic HBM bytes
 KERNELS = ["raw_to_rgba", "warp_wb_cm", "denoise", "denoise_tone"]
 
@@ -168,6 +173,36 @@ def reference_arm(args):
     return 0
 
 
+SURROGATE_FLOP_PER_PX = 2 * 9 * (4 * 32 + 6 * 32 * 32 + 32 * 3)  # real channels, 8 layers
+HIDDEN_FLOP_PER_PX = 2 * 9 * 32 * 32
+
+
+def measured_bf16_tflops():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["bf16_tflops_sustained"]), "measured (sustained)"
+    except Exception:
+        return 1385.0, "fallback (sustained)"
+
+
+def traffic_surrogate_hidden(px):
+    """DRAM bytes per hidden-conv launch scaled from the committed ncu capture
+    (traffic grows with the pixel count), or None."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic_surrogate_conv.json")) as f:
+            t = json.load(f)
+        return int(t["dram_bytes_per_launch"] * px / t["pixels"])
+    except Exception:
+        return None
+
+
+def psnr(a, b):
+    import numpy as np
+    d = np.asarray(a, np.float64)[..., :3] - np.asarray(b, np.float64)[..., :3]
+    mse = float(np.mean(d * d))
+    return float("inf") if mse == 0.0 else 10.0 * np.log10(1.0 / mse)
+
+
 def b200_arm(args):
     import numpy as np
     rank, world, local = rank_env(args.gpus)
@@ -178,6 +213,7 @@ def b200_arm(args):
         torch.cuda.set_device(local)
         dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
     from cpipe_b200 import _abi as A
+    from cpipe_b200 import surrogate as S
     from cpipe_b200.chain import Chain, ChainConfig
     L = A.lib()
     assert L.cpipe_cuda_set_device(local) == 0, "no CUDA device"
@@ -188,7 +224,9 @@ def b200_arm(args):
             dist.barrier(device_ids=[local])
             torch.cuda.synchronize()
 
-    cfg = ChainConfig.full_12mp(seed=frame_seed(rank))
+    weights = S.load_weights()
+    base_cfg = dict(seed=frame_seed(rank), surrogate_blob=weights)
+    cfg = ChainConfig.full_12mp(denoise="surrogate", **base_cfg)
     w, h = cfg.width, cfg.height
     base = cfg.make_raw()
     ring = [np.ascontiguousarray(np.roll(base, (2 * k, 4 * k), axis=(0, 1))) for k in range(8)]
@@ -206,28 +244,22 @@ def b200_arm(args):
         d_out.append(p.value)
     stream = C.c_void_p()
     assert L.cpipe_cuda_stream_create(C.byref(stream)) == 0
-    chain = Chain(cfg)
     ev0, ev1 = C.c_void_p(), C.c_void_p()
     L.cpipe_cuda_event_create(C.byref(ev0))
     L.cpipe_cuda_event_create(C.byref(ev1))
 
-    for i in range(args.warmup):
-        chain.run(d_raw[i % 8], d_out[i % 2], stream)
-    L.cpipe_cuda_stream_synchronize(stream)
-    L.cpipe_cuda_chain_set_profiling(chain._h, 1)
-
-    with ClockSampler(local) as clocks:
-        # keep the GPU busy while the sampler starts, then time exactly K steps
-        for i in range(max(args.warmup, 3)):
+    def timed(chain, frames, warmup):
+        """warm-up, then exactly `frames` steps between events (stage events on)."""
+        for i in range(warmup):
             chain.run(d_raw[i % 8], d_out[i % 2], stream)
         L.cpipe_cuda_stream_synchronize(stream)
-        ms_k = (C.c_double * 4)()
-        nfr = C.c_int32()
-        L.cpipe_cuda_chain_profile(chain._h, ms_k, C.byref(nfr))  # discard the extra warm-up frames
+        L.cpipe_cuda_chain_set_profiling(chain._h, 1)
+        ms_k, nfr = (C.c_double * 4)(), C.c_int32()
+        L.cpipe_cuda_chain_profile(chain._h, ms_k, C.byref(nfr))
         barrier()
         L.cpipe_cuda_stream_synchronize(stream)
         L.cpipe_cuda_event_record(ev0, stream)
-        for i in range(args.steps):
+        for i in range(frames):
             chain.run(d_raw[i % 8], d_out[i % 2], stream)
         L.cpipe_cuda_event_record(ev1, stream)
         L.cpipe_cuda_stream_synchronize(stream)
@@ -235,16 +267,25 @@ def b200_arm(args):
         ms = C.c_float()
         L.cpipe_cuda_event_elapsed_ms(ev0, ev1, C.byref(ms))
         L.cpipe_cuda_chain_profile(chain._h, ms_k, C.byref(nfr))
-        # end-to-end through the host entry point: pinned frames in and out
         L.cpipe_cuda_chain_set_profiling(chain._h, 0)
+        stages = {k: ms_k[i] / max(1, nfr.value) for i, k in enumerate(KERNELS)}
+        return max_over_ranks(float(ms.value), dist, f"cuda:{local}"), stages
+
+    chain = Chain(cfg)
+    bm3d_chain = Chain(ChainConfig.full_12mp(denoise="bm3d", **base_cfg))
+    ref_chain = Chain(ChainConfig.full_12mp(**base_cfg))
+    bm3d_frames = max(3, min(args.steps, 10))
+    with ClockSampler(local) as clocks:
+        total_ms, stages = timed(chain, args.steps, max(args.warmup, 3))
+        bm3d_ms, bm3d_stages = timed(bm3d_chain, bm3d_frames, 3)
+        ref_ms, ref_stages = timed(ref_chain, args.steps, 3)
+        # end to end through the C-ABI host entry point: pinned frames in and out
         e2e_steps = max(3, min(args.steps, 20))
-        h_raw = C.c_void_p()
-        h_out = C.c_void_p()
+        h_raw, h_out = C.c_void_p(), C.c_void_p()
         assert L.cpipe_cuda_pinned_alloc(raw_bytes, C.byref(h_raw)) == 0
         assert L.cpipe_cuda_pinned_alloc(out_bytes, C.byref(h_out)) == 0
         C.memmove(h_raw, ring[0].ctypes.data, raw_bytes)
-        st = L.cpipe_cuda_chain_run_host(chain._h, h_raw, h_out, stream)
-        assert st == 0, st
+        assert L.cpipe_cuda_chain_run_host(chain._h, h_raw, h_out, stream) == 0
         barrier()
         t0 = time.perf_counter()
         for i in range(e2e_steps):
@@ -253,35 +294,76 @@ def b200_arm(args):
         barrier()
     clk = clocks.summary()
 
-    total_ms = max_over_ranks(float(ms.value), dist, f"cuda:{local}")
+    # quality: the surrogate chain against the BM3D chain on the same frame
+    outs = {}
+    for name, c in (("surrogate", chain), ("bm3d", bm3d_chain)):
+        c.run(d_raw[0], d_out[0], stream)
+        L.cpipe_cuda_stream_synchronize(stream)
+        arr = np.empty((h, w, 4), np.float16)
+        L.cpipe_cuda_memcpy_d2h(arr.ctypes.data, C.c_void_p(d_out[0]), out_bytes)
+        outs[name] = arr.astype(np.float32)
+    chain_psnr = psnr(outs["surrogate"], outs["bm3d"])
+    den = {}
+    for mode in ("surrogate", "bm3d"):
+        c = Chain(ChainConfig.full_12mp(denoise=mode, stop_after=2, **base_cfg))
+        den[mode] = c.run_host(ring[0]).astype(np.float32)
+        c.close()
+    den_psnr = psnr(den["surrogate"], den["bm3d"])
+    # per-kernel times of the denoiser on this frame's denoiser input
+    front = Chain(ChainConfig.full_12mp(stop_after=1, **base_cfg))
+    front.run(d_raw[0], d_out[0], stream)
+    L.cpipe_cuda_stream_synchronize(stream)
+    front.close()
+    sg = S.Surrogate(weights)
+    sg.profile(d_out[0], d_out[1], 1, w, h, [(cfg.noise_a, cfg.noise_b)], stream=stream)
+    layer_ms = sg.profile(d_out[0], d_out[1], 1, w, h, [(cfg.noise_a, cfg.noise_b)], stream=stream)
+    sg.close()
+
     e2e_ms = max_over_ranks(e2e_s * 1000.0, dist, f"cuda:{local}")
-    per_kernel = {k: ms_k[i] / max(1, nfr.value) for i, k in enumerate(KERNELS) if k != "denoise" or ms_k[i] > 0}
     value = whole_job_ms_per_frame(total_ms, args.steps, world)
-    dominant = max(per_kernel, key=per_kernel.get)
-    peak, peak_kind = measured_peak_gbs()
-    alg_bytes = BYTES_PER_PX[dominant] * w * h
-    achieved = alg_bytes / (per_kernel[dominant] * 1e-3) / 1e9
-    traffic = traffic_per_launch(dominant)
+    bm3d_value = whole_job_ms_per_frame(bm3d_ms, bm3d_frames, world)
+    ref_value = whole_job_ms_per_frame(ref_ms, args.steps, world)
+    hidden_ms = sum(layer_ms[2:8]) / 6.0
+    peak_tf, peak_kind = measured_bf16_tflops()
+    hidden_flop = HIDDEN_FLOP_PER_PX * w * h
+    achieved_tf = hidden_flop / (hidden_ms * 1e-3) / 1e12
+    peak_gbs, gbs_kind = measured_peak_gbs()
+    hbm = {k: {"ms": round(stages[k], 4),
+               "achieved_gbs": round(BYTES_PER_PX[k] * w * h / (stages[k] * 1e-3) / 1e9, 1),
+               "frac": round(BYTES_PER_PX[k] * w * h / (stages[k] * 1e-3) / 1e9 / peak_gbs, 4),
+               "traffic": traffic_per_launch(k)} for k in BYTES_PER_PX}
     line = {
         "metric": METRIC, "value": round(value, 4), "unit": "ms/frame", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": False,
-        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Philox scene)",
-        "config": {"workload": cfg.name, "frame": f"{w}x{h} RGGB 10-bit", "mode": "parity (RGBA16F between nodes)",
+        "scaling": "weak", "vs_baseline": None, "dtype": "bf16", "data": "synthetic (seeded Philox scene)",
+        "config": {"workload": cfg.name, "frame": f"{w}x{h} RGGB 10-bit",
+                   "denoiser": "learned surrogate: 8 3x3 conv layers, 32 channels, BF16, FP32 accumulation",
+                   "compared_with": "the same chain with two-stage BM3D (8x8 blocks, 16-block groups, 39x39 "
+                                    "search, step 3, hard threshold + Wiener), FP32",
                    "nodes": ["precision_convert", "blacklevel", "gainmap 17x13", "demosaic.rcd",
-                             "opcode_list_3 warp", "wb.dual_illuminant", "colormatrix", "bm3d", "guided r8",
+                             "opcode_list_3 warp", "wb.dual_illuminant", "colormatrix", "denoiser", "guided r8",
                              "wavelet", "filmic", "3d_lut 33^3"],
                    "l2": "inputs larger than L2: ring of 8 raw frames (195 MB) and 2 output frames",
                    "parallelism": f"replicas x{world}"},
-        "per_kernel_ms": {k: round(v, 4) for k, v in per_kernel.items()},
-        "roofline": {"bound": "hbm", "kernel": dominant, "achieved": round(achieved, 1), "peak": peak,
-                     "peak_kind": peak_kind, "unit": "GB/s", "frac": round(achieved / peak, 4),
-                     "algorithmic_bytes": alg_bytes, "traffic": traffic},
-        "chain_roofline": {"achieved": round(sum(BYTES_PER_PX.values()) * w * h / (total_ms / args.steps * 1e-3) / 1e9,
-                                             1), "unit": "GB/s", "bytes_per_px": sum(BYTES_PER_PX.values())},
-        "e2e": {"value": round(whole_job_ms_per_frame(e2e_ms, e2e_steps, world), 4), "unit": "ms/frame", "h2d_bytes_per_step": raw_bytes,
-                "d2h_bytes_per_step": out_bytes},
+        "per_stage_ms": {k: round(v, 4) for k, v in stages.items()},
+        "bm3d_chain": {"ms_per_frame": round(bm3d_value, 3), "frames": bm3d_frames,
+                       "per_stage_ms": {k: round(v, 4) for k, v in bm3d_stages.items()}},
+        "speedup_vs_bm3d_chain": round(bm3d_value / value, 2),
+        "psnr_vs_bm3d_chain_db": round(chain_psnr, 2),
+        "psnr_denoiser_vs_bm3d_db": round(den_psnr, 2),
+        "reference_computation_chain": {"ms_per_frame": round(ref_value, 4),
+                                        "note": "denoise.bm3d as the reference computes it (2x2 box blend)",
+                                        "per_stage_ms": {k: round(v, 4) for k, v in ref_stages.items()}},
+        "surrogate_layer_ms": [round(v, 4) for v in layer_ms],
+        "roofline": {"bound": "tensor", "kernel": "sg_conv_kernel<32,32> (hidden 3x3 conv layer)",
+                     "achieved": round(achieved_tf, 1), "peak": peak_tf, "peak_kind": peak_kind,
+                     "unit": "TFLOP/s", "frac": round(achieved_tf / peak_tf, 4),
+                     "algorithmic_flop": hidden_flop, "traffic": traffic_surrogate_hidden(w * h)},
+        "hbm_roofline": {"peak_gbs": peak_gbs, "peak_kind": gbs_kind, "kernels": hbm},
+        "e2e": {"value": round(whole_job_ms_per_frame(e2e_ms, e2e_steps, world), 4), "unit": "ms/frame",
+                "h2d_bytes_per_step": raw_bytes, "d2h_bytes_per_step": out_bytes},
         "clocks": clk,
-        "gpu_launches": 3 * args.steps,
+        "gpu_launches": 12 * args.steps,
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sample = ChainConfig.full_12mp(width=2016, height=1512, name="sample_2016x1512")
@@ -289,10 +371,12 @@ def b200_arm(args):
         os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
         v = cpu_chain_ms(sample, scale)
         line["cpu_baseline"] = {"value": round(v, 1), "unit": "ms/frame", "cores": os.cpu_count(), "kind": "port",
-                                "sample": "one 2016x1512 frame of the same chain, scaled x4 by area; C "
-                                          "restatement of the reference nodes (plain-C++ filters single-threaded "
-                                          "as in the reference, Halide restatements OpenMP over rows)"}
-    chain.close()
+                                "sample": "one 2016x1512 frame of the reference's chain (denoise.bm3d as the "
+                                          "reference computes it), scaled x4 by area; C restatement of the "
+                                          "reference nodes (plain-C++ filters single-threaded as in the "
+                                          "reference, Halide restatements OpenMP over rows)"}
+    for c in (chain, bm3d_chain, ref_chain):
+        c.close()
     if rank == 0:
         print(json.dumps(line), flush=True)
     if dist is not None:

@@ -557,7 +557,8 @@ static ConvArgs conv_args(const SurrogateNet* s, int l, const bf16* x, bf16* y, 
 
 // Forward through layers 0..6 (ReLU); a0 must hold the prepared input.
 // training: activations a1..a7 kept; else ping-pong in two buffers.
-static const bf16* forward_hidden(SurrogateNet* s, int n, int h, int w, bool training, cudaStream_t st) {
+static const bf16* forward_hidden(SurrogateNet* s, int n, int h, int w, bool training, cudaStream_t st,
+                                  cudaEvent_t* ev = nullptr) {
     const long long px = (long long)n * h * w;
     const long long tiles = (long long)n * ((h + kTileH - 1) / kTileH) * ((w + kTileW - 1) / kTileW);
     const bf16* cur = s->d_act;
@@ -567,6 +568,7 @@ static const bf16* forward_hidden(SurrogateNet* s, int n, int h, int w, bool tra
         const ConvArgs a = conv_args(s, l, cur, nxt, n, h, w);
         if (l == 0) conv<8, kCh, kEpiRelu, __half>(a, tiles, st);
         else conv<kCh, kCh, kEpiRelu, __half>(a, tiles, st);
+        if (ev) cudaEventRecord(ev[l + 2], st);
         cur = nxt;
     }
     return cur;
@@ -586,21 +588,31 @@ static cudaError_t upload_ab(SurrogateNet* s, const float* ab, int n, cudaStream
 
 cudaError_t surrogate_reserve(SurrogateNet* s, long long pixels) { return ensure_acts(s, pixels, false); }
 
-cudaError_t surrogate_infer(SurrogateNet* s, const void* in, void* out, int n, int h, int w, bool f16,
-                            const float* d_ab, cudaStream_t st) {
+// ev (optional): kLayers + 2 events recorded before the input preparation,
+// after it, and after each layer.
+static cudaError_t infer(SurrogateNet* s, const void* in, void* out, int n, int h, int w, bool f16,
+                         const float* d_ab, cudaStream_t st, cudaEvent_t* ev) {
     const long long px = (long long)n * h * w;
     cudaError_t e = ensure_acts(s, px, false);
     if (e != cudaSuccess) return e;
+    if (ev) cudaEventRecord(ev[0], st);
     if (f16) sg_prep_kernel<__half><<<(unsigned)((px + 255) / 256), 256, 0, st>>>(static_cast<const __half*>(in), s->d_act, d_ab, (long long)h * w, n);
     else sg_prep_kernel<float><<<(unsigned)((px + 255) / 256), 256, 0, st>>>(static_cast<const float*>(in), s->d_act, d_ab, (long long)h * w, n);
-    const bf16* a7 = forward_hidden(s, n, h, w, false, st);
+    if (ev) cudaEventRecord(ev[1], st);
+    const bf16* a7 = forward_hidden(s, n, h, w, false, st, ev);
     ConvArgs a = conv_args(s, kLayers - 1, a7, nullptr, n, h, w);
     a.rgba = in;
     a.out = out;
     const long long tiles = (long long)n * ((h + kTileH - 1) / kTileH) * ((w + kTileW - 1) / kTileW);
     if (f16) conv<kCh, 8, kEpiResidual, __half>(a, tiles, st);
     else conv<kCh, 8, kEpiResidual, float>(a, tiles, st);
+    if (ev) cudaEventRecord(ev[kLayers + 1], st);
     return cudaGetLastError();
+}
+
+cudaError_t surrogate_infer(SurrogateNet* s, const void* in, void* out, int n, int h, int w, bool f16,
+                            const float* d_ab, cudaStream_t st) {
+    return infer(s, in, out, n, h, w, f16, d_ab, st, nullptr);
 }
 
 SurrogateNet* surrogate_new(const void* blob, size_t size, int* status) {
@@ -699,6 +711,25 @@ int cpipe_surrogate_denoise(cpipe_surrogate* s, const void* d_in, void* d_out, i
     cudaError_t e = upload_ab(s->net, noise_ab, n, st);
     if (e == cudaSuccess) e = surrogate_infer(s->net, d_in, d_out, n, height, width, f16 != 0, s->net->d_ab, st);
     return cuda_status(e, "surrogate denoise");
+}
+
+int cpipe_surrogate_profile(cpipe_surrogate* s, const void* d_in, void* d_out, int n, int width, int height, int f16,
+                            const float* noise_ab, float ms[9], void* stream) {
+    if (!s || !d_in || !d_out || !noise_ab || !ms || n <= 0 || width <= 0 || height <= 0) return CPIPE_BAD_INDEX;
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaEvent_t ev[kLayers + 2] = {};
+    int status = CPIPE_OK;
+    for (auto& e : ev)
+        if (cudaEventCreate(&e) != cudaSuccess) status = CPIPE_INTERNAL_ERROR;
+    cudaError_t e = status == CPIPE_OK ? upload_ab(s->net, noise_ab, n, st) : cudaSuccess;
+    if (status == CPIPE_OK && e == cudaSuccess)
+        e = infer(s->net, d_in, d_out, n, height, width, f16 != 0, s->net->d_ab, st, ev);
+    if (status == CPIPE_OK && e == cudaSuccess) e = cudaEventSynchronize(ev[kLayers + 1]);
+    if (status == CPIPE_OK && e == cudaSuccess)
+        for (int k = 0; k <= kLayers; ++k) cudaEventElapsedTime(&ms[k], ev[k], ev[k + 1]);
+    for (auto& x : ev)
+        if (x) cudaEventDestroy(x);
+    return status != CPIPE_OK ? status : cuda_status(e, "surrogate profile");
 }
 
 int cpipe_surrogate_train_step(cpipe_surrogate* s, const void* d_noisy, const void* d_target, const float* noise_ab,

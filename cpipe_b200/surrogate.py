@@ -160,6 +160,15 @@ class Surrogate:
         if st:
             raise CpipeError(st, "surrogate_denoise " + A.lib().cpipe_cuda_last_error().decode())
 
+    def profile(self, d_in, d_out, n, width, height, noise_ab, f16=True, stream=None):
+        """Per-kernel times (ms) of one denoise: [input map, layer 0, ..., layer 7]."""
+        keep, p = _ab(noise_ab)
+        ms = (C.c_float * 9)()
+        st = A.lib().cpipe_surrogate_profile(self._h, d_in, d_out, n, width, height, int(f16), p, ms, stream)
+        if st:
+            raise CpipeError(st, "surrogate_profile " + A.lib().cpipe_cuda_last_error().decode())
+        return list(ms)
+
     def train_step(self, d_noisy, d_target, noise_ab, n, width, height, lr, update=True, want_loss=True,
                    stream=None):
         keep, p = _ab(noise_ab)

@@ -262,6 +262,10 @@ void cpipe_surrogate_destroy(cpipe_surrogate* s);
 int cpipe_surrogate_export(const cpipe_surrogate* s, void* blob, size_t blob_size);
 int cpipe_surrogate_denoise(cpipe_surrogate* s, const void* d_in, void* d_out, int n, int width, int height, int f16,
                             const float* noise_ab, void* stream);
+/* One denoise with CUDA events between its kernels: ms[0] the input map,
+ * ms[1 + l] layer l (l = 0..7).  Waits for the stream. */
+int cpipe_surrogate_profile(cpipe_surrogate* s, const void* d_in, void* d_out, int n, int width, int height, int f16,
+                            const float* noise_ab, float ms[9], void* stream);
 /* One step on a batch: forward, mean-squared-error loss against the target,
  * backward; with update != 0 also an Adam step (lr).  *loss (optional) gets
  * the batch loss (the call then waits for the stream). */
