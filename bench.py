@@ -293,6 +293,7 @@ def b200_arm(args):
         e2e_s = time.perf_counter() - t0
         barrier()
     clk = clocks.summary()
+    spot_frames, spot_fallbacks, spot_worst = chain.denoise_stats()
 
     # quality: the surrogate chain against the BM3D chain on the same frame
     outs = {}
@@ -337,7 +338,8 @@ def b200_arm(args):
         "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "bf16", "data": "synthetic (seeded Philox scene)",
         "config": {"workload": cfg.name, "frame": f"{w}x{h} RGGB 10-bit",
-                   "denoiser": "learned surrogate: 8 3x3 conv layers, 32 channels, BF16, FP32 accumulation",
+                   "denoiser": "learned surrogate: 8 3x3 conv layers, 32 channels, BF16, FP32 accumulation; "
+                               "per frame BM3D spot check on 16 256x256 tiles, BM3D fallback below 40 dB",
                    "compared_with": "the same chain with two-stage BM3D (8x8 blocks, 16-block groups, 39x39 "
                                     "search, step 3, hard threshold + Wiener), FP32",
                    "nodes": ["precision_convert", "blacklevel", "gainmap 17x13", "demosaic.rcd",
@@ -351,6 +353,9 @@ def b200_arm(args):
         "speedup_vs_bm3d_chain": round(bm3d_value / value, 2),
         "psnr_vs_bm3d_chain_db": round(chain_psnr, 2),
         "psnr_denoiser_vs_bm3d_db": round(den_psnr, 2),
+        "spot_check": {"tiles_per_frame": cfg.spot_tiles, "tile": "256x256", "min_psnr_db": cfg.spot_min_psnr_db,
+                       "frames": spot_frames, "fallbacks_to_bm3d": spot_fallbacks,
+                       "worst_tile_psnr_db": round(spot_worst, 2)},
         "reference_computation_chain": {"ms_per_frame": round(ref_value, 4),
                                         "note": "denoise.bm3d as the reference computes it (2x2 box blend)",
                                         "per_stage_ms": {k: round(v, 4) for k, v in ref_stages.items()}},
@@ -363,7 +368,7 @@ def b200_arm(args):
         "e2e": {"value": round(whole_job_ms_per_frame(e2e_ms, e2e_steps, world), 4), "unit": "ms/frame",
                 "h2d_bytes_per_step": raw_bytes, "d2h_bytes_per_step": out_bytes},
         "clocks": clk,
-        "gpu_launches": 12 * args.steps,
+        "gpu_launches": 65 * args.steps,  # K1, K2, K3, 9 denoiser, 3 spot check, 2 x 25 BM3D (tiles; gated fallback)
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sample = ChainConfig.full_12mp(width=2016, height=1512, name="sample_2016x1512")

@@ -121,7 +121,8 @@ class ChainConfig(C.Structure):
                 ("filmic", FilmicRgbParams), ("lut_blob", C.c_void_p), ("lut_blob_size", C.c_size_t),
                 ("plain_f32", C.c_int32), ("use_graph", C.c_int32), ("denoise_mode", C.c_int32),
                 ("bm3d_spec", Bm3dSpecParams), ("surrogate_blob", C.c_void_p), ("surrogate_blob_size", C.c_size_t),
-                ("noise_a", C.c_float), ("noise_b", C.c_float), ("stop_after", C.c_int32)]
+                ("noise_a", C.c_float), ("noise_b", C.c_float), ("stop_after", C.c_int32),
+                ("spot_tiles", C.c_int32), ("spot_min_psnr_db", C.c_float)]
 
 
 MAIN_ENTRY = C.CFUNCTYPE(C.c_int, C.c_char_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p)
@@ -172,7 +173,7 @@ EXPORTS = [
     "cpipe_b200_host_last_error",
     "cpipe_cuda_chain_create", "cpipe_cuda_chain_destroy", "cpipe_cuda_chain_output_bytes", "cpipe_cuda_chain_run",
     "cpipe_cuda_chain_run_host", "cpipe_cuda_pinned_alloc", "cpipe_cuda_pinned_free",
-    "cpipe_cuda_chain_set_profiling", "cpipe_cuda_chain_profile", "cpipe_cuda_set_device", "cpipe_cuda_device_alloc",
+    "cpipe_cuda_chain_set_profiling", "cpipe_cuda_chain_profile", "cpipe_cuda_chain_denoise_stats", "cpipe_cuda_set_device", "cpipe_cuda_device_alloc",
     "cpipe_cuda_device_free", "cpipe_cuda_memcpy_h2d", "cpipe_cuda_memcpy_d2h", "cpipe_cuda_memcpy_d2d_async", "cpipe_cuda_count_nonfinite",
     "cpipe_cuda_stream_create",
     "cpipe_cuda_stream_destroy", "cpipe_cuda_stream_synchronize", "cpipe_cuda_event_create",
@@ -232,6 +233,7 @@ def lib():
         "cpipe_cuda_pinned_alloc": (i32, [sz, C.POINTER(vp)]), "cpipe_cuda_pinned_free": (None, [vp]),
         "cpipe_cuda_chain_set_profiling": (i32, [vp, i32]),
         "cpipe_cuda_chain_profile": (i32, [vp, C.POINTER(C.c_double), C.POINTER(i32)]),
+        "cpipe_cuda_chain_denoise_stats": (i32, [vp, C.POINTER(u32), C.POINTER(u32), C.POINTER(C.c_float)]),
         "cpipe_cuda_set_device": (i32, [i32]), "cpipe_cuda_device_alloc": (i32, [sz, C.POINTER(vp)]),
         "cpipe_cuda_device_free": (None, [vp]), "cpipe_cuda_memcpy_h2d": (i32, [vp, vp, sz]),
         "cpipe_cuda_memcpy_d2h": (i32, [vp, vp, sz]), "cpipe_cuda_memcpy_d2d_async": (i32, [vp, vp, sz, vp]),

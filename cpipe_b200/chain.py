@@ -85,6 +85,8 @@ class ChainConfig:
     bm3d_stages: int = 2
     surrogate_blob: bytes = None   # trained network (cpipe_b200.surrogate) for denoise="surrogate"
     stop_after: int = 0            # 1: output the denoiser's input; 2: the denoiser's output
+    spot_tiles: int = 16           # surrogate spot check: BM3D on this many 256x256 tiles per frame
+    spot_min_psnr_db: float = 40.0  # ... and BM3D for the whole frame when a tile is below this
 
     # ------------------------------------------------------------ workloads
     @classmethod
@@ -227,6 +229,8 @@ class ChainConfig:
             cfg.surrogate_blob, cfg.surrogate_blob_size = ptr(bytes(self.surrogate_blob))
         cfg.noise_a, cfg.noise_b = self.noise_a, self.noise_b
         cfg.stop_after = int(self.stop_after)
+        cfg.spot_tiles = int(self.spot_tiles)
+        cfg.spot_min_psnr_db = float(self.spot_min_psnr_db)
         return cfg, keep
 
 
@@ -260,6 +264,14 @@ class Chain:
         st = A.lib().cpipe_cuda_chain_run(self._h, d_raw, d_out, stream)
         if st:
             raise CpipeError(st, "chain_run " + A.lib().cpipe_cuda_last_error().decode())
+
+    def denoise_stats(self):
+        """(frames checked, frames that fell back to BM3D, worst tile PSNR dB)."""
+        f, b, p = C.c_uint32(), C.c_uint32(), C.c_float()
+        st = A.lib().cpipe_cuda_chain_denoise_stats(self._h, C.byref(f), C.byref(b), C.byref(p))
+        if st:
+            raise CpipeError(st, "chain_denoise_stats")
+        return f.value, b.value, p.value
 
     def run_host(self, raw, out=None, stream=None):
         raw = np.ascontiguousarray(raw, dtype=np.uint16)

@@ -88,10 +88,14 @@ __device__ __forceinline__ uint8_t quantise(float l) {
 }
 
 // ------------------------------------------------------------------- prep
+// gate (optional): the kernels of a gated run return at once unless *gate != 0.
+__device__ __forceinline__ bool gated_off(const int* gate) { return gate != nullptr && *gate == 0; }
+
 template <class T>
-__global__ void bm3d_prep_kernel(Img in, float* __restrict__ yuv, uint8_t* __restrict__ q, long long npx) {
+__global__ void bm3d_prep_kernel(Img in, float* __restrict__ yuv, uint8_t* __restrict__ q, long long npx,
+                                 const int* gate) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-    if (x >= in.w) return;
+    if (x >= in.w || gated_off(gate)) return;
     const Rgba p = load_rgba(px<const T>(in, x, y));
     const float s = (p.r + p.g) + p.b;
     const long long o = (long long)y * in.w + x;
@@ -103,23 +107,26 @@ __global__ void bm3d_prep_kernel(Img in, float* __restrict__ yuv, uint8_t* __res
 
 // ------------------------------------------------------------------ match
 struct MatchArgs {
-    int w, h, nrx, nry, nstep, R, ns, n2, wpr, rows;
+    int w, h, nrx, nry, nstep, R, ns, n2, wpr, rows;  // h: one image's height (blockIdx.z = image)
     uint32_t dthr;
     const uint8_t* q;
     uint32_t* list;
     uint8_t* cnt;
+    const int* gate;
 };
 
 constexpr int kMatchTile = 16;  // reference blocks per CTA edge (one thread each)
 
 __global__ void __launch_bounds__(256) bm3d_match_kernel(MatchArgs a) {
     extern __shared__ uint32_t s_w[];
+    if (gated_off(a.gate)) return;
+    const int img = blockIdx.z, row0 = img * a.h;  // images are stacked in rows
     const int i0 = blockIdx.x * kMatchTile, j0 = blockIdx.y * kMatchTile;
     const int iL = min(i0 + kMatchTile - 1, a.nrx - 1), jL = min(j0 + kMatchTile - 1, a.nry - 1);
     const int rx0 = max(0, refpos(i0, a.w, a.nstep) - a.R);
     const int rx1 = min(a.w, refpos(iL, a.w, a.nstep) + a.R + 8);
-    const int ry0 = max(0, refpos(j0, a.h, a.nstep) - a.R);
-    const int ry1 = min(a.h, refpos(jL, a.h, a.nstep) + a.R + 8);
+    const int ry0 = row0 + max(0, refpos(j0, a.h, a.nstep) - a.R);
+    const int ry1 = row0 + min(a.h, refpos(jL, a.h, a.nstep) + a.R + 8);
     const int RW = rx1 - rx0, RH = ry1 - ry0;
     const int plane = a.rows * a.wpr;  // words per shifted copy
     // Copy s, row r, word k holds region bytes 4k+s .. 4k+s+3 (little endian).
@@ -139,7 +146,7 @@ __global__ void __launch_bounds__(256) bm3d_match_kernel(MatchArgs a) {
     __syncthreads();
     const int i = i0 + (int)(threadIdx.x % kMatchTile), j = j0 + (int)(threadIdx.x / kMatchTile);
     if (i >= a.nrx || j >= a.nry) return;
-    const int x = refpos(i, a.w, a.nstep), y = refpos(j, a.h, a.nstep);
+    const int x = refpos(i, a.w, a.nstep), y = row0 + refpos(j, a.h, a.nstep);
     uint32_t rw[16];
     {
         const int c = x - rx0;
@@ -153,7 +160,7 @@ __global__ void __launch_bounds__(256) bm3d_match_kernel(MatchArgs a) {
     uint32_t keys[15];
 #pragma unroll
     for (int m = 0; m < 15; ++m) keys[m] = 0xFFFFFFFFU;
-    const int ylo = max(0, y - a.R), yhi = min(a.h - 8, y + a.R);
+    const int ylo = max(row0, y - a.R), yhi = min(row0 + a.h - 8, y + a.R);
     const int xlo = max(0, x - a.R), xhi = min(a.w - 8, x + a.R);
     if (a.n2 > 1) {
         for (int yy = ylo; yy <= yhi; ++yy) {
@@ -184,7 +191,7 @@ __global__ void __launch_bounds__(256) bm3d_match_kernel(MatchArgs a) {
             }
         }
     }
-    const long long ref = (long long)j * a.nrx + i;
+    const long long ref = ((long long)img * a.nry + j) * a.nrx + i;
     uint32_t* out = a.list + ref * 16;
     out[0] = ((uint32_t)y << 16) | (uint32_t)x;
     int n = 1;
@@ -210,6 +217,7 @@ struct FilterArgs {
     const float* noisy;
     const float* basic;
     float* acc;  // num of channel c at c*npx, den at (3+c)*npx
+    const int* gate;
     float kaiser[64];
 };
 
@@ -284,15 +292,15 @@ __device__ __forceinline__ void forward3d(const float* img, int fw, int bx, int 
 template <int STAGE>
 __global__ void __launch_bounds__(256, 2) bm3d_filter_kernel(FilterArgs a, int phx, int phy) {
     extern __shared__ float sm[];
-    const int c = blockIdx.z;
+    const int c = blockIdx.z % 3, img = blockIdx.z / 3, row0 = img * a.h;  // h: one image's height
     const int tx = blockIdx.x * a.phases + phx, ty = blockIdx.y * a.phases + phy;
-    if (tx >= a.ntx || ty >= a.nty) return;
+    if (tx >= a.ntx || ty >= a.nty || gated_off(a.gate)) return;
     const int i0 = tx * kRefTile, j0 = ty * kRefTile;
     const int i1 = min(i0 + kRefTile, a.nrx), j1 = min(j0 + kRefTile, a.nry);
     const int fx0 = max(0, refpos(i0, a.w, a.nstep) - a.R);
     const int fx1 = min(a.w, refpos(i1 - 1, a.w, a.nstep) + a.R + 8);
-    const int fy0 = max(0, refpos(j0, a.h, a.nstep) - a.R);
-    const int fy1 = min(a.h, refpos(j1 - 1, a.h, a.nstep) + a.R + 8);
+    const int fy0 = row0 + max(0, refpos(j0, a.h, a.nstep) - a.R);
+    const int fy1 = row0 + min(a.h, refpos(j1 - 1, a.h, a.nstep) + a.R + 8);
     const int fw = fx1 - fx0, fn = fw * (fy1 - fy0);
     const int FN = a.fw * a.fw;
     float* s_num = sm;
@@ -318,7 +326,7 @@ __global__ void __launch_bounds__(256, 2) bm3d_filter_kernel(FilterArgs a, int p
     float* buf = s_buf + warp * kWarpBuf;
     const int nti = i1 - i0, nref = nti * (j1 - j0);
     for (int k = warp; k < nref; k += kFilterWarps) {
-        const long long ref = (long long)(j0 + k / nti) * a.nrx + i0 + k % nti;
+        const long long ref = ((long long)img * a.nry + j0 + k / nti) * a.nrx + i0 + k % nti;
         const int cnt = a.cnt[ref];
         const int N = cnt >= 16 ? 16 : cnt >= 8 ? 8 : cnt >= 4 ? 4 : cnt >= 2 ? 2 : 1;
         const bool act = b < N;
@@ -405,9 +413,9 @@ __global__ void __launch_bounds__(256, 2) bm3d_filter_kernel(FilterArgs a, int p
 
 // --------------------------------------------------------- basic / final
 __global__ void bm3d_basic_kernel(const float* __restrict__ acc, float* __restrict__ basic, uint8_t* __restrict__ q,
-                                  long long npx) {
+                                  long long npx, const int* gate) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= npx) return;
+    if (i >= npx || gated_off(gate)) return;
     float y = 0.0F;
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -419,9 +427,9 @@ __global__ void bm3d_basic_kernel(const float* __restrict__ acc, float* __restri
 }
 
 template <class T>
-__global__ void bm3d_final_kernel(const float* __restrict__ acc, Img in, Img out, long long npx) {
+__global__ void bm3d_final_kernel(const float* __restrict__ acc, Img in, Img out, long long npx, const int* gate) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-    if (x >= in.w) return;
+    if (x >= in.w || gated_off(gate)) return;
     const long long i = (long long)y * in.w + x;
     const float Y = acc[i] / acc[3 * npx + i];
     const float U = acc[npx + i] / acc[4 * npx + i];
@@ -429,6 +437,12 @@ __global__ void bm3d_final_kernel(const float* __restrict__ acc, Img in, Img out
     const float yy = Y * kInvS3, uu = U * kInvS2, vv = V * kInvS6;
     const Rgba o{(yy + uu) + vv, yy - 2.0F * vv, (yy - uu) + vv, 0.0F};
     store_rgb_keep_alpha(px<T>(out, x, y), o, px<const T>(in, x, y));
+}
+
+__global__ void bm3d_zero_kernel(float* __restrict__ p, long long n, const int* gate) {
+    if (gated_off(gate)) return;
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        p[i] = 0.0F;
 }
 
 double bessel_i0(double x) {
@@ -458,7 +472,7 @@ size_t match_smem(const Bm3dPlan& p) { return sizeof(uint32_t) * 4 * (size_t)p.m
 
 }  // namespace
 
-int bm3d_plan(const cpipe_Bm3dSpecParams* p, int w, int h, Bm3dPlan* out) {
+int bm3d_plan(const cpipe_Bm3dSpecParams* p, int w, int h, Bm3dPlan* out, int batch) {
     if (p == nullptr || out == nullptr) return CPIPE_BAD_INDEX;
     const int n2 = p->n2;
     if (!(n2 == 1 || n2 == 2 || n2 == 4 || n2 == 8 || n2 == 16)) return CPIPE_BAD_INDEX;
@@ -468,11 +482,12 @@ int bm3d_plan(const cpipe_Bm3dSpecParams* p, int w, int h, Bm3dPlan* out) {
     if (!(p->tau_match2 >= 0.0F && p->tau_match2 <= 16000.0F)) return CPIPE_BAD_INDEX;
     if (p->stages != 1 && p->stages != 2) return CPIPE_BAD_INDEX;
     if (!(p->lambda3d >= 0.0F) || !(p->kaiser_beta >= 0.0F)) return CPIPE_BAD_INDEX;
-    if (w <= 0 || h <= 0 || w > 65535 || h > 65535) return CPIPE_BAD_INDEX;
+    if (w <= 0 || h <= 0 || batch < 1 || w > 65535 || (long long)h * batch > 65535) return CPIPE_BAD_INDEX;
     Bm3dPlan& q = *out;
     q = Bm3dPlan{};
     q.w = w;
     q.h = h;
+    q.batch = batch;
     q.ns = p->ns;
     q.R = (p->ns - 1) / 2;
     q.n2 = n2;
@@ -502,7 +517,7 @@ int bm3d_plan(const cpipe_Bm3dSpecParams* p, int w, int h, Bm3dPlan* out) {
     q.nty = (q.nry + kRefTile - 1) / kRefTile;
     q.mwin = (kMatchTile - 1) * q.nstep + 2 * q.R + 8;
     q.mwpr = (q.mwin + 3) / 4 + 1;
-    const size_t npx = (size_t)w * h, nref = (size_t)q.nrx * q.nry;
+    const size_t npx = (size_t)w * h * batch, nref = (size_t)q.nrx * q.nry * batch;
     size_t o = 0;
     q.off_yuv = o;
     o = align256(o + 3 * npx * sizeof(float));
@@ -534,7 +549,8 @@ cudaError_t bm3d_setup(const Bm3dPlan& p) {
 }
 
 cudaError_t bm3d_run(const Bm3dPlan& p, const Img& in, const Img& out, bool f16, void* scratch, cudaStream_t st,
-                     bool setup) {
+                     bool setup, const int* gate) {
+    if (p.copy && gate) return cudaSuccess;  // a gated run leaves the output alone
     if (p.copy) {
         const int elem = f16 ? 2 : 4;
         return launch_copy(in.data, in.row_stride * elem, out.data, out.row_stride * elem, (long long)in.w * 4 * elem,
@@ -547,17 +563,17 @@ cudaError_t bm3d_run(const Bm3dPlan& p, const Img& in, const Img& out, bool f16,
     uint8_t* q = reinterpret_cast<uint8_t*>(base + p.off_q);
     uint32_t* list = reinterpret_cast<uint32_t*>(base + p.off_list);
     uint8_t* cnt = reinterpret_cast<uint8_t*>(base + p.off_cnt);
-    const long long npx = (long long)p.w * p.h;
+    const long long npx = (long long)p.w * p.h * p.batch;
     cudaError_t e;
     if (setup && (e = bm3d_setup(p)) != cudaSuccess) return e;
     const size_t ms = match_smem(p), fs1 = filter_smem(p, 1), fs2 = filter_smem(p, 2);
 
-    const dim3 pgrid((p.w + 255) / 256, p.h);
-    if (f16) bm3d_prep_kernel<__half><<<pgrid, 256, 0, st>>>(in, yuv, q, npx);
-    else bm3d_prep_kernel<float><<<pgrid, 256, 0, st>>>(in, yuv, q, npx);
+    const dim3 pgrid((p.w + 255) / 256, p.h * p.batch);
+    if (f16) bm3d_prep_kernel<__half><<<pgrid, 256, 0, st>>>(in, yuv, q, npx, gate);
+    else bm3d_prep_kernel<float><<<pgrid, 256, 0, st>>>(in, yuv, q, npx, gate);
 
-    MatchArgs ma{p.w, p.h, p.nrx, p.nry, p.nstep, p.R, p.ns, p.n2, p.mwpr, p.mwin, p.dthr[0], q, list, cnt};
-    const dim3 mgrid((p.nrx + kMatchTile - 1) / kMatchTile, (p.nry + kMatchTile - 1) / kMatchTile);
+    MatchArgs ma{p.w, p.h, p.nrx, p.nry, p.nstep, p.R, p.ns, p.n2, p.mwpr, p.mwin, p.dthr[0], q, list, cnt, gate};
+    const dim3 mgrid((p.nrx + kMatchTile - 1) / kMatchTile, (p.nry + kMatchTile - 1) / kMatchTile, p.batch);
     FilterArgs fa{};
     fa.w = p.w;
     fa.h = p.h;
@@ -577,11 +593,12 @@ cudaError_t bm3d_run(const Bm3dPlan& p, const Img& in, const Img& out, bool f16,
     fa.noisy = yuv;
     fa.basic = basic;
     fa.acc = acc;
+    fa.gate = gate;
     for (int i = 0; i < 64; ++i) fa.kaiser[i] = p.kaiser[i];
-    const dim3 fgrid((p.ntx + p.phases - 1) / p.phases, (p.nty + p.phases - 1) / p.phases, 3);
+    const dim3 fgrid((p.ntx + p.phases - 1) / p.phases, (p.nty + p.phases - 1) / p.phases, 3 * p.batch);
 
     for (int stage = 1; stage <= p.stages; ++stage) {
-        if ((e = cudaMemsetAsync(acc, 0, 6 * (size_t)npx * sizeof(float), st)) != cudaSuccess) return e;
+        bm3d_zero_kernel<<<kSmCount * 8, 256, 0, st>>>(acc, 6 * npx, gate);
         ma.dthr = p.dthr[stage - 1];
         bm3d_match_kernel<<<mgrid, kMatchTile * kMatchTile, ms, st>>>(ma);
         for (int py = 0; py < p.phases; ++py)
@@ -590,10 +607,10 @@ cudaError_t bm3d_run(const Bm3dPlan& p, const Img& in, const Img& out, bool f16,
                 else bm3d_filter_kernel<2><<<fgrid, 32 * kFilterWarps, fs2, st>>>(fa, pxh, py);
             }
         if (stage == 1 && p.stages == 2)
-            bm3d_basic_kernel<<<(unsigned)((npx + 255) / 256), 256, 0, st>>>(acc, basic, q, npx);
+            bm3d_basic_kernel<<<(unsigned)((npx + 255) / 256), 256, 0, st>>>(acc, basic, q, npx, gate);
     }
-    if (f16) bm3d_final_kernel<__half><<<pgrid, 256, 0, st>>>(acc, in, out, npx);
-    else bm3d_final_kernel<float><<<pgrid, 256, 0, st>>>(acc, in, out, npx);
+    if (f16) bm3d_final_kernel<__half><<<pgrid, 256, 0, st>>>(acc, in, out, npx, gate);
+    else bm3d_final_kernel<float><<<pgrid, 256, 0, st>>>(acc, in, out, npx, gate);
     return cudaGetLastError();
 }
 

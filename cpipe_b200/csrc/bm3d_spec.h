@@ -12,7 +12,8 @@
 namespace cpb {
 
 struct Bm3dPlan {
-    int w = 0, h = 0;
+    int w = 0, h = 0;     // one image (a batch stacks `batch` images in rows)
+    int batch = 1;
     int nrx = 0, nry = 0;  // reference blocks per axis
     int ns = 0, R = 0, n2 = 0, nstep = 0, stages = 0;
     float sigma = 0.0F, sigma2 = 0.0F, thr = 0.0F;
@@ -27,17 +28,20 @@ struct Bm3dPlan {
 };
 
 // Validates the parameters (CPIPE_BAD_INDEX when out of range) and sizes the
-// scratch buffer for a w x h frame.
-int bm3d_plan(const cpipe_Bm3dSpecParams* p, int w, int h, Bm3dPlan* out);
+// scratch buffer for `batch` w x h images stacked in rows (batch * h <= 65535);
+// each image is denoised on its own (search windows stay inside it).
+int bm3d_plan(const cpipe_Bm3dSpecParams* p, int w, int h, Bm3dPlan* out, int batch = 1);
 
 // Sets the kernels' shared-memory limits for the plan (host-side; call
 // before capturing bm3d_run into a graph).
 cudaError_t bm3d_setup(const Bm3dPlan& plan);
 
-// RGBA in -> RGBA out (both binary16 when f16, else float32; alpha copied).
-// scratch: plan.bytes of device memory, 256-byte aligned.  setup = true runs
-// bm3d_setup first.
+// RGBA in -> RGBA out (both binary16 when f16, else float32; alpha copied);
+// for a batch, `in` and `out` span all batch * h rows.  scratch: plan.bytes of
+// device memory, 256-byte aligned.  setup = true runs bm3d_setup first.  gate
+// (optional device int): every kernel returns at once while *gate == 0, so
+// the run can sit in a graph and happen only when a device-side test asks.
 cudaError_t bm3d_run(const Bm3dPlan& plan, const Img& in, const Img& out, bool f16, void* scratch,
-                     cudaStream_t stream, bool setup = true);
+                     cudaStream_t stream, bool setup = true, const int* gate = nullptr);
 
 }  // namespace cpb

@@ -15,6 +15,8 @@
 // RGBA nodes; none in the FP32 plain form), so the fused result equals running
 // the nodes one by one.  OpcodeList3 lists other than a single WarpRectilinear
 // run through the per-node OpcodeList3 path between K1 and a WB+colormatrix K2.
+#include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <vector>
 
@@ -315,6 +317,60 @@ size_t denoise_tone_smem() {
 
 using namespace cpb;
 
+namespace cpb {
+struct SpotOrigins {
+    int x[16], y[16];
+};
+struct SpotStats {
+    unsigned frames, fallbacks;
+    float worst_mse;
+};
+namespace spot {
+// tiles of src at the origins -> dense [n][edge][edge][4]
+template <class T>
+__global__ void gather_kernel(Img src, T* __restrict__ dst, int edge, SpotOrigins o) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, t = blockIdx.z;
+    if (x >= edge) return;
+    const T* s = px<const T>(src, o.x[t] + x, o.y[t] + y);
+    T* d = dst + (((size_t)t * edge + y) * edge + x) * 4;
+    store_rgba(d, load_rgba(s));
+}
+// per tile: mean squared RGB difference between the frame (at the origin) and the reference tile
+template <class T>
+__global__ void mse_kernel(Img den, const T* __restrict__ ref, int edge, SpotOrigins o, float* __restrict__ mse) {
+    const int t = blockIdx.x;
+    __shared__ float part[32];
+    float acc = 0.0F;
+    for (int i = threadIdx.x; i < edge * edge; i += blockDim.x) {
+        const int y = i / edge, x = i - y * edge;
+        const Rgba a = load_rgba(px<const T>(den, o.x[t] + x, o.y[t] + y));
+        const Rgba b = load_rgba(ref + (((size_t)t * edge + y) * edge + x) * 4);
+        const float dr = a.r - b.r, dg = a.g - b.g, db = a.b - b.b;
+        acc += (dr * dr + dg * dg) + db * db;
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFU, acc, off);
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+    __syncthreads();
+    if (threadIdx.x < 32) {
+        acc = threadIdx.x < blockDim.x / 32 ? part[threadIdx.x] : 0.0F;
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFU, acc, off);
+        if (threadIdx.x == 0) mse[t] = acc / (3.0F * (float)(edge * edge));
+    }
+}
+__global__ void decide_kernel(const float* __restrict__ mse, int n, float mse_max, int* gate, SpotStats* stats) {
+    float worst = 0.0F;
+    for (int t = 0; t < n; ++t) worst = fmaxf(worst, mse[t]);
+    const int fall = !(worst <= mse_max);  // a non-finite tile error also falls back
+    *gate = fall;
+    stats->frames += 1U;
+    stats->fallbacks += (unsigned)fall;
+    stats->worst_mse = fmaxf(stats->worst_mse, worst);
+}
+}  // namespace spot
+}  // namespace cpb
+
 struct cpipe_cuda_chain {
     cpipe_cuda_chain_config cfg{};
     bool f16 = true;
@@ -335,6 +391,17 @@ struct cpipe_cuda_chain {
     void* d_denoise = nullptr;            // scratch of the mode-1 denoiser
     SurrogateNet* sg = nullptr;           // mode-2 network
     float* d_ab = nullptr;                // its noise model (a, b) on the device
+    // mode-2 spot check
+    int spot_tiles = 0, spot_edge = 0;
+    float spot_mse_max = 0.0F;
+    SpotOrigins spot{};
+    Bm3dPlan tile_plan{};
+    void* d_tile_in = nullptr;            // [tiles][edge][edge] RGBA, the denoiser's input
+    void* d_tile_ref = nullptr;           // BM3D of the tiles
+    void* d_tile_scratch = nullptr;
+    float* d_tile_mse = nullptr;
+    int* d_gate = nullptr;                // 1: fall back to BM3D for this frame
+    SpotStats* d_stats = nullptr;
     void* d_io[2] = {nullptr, nullptr};   // device staging for run_host
     size_t frame_bytes = 0;
     // profiling: 5 events per frame (start, after K1, after K2, after the denoiser, after K3)
@@ -407,9 +474,24 @@ int launch_chain(cpipe_cuda_chain* c, const void* d_raw, size_t raw_pitch, void*
     }
     if (c->denoise_mode != 0) {
         const Img dn_out = c->stop_after == 2 ? out : (k2_out.data == mid1.data) ? mid0 : mid1;
-        const cudaError_t e =
+        cudaError_t e =
             c->denoise_mode == 1 ? bm3d_run(c->bm3d, k2_out, dn_out, c->f16, c->d_denoise, st, false)
                                  : surrogate_infer(c->sg, k2_out.data, dn_out.data, 1, h, w, c->f16, c->d_ab, st);
+        if (e == cudaSuccess && c->denoise_mode == 2 && c->spot_tiles > 0) {
+            const int E = c->spot_edge, n = c->spot_tiles;
+            const Img tin{c->d_tile_in, E, E * n, (long long)E * 4, 4};
+            const Img tref{c->d_tile_ref, E, E * n, (long long)E * 4, 4};
+            const dim3 gg((unsigned)((E + 127) / 128), (unsigned)E, (unsigned)n);
+            if (c->f16) spot::gather_kernel<__half><<<gg, 128, 0, st>>>(k2_out, static_cast<__half*>(c->d_tile_in), E, c->spot);
+            else spot::gather_kernel<float><<<gg, 128, 0, st>>>(k2_out, static_cast<float*>(c->d_tile_in), E, c->spot);
+            e = bm3d_run(c->tile_plan, tin, tref, c->f16, c->d_tile_scratch, st, false);
+            if (e == cudaSuccess) {
+                if (c->f16) spot::mse_kernel<__half><<<n, 256, 0, st>>>(dn_out, static_cast<const __half*>(c->d_tile_ref), E, c->spot, c->d_tile_mse);
+                else spot::mse_kernel<float><<<n, 256, 0, st>>>(dn_out, static_cast<const float*>(c->d_tile_ref), E, c->spot, c->d_tile_mse);
+                spot::decide_kernel<<<1, 1, 0, st>>>(c->d_tile_mse, n, c->spot_mse_max, c->d_gate, c->d_stats);
+                e = bm3d_run(c->bm3d, k2_out, dn_out, c->f16, c->d_denoise, st, false, c->d_gate);
+            }
+        }
         if (e != cudaSuccess) return cuda_status(e, "chain denoise");
         k2_out = dn_out;
     }
@@ -528,6 +610,33 @@ cpipe_cuda_chain* cpipe_cuda_chain_create(const cpipe_cuda_chain_config* cfg, in
         if (cudaMemcpy(c->d_ab, ab, sizeof(ab), cudaMemcpyHostToDevice) != cudaSuccess)
             return fail(CPIPE_INTERNAL_ERROR, c);
         if (surrogate_reserve(c->sg, (long long)w * h) != cudaSuccess) return fail(CPIPE_OOM, c);
+        c->spot_tiles = cfg->spot_tiles < 0 ? 0 : (cfg->spot_tiles > 16 ? 16 : cfg->spot_tiles);
+        if (c->spot_tiles > 0) {
+            // stratified tiles: the centres of a 4x4 grid of cells, clamped inside the frame
+            const int E = std::min(256, std::min(w, h));
+            c->spot_edge = E;
+            c->spot_mse_max = (float)std::pow(10.0, -(double)cfg->spot_min_psnr_db / 10.0);
+            for (int t = 0; t < c->spot_tiles; ++t) {
+                const int i = t % 4, j = t / 4;
+                c->spot.x[t] = std::min(std::max((2 * i + 1) * w / 8 - E / 2, 0), w - E);
+                c->spot.y[t] = std::min(std::max((2 * j + 1) * h / 8 - E / 2, 0), h - E);
+            }
+            cpipe_Bm3dSpecParams sp = cfg->bm3d_spec;
+            if (!(sp.sigma > 0.0F)) sp.sigma = cfg->bm3d_sigma;
+            if ((st = bm3d_plan(&sp, w, h, &c->bm3d)) != CPIPE_OK) return fail(st, c);
+            if ((st = bm3d_plan(&sp, E, E, &c->tile_plan, c->spot_tiles)) != CPIPE_OK) return fail(st, c);
+            const size_t tile_bytes = (size_t)E * E * c->spot_tiles * 4 * (c->f16 ? 2 : 4);
+            if (cudaMalloc(&c->d_tile_in, tile_bytes) != cudaSuccess || cudaMalloc(&c->d_tile_ref, tile_bytes) != cudaSuccess ||
+                (!c->tile_plan.copy && cudaMalloc(&c->d_tile_scratch, c->tile_plan.bytes) != cudaSuccess) ||
+                (!c->bm3d.copy && cudaMalloc(&c->d_denoise, c->bm3d.bytes) != cudaSuccess) ||
+                cudaMalloc(&c->d_tile_mse, sizeof(float) * 16) != cudaSuccess ||
+                cudaMalloc(&c->d_gate, sizeof(int)) != cudaSuccess || cudaMalloc(&c->d_stats, sizeof(SpotStats)) != cudaSuccess)
+                return fail(CPIPE_OOM, c);
+            if (cudaMemset(c->d_stats, 0, sizeof(SpotStats)) != cudaSuccess || cudaMemset(c->d_gate, 0, sizeof(int)) != cudaSuccess)
+                return fail(CPIPE_INTERNAL_ERROR, c);
+            if (cudaError_t e = bm3d_setup(c->bm3d); e != cudaSuccess) return fail(cuda_status(e, "bm3d setup"), c);
+            if (cudaError_t e = bm3d_setup(c->tile_plan); e != cudaSuccess) return fail(cuda_status(e, "bm3d setup"), c);
+        }
     }
     c->tone.bm3d_strength = c->denoise_mode == 0 ? fminf(1.0F, fmaxf(0.0F, cfg->bm3d_sigma / 0.03F)) : 0.0F;
     if (c->denoise_mode == 1) {
@@ -563,6 +672,12 @@ void cpipe_cuda_chain_destroy(cpipe_cuda_chain* c) {
     cudaFree(c->d_tables);
     cudaFree(c->d_denoise);
     cudaFree(c->d_ab);
+    cudaFree(c->d_tile_in);
+    cudaFree(c->d_tile_ref);
+    cudaFree(c->d_tile_scratch);
+    cudaFree(c->d_tile_mse);
+    cudaFree(c->d_gate);
+    cudaFree(c->d_stats);
     surrogate_free(c->sg);
     for (void* p : c->d_mid) cudaFree(p);
     for (void* p : c->d_io) cudaFree(p);
@@ -642,6 +757,20 @@ int cpipe_cuda_chain_profile(cpipe_cuda_chain* c, double ms_per_stage[4], int* f
     }
     *frames = (int)c->profiled;
     c->profiled = 0;
+    return CPIPE_OK;
+}
+
+int cpipe_cuda_chain_denoise_stats(cpipe_cuda_chain* c, uint32_t* frames, uint32_t* fallbacks, float* worst_tile_psnr_db) {
+    if (!c || !frames || !fallbacks || !worst_tile_psnr_db) return CPIPE_BAD_INDEX;
+    SpotStats h{};
+    if (c->d_stats) {
+        const int st = cuda_status(cudaDeviceSynchronize(), "stats sync");
+        if (st != CPIPE_OK) return st;
+        if (cudaMemcpy(&h, c->d_stats, sizeof(h), cudaMemcpyDeviceToHost) != cudaSuccess) return CPIPE_INTERNAL_ERROR;
+    }
+    *frames = h.frames;
+    *fallbacks = h.fallbacks;
+    *worst_tile_psnr_db = h.frames == 0 ? 0.0F : (h.worst_mse > 0.0F ? (float)(-10.0 * std::log10((double)h.worst_mse)) : INFINITY);
     return CPIPE_OK;
 }
 

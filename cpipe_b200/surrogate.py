@@ -17,7 +17,10 @@ activations, FP32 accumulation) that stands in for the two-stage BM3D
 No reference counterpart exists (the reference's AI denoise node is planned,
 docs/research/08-ai-isp-algorithms.md:37, but not implemented).
 
-    python -m cpipe_b200.surrogate train --pairs 20000 --steps 4000 --out weights.cpsn
+    python -m cpipe_b200.surrogate train --pairs 40000 --steps 16000 --lr 1e-3 --out weights.cpsn
+
+(the committed cpipe_b200/weights/surrogate_bm3d.cpsn was made by this command;
+its report is surrogate_bm3d.report.json beside it)
 """
 import argparse
 import ctypes as C
@@ -353,10 +356,10 @@ def _main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     sub = ap.add_subparsers(dest="cmd", required=True)
     t = sub.add_parser("train")
-    t.add_argument("--pairs", type=int, default=20000)
-    t.add_argument("--steps", type=int, default=4000)
+    t.add_argument("--pairs", type=int, default=40000)
+    t.add_argument("--steps", type=int, default=16000)
     t.add_argument("--batch", type=int, default=16)
-    t.add_argument("--lr", type=float, default=5e-4)
+    t.add_argument("--lr", type=float, default=1e-3)
     t.add_argument("--seed", type=int, default=1)
     t.add_argument("--out", default=DEFAULT_WEIGHTS)
     t.add_argument("--report", default=None)

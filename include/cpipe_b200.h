@@ -221,6 +221,13 @@ typedef struct {
     float noise_a, noise_b;             /* noise model var = a*x + b (the surrogate's noise-map input) */
     int32_t stop_after;                 /* 0: whole chain; 1: output the colormatrix result (the
                                            denoiser's input); 2: output the denoiser's result */
+    /* denoise_mode 2 spot check: every frame, two-stage BM3D on spot_tiles (<= 16)
+     * stratified 256x256 tiles of the denoiser's input; if any tile of the
+     * surrogate's output is below spot_min_psnr_db against it (peak 1), the
+     * whole frame is denoised by BM3D instead.  Decided on the device (no host
+     * synchronisation); 0 tiles: no check. */
+    int32_t spot_tiles;
+    float spot_min_psnr_db;
 } cpipe_cuda_chain_config;
 
 typedef struct cpipe_cuda_chain cpipe_cuda_chain;
@@ -238,6 +245,11 @@ int cpipe_cuda_chain_run_host(cpipe_cuda_chain* chain, const uint16_t* h_raw, vo
  * [2] the denoiser of denoise_mode 1 or 2 (0 in mode 0), [3] denoise_tone. */
 int cpipe_cuda_chain_set_profiling(cpipe_cuda_chain* chain, int enable);
 int cpipe_cuda_chain_profile(cpipe_cuda_chain* chain, double ms_per_stage[4], int* frames);
+/* Spot-check counters since creation (denoise_mode 2): frames checked, frames
+ * that fell back to BM3D, and the lowest tile PSNR seen (dB).  Waits for the
+ * device. */
+int cpipe_cuda_chain_denoise_stats(cpipe_cuda_chain* chain, uint32_t* frames, uint32_t* fallbacks,
+                                   float* worst_tile_psnr_db);
 /* Seeded synthetic raw frame on the device (uint16, width x height): linear
  * gradients, `rects` (<= 64) rectangles of uniform reflectance, a zone plate,
  * 2x2 CFA mosaic, Gaussian-form noise var = a*x + b, `bits`-bit values above

@@ -112,7 +112,7 @@ def test_short_training_reduces_loss(cuda_device):
 
 def test_chain_surrogate_mode_equals_network_on_chain_input(cuda_device):
     blob = S.to_blob(S.init_params(4))
-    base = dict(width=96, height=64, surrogate_blob=blob)
+    base = dict(width=96, height=64, surrogate_blob=blob, spot_tiles=0)
     front = Chain(ChainConfig.full_12mp(stop_after=1, **base))
     mid = Chain(ChainConfig.full_12mp(denoise="surrogate", stop_after=2, **base))
     full = Chain(ChainConfig.full_12mp(denoise="surrogate", **base))
@@ -145,3 +145,57 @@ def test_trained_weights_gain_over_no_network(cuda_device):
     assert r["surrogate"] >= 40.0
     assert r["surrogate"] > r["noisy"] + 6.0 and r["surrogate"] > r["box2x2"] + 3.0
     sg.close()
+
+
+def spot_chain(blob, min_psnr, **kw):
+    return Chain(ChainConfig.full_12mp(width=320, height=288, surrogate_blob=blob, denoise="surrogate",
+                                       spot_tiles=16, spot_min_psnr_db=min_psnr, **kw))
+
+
+def test_spot_check_passes_and_keeps_the_network_output(cuda_device):
+    """A threshold of 0 dB never falls back: the output is the network's, bit
+    for bit, and the counters record one checked frame."""
+    blob = S.to_blob(S.init_params(6))
+    raw = ChainConfig.full_12mp(width=320, height=288).make_raw()
+    plain = Chain(ChainConfig.full_12mp(width=320, height=288, surrogate_blob=blob, denoise="surrogate",
+                                        spot_tiles=0, stop_after=2))
+    checked = spot_chain(blob, 0.0, stop_after=2)
+    a, b = plain.run_host(raw), checked.run_host(raw)
+    np.testing.assert_array_equal(a.view(np.uint16), b.view(np.uint16))
+    frames, fallbacks, worst = checked.denoise_stats()
+    assert (frames, fallbacks) == (1, 0) and np.isfinite(worst)
+    plain.close()
+    checked.close()
+
+
+def test_spot_check_falls_back_to_bm3d(cuda_device):
+    """An unreachable threshold makes every frame fall back: the denoiser's
+    output is then the two-stage BM3D of the frame (its aggregation order on
+    the GPU is not fixed, hence a PSNR bound)."""
+    blob = S.to_blob(S.init_params(6))
+    raw = ChainConfig.full_12mp(width=320, height=288).make_raw()
+    checked = spot_chain(blob, 300.0, stop_after=2)
+    bm3d = Chain(ChainConfig.full_12mp(width=320, height=288, denoise="bm3d", stop_after=2))
+    for _ in range(2):
+        got = checked.run_host(raw).astype(np.float32)
+    want = bm3d.run_host(raw).astype(np.float32)
+    p = 10 * np.log10(1.0 / np.mean((got[..., :3] - want[..., :3]) ** 2))
+    print(f"fallback vs BM3D chain: {p:.1f} dB")
+    assert p >= 60.0
+    assert checked.denoise_stats()[:2] == (2, 2)
+    checked.close()
+    bm3d.close()
+
+
+@pytest.mark.skipif(not os.path.exists(S.DEFAULT_WEIGHTS), reason="no trained weights committed")
+def test_trained_surrogate_passes_spot_check_at_12mp(cuda_device):
+    """The committed network on the 4032x3024 benchmark frame: every sampled
+    tile is within 40 dB of BM3D, so the chain keeps the network's output."""
+    chain = Chain(ChainConfig.full_12mp(denoise="surrogate", surrogate_blob=S.load_weights()))
+    raw = chain.config.make_raw()
+    out = chain.run_host(raw)
+    frames, fallbacks, worst = chain.denoise_stats()
+    print(f"12 MP spot check: {frames} frame, {fallbacks} fallbacks, worst tile {worst:.2f} dB")
+    assert frames == 1 and fallbacks == 0 and worst >= 40.0
+    assert np.isfinite(out.astype(np.float32)).all()
+    chain.close()
