@@ -157,7 +157,7 @@ EXPORTS = [
     "cpipe_cuda_color_3d_lut_noalloc",
     "cpipe_b200_node_descs", "cpipe_b200_find_node",
     "cpipe_cuda_scene_raw", "cpipe_surrogate_blob_size", "cpipe_surrogate_create", "cpipe_surrogate_destroy", "cpipe_surrogate_export",
-    "cpipe_surrogate_denoise", "cpipe_surrogate_profile", "cpipe_surrogate_train_step", "cpipe_surrogate_gradients",
+    "cpipe_surrogate_denoise", "cpipe_surrogate_set_engine", "cpipe_surrogate_check", "cpipe_surrogate_profile", "cpipe_surrogate_train_step", "cpipe_surrogate_gradients",
     "cpipe_b200_wb_prepare", "cpipe_b200_colormatrix_compose", "cpipe_b200_pack_gain_maps",
     "cpipe_b200_pack_opcode_list_3", "cpipe_b200_load_lut",
     "cpipe_b200_host_create", "cpipe_b200_host_destroy", "cpipe_b200_host_abi", "cpipe_b200_host_set_memory_cap",
@@ -247,6 +247,7 @@ def lib():
         "cpipe_surrogate_destroy": (None, [vp]), "cpipe_surrogate_export": (i32, [vp, vp, sz]),
         "cpipe_surrogate_denoise": (i32, [vp, vp, vp, i32, i32, i32, i32, vp, vp]),
         "cpipe_surrogate_profile": (i32, [vp, vp, vp, i32, i32, i32, i32, vp, vp, vp]),
+        "cpipe_surrogate_set_engine": (i32, [vp, i32]), "cpipe_surrogate_check": (i32, [vp]),
         "cpipe_surrogate_train_step": (i32, [vp, vp, vp, vp, i32, i32, i32, C.c_float, i32, C.POINTER(C.c_float),
                                              vp]),
         "cpipe_surrogate_gradients": (i32, [vp, vp, sz]),

@@ -44,6 +44,7 @@
 #include "common.cuh"
 #include "filters_impl.h"
 #include "surrogate.h"
+#include "surrogate_tc.h"
 
 namespace cpb {
 namespace sg {
@@ -466,6 +467,8 @@ struct SurrogateNet {
     float* d_gnorm = nullptr;    // squared gradient norm of the last step
     float* d_ab = nullptr;       // per-image noise model (a, b)
     int ab_cap = 0;
+    int* d_err = nullptr;        // nonzero: a tcgen05 pipeline wait ran out
+    bool use_tc = true;          // inference on tcgen05 (else the mma.sync kernels)
     int step = 0;
     // activations for a batch of n x h x w
     long long act_px = 0;
@@ -599,6 +602,34 @@ static cudaError_t infer(SurrogateNet* s, const void* in, void* out, int n, int 
     if (f16) sg_prep_kernel<__half><<<(unsigned)((px + 255) / 256), 256, 0, st>>>(static_cast<const __half*>(in), s->d_act, d_ab, (long long)h * w, n);
     else sg_prep_kernel<float><<<(unsigned)((px + 255) / 256), 256, 0, st>>>(static_cast<const float*>(in), s->d_act, d_ab, (long long)h * w, n);
     if (ev) cudaEventRecord(ev[1], st);
+    if (s->use_tc) {
+        const bf16* cur = s->d_act;
+        bf16* hid = s->d_act + (size_t)px * 8;
+        for (int l = 0; l < kLayers; ++l) {
+            TcConvArgs t{};
+            t.n = n;
+            t.h = h;
+            t.w = w;
+            t.w_rows = cout_pad(l);
+            t.bias = s->d_params + s->t.boff[l];
+            t.cout_real = cout_real(l);
+            t.err = s->d_err;
+            cudaError_t e2;
+            if (l < kLayers - 1) {
+                bf16* nxt = hid + (size_t)(l & 1) * px * kCh;
+                t.y = nxt;
+                e2 = tc_conv(cin_pad(l), kCh, 0, f16, cur, s->d_packed + s->t.fwoff[l], t, st);
+                cur = nxt;
+            } else {
+                t.rgba = in;
+                t.out = out;
+                e2 = tc_conv(kCh, 16, 1, f16, cur, s->d_packed + s->t.fwoff[l], t, st);
+            }
+            if (e2 != cudaSuccess) return e2;
+            if (ev) cudaEventRecord(ev[l + 2], st);
+        }
+        return cudaGetLastError();
+    }
     const bf16* a7 = forward_hidden(s, n, h, w, false, st, ev);
     ConvArgs a = conv_args(s, kLayers - 1, a7, nullptr, n, h, w);
     a.rgba = in;
@@ -635,11 +666,13 @@ SurrogateNet* surrogate_new(const void* blob, size_t size, int* status) {
         if (!std::isfinite(params[i])) return fail(CPIPE_BAD_INDEX, s);
     if (cudaMalloc(&s->d_params, sizeof(float) * s->nparams) != cudaSuccess ||
         cudaMalloc(&s->d_packed, sizeof(bf16) * s->npacked) != cudaSuccess ||
-        cudaMalloc(&s->d_loss, sizeof(float)) != cudaSuccess || cudaMalloc(&s->d_gnorm, sizeof(float)) != cudaSuccess)
+        cudaMalloc(&s->d_loss, sizeof(float)) != cudaSuccess || cudaMalloc(&s->d_gnorm, sizeof(float)) != cudaSuccess ||
+        cudaMalloc(&s->d_err, sizeof(int)) != cudaSuccess || cudaMemset(s->d_err, 0, sizeof(int)) != cudaSuccess)
         return fail(CPIPE_OOM, s);
     if (cudaMemcpy(s->d_params, params, sizeof(float) * s->nparams, cudaMemcpyHostToDevice) != cudaSuccess)
         return fail(CPIPE_INTERNAL_ERROR, s);
     if (pack(s, nullptr) != cudaSuccess || cudaDeviceSynchronize() != cudaSuccess) return fail(CPIPE_INTERNAL_ERROR, s);
+    s->use_tc = tc_conv_available();
     if (status) *status = CPIPE_OK;
     return s;
 }
@@ -654,6 +687,7 @@ void surrogate_free(SurrogateNet* s) {
     cudaFree(s->d_packed);
     cudaFree(s->d_loss);
     cudaFree(s->d_gnorm);
+    cudaFree(s->d_err);
     cudaFree(s->d_ab);
     delete s;
 }
@@ -711,6 +745,30 @@ int cpipe_surrogate_denoise(cpipe_surrogate* s, const void* d_in, void* d_out, i
     cudaError_t e = upload_ab(s->net, noise_ab, n, st);
     if (e == cudaSuccess) e = surrogate_infer(s->net, d_in, d_out, n, height, width, f16 != 0, s->net->d_ab, st);
     return cuda_status(e, "surrogate denoise");
+}
+
+int cpipe_surrogate_set_engine(cpipe_surrogate* s, int engine) {
+    if (!s || (engine != 0 && engine != 1)) return CPIPE_BAD_INDEX;
+    if (engine == 1 && !tc_conv_available()) {
+        set_error("surrogate: %s", "tensor-map encoder unavailable for the tcgen05 engine");
+        return CPIPE_UNSUPPORTED;
+    }
+    s->net->use_tc = engine == 1;
+    return CPIPE_OK;
+}
+
+int cpipe_surrogate_check(cpipe_surrogate* s) {
+    if (!s) return CPIPE_BAD_INDEX;
+    int err = 0;
+    const int st = cuda_status(cudaDeviceSynchronize(), "surrogate check");
+    if (st != CPIPE_OK) return st;
+    if (cudaMemcpy(&err, s->net->d_err, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess) return CPIPE_INTERNAL_ERROR;
+    if (err) {
+        set_error("surrogate: tcgen05 pipeline wait ran out (%s)", err == 1 ? "input stage" : err == 2 ? "tile load"
+                                                                    : err == 3 ? "accumulator" : "MMA completion");
+        return CPIPE_INTERNAL_ERROR;
+    }
+    return CPIPE_OK;
 }
 
 int cpipe_surrogate_profile(cpipe_surrogate* s, const void* d_in, void* d_out, int n, int width, int height, int f16,

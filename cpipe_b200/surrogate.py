@@ -163,6 +163,17 @@ class Surrogate:
         if st:
             raise CpipeError(st, "surrogate_denoise " + A.lib().cpipe_cuda_last_error().decode())
 
+    def set_engine(self, engine):
+        """'tcgen05' (default) or 'mma' for inference."""
+        st = A.lib().cpipe_surrogate_set_engine(self._h, {"mma": 0, "tcgen05": 1}[engine])
+        if st:
+            raise CpipeError(st, "surrogate_set_engine " + A.lib().cpipe_cuda_last_error().decode())
+
+    def check(self):
+        st = A.lib().cpipe_surrogate_check(self._h)
+        if st:
+            raise CpipeError(st, "surrogate_check " + A.lib().cpipe_cuda_last_error().decode())
+
     def profile(self, d_in, d_out, n, width, height, noise_ab, f16=True, stream=None):
         """Per-kernel times (ms) of one denoise: [input map, layer 0, ..., layer 7]."""
         keep, p = _ab(noise_ab)

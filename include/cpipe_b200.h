@@ -274,6 +274,12 @@ void cpipe_surrogate_destroy(cpipe_surrogate* s);
 int cpipe_surrogate_export(const cpipe_surrogate* s, void* blob, size_t blob_size);
 int cpipe_surrogate_denoise(cpipe_surrogate* s, const void* d_in, void* d_out, int n, int width, int height, int f16,
                             const float* noise_ab, void* stream);
+/* Inference engine: 1 = tcgen05 kernels (default where the driver provides the
+ * tensor-map encoder), 0 = the mma.sync kernels the training uses. */
+int cpipe_surrogate_set_engine(cpipe_surrogate* s, int engine);
+/* Waits for the device; CPIPE_INTERNAL_ERROR (with a message) when a bounded
+ * wait inside a tcgen05 kernel ran out since creation. */
+int cpipe_surrogate_check(cpipe_surrogate* s);
 /* One denoise with CUDA events between its kernels: ms[0] the input map,
  * ms[1 + l] layer l (l = 0..7).  Waits for the stream. */
 int cpipe_surrogate_profile(cpipe_surrogate* s, const void* d_in, void* d_out, int n, int width, int height, int f16,
