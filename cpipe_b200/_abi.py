@@ -97,7 +97,7 @@ class Bm3dSpecParams(C.Structure):
     """cpipe_Bm3dSpecParams (two-stage colour BM3D, aot_id denoise_bm3d_spec)."""
     _fields_ = [("sigma", C.c_float), ("lambda3d", C.c_float), ("tau_match1", C.c_float),
                 ("tau_match2", C.c_float), ("n2", C.c_int32), ("ns", C.c_int32), ("nstep", C.c_int32),
-                ("kaiser_beta", C.c_float), ("stages", C.c_int32), ("reserved", C.c_int32)]
+                ("kaiser_beta", C.c_float), ("stages", C.c_int32), ("transform", C.c_int32)]
 
 
 class GuidedFilterParams(C.Structure):

@@ -411,6 +411,356 @@ __global__ void __launch_bounds__(256, 2) bm3d_filter_kernel(FilterArgs a, int p
     }
 }
 
+// ------------------------------------------- filter on the tensor cores
+// The group transform as small GEMMs on mma.sync.m16n8k16 (FP16 operands, FP32
+// accumulation).  Every product whose operands are not exact in FP16 is split
+// hi/lo (x = hi + lo, both FP16): a*b ~ ahi*bhi + alo*bhi + ahi*blo, which
+// keeps FP32-level accuracy for the threshold and Wiener decisions.  With
+// Xt[64 px][16 blocks] the group of one channel:
+//   forward  P = D * Xt          (D = C (x) C, the 64x64 2D DCT; K = pixels)
+//            T = P * H^T         (H = unnormalised Haar rows, +-1/0: exact; K = blocks)
+//            Tn = T * scale      (per Haar row: 1/sqrt(N) or 1/sqrt(2s))
+//   shrink   hard threshold / Wiener on Tn (FP32)
+//   inverse  Q = (Tn * scale) * H  (K = Haar index)
+//            X' = Q^T * D        (K = coefficients; Q^T from Q's fragments by
+//                                 movmatrix.trans, in registers)
+// The accumulator fragment of two adjacent n8 tiles is the A fragment of the
+// next product (P -> T, Tn -> Q), and movmatrix transposes Q in registers, so
+// the transform needs no shared-memory pass beyond the constant tables.
+struct TcTables {
+    __half dhi[64 * 72];     // D[coeff][pixel], rows padded to 72 halves (conflict-free ldmatrix)
+    __half dlo[64 * 72];
+    __half haar[5][16 * 24]; // unnormalised Haar for N = 1, 2, 4, 8, 16: [row][block], rows padded to 24
+    float scale[5][16];
+};
+
+__global__ void bm3d_tables_kernel(TcTables* t) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < 64 * 64) {
+        const int k = i >> 6, px = i & 63;
+        const float d = dctc(k >> 3, px >> 3) * dctc(k & 7, px & 7);
+        const __half hi = __float2half_rn(d);
+        t->dhi[k * 72 + px] = hi;
+        t->dlo[k * 72 + px] = __float2half_rn(d - __half2float(hi));
+    }
+    if (i < 5 * 16 * 16) {
+        const int L = i >> 8, r = (i >> 4) & 15, b = i & 15, N = 1 << L;
+        float h = 0.0F;
+        if (r < N && b < N) {
+            if (r == 0) {
+                h = 1.0F;
+            } else {
+                const int sft = r & -r;  // lowest set bit: the level of this detail row
+                h = (b >= r - sft && b < r) ? 1.0F : (b >= r && b < r + sft) ? -1.0F : 0.0F;
+            }
+        }
+        t->haar[L][r * 24 + b] = __float2half_rn(h);
+        if (b == 0) {
+            const int sft = r & -r;
+            t->scale[L][r] = r >= N ? 0.0F : r == 0 ? rsqrtf((float)N) : rsqrtf(2.0F * (float)sft);
+        }
+    }
+}
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void ldsm4(uint32_t (&r)[4], const void* p) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(smem_u32(p)));
+}
+__device__ __forceinline__ void ldsm4t(uint32_t (&r)[4], const void* p) {
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(smem_u32(p)));
+}
+// 8x8 b16 matrix held as a fragment (row lane/4, columns 2(lane%4)..+1) -> its transpose.
+__device__ __forceinline__ uint32_t movtrans(uint32_t x) {
+    uint32_t y;
+    asm volatile("movmatrix.sync.aligned.m8n8.trans.b16 %0, %1;\n" : "=r"(y) : "r"(x));
+    return y;
+}
+__device__ __forceinline__ void mma16816(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+// FP16 hi/lo halves of two floats, packed as (x0, x1) pairs.
+__device__ __forceinline__ void split2(float x0, float x1, uint32_t& hi, uint32_t& lo) {
+    const __half2 h = __floats2half2_rn(x0, x1);
+    const float2 hf = __half22float2(h);
+    const __half2 l = __floats2half2_rn(x0 - hf.x, x1 - hf.y);
+    hi = *reinterpret_cast<const uint32_t*>(&h);
+    lo = *reinterpret_cast<const uint32_t*>(&l);
+}
+
+constexpr int kTcWarps = 8;
+
+// Forward transform of one group (channel image `img`, footprint row stride
+// fw): returns Tn in accumulator layout, acc[mt][nt][e] = Tn[coeff 16mt + g
+// (+8 for e >= 2)][haar 8nt + 2q + (e & 1)].
+__device__ __forceinline__ void tc_forward(const float* img, int fw, const int (&bxy)[2][2], bool (&act)[2],
+                                           const TcTables* tb, int L, float (&acc)[4][2][4]) {
+    const int lane = threadIdx.x & 31, q = lane & 3, mi = lane >> 3, rr = lane & 7;
+#pragma unroll
+    for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) acc[mt][nt][e] = 0.0F;
+#pragma unroll
+    for (int ks = 0; ks < 4; ++ks) {  // pixels 16ks .. 16ks+15 = block rows 2ks, 2ks+1
+        uint32_t bh[2][2], bl[2][2];
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt) {
+            float v[4] = {0.0F, 0.0F, 0.0F, 0.0F};
+            if (act[nt]) {
+                const float* r0 = img + (bxy[nt][1] + 2 * ks) * fw + bxy[nt][0] + 2 * q;
+                v[0] = r0[0];
+                v[1] = r0[1];
+                v[2] = r0[fw];
+                v[3] = r0[fw + 1];
+            }
+            split2(v[0], v[1], bh[nt][0], bl[nt][0]);
+            split2(v[2], v[3], bh[nt][1], bl[nt][1]);
+        }
+#pragma unroll
+        for (int mt = 0; mt < 4; ++mt) {
+            uint32_t ah[4], al[4];
+            const int off = (16 * mt + rr + 8 * (mi & 1)) * 72 + 16 * ks + 8 * (mi >> 1);
+            ldsm4(ah, tb->dhi + off);
+            ldsm4(al, tb->dlo + off);
+#pragma unroll
+            for (int nt = 0; nt < 2; ++nt) {
+                mma16816(acc[mt][nt], ah, bh[nt][0], bh[nt][1]);
+                mma16816(acc[mt][nt], al, bh[nt][0], bh[nt][1]);
+                mma16816(acc[mt][nt], ah, bl[nt][0], bl[nt][1]);
+            }
+        }
+    }
+    // T = P * H^T: the B operand H^T[block][haar] comes from H[haar][block] rows
+    uint32_t hb[4];
+    ldsm4(hb, tb->haar[L] + (8 * (mi >> 1) + rr) * 24 + 8 * (mi & 1));
+    const float* sc = tb->scale[L];
+#pragma unroll
+    for (int mt = 0; mt < 4; ++mt) {
+        uint32_t ah[4], al[4];
+        split2(acc[mt][0][0], acc[mt][0][1], ah[0], al[0]);
+        split2(acc[mt][0][2], acc[mt][0][3], ah[1], al[1]);
+        split2(acc[mt][1][0], acc[mt][1][1], ah[2], al[2]);
+        split2(acc[mt][1][2], acc[mt][1][3], ah[3], al[3]);
+        float t[2][4] = {{0.0F, 0.0F, 0.0F, 0.0F}, {0.0F, 0.0F, 0.0F, 0.0F}};
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt) {
+            mma16816(t[nt], ah, hb[2 * nt], hb[2 * nt + 1]);
+            mma16816(t[nt], al, hb[2 * nt], hb[2 * nt + 1]);
+        }
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt) {
+            const float s0 = sc[8 * nt + 2 * q], s1 = sc[8 * nt + 2 * q + 1];
+            acc[mt][nt][0] = t[nt][0] * s0;
+            acc[mt][nt][1] = t[nt][1] * s1;
+            acc[mt][nt][2] = t[nt][2] * s0;
+            acc[mt][nt][3] = t[nt][3] * s1;
+        }
+    }
+}
+
+template <int STAGE>
+__global__ void __launch_bounds__(32 * kTcWarps, 2) bm3d_filter_tc_kernel(FilterArgs a, const TcTables* tables,
+                                                                           int phx, int phy) {
+    extern __shared__ __align__(16) float sm[];
+    const int c = blockIdx.z % 3, img = blockIdx.z / 3, row0 = img * a.h;
+    const int tx = blockIdx.x * a.phases + phx, ty = blockIdx.y * a.phases + phy;
+    if (tx >= a.ntx || ty >= a.nty || gated_off(a.gate)) return;
+    const int i0 = tx * kRefTile, j0 = ty * kRefTile;
+    const int i1 = min(i0 + kRefTile, a.nrx), j1 = min(j0 + kRefTile, a.nry);
+    const int fx0 = max(0, refpos(i0, a.w, a.nstep) - a.R);
+    const int fx1 = min(a.w, refpos(i1 - 1, a.w, a.nstep) + a.R + 8);
+    const int fy0 = row0 + max(0, refpos(j0, a.h, a.nstep) - a.R);
+    const int fy1 = row0 + min(a.h, refpos(j1 - 1, a.h, a.nstep) + a.R + 8);
+    const int fw = fx1 - fx0, fn = fw * (fy1 - fy0);
+    const int FN = a.fw * a.fw;
+    float* s_num = sm;
+    float* s_den = sm + FN;
+    float* s_img = sm + 2 * FN;
+    float* s_bas = sm + 3 * FN;
+    float* s_k = sm + (STAGE == 2 ? 4 : 3) * FN;
+    TcTables* s_tb = reinterpret_cast<TcTables*>((reinterpret_cast<uintptr_t>(s_k + 64) + 127) & ~(uintptr_t)127);
+    uint32_t* s_list = reinterpret_cast<uint32_t*>(s_tb + 1);  // the tile's groups
+    uint32_t* s_cnt = s_list + kRefTile * kRefTile * 16;
+    const float* gz = a.noisy + (long long)c * a.npx;
+    const float* gb = STAGE == 2 ? a.basic + (long long)c * a.npx : nullptr;
+    for (int idx = threadIdx.x; idx < fn; idx += blockDim.x) {
+        const int yy = idx / fw, xx = idx - yy * fw;
+        const long long o = (long long)(fy0 + yy) * a.w + fx0 + xx;
+        s_num[idx] = 0.0F;
+        s_den[idx] = 0.0F;
+        s_img[idx] = gz[o];
+        if (STAGE == 2) s_bas[idx] = gb[o];
+    }
+    if (threadIdx.x < 64) s_k[threadIdx.x] = a.kaiser[threadIdx.x];
+    {
+        const uint4* src = reinterpret_cast<const uint4*>(tables);
+        uint4* dst = reinterpret_cast<uint4*>(s_tb);
+        for (int i = threadIdx.x; i < (int)(sizeof(TcTables) / 16); i += blockDim.x) dst[i] = src[i];
+    }
+    const int nti = i1 - i0, nref = nti * (j1 - j0);
+    for (int i = threadIdx.x; i < nref * 16; i += blockDim.x) {
+        const int k = i >> 4;
+        const long long ref = ((long long)img * a.nry + j0 + k / nti) * a.nrx + i0 + k % nti;
+        s_list[i] = a.list[ref * 16 + (i & 15)];
+        if ((i & 15) == 0) s_cnt[k] = a.cnt[ref];
+    }
+    __syncthreads();
+
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
+    const int mi = lane >> 3, rr = lane & 7;
+    for (int k = warp; k < nref; k += kTcWarps) {
+        const int cnt = (int)s_cnt[k];
+        const int L = cnt >= 16 ? 4 : cnt >= 8 ? 3 : cnt >= 4 ? 2 : cnt >= 2 ? 1 : 0;
+        const int N = 1 << L;
+        const uint32_t* lst = s_list + k * 16;
+        // blocks this lane loads (n = g of each n-tile) ...
+        int bxy[2][2];
+        bool act[2];
+#pragma unroll
+        for (int nt = 0; nt < 2; ++nt) {
+            const int b = 8 * nt + g;
+            act[nt] = b < N;
+            const uint32_t p = act[nt] ? lst[b] : 0U;
+            bxy[nt][0] = (int)(p & 0xFFFFU) - fx0;
+            bxy[nt][1] = (int)(p >> 16) - fy0;
+        }
+        float T[4][2][4];
+        tc_forward(s_img, fw, bxy, act, s_tb, L, T);
+        float wgt;
+        if (STAGE == 1) {
+            unsigned kept = 0;
+#pragma unroll
+            for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+                for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        const bool keep = fabsf(T[mt][nt][e]) > a.thr;
+                        T[mt][nt][e] = keep ? T[mt][nt][e] : 0.0F;
+                        kept += keep ? 1U : 0U;
+                    }
+            kept = __reduce_add_sync(0xFFFFFFFFU, kept);
+            wgt = kept > 0U ? 1.0F / (float)kept : a.sigma2;
+        } else {
+            float Bc[4][2][4];
+            tc_forward(s_bas, fw, bxy, act, s_tb, L, Bc);
+            float sw2 = 0.0F;
+#pragma unroll
+            for (int mt = 0; mt < 4; ++mt)
+#pragma unroll
+                for (int nt = 0; nt < 2; ++nt)
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) {
+                        const float b2 = Bc[mt][nt][e] * Bc[mt][nt][e];
+                        const float W = b2 / (b2 + a.sigma2);
+                        T[mt][nt][e] = T[mt][nt][e] * W;
+                        sw2 = __fmaf_rn(W, W, sw2);
+                    }
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) sw2 += __shfl_xor_sync(0xFFFFFFFFU, sw2, off);
+            wgt = sw2 > 0.0F ? 1.0F / fmaxf(sw2, kMinWienerEnergy) : a.sigma2;
+        }
+        // Q = (Tn * scale) * H  (B = H[haar][block] via transposing ldmatrix)
+        uint32_t hb[4];
+        ldsm4t(hb, s_tb->haar[L] + (8 * (mi & 1) + rr) * 24 + 8 * (mi >> 1));
+        const float* sc = s_tb->scale[L];
+        // Q^T as A fragments of X' = Q^T * D: qa[ks][0..3] (hi), qb (lo), k-step ks = coefficients 16ks..
+        uint32_t qa[4][4], qb[4][4];
+#pragma unroll
+        for (int mt = 0; mt < 4; ++mt) {
+            float z[2][4];
+#pragma unroll
+            for (int nt = 0; nt < 2; ++nt) {
+                const float s0 = sc[8 * nt + 2 * q], s1 = sc[8 * nt + 2 * q + 1];
+                z[nt][0] = T[mt][nt][0] * s0;
+                z[nt][1] = T[mt][nt][1] * s1;
+                z[nt][2] = T[mt][nt][2] * s0;
+                z[nt][3] = T[mt][nt][3] * s1;
+            }
+            uint32_t ah[4], al[4];
+            split2(z[0][0], z[0][1], ah[0], al[0]);
+            split2(z[0][2], z[0][3], ah[1], al[1]);
+            split2(z[1][0], z[1][1], ah[2], al[2]);
+            split2(z[1][2], z[1][3], ah[3], al[3]);
+            float qv[2][4] = {{0.0F, 0.0F, 0.0F, 0.0F}, {0.0F, 0.0F, 0.0F, 0.0F}};
+#pragma unroll
+            for (int nt = 0; nt < 2; ++nt) {
+                mma16816(qv[nt], ah, hb[2 * nt], hb[2 * nt + 1]);
+                mma16816(qv[nt], al, hb[2 * nt], hb[2 * nt + 1]);
+            }
+            // Q[coeff 16mt + (g | g+8)][block 8nt + 2q..]: four 8x8 pieces, transposed in registers
+            uint32_t h00, l00, h01, l01, h10, l10, h11, l11;  // [nt][row half]
+            split2(qv[0][0], qv[0][1], h00, l00);
+            split2(qv[0][2], qv[0][3], h01, l01);
+            split2(qv[1][0], qv[1][1], h10, l10);
+            split2(qv[1][2], qv[1][3], h11, l11);
+            qa[mt][0] = movtrans(h00);  // blocks 0-7  x coeffs 16mt + 0..7
+            qa[mt][1] = movtrans(h10);  // blocks 8-15 x coeffs 16mt + 0..7
+            qa[mt][2] = movtrans(h01);  // blocks 0-7  x coeffs 16mt + 8..15
+            qa[mt][3] = movtrans(h11);  // blocks 8-15 x coeffs 16mt + 8..15
+            qb[mt][0] = movtrans(l00);
+            qb[mt][1] = movtrans(l10);
+            qb[mt][2] = movtrans(l01);
+            qb[mt][3] = movtrans(l11);
+        }
+        // X' = Q^T * D: M = 16 blocks, N = 64 pixels, K = 64 coefficients; B = D[coeff][pixel]
+        // through transposing ldmatrix.  X[nt][e] = block g (+8 for e >= 2), pixel 8nt + 2q + (e & 1)
+        float X[8][4];
+#pragma unroll
+        for (int nt = 0; nt < 8; ++nt)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) X[nt][e] = 0.0F;
+#pragma unroll
+        for (int ks = 0; ks < 4; ++ks)
+#pragma unroll
+            for (int nt = 0; nt < 8; nt += 2) {
+                uint32_t bh[4], bl[4];
+                const int boff = (16 * ks + 8 * (mi & 1) + rr) * 72 + 8 * (nt + (mi >> 1));
+                ldsm4t(bh, s_tb->dhi + boff);
+                ldsm4t(bl, s_tb->dlo + boff);
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    mma16816(X[nt + j], qa[ks], bh[2 * j], bh[2 * j + 1]);
+                    mma16816(X[nt + j], qb[ks], bh[2 * j], bh[2 * j + 1]);
+                    mma16816(X[nt + j], qa[ks], bl[2 * j], bl[2 * j + 1]);
+                }
+            }
+        // aggregation: this lane holds blocks g and g + 8 (the blocks it loaded), rows nt, columns 2q, 2q+1
+#pragma unroll
+        for (int hb2 = 0; hb2 < 2; ++hb2) {
+            if (!act[hb2]) continue;
+            const int bx = bxy[hb2][0], by = bxy[hb2][1];
+#pragma unroll
+            for (int nt = 0; nt < 8; ++nt)
+#pragma unroll
+                for (int j = 0; j < 2; ++j) {
+                    const int px = 8 * nt + 2 * q + j;
+                    const float kw = wgt * s_k[px];
+                    const int o = (by + nt) * fw + bx + 2 * q + j;
+                    atomicAdd(s_num + o, kw * X[nt][2 * hb2 + j]);
+                    atomicAdd(s_den + o, kw);
+                }
+        }
+    }
+    __syncthreads();
+    float* gn = a.acc + (long long)c * a.npx;
+    float* gd = a.acc + (long long)(3 + c) * a.npx;
+    for (int idx = threadIdx.x; idx < fn; idx += blockDim.x) {
+        const int yy = idx / fw, xx = idx - yy * fw;
+        const long long o = (long long)(fy0 + yy) * a.w + fx0 + xx;
+        gn[o] += s_num[idx];
+        gd[o] += s_den[idx];
+    }
+}
+
 // --------------------------------------------------------- basic / final
 __global__ void bm3d_basic_kernel(const float* __restrict__ acc, float* __restrict__ basic, uint8_t* __restrict__ q,
                                   long long npx, const int* gate) {
@@ -469,6 +819,10 @@ size_t filter_smem(const Bm3dPlan& p, int stage) {
     return sizeof(float) * ((size_t)(stage == 2 ? 4 : 3) * p.fw * p.fw + (size_t)kFilterWarps * kWarpBuf + 64);
 }
 size_t match_smem(const Bm3dPlan& p) { return sizeof(uint32_t) * 4 * (size_t)p.mwin * p.mwpr; }
+size_t filter_tc_smem(const Bm3dPlan& p, int stage) {
+    return sizeof(float) * ((size_t)(stage == 2 ? 4 : 3) * p.fw * p.fw + 64) + 128 + sizeof(TcTables) +
+           sizeof(uint32_t) * kRefTile * kRefTile * 17;
+}
 
 }  // namespace
 
@@ -482,6 +836,7 @@ int bm3d_plan(const cpipe_Bm3dSpecParams* p, int w, int h, Bm3dPlan* out, int ba
     if (!(p->tau_match2 >= 0.0F && p->tau_match2 <= 16000.0F)) return CPIPE_BAD_INDEX;
     if (p->stages != 1 && p->stages != 2) return CPIPE_BAD_INDEX;
     if (!(p->lambda3d >= 0.0F) || !(p->kaiser_beta >= 0.0F)) return CPIPE_BAD_INDEX;
+    if (p->transform != 0 && p->transform != 1) return CPIPE_BAD_INDEX;
     if (w <= 0 || h <= 0 || batch < 1 || w > 65535 || (long long)h * batch > 65535) return CPIPE_BAD_INDEX;
     Bm3dPlan& q = *out;
     q = Bm3dPlan{};
@@ -493,6 +848,7 @@ int bm3d_plan(const cpipe_Bm3dSpecParams* p, int w, int h, Bm3dPlan* out, int ba
     q.n2 = n2;
     q.nstep = p->nstep;
     q.stages = p->stages;
+    q.tensor = p->transform == 0;
     q.sigma = p->sigma;
     q.sigma2 = p->sigma * p->sigma;
     q.thr = p->lambda3d * p->sigma;
@@ -531,6 +887,8 @@ int bm3d_plan(const cpipe_Bm3dSpecParams* p, int w, int h, Bm3dPlan* out, int ba
     o = align256(o + nref * 16 * sizeof(uint32_t));
     q.off_cnt = o;
     o = align256(o + nref);
+    q.off_tables = o;
+    o = align256(o + sizeof(TcTables));
     q.bytes = o;
     return CPIPE_OK;
 }
@@ -545,6 +903,14 @@ cudaError_t bm3d_setup(const Bm3dPlan& p) {
         e = cudaFuncSetAttribute(bm3d_filter_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fs1);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(bm3d_filter_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fs2);
+    if (p.tensor) {
+        const size_t t1 = filter_tc_smem(p, 1), t2 = filter_tc_smem(p, 2);
+        if (t2 > kSmemOptIn) return cudaErrorInvalidConfiguration;
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(bm3d_filter_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t1);
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(bm3d_filter_tc_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t2);
+    }
     return e;
 }
 
@@ -563,10 +929,13 @@ cudaError_t bm3d_run(const Bm3dPlan& p, const Img& in, const Img& out, bool f16,
     uint8_t* q = reinterpret_cast<uint8_t*>(base + p.off_q);
     uint32_t* list = reinterpret_cast<uint32_t*>(base + p.off_list);
     uint8_t* cnt = reinterpret_cast<uint8_t*>(base + p.off_cnt);
+    TcTables* tables = reinterpret_cast<TcTables*>(base + p.off_tables);
     const long long npx = (long long)p.w * p.h * p.batch;
     cudaError_t e;
     if (setup && (e = bm3d_setup(p)) != cudaSuccess) return e;
     const size_t ms = match_smem(p), fs1 = filter_smem(p, 1), fs2 = filter_smem(p, 2);
+    const size_t ts1 = filter_tc_smem(p, 1), ts2 = filter_tc_smem(p, 2);
+    if (p.tensor) bm3d_tables_kernel<<<16, 256, 0, st>>>(tables);
 
     const dim3 pgrid((p.w + 255) / 256, p.h * p.batch);
     if (f16) bm3d_prep_kernel<__half><<<pgrid, 256, 0, st>>>(in, yuv, q, npx, gate);
@@ -603,8 +972,13 @@ cudaError_t bm3d_run(const Bm3dPlan& p, const Img& in, const Img& out, bool f16,
         bm3d_match_kernel<<<mgrid, kMatchTile * kMatchTile, ms, st>>>(ma);
         for (int py = 0; py < p.phases; ++py)
             for (int pxh = 0; pxh < p.phases; ++pxh) {
-                if (stage == 1) bm3d_filter_kernel<1><<<fgrid, 32 * kFilterWarps, fs1, st>>>(fa, pxh, py);
-                else bm3d_filter_kernel<2><<<fgrid, 32 * kFilterWarps, fs2, st>>>(fa, pxh, py);
+                if (p.tensor) {
+                    if (stage == 1) bm3d_filter_tc_kernel<1><<<fgrid, 32 * kTcWarps, ts1, st>>>(fa, tables, pxh, py);
+                    else bm3d_filter_tc_kernel<2><<<fgrid, 32 * kTcWarps, ts2, st>>>(fa, tables, pxh, py);
+                } else {
+                    if (stage == 1) bm3d_filter_kernel<1><<<fgrid, 32 * kFilterWarps, fs1, st>>>(fa, pxh, py);
+                    else bm3d_filter_kernel<2><<<fgrid, 32 * kFilterWarps, fs2, st>>>(fa, pxh, py);
+                }
             }
         if (stage == 1 && p.stages == 2)
             bm3d_basic_kernel<<<(unsigned)((npx + 255) / 256), 256, 0, st>>>(acc, basic, q, npx, gate);

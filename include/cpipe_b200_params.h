@@ -173,7 +173,8 @@ typedef struct {
     int32_t nstep;      /* reference-block step, 1..8 (3) */
     float kaiser_beta;  /* aggregation window parameter (2.0) */
     int32_t stages;     /* 1 = hard threshold only, 2 = hard threshold then Wiener */
-    int32_t reserved;   /* 0 */
+    int32_t transform;  /* 0 = DCT/Haar on the tensor cores (FP16 hi/lo split products, FP32
+                           accumulation); 1 = FP32 on the CUDA cores.  Same definition. */
 } cpipe_Bm3dSpecParams;
 
 /* Learned surrogate denoiser weights (no reference counterpart: the

@@ -131,3 +131,21 @@ def test_bm3d_spec_full_frame_12mp(cuda_device):
     want = oracle.bm3d_spec(crop, blob)
     inner = slice(margin, n - margin)
     compare(got[y0:y0 + n, x0:x0 + n][inner, inner].astype(np.float32), want[inner, inner], "12MP crop interior")
+
+
+@pytest.mark.parametrize("h,w,sigma,kw", [(96, 128, 0.03, {}), (77, 101, 0.05, dict(stages=1)),
+                                          (50, 61, 0.02, dict(n2=4, nstep=2))])
+def test_bm3d_precision_forms_against_fp64(cuda_device, h, w, sigma, kw):
+    """Both transform forms against the FP64 oracle on the same input: the
+    tensor-core form (FP16 hi/lo split products, FP32 accumulation) and the FP32
+    CUDA-core form; binary16 and float32 frames.  The per-form error is printed."""
+    clean = clean_rgb(h + 3 * w, h, w)
+    for dtype in (np.float16, np.float32):
+        x = noisy_rgba(clean, sigma, h * w, dtype=dtype)
+        want = oracle.bm3d_spec(x.astype(np.float32), blobs.bm3d_spec(sigma, **kw))
+        errs = {}
+        for form in ("tensor", "fp32"):
+            got = gpu_bm3d(x, blobs.bm3d_spec(sigma, transform=form, **kw)).astype(np.float32)
+            errs[form] = compare(got, want, f"{form} {np.dtype(dtype).name} {w}x{h} {kw}")
+        if dtype == np.float32:
+            assert errs["tensor"][0] <= 2e-3 and errs["fp32"][0] <= 1e-3
