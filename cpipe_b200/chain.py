@@ -85,6 +85,7 @@ class ChainConfig:
     bm3d_stages: int = 2
     surrogate_blob: bytes = None   # trained network (cpipe_b200.surrogate) for denoise="surrogate"
     stop_after: int = 0            # 1: output the denoiser's input; 2: the denoiser's output
+    quad_bayer: bool = False       # raw input is a Sony Quad-Bayer mosaic, remosaiced first
     spot_tiles: int = 16           # surrogate spot check: BM3D on this many 256x256 tiles per frame
     spot_min_psnr_db: float = 40.0  # ... and BM3D for the whole frame when a tile is below this
 
@@ -99,6 +100,15 @@ class ChainConfig:
         base = dict(width=w, height=h, name=f"small_frame_{w}x{h}", wavelet_strength=1.0)
         base.update(kw)
         return cls(**base)
+
+    @classmethod
+    def qbc_50mp(cls, **kw):
+        """8160x6120 Sony Quad-Bayer 10-bit frame (the 12 MP workload's scene,
+        noise, GainMap, warp, guided, wavelet and LUT), remosaiced to RGGB by
+        demosaic.quad_bayer_remosaic ahead of the chain."""
+        base = dict(width=8160, height=6120, name="qbc_chain_50mp_8160x6120", quad_bayer=True)
+        base.update(kw)
+        return cls.full_12mp(**base)
 
     @classmethod
     def full_12mp(cls, **kw):
@@ -123,7 +133,8 @@ class ChainConfig:
 
     def make_raw(self, seed=None):
         return raw_frame(self.width, self.height, self.seed if seed is None else seed, bits=self.bits,
-                         black=int(self.black), a=self.noise_a, b=self.noise_b, cfa=self.cfa)
+                         black=int(self.black), a=self.noise_a, b=self.noise_b, cfa=self.cfa,
+                         quad_bayer=self.quad_bayer)
 
     @property
     def neutral(self):
@@ -231,6 +242,7 @@ class ChainConfig:
         cfg.stop_after = int(self.stop_after)
         cfg.spot_tiles = int(self.spot_tiles)
         cfg.spot_min_psnr_db = float(self.spot_min_psnr_db)
+        cfg.quad_bayer = int(self.quad_bayer)
         return cfg, keep
 
 

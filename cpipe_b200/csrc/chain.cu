@@ -387,6 +387,7 @@ struct cpipe_cuda_chain {
     void* d_mid[2] = {nullptr, nullptr};  // K1 output, K2 output (scratch frames)
     int denoise_mode = 0;
     int stop_after = 0;
+    void* d_bayer = nullptr;              // remosaiced Bayer frame (Quad-Bayer input)
     Bm3dPlan bm3d{};
     void* d_denoise = nullptr;            // scratch of the mode-1 denoiser
     SurrogateNet* sg = nullptr;           // mode-2 network
@@ -435,7 +436,13 @@ int launch_chain(cpipe_cuda_chain* c, const void* d_raw, size_t raw_pitch, void*
     if (ev) cudaEventRecord(ev[0], st);
     const int w = c->cfg.width, h = c->cfg.height;
     const int elem = c->f16 ? 2 : 4;
-    const Img raw{const_cast<void*>(d_raw), w, h, (long long)(raw_pitch ? raw_pitch / 2 : (size_t)w), 1};
+    Img raw{const_cast<void*>(d_raw), w, h, (long long)(raw_pitch ? raw_pitch / 2 : (size_t)w), 1};
+    if (c->d_bayer) {  // demosaic.quad_bayer_remosaic (u16 -> u16) ahead of the Bayer chain
+        const Img bayer{c->d_bayer, w, h, (long long)w, 1};
+        const cudaError_t e = launch_qbc_remosaic(raw, bayer, st);
+        if (e != cudaSuccess) return cuda_status(e, "chain remosaic");
+        raw = bayer;
+    }
     const Img mid0{c->d_mid[0], w, h, (long long)w * 4, 4};
     const Img mid1{c->d_mid[1], w, h, (long long)w * 4, 4};
     const Img out{d_out, w, h, (long long)(out_pitch ? out_pitch / elem : (size_t)w * 4), 4};
@@ -599,6 +606,8 @@ cpipe_cuda_chain* cpipe_cuda_chain_create(const cpipe_cuda_chain_config* cfg, in
     std::memcpy(c->color.cm, cfg->colormatrix, sizeof(c->color.cm));
     c->denoise_mode = cfg->denoise_mode;
     c->stop_after = cfg->stop_after;
+    if (cfg->quad_bayer && cudaMalloc(&c->d_bayer, (size_t)w * h * sizeof(uint16_t)) != cudaSuccess)
+        return fail(CPIPE_OOM, c);
     if (c->denoise_mode < 0 || c->denoise_mode > 2) return fail(CPIPE_UNSUPPORTED, c);
     if (c->stop_after < 0 || c->stop_after > 2 || (c->stop_after == 2 && c->denoise_mode == 0))
         return fail(CPIPE_UNSUPPORTED, c);
@@ -671,6 +680,7 @@ void cpipe_cuda_chain_destroy(cpipe_cuda_chain* c) {
     if (c->graph) cudaGraphExecDestroy(c->graph);
     cudaFree(c->d_tables);
     cudaFree(c->d_denoise);
+    cudaFree(c->d_bayer);
     cudaFree(c->d_ab);
     cudaFree(c->d_tile_in);
     cudaFree(c->d_tile_ref);

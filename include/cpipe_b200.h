@@ -228,6 +228,10 @@ typedef struct {
      * synchronisation); 0 tiles: no check. */
     int32_t spot_tiles;
     float spot_min_psnr_db;
+    /* 1: the raw input is a Sony Quad-Bayer mosaic (4x4 CFA repeat); the chain
+     * starts with demosaic.quad_bayer_remosaic to an RGGB Bayer frame (then
+     * `black.cfa_pattern` must be RGGB). */
+    int32_t quad_bayer;
 } cpipe_cuda_chain_config;
 
 typedef struct cpipe_cuda_chain cpipe_cuda_chain;

@@ -12,6 +12,8 @@ import oracle
 def run_chain_oracle(cfg, raw, blobs=None):
     b = blobs or cfg.blobs()
     f16 = not cfg.plain_f32
+    if getattr(cfg, "quad_bayer", False):
+        raw = oracle.qbc_remosaic(raw)
     x = oracle.r16u_to_f32(raw)
     st, x = oracle.blacklevel(x, b["blacklevel"])
     assert st == 0

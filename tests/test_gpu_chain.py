@@ -4,6 +4,8 @@ frames (including odd sizes) are compared element by element; the full 12 MP
 workload is compared with the oracle and checked for the size-independent
 properties: fused == unfused bit for bit, deterministic, graph replay equal to
 direct launch, finite and in [0, 1]."""
+import os
+
 import numpy as np
 import pytest
 from chain_oracle import run_chain_oracle
@@ -177,3 +179,50 @@ def test_chain_with_two_stage_bm3d(host, demosaic):
     print(f"bm3d chain {demosaic}: vs nodes {p_nodes:.1f} dB, vs oracle {p_oracle:.1f} dB")
     assert p_nodes >= 60.0 and p_oracle >= 50.0
     np.testing.assert_array_equal(got[..., 3], want[..., 3])
+
+
+def test_chain_quad_bayer_matches_oracle(cuda_device):
+    """A Quad-Bayer raw frame: demosaic.quad_bayer_remosaic (integer, bit-exact)
+    then the Bayer chain, against the oracle chain."""
+    cfg = ChainConfig.small(200, 148, quad_bayer=True)
+    raw = cfg.make_raw()
+    chain = Chain(cfg)
+    got = chain.run_host(raw)
+    assert_f16_parity(got, run_chain_oracle(cfg, raw), what="quad bayer chain")
+    chain.close()
+
+
+def test_qbc_50mp_remosaic_and_bm3d_precision_forms(cuda_device):
+    """The 50 MP case: an 8160x6120 Quad-Bayer frame.  The remosaic is bit-exact
+    against the oracle over the whole frame; the chain runs to the end with finite
+    output; and the two-stage BM3D of the chain's denoiser input, in its
+    tensor-core form (FP16 hi/lo split) and its FP32 CUDA-core form, is compared
+    with the FP64 oracle on the interior of a reference-grid-aligned crop (the
+    error of each form is printed)."""
+    import oracle as O
+    from bm3d_scenes import psnr as bpsnr
+    from cpipe_b200 import blobs, call_filter, last_error
+    cfg = ChainConfig.qbc_50mp()
+    raw = cfg.make_raw()
+    bayer = np.zeros_like(raw)
+    assert call_filter("demosaic_quad_bayer_remosaic", [raw], [bayer]) == 0, last_error()
+    np.testing.assert_array_equal(bayer, O.qbc_remosaic(raw))
+    full = Chain(cfg)
+    out = full.run_host(raw)
+    assert np.isfinite(out.astype(np.float32)).all()
+    full.close()
+    front = Chain(ChainConfig.qbc_50mp(stop_after=1))
+    x = front.run_host(raw)
+    front.close()
+    y0, x0, n, margin = 3000, 4200, 420, 2 * (2 * 19 + 8)
+    crop = x[y0:y0 + n, x0:x0 + n].astype(np.float32)
+    want = O.bm3d_spec(crop, blobs.bm3d_spec(cfg.bm3d_sigma))
+    inner = slice(margin, n - margin)
+    for form in ("tensor", "fp32"):
+        got = np.zeros_like(x)
+        assert call_filter("denoise_bm3d_spec", [x], [got], blobs.bm3d_spec(cfg.bm3d_sigma, transform=form)) == 0
+        g = got[y0:y0 + n, x0:x0 + n][inner, inner].astype(np.float64)[..., :3]
+        w_ = want[inner, inner][..., :3]
+        err, p = float(np.abs(g - w_).max()), bpsnr(g, w_)
+        print(f"50 MP BM3D {form}: max-abs {err:.3g} PSNR {p:.1f} dB vs FP64 oracle")
+        assert p >= 55.0 and err <= 5e-3
