@@ -203,6 +203,52 @@ def psnr(a, b):
     return float("inf") if mse == 0.0 else 10.0 * np.log10(1.0 / mse)
 
 
+def batched_form():
+    """The 64-frame uneven batch (cpipe_b200.batch): aggregate MP/s of one launch
+    per stage over all frames, per-frame latency alone."""
+    from cpipe_b200 import batch as B
+    r = B.measure(64, 3)
+    r.pop("sizes_mp", None)
+    return r
+
+
+def qbc_50mp(weights):
+    """8160x6120 Quad-Bayer frame (remosaic + chain), generated on the device:
+    ms/frame of the reference-computation chain and of the surrogate chain."""
+    from cpipe_b200 import _abi as A
+    from cpipe_b200 import batch as B
+    from cpipe_b200.chain import Chain, ChainConfig
+    L = A.lib()
+    out = {"frame": "8160x6120 Quad Bayer 10-bit"}
+    d_raw, d_out = C.c_void_p(), C.c_void_p()
+    cfg0 = ChainConfig.qbc_50mp()
+    assert L.cpipe_cuda_device_alloc(cfg0.width * cfg0.height * 2, C.byref(d_raw)) == 0
+    assert L.cpipe_cuda_device_alloc(cfg0.width * cfg0.height * 8, C.byref(d_out)) == 0
+    B.scene_raw(d_raw.value, cfg0, "qbc")
+    e0, e1 = C.c_void_p(), C.c_void_p()
+    L.cpipe_cuda_event_create(C.byref(e0))
+    L.cpipe_cuda_event_create(C.byref(e1))
+    for mode in ("box2x2", "surrogate"):
+        ch = Chain(ChainConfig.qbc_50mp(denoise=mode, surrogate_blob=weights))
+        for _ in range(2):
+            ch.run(d_raw.value, d_out.value)
+        L.cpipe_cuda_event_record(e0, None)
+        for _ in range(3):
+            ch.run(d_raw.value, d_out.value)
+        L.cpipe_cuda_event_record(e1, None)
+        ms = C.c_float()
+        L.cpipe_cuda_event_elapsed_ms(e0, e1, C.byref(ms))
+        key = "reference_computation_chain_ms" if mode == "box2x2" else "surrogate_chain_ms"
+        out[key] = round(ms.value / 3, 3)
+        if mode == "surrogate":
+            f, fb, worst = ch.denoise_stats()
+            out["spot_check"] = {"frames": f, "fallbacks_to_bm3d": fb, "worst_tile_psnr_db": round(worst, 2)}
+        ch.close()
+    L.cpipe_cuda_device_free(d_raw)
+    L.cpipe_cuda_device_free(d_out)
+    return out
+
+
 def b200_arm(args):
     import numpy as np
     rank, world, local = rank_env(args.gpus)
@@ -370,6 +416,9 @@ def b200_arm(args):
         "clocks": clk,
         "gpu_launches": 65 * args.steps,  # K1, K2, K3, 9 denoiser, 3 spot check, 2 x 25 BM3D (tiles; gated fallback)
     }
+    if rank == 0 and world == 1 and not args.no_extra:
+        line["batched_form"] = batched_form()
+        line["qbc_50mp"] = qbc_50mp(weights)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sample = ChainConfig.full_12mp(width=2016, height=1512, name="sample_2016x1512")
         scale = (w * h) / (sample.width * sample.height)
@@ -396,6 +445,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extra", action="store_true", help="skip the batched-form and 50 MP measurements")
     args = ap.parse_args()
     if args.impl == "reference":
         return reference_arm(args)

@@ -156,7 +156,7 @@ EXPORTS = [
     "cpipe_cuda_tone_filmic_rgb", "cpipe_cuda_copy", "cpipe_cuda_filters", "cpipe_cuda_find_filter",
     "cpipe_cuda_color_3d_lut_noalloc",
     "cpipe_b200_node_descs", "cpipe_b200_find_node",
-    "cpipe_cuda_scene_raw", "cpipe_surrogate_blob_size", "cpipe_surrogate_create", "cpipe_surrogate_destroy", "cpipe_surrogate_export",
+    "cpipe_cuda_scene_raw", "cpipe_cuda_scene_raw_cfa", "cpipe_surrogate_blob_size", "cpipe_surrogate_create", "cpipe_surrogate_destroy", "cpipe_surrogate_export",
     "cpipe_surrogate_denoise", "cpipe_surrogate_set_engine", "cpipe_surrogate_check", "cpipe_surrogate_profile", "cpipe_surrogate_train_step", "cpipe_surrogate_gradients",
     "cpipe_b200_wb_prepare", "cpipe_b200_colormatrix_compose", "cpipe_b200_pack_gain_maps",
     "cpipe_b200_pack_opcode_list_3", "cpipe_b200_load_lut",
@@ -173,7 +173,8 @@ EXPORTS = [
     "cpipe_b200_host_last_error",
     "cpipe_cuda_chain_create", "cpipe_cuda_chain_destroy", "cpipe_cuda_chain_output_bytes", "cpipe_cuda_chain_run",
     "cpipe_cuda_chain_run_host", "cpipe_cuda_pinned_alloc", "cpipe_cuda_pinned_free",
-    "cpipe_cuda_chain_set_profiling", "cpipe_cuda_chain_profile", "cpipe_cuda_chain_denoise_stats", "cpipe_cuda_set_device", "cpipe_cuda_device_alloc",
+    "cpipe_cuda_batch_create", "cpipe_cuda_batch_destroy", "cpipe_cuda_batch_run", "cpipe_cuda_batch_autotune",
+    "cpipe_cuda_batch_frame_chain", "cpipe_cuda_chain_set_profiling", "cpipe_cuda_chain_profile", "cpipe_cuda_chain_denoise_stats", "cpipe_cuda_set_device", "cpipe_cuda_device_alloc",
     "cpipe_cuda_device_free", "cpipe_cuda_memcpy_h2d", "cpipe_cuda_memcpy_d2h", "cpipe_cuda_memcpy_d2d_async", "cpipe_cuda_count_nonfinite",
     "cpipe_cuda_stream_create",
     "cpipe_cuda_stream_destroy", "cpipe_cuda_stream_synchronize", "cpipe_cuda_event_create",
@@ -232,6 +233,9 @@ def lib():
         "cpipe_cuda_chain_run": (i32, [vp, vp, vp, vp]), "cpipe_cuda_chain_run_host": (i32, [vp, vp, vp, vp]),
         "cpipe_cuda_pinned_alloc": (i32, [sz, C.POINTER(vp)]), "cpipe_cuda_pinned_free": (None, [vp]),
         "cpipe_cuda_chain_set_profiling": (i32, [vp, i32]),
+        "cpipe_cuda_batch_create": (vp, [vp, sz, C.POINTER(i32)]), "cpipe_cuda_batch_destroy": (None, [vp]),
+        "cpipe_cuda_batch_run": (i32, [vp, vp, vp, vp]), "cpipe_cuda_batch_autotune": (i32, [vp, vp, vp, vp, vp]),
+        "cpipe_cuda_batch_frame_chain": (vp, [vp, sz]),
         "cpipe_cuda_chain_profile": (i32, [vp, C.POINTER(C.c_double), C.POINTER(i32)]),
         "cpipe_cuda_chain_denoise_stats": (i32, [vp, C.POINTER(u32), C.POINTER(u32), C.POINTER(C.c_float)]),
         "cpipe_cuda_set_device": (i32, [i32]), "cpipe_cuda_device_alloc": (i32, [sz, C.POINTER(vp)]),
@@ -243,6 +247,8 @@ def lib():
         "cpipe_cuda_event_record": (i32, [vp, vp]),
         "cpipe_cuda_event_elapsed_ms": (i32, [vp, vp, C.POINTER(C.c_float)]),
         "cpipe_cuda_scene_raw": (i32, [vp, i32, i32, C.c_uint64, i32, i32, C.c_float, C.c_float, vp, i32, vp]),
+        "cpipe_cuda_scene_raw_cfa": (i32, [vp, i32, i32, C.c_uint64, i32, i32, C.c_float, C.c_float, vp, i32, i32,
+                                           vp]),
         "cpipe_surrogate_blob_size": (sz, []), "cpipe_surrogate_create": (vp, [vp, sz, C.POINTER(i32)]),
         "cpipe_surrogate_destroy": (None, [vp]), "cpipe_surrogate_export": (i32, [vp, vp, sz]),
         "cpipe_surrogate_denoise": (i32, [vp, vp, vp, i32, i32, i32, i32, vp, vp]),

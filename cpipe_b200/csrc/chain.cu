@@ -63,9 +63,8 @@ struct ColorParams {
 };
 
 template <class T, bool F16, bool WARP>
-__global__ void __launch_bounds__(128) warp_wb_cm_kernel(Img in, Img out, WarpDev w, ColorParams cp) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-    if (x >= out.w) return;
+__device__ __forceinline__ void warp_wb_cm_px(const Img& in, const Img& out, const WarpDev& w, const ColorParams& cp,
+                                              int x, int y) {
     Rgba v;
     if (WARP) {
         const Rgba wv = warp_px<T>(in, w, x, y);
@@ -77,6 +76,13 @@ __global__ void __launch_bounds__(128) warp_wb_cm_kernel(Img in, Img out, WarpDe
     b = Rgba{rnd<F16>(b.r), rnd<F16>(b.g), rnd<F16>(b.b), v.a};
     const Rgba c = cm_px(b, cp.cm);
     store_rgba(px<T>(out, x, y), Rgba{c.r, c.g, c.b, v.a});
+}
+
+template <class T, bool F16, bool WARP>
+__global__ void __launch_bounds__(128) warp_wb_cm_kernel(Img in, Img out, WarpDev w, ColorParams cp) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= out.w) return;
+    warp_wb_cm_px<T, F16, WARP>(in, out, w, cp, x, y);
 }
 
 // ------------------------------------------------------------------ K3
@@ -155,17 +161,17 @@ __device__ __forceinline__ void load_pair<float>(const Img& in, int x, int y, Rg
     *b = load_rgba(px<const float>(in, x + 1, y));
 }
 
+// One kCTW x kCTH output tile at (x0, y0); smem_f: denoise_tone_smem bytes.
 template <class T, bool F16, int R>
-__global__ void __launch_bounds__(256, 3) denoise_tone_kernel(Img in, Img out, ToneParams p) {
+__device__ __forceinline__ void denoise_tone_tile(const Img& in, const Img& out, const ToneParams& p, int x0, int y0,
+                                                  float* smem_f) {
     using Gm = ToneGeom<R>;
     constexpr int H = Gm::H, CW = Gm::CW, CH = Gm::CH, CP = Gm::CP, AW = Gm::AW, AH = Gm::AH, AP = Gm::AP;
     constexpr int AB = Gm::AB, D = Gm::D;
-    extern __shared__ __align__(16) float smem_f[];
     float* s_bm = smem_f;
     float* s_a = s_bm + 3 * CP * CH;
     float* s_b = s_a + 3 * AB;
     float* s_gf = s_b + 3 * AB;
-    const int x0 = blockIdx.x * kCTW, y0 = blockIdx.y * kCTH;
     const int cx0 = x0 - H, cy0 = y0 - H;
     const float s = p.bm3d_strength;
     // 1) BM3D parity form (bm3d_step1_generator.cpp:42-56) per 2x2 block of the extent
@@ -305,6 +311,12 @@ __global__ void __launch_bounds__(256, 3) denoise_tone_kernel(Img in, Img out, T
         }
         store_rgba(px<T>(out, x, y), v);
     }
+}
+
+template <class T, bool F16, int R>
+__global__ void __launch_bounds__(256, 3) denoise_tone_kernel(Img in, Img out, ToneParams p) {
+    extern __shared__ __align__(16) float smem_f[];
+    denoise_tone_tile<T, F16, R>(in, out, p, (int)blockIdx.x * kCTW, (int)blockIdx.y * kCTH, smem_f);
 }
 
 template <class T, bool F16, int R>
@@ -874,5 +886,340 @@ int cpipe_cuda_pinned_alloc(size_t bytes, void** out) {
     return cudaHostAlloc(out, bytes, cudaHostAllocDefault) == cudaSuccess ? CPIPE_OK : CPIPE_OOM;
 }
 void cpipe_cuda_pinned_free(void* p) { cudaFreeHost(p); }
+
+}  // extern "C"
+
+// ------------------------------------------------------------- batched form
+// Frames of any size, CFA and bit depth through the same chain in one launch
+// per stage: persistent kernels walk a queue of (frame, tile) work items.
+// Tile t belongs to the frame f with prefix[f] <= t < prefix[f + 1] (binary
+// search over the per-frame tile counts); the frame's descriptor (buffers and
+// node parameters) is copied to shared memory when a CTA moves to a new frame.
+// Per frame, the host-side preparation is that of a single-frame chain
+// (cpipe_cuda_chain_create), whose intermediate frames the batch uses.
+namespace cpb {
+namespace batch {
+
+constexpr int kMaxFrames = 64;
+constexpr int kK2Rows = 8;  // stage-2 work item: 128 pixels x 8 rows
+
+struct Frame {
+    Img bayer, mid0, mid1, out;  // bayer: the raw input, or its remosaic for Quad-Bayer frames
+    RawParams raw;
+    WarpDev warp;
+    ColorParams color;
+    ToneParams tone;
+    int t1x, t2x, t3x;  // work items per row, per stage
+    int pad;
+};
+
+__device__ __forceinline__ int find_frame(const int* prefix, int n, int t) {
+    int lo = 0, hi = n - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (prefix[mid] <= t) lo = mid;
+        else hi = mid - 1;
+    }
+    return lo;
+}
+
+// Work item t of this stage: returns its frame's local index, having loaded
+// the frame descriptor into s_f when the frame changed (uniform per CTA).
+__device__ __forceinline__ int next_item(const Frame* __restrict__ frames, const int* s_prefix, int n, int t,
+                                         Frame* s_f, int* cur) {
+    const int f = find_frame(s_prefix, n, t);
+    if (f != *cur) {
+        __syncthreads();
+        const int* src = reinterpret_cast<const int*>(frames + f);
+        int* dst = reinterpret_cast<int*>(s_f);
+        for (int i = threadIdx.x; i < (int)(sizeof(Frame) / 4); i += blockDim.x) dst[i] = src[i];
+        *cur = f;
+        __syncthreads();
+    }
+    return t - s_prefix[f];
+}
+
+template <int ALGO>
+__global__ void __launch_bounds__(256) batch_raw_kernel(const Frame* __restrict__ frames,
+                                                        const int* __restrict__ prefix, int n) {
+    __shared__ int s_prefix[kMaxFrames + 1];
+    __shared__ Frame s_f;
+    for (int i = threadIdx.x; i <= n; i += blockDim.x) s_prefix[i] = prefix[i];
+    __syncthreads();
+    int cur = -1;
+    for (int t = blockIdx.x; t < s_prefix[n]; t += gridDim.x) {
+        const int local = next_item(frames, s_prefix, n, t, &s_f, &cur);
+        demosaic_tile_at<ALGO, __half>(RawLoader{s_f.bayer, &s_f.raw}, s_f.bayer.w, s_f.bayer.h, s_f.mid0, s_f.raw.cfa,
+                                       (local % s_f.t1x) * kDmTW, (local / s_f.t1x) * kDmTH);
+        __syncthreads();
+    }
+}
+
+template <bool WARP>
+__global__ void __launch_bounds__(128) batch_color_kernel(const Frame* __restrict__ frames,
+                                                          const int* __restrict__ prefix, int n) {
+    __shared__ int s_prefix[kMaxFrames + 1];
+    __shared__ Frame s_f;
+    for (int i = threadIdx.x; i <= n; i += blockDim.x) s_prefix[i] = prefix[i];
+    __syncthreads();
+    int cur = -1;
+    for (int t = blockIdx.x; t < s_prefix[n]; t += gridDim.x) {
+        const int local = next_item(frames, s_prefix, n, t, &s_f, &cur);
+        const int x = (local % s_f.t2x) * 128 + (int)threadIdx.x, y0 = (local / s_f.t2x) * kK2Rows;
+        if (x < s_f.mid1.w)
+            for (int r = 0; r < kK2Rows && y0 + r < s_f.mid1.h; ++r)
+                warp_wb_cm_px<__half, true, WARP>(s_f.mid0, s_f.mid1, s_f.warp, s_f.color, x, y0 + r);
+    }
+}
+
+template <int R>
+__global__ void __launch_bounds__(256, 3) batch_tone_kernel(const Frame* __restrict__ frames,
+                                                            const int* __restrict__ prefix, int n) {
+    extern __shared__ __align__(16) float smem_f[];
+    __shared__ int s_prefix[kMaxFrames + 1];
+    __shared__ Frame s_f;
+    for (int i = threadIdx.x; i <= n; i += blockDim.x) s_prefix[i] = prefix[i];
+    __syncthreads();
+    int cur = -1;
+    for (int t = blockIdx.x; t < s_prefix[n]; t += gridDim.x) {
+        const int local = next_item(frames, s_prefix, n, t, &s_f, &cur);
+        denoise_tone_tile<__half, true, R>(s_f.mid1, s_f.out, s_f.tone, (local % s_f.t3x) * kCTW,
+                                           (local / s_f.t3x) * kCTH, smem_f);
+        __syncthreads();
+    }
+}
+
+}  // namespace batch
+}  // namespace cpb
+
+struct cpipe_cuda_batch {
+    std::vector<cpipe_cuda_chain*> chains;
+    std::vector<cpb::batch::Frame> frames;
+    cpb::batch::Frame* d_frames = nullptr;
+    int* d_prefix = nullptr;  // three arrays of n + 1
+    int n = 0, algo = 1, radius = 2;
+    bool warp = false;
+    int per_sm[3] = {2, 8, 3};  // persistent CTAs per SM for the three stages (autotuned)
+    cudaGraphExec_t graph = nullptr;
+    std::vector<const void*> graph_in;
+    std::vector<void*> graph_out;
+    cudaStream_t graph_stream = nullptr;
+};
+
+namespace {
+
+using cpb::batch::Frame;
+
+int batch_launch_stage(cpipe_cuda_batch* b, int stage, cudaStream_t st) {
+    const int grid = kSmCount * b->per_sm[stage];
+    const int* pf = b->d_prefix + stage * (b->n + 1);
+    if (stage == 0) {
+        if (b->algo == 0) cpb::batch::batch_raw_kernel<0><<<grid, 256, 0, st>>>(b->d_frames, pf, b->n);
+        else if (b->algo == 1) cpb::batch::batch_raw_kernel<1><<<grid, 256, 0, st>>>(b->d_frames, pf, b->n);
+        else cpb::batch::batch_raw_kernel<2><<<grid, 256, 0, st>>>(b->d_frames, pf, b->n);
+    } else if (stage == 1) {
+        if (b->warp) cpb::batch::batch_color_kernel<true><<<grid, 128, 0, st>>>(b->d_frames, pf, b->n);
+        else cpb::batch::batch_color_kernel<false><<<grid, 128, 0, st>>>(b->d_frames, pf, b->n);
+    } else {
+        if (b->radius == 0)
+            cpb::batch::batch_tone_kernel<0><<<grid, 256, denoise_tone_smem<__half, true, 0>(), st>>>(b->d_frames, pf, b->n);
+        else if (b->radius == 1)
+            cpb::batch::batch_tone_kernel<1><<<grid, 256, denoise_tone_smem<__half, true, 1>(), st>>>(b->d_frames, pf, b->n);
+        else
+            cpb::batch::batch_tone_kernel<2><<<grid, 256, denoise_tone_smem<__half, true, 2>(), st>>>(b->d_frames, pf, b->n);
+    }
+    return cuda_status(cudaGetLastError(), "batch stage");
+}
+
+int batch_launch(cpipe_cuda_batch* b, cudaStream_t st) {
+    for (int i = 0; i < b->n; ++i) {  // demosaic.quad_bayer_remosaic for Quad-Bayer frames
+        cpipe_cuda_chain* c = b->chains[i];
+        if (c->d_bayer) {
+            const cudaError_t e = launch_qbc_remosaic(Img{const_cast<void*>(b->graph_in[i]), c->cfg.width, c->cfg.height,
+                                                          (long long)c->cfg.width, 1},
+                                                      b->frames[i].bayer, st);
+            if (e != cudaSuccess) return cuda_status(e, "batch remosaic");
+        }
+    }
+    for (int stage = 0; stage < 3; ++stage) {
+        const int s = batch_launch_stage(b, stage, st);
+        if (s != CPIPE_OK) return s;
+    }
+    return CPIPE_OK;
+}
+
+template <int R>
+cudaError_t allow_batch_smem() {
+    cudaError_t e = cudaFuncSetAttribute(cpb::batch::batch_tone_kernel<R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)denoise_tone_smem<__half, true, R>());
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(cpb::batch::batch_tone_kernel<R>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                 cudaSharedmemCarveoutMaxShared);
+    return e;
+}
+
+}  // namespace
+
+extern "C" {
+
+void cpipe_cuda_batch_destroy(cpipe_cuda_batch* b) {
+    if (!b) return;
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    for (cpipe_cuda_chain* c : b->chains) cpipe_cuda_chain_destroy(c);
+    cudaFree(b->d_frames);
+    cudaFree(b->d_prefix);
+    delete b;
+}
+
+cpipe_cuda_batch* cpipe_cuda_batch_create(const cpipe_cuda_chain_config* cfgs, size_t n, int* status) {
+    auto fail = [&](int st, cpipe_cuda_batch* b) -> cpipe_cuda_batch* {
+        if (status) *status = st;
+        cpipe_cuda_batch_destroy(b);
+        return nullptr;
+    };
+    if (!cfgs || n == 0 || n > (size_t)cpb::batch::kMaxFrames) return fail(CPIPE_BAD_INDEX, nullptr);
+    auto* b = new (std::nothrow) cpipe_cuda_batch();
+    if (!b) return fail(CPIPE_OOM, nullptr);
+    b->n = (int)n;
+    std::vector<int> prefix(3 * (n + 1), 0);
+    for (size_t i = 0; i < n; ++i) {
+        cpipe_cuda_chain_config c = cfgs[i];
+        if (c.plain_f32 || c.denoise_mode != 0 || c.stop_after != 0) {
+            set_error("batch: %s", "frames run the parity chain (binary16, the reference's denoise.bm3d)");
+            return fail(CPIPE_UNSUPPORTED, b);
+        }
+        c.use_graph = 0;
+        int st = CPIPE_OK;
+        cpipe_cuda_chain* ch = cpipe_cuda_chain_create(&c, &st);
+        if (!ch) return fail(st, b);
+        b->chains.push_back(ch);
+        if (i == 0) {
+            b->algo = ch->algo;
+            b->radius = ch->radius;
+            b->warp = ch->warp_mode == 1;
+        }
+        if (ch->algo != b->algo || ch->radius != b->radius || (ch->warp_mode == 1) != b->warp || ch->warp_mode == 2) {
+            set_error("batch: %s", "all frames need the same demosaic, guided radius class and warp form");
+            return fail(CPIPE_UNSUPPORTED, b);
+        }
+        const int w = c.width, h = c.height;
+        Frame f{};
+        f.mid0 = Img{ch->d_mid[0], w, h, (long long)w * 4, 4};
+        f.mid1 = Img{ch->d_mid[1], w, h, (long long)w * 4, 4};
+        f.raw = ch->raw;
+        f.warp = ch->warp;
+        f.color = ch->color;
+        f.tone = ch->tone;
+        f.t1x = (w + kDmTW - 1) / kDmTW;
+        f.t2x = (w + 127) / 128;
+        f.t3x = (w + kCTW - 1) / kCTW;
+        b->frames.push_back(f);
+        prefix[0 * (n + 1) + i + 1] = prefix[0 * (n + 1) + i] + f.t1x * ((h + kDmTH - 1) / kDmTH);
+        prefix[1 * (n + 1) + i + 1] = prefix[1 * (n + 1) + i] + f.t2x * ((h + cpb::batch::kK2Rows - 1) / cpb::batch::kK2Rows);
+        prefix[2 * (n + 1) + i + 1] = prefix[2 * (n + 1) + i] + f.t3x * ((h + kCTH - 1) / kCTH);
+    }
+    if (cudaMalloc(&b->d_frames, sizeof(Frame) * n) != cudaSuccess ||
+        cudaMalloc(&b->d_prefix, sizeof(int) * prefix.size()) != cudaSuccess)
+        return fail(CPIPE_OOM, b);
+    if (cudaMemcpy(b->d_prefix, prefix.data(), sizeof(int) * prefix.size(), cudaMemcpyHostToDevice) != cudaSuccess)
+        return fail(CPIPE_INTERNAL_ERROR, b);
+    cudaError_t e = b->radius == 0 ? allow_batch_smem<0>() : b->radius == 1 ? allow_batch_smem<1>() : allow_batch_smem<2>();
+    if (e != cudaSuccess) return fail(cuda_status(e, "batch smem"), b);
+    if (status) *status = CPIPE_OK;
+    return b;
+}
+
+static int batch_bind(cpipe_cuda_batch* b, const void* const* d_raw, void* const* d_out) {
+    for (int i = 0; i < b->n; ++i) {
+        if (!d_raw[i] || !d_out[i]) return CPIPE_BAD_INDEX;
+        cpipe_cuda_chain* c = b->chains[i];
+        const int w = c->cfg.width, h = c->cfg.height;
+        b->frames[i].bayer = c->d_bayer ? Img{c->d_bayer, w, h, (long long)w, 1}
+                                        : Img{const_cast<void*>(d_raw[i]), w, h, (long long)w, 1};
+        b->frames[i].out = Img{d_out[i], w, h, (long long)w * 4, 4};
+    }
+    b->graph_in.assign(d_raw, d_raw + b->n);
+    b->graph_out.assign(d_out, d_out + b->n);
+    return cuda_status(cudaMemcpy(b->d_frames, b->frames.data(), sizeof(Frame) * b->n, cudaMemcpyHostToDevice),
+                       "batch descriptors");
+}
+
+int cpipe_cuda_batch_run(cpipe_cuda_batch* b, const void* const* d_raw, void* const* d_out, void* stream) {
+    if (!b || !d_raw || !d_out) return CPIPE_BAD_INDEX;
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    bool same = b->graph && b->graph_stream == st;
+    for (int i = 0; same && i < b->n; ++i) same = b->graph_in[i] == d_raw[i] && b->graph_out[i] == d_out[i];
+    if (!same) {
+        if (b->graph) cudaGraphExecDestroy(b->graph);
+        b->graph = nullptr;
+        int s = batch_bind(b, d_raw, d_out);
+        if (s != CPIPE_OK) return s;
+        cudaStream_t cap = st, own = nullptr;
+        if (cap == nullptr) {
+            if (cudaStreamCreateWithFlags(&own, cudaStreamNonBlocking) != cudaSuccess) return CPIPE_INTERNAL_ERROR;
+            cap = own;
+        }
+        cudaGraph_t g;
+        s = cuda_status(cudaStreamBeginCapture(cap, cudaStreamCaptureModeThreadLocal), "batch capture");
+        if (s == CPIPE_OK) {
+            const int ls = batch_launch(b, cap);
+            s = cuda_status(cudaStreamEndCapture(cap, &g), "batch end capture");
+            if (ls != CPIPE_OK) s = ls;
+        }
+        if (s == CPIPE_OK) {
+            s = cuda_status(cudaGraphInstantiate(&b->graph, g, 0), "batch instantiate");
+            cudaGraphDestroy(g);
+        }
+        if (own) cudaStreamDestroy(own);
+        if (s != CPIPE_OK) return s;
+        b->graph_stream = st;
+    }
+    return cuda_status(cudaGraphLaunch(b->graph, st), "batch graph launch");
+}
+
+int cpipe_cuda_batch_autotune(cpipe_cuda_batch* b, const void* const* d_raw, void* const* d_out, void* stream,
+                              int per_sm_out[3]) {
+    if (!b || !d_raw || !d_out) return CPIPE_BAD_INDEX;
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int s = batch_bind(b, d_raw, d_out);
+    if (s != CPIPE_OK) return s;
+    if (b->graph) cudaGraphExecDestroy(b->graph);
+    b->graph = nullptr;
+    static const int cand[3][6] = {{1, 2, 3, 4, 6, 8}, {2, 4, 8, 12, 16, 24}, {1, 2, 3, 4, 6, 8}};
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return CPIPE_INTERNAL_ERROR;
+    s = batch_launch(b, st);  // fills every stage's input once
+    for (int stage = 0; stage < 3 && s == CPIPE_OK; ++stage) {
+        float best = 1e30F;
+        int best_k = b->per_sm[stage];
+        for (int k : cand[stage]) {
+            b->per_sm[stage] = k;
+            float total = 0.0F;
+            for (int r = 0; r < 3 && s == CPIPE_OK; ++r) {
+                cudaEventRecord(e0, st);
+                s = batch_launch_stage(b, stage, st);
+                cudaEventRecord(e1, st);
+                if (cudaEventSynchronize(e1) != cudaSuccess) s = CPIPE_INTERNAL_ERROR;
+                float ms = 0.0F;
+                cudaEventElapsedTime(&ms, e0, e1);
+                if (r > 0) total += ms;  // the first run warms up
+            }
+            if (total < best) {
+                best = total;
+                best_k = k;
+            }
+        }
+        b->per_sm[stage] = best_k;
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (per_sm_out)
+        for (int i = 0; i < 3; ++i) per_sm_out[i] = b->per_sm[i];
+    return s;
+}
+
+cpipe_cuda_chain* cpipe_cuda_batch_frame_chain(cpipe_cuda_batch* b, size_t i) {
+    return (b && i < b->chains.size()) ? b->chains[i] : nullptr;
+}
 
 }  // extern "C"

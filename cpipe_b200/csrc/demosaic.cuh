@@ -24,11 +24,11 @@ struct DmTap {
 // or the AMaZE chroma c - g (demosaic_amaze_generator.cpp:48-49), computed once
 // per cell instead of once per reading pixel (same values).
 template <int ALGO, class TOut, class Loader>
-__device__ __forceinline__ void demosaic_tile(const Loader& load, int w, int h, const Img& out, const Cfa& cfa) {
+__device__ __forceinline__ void demosaic_tile_at(const Loader& load, int w, int h, const Img& out, const Cfa& cfa, int x0,
+                                                 int y0) {
     __shared__ float s_in[kDmIH * kDmIW];
     __shared__ float s_g[kDmGH * kDmGW];
     __shared__ float s_q[kDmGH * kDmGW];
-    const int x0 = blockIdx.x * kDmTW, y0 = blockIdx.y * kDmTH;
     for (int i = threadIdx.x; i < kDmIH * kDmIW; i += blockDim.x) {
         const int ty = i / kDmIW, tx = i - ty * kDmIW;
         s_in[i] = load(clampi(x0 - kDmHalo + tx, 0, w - 1), clampi(y0 - kDmHalo + ty, 0, h - 1));
@@ -88,6 +88,12 @@ __device__ __forceinline__ void demosaic_tile(const Loader& load, int w, int h, 
         }
         store_rgba(px<TOut>(out, x, y), Rgba{r, g, b, 1.0F});
     }
+}
+
+// One kDmTW x kDmTH tile at the block's grid position.
+template <int ALGO, class TOut, class Loader>
+__device__ __forceinline__ void demosaic_tile(const Loader& load, int w, int h, const Img& out, const Cfa& cfa) {
+    demosaic_tile_at<ALGO, TOut>(load, w, h, out, cfa, (int)blockIdx.x * kDmTW, (int)blockIdx.y * kDmTH);
 }
 
 }  // namespace cpb

@@ -4,7 +4,7 @@
 // Scene (the family of the benchmark's CPU generator): linear RGB gradients,
 // `rects` axis-aligned rectangles of uniform reflectance in [0.05, 0.9]
 // painted in order, and a sinusoidal zone plate in the central third; mosaicked
-// with a 2x2 CFA; noise from the model var = a*x + b in normalised units in its
+// with a 2x2 (Bayer) or 4x4 (Quad-Bayer) CFA; noise from the model var = a*x + b in normalised units in its
 // Gaussian form x + sqrt(a*x + b) * N(0, 1); scaled above the black level,
 // rounded and clamped to the white level.  Random numbers come from the
 // counter-based Philox4x32-10 generator (Salmon, Moraes, Dror, Shaw, "Parallel
@@ -59,7 +59,8 @@ struct SceneArgs {
     uint32_t k0, k1;
     float a, b;
     int black, white;
-    uint8_t cfa[4];
+    int rep;            // CFA repeat: 2 (Bayer) or 4 (Quad Bayer)
+    uint8_t cfa[16];    // rep x rep pattern, row-major
     int rx0[kMaxRects], rx1[kMaxRects], ry0[kMaxRects], ry1[kMaxRects];
     float refl[kMaxRects][3];
 };
@@ -86,7 +87,7 @@ __global__ void scene_raw_kernel(SceneArgs s) {
         rgb[1] = zp * 0.85F;
         rgb[2] = zp * 0.8F;
     }
-    const float clean = fminf(fmaxf(rgb[s.cfa[(y & 1) * 2 + (x & 1)]], 0.0F), 1.0F);
+    const float clean = fminf(fmaxf(rgb[s.cfa[(y % s.rep) * s.rep + (x % s.rep)]], 0.0F), 1.0F);
     const uint64_t p = (uint64_t)y * (uint64_t)s.w + (uint64_t)x;
     const Philox4 r = philox((uint32_t)p, (uint32_t)(p >> 32), 3U, 0U, s.k0, s.k1);
     const float u1 = unit(r.v[0]), u2 = unit(r.v[1]);
@@ -101,10 +102,11 @@ __global__ void scene_raw_kernel(SceneArgs s) {
 
 using namespace cpb;
 
-extern "C" int cpipe_cuda_scene_raw(void* d_out, int width, int height, uint64_t seed, int bits, int black,
-                                    float noise_a, float noise_b, const uint8_t cfa[4], int rects, void* stream) {
+extern "C" int cpipe_cuda_scene_raw_cfa(void* d_out, int width, int height, uint64_t seed, int bits, int black,
+                                        float noise_a, float noise_b, const uint8_t* cfa, int cfa_repeat, int rects,
+                                        void* stream) {
     if (!d_out || width <= 0 || height <= 0 || bits < 8 || bits > 16 || black < 0 || black >= (1 << bits) - 1 ||
-        rects < 0 || rects > kMaxRects || !cfa)
+        rects < 0 || rects > kMaxRects || !cfa || (cfa_repeat != 2 && cfa_repeat != 4))
         return CPIPE_BAD_INDEX;
     if (!device_ready()) return CPIPE_INTERNAL_ERROR;
     SceneArgs s{};
@@ -118,7 +120,8 @@ extern "C" int cpipe_cuda_scene_raw(void* d_out, int width, int height, uint64_t
     s.b = noise_b;
     s.black = black;
     s.white = (1 << bits) - 1;
-    for (int i = 0; i < 4; ++i) s.cfa[i] = cfa[i] > 2 ? 1 : cfa[i];
+    s.rep = cfa_repeat;
+    for (int i = 0; i < cfa_repeat * cfa_repeat; ++i) s.cfa[i] = cfa[i] > 2 ? 1 : cfa[i];
     for (int i = 0; i < rects; ++i) {
         const Philox4 g = philox((uint32_t)i, 1U, 0U, 0U, s.k0, s.k1);
         const int xa = (int)(g.v[0] % (uint32_t)width), xb = (int)(g.v[1] % (uint32_t)width);
@@ -133,4 +136,9 @@ extern "C" int cpipe_cuda_scene_raw(void* d_out, int width, int height, uint64_t
     const dim3 grid((unsigned)((width + 255) / 256), (unsigned)height);
     scene_raw_kernel<<<grid, 256, 0, static_cast<cudaStream_t>(stream)>>>(s);
     return cuda_status(cudaGetLastError(), "scene_raw");
+}
+
+extern "C" int cpipe_cuda_scene_raw(void* d_out, int width, int height, uint64_t seed, int bits, int black,
+                                    float noise_a, float noise_b, const uint8_t cfa[4], int rects, void* stream) {
+    return cpipe_cuda_scene_raw_cfa(d_out, width, height, seed, bits, black, noise_a, noise_b, cfa, 2, rects, stream);
 }

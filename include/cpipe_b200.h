@@ -261,6 +261,9 @@ int cpipe_cuda_chain_denoise_stats(cpipe_cuda_chain* chain, uint32_t* frames, ui
  * every launch.  No reference counterpart (training data and benchmarks). */
 int cpipe_cuda_scene_raw(void* d_out, int width, int height, uint64_t seed, int bits, int black, float noise_a,
                          float noise_b, const uint8_t cfa[4], int rects, void* stream);
+/* The same with a cfa_repeat x cfa_repeat pattern (2: Bayer, 4: Quad Bayer). */
+int cpipe_cuda_scene_raw_cfa(void* d_out, int width, int height, uint64_t seed, int bits, int black, float noise_a,
+                             float noise_b, const uint8_t* cfa, int cfa_repeat, int rects, void* stream);
 
 /* ---------------------------------------------------------- learned surrogate */
 /* A residual convolutional denoiser that stands in for BM3D (weights:
@@ -295,6 +298,24 @@ int cpipe_surrogate_train_step(cpipe_surrogate* s, const void* d_noisy, const vo
                                int n, int width, int height, float lr, int update, float* loss, void* stream);
 /* Gradients of the last train_step, in blob parameter order. */
 int cpipe_surrogate_gradients(const cpipe_surrogate* s, float* grad, size_t count);
+
+/* ----------------------------------------------------------- batched form */
+/* Up to 64 frames of any size, CFA (Bayer, or Quad Bayer with quad_bayer = 1),
+ * bit depth and noise through the chain (binary16 between nodes, the
+ * reference's denoise.bm3d) in one launch per stage: persistent kernels walk a
+ * queue of (frame, tile) work items.  The frames share the demosaic, the guided
+ * radius class and the warp form.  run() replays one CUDA graph for a given set
+ * of input / output pointers.  autotune() times candidate persistent grid sizes
+ * per stage on the given frames and keeps the fastest (per_sm_out: CTAs per SM
+ * chosen for the three stages). */
+typedef struct cpipe_cuda_batch cpipe_cuda_batch;
+cpipe_cuda_batch* cpipe_cuda_batch_create(const cpipe_cuda_chain_config* cfgs, size_t n, int* status);
+void cpipe_cuda_batch_destroy(cpipe_cuda_batch* batch);
+int cpipe_cuda_batch_run(cpipe_cuda_batch* batch, const void* const* d_raw, void* const* d_out, void* stream);
+int cpipe_cuda_batch_autotune(cpipe_cuda_batch* batch, const void* const* d_raw, void* const* d_out, void* stream,
+                              int per_sm_out[3]);
+/* Frame i's single-frame chain (the same node parameters; for per-frame runs). */
+cpipe_cuda_chain* cpipe_cuda_batch_frame_chain(cpipe_cuda_batch* batch, size_t i);
 
 /* Device memory, streams and events for callers without their own CUDA runtime. */
 int cpipe_cuda_set_device(int device);
