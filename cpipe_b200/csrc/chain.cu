@@ -415,6 +415,10 @@ struct cpipe_cuda_chain {
     float* d_tile_mse = nullptr;
     int* d_gate = nullptr;                // 1: fall back to BM3D for this frame
     SpotStats* d_stats = nullptr;
+    // The tiles' BM3D runs on a second stream beside the network (both read
+    // only the denoiser's input), forked after K2 and joined before the MSE.
+    cudaStream_t spot_stream = nullptr;
+    cudaEvent_t spot_fork = nullptr, spot_join = nullptr;
     void* d_io[2] = {nullptr, nullptr};   // device staging for run_host
     size_t frame_bytes = 0;
     // profiling: 5 events per frame (start, after K1, after K2, after the denoiser, after K3)
@@ -493,18 +497,34 @@ int launch_chain(cpipe_cuda_chain* c, const void* d_raw, size_t raw_pitch, void*
     }
     if (c->denoise_mode != 0) {
         const Img dn_out = c->stop_after == 2 ? out : (k2_out.data == mid1.data) ? mid0 : mid1;
-        cudaError_t e =
-            c->denoise_mode == 1 ? bm3d_run(c->bm3d, k2_out, dn_out, c->f16, c->d_denoise, st, false)
-                                 : surrogate_infer(c->sg, k2_out.data, dn_out.data, 1, h, w, c->f16, c->d_ab, st);
-        if (e == cudaSuccess && c->denoise_mode == 2 && c->spot_tiles > 0) {
+        const bool spot = c->denoise_mode == 2 && c->spot_tiles > 0;
+        cudaError_t e = cudaSuccess;
+        if (spot) {  // fork: gather + the tiles' BM3D on the side stream
             const int E = c->spot_edge, n = c->spot_tiles;
             const Img tin{c->d_tile_in, E, E * n, (long long)E * 4, 4};
             const Img tref{c->d_tile_ref, E, E * n, (long long)E * 4, 4};
             const dim3 gg((unsigned)((E + 127) / 128), (unsigned)E, (unsigned)n);
-            if (c->f16) spot::gather_kernel<__half><<<gg, 128, 0, st>>>(k2_out, static_cast<__half*>(c->d_tile_in), E, c->spot);
-            else spot::gather_kernel<float><<<gg, 128, 0, st>>>(k2_out, static_cast<float*>(c->d_tile_in), E, c->spot);
-            e = bm3d_run(c->tile_plan, tin, tref, c->f16, c->d_tile_scratch, st, false);
-            if (e == cudaSuccess) {
+            cudaStream_t ss = c->spot_stream;
+            e = cudaEventRecord(c->spot_fork, st);
+            if (e == cudaSuccess) e = cudaStreamWaitEvent(ss, c->spot_fork, 0);
+            if (e != cudaSuccess) return cuda_status(e, "chain spot fork");
+            if (c->f16) spot::gather_kernel<__half><<<gg, 128, 0, ss>>>(k2_out, static_cast<__half*>(c->d_tile_in), E, c->spot);
+            else spot::gather_kernel<float><<<gg, 128, 0, ss>>>(k2_out, static_cast<float*>(c->d_tile_in), E, c->spot);
+            e = bm3d_run(c->tile_plan, tin, tref, c->f16, c->d_tile_scratch, ss, false);
+            // the join is recorded even after a launch error, so the side stream never stays forked
+            const cudaError_t ej = cudaEventRecord(c->spot_join, ss);
+            if (e == cudaSuccess) e = ej;
+        }
+        if (e == cudaSuccess)
+            e = c->denoise_mode == 1 ? bm3d_run(c->bm3d, k2_out, dn_out, c->f16, c->d_denoise, st, false)
+                                     : surrogate_infer(c->sg, k2_out.data, dn_out.data, 1, h, w, c->f16, c->d_ab, st);
+        if (spot) {
+            const cudaError_t ew = cudaStreamWaitEvent(st, c->spot_join, 0);
+            if (e == cudaSuccess) e = ew;
+        }
+        if (e == cudaSuccess && spot) {
+            const int E = c->spot_edge, n = c->spot_tiles;
+            {
                 if (c->f16) spot::mse_kernel<__half><<<n, 256, 0, st>>>(dn_out, static_cast<const __half*>(c->d_tile_ref), E, c->spot, c->d_tile_mse);
                 else spot::mse_kernel<float><<<n, 256, 0, st>>>(dn_out, static_cast<const float*>(c->d_tile_ref), E, c->spot, c->d_tile_mse);
                 spot::decide_kernel<<<1, 1, 0, st>>>(c->d_tile_mse, n, c->spot_mse_max, c->d_gate, c->d_stats);
@@ -655,6 +675,10 @@ cpipe_cuda_chain* cpipe_cuda_chain_create(const cpipe_cuda_chain_config* cfg, in
                 return fail(CPIPE_OOM, c);
             if (cudaMemset(c->d_stats, 0, sizeof(SpotStats)) != cudaSuccess || cudaMemset(c->d_gate, 0, sizeof(int)) != cudaSuccess)
                 return fail(CPIPE_INTERNAL_ERROR, c);
+            if (cudaStreamCreateWithFlags(&c->spot_stream, cudaStreamNonBlocking) != cudaSuccess ||
+                cudaEventCreateWithFlags(&c->spot_fork, cudaEventDisableTiming) != cudaSuccess ||
+                cudaEventCreateWithFlags(&c->spot_join, cudaEventDisableTiming) != cudaSuccess)
+                return fail(CPIPE_INTERNAL_ERROR, c);
             if (cudaError_t e = bm3d_setup(c->bm3d); e != cudaSuccess) return fail(cuda_status(e, "bm3d setup"), c);
             if (cudaError_t e = bm3d_setup(c->tile_plan); e != cudaSuccess) return fail(cuda_status(e, "bm3d setup"), c);
         }
@@ -700,6 +724,9 @@ void cpipe_cuda_chain_destroy(cpipe_cuda_chain* c) {
     cudaFree(c->d_tile_mse);
     cudaFree(c->d_gate);
     cudaFree(c->d_stats);
+    if (c->spot_fork) cudaEventDestroy(c->spot_fork);
+    if (c->spot_join) cudaEventDestroy(c->spot_join);
+    if (c->spot_stream) cudaStreamDestroy(c->spot_stream);
     surrogate_free(c->sg);
     for (void* p : c->d_mid) cudaFree(p);
     for (void* p : c->d_io) cudaFree(p);

@@ -5,8 +5,9 @@ activations, FP32 accumulation) that stands in for the two-stage BM3D
 (denoise_bm3d_spec).  Everything runs on the GPU through libcpipe_b200:
 
 * training pairs: seeded raw frames from the device scene generator
-  (cpipe_cuda_scene_raw, noise a in [1e-3, 1e-2], b in [1e-5, 1e-4]
-  log-uniform), the chain's front (convert, black level, GainMap, RCD,
+  (cpipe_cuda_scene_raw_cfa: Bayer or Quad-Bayer mosaics, 10/12/14-bit, 1/4/20
+  rectangles, noise a in [1e-3, 1e-2], b in [1e-5, 1e-4] log-uniform), the
+  chain's front (Quad-Bayer frames remosaiced first) (convert, black level, GainMap, RCD,
   OpcodeList3 warp, WB, colormatrix; chain stop_after = 1) giving the
   denoiser's input, and the two-stage BM3D of that input (sigma from the noise
   profile as the denoise.bm3d node computes it) as the target;
@@ -17,7 +18,7 @@ activations, FP32 accumulation) that stands in for the two-stage BM3D
 No reference counterpart exists (the reference's AI denoise node is planned,
 docs/research/08-ai-isp-algorithms.md:37, but not implemented).
 
-    python -m cpipe_b200.surrogate train --pairs 40000 --steps 16000 --lr 1e-3 --out weights.cpsn
+    python -m cpipe_b200.surrogate train --pairs 80000 --steps 40000 --lr 1e-3 --out weights.cpsn
 
 (the committed cpipe_b200/weights/surrogate_bm3d.cpsn was made by this command;
 its report is surrogate_bm3d.report.json beside it)
@@ -215,19 +216,36 @@ class PairGenerator:
     """(denoiser input, two-stage BM3D output) tile pairs made on the GPU.
 
     Each frame is `tile` wide and `tile * per_frame` tall, so its tiles are
-    contiguous in memory; BM3D runs on the whole frame."""
+    contiguous in memory; BM3D runs on the whole frame.  Frames vary at random
+    between a Bayer (RGGB) and a Quad-Bayer mosaic (remosaiced by the chain's
+    demosaic.quad_bayer_remosaic), between 10, 12 and 14 bits, and between 1, 4
+    and 20 scene rectangles (large frames seen through 256x256 tiles are mostly
+    flat)."""
 
-    def __init__(self, tile=256, per_frame=8, seed=0x5EED0005):
-        from .chain import Chain, ChainConfig
+    KINDS = ("rggb", "qbc")
+    BITS = (10, 12, 14)
+    BLACK = {10: 16, 12: 64, 14: 256}
+    RECTS = (1, 4, 20)
+
+    def __init__(self, tile=256, per_frame=8, seed=0x5EED0005, kinds=KINDS, bits=BITS, rects=RECTS):
         self.tile, self.per_frame, self.seed = tile, per_frame, seed
         self.w, self.h = tile, tile * per_frame
-        self.cfg = ChainConfig.full_12mp(width=self.w, height=self.h, stop_after=1, use_graph=False,
-                                         name=f"surrogate_pairs_{self.w}x{self.h}")
-        self.front = Chain(self.cfg)
+        self.kinds, self.bits, self.rects = tuple(kinds), tuple(bits), tuple(rects)
+        self.fronts = {}
         self.raw = DeviceArray(self.w * self.h * 2)
         self.noisy = DeviceArray(self.w * self.h * 8)
         self.target = DeviceArray(self.w * self.h * 8)
-        self.cfa = (C.c_uint8 * 4)(*self.cfg.cfa[:4])
+
+    def front(self, kind, bits):
+        """The chain front (stop_after = 1) for one mosaic kind and bit depth."""
+        from .chain import Chain, ChainConfig
+        key = (kind, bits)
+        if key not in self.fronts:
+            cfg = ChainConfig.full_12mp(width=self.w, height=self.h, stop_after=1, use_graph=False, bits=bits,
+                                        black=float(self.BLACK[bits]), quad_bayer=kind == "qbc",
+                                        name=f"surrogate_pairs_{self.w}x{self.h}_{kind}_{bits}")
+            self.fronts[key] = Chain(cfg)
+        return self.fronts[key]
 
     def nonfinite(self):
         """Non-finite values in the current frame's input and target.  The
@@ -241,13 +259,16 @@ class PairGenerator:
             total += n.value
         return total
 
-    def frame(self, index, a, b):
+    def frame(self, index, a, b, kind="rggb", bits=10, rects=20):
+        from .scene import RGGB, SONY_QBC
         L = A.lib()
-        st = L.cpipe_cuda_scene_raw(self.raw.ptr, self.w, self.h, C.c_uint64(self.seed + index), self.cfg.bits,
-                                    int(self.cfg.black), float(a), float(b), self.cfa, 20, None)
+        pat = (C.c_uint8 * 16)(*(SONY_QBC if kind == "qbc" else RGGB))
+        st = L.cpipe_cuda_scene_raw_cfa(self.raw.ptr, self.w, self.h, C.c_uint64(self.seed + index), bits,
+                                        self.BLACK[bits], float(a), float(b), pat, 4 if kind == "qbc" else 2,
+                                        int(rects), None)
         if st:
             raise CpipeError(st, "scene_raw " + L.cpipe_cuda_last_error().decode())
-        self.front.run(self.raw.ptr, self.noisy.ptr, None)
+        self.front(kind, bits).run(self.raw.ptr, self.noisy.ptr, None)
         img = lambda d: DeviceImage(d.ptr, (self.h, self.w, 4), np.float16)
         st = call_filter("denoise_bm3d_spec", [img(self.noisy)], [img(self.target)], B.bm3d_spec(noise_sigma(a, b)))
         if st:
@@ -265,7 +286,10 @@ class PairGenerator:
         while k < count:
             a = float(np.exp(rng.uniform(np.log(NOISE_A[0]), np.log(NOISE_A[1]))))
             b = float(np.exp(rng.uniform(np.log(NOISE_B[0]), np.log(NOISE_B[1]))))
-            self.frame(f, a, b)
+            kind = self.kinds[int(rng.integers(len(self.kinds)))]
+            bits = self.bits[int(rng.integers(len(self.bits)))]
+            rects = self.rects[int(rng.integers(len(self.rects)))]
+            self.frame(f, a, b, kind, bits, rects)
             f += 1
             if self.nonfinite():
                 self.skipped += 1
@@ -282,7 +306,9 @@ class PairGenerator:
         return noisy, target, ab
 
     def close(self):
-        self.front.close()
+        for c in self.fronts.values():
+            c.close()
+        self.fronts = {}
         for d in (self.raw, self.noisy, self.target):
             d.free()
 
@@ -367,8 +393,8 @@ def _main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n")[0])
     sub = ap.add_subparsers(dest="cmd", required=True)
     t = sub.add_parser("train")
-    t.add_argument("--pairs", type=int, default=40000)
-    t.add_argument("--steps", type=int, default=16000)
+    t.add_argument("--pairs", type=int, default=80000)
+    t.add_argument("--steps", type=int, default=40000)
     t.add_argument("--batch", type=int, default=16)
     t.add_argument("--lr", type=float, default=1e-3)
     t.add_argument("--seed", type=int, default=1)

@@ -199,3 +199,26 @@ def test_trained_surrogate_passes_spot_check_at_12mp(cuda_device):
     assert frames == 1 and fallbacks == 0 and worst >= 40.0
     assert np.isfinite(out.astype(np.float32)).all()
     chain.close()
+
+
+def test_trained_surrogate_passes_spot_check_at_50mp_quad_bayer(cuda_device):
+    """The committed network on an 8160x6120 Sony Quad-Bayer frame (remosaiced
+    ahead of the chain, scene made on the device): two frames, every sampled
+    tile within 40 dB of BM3D."""
+    from cpipe_b200 import batch as B
+    cfg = ChainConfig.qbc_50mp(denoise="surrogate", surrogate_blob=S.load_weights())
+    L = A.lib()
+    d_raw, d_out = C.c_void_p(), C.c_void_p()
+    assert L.cpipe_cuda_device_alloc(cfg.width * cfg.height * 2, C.byref(d_raw)) == 0
+    assert L.cpipe_cuda_device_alloc(cfg.width * cfg.height * 8, C.byref(d_out)) == 0
+    B.scene_raw(d_raw.value, cfg, "qbc")
+    chain = Chain(cfg)
+    for _ in range(2):
+        chain.run(d_raw.value, d_out.value)
+    assert L.cpipe_cuda_synchronize() == 0
+    frames, fallbacks, worst = chain.denoise_stats()
+    print(f"50 MP Quad-Bayer spot check: {frames} frames, {fallbacks} fallbacks, worst tile {worst:.2f} dB")
+    assert frames == 2 and fallbacks == 0 and worst >= 40.0
+    chain.close()
+    L.cpipe_cuda_device_free(d_raw)
+    L.cpipe_cuda_device_free(d_out)
