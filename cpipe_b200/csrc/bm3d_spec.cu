@@ -44,6 +44,8 @@
 
 #include <math.h>
 
+#include <algorithm>
+
 #include "../../include/cpipe_node_abi.h"
 #include "kernels.h"
 
@@ -219,6 +221,8 @@ struct FilterArgs {
     float* acc;  // num of channel c at c*npx, den at (3+c)*npx
     const int* gate;
     float kaiser[64];
+    float kaiser1[8];
+    int np;  // tensor-core form: row pitch of the numerator footprint (= 8 mod 32)
 };
 
 constexpr int kBufStride = 65;                 // floats per block in a warp buffer
@@ -566,6 +570,30 @@ __device__ __forceinline__ void tc_forward(const float* img, int fw, const int (
     }
 }
 
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(smem_u32(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+    asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
+}
+
+constexpr int kStageStride = 72;  // floats per block in a warp's staging buffer (64 + 8: conflict-free float2 stores)
+
+// One launch per stage covers every tile: footprints of neighbouring tiles
+// overlap, and the flush adds into the frame accumulators with global
+// reductions.  Aggregation inside a tile:
+//   numerator    the group's inverse-transformed blocks go through the warp's
+//                staging buffer, so each shared-memory atomic instruction
+//                covers 32 distinct pixels (4 rows x 8 columns) of one block;
+//                the numerator's row pitch is 8 mod 32, so those 32 atomics
+//                also fall in 32 different banks;
+//   denominator  sum over placements of weight x Kaiser(pixel - origin): the
+//                weights are added at the block origins (a weight map, one
+//                atomic per block), and the separable Kaiser window is applied
+//                to that map at the flush.
 template <int STAGE>
 __global__ void __launch_bounds__(32 * kTcWarps, 2) bm3d_filter_tc_kernel(FilterArgs a, const TcTables* tables,
                                                                            int phx, int phy) {
@@ -580,13 +608,15 @@ __global__ void __launch_bounds__(32 * kTcWarps, 2) bm3d_filter_tc_kernel(Filter
     const int fy0 = row0 + max(0, refpos(j0, a.h, a.nstep) - a.R);
     const int fy1 = row0 + min(a.h, refpos(j1 - 1, a.h, a.nstep) + a.R + 8);
     const int fw = fx1 - fx0, fn = fw * (fy1 - fy0);
-    const int FN = a.fw * a.fw;
-    float* s_num = sm;
-    float* s_den = sm + FN;
-    float* s_img = sm + 2 * FN;
-    float* s_bas = sm + 3 * FN;
-    float* s_k = sm + (STAGE == 2 ? 4 : 3) * FN;
-    TcTables* s_tb = reinterpret_cast<TcTables*>((reinterpret_cast<uintptr_t>(s_k + 64) + 127) & ~(uintptr_t)127);
+    const int FN = (a.fw * a.fw + 3) & ~3, FNN = a.fw * a.np;  // planes rounded to 16 bytes (float2 staging)
+    float* s_num = sm;                                  // [fh][np]
+    float* s_img = sm + FNN;                            // [fh][fw]; after the groups: the weight map, then den
+    float* s_bas = s_img + FN;                          // stage 2
+    float* s_aux = s_img + (STAGE == 2 ? 2 : 1) * FN;  // staging buffers; at the flush the row-filtered map
+    float* s_k = s_aux + max(FN, kTcWarps * 8 * kStageStride);
+    float* s_k1 = s_k + 64;
+    float* s_wgt = s_k1 + 8;
+    TcTables* s_tb = reinterpret_cast<TcTables*>((reinterpret_cast<uintptr_t>(s_wgt + 64) + 127) & ~(uintptr_t)127);
     uint32_t* s_list = reinterpret_cast<uint32_t*>(s_tb + 1);  // the tile's groups
     uint32_t* s_cnt = s_list + kRefTile * kRefTile * 16;
     const float* gz = a.noisy + (long long)c * a.npx;
@@ -594,28 +624,35 @@ __global__ void __launch_bounds__(32 * kTcWarps, 2) bm3d_filter_tc_kernel(Filter
     for (int idx = threadIdx.x; idx < fn; idx += blockDim.x) {
         const int yy = idx / fw, xx = idx - yy * fw;
         const long long o = (long long)(fy0 + yy) * a.w + fx0 + xx;
-        s_num[idx] = 0.0F;
-        s_den[idx] = 0.0F;
-        s_img[idx] = gz[o];
-        if (STAGE == 2) s_bas[idx] = gb[o];
+        cp_async4(s_img + idx, gz + o);
+        if (STAGE == 2) cp_async4(s_bas + idx, gb + o);
     }
-    if (threadIdx.x < 64) s_k[threadIdx.x] = a.kaiser[threadIdx.x];
     {
         const uint4* src = reinterpret_cast<const uint4*>(tables);
         uint4* dst = reinterpret_cast<uint4*>(s_tb);
-        for (int i = threadIdx.x; i < (int)(sizeof(TcTables) / 16); i += blockDim.x) dst[i] = src[i];
+        for (int i = threadIdx.x; i < (int)(sizeof(TcTables) / 16); i += blockDim.x) cp_async16(dst + i, src + i);
     }
     const int nti = i1 - i0, nref = nti * (j1 - j0);
-    for (int i = threadIdx.x; i < nref * 16; i += blockDim.x) {
-        const int k = i >> 4;
+    for (int i = threadIdx.x; i < nref * 4; i += blockDim.x) {
+        const int k = i >> 2;
         const long long ref = ((long long)img * a.nry + j0 + k / nti) * a.nrx + i0 + k % nti;
-        s_list[i] = a.list[ref * 16 + (i & 15)];
-        if ((i & 15) == 0) s_cnt[k] = a.cnt[ref];
+        cp_async16(s_list + 4 * i, a.list + ref * 16 + 4 * (i & 3));
     }
+    if (threadIdx.x < nref) {
+        const int k = threadIdx.x;
+        s_cnt[k] = a.cnt[((long long)img * a.nry + j0 + k / nti) * a.nrx + i0 + k % nti];
+    }
+    for (int idx = threadIdx.x; idx < FNN; idx += blockDim.x) s_num[idx] = 0.0F;
+    if (threadIdx.x < 64) s_k[threadIdx.x] = a.kaiser[threadIdx.x];
+    if (threadIdx.x < 8) s_k1[threadIdx.x] = a.kaiser1[threadIdx.x];
+    cp_async_wait_all();
     __syncthreads();
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
     const int mi = lane >> 3, rr = lane & 7;
+    float* stg = s_aux + warp * (8 * kStageStride);
+    const int r8 = lane >> 3, c8 = lane & 7;  // a lane's pixel in a 4x8 quarter-block
+    const float kq0 = s_k[r8 * 8 + c8], kq1 = s_k[(4 + r8) * 8 + c8];
     for (int k = warp; k < nref; k += kTcWarps) {
         const int cnt = (int)s_cnt[k];
         const int L = cnt >= 16 ? 4 : cnt >= 8 ? 3 : cnt >= 4 ? 2 : cnt >= 2 ? 1 : 0;
@@ -660,7 +697,7 @@ __global__ void __launch_bounds__(32 * kTcWarps, 2) bm3d_filter_tc_kernel(Filter
 #pragma unroll
                     for (int e = 0; e < 4; ++e) {
                         const float b2 = Bc[mt][nt][e] * Bc[mt][nt][e];
-                        const float W = b2 / (b2 + a.sigma2);
+                        const float W = __fdividef(b2, b2 + a.sigma2);
                         T[mt][nt][e] = T[mt][nt][e] * W;
                         sw2 = __fmaf_rn(W, W, sw2);
                     }
@@ -668,6 +705,7 @@ __global__ void __launch_bounds__(32 * kTcWarps, 2) bm3d_filter_tc_kernel(Filter
             for (int off = 16; off > 0; off >>= 1) sw2 += __shfl_xor_sync(0xFFFFFFFFU, sw2, off);
             wgt = sw2 > 0.0F ? 1.0F / fmaxf(sw2, kMinWienerEnergy) : a.sigma2;
         }
+        if (lane == 0) s_wgt[k] = wgt;
         // Q = (Tn * scale) * H  (B = H[haar][block] via transposing ldmatrix)
         uint32_t hb[4];
         ldsm4t(hb, s_tb->haar[L] + (8 * (mi & 1) + rr) * 24 + 8 * (mi >> 1));
@@ -733,31 +771,65 @@ __global__ void __launch_bounds__(32 * kTcWarps, 2) bm3d_filter_tc_kernel(Filter
                     mma16816(X[nt + j], qa[ks], bl[2 * j], bl[2 * j + 1]);
                 }
             }
-        // aggregation: this lane holds blocks g and g + 8 (the blocks it loaded), rows nt, columns 2q, 2q+1
+        // numerator: X[nt][e] = block g (+8 for e >= 2), row nt, columns 2q, 2q+1 ->
+        // staging [block][row][column] -> one block's 4x8 quarter per atomic instruction
+        const float kw0 = wgt * kq0, kw1 = wgt * kq1;
 #pragma unroll
         for (int hb2 = 0; hb2 < 2; ++hb2) {
-            if (!act[hb2]) continue;
-            const int bx = bxy[hb2][0], by = bxy[hb2][1];
+            if (8 * hb2 >= N) break;
 #pragma unroll
             for (int nt = 0; nt < 8; ++nt)
-#pragma unroll
-                for (int j = 0; j < 2; ++j) {
-                    const int px = 8 * nt + 2 * q + j;
-                    const float kw = wgt * s_k[px];
-                    const int o = (by + nt) * fw + bx + 2 * q + j;
-                    atomicAdd(s_num + o, kw * X[nt][2 * hb2 + j]);
-                    atomicAdd(s_den + o, kw);
-                }
+                *reinterpret_cast<float2*>(stg + g * kStageStride + nt * 8 + 2 * q) =
+                    make_float2(X[nt][2 * hb2], X[nt][2 * hb2 + 1]);
+            __syncwarp();
+            const int nb = min(8, N - 8 * hb2);
+            for (int bb = 0; bb < nb; ++bb) {
+                const uint32_t p = lst[8 * hb2 + bb];
+                const int bx = (int)(p & 0xFFFFU) - fx0, by = (int)(p >> 16) - fy0;
+                float* dst = s_num + (by + r8) * a.np + bx + c8;
+                atomicAdd(dst, kw0 * stg[bb * kStageStride + r8 * 8 + c8]);
+                atomicAdd(dst + 4 * a.np, kw1 * stg[bb * kStageStride + (4 + r8) * 8 + c8]);
+            }
+            __syncwarp();
         }
+    }
+    __syncthreads();
+    // weight map at the block origins (in the footprint's own buffer, now free)
+    float* s_w = s_img;
+    for (int idx = threadIdx.x; idx < fn; idx += blockDim.x) s_w[idx] = 0.0F;
+    __syncthreads();
+    for (int i = threadIdx.x; i < nref * 16; i += blockDim.x) {
+        const int k = i >> 4, cnt = (int)s_cnt[k];
+        const int N = cnt >= 16 ? 16 : cnt >= 8 ? 8 : cnt >= 4 ? 4 : cnt >= 2 ? 2 : 1;
+        if ((i & 15) < N) {
+            const uint32_t p = s_list[i];
+            atomicAdd(s_w + ((int)(p >> 16) - fy0) * fw + (int)(p & 0xFFFFU) - fx0, s_wgt[k]);
+        }
+    }
+    __syncthreads();
+    // den = map correlated with the Kaiser window: rows into s_aux, then columns
+    for (int idx = threadIdx.x; idx < fn; idx += blockDim.x) {
+        const int yy = idx / fw, xx = idx - yy * fw;
+        float h = 0.0F;
+#pragma unroll
+        for (int u = 0; u < 8; ++u)
+            if (xx - u >= 0) h = __fmaf_rn(s_k1[u], s_w[idx - u], h);
+        s_aux[idx] = h;
     }
     __syncthreads();
     float* gn = a.acc + (long long)c * a.npx;
     float* gd = a.acc + (long long)(3 + c) * a.npx;
     for (int idx = threadIdx.x; idx < fn; idx += blockDim.x) {
         const int yy = idx / fw, xx = idx - yy * fw;
-        const long long o = (long long)(fy0 + yy) * a.w + fx0 + xx;
-        gn[o] += s_num[idx];
-        gd[o] += s_den[idx];
+        float d = 0.0F;
+#pragma unroll
+        for (int v = 0; v < 8; ++v)
+            if (yy - v >= 0) d = __fmaf_rn(s_k1[v], s_aux[idx - v * fw], d);
+        if (d > 0.0F) {
+            const long long o = (long long)(fy0 + yy) * a.w + fx0 + xx;
+            atomicAdd(gn + o, s_num[yy * a.np + xx]);
+            atomicAdd(gd + o, d);
+        }
     }
 }
 
@@ -819,9 +891,14 @@ size_t filter_smem(const Bm3dPlan& p, int stage) {
     return sizeof(float) * ((size_t)(stage == 2 ? 4 : 3) * p.fw * p.fw + (size_t)kFilterWarps * kWarpBuf + 64);
 }
 size_t match_smem(const Bm3dPlan& p) { return sizeof(uint32_t) * 4 * (size_t)p.mwin * p.mwpr; }
+// Row pitch of the tensor-core form's numerator footprint: at least fw and
+// 8 mod 32, so four rows of eight columns fall in 32 different banks.
+int num_pitch(int fw) { return fw + ((8 - fw) % 32 + 32) % 32; }
 size_t filter_tc_smem(const Bm3dPlan& p, int stage) {
-    return sizeof(float) * ((size_t)(stage == 2 ? 4 : 3) * p.fw * p.fw + 64) + 128 + sizeof(TcTables) +
-           sizeof(uint32_t) * kRefTile * kRefTile * 17;
+    const size_t fn = ((size_t)p.fw * p.fw + 3) & ~(size_t)3;
+    const size_t aux = std::max(fn, (size_t)kTcWarps * 8 * kStageStride);
+    const size_t floats = (size_t)p.fw * num_pitch(p.fw) + (stage == 2 ? 2 : 1) * fn + aux + 64 + 8 + 64;
+    return sizeof(float) * floats + 128 + sizeof(TcTables) + sizeof(uint32_t) * kRefTile * kRefTile * 17;
 }
 
 }  // namespace
@@ -864,6 +941,7 @@ int bm3d_plan(const cpipe_Bm3dSpecParams* p, int w, int h, Bm3dPlan* out, int ba
     }
     for (int v = 0; v < 8; ++v)
         for (int u = 0; u < 8; ++u) q.kaiser[v * 8 + u] = (float)(k1[v] * k1[u]);
+    for (int n = 0; n < 8; ++n) q.kaiser1[n] = (float)k1[n];
     q.nrx = ref_count(w, q.nstep);
     q.nry = ref_count(h, q.nstep);
     q.fw = (kRefTile - 1) * q.nstep + 2 * q.R + 8;
@@ -964,22 +1042,27 @@ cudaError_t bm3d_run(const Bm3dPlan& p, const Img& in, const Img& out, bool f16,
     fa.acc = acc;
     fa.gate = gate;
     for (int i = 0; i < 64; ++i) fa.kaiser[i] = p.kaiser[i];
+    for (int i = 0; i < 8; ++i) fa.kaiser1[i] = p.kaiser1[i];
+    fa.np = num_pitch(p.fw);
+    FilterArgs ta = fa;  // tensor-core form: one launch over all tiles (global reductions at the flush)
+    ta.phases = 1;
+    const dim3 tgrid(p.ntx, p.nty, 3 * p.batch);
     const dim3 fgrid((p.ntx + p.phases - 1) / p.phases, (p.nty + p.phases - 1) / p.phases, 3 * p.batch);
 
     for (int stage = 1; stage <= p.stages; ++stage) {
         bm3d_zero_kernel<<<kSmCount * 8, 256, 0, st>>>(acc, 6 * npx, gate);
         ma.dthr = p.dthr[stage - 1];
         bm3d_match_kernel<<<mgrid, kMatchTile * kMatchTile, ms, st>>>(ma);
-        for (int py = 0; py < p.phases; ++py)
-            for (int pxh = 0; pxh < p.phases; ++pxh) {
-                if (p.tensor) {
-                    if (stage == 1) bm3d_filter_tc_kernel<1><<<fgrid, 32 * kTcWarps, ts1, st>>>(fa, tables, pxh, py);
-                    else bm3d_filter_tc_kernel<2><<<fgrid, 32 * kTcWarps, ts2, st>>>(fa, tables, pxh, py);
-                } else {
+        if (p.tensor) {
+            if (stage == 1) bm3d_filter_tc_kernel<1><<<tgrid, 32 * kTcWarps, ts1, st>>>(ta, tables, 0, 0);
+            else bm3d_filter_tc_kernel<2><<<tgrid, 32 * kTcWarps, ts2, st>>>(ta, tables, 0, 0);
+        } else {
+            for (int py = 0; py < p.phases; ++py)
+                for (int pxh = 0; pxh < p.phases; ++pxh) {
                     if (stage == 1) bm3d_filter_kernel<1><<<fgrid, 32 * kFilterWarps, fs1, st>>>(fa, pxh, py);
                     else bm3d_filter_kernel<2><<<fgrid, 32 * kFilterWarps, fs2, st>>>(fa, pxh, py);
                 }
-            }
+        }
         if (stage == 1 && p.stages == 2)
             bm3d_basic_kernel<<<(unsigned)((npx + 255) / 256), 256, 0, st>>>(acc, basic, q, npx, gate);
     }

@@ -19,6 +19,7 @@ struct Bm3dPlan {
     float sigma = 0.0F, sigma2 = 0.0F, thr = 0.0F;
     uint32_t dthr[2] = {0, 0};  // integer match thresholds (64 * tau)
     float kaiser[64] = {};
+    float kaiser1[8] = {};  // the 1D window: kaiser[v * 8 + u] = kaiser1[v] * kaiser1[u] (rounded from double)
     int fw = 0;            // filter footprint edge bound (pixels)
     int phases = 0;        // filter launch phases per axis
     int ntx = 0, nty = 0;  // filter tiles (8x8 reference blocks each)
