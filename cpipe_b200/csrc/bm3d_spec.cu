@@ -222,7 +222,7 @@ struct FilterArgs {
     const int* gate;
     float kaiser[64];
     float kaiser1[8];
-    int np;  // tensor-core form: row pitch of the numerator footprint (= 8 mod 32)
+    int np;  // tensor-core form: row pitch of the footprint planes (= 4 mod 32)
 };
 
 constexpr int kBufStride = 65;                 // floats per block in a warp buffer
@@ -416,78 +416,34 @@ __global__ void __launch_bounds__(256, 2) bm3d_filter_kernel(FilterArgs a, int p
 }
 
 // ------------------------------------------- filter on the tensor cores
-// The group transform as small GEMMs on mma.sync.m16n8k16 (FP16 operands, FP32
-// accumulation).  Every product whose operands are not exact in FP16 is split
-// hi/lo (x = hi + lo, both FP16): a*b ~ ahi*bhi + alo*bhi + ahi*blo, which
-// keeps FP32-level accuracy for the threshold and Wiener decisions.  With
-// Xt[64 px][16 blocks] the group of one channel:
-//   forward  P = D * Xt          (D = C (x) C, the 64x64 2D DCT; K = pixels)
-//            T = P * H^T         (H = unnormalised Haar rows, +-1/0: exact; K = blocks)
-//            Tn = T * scale      (per Haar row: 1/sqrt(N) or 1/sqrt(2s))
-//   shrink   hard threshold / Wiener on Tn (FP32)
-//   inverse  Q = (Tn * scale) * H  (K = Haar index)
-//            X' = Q^T * D        (K = coefficients; Q^T from Q's fragments by
-//                                 movmatrix.trans, in registers)
-// The accumulator fragment of two adjacent n8 tiles is the A fragment of the
-// next product (P -> T, Tn -> Q), and movmatrix transposes Q in registers, so
-// the transform needs no shared-memory pass beyond the constant tables.
-struct TcTables {
-    __half dhi[64 * 72];     // D[coeff][pixel], rows padded to 72 halves (conflict-free ldmatrix)
-    __half dlo[64 * 72];
-    __half haar[5][16 * 24]; // unnormalised Haar for N = 1, 2, 4, 8, 16: [row][block], rows padded to 24
-    float scale[5][16];
-};
-
-__global__ void bm3d_tables_kernel(TcTables* t) {
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < 64 * 64) {
-        const int k = i >> 6, px = i & 63;
-        const float d = dctc(k >> 3, px >> 3) * dctc(k & 7, px & 7);
-        const __half hi = __float2half_rn(d);
-        t->dhi[k * 72 + px] = hi;
-        t->dlo[k * 72 + px] = __float2half_rn(d - __half2float(hi));
-    }
-    if (i < 5 * 16 * 16) {
-        const int L = i >> 8, r = (i >> 4) & 15, b = i & 15, N = 1 << L;
-        float h = 0.0F;
-        if (r < N && b < N) {
-            if (r == 0) {
-                h = 1.0F;
-            } else {
-                const int sft = r & -r;  // lowest set bit: the level of this detail row
-                h = (b >= r - sft && b < r) ? 1.0F : (b >= r && b < r + sft) ? -1.0F : 0.0F;
-            }
-        }
-        t->haar[L][r * 24 + b] = __float2half_rn(h);
-        if (b == 0) {
-            const int sft = r & -r;
-            t->scale[L][r] = r >= N ? 0.0F : r == 0 ? rsqrtf((float)N) : rsqrtf(2.0F * (float)sft);
-        }
-    }
-}
-
+// The 2D DCTs of a group as separable 8-point transforms on
+// mma.sync.m16n8k8 (FP16 operands, FP32 accumulation).  Every operand is split
+// hi/lo (x = hi + lo, both FP16): a*b ~ ahi*bhi + alo*bhi + ahi*blo, which keeps
+// FP32-level accuracy for the threshold and Wiener decisions.  One m16 tile
+// holds two blocks of the group (rows 0-7 block 2t, rows 8-15 block 2t+1):
+//   forward  Rc = X^T C^T   rows (block, x), K = y  (columns of each block)
+//            H  = Rc^T C^T  rows (block, v), K = x  (rows; Rc^T per 8x8 piece by
+//                                                    movmatrix.trans in registers)
+//   Haar     along the group, in FP32: a lane holds the same two coefficients
+//            (v = g, u = 2q, 2q+1) of all 16 blocks, so every level is register
+//            arithmetic (unnormalised butterflies; the normalisation is an exact
+//            power of two applied in the shrink step)
+//   shrink   hard threshold / Wiener on H (FP32)
+//   inverse  Rr = H C       rows (block, v), K = u  (the accumulator is the A
+//                                                    operand as it stands)
+//            X' = Rr^T C    rows (block, x), K = v
+// The DCT matrix enters only as B fragments: four registers per lane.
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-__device__ __forceinline__ void ldsm4(uint32_t (&r)[4], const void* p) {
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-                 : "r"(smem_u32(p)));
-}
-__device__ __forceinline__ void ldsm4t(uint32_t (&r)[4], const void* p) {
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-                 : "r"(smem_u32(p)));
-}
 // 8x8 b16 matrix held as a fragment (row lane/4, columns 2(lane%4)..+1) -> its transpose.
 __device__ __forceinline__ uint32_t movtrans(uint32_t x) {
     uint32_t y;
     asm volatile("movmatrix.sync.aligned.m8n8.trans.b16 %0, %1;\n" : "=r"(y) : "r"(x));
     return y;
 }
-__device__ __forceinline__ void mma16816(float (&c)[4], const uint32_t (&a)[4], uint32_t b0, uint32_t b1) {
-    asm volatile(
-        "mma.sync.aligned.m16n8k16.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, {%0,%1,%2,%3};\n"
-        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
-        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+__device__ __forceinline__ void mma1688(float (&c)[4], uint32_t a0, uint32_t a1, uint32_t b0) {
+    asm volatile("mma.sync.aligned.m16n8k8.row.col.f32.f16.f16.f32 {%0,%1,%2,%3}, {%4,%5}, {%6}, {%0,%1,%2,%3};\n"
+                 : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+                 : "r"(a0), "r"(a1), "r"(b0));
 }
 // FP16 hi/lo halves of two floats, packed as (x0, x1) pairs.
 __device__ __forceinline__ void split2(float x0, float x1, uint32_t& hi, uint32_t& lo) {
@@ -497,76 +453,121 @@ __device__ __forceinline__ void split2(float x0, float x1, uint32_t& hi, uint32_
     hi = *reinterpret_cast<const uint32_t*>(&h);
     lo = *reinterpret_cast<const uint32_t*>(&l);
 }
+// c = A * B over one 8-wide k-step with A = (a0, a1) given as FP32 pairs and B split hi/lo.
+__device__ __forceinline__ void mma_split(float (&c)[4], float a00, float a01, float a10, float a11, uint32_t bh,
+                                          uint32_t bl) {
+    uint32_t h0, l0, h1, l1;
+    split2(a00, a01, h0, l0);
+    split2(a10, a11, h1, l1);
+    c[0] = c[1] = c[2] = c[3] = 0.0F;
+    mma1688(c, h0, h1, bh);
+    mma1688(c, l0, l1, bh);
+    mma1688(c, h0, h1, bl);
+}
+// The same with A = each 8x8 piece of an accumulator tile transposed.
+__device__ __forceinline__ void mma_split_t(float (&c)[4], const float (&r)[4], uint32_t bh, uint32_t bl) {
+    uint32_t h0, l0, h1, l1;
+    split2(r[0], r[1], h0, l0);
+    split2(r[2], r[3], h1, l1);
+    h0 = movtrans(h0);
+    l0 = movtrans(l0);
+    h1 = movtrans(h1);
+    l1 = movtrans(l1);
+    c[0] = c[1] = c[2] = c[3] = 0.0F;
+    mma1688(c, h0, h1, bh);
+    mma1688(c, l0, l1, bh);
+    mma1688(c, h0, h1, bl);
+}
 
-constexpr int kTcWarps = 8;
+struct DctFrags {
+    uint32_t fh, fl;  // B[k][n] = C[n][k] (k = 2q, 2q+1; n = g): products with C^T
+    uint32_t ih, il;  // B[k][n] = C[k][n]: products with C
+};
+__device__ __forceinline__ DctFrags dct_frags(int g, int q) {
+    DctFrags d;
+    split2(dctc(g, 2 * q), dctc(g, 2 * q + 1), d.fh, d.fl);
+    split2(dctc(2 * q, g), dctc(2 * q + 1, g), d.ih, d.il);
+    return d;
+}
 
-// Forward transform of one group (channel image `img`, footprint row stride
-// fw): returns Tn in accumulator layout, acc[mt][nt][e] = Tn[coeff 16mt + g
-// (+8 for e >= 2)][haar 8nt + 2q + (e & 1)].
-__device__ __forceinline__ void tc_forward(const float* img, int fw, const int (&bxy)[2][2], bool (&act)[2],
-                                           const TcTables* tb, int L, float (&acc)[4][2][4]) {
-    const int lane = threadIdx.x & 31, q = lane & 3, mi = lane >> 3, rr = lane & 7;
+// One level of the unnormalised Haar along the group: block b = 2t + (e >= 2)
+// pairs with b + S, (lo, hi) -> (lo + hi, lo - hi).  A level is its own
+// transpose, so the inverse runs the same levels in reverse order.  The
+// orthonormal transform's coefficient at position b is the unnormalised one
+// times 2^(-k/2), k = log2 N for b = 0 and ctz(b) + 1 otherwise: the shrink
+// step compares against thresholds scaled by 2^(k/2) (the Wiener step against
+// sigma^2 2^k) and multiplies the kept coefficients by 2^-k, exactly, which is
+// the forward and the inverse normalisation together.
+template <int S>
+__device__ __forceinline__ void haar_level(float (&H)[8][4]) {
+    if (S == 1) {
 #pragma unroll
-    for (int mt = 0; mt < 4; ++mt)
+        for (int t = 0; t < 8; ++t)
 #pragma unroll
-        for (int nt = 0; nt < 2; ++nt)
-#pragma unroll
-            for (int e = 0; e < 4; ++e) acc[mt][nt][e] = 0.0F;
-#pragma unroll
-    for (int ks = 0; ks < 4; ++ks) {  // pixels 16ks .. 16ks+15 = block rows 2ks, 2ks+1
-        uint32_t bh[2][2], bl[2][2];
-#pragma unroll
-        for (int nt = 0; nt < 2; ++nt) {
-            float v[4] = {0.0F, 0.0F, 0.0F, 0.0F};
-            if (act[nt]) {
-                const float* r0 = img + (bxy[nt][1] + 2 * ks) * fw + bxy[nt][0] + 2 * q;
-                v[0] = r0[0];
-                v[1] = r0[1];
-                v[2] = r0[fw];
-                v[3] = r0[fw + 1];
+            for (int e = 0; e < 2; ++e) {
+                const float lo = H[t][e], hi = H[t][e + 2];
+                H[t][e] = lo + hi;
+                H[t][e + 2] = lo - hi;
             }
-            split2(v[0], v[1], bh[nt][0], bl[nt][0]);
-            split2(v[2], v[3], bh[nt][1], bl[nt][1]);
-        }
+    } else {
+        constexpr int D = S / 2;  // distance in t
 #pragma unroll
-        for (int mt = 0; mt < 4; ++mt) {
-            uint32_t ah[4], al[4];
-            const int off = (16 * mt + rr + 8 * (mi & 1)) * 72 + 16 * ks + 8 * (mi >> 1);
-            ldsm4(ah, tb->dhi + off);
-            ldsm4(al, tb->dlo + off);
+        for (int t = 0; t < 8; t += 2 * D)
 #pragma unroll
-            for (int nt = 0; nt < 2; ++nt) {
-                mma16816(acc[mt][nt], ah, bh[nt][0], bh[nt][1]);
-                mma16816(acc[mt][nt], al, bh[nt][0], bh[nt][1]);
-                mma16816(acc[mt][nt], ah, bl[nt][0], bl[nt][1]);
+            for (int e = 0; e < 2; ++e) {
+                const float lo = H[t][e], hi = H[t + D][e];
+                H[t][e] = lo + hi;
+                H[t + D][e] = lo - hi;
             }
-        }
     }
-    // T = P * H^T: the B operand H^T[block][haar] comes from H[haar][block] rows
-    uint32_t hb[4];
-    ldsm4(hb, tb->haar[L] + (8 * (mi >> 1) + rr) * 24 + 8 * (mi & 1));
-    const float* sc = tb->scale[L];
+}
+// k of position b > 0 (compile-time after unrolling); position 0 uses log2 N.
+__device__ __forceinline__ constexpr int haar_k(int b) { return (b & 1) ? 1 : (b & 2) ? 2 : (b & 4) ? 3 : 4; }
+// 2^e for a small integer e (exact).
+__device__ __forceinline__ float exp2i(int e) { return __int_as_float((127 + e) << 23); }
+
+// Forward 2D DCT and Haar of one group of N blocks read from `img` (row pitch P,
+// footprint origin fx0, fy0).  H[t][e]: block 2t (e < 2) or 2t + 1 (e >= 2),
+// coefficient (v = g, u = 2q + (e & 1)).
+__device__ __forceinline__ void tc_forward(const float* img, int P, const uint32_t* lst, int fx0, int fy0, int N,
+                                           const DctFrags& d, float (&H)[8][4]) {
+    const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
 #pragma unroll
-    for (int mt = 0; mt < 4; ++mt) {
-        uint32_t ah[4], al[4];
-        split2(acc[mt][0][0], acc[mt][0][1], ah[0], al[0]);
-        split2(acc[mt][0][2], acc[mt][0][3], ah[1], al[1]);
-        split2(acc[mt][1][0], acc[mt][1][1], ah[2], al[2]);
-        split2(acc[mt][1][2], acc[mt][1][3], ah[3], al[3]);
-        float t[2][4] = {{0.0F, 0.0F, 0.0F, 0.0F}, {0.0F, 0.0F, 0.0F, 0.0F}};
+    for (int t = 0; t < 8; ++t) {
+        H[t][0] = H[t][1] = H[t][2] = H[t][3] = 0.0F;
+        if (2 * t >= N) continue;
+        float v[2][2] = {{0.0F, 0.0F}, {0.0F, 0.0F}};
 #pragma unroll
-        for (int nt = 0; nt < 2; ++nt) {
-            mma16816(t[nt], ah, hb[2 * nt], hb[2 * nt + 1]);
-            mma16816(t[nt], al, hb[2 * nt], hb[2 * nt + 1]);
-        }
+        for (int hh = 0; hh < 2; ++hh)
+            if (2 * t + hh < N) {
+                const uint32_t p = lst[2 * t + hh];
+                const float* src = img + ((int)(p >> 16) - fy0 + 2 * q) * P + (int)(p & 0xFFFFU) - fx0 + g;
+                v[hh][0] = src[0];
+                v[hh][1] = src[P];
+            }
+        float rc[4];
+        mma_split(rc, v[0][0], v[0][1], v[1][0], v[1][1], d.fh, d.fl);  // rows (block, x = g), columns v
+        mma_split_t(H[t], rc, d.fh, d.fl);                             // rows (block, v = g), columns u
+    }
+    if (N > 1) haar_level<1>(H);
+    if (N > 2) haar_level<2>(H);
+    if (N > 4) haar_level<4>(H);
+    if (N > 8) haar_level<8>(H);
+}
+
+// Inverse Haar and 2D DCT: X[t][e] = block 2t (e < 2) or 2t + 1, pixel (x = g, y = 2q + (e & 1)).
+__device__ __forceinline__ void tc_inverse(float (&H)[8][4], int N, const DctFrags& d, float (&X)[8][4]) {
+    if (N > 8) haar_level<8>(H);
+    if (N > 4) haar_level<4>(H);
+    if (N > 2) haar_level<2>(H);
+    if (N > 1) haar_level<1>(H);
 #pragma unroll
-        for (int nt = 0; nt < 2; ++nt) {
-            const float s0 = sc[8 * nt + 2 * q], s1 = sc[8 * nt + 2 * q + 1];
-            acc[mt][nt][0] = t[nt][0] * s0;
-            acc[mt][nt][1] = t[nt][1] * s1;
-            acc[mt][nt][2] = t[nt][2] * s0;
-            acc[mt][nt][3] = t[nt][3] * s1;
-        }
+    for (int t = 0; t < 8; ++t) {
+        X[t][0] = X[t][1] = X[t][2] = X[t][3] = 0.0F;
+        if (2 * t >= N) continue;
+        float rr[4];
+        mma_split(rr, H[t][0], H[t][1], H[t][2], H[t][3], d.ih, d.il);  // rows (block, v = g), columns x
+        mma_split_t(X[t], rr, d.ih, d.il);                             // rows (block, x = g), columns y
     }
 }
 
@@ -580,26 +581,27 @@ __device__ __forceinline__ void cp_async_wait_all() {
     asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory");
 }
 
+constexpr int kTcWarps = 8;
 constexpr int kStageStride = 72;  // floats per block in a warp's staging buffer (64 + 8: conflict-free float2 stores)
 
 // One launch per stage covers every tile: footprints of neighbouring tiles
 // overlap, and the flush adds into the frame accumulators with global
-// reductions.  Aggregation inside a tile:
+// reductions.  The footprint planes use a row pitch P = 4 mod 32 (>= the
+// footprint edge), which makes the column loads of the forward transform and
+// the numerator atomics fall in 32 different banks.  Aggregation inside a tile:
 //   numerator    the group's inverse-transformed blocks go through the warp's
-//                staging buffer, so each shared-memory atomic instruction
-//                covers 32 distinct pixels (4 rows x 8 columns) of one block;
-//                the numerator's row pitch is 8 mod 32, so those 32 atomics
-//                also fall in 32 different banks;
+//                staging buffer ([block][x][y]), so each shared-memory atomic
+//                instruction covers 32 distinct pixels (8 rows x 4 columns) of
+//                one block;
 //   denominator  sum over placements of weight x Kaiser(pixel - origin): the
 //                weights are added at the block origins (a weight map, one
 //                atomic per block), and the separable Kaiser window is applied
 //                to that map at the flush.
 template <int STAGE>
-__global__ void __launch_bounds__(32 * kTcWarps, 2) bm3d_filter_tc_kernel(FilterArgs a, const TcTables* tables,
-                                                                           int phx, int phy) {
+__global__ void __launch_bounds__(32 * kTcWarps, STAGE == 1 ? 3 : 2) bm3d_filter_tc_kernel(FilterArgs a) {
     extern __shared__ __align__(16) float sm[];
     const int c = blockIdx.z % 3, img = blockIdx.z / 3, row0 = img * a.h;
-    const int tx = blockIdx.x * a.phases + phx, ty = blockIdx.y * a.phases + phy;
+    const int tx = blockIdx.x, ty = blockIdx.y;
     if (tx >= a.ntx || ty >= a.nty || gated_off(a.gate)) return;
     const int i0 = tx * kRefTile, j0 = ty * kRefTile;
     const int i1 = min(i0 + kRefTile, a.nrx), j1 = min(j0 + kRefTile, a.nry);
@@ -607,30 +609,26 @@ __global__ void __launch_bounds__(32 * kTcWarps, 2) bm3d_filter_tc_kernel(Filter
     const int fx1 = min(a.w, refpos(i1 - 1, a.w, a.nstep) + a.R + 8);
     const int fy0 = row0 + max(0, refpos(j0, a.h, a.nstep) - a.R);
     const int fy1 = row0 + min(a.h, refpos(j1 - 1, a.h, a.nstep) + a.R + 8);
-    const int fw = fx1 - fx0, fn = fw * (fy1 - fy0);
-    const int FN = (a.fw * a.fw + 3) & ~3, FNN = a.fw * a.np;  // planes rounded to 16 bytes (float2 staging)
-    float* s_num = sm;                                  // [fh][np]
-    float* s_img = sm + FNN;                            // [fh][fw]; after the groups: the weight map, then den
-    float* s_bas = s_img + FN;                          // stage 2
-    float* s_aux = s_img + (STAGE == 2 ? 2 : 1) * FN;  // staging buffers; at the flush the row-filtered map
-    float* s_k = s_aux + max(FN, kTcWarps * 8 * kStageStride);
+    const int fw = fx1 - fx0, fh = fy1 - fy0;
+    const int P = a.np, FP = a.fw * P;  // planes [a.fw rows][P]
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    float* s_num = sm;
+    float* s_img = sm + FP;                             // after the groups: the weight map, then den
+    float* s_bas = s_img + FP;                          // stage 2
+    float* s_aux = s_img + (STAGE == 2 ? 2 : 1) * FP;  // staging buffers (stage 1: at the flush the row-filtered map)
+    float* s_k = s_aux + (STAGE == 2 ? kTcWarps * 8 * kStageStride : max(FP, kTcWarps * 8 * kStageStride));
     float* s_k1 = s_k + 64;
     float* s_wgt = s_k1 + 8;
-    TcTables* s_tb = reinterpret_cast<TcTables*>((reinterpret_cast<uintptr_t>(s_wgt + 64) + 127) & ~(uintptr_t)127);
-    uint32_t* s_list = reinterpret_cast<uint32_t*>(s_tb + 1);  // the tile's groups
+    uint32_t* s_list = reinterpret_cast<uint32_t*>((reinterpret_cast<uintptr_t>(s_wgt + 64) + 15) & ~(uintptr_t)15);
     uint32_t* s_cnt = s_list + kRefTile * kRefTile * 16;
     const float* gz = a.noisy + (long long)c * a.npx;
     const float* gb = STAGE == 2 ? a.basic + (long long)c * a.npx : nullptr;
-    for (int idx = threadIdx.x; idx < fn; idx += blockDim.x) {
-        const int yy = idx / fw, xx = idx - yy * fw;
-        const long long o = (long long)(fy0 + yy) * a.w + fx0 + xx;
-        cp_async4(s_img + idx, gz + o);
-        if (STAGE == 2) cp_async4(s_bas + idx, gb + o);
-    }
-    {
-        const uint4* src = reinterpret_cast<const uint4*>(tables);
-        uint4* dst = reinterpret_cast<uint4*>(s_tb);
-        for (int i = threadIdx.x; i < (int)(sizeof(TcTables) / 16); i += blockDim.x) cp_async16(dst + i, src + i);
+    for (int yy = warp; yy < fh; yy += kTcWarps) {
+        const long long o = (long long)(fy0 + yy) * a.w + fx0;
+        for (int xx = lane; xx < fw; xx += 32) {
+            cp_async4(s_img + yy * P + xx, gz + o + xx);
+            if (STAGE == 2) cp_async4(s_bas + yy * P + xx, gb + o + xx);
+        }
     }
     const int nti = i1 - i0, nref = nti * (j1 - j0);
     for (int i = threadIdx.x; i < nref * 4; i += blockDim.x) {
@@ -642,193 +640,132 @@ __global__ void __launch_bounds__(32 * kTcWarps, 2) bm3d_filter_tc_kernel(Filter
         const int k = threadIdx.x;
         s_cnt[k] = a.cnt[((long long)img * a.nry + j0 + k / nti) * a.nrx + i0 + k % nti];
     }
-    for (int idx = threadIdx.x; idx < FNN; idx += blockDim.x) s_num[idx] = 0.0F;
+    for (int idx = threadIdx.x; idx < FP; idx += blockDim.x) s_num[idx] = 0.0F;
     if (threadIdx.x < 64) s_k[threadIdx.x] = a.kaiser[threadIdx.x];
     if (threadIdx.x < 8) s_k1[threadIdx.x] = a.kaiser1[threadIdx.x];
     cp_async_wait_all();
     __syncthreads();
 
-    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
-    const int mi = lane >> 3, rr = lane & 7;
+    const int g = lane >> 2, q = lane & 3;
+    const DctFrags dct = dct_frags(g, q);
+    // hard thresholds of the unnormalised coefficients: lambda sigma 2^(k/2)
+    const float thr1 = a.thr * 1.41421356237309515F, thr2 = a.thr * 2.0F, thr3 = a.thr * 2.82842712474619030F,
+                thr4 = a.thr * 4.0F;
     float* stg = s_aux + warp * (8 * kStageStride);
-    const int r8 = lane >> 3, c8 = lane & 7;  // a lane's pixel in a 4x8 quarter-block
-    const float kq0 = s_k[r8 * 8 + c8], kq1 = s_k[(4 + r8) * 8 + c8];
+    const int ly = lane & 7, lx = lane >> 3;  // a lane's pixel in an 8x4 half-block (y, x) and (y, x + 4)
+    const float kq0 = s_k[ly * 8 + lx], kq1 = s_k[ly * 8 + lx + 4];
     for (int k = warp; k < nref; k += kTcWarps) {
         const int cnt = (int)s_cnt[k];
-        const int L = cnt >= 16 ? 4 : cnt >= 8 ? 3 : cnt >= 4 ? 2 : cnt >= 2 ? 1 : 0;
-        const int N = 1 << L;
+        const int N = cnt >= 16 ? 16 : cnt >= 8 ? 8 : cnt >= 4 ? 4 : cnt >= 2 ? 2 : 1;
         const uint32_t* lst = s_list + k * 16;
-        // blocks this lane loads (n = g of each n-tile) ...
-        int bxy[2][2];
-        bool act[2];
-#pragma unroll
-        for (int nt = 0; nt < 2; ++nt) {
-            const int b = 8 * nt + g;
-            act[nt] = b < N;
-            const uint32_t p = act[nt] ? lst[b] : 0U;
-            bxy[nt][0] = (int)(p & 0xFFFFU) - fx0;
-            bxy[nt][1] = (int)(p >> 16) - fy0;
-        }
-        float T[4][2][4];
-        tc_forward(s_img, fw, bxy, act, s_tb, L, T);
+        float H[8][4];
+        tc_forward(s_img, P, lst, fx0, fy0, N, dct, H);
+        const int L = 31 - __clz(N);
         float wgt;
         if (STAGE == 1) {
+            const float th0 = L == 0 ? a.thr : L == 1 ? thr1 : L == 2 ? thr2 : L == 3 ? thr3 : thr4;
+            const float sc0 = exp2i(-L);
             unsigned kept = 0;
 #pragma unroll
-            for (int mt = 0; mt < 4; ++mt)
+            for (int t = 0; t < 8; ++t)
 #pragma unroll
-                for (int nt = 0; nt < 2; ++nt)
-#pragma unroll
-                    for (int e = 0; e < 4; ++e) {
-                        const bool keep = fabsf(T[mt][nt][e]) > a.thr;
-                        T[mt][nt][e] = keep ? T[mt][nt][e] : 0.0F;
-                        kept += keep ? 1U : 0U;
-                    }
+                for (int e = 0; e < 4; ++e) {
+                    const int b = 2 * t + (e >> 1), kb = haar_k(b);
+                    const float th = b == 0 ? th0 : kb == 1 ? thr1 : kb == 2 ? thr2 : kb == 3 ? thr3 : thr4;
+                    const float sc = b == 0 ? sc0 : (kb == 1 ? 0.5F : kb == 2 ? 0.25F : kb == 3 ? 0.125F : 0.0625F);
+                    const bool keep = fabsf(H[t][e]) > th;
+                    H[t][e] = keep ? H[t][e] * sc : 0.0F;
+                    kept += keep ? 1U : 0U;
+                }
             kept = __reduce_add_sync(0xFFFFFFFFU, kept);
             wgt = kept > 0U ? 1.0F / (float)kept : a.sigma2;
         } else {
-            float Bc[4][2][4];
-            tc_forward(s_bas, fw, bxy, act, s_tb, L, Bc);
+            float B[8][4];
+            tc_forward(s_bas, P, lst, fx0, fy0, N, dct, B);
+            const float s0 = a.sigma2 * exp2i(L), sc0 = exp2i(-L);
             float sw2 = 0.0F;
 #pragma unroll
-            for (int mt = 0; mt < 4; ++mt)
+            for (int t = 0; t < 8; ++t)
 #pragma unroll
-                for (int nt = 0; nt < 2; ++nt)
-#pragma unroll
-                    for (int e = 0; e < 4; ++e) {
-                        const float b2 = Bc[mt][nt][e] * Bc[mt][nt][e];
-                        const float W = __fdividef(b2, b2 + a.sigma2);
-                        T[mt][nt][e] = T[mt][nt][e] * W;
-                        sw2 = __fmaf_rn(W, W, sw2);
-                    }
+                for (int e = 0; e < 4; ++e) {
+                    const int b = 2 * t + (e >> 1), kb = haar_k(b);
+                    const float sk = b == 0 ? s0 : a.sigma2 * (float)(1 << kb);
+                    const float sc = b == 0 ? sc0 : (kb == 1 ? 0.5F : kb == 2 ? 0.25F : kb == 3 ? 0.125F : 0.0625F);
+                    const float b2 = B[t][e] * B[t][e];
+                    const float W = __fdividef(b2, b2 + sk);
+                    H[t][e] = (H[t][e] * W) * sc;
+                    sw2 = __fmaf_rn(W, W, sw2);
+                }
 #pragma unroll
             for (int off = 16; off > 0; off >>= 1) sw2 += __shfl_xor_sync(0xFFFFFFFFU, sw2, off);
             wgt = sw2 > 0.0F ? 1.0F / fmaxf(sw2, kMinWienerEnergy) : a.sigma2;
         }
         if (lane == 0) s_wgt[k] = wgt;
-        // Q = (Tn * scale) * H  (B = H[haar][block] via transposing ldmatrix)
-        uint32_t hb[4];
-        ldsm4t(hb, s_tb->haar[L] + (8 * (mi & 1) + rr) * 24 + 8 * (mi >> 1));
-        const float* sc = s_tb->scale[L];
-        // Q^T as A fragments of X' = Q^T * D: qa[ks][0..3] (hi), qb (lo), k-step ks = coefficients 16ks..
-        uint32_t qa[4][4], qb[4][4];
-#pragma unroll
-        for (int mt = 0; mt < 4; ++mt) {
-            float z[2][4];
-#pragma unroll
-            for (int nt = 0; nt < 2; ++nt) {
-                const float s0 = sc[8 * nt + 2 * q], s1 = sc[8 * nt + 2 * q + 1];
-                z[nt][0] = T[mt][nt][0] * s0;
-                z[nt][1] = T[mt][nt][1] * s1;
-                z[nt][2] = T[mt][nt][2] * s0;
-                z[nt][3] = T[mt][nt][3] * s1;
-            }
-            uint32_t ah[4], al[4];
-            split2(z[0][0], z[0][1], ah[0], al[0]);
-            split2(z[0][2], z[0][3], ah[1], al[1]);
-            split2(z[1][0], z[1][1], ah[2], al[2]);
-            split2(z[1][2], z[1][3], ah[3], al[3]);
-            float qv[2][4] = {{0.0F, 0.0F, 0.0F, 0.0F}, {0.0F, 0.0F, 0.0F, 0.0F}};
-#pragma unroll
-            for (int nt = 0; nt < 2; ++nt) {
-                mma16816(qv[nt], ah, hb[2 * nt], hb[2 * nt + 1]);
-                mma16816(qv[nt], al, hb[2 * nt], hb[2 * nt + 1]);
-            }
-            // Q[coeff 16mt + (g | g+8)][block 8nt + 2q..]: four 8x8 pieces, transposed in registers
-            uint32_t h00, l00, h01, l01, h10, l10, h11, l11;  // [nt][row half]
-            split2(qv[0][0], qv[0][1], h00, l00);
-            split2(qv[0][2], qv[0][3], h01, l01);
-            split2(qv[1][0], qv[1][1], h10, l10);
-            split2(qv[1][2], qv[1][3], h11, l11);
-            qa[mt][0] = movtrans(h00);  // blocks 0-7  x coeffs 16mt + 0..7
-            qa[mt][1] = movtrans(h10);  // blocks 8-15 x coeffs 16mt + 0..7
-            qa[mt][2] = movtrans(h01);  // blocks 0-7  x coeffs 16mt + 8..15
-            qa[mt][3] = movtrans(h11);  // blocks 8-15 x coeffs 16mt + 8..15
-            qb[mt][0] = movtrans(l00);
-            qb[mt][1] = movtrans(l10);
-            qb[mt][2] = movtrans(l01);
-            qb[mt][3] = movtrans(l11);
-        }
-        // X' = Q^T * D: M = 16 blocks, N = 64 pixels, K = 64 coefficients; B = D[coeff][pixel]
-        // through transposing ldmatrix.  X[nt][e] = block g (+8 for e >= 2), pixel 8nt + 2q + (e & 1)
         float X[8][4];
-#pragma unroll
-        for (int nt = 0; nt < 8; ++nt)
-#pragma unroll
-            for (int e = 0; e < 4; ++e) X[nt][e] = 0.0F;
-#pragma unroll
-        for (int ks = 0; ks < 4; ++ks)
-#pragma unroll
-            for (int nt = 0; nt < 8; nt += 2) {
-                uint32_t bh[4], bl[4];
-                const int boff = (16 * ks + 8 * (mi & 1) + rr) * 72 + 8 * (nt + (mi >> 1));
-                ldsm4t(bh, s_tb->dhi + boff);
-                ldsm4t(bl, s_tb->dlo + boff);
-#pragma unroll
-                for (int j = 0; j < 2; ++j) {
-                    mma16816(X[nt + j], qa[ks], bh[2 * j], bh[2 * j + 1]);
-                    mma16816(X[nt + j], qb[ks], bh[2 * j], bh[2 * j + 1]);
-                    mma16816(X[nt + j], qa[ks], bl[2 * j], bl[2 * j + 1]);
-                }
-            }
-        // numerator: X[nt][e] = block g (+8 for e >= 2), row nt, columns 2q, 2q+1 ->
-        // staging [block][row][column] -> one block's 4x8 quarter per atomic instruction
+        tc_inverse(H, N, dct, X);
+        // numerator: X -> staging [block][x][y] -> one block's 8x4 half per atomic instruction
         const float kw0 = wgt * kq0, kw1 = wgt * kq1;
 #pragma unroll
         for (int hb2 = 0; hb2 < 2; ++hb2) {
             if (8 * hb2 >= N) break;
 #pragma unroll
-            for (int nt = 0; nt < 8; ++nt)
-                *reinterpret_cast<float2*>(stg + g * kStageStride + nt * 8 + 2 * q) =
-                    make_float2(X[nt][2 * hb2], X[nt][2 * hb2 + 1]);
+            for (int tt = 0; tt < 4; ++tt) {
+                const int t = 4 * hb2 + tt;
+                *reinterpret_cast<float2*>(stg + (2 * tt) * kStageStride + g * 8 + 2 * q) = make_float2(X[t][0], X[t][1]);
+                *reinterpret_cast<float2*>(stg + (2 * tt + 1) * kStageStride + g * 8 + 2 * q) =
+                    make_float2(X[t][2], X[t][3]);
+            }
             __syncwarp();
             const int nb = min(8, N - 8 * hb2);
             for (int bb = 0; bb < nb; ++bb) {
                 const uint32_t p = lst[8 * hb2 + bb];
                 const int bx = (int)(p & 0xFFFFU) - fx0, by = (int)(p >> 16) - fy0;
-                float* dst = s_num + (by + r8) * a.np + bx + c8;
-                atomicAdd(dst, kw0 * stg[bb * kStageStride + r8 * 8 + c8]);
-                atomicAdd(dst + 4 * a.np, kw1 * stg[bb * kStageStride + (4 + r8) * 8 + c8]);
+                float* dst = s_num + (by + ly) * P + bx + lx;
+                atomicAdd(dst, kw0 * stg[bb * kStageStride + lane]);
+                atomicAdd(dst + 4, kw1 * stg[bb * kStageStride + 32 + lane]);
             }
             __syncwarp();
         }
     }
     __syncthreads();
-    // weight map at the block origins (in the footprint's own buffer, now free)
+    // weight map at the block origins (in the footprint's own plane, now free)
     float* s_w = s_img;
-    for (int idx = threadIdx.x; idx < fn; idx += blockDim.x) s_w[idx] = 0.0F;
+    for (int idx = threadIdx.x; idx < FP; idx += blockDim.x) s_w[idx] = 0.0F;
     __syncthreads();
     for (int i = threadIdx.x; i < nref * 16; i += blockDim.x) {
         const int k = i >> 4, cnt = (int)s_cnt[k];
         const int N = cnt >= 16 ? 16 : cnt >= 8 ? 8 : cnt >= 4 ? 4 : cnt >= 2 ? 2 : 1;
         if ((i & 15) < N) {
             const uint32_t p = s_list[i];
-            atomicAdd(s_w + ((int)(p >> 16) - fy0) * fw + (int)(p & 0xFFFFU) - fx0, s_wgt[k]);
+            atomicAdd(s_w + ((int)(p >> 16) - fy0) * P + (int)(p & 0xFFFFU) - fx0, s_wgt[k]);
         }
     }
     __syncthreads();
-    // den = map correlated with the Kaiser window: rows into s_aux, then columns
-    for (int idx = threadIdx.x; idx < fn; idx += blockDim.x) {
-        const int yy = idx / fw, xx = idx - yy * fw;
-        float h = 0.0F;
+    // den = map correlated with the Kaiser window: rows into a free plane, then columns
+    float* s_row = STAGE == 2 ? s_bas : s_aux;
+    for (int yy = warp; yy < fh; yy += kTcWarps)
+        for (int xx = lane; xx < fw; xx += 32) {
+            const float* wr = s_w + yy * P + xx;
+            float h = 0.0F;
 #pragma unroll
-        for (int u = 0; u < 8; ++u)
-            if (xx - u >= 0) h = __fmaf_rn(s_k1[u], s_w[idx - u], h);
-        s_aux[idx] = h;
-    }
+            for (int u = 0; u < 8; ++u)
+                if (xx - u >= 0) h = __fmaf_rn(s_k1[u], wr[-u], h);
+            s_row[yy * P + xx] = h;
+        }
     __syncthreads();
     float* gn = a.acc + (long long)c * a.npx;
     float* gd = a.acc + (long long)(3 + c) * a.npx;
-    for (int idx = threadIdx.x; idx < fn; idx += blockDim.x) {
-        const int yy = idx / fw, xx = idx - yy * fw;
-        float d = 0.0F;
+    for (int yy = warp; yy < fh; yy += kTcWarps) {
+        const long long o = (long long)(fy0 + yy) * a.w + fx0;
+        for (int xx = lane; xx < fw; xx += 32) {
+            float d = 0.0F;
 #pragma unroll
-        for (int v = 0; v < 8; ++v)
-            if (yy - v >= 0) d = __fmaf_rn(s_k1[v], s_aux[idx - v * fw], d);
-        if (d > 0.0F) {
-            const long long o = (long long)(fy0 + yy) * a.w + fx0 + xx;
-            atomicAdd(gn + o, s_num[yy * a.np + xx]);
-            atomicAdd(gd + o, d);
+            for (int v = 0; v < 8; ++v)
+                if (yy - v >= 0) d = __fmaf_rn(s_k1[v], s_row[(yy - v) * P + xx], d);
+            if (d > 0.0F) {
+                atomicAdd(gn + o + xx, s_num[yy * P + xx]);
+                atomicAdd(gd + o + xx, d);
+            }
         }
     }
 }
@@ -891,14 +828,16 @@ size_t filter_smem(const Bm3dPlan& p, int stage) {
     return sizeof(float) * ((size_t)(stage == 2 ? 4 : 3) * p.fw * p.fw + (size_t)kFilterWarps * kWarpBuf + 64);
 }
 size_t match_smem(const Bm3dPlan& p) { return sizeof(uint32_t) * 4 * (size_t)p.mwin * p.mwpr; }
-// Row pitch of the tensor-core form's numerator footprint: at least fw and
-// 8 mod 32, so four rows of eight columns fall in 32 different banks.
-int num_pitch(int fw) { return fw + ((8 - fw) % 32 + 32) % 32; }
+// Row pitch of the tensor-core form's footprint planes: at least fw and 4 mod
+// 32 (column loads of eight columns x two rows, and atomics of eight rows x
+// four columns, fall in 32 different banks).
+int tile_pitch(int fw) { return fw + ((4 - fw) % 32 + 32) % 32; }
 size_t filter_tc_smem(const Bm3dPlan& p, int stage) {
-    const size_t fn = ((size_t)p.fw * p.fw + 3) & ~(size_t)3;
-    const size_t aux = std::max(fn, (size_t)kTcWarps * 8 * kStageStride);
-    const size_t floats = (size_t)p.fw * num_pitch(p.fw) + (stage == 2 ? 2 : 1) * fn + aux + 64 + 8 + 64;
-    return sizeof(float) * floats + 128 + sizeof(TcTables) + sizeof(uint32_t) * kRefTile * kRefTile * 17;
+    const size_t fp = (size_t)p.fw * tile_pitch(p.fw);
+    const size_t stg = (size_t)kTcWarps * 8 * kStageStride;
+    const size_t aux = stage == 2 ? stg : std::max(fp, stg);
+    const size_t floats = fp + (stage == 2 ? 2 : 1) * fp + aux + 64 + 8 + 64;
+    return sizeof(float) * floats + 16 + sizeof(uint32_t) * kRefTile * kRefTile * 17;
 }
 
 }  // namespace
@@ -965,8 +904,6 @@ int bm3d_plan(const cpipe_Bm3dSpecParams* p, int w, int h, Bm3dPlan* out, int ba
     o = align256(o + nref * 16 * sizeof(uint32_t));
     q.off_cnt = o;
     o = align256(o + nref);
-    q.off_tables = o;
-    o = align256(o + sizeof(TcTables));
     q.bytes = o;
     return CPIPE_OK;
 }
@@ -1007,13 +944,11 @@ cudaError_t bm3d_run(const Bm3dPlan& p, const Img& in, const Img& out, bool f16,
     uint8_t* q = reinterpret_cast<uint8_t*>(base + p.off_q);
     uint32_t* list = reinterpret_cast<uint32_t*>(base + p.off_list);
     uint8_t* cnt = reinterpret_cast<uint8_t*>(base + p.off_cnt);
-    TcTables* tables = reinterpret_cast<TcTables*>(base + p.off_tables);
     const long long npx = (long long)p.w * p.h * p.batch;
     cudaError_t e;
     if (setup && (e = bm3d_setup(p)) != cudaSuccess) return e;
     const size_t ms = match_smem(p), fs1 = filter_smem(p, 1), fs2 = filter_smem(p, 2);
     const size_t ts1 = filter_tc_smem(p, 1), ts2 = filter_tc_smem(p, 2);
-    if (p.tensor) bm3d_tables_kernel<<<16, 256, 0, st>>>(tables);
 
     const dim3 pgrid((p.w + 255) / 256, p.h * p.batch);
     if (f16) bm3d_prep_kernel<__half><<<pgrid, 256, 0, st>>>(in, yuv, q, npx, gate);
@@ -1043,7 +978,7 @@ cudaError_t bm3d_run(const Bm3dPlan& p, const Img& in, const Img& out, bool f16,
     fa.gate = gate;
     for (int i = 0; i < 64; ++i) fa.kaiser[i] = p.kaiser[i];
     for (int i = 0; i < 8; ++i) fa.kaiser1[i] = p.kaiser1[i];
-    fa.np = num_pitch(p.fw);
+    fa.np = tile_pitch(p.fw);
     FilterArgs ta = fa;  // tensor-core form: one launch over all tiles (global reductions at the flush)
     ta.phases = 1;
     const dim3 tgrid(p.ntx, p.nty, 3 * p.batch);
@@ -1054,8 +989,8 @@ cudaError_t bm3d_run(const Bm3dPlan& p, const Img& in, const Img& out, bool f16,
         ma.dthr = p.dthr[stage - 1];
         bm3d_match_kernel<<<mgrid, kMatchTile * kMatchTile, ms, st>>>(ma);
         if (p.tensor) {
-            if (stage == 1) bm3d_filter_tc_kernel<1><<<tgrid, 32 * kTcWarps, ts1, st>>>(ta, tables, 0, 0);
-            else bm3d_filter_tc_kernel<2><<<tgrid, 32 * kTcWarps, ts2, st>>>(ta, tables, 0, 0);
+            if (stage == 1) bm3d_filter_tc_kernel<1><<<tgrid, 32 * kTcWarps, ts1, st>>>(ta);
+            else bm3d_filter_tc_kernel<2><<<tgrid, 32 * kTcWarps, ts2, st>>>(ta);
         } else {
             for (int py = 0; py < p.phases; ++py)
                 for (int pxh = 0; pxh < p.phases; ++pxh) {

@@ -26,7 +26,7 @@ struct Bm3dPlan {
     int mwin = 0, mwpr = 0;  // match tile region edge bound, words per smem row
     bool copy = false;       // image below 8x8 or sigma <= 0: output = input
     bool tensor = true;      // transforms on the tensor cores (FP16 hi/lo split) or FP32 CUDA cores
-    size_t off_yuv = 0, off_basic = 0, off_acc = 0, off_q = 0, off_list = 0, off_cnt = 0, off_tables = 0, bytes = 0;
+    size_t off_yuv = 0, off_basic = 0, off_acc = 0, off_q = 0, off_list = 0, off_cnt = 0, bytes = 0;
 };
 
 // Validates the parameters (CPIPE_BAD_INDEX when out of range) and sizes the
