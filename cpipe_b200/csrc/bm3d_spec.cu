@@ -118,9 +118,14 @@ struct MatchArgs {
 };
 
 constexpr int kMatchTile = 16;  // reference blocks per CTA edge (one thread each)
+constexpr int kMatchWprStd = 24;  // words per staged row for the 39x39 window at step 3
 
+// WPR > 0: words per staged row fixed at compile time (the standard 39x39
+// window), 0: taken from the arguments.
+template <int WPR>
 __global__ void __launch_bounds__(256) bm3d_match_kernel(MatchArgs a) {
     extern __shared__ uint32_t s_w[];
+    const int wpr = WPR > 0 ? WPR : a.wpr;
     if (gated_off(a.gate)) return;
     const int img = blockIdx.z, row0 = img * a.h;  // images are stacked in rows
     const int i0 = blockIdx.x * kMatchTile, j0 = blockIdx.y * kMatchTile;
@@ -130,11 +135,11 @@ __global__ void __launch_bounds__(256) bm3d_match_kernel(MatchArgs a) {
     const int ry0 = row0 + max(0, refpos(j0, a.h, a.nstep) - a.R);
     const int ry1 = row0 + min(a.h, refpos(jL, a.h, a.nstep) + a.R + 8);
     const int RW = rx1 - rx0, RH = ry1 - ry0;
-    const int plane = a.rows * a.wpr;  // words per shifted copy
+    const int plane = a.rows * wpr;  // words per shifted copy
     // Copy s, row r, word k holds region bytes 4k+s .. 4k+s+3 (little endian).
-    for (int idx = threadIdx.x; idx < 4 * RH * a.wpr; idx += blockDim.x) {
-        const int s = idx / (RH * a.wpr), rem = idx - s * RH * a.wpr;
-        const int r = rem / a.wpr, k = rem - r * a.wpr;
+    for (int idx = threadIdx.x; idx < 4 * RH * wpr; idx += blockDim.x) {
+        const int s = idx / (RH * wpr), rem = idx - s * RH * wpr;
+        const int r = rem / wpr, k = rem - r * wpr;
         const uint8_t* row = a.q + (size_t)(ry0 + r) * a.w + rx0;
         const int c0 = 4 * k + s;
         uint32_t word = 0;
@@ -143,7 +148,7 @@ __global__ void __launch_bounds__(256) bm3d_match_kernel(MatchArgs a) {
             const int cc = c0 + b;
             word |= (cc < RW ? (uint32_t)row[cc] : 0U) << (8 * b);
         }
-        s_w[s * plane + r * a.wpr + k] = word;
+        s_w[s * plane + r * wpr + k] = word;
     }
     __syncthreads();
     const int i = i0 + (int)(threadIdx.x % kMatchTile), j = j0 + (int)(threadIdx.x / kMatchTile);
@@ -152,11 +157,11 @@ __global__ void __launch_bounds__(256) bm3d_match_kernel(MatchArgs a) {
     uint32_t rw[16];
     {
         const int c = x - rx0;
-        const uint32_t* p = s_w + (c & 3) * plane + (y - ry0) * a.wpr + (c >> 2);
+        const uint32_t* p = s_w + (c & 3) * plane + (y - ry0) * wpr + (c >> 2);
 #pragma unroll
         for (int r = 0; r < 8; ++r) {
-            rw[2 * r] = p[r * a.wpr];
-            rw[2 * r + 1] = p[r * a.wpr + 1];
+            rw[2 * r] = p[r * wpr];
+            rw[2 * r + 1] = p[r * wpr + 1];
         }
     }
     uint32_t keys[15];
@@ -165,28 +170,48 @@ __global__ void __launch_bounds__(256) bm3d_match_kernel(MatchArgs a) {
     const int ylo = max(row0, y - a.R), yhi = min(row0 + a.h - 8, y + a.R);
     const int xlo = max(0, x - a.R), xhi = min(a.w - 8, x + a.R);
     if (a.n2 > 1) {
-        for (int yy = ylo; yy <= yhi; ++yy) {
-            const uint32_t wrow = (uint32_t)((yy - y + a.R) * a.ns + a.R - x);
-            const uint32_t* rowp = s_w + (yy - ry0) * a.wpr;
-            for (int xx = xlo; xx <= xhi; ++xx) {
-                const int c = xx - rx0;
-                const uint32_t* p = rowp + (c & 3) * plane + (c >> 2);
-                uint32_t d = 0;
+        // Columns of the search window outer, rows inner: the candidate's eight
+        // rows sit in a register ring (slot = row & 7, rows counted from ylo), so
+        // each candidate loads one new row.  Keys are unique (distance, window
+        // index), so the sorted list does not depend on the visiting order.
+        const int ny = yhi - ylo + 1;
+        for (int xx = xlo; xx <= xhi; ++xx) {
+            const int c = xx - rx0;
+            const uint32_t* colp = s_w + (c & 3) * plane + (ylo - ry0) * wpr + (c >> 2);
+            const uint32_t wcol = (uint32_t)((ylo - y + a.R) * a.ns + a.R - x + xx);
+            uint32_t cw[8][2];
 #pragma unroll
-                for (int r = 0; r < 8; ++r) {
-                    const uint32_t a0 = __vabsdiffu4(rw[2 * r], p[r * a.wpr]);
-                    d = __dp4a(a0, a0, d);
-                    const uint32_t a1 = __vabsdiffu4(rw[2 * r + 1], p[r * a.wpr + 1]);
-                    d = __dp4a(a1, a1, d);
-                }
-                if (d <= a.dthr && (xx != x || yy != y)) {
-                    uint32_t key = (d << 11) | (wrow + (uint32_t)xx);
-                    if (key < keys[14]) {
+            for (int r = 0; r < 7; ++r) {
+                cw[r][0] = colp[r * wpr];
+                cw[r][1] = colp[r * wpr + 1];
+            }
+            cw[7][0] = cw[7][1] = 0U;
+            for (int y0 = 0; y0 < ny; y0 += 8) {
+                const uint32_t* rp = colp + (y0 + 7) * wpr;
 #pragma unroll
-                        for (int m = 0; m < 15; ++m) {
-                            const uint32_t lo = min(keys[m], key);
-                            key = max(keys[m], key);
-                            keys[m] = lo;
+                for (int st = 0; st < 8; ++st) {
+                    if (y0 + st < ny) {
+                        cw[(st + 7) & 7][0] = rp[st * wpr];
+                        cw[(st + 7) & 7][1] = rp[st * wpr + 1];
+                        uint32_t d = 0;
+#pragma unroll
+                        for (int r = 0; r < 8; ++r) {
+                            const uint32_t a0 = __vabsdiffu4(rw[2 * r], cw[(st + r) & 7][0]);
+                            d = __dp4a(a0, a0, d);
+                            const uint32_t a1 = __vabsdiffu4(rw[2 * r + 1], cw[(st + r) & 7][1]);
+                            d = __dp4a(a1, a1, d);
+                        }
+                        const int yy = ylo + y0 + st;
+                        if (d <= a.dthr && (xx != x || yy != y)) {
+                            uint32_t key = (d << 11) | (wcol + (uint32_t)((y0 + st) * a.ns));
+                            if (key < keys[14]) {
+#pragma unroll
+                                for (int m = 0; m < 15; ++m) {
+                                    const uint32_t lo = min(keys[m], key);
+                                    key = max(keys[m], key);
+                                    keys[m] = lo;
+                                }
+                            }
                         }
                     }
                 }
@@ -913,7 +938,9 @@ cudaError_t bm3d_setup(const Bm3dPlan& p) {
     static const size_t kSmemOptIn = 227 * 1024;
     const size_t ms = match_smem(p), fs1 = filter_smem(p, 1), fs2 = filter_smem(p, 2);
     if (ms > kSmemOptIn || fs2 > kSmemOptIn) return cudaErrorInvalidConfiguration;
-    cudaError_t e = cudaFuncSetAttribute(bm3d_match_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ms);
+    cudaError_t e = cudaFuncSetAttribute(bm3d_match_kernel<kMatchWprStd>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ms);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(bm3d_match_kernel<0>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)ms);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(bm3d_filter_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fs1);
     if (e == cudaSuccess)
@@ -987,7 +1014,8 @@ cudaError_t bm3d_run(const Bm3dPlan& p, const Img& in, const Img& out, bool f16,
     for (int stage = 1; stage <= p.stages; ++stage) {
         bm3d_zero_kernel<<<kSmCount * 8, 256, 0, st>>>(acc, 6 * npx, gate);
         ma.dthr = p.dthr[stage - 1];
-        bm3d_match_kernel<<<mgrid, kMatchTile * kMatchTile, ms, st>>>(ma);
+        if (p.mwpr == kMatchWprStd) bm3d_match_kernel<kMatchWprStd><<<mgrid, kMatchTile * kMatchTile, ms, st>>>(ma);
+        else bm3d_match_kernel<0><<<mgrid, kMatchTile * kMatchTile, ms, st>>>(ma);
         if (p.tensor) {
             if (stage == 1) bm3d_filter_tc_kernel<1><<<tgrid, 32 * kTcWarps, ts1, st>>>(ta);
             else bm3d_filter_tc_kernel<2><<<tgrid, 32 * kTcWarps, ts2, st>>>(ta);
