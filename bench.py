@@ -414,7 +414,7 @@ def b200_arm(args):
         "e2e": {"value": round(whole_job_ms_per_frame(e2e_ms, e2e_steps, world), 4), "unit": "ms/frame",
                 "h2d_bytes_per_step": raw_bytes, "d2h_bytes_per_step": out_bytes},
         "clocks": clk,
-        "gpu_launches": 65 * args.steps,  # K1, K2, K3, 9 denoiser, 3 spot check, 2 x 25 BM3D (tiles; gated fallback)
+        "gpu_launches": 33 * args.steps,  # K1, K2, K3, 9 denoiser, 3 spot check, 2 x 9 BM3D (tiles; gated fallback)
     }
     if rank == 0 and world == 1 and not args.no_extra:
         line["batched_form"] = batched_form()

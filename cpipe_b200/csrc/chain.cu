@@ -347,33 +347,44 @@ __global__ void gather_kernel(Img src, T* __restrict__ dst, int edge, SpotOrigin
     T* d = dst + (((size_t)t * edge + y) * edge + x) * 4;
     store_rgba(d, load_rgba(s));
 }
-// per tile: mean squared RGB difference between the frame (at the origin) and the reference tile
+// Mean squared RGB difference between the frame (at the origins) and the
+// reference tiles, in two steps: mse_kernel sums kMseRows rows of one tile per
+// CTA into part[tile][chunk]; decide_kernel adds a tile's chunks in a fixed
+// order (so the decision does not depend on scheduling) and tests the worst tile.
+constexpr int kMseRows = 8;
+constexpr int kMseChunks = 256 / kMseRows;  // chunks per tile at the largest edge (256)
 template <class T>
-__global__ void mse_kernel(Img den, const T* __restrict__ ref, int edge, SpotOrigins o, float* __restrict__ mse) {
-    const int t = blockIdx.x;
-    __shared__ float part[32];
+__global__ void mse_kernel(Img den, const T* __restrict__ ref, int edge, SpotOrigins o, float* __restrict__ part) {
+    const int t = blockIdx.y, chunk = blockIdx.x;
+    __shared__ float warps[8];
     float acc = 0.0F;
-    for (int i = threadIdx.x; i < edge * edge; i += blockDim.x) {
-        const int y = i / edge, x = i - y * edge;
-        const Rgba a = load_rgba(px<const T>(den, o.x[t] + x, o.y[t] + y));
-        const Rgba b = load_rgba(ref + (((size_t)t * edge + y) * edge + x) * 4);
-        const float dr = a.r - b.r, dg = a.g - b.g, db = a.b - b.b;
-        acc += (dr * dr + dg * dg) + db * db;
-    }
+    const int y1 = min(edge, (chunk + 1) * kMseRows);
+    for (int y = chunk * kMseRows + (int)(threadIdx.x >> 5); y < y1; y += (int)(blockDim.x >> 5))
+        for (int x = (int)(threadIdx.x & 31); x < edge; x += 32) {
+            const Rgba a = load_rgba(px<const T>(den, o.x[t] + x, o.y[t] + y));
+            const Rgba b = load_rgba(ref + (((size_t)t * edge + y) * edge + x) * 4);
+            const float dr = a.r - b.r, dg = a.g - b.g, db = a.b - b.b;
+            acc += (dr * dr + dg * dg) + db * db;
+        }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFU, acc, off);
-    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = acc;
+    if ((threadIdx.x & 31) == 0) warps[threadIdx.x >> 5] = acc;
     __syncthreads();
-    if (threadIdx.x < 32) {
-        acc = threadIdx.x < blockDim.x / 32 ? part[threadIdx.x] : 0.0F;
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) acc += __shfl_xor_sync(0xFFFFFFFFU, acc, off);
-        if (threadIdx.x == 0) mse[t] = acc / (3.0F * (float)(edge * edge));
+    if (threadIdx.x == 0) {
+        float s = 0.0F;
+        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) s += warps[k];
+        part[t * kMseChunks + chunk] = s;
     }
 }
-__global__ void decide_kernel(const float* __restrict__ mse, int n, float mse_max, int* gate, SpotStats* stats) {
+__global__ void decide_kernel(const float* __restrict__ part, int n, int edge, float mse_max, int* gate,
+                              SpotStats* stats) {
+    const int chunks = (edge + kMseRows - 1) / kMseRows;
     float worst = 0.0F;
-    for (int t = 0; t < n; ++t) worst = fmaxf(worst, mse[t]);
+    for (int t = 0; t < n; ++t) {
+        float s = 0.0F;
+        for (int k = 0; k < chunks; ++k) s += part[t * kMseChunks + k];
+        worst = fmaxf(worst, s / (3.0F * (float)(edge * edge)));
+    }
     const int fall = !(worst <= mse_max);  // a non-finite tile error also falls back
     *gate = fall;
     stats->frames += 1U;
@@ -412,7 +423,7 @@ struct cpipe_cuda_chain {
     void* d_tile_in = nullptr;            // [tiles][edge][edge] RGBA, the denoiser's input
     void* d_tile_ref = nullptr;           // BM3D of the tiles
     void* d_tile_scratch = nullptr;
-    float* d_tile_mse = nullptr;
+    float* d_tile_mse = nullptr;          // per-tile partial sums of squared differences
     int* d_gate = nullptr;                // 1: fall back to BM3D for this frame
     SpotStats* d_stats = nullptr;
     // The tiles' BM3D runs on a second stream beside the network (both read
@@ -525,9 +536,10 @@ int launch_chain(cpipe_cuda_chain* c, const void* d_raw, size_t raw_pitch, void*
         if (e == cudaSuccess && spot) {
             const int E = c->spot_edge, n = c->spot_tiles;
             {
-                if (c->f16) spot::mse_kernel<__half><<<n, 256, 0, st>>>(dn_out, static_cast<const __half*>(c->d_tile_ref), E, c->spot, c->d_tile_mse);
-                else spot::mse_kernel<float><<<n, 256, 0, st>>>(dn_out, static_cast<const float*>(c->d_tile_ref), E, c->spot, c->d_tile_mse);
-                spot::decide_kernel<<<1, 1, 0, st>>>(c->d_tile_mse, n, c->spot_mse_max, c->d_gate, c->d_stats);
+                const dim3 gm((unsigned)((E + spot::kMseRows - 1) / spot::kMseRows), (unsigned)n);
+                if (c->f16) spot::mse_kernel<__half><<<gm, 256, 0, st>>>(dn_out, static_cast<const __half*>(c->d_tile_ref), E, c->spot, c->d_tile_mse);
+                else spot::mse_kernel<float><<<gm, 256, 0, st>>>(dn_out, static_cast<const float*>(c->d_tile_ref), E, c->spot, c->d_tile_mse);
+                spot::decide_kernel<<<1, 1, 0, st>>>(c->d_tile_mse, n, E, c->spot_mse_max, c->d_gate, c->d_stats);
                 e = bm3d_run(c->bm3d, k2_out, dn_out, c->f16, c->d_denoise, st, false, c->d_gate);
             }
         }
@@ -670,12 +682,16 @@ cpipe_cuda_chain* cpipe_cuda_chain_create(const cpipe_cuda_chain_config* cfg, in
             if (cudaMalloc(&c->d_tile_in, tile_bytes) != cudaSuccess || cudaMalloc(&c->d_tile_ref, tile_bytes) != cudaSuccess ||
                 (!c->tile_plan.copy && cudaMalloc(&c->d_tile_scratch, c->tile_plan.bytes) != cudaSuccess) ||
                 (!c->bm3d.copy && cudaMalloc(&c->d_denoise, c->bm3d.bytes) != cudaSuccess) ||
-                cudaMalloc(&c->d_tile_mse, sizeof(float) * 16) != cudaSuccess ||
+                cudaMalloc(&c->d_tile_mse, sizeof(float) * 16 * spot::kMseChunks) != cudaSuccess ||
                 cudaMalloc(&c->d_gate, sizeof(int)) != cudaSuccess || cudaMalloc(&c->d_stats, sizeof(SpotStats)) != cudaSuccess)
                 return fail(CPIPE_OOM, c);
             if (cudaMemset(c->d_stats, 0, sizeof(SpotStats)) != cudaSuccess || cudaMemset(c->d_gate, 0, sizeof(int)) != cudaSuccess)
                 return fail(CPIPE_INTERNAL_ERROR, c);
-            if (cudaStreamCreateWithFlags(&c->spot_stream, cudaStreamNonBlocking) != cudaSuccess ||
+            // the check runs at the device's highest stream priority, so its small
+            // launches take free SM slots ahead of the network's next layer
+            int prio_low = 0, prio_high = 0;
+            if (cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high) != cudaSuccess ||
+                cudaStreamCreateWithPriority(&c->spot_stream, cudaStreamNonBlocking, prio_high) != cudaSuccess ||
                 cudaEventCreateWithFlags(&c->spot_fork, cudaEventDisableTiming) != cudaSuccess ||
                 cudaEventCreateWithFlags(&c->spot_join, cudaEventDisableTiming) != cudaSuccess)
                 return fail(CPIPE_INTERNAL_ERROR, c);
@@ -756,7 +772,7 @@ int cpipe_cuda_chain_run(cpipe_cuda_chain* c, const void* d_raw, void* d_out, vo
                 if (ls != CPIPE_OK) s = ls;
             }
             if (s == CPIPE_OK) {
-                s = cuda_status(cudaGraphInstantiate(&c->graph, g, 0), "instantiate");
+                s = cuda_status(cudaGraphInstantiate(&c->graph, g, cudaGraphInstantiateFlagUseNodePriority), "instantiate");
                 cudaGraphDestroy(g);
             }
             if (own) cudaStreamDestroy(own);

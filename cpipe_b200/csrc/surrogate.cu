@@ -8,6 +8,8 @@
 //
 // Layout.  Activations are NHWC bf16: the input a0 has 8 channels (R, G, B,
 // sigma/0.03, four zeros), hidden activations a1..a7 32 channels (post-ReLU).
+// The tcgen05 inference path keeps its hidden activations in 8-channel planes,
+// [n][4][h][w][8] (surrogate_tc.cu); a0 is the same in both layouts.
 // Layer l is an implicit GEMM  out[p][co] = sum_k A[p][k] * W[co][k]  with
 // k = tap * CIN + ci (tap = 3*(dy+1) + (dx+1)), K padded to a multiple of 16;
 // the weights are stored [COUT][K] (the col-major B operand of mma).

@@ -5,10 +5,12 @@
 // all output channels (N = 32, or 16 for the 3-channel last layer padded with
 // zero weights) as an implicit GEMM over K = 9 taps x CIN channels:
 //
-//  * TMA (cp.async.bulk.tensor.4d, no multicast) loads the 10 x 18-pixel halo
-//    tile of the NHWC bf16 activation as CIN/8 planes of 16-byte channel
-//    chunks ([row][col][8 ch]); out-of-image pixels are zero-filled by the
-//    copy, which is the convolution's zero padding.
+//  * Activations between the layers are bf16 in 8-channel planes,
+//    [n][C/8][h][w][8], so one plane row is a contiguous run of 16-byte pixels
+//    (whole sectors for the copy engine and for the epilogue's stores).  TMA
+//    (cp.async.bulk.tensor.4d, no multicast) loads the 10 x 18-pixel halo tile
+//    as CIN/8 planes ([row][col][8 ch]); out-of-image pixels are zero-filled by
+//    the copy, which is the convolution's zero padding.
 //  * In that layout the im2col operand of one tap is a K-major, unswizzled
 //    shared-memory matrix: 8 consecutive output pixels of a row are one core
 //    matrix (16 B apart), the next output row is one halo row further (SBO =
@@ -20,7 +22,7 @@
 //    next; tcgen05.commit signals the mbarriers that free an input stage and
 //    publish an accumulator.
 //  * Four epilogue warps read their 32 TMEM lanes each (tcgen05.ld 32x32b),
-//    add the bias and apply ReLU (hidden layers: bf16 NHWC out) or add the
+//    add the bias and apply ReLU (hidden layers: bf16 planes out) or add the
 //    residual to the RGBA input (last layer).
 //
 // Warp roles: 0-3 epilogue, 4 TMA producer, 5 MMA issuer and TMEM owner.  A
@@ -47,6 +49,8 @@ constexpr int kHW = kTW + 2, kHH = kTH + 2;    // halo tile
 constexpr int kPlaneBytes = kHW * kHH * 16;    // one 8-channel plane as TMA writes it (2880 B)
 constexpr int kPlaneStride = 2944;             // planes 128-byte aligned
 constexpr int kStages = 3;
+constexpr int kBarBytes = 256;  // mbarriers (2 per stage + 4) and the TMEM address slot
+static_assert((2 * kStages + 4) * 8 + 4 <= kBarBytes, "barrier area");
 constexpr int kTmemCols = 64;                  // two accumulators of up to 32 columns
 constexpr uint32_t kSpinLimit = 1U << 20;  // try_wait suspends between polls: about a second in all
 
@@ -153,7 +157,7 @@ struct TcShape {
     static constexpr int KSLICES = KP / 16;
     static constexpr int WBYTES = N * KP * 2;
     static constexpr int BAR_OFF = kStages * STAGE + WBYTES;
-    static constexpr int SMEM = BAR_OFF + 128 + N * 4 + 1024;  // + barriers/TMEM slot, bias, alignment slack
+    static constexpr int SMEM = BAR_OFF + kBarBytes + N * 4 + 1024;  // + barriers/TMEM slot, bias, alignment slack
 };
 
 enum { kTcRelu = 0, kTcResidual = 1 };
@@ -171,7 +175,7 @@ __global__ void __launch_bounds__(192, 1)
     uint64_t* accf = empty + kStages;
     uint64_t* acce = accf + 2;
     uint32_t* s_tmem = reinterpret_cast<uint32_t*>(acce + 2);
-    float* s_bias = reinterpret_cast<float*>(smem + S::BAR_OFF + 128);
+    float* s_bias = reinterpret_cast<float*>(smem + S::BAR_OFF + kBarBytes);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
     // weights -> core-matrix order: (n-group, k-group) at (kg * N/8 + ng) * 128 B
@@ -222,7 +226,8 @@ __global__ void __launch_bounds__(192, 1)
                 mbar_expect_tx(&full[s], S::STAGE_TX);
 #pragma unroll
                 for (int p = 0; p < S::PLANES; ++p)
-                    tma_load_4d(s_in + s * S::STAGE + p * kPlaneStride, &tmap, &full[s], p * 8, x0, y0, img);
+                    tma_load_4d(s_in + s * S::STAGE + p * kPlaneStride, &tmap, &full[s], 0, x0, y0,
+                                img * S::PLANES + p);
             }
         }
     } else if (warp == 5) {
@@ -285,9 +290,11 @@ __global__ void __launch_bounds__(192, 1)
                 for (int k = 0; k < N / 2; ++k)
                     o[k] = __floats2bfloat162_rn(fmaxf(c[2 * k] + s_bias[2 * k], 0.0F),
                                                  fmaxf(c[2 * k + 1] + s_bias[2 * k + 1], 0.0F));
-                uint4* dst = reinterpret_cast<uint4*>(a.y + p * N);
+                // planar output [img][N / 8][h][w][8]: each store of a warp is four 128-byte rows
+                const long long plane = (long long)a.h * a.w;
+                uint4* dst = reinterpret_cast<uint4*>(a.y) + (long long)img * (N / 8) * plane + (long long)gy * a.w + gx;
 #pragma unroll
-                for (int k = 0; k < N / 8; ++k) dst[k] = reinterpret_cast<const uint4*>(o)[k];
+                for (int k = 0; k < N / 8; ++k) dst[k * plane] = reinterpret_cast<const uint4*>(o)[k];
             } else {
                 const T* src = static_cast<const T*>(a.rgba) + 4 * p;
                 const Rgba x = load_rgba(src);
@@ -323,8 +330,9 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 bool make_map(CUtensorMap* map, const bf16* act, int cin, int n, int h, int w) {
     auto fn = encode_fn();
     if (!fn) return false;
-    const cuuint64_t dims[4] = {(cuuint64_t)cin, (cuuint64_t)w, (cuuint64_t)h, (cuuint64_t)n};
-    const cuuint64_t strides[3] = {(cuuint64_t)cin * 2, (cuuint64_t)w * cin * 2, (cuuint64_t)h * w * cin * 2};
+    // [n][cin / 8][h][w][8]: one 8-channel plane per (image, plane) index
+    const cuuint64_t dims[4] = {8, (cuuint64_t)w, (cuuint64_t)h, (cuuint64_t)n * (cuuint64_t)(cin / 8)};
+    const cuuint64_t strides[3] = {16, (cuuint64_t)w * 16, (cuuint64_t)h * w * 16};
     const cuuint32_t box[4] = {8, (cuuint32_t)kHW, (cuuint32_t)kHH, 1};
     const cuuint32_t es[4] = {1, 1, 1, 1};
     return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16*>(act), dims, strides, box, es,
