@@ -17,15 +17,15 @@
 //    160 B) and the second 8-channel chunk of the 16-wide K slice is the next
 //    plane (LBO).  So every MMA reads the halo tile in place: no im2col copy.
 //  * Weights are staged once per CTA in core-matrix order; one elected thread
-//    issues tcgen05.mma (kind::f16, BF16 x BF16 -> FP32) into TMEM, two
-//    accumulator buffers so the epilogue of a tile overlaps the MMAs of the
-//    next; tcgen05.commit signals the mbarriers that free an input stage and
-//    publish an accumulator.
-//  * Four epilogue warps read their 32 TMEM lanes each (tcgen05.ld 32x32b),
-//    add the bias and apply ReLU (hidden layers: bf16 planes out) or add the
-//    residual to the RGBA input (last layer).
+//    issues tcgen05.mma (kind::f16, BF16 x BF16 -> FP32) into TMEM, four
+//    accumulator buffers so the epilogues of earlier tiles overlap the MMAs of
+//    the next; tcgen05.commit signals the mbarriers that free an input stage
+//    and publish an accumulator.
+//  * Two epilogue warpgroups take alternate tiles; each warp reads its 32 TMEM
+//    lanes (tcgen05.ld 32x32b), adds the bias and applies ReLU (hidden layers:
+//    bf16 planes out) or adds the residual to the RGBA input (last layer).
 //
-// Warp roles: 0-3 epilogue, 4 TMA producer, 5 MMA issuer and TMEM owner.  A
+// Warp roles: 0-7 epilogue, 8 TMA producer, 9 MMA issuer and TMEM owner.  A
 // 3-stage input ring and every mbarrier wait is bounded: a wait that runs out
 // records an error code in *err and ends that role, and the CTA still reaches
 // its teardown (TMEM released) so the context stays usable.
@@ -49,9 +49,12 @@ constexpr int kHW = kTW + 2, kHH = kTH + 2;    // halo tile
 constexpr int kPlaneBytes = kHW * kHH * 16;    // one 8-channel plane as TMA writes it (2880 B)
 constexpr int kPlaneStride = 2944;             // planes 128-byte aligned
 constexpr int kStages = 3;
-constexpr int kBarBytes = 256;  // mbarriers (2 per stage + 4) and the TMEM address slot
-static_assert((2 * kStages + 4) * 8 + 4 <= kBarBytes, "barrier area");
-constexpr int kTmemCols = 64;                  // two accumulators of up to 32 columns
+constexpr int kAcc = 4;                         // TMEM accumulators of up to 32 columns
+constexpr int kTmemCols = kAcc * 32;
+constexpr int kEpiWarps = 8;                    // two epilogue warpgroups, alternate tiles
+constexpr int kThreads = 32 * (kEpiWarps + 2);  // + TMA producer warp + MMA warp
+constexpr int kBarBytes = 256;  // mbarriers (2 per stage + 2 per accumulator) and the TMEM address slot
+static_assert((2 * kStages + 2 * kAcc) * 8 + 4 <= kBarBytes, "barrier area");
 constexpr uint32_t kSpinLimit = 1U << 20;  // try_wait suspends between polls: about a second in all
 
 __host__ __device__ constexpr int kpad(int cin) { return (9 * cin + 15) / 16 * 16; }
@@ -163,7 +166,7 @@ struct TcShape {
 enum { kTcRelu = 0, kTcResidual = 1 };
 
 template <int CIN, int N, int EPI, class T>
-__global__ void __launch_bounds__(192, 1)
+__global__ void __launch_bounds__(kThreads, 1)
     sg_tc_conv_kernel(const __grid_constant__ CUtensorMap tmap, const bf16* __restrict__ wpk, TcConvArgs a) {
     using S = TcShape<CIN, N>;
     extern __shared__ uint8_t smem_raw[];
@@ -173,8 +176,8 @@ __global__ void __launch_bounds__(192, 1)
     uint64_t* full = reinterpret_cast<uint64_t*>(smem + S::BAR_OFF);
     uint64_t* empty = full + kStages;
     uint64_t* accf = empty + kStages;
-    uint64_t* acce = accf + 2;
-    uint32_t* s_tmem = reinterpret_cast<uint32_t*>(acce + 2);
+    uint64_t* acce = accf + kAcc;
+    uint32_t* s_tmem = reinterpret_cast<uint32_t*>(acce + kAcc);
     float* s_bias = reinterpret_cast<float*>(smem + S::BAR_OFF + kBarBytes);
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 
@@ -191,15 +194,15 @@ __global__ void __launch_bounds__(192, 1)
             mbar_init(&full[s], 1);
             mbar_init(&empty[s], 1);
         }
-        for (int s = 0; s < 2; ++s) {
+        for (int s = 0; s < kAcc; ++s) {
             mbar_init(&accf[s], 1);
-            mbar_init(&acce[s], 4);
+            mbar_init(&acce[s], 4);  // the four warps of the warpgroup that drains it
         }
         asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
     }
     // generic-proxy writes of the weights must be visible to the tensor core (async proxy)
     asm volatile("fence.proxy.async.shared::cta;\n" ::: "memory");
-    if (warp == 5) {
+    if (warp == kEpiWarps + 1) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;\n" ::"r"(saddr(s_tmem)),
                      "r"(kTmemCols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;\n" ::);
@@ -212,7 +215,7 @@ __global__ void __launch_bounds__(192, 1)
     const int tiles_x = (a.w + kTW - 1) / kTW, tiles_y = (a.h + kTH - 1) / kTH;
     const int per_img = tiles_x * tiles_y, tiles = per_img * a.n;
 
-    if (warp == 4) {
+    if (warp == kEpiWarps) {
         if (lane == 0) {  // TMA producer
             int i = 0;
             for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++i) {
@@ -226,17 +229,17 @@ __global__ void __launch_bounds__(192, 1)
                 mbar_expect_tx(&full[s], S::STAGE_TX);
 #pragma unroll
                 for (int p = 0; p < S::PLANES; ++p)
-                    tma_load_4d(s_in + s * S::STAGE + p * kPlaneStride, &tmap, &full[s], 0, x0, y0,
-                                img * S::PLANES + p);
+                    tma_load_4d(s_in + s * S::STAGE + p * kPlaneStride, &tmap, &full[s], x0 * 8, y0,
+                                img * S::PLANES + p, 0);
             }
         }
-    } else if (warp == 5) {
+    } else if (warp == kEpiWarps + 1) {
         if (lane == 0) {  // MMA issuer
             constexpr uint32_t idesc = instr_desc<N>();
             const uint32_t wbase = saddr(s_w);
             int i = 0;
             for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++i) {
-                const int s = i % kStages, u = i / kStages, acc = i & 1, v = i >> 1;
+                const int s = i % kStages, u = i / kStages, acc = i % kAcc, v = i / kAcc;
                 if (!mbar_wait(&full[s], (uint32_t)u & 1U)) {
                     atomicExch(a.err, 2);
                     break;
@@ -247,7 +250,7 @@ __global__ void __launch_bounds__(192, 1)
                 }
                 tc_fence_after();
                 const uint32_t abase = saddr(s_in + s * S::STAGE);
-                const uint32_t d = tmem + (uint32_t)(acc * N);
+                const uint32_t d = tmem + (uint32_t)(acc * 32);
 #pragma unroll
                 for (int ks = 0; ks < S::KSLICES; ++ks) {
                     uint64_t ad;
@@ -265,18 +268,22 @@ __global__ void __launch_bounds__(192, 1)
                 mma_commit(&accf[acc]);
             }
         }
-    } else {  // epilogue warps 0-3: TMEM lanes 32*warp .. 32*warp+31 = tile pixels
-        const int m = warp * 32 + lane;
+    } else {  // epilogue warps: TMEM lanes 32*(warp%4) .. +31 = tile pixels; warpgroup warp/4 takes every other tile
+        const int m = (warp & 3) * 32 + lane, wg = warp >> 2;
+        float bias_r[N];
+#pragma unroll
+        for (int k = 0; k < N; ++k) bias_r[k] = s_bias[k];
         int i = 0;
         for (int tile = blockIdx.x; tile < tiles; tile += gridDim.x, ++i) {
-            const int acc = i & 1, v = i >> 1;
+            if ((i & 1) != wg) continue;
+            const int acc = i % kAcc, v = i / kAcc;
             if (!mbar_wait(&accf[acc], (uint32_t)v & 1U)) {
                 atomicExch(a.err, 4);
                 break;
             }
             tc_fence_after();
             float c[N];
-            tmem_load<N>(tmem + ((uint32_t)(warp * 32) << 16) + (uint32_t)(acc * N), c);
+            tmem_load<N>(tmem + ((uint32_t)((warp & 3) * 32) << 16) + (uint32_t)(acc * 32), c);
             tc_fence_before();
             __syncwarp();
             if (lane == 0) mbar_arrive(&acce[acc]);
@@ -288,8 +295,8 @@ __global__ void __launch_bounds__(192, 1)
                 __nv_bfloat162 o[N / 2];
 #pragma unroll
                 for (int k = 0; k < N / 2; ++k)
-                    o[k] = __floats2bfloat162_rn(fmaxf(c[2 * k] + s_bias[2 * k], 0.0F),
-                                                 fmaxf(c[2 * k + 1] + s_bias[2 * k + 1], 0.0F));
+                    o[k] = __floats2bfloat162_rn(fmaxf(c[2 * k] + bias_r[2 * k], 0.0F),
+                                                 fmaxf(c[2 * k + 1] + bias_r[2 * k + 1], 0.0F));
                 // planar output [img][N / 8][h][w][8]: each store of a warp is four 128-byte rows
                 const long long plane = (long long)a.h * a.w;
                 uint4* dst = reinterpret_cast<uint4*>(a.y) + (long long)img * (N / 8) * plane + (long long)gy * a.w + gx;
@@ -299,7 +306,7 @@ __global__ void __launch_bounds__(192, 1)
                 const T* src = static_cast<const T*>(a.rgba) + 4 * p;
                 const Rgba x = load_rgba(src);
                 store_rgb_keep_alpha(static_cast<T*>(a.out) + 4 * p,
-                                     Rgba{x.r + (c[0] + s_bias[0]), x.g + (c[1] + s_bias[1]), x.b + (c[2] + s_bias[2]),
+                                     Rgba{x.r + (c[0] + bias_r[0]), x.g + (c[1] + bias_r[1]), x.b + (c[2] + bias_r[2]),
                                           0.0F},
                                      src);
             }
@@ -307,7 +314,7 @@ __global__ void __launch_bounds__(192, 1)
     }
     tc_fence_before();
     __syncthreads();
-    if (warp == 5) {
+    if (warp == kEpiWarps + 1) {
         tc_fence_after();
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;\n" ::"r"(tmem), "r"(kTmemCols));
     }
@@ -330,10 +337,12 @@ PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
 bool make_map(CUtensorMap* map, const bf16* act, int cin, int n, int h, int w) {
     auto fn = encode_fn();
     if (!fn) return false;
-    // [n][cin / 8][h][w][8]: one 8-channel plane per (image, plane) index
-    const cuuint64_t dims[4] = {8, (cuuint64_t)w, (cuuint64_t)h, (cuuint64_t)n * (cuuint64_t)(cin / 8)};
-    const cuuint64_t strides[3] = {16, (cuuint64_t)w * 16, (cuuint64_t)h * w * 16};
-    const cuuint32_t box[4] = {8, (cuuint32_t)kHW, (cuuint32_t)kHH, 1};
+    // [n][cin / 8][h][w][8] seen as rows of w * 8 elements: a box row is one
+    // contiguous 160-byte run (the copy engine fetches whole sectors), and the
+    // x coordinate 8 * px is a multiple of 16 bytes for every pixel px
+    const cuuint64_t dims[4] = {(cuuint64_t)w * 8, (cuuint64_t)h, (cuuint64_t)n * (cuuint64_t)(cin / 8), 1};
+    const cuuint64_t strides[3] = {(cuuint64_t)w * 16, (cuuint64_t)h * w * 16, (cuuint64_t)n * (cin / 8) * h * w * 16};
+    const cuuint32_t box[4] = {(cuuint32_t)kHW * 8, (cuuint32_t)kHH, 1, 1};
     const cuuint32_t es[4] = {1, 1, 1, 1};
     return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 4, const_cast<bf16*>(act), dims, strides, box, es,
               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
@@ -355,7 +364,7 @@ cudaError_t launch(const bf16* x, const bf16* wpk, const TcConvArgs& a, cudaStre
     const long long tiles = (long long)a.n * ((a.h + kTH - 1) / kTH) * ((a.w + kTW - 1) / kTW);
     const long long cap = (long long)kSmCount * 2;
     const int grid = (int)(tiles < cap ? tiles : cap);
-    sg_tc_conv_kernel<CIN, N, EPI, T><<<grid, 192, S::SMEM, st>>>(map, wpk, a);
+    sg_tc_conv_kernel<CIN, N, EPI, T><<<grid, kThreads, S::SMEM, st>>>(map, wpk, a);
     return cudaGetLastError();
 }
 
