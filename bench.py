@@ -189,7 +189,7 @@ def traffic_surrogate_hidden(px):
     """DRAM bytes per hidden-conv launch scaled from the committed ncu capture
     (traffic grows with the pixel count), or None."""
     try:
-        with open(os.path.join(ROOT, "profiles", "traffic_surrogate_conv.json")) as f:
+        with open(os.path.join(ROOT, "profiles", "traffic_surrogate_tc_conv.json")) as f:
             t = json.load(f)
         return int(t["dram_bytes_per_launch"] * px / t["pixels"])
     except Exception:
@@ -406,7 +406,7 @@ def b200_arm(args):
                                         "note": "denoise.bm3d as the reference computes it (2x2 box blend)",
                                         "per_stage_ms": {k: round(v, 4) for k, v in ref_stages.items()}},
         "surrogate_layer_ms": [round(v, 4) for v in layer_ms],
-        "roofline": {"bound": "tensor", "kernel": "sg_conv_kernel<32,32> (hidden 3x3 conv layer)",
+        "roofline": {"bound": "tensor", "kernel": "sg_tc_conv_kernel<32,32> (tcgen05 hidden 3x3 conv layer)",
                      "achieved": round(achieved_tf, 1), "peak": peak_tf, "peak_kind": peak_kind,
                      "unit": "TFLOP/s", "frac": round(achieved_tf / peak_tf, 4),
                      "algorithmic_flop": hidden_flop, "traffic": traffic_surrogate_hidden(w * h)},
