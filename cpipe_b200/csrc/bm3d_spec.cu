@@ -608,6 +608,8 @@ __device__ __forceinline__ void cp_async_wait_all() {
 
 constexpr int kTcWarps = 8;
 constexpr int kStageStride = 72;  // floats per block in a warp's staging buffer (64 + 8: conflict-free float2 stores)
+// blocks staged per round: 4 in stage 2 keeps three CTAs of it within one SM's shared memory
+__host__ __device__ constexpr int tc_stage_blocks(int stage) { return stage == 2 ? 4 : 8; }
 
 // One launch per stage covers every tile: footprints of neighbouring tiles
 // overlap, and the flush adds into the frame accumulators with global
@@ -623,7 +625,8 @@ constexpr int kStageStride = 72;  // floats per block in a warp's staging buffer
 //                atomic per block), and the separable Kaiser window is applied
 //                to that map at the flush.
 template <int STAGE>
-__global__ void __launch_bounds__(32 * kTcWarps, STAGE == 1 ? 3 : 2) bm3d_filter_tc_kernel(FilterArgs a) {
+__global__ void __launch_bounds__(32 * kTcWarps, 3) bm3d_filter_tc_kernel(FilterArgs a) {
+    constexpr int SB = tc_stage_blocks(STAGE);
     extern __shared__ __align__(16) float sm[];
     const int c = blockIdx.z % 3, img = blockIdx.z / 3, row0 = img * a.h;
     const int tx = blockIdx.x, ty = blockIdx.y;
@@ -641,7 +644,7 @@ __global__ void __launch_bounds__(32 * kTcWarps, STAGE == 1 ? 3 : 2) bm3d_filter
     float* s_img = sm + FP;                             // after the groups: the weight map, then den
     float* s_bas = s_img + FP;                          // stage 2
     float* s_aux = s_img + (STAGE == 2 ? 2 : 1) * FP;  // staging buffers (stage 1: at the flush the row-filtered map)
-    float* s_k = s_aux + (STAGE == 2 ? kTcWarps * 8 * kStageStride : max(FP, kTcWarps * 8 * kStageStride));
+    float* s_k = s_aux + (STAGE == 2 ? kTcWarps * SB * kStageStride : max(FP, kTcWarps * SB * kStageStride));
     float* s_k1 = s_k + 64;
     float* s_wgt = s_k1 + 8;
     uint32_t* s_list = reinterpret_cast<uint32_t*>((reinterpret_cast<uintptr_t>(s_wgt + 64) + 15) & ~(uintptr_t)15);
@@ -676,7 +679,7 @@ __global__ void __launch_bounds__(32 * kTcWarps, STAGE == 1 ? 3 : 2) bm3d_filter
     // hard thresholds of the unnormalised coefficients: lambda sigma 2^(k/2)
     const float thr1 = a.thr * 1.41421356237309515F, thr2 = a.thr * 2.0F, thr3 = a.thr * 2.82842712474619030F,
                 thr4 = a.thr * 4.0F;
-    float* stg = s_aux + warp * (8 * kStageStride);
+    float* stg = s_aux + warp * (SB * kStageStride);
     const int ly = lane & 7, lx = lane >> 3;  // a lane's pixel in an 8x4 half-block (y, x) and (y, x + 4)
     const float kq0 = s_k[ly * 8 + lx], kq1 = s_k[ly * 8 + lx + 4];
     for (int k = warp; k < nref; k += kTcWarps) {
@@ -728,22 +731,23 @@ __global__ void __launch_bounds__(32 * kTcWarps, STAGE == 1 ? 3 : 2) bm3d_filter
         if (lane == 0) s_wgt[k] = wgt;
         float X[8][4];
         tc_inverse(H, N, dct, X);
-        // numerator: X -> staging [block][x][y] -> one block's 8x4 half per atomic instruction
+        // numerator: X -> staging [block][x][y], SB blocks per round -> one block's
+        // 8x4 half per atomic instruction
         const float kw0 = wgt * kq0, kw1 = wgt * kq1;
 #pragma unroll
-        for (int hb2 = 0; hb2 < 2; ++hb2) {
-            if (8 * hb2 >= N) break;
+        for (int rb = 0; rb < 16 / SB; ++rb) {
+            if (SB * rb >= N) break;
 #pragma unroll
-            for (int tt = 0; tt < 4; ++tt) {
-                const int t = 4 * hb2 + tt;
+            for (int tt = 0; tt < SB / 2; ++tt) {
+                const int t = rb * (SB / 2) + tt;
                 *reinterpret_cast<float2*>(stg + (2 * tt) * kStageStride + g * 8 + 2 * q) = make_float2(X[t][0], X[t][1]);
                 *reinterpret_cast<float2*>(stg + (2 * tt + 1) * kStageStride + g * 8 + 2 * q) =
                     make_float2(X[t][2], X[t][3]);
             }
             __syncwarp();
-            const int nb = min(8, N - 8 * hb2);
+            const int nb = min(SB, N - SB * rb);
             for (int bb = 0; bb < nb; ++bb) {
-                const uint32_t p = lst[8 * hb2 + bb];
+                const uint32_t p = lst[SB * rb + bb];
                 const int bx = (int)(p & 0xFFFFU) - fx0, by = (int)(p >> 16) - fy0;
                 float* dst = s_num + (by + ly) * P + bx + lx;
                 atomicAdd(dst, kw0 * stg[bb * kStageStride + lane]);
@@ -859,7 +863,7 @@ size_t match_smem(const Bm3dPlan& p) { return sizeof(uint32_t) * 4 * (size_t)p.m
 int tile_pitch(int fw) { return fw + ((4 - fw) % 32 + 32) % 32; }
 size_t filter_tc_smem(const Bm3dPlan& p, int stage) {
     const size_t fp = (size_t)p.fw * tile_pitch(p.fw);
-    const size_t stg = (size_t)kTcWarps * 8 * kStageStride;
+    const size_t stg = (size_t)kTcWarps * tc_stage_blocks(stage) * kStageStride;
     const size_t aux = stage == 2 ? stg : std::max(fp, stg);
     const size_t floats = fp + (stage == 2 ? 2 : 1) * fp + aux + 64 + 8 + 64;
     return sizeof(float) * floats + 16 + sizeof(uint32_t) * kRefTile * kRefTile * 17;
