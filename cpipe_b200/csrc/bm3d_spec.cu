@@ -551,11 +551,11 @@ __device__ __forceinline__ constexpr int haar_k(int b) { return (b & 1) ? 1 : (b
 // 2^e for a small integer e (exact).
 __device__ __forceinline__ float exp2i(int e) { return __int_as_float((127 + e) << 23); }
 
-// Forward 2D DCT and Haar of one group of N blocks read from `img` (row pitch P,
-// footprint origin fx0, fy0).  H[t][e]: block 2t (e < 2) or 2t + 1 (e >= 2),
+// Forward 2D DCT and Haar of one group of N blocks read from `img` (row pitch P;
+// off[b]: block b's offset in the footprint plane).  H[t][e]: block 2t (e < 2) or 2t + 1 (e >= 2),
 // coefficient (v = g, u = 2q + (e & 1)).
-__device__ __forceinline__ void tc_forward(const float* img, int P, const uint32_t* lst, int fx0, int fy0, int N,
-                                           const DctFrags& d, float (&H)[8][4]) {
+__device__ __forceinline__ void tc_forward(const float* img, int P, const int* off, int N, const DctFrags& d,
+                                           float (&H)[8][4]) {
     const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
 #pragma unroll
     for (int t = 0; t < 8; ++t) {
@@ -565,8 +565,7 @@ __device__ __forceinline__ void tc_forward(const float* img, int P, const uint32
 #pragma unroll
         for (int hh = 0; hh < 2; ++hh)
             if (2 * t + hh < N) {
-                const uint32_t p = lst[2 * t + hh];
-                const float* src = img + ((int)(p >> 16) - fy0 + 2 * q) * P + (int)(p & 0xFFFFU) - fx0 + g;
+                const float* src = img + off[2 * t + hh] + 2 * q * P + g;
                 v[hh][0] = src[0];
                 v[hh][1] = src[P];
             }
@@ -649,6 +648,7 @@ __global__ void __launch_bounds__(32 * kTcWarps, 3) bm3d_filter_tc_kernel(Filter
     float* s_wgt = s_k1 + 8;
     uint32_t* s_list = reinterpret_cast<uint32_t*>((reinterpret_cast<uintptr_t>(s_wgt + 64) + 15) & ~(uintptr_t)15);
     uint32_t* s_cnt = s_list + kRefTile * kRefTile * 16;
+    int* s_off = reinterpret_cast<int*>(s_cnt + kRefTile * kRefTile);  // [warp][16] block offsets of the group
     const float* gz = a.noisy + (long long)c * a.npx;
     const float* gb = STAGE == 2 ? a.basic + (long long)c * a.npx : nullptr;
     for (int yy = warp; yy < fh; yy += kTcWarps) {
@@ -686,8 +686,15 @@ __global__ void __launch_bounds__(32 * kTcWarps, 3) bm3d_filter_tc_kernel(Filter
         const int cnt = (int)s_cnt[k];
         const int N = cnt >= 16 ? 16 : cnt >= 8 ? 8 : cnt >= 4 ? 4 : cnt >= 2 ? 2 : 1;
         const uint32_t* lst = s_list + k * 16;
+        int* woff = s_off + warp * 16;
+        __syncwarp();
+        if (lane < 16) {
+            const uint32_t p = lst[lane];
+            woff[lane] = ((int)(p >> 16) - fy0) * P + (int)(p & 0xFFFFU) - fx0;
+        }
+        __syncwarp();
         float H[8][4];
-        tc_forward(s_img, P, lst, fx0, fy0, N, dct, H);
+        tc_forward(s_img, P, woff, N, dct, H);
         const int L = 31 - __clz(N);
         float wgt;
         if (STAGE == 1) {
@@ -709,7 +716,7 @@ __global__ void __launch_bounds__(32 * kTcWarps, 3) bm3d_filter_tc_kernel(Filter
             wgt = kept > 0U ? 1.0F / (float)kept : a.sigma2;
         } else {
             float B[8][4];
-            tc_forward(s_bas, P, lst, fx0, fy0, N, dct, B);
+            tc_forward(s_bas, P, woff, N, dct, B);
             const float s0 = a.sigma2 * exp2i(L), sc0 = exp2i(-L);
             float sw2 = 0.0F;
 #pragma unroll
@@ -747,9 +754,7 @@ __global__ void __launch_bounds__(32 * kTcWarps, 3) bm3d_filter_tc_kernel(Filter
             __syncwarp();
             const int nb = min(SB, N - SB * rb);
             for (int bb = 0; bb < nb; ++bb) {
-                const uint32_t p = lst[SB * rb + bb];
-                const int bx = (int)(p & 0xFFFFU) - fx0, by = (int)(p >> 16) - fy0;
-                float* dst = s_num + (by + ly) * P + bx + lx;
+                float* dst = s_num + woff[SB * rb + bb] + ly * P + lx;
                 atomicAdd(dst, kw0 * stg[bb * kStageStride + lane]);
                 atomicAdd(dst + 4, kw1 * stg[bb * kStageStride + 32 + lane]);
             }
@@ -772,13 +777,17 @@ __global__ void __launch_bounds__(32 * kTcWarps, 3) bm3d_filter_tc_kernel(Filter
     __syncthreads();
     // den = map correlated with the Kaiser window: rows into a free plane, then columns
     float* s_row = STAGE == 2 ? s_bas : s_aux;
+    // (the window comes from the kernel arguments; bounds tests only in the first 7 columns / rows)
     for (int yy = warp; yy < fh; yy += kTcWarps)
         for (int xx = lane; xx < fw; xx += 32) {
             const float* wr = s_w + yy * P + xx;
             float h = 0.0F;
+            if (xx >= 7) {
 #pragma unroll
-            for (int u = 0; u < 8; ++u)
-                if (xx - u >= 0) h = __fmaf_rn(s_k1[u], wr[-u], h);
+                for (int u = 0; u < 8; ++u) h = __fmaf_rn(a.kaiser1[u], wr[-u], h);
+            } else {
+                for (int u = 0; u <= xx; ++u) h = __fmaf_rn(a.kaiser1[u], wr[-u], h);
+            }
             s_row[yy * P + xx] = h;
         }
     __syncthreads();
@@ -787,10 +796,14 @@ __global__ void __launch_bounds__(32 * kTcWarps, 3) bm3d_filter_tc_kernel(Filter
     for (int yy = warp; yy < fh; yy += kTcWarps) {
         const long long o = (long long)(fy0 + yy) * a.w + fx0;
         for (int xx = lane; xx < fw; xx += 32) {
+            const float* cr = s_row + yy * P + xx;
             float d = 0.0F;
+            if (yy >= 7) {
 #pragma unroll
-            for (int v = 0; v < 8; ++v)
-                if (yy - v >= 0) d = __fmaf_rn(s_k1[v], s_row[(yy - v) * P + xx], d);
+                for (int v = 0; v < 8; ++v) d = __fmaf_rn(a.kaiser1[v], cr[-v * P], d);
+            } else {
+                for (int v = 0; v <= yy; ++v) d = __fmaf_rn(a.kaiser1[v], cr[-v * P], d);
+            }
             if (d > 0.0F) {
                 atomicAdd(gn + o + xx, s_num[yy * P + xx]);
                 atomicAdd(gd + o + xx, d);
@@ -866,7 +879,7 @@ size_t filter_tc_smem(const Bm3dPlan& p, int stage) {
     const size_t stg = (size_t)kTcWarps * tc_stage_blocks(stage) * kStageStride;
     const size_t aux = stage == 2 ? stg : std::max(fp, stg);
     const size_t floats = fp + (stage == 2 ? 2 : 1) * fp + aux + 64 + 8 + 64;
-    return sizeof(float) * floats + 16 + sizeof(uint32_t) * kRefTile * kRefTile * 17;
+    return sizeof(float) * floats + 16 + sizeof(uint32_t) * kRefTile * kRefTile * 17 + sizeof(int) * kTcWarps * 16;
 }
 
 }  // namespace
