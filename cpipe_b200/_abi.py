@@ -172,7 +172,7 @@ EXPORTS = [
     "cpipe_b200_params_set_string", "cpipe_b200_params_set_bool", "cpipe_b200_run_node",
     "cpipe_b200_host_last_error",
     "cpipe_cuda_chain_create", "cpipe_cuda_chain_destroy", "cpipe_cuda_chain_output_bytes", "cpipe_cuda_chain_run",
-    "cpipe_cuda_chain_run_host", "cpipe_cuda_pinned_alloc", "cpipe_cuda_pinned_free",
+    "cpipe_cuda_chain_run_host", "cpipe_cuda_chain_run_host_frames", "cpipe_cuda_pinned_alloc", "cpipe_cuda_pinned_free",
     "cpipe_cuda_batch_create", "cpipe_cuda_batch_destroy", "cpipe_cuda_batch_run", "cpipe_cuda_batch_autotune",
     "cpipe_cuda_batch_frame_chain", "cpipe_cuda_chain_set_profiling", "cpipe_cuda_chain_profile", "cpipe_cuda_chain_denoise_stats", "cpipe_cuda_set_device", "cpipe_cuda_device_alloc",
     "cpipe_cuda_device_free", "cpipe_cuda_memcpy_h2d", "cpipe_cuda_memcpy_d2h", "cpipe_cuda_memcpy_d2d_async", "cpipe_cuda_count_nonfinite",
@@ -231,6 +231,7 @@ def lib():
         "cpipe_cuda_chain_create": (vp, [C.POINTER(ChainConfig), C.POINTER(i32)]),
         "cpipe_cuda_chain_destroy": (None, [vp]), "cpipe_cuda_chain_output_bytes": (sz, [vp]),
         "cpipe_cuda_chain_run": (i32, [vp, vp, vp, vp]), "cpipe_cuda_chain_run_host": (i32, [vp, vp, vp, vp]),
+        "cpipe_cuda_chain_run_host_frames": (i32, [vp, vp, vp, i32, vp]),
         "cpipe_cuda_pinned_alloc": (i32, [sz, C.POINTER(vp)]), "cpipe_cuda_pinned_free": (None, [vp]),
         "cpipe_cuda_chain_set_profiling": (i32, [vp, i32]),
         "cpipe_cuda_batch_create": (vp, [vp, sz, C.POINTER(i32)]), "cpipe_cuda_batch_destroy": (None, [vp]),

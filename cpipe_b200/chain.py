@@ -295,6 +295,22 @@ class Chain:
             raise CpipeError(st, "chain_run_host " + A.lib().cpipe_cuda_last_error().decode())
         return out
 
+    def run_host_frames(self, raws, outs=None, stream=None):
+        """Several host frames through cpipe_cuda_chain_run_host_frames (uploads
+        and downloads overlapped with the neighbouring frames' chain)."""
+        raws = [np.ascontiguousarray(r, dtype=np.uint16) for r in raws]
+        for r in raws:
+            assert r.shape == (self.config.height, self.config.width)
+        if outs is None:
+            outs = [np.empty(self.out_shape, self.out_dtype) for _ in raws]
+        n = len(raws)
+        pr = (C.c_void_p * n)(*[r.ctypes.data for r in raws])
+        po = (C.c_void_p * n)(*[o.ctypes.data for o in outs])
+        st = A.lib().cpipe_cuda_chain_run_host_frames(self._h, pr, po, n, stream)
+        if st:
+            raise CpipeError(st, "chain_run_host_frames " + A.lib().cpipe_cuda_last_error().decode())
+        return outs
+
 
 def _main():
     """Run the 12 MP chain a few times on the GPU (used for profiler captures):

@@ -436,10 +436,22 @@ struct cpipe_cuda_chain {
     bool profiling = false;
     std::vector<cudaEvent_t> events;
     size_t profiled = 0;
-    cudaGraphExec_t graph = nullptr;
-    const void* graph_in = nullptr;
-    void* graph_out = nullptr;
-    cudaStream_t graph_stream = nullptr;
+    // captured graphs, one per (input, output, stream) triple seen, least recently used replaced
+    struct GraphSlot {
+        cudaGraphExec_t exec = nullptr;
+        const void* in = nullptr;
+        void* out = nullptr;
+        cudaStream_t stream = nullptr;
+        unsigned long long used = 0;
+    };
+    static constexpr int kGraphSlots = 8;
+    GraphSlot graphs[kGraphSlots];
+    unsigned long long graph_clock = 0;
+    // run_host_frames: two device frames each way, copy streams and their events
+    void* d_pipe_in[2] = {nullptr, nullptr};
+    void* d_pipe_out[2] = {nullptr, nullptr};
+    cudaStream_t s_h2d = nullptr, s_d2h = nullptr;
+    cudaEvent_t ev_in[2] = {nullptr, nullptr}, ev_done[2] = {nullptr, nullptr}, ev_out[2] = {nullptr, nullptr};
 };
 
 namespace {
@@ -729,7 +741,15 @@ cpipe_cuda_chain* cpipe_cuda_chain_create(const cpipe_cuda_chain_config* cfg, in
 void cpipe_cuda_chain_destroy(cpipe_cuda_chain* c) {
     if (!c) return;
     for (cudaEvent_t e : c->events) cudaEventDestroy(e);
-    if (c->graph) cudaGraphExecDestroy(c->graph);
+    for (auto& g : c->graphs)
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+    for (void* p : c->d_pipe_in) cudaFree(p);
+    for (void* p : c->d_pipe_out) cudaFree(p);
+    for (int k = 0; k < 2; ++k)
+        for (cudaEvent_t e : {c->ev_in[k], c->ev_done[k], c->ev_out[k]})
+            if (e) cudaEventDestroy(e);
+    if (c->s_h2d) cudaStreamDestroy(c->s_h2d);
+    if (c->s_d2h) cudaStreamDestroy(c->s_d2h);
     cudaFree(c->d_tables);
     cudaFree(c->d_denoise);
     cudaFree(c->d_bayer);
@@ -755,9 +775,17 @@ int cpipe_cuda_chain_run(cpipe_cuda_chain* c, const void* d_raw, void* d_out, vo
     if (!c || !d_raw || !d_out) return CPIPE_BAD_INDEX;
     const cudaStream_t st = static_cast<cudaStream_t>(stream);
     if (c->cfg.use_graph && c->warp_mode != 2 && !c->profiling) {
-        if (!c->graph || c->graph_in != d_raw || c->graph_out != d_out || c->graph_stream != st) {
-            if (c->graph) cudaGraphExecDestroy(c->graph);
-            c->graph = nullptr;
+        using Slot = cpipe_cuda_chain::GraphSlot;
+        Slot* hit = nullptr;
+        Slot* lru = &c->graphs[0];
+        for (Slot& g : c->graphs) {
+            if (g.exec && g.in == d_raw && g.out == d_out && g.stream == st) hit = &g;
+            if (!g.exec || (lru->exec && g.used < lru->used)) lru = &g;
+        }
+        if (!hit) {
+            hit = lru;
+            if (hit->exec) cudaGraphExecDestroy(hit->exec);
+            hit->exec = nullptr;
             cudaGraph_t g;
             cudaStream_t cap = st;
             cudaStream_t own = nullptr;
@@ -772,16 +800,17 @@ int cpipe_cuda_chain_run(cpipe_cuda_chain* c, const void* d_raw, void* d_out, vo
                 if (ls != CPIPE_OK) s = ls;
             }
             if (s == CPIPE_OK) {
-                s = cuda_status(cudaGraphInstantiate(&c->graph, g, cudaGraphInstantiateFlagUseNodePriority), "instantiate");
+                s = cuda_status(cudaGraphInstantiate(&hit->exec, g, cudaGraphInstantiateFlagUseNodePriority), "instantiate");
                 cudaGraphDestroy(g);
             }
             if (own) cudaStreamDestroy(own);
             if (s != CPIPE_OK) return s;
-            c->graph_in = d_raw;
-            c->graph_out = d_out;
-            c->graph_stream = st;
+            hit->in = d_raw;
+            hit->out = d_out;
+            hit->stream = st;
         }
-        return cuda_status(cudaGraphLaunch(c->graph, st), "graph launch");
+        hit->used = ++c->graph_clock;
+        return cuda_status(cudaGraphLaunch(hit->exec, st), "graph launch");
     }
     return launch_chain(c, d_raw, 0, d_out, 0, st);
 }
@@ -798,6 +827,50 @@ int cpipe_cuda_chain_run_host(cpipe_cuda_chain* c, const uint16_t* h_raw, void* 
         s = cuda_status(cudaMemcpyAsync(h_out, c->d_io[1], c->frame_bytes, cudaMemcpyDeviceToHost, st), "chain D2H");
     const int ss = cuda_status(cudaStreamSynchronize(st), "chain sync");
     return s != CPIPE_OK ? s : ss;
+}
+
+int cpipe_cuda_chain_run_host_frames(cpipe_cuda_chain* c, const uint16_t* const* h_raws, void* const* h_outs, int n,
+                                     void* stream) {
+    if (!c || !h_raws || !h_outs || n < 0) return CPIPE_BAD_INDEX;
+    for (int i = 0; i < n; ++i)
+        if (!h_raws[i] || !h_outs[i]) return CPIPE_BAD_INDEX;
+    if (n == 0) return CPIPE_OK;
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const size_t raw_bytes = (size_t)c->cfg.width * c->cfg.height * sizeof(uint16_t);
+    for (int k = 0; k < 2; ++k) {
+        if (!c->d_pipe_in[k] && cudaMalloc(&c->d_pipe_in[k], raw_bytes) != cudaSuccess) return CPIPE_OOM;
+        if (!c->d_pipe_out[k] && cudaMalloc(&c->d_pipe_out[k], c->frame_bytes) != cudaSuccess) return CPIPE_OOM;
+        for (cudaEvent_t* e : {&c->ev_in[k], &c->ev_done[k], &c->ev_out[k]})
+            if (!*e && cudaEventCreateWithFlags(e, cudaEventDisableTiming) != cudaSuccess) return CPIPE_INTERNAL_ERROR;
+    }
+    if (!c->s_h2d && cudaStreamCreateWithFlags(&c->s_h2d, cudaStreamNonBlocking) != cudaSuccess) return CPIPE_INTERNAL_ERROR;
+    if (!c->s_d2h && cudaStreamCreateWithFlags(&c->s_d2h, cudaStreamNonBlocking) != cudaSuccess) return CPIPE_INTERNAL_ERROR;
+    // Frame i uses device frames k = i & 1: its upload waits until frame i - 2's
+    // chain has read input k, its chain until the upload is in and frame i - 2's
+    // download has emptied output k; the download follows the chain.
+    int s = CPIPE_OK;
+    for (int i = 0; i < n && s == CPIPE_OK; ++i) {
+        const int k = i & 1;
+        if (i >= 2) s = cuda_status(cudaStreamWaitEvent(c->s_h2d, c->ev_done[k], 0), "pipe wait");
+        if (s == CPIPE_OK)
+            s = cuda_status(cudaMemcpyAsync(c->d_pipe_in[k], h_raws[i], raw_bytes, cudaMemcpyHostToDevice, c->s_h2d),
+                            "pipe H2D");
+        if (s == CPIPE_OK) s = cuda_status(cudaEventRecord(c->ev_in[k], c->s_h2d), "pipe record");
+        if (s == CPIPE_OK) s = cuda_status(cudaStreamWaitEvent(st, c->ev_in[k], 0), "pipe wait");
+        if (s == CPIPE_OK && i >= 2) s = cuda_status(cudaStreamWaitEvent(st, c->ev_out[k], 0), "pipe wait");
+        if (s == CPIPE_OK) s = cpipe_cuda_chain_run(c, c->d_pipe_in[k], c->d_pipe_out[k], stream);
+        if (s == CPIPE_OK) s = cuda_status(cudaEventRecord(c->ev_done[k], st), "pipe record");
+        if (s == CPIPE_OK) s = cuda_status(cudaStreamWaitEvent(c->s_d2h, c->ev_done[k], 0), "pipe wait");
+        if (s == CPIPE_OK)
+            s = cuda_status(cudaMemcpyAsync(h_outs[i], c->d_pipe_out[k], c->frame_bytes, cudaMemcpyDeviceToHost, c->s_d2h),
+                            "pipe D2H");
+        if (s == CPIPE_OK) s = cuda_status(cudaEventRecord(c->ev_out[k], c->s_d2h), "pipe record");
+    }
+    // every queued copy and chain finishes before the call returns, also after an error
+    const int s1 = cuda_status(cudaStreamSynchronize(c->s_h2d), "pipe sync");
+    const int s2 = cuda_status(cudaStreamSynchronize(st), "pipe sync");
+    const int s3 = cuda_status(cudaStreamSynchronize(c->s_d2h), "pipe sync");
+    return s != CPIPE_OK ? s : s1 != CPIPE_OK ? s1 : s2 != CPIPE_OK ? s2 : s3;
 }
 
 int cpipe_cuda_chain_set_profiling(cpipe_cuda_chain* c, int enable) {

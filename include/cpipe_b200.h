@@ -243,6 +243,14 @@ size_t cpipe_cuda_chain_output_bytes(const cpipe_cuda_chain* chain);
 int cpipe_cuda_chain_run(cpipe_cuda_chain* chain, const void* d_raw_u16, void* d_out, void* stream);
 /* Host pointers: H2D of the raw frame, the chain, D2H of the result; returns after the copy-out. */
 int cpipe_cuda_chain_run_host(cpipe_cuda_chain* chain, const uint16_t* h_raw, void* h_out, void* stream);
+/* n frames from host memory, pipelined: frame i's upload and download overlap
+ * the chain of its neighbours (two device frames each way, copy streams of the
+ * chain's own); h_outs[i] receives frame i's result, the same bytes run_host
+ * gives.  Returns after every frame is back.  Pinned host buffers let the
+ * copies run asynchronously.  (The reference's filters take one frame per
+ * call, HalideFilterRegistry.hpp:18-21; this is the batched form of run_host.) */
+int cpipe_cuda_chain_run_host_frames(cpipe_cuda_chain* chain, const uint16_t* const* h_raws, void* const* h_outs,
+                                     int n, void* stream);
 /* Per-stage timing: while enabled, each run records CUDA events around its
  * stages (and bypasses the graph); chain_profile sums the stage times of the
  * runs recorded since the last call: [0] raw_to_rgba, [1] warp_wb_cm,

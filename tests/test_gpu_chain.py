@@ -226,3 +226,27 @@ def test_qbc_50mp_remosaic_and_bm3d_precision_forms(cuda_device):
         err, p = float(np.abs(g - w_).max()), bpsnr(g, w_)
         print(f"50 MP BM3D {form}: max-abs {err:.3g} PSNR {p:.1f} dB vs FP64 oracle")
         assert p >= 55.0 and err <= 5e-3
+
+
+@pytest.mark.parametrize("mode", ["reference", "surrogate"])
+def test_run_host_frames_matches_run_host(cuda_device, mode):
+    """The pipelined host entry point (uploads and downloads overlapping the
+    neighbouring frames' chain, two device frames each way, several graphs)
+    returns for every frame what run_host returns for it alone; five distinct
+    frames so both staging slots are reused."""
+    from cpipe_b200 import surrogate as S
+    kw = dict(width=320, height=288)
+    if mode == "surrogate":
+        kw.update(denoise="surrogate", surrogate_blob=S.load_weights())
+    chain = Chain(ChainConfig.full_12mp(**kw))
+    raw0 = chain.config.make_raw()
+    raws = [np.ascontiguousarray(np.roll(raw0, (2 * k, 4 * k), axis=(0, 1))) for k in range(5)]
+    want = [chain.run_host(r) for r in raws]
+    got = chain.run_host_frames(raws)
+    for k in range(5):
+        if mode == "reference":
+            np.testing.assert_array_equal(got[k].view(np.uint16), want[k].view(np.uint16), err_msg=f"frame {k}")
+        else:  # a spot-check fallback would add BM3D, whose last bits vary between runs
+            np.testing.assert_allclose(got[k].astype(np.float32), want[k].astype(np.float32), rtol=2e-3, atol=2e-3,
+                                       err_msg=f"frame {k}")
+    chain.close()
