@@ -108,6 +108,12 @@ class WaveletBayesShrinkParams(C.Structure):
     _fields_ = [("chroma_strength", C.c_float)]
 
 
+class AtrousWaveletParams(C.Structure):
+    """cpipe_AtrousWaveletParams (a-trous wavelet denoiser, aot_id denoise_wavelet_atrous_spec)."""
+    _fields_ = [("levels", C.c_int32), ("sigma", C.c_float), ("luma_strength", C.c_float),
+                ("chroma_strength", C.c_float)]
+
+
 class FilmicRgbParams(C.Structure):
     _fields_ = [(n, C.c_float) for n in ("ev", "contrast", "saturation", "highlights", "shadows")]
 
@@ -151,6 +157,7 @@ EXPORTS = [
     "cpipe_cuda_lens_shading_gainmap", "cpipe_cuda_demosaic_bilinear", "cpipe_cuda_demosaic_rcd",
     "cpipe_cuda_demosaic_amaze", "cpipe_cuda_wb_dual_illuminant", "cpipe_cuda_colormatrix_dng_to_working",
     "cpipe_cuda_denoise_bm3d_step1", "cpipe_cuda_denoise_bm3d_step2", "cpipe_cuda_denoise_bm3d_spec",
+    "cpipe_cuda_denoise_guided_filter_spec", "cpipe_cuda_denoise_wavelet_atrous_spec",
     "cpipe_cuda_denoise_guided_filter",
     "cpipe_cuda_denoise_wavelet_bayes_shrink", "cpipe_cuda_lens_dng_opcode_list_3", "cpipe_cuda_color_3d_lut",
     "cpipe_cuda_tone_filmic_rgb", "cpipe_cuda_copy", "cpipe_cuda_filters", "cpipe_cuda_find_filter",

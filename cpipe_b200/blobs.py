@@ -66,6 +66,11 @@ def guided(radius, eps):
     return raw(A.GuidedFilterParams(int(radius), float(eps)))
 
 
+def atrous(levels=5, sigma=0.03, luma_strength=1.0, chroma_strength=1.0):
+    """cpipe_AtrousWaveletParams for denoise_wavelet_atrous_spec."""
+    return raw(A.AtrousWaveletParams(int(levels), float(sigma), float(luma_strength), float(chroma_strength)))
+
+
 def wavelet(strength):
     return raw(A.WaveletBayesShrinkParams(float(strength)))
 

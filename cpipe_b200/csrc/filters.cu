@@ -18,6 +18,7 @@
 
 #include "../../include/cpipe_b200.h"
 #include "bm3d_spec.h"
+#include "spec_denoise.h"
 #include "filters_impl.h"
 #include "kernels.h"
 
@@ -553,6 +554,50 @@ int cpipe_cuda_denoise_bm3d_spec(halide_buffer_t* const* inputs, size_t n_in, ha
     if (!plan.copy && (st = call.alloc(plan.bytes, &scratch)) != CPIPE_OK) return call.finish(st);
     return call.finish(cuda_status(bm3d_run(plan, in.img, out.img, in.elem == 2, scratch, call.stream), "bm3d_spec"));
 }
+int cpipe_cuda_denoise_guided_filter_spec(halide_buffer_t* const* inputs, size_t n_in,
+                                          halide_buffer_t* const* outputs, size_t n_out, const void* blob,
+                                          size_t blob_size) {
+    CHECK_ARITY(1, 1);
+    if (blob == nullptr || blob_size < sizeof(cpipe_GuidedFilterParams)) return CPIPE_BAD_INDEX;
+    cpipe_GuidedFilterParams prm;
+    std::memcpy(&prm, blob, sizeof(prm));
+    if (prm.radius < 1 || prm.radius > kGuidedSpecMaxRadius || !(prm.eps > 0.0F) || !std::isfinite(prm.eps)) {
+        set_error("guided_filter_spec: %s", "radius must be 1..16 and eps positive");
+        return CPIPE_BAD_INDEX;
+    }
+    if (!device_ready()) return CPIPE_INTERNAL_ERROR;
+    static const cudaError_t setup = guided_spec_setup();
+    if (setup != cudaSuccess) return cuda_status(setup, "guided_filter_spec setup");
+    Call call;
+    Bound in, out;
+    const int st = rgba_pair(call, inputs, outputs, &in, &out);
+    if (st != CPIPE_OK) return call.finish(st);
+    return call.finish(
+        cuda_status(guided_spec_run(in.img, out.img, in.elem == 2, prm.radius, prm.eps, call.stream), "guided_spec"));
+}
+int cpipe_cuda_denoise_wavelet_atrous_spec(halide_buffer_t* const* inputs, size_t n_in,
+                                           halide_buffer_t* const* outputs, size_t n_out, const void* blob,
+                                           size_t blob_size) {
+    CHECK_ARITY(1, 1);
+    if (blob == nullptr || blob_size < sizeof(cpipe_AtrousWaveletParams)) return CPIPE_BAD_INDEX;
+    cpipe_AtrousWaveletParams prm;
+    std::memcpy(&prm, blob, sizeof(prm));
+    if (!device_ready()) return CPIPE_INTERNAL_ERROR;
+    static const cudaError_t setup = atrous_setup();
+    if (setup != cudaSuccess) return cuda_status(setup, "wavelet_atrous_spec setup");
+    Call call;
+    Bound in, out;
+    int st = rgba_pair(call, inputs, outputs, &in, &out);
+    if (st != CPIPE_OK) return call.finish(st);
+    AtrousPlan plan;
+    if ((st = atrous_plan(&prm, in.img.w, in.img.h, &plan)) != CPIPE_OK) {
+        set_error("wavelet_atrous_spec: %s", "parameters out of range");
+        return call.finish(st);
+    }
+    void* scratch = nullptr;
+    if (!plan.copy && (st = call.alloc(plan.bytes, &scratch)) != CPIPE_OK) return call.finish(st);
+    return call.finish(cuda_status(atrous_run(plan, in.img, out.img, in.elem == 2, scratch, call.stream), "atrous"));
+}
 int cpipe_cuda_denoise_guided_filter(halide_buffer_t* const* inputs, size_t n_in, halide_buffer_t* const* outputs,
                                      size_t n_out, const void* blob, size_t blob_size) {
     CHECK_ARITY(1, 1);
@@ -842,6 +887,8 @@ static const cpipe_cuda_filter_desc kFilters[] = {
     {"denoise_bm3d_spec", (void*)&cpipe_cuda_denoise_bm3d_spec, 1},
     {"denoise_guided_filter", (void*)&cpipe_cuda_denoise_guided_filter, 1},
     {"denoise_wavelet_bayes_shrink", (void*)&cpipe_cuda_denoise_wavelet_bayes_shrink, 1},
+    {"denoise_guided_filter_spec", (void*)&cpipe_cuda_denoise_guided_filter_spec, 1},
+    {"denoise_wavelet_atrous_spec", (void*)&cpipe_cuda_denoise_wavelet_atrous_spec, 1},
     {"lens_dng_opcode_list_3", (void*)&cpipe_cuda_lens_dng_opcode_list_3, 1},
     {"color_3d_lut", (void*)&cpipe_cuda_color_3d_lut, 1},
     {"tone_filmic_rgb", (void*)&cpipe_cuda_tone_filmic_rgb, 1},

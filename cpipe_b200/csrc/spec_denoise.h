@@ -1,0 +1,43 @@
+// Spec-mode guided filter and a-trous wavelet denoiser: host plans and
+// launchers shared by the filter entries and the fused chain.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stddef.h>
+
+#include "../../include/cpipe_b200_params.h"
+#include "common.cuh"
+
+namespace cpb {
+
+constexpr int kGuidedSpecMaxRadius = 16;
+constexpr int kAtrousMaxLevels = 6;
+
+// Guided filter with a true (2r+1)^2 box, r in 1..kGuidedSpecMaxRadius; RGBA
+// in and out (binary16 when f16, else float32), alpha copied.  No scratch.
+cudaError_t guided_spec_setup();
+cudaError_t guided_spec_run(const Img& in, const Img& out, bool f16, int radius, float eps, cudaStream_t stream);
+
+struct AtrousPlan {
+    int w = 0, h = 0, levels = 0;
+    int gx = 0, gy = 0;          // level-kernel grid (partial sums per CTA)
+    float noise[kAtrousMaxLevels][3] = {};  // band noise std per level and channel (Y, Co, Cg)
+    float strength[3] = {};
+    bool copy = false;           // levels 0: output = input
+    size_t off_c0 = 0, off_c1 = 0, off_w = 0, off_part = 0, off_thr = 0, bytes = 0;
+};
+
+// Validates the parameters (CPIPE_BAD_INDEX when out of range) and sizes the
+// scratch buffer for a w x h frame.
+int atrous_plan(const cpipe_AtrousWaveletParams* p, int w, int h, AtrousPlan* out);
+// Sets the level kernel's shared-memory limit (host side; before a capture).
+cudaError_t atrous_setup();
+// RGBA in -> RGBA out; scratch: plan.bytes of device memory, 256-byte aligned.
+cudaError_t atrous_run(const AtrousPlan& plan, const Img& in, const Img& out, bool f16, void* scratch,
+                       cudaStream_t stream);
+
+// White-noise gain of level j (1-based) of the B3-spline a-trous transform in
+// 2D: the L2 norm of its detail filter (exact, from the filter taps).
+double atrous_band_gain(int level);
+
+}  // namespace cpb

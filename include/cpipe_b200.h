@@ -81,6 +81,17 @@ CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_denoise_bm3d_step2);         /* bm3d_dispatch
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_denoise_bm3d_spec);
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_denoise_guided_filter);      /* guided_filter_dispatch.cpp */
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_denoise_wavelet_bayes_shrink); /* wavelet_bayes_shrink_dispatch.cpp */
+/* Guided filter with a true (2r+1)^2 box (aot_id "denoise_guided_filter_spec",
+ * blob cpipe_GuidedFilterParams, radius 1..16): the reference's
+ * guided_filter formula (guided_filter_generator.cpp:45-85) without its
+ * clamp of every radius above 1 to a 5x5 box.  The guided_filter node selects
+ * it with param algorithm = "spec". */
+CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_denoise_guided_filter_spec);
+/* Multi-level a-trous wavelet denoiser (aot_id "denoise_wavelet_atrous_spec",
+ * blob cpipe_AtrousWaveletParams); the wavelet_bayes_shrink node selects it
+ * with param algorithm = "atrous".  No reference filter counterpart (the
+ * reference's node is one 2x2 Haar level on chroma). */
+CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_denoise_wavelet_atrous_spec);
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_lens_dng_opcode_list_3);     /* dng_opcode_list_3_dispatch.cpp:333-398 */
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_color_3d_lut);               /* lut3d_dispatch.cpp:20-60 */
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_tone_filmic_rgb);            /* filmic_rgb_dispatch.cpp:22-36 */

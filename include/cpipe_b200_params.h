@@ -145,6 +145,23 @@ typedef struct {
     float chroma_strength;
 } cpipe_WaveletBayesShrinkParams;
 
+/* Multi-level a-trous wavelet denoiser ("spec mode"; aot_id
+ * denoise_wavelet_atrous_spec).  The reference's denoise.wavelet_bayes_shrink
+ * node is a single-level 2x2 Haar chroma shrink
+ * (nodes/denoise/wavelet_bayes_shrink_generator.cpp:57-86); this is the
+ * undecimated form that the node is named after, on the node's own colour
+ * space (Y = (r+2g+b)/4, Co = r-b, Cg = g-(r+b)/2): B3-spline a-trous
+ * decomposition (Starck, Murtagh, "Image restoration with noise suppression
+ * using the wavelet transform", A&A 288, 1994), per band soft thresholds of
+ * BayesShrink form (Chang, Yu, Vetterli, IEEE TIP 9(9), 2000),
+ * T = sigma_n^2 / sigma_x.  There is no reference counterpart. */
+typedef struct {
+    int32_t levels;         /* detail levels, 0..6 (5); 0 copies */
+    float sigma;            /* noise standard deviation per RGB channel (linear units) */
+    float luma_strength;    /* threshold scale on Y (1); 0 leaves Y unchanged */
+    float chroma_strength;  /* threshold scale on Co and Cg (1) */
+} cpipe_AtrousWaveletParams;
+
 typedef struct {
     float ev;
     float contrast;
@@ -209,6 +226,7 @@ CPIPE_STATIC_ASSERT(sizeof(cpipe_Opcode3DispatchRecord) == 320, "Opcode3Dispatch
 CPIPE_STATIC_ASSERT(sizeof(cpipe_Lut3dParamHeader) == 12, "Lut3dParamHeader layout");
 CPIPE_STATIC_ASSERT(sizeof(cpipe_Bm3dSpecParams) == 40, "Bm3dSpecParams layout");
 CPIPE_STATIC_ASSERT(sizeof(cpipe_SurrogateHeader) == 32, "SurrogateHeader layout");
+CPIPE_STATIC_ASSERT(sizeof(cpipe_AtrousWaveletParams) == 16, "AtrousWaveletParams layout");
 
 #ifdef __cplusplus
 } /* extern "C" */

@@ -1,0 +1,80 @@
+"""Spec-mode guided filter (denoise_guided_filter_spec) and a-trous wavelet
+denoiser (denoise_wavelet_atrous_spec) on the GPU against the FP64 oracle
+(oracle/oracle_spec_denoise.py): float32 frames within max-abs 1e-4 and PSNR
+>= 60 dB, binary16 frames within one binary16 ulp and PSNR >= 60 dB; odd and
+tiny sizes; every radius class and level count; the parameter refusals; and
+at radius 1 and 2 the spec guided filter against the GPU's parity guided
+filter (the reference's own computation)."""
+import numpy as np
+import oracle_spec_denoise as S
+import pytest
+from bm3d_scenes import clean_rgb, noisy_rgba
+from cpipe_b200 import blobs, call_filter, last_error
+from parity import assert_f16_parity, assert_f32_parity
+
+pytestmark = pytest.mark.gpu
+
+
+def run(aot, x, blob):
+    out = np.zeros_like(x)
+    st = call_filter(aot, [x], [out], blob)
+    assert st == 0, f"{aot}: status {st}: {last_error()}"
+    return out
+
+
+def frame(h, w, sigma, seed, dtype):
+    return noisy_rgba(clean_rgb(seed, h, w, rects=12), sigma, seed, dtype=dtype)
+
+
+def check(got, want, dtype, what):
+    if dtype == np.float16:
+        assert_f16_parity(got, want, what=what)
+    else:
+        assert_f32_parity(got, want, max_abs=1e-4, what=what)
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float16])
+@pytest.mark.parametrize("h,w,radius,eps", [(70, 53, 1, 1e-3), (129, 257, 4, 1e-3), (96, 128, 8, 1e-3),
+                                            (61, 75, 16, 5e-3), (5, 9, 8, 1e-3)])
+def test_guided_spec_matches_oracle(cuda_device, dtype, h, w, radius, eps):
+    x = frame(h, w, 0.03, h + w, dtype)
+    got = run("denoise_guided_filter_spec", x, blobs.guided(radius, eps))
+    want = S.guided_spec(x.astype(np.float64), radius, eps)
+    check(got, want, dtype, f"guided spec r={radius} {w}x{h} {np.dtype(dtype).name}")
+    np.testing.assert_array_equal(got[..., 3], x[..., 3])
+
+
+@pytest.mark.parametrize("radius", [1, 2])
+def test_guided_spec_equals_parity_filter_at_small_radius(cuda_device, radius):
+    x = frame(80, 96, 0.03, 4, np.float32)
+    spec = run("denoise_guided_filter_spec", x, blobs.guided(radius, 1e-3))
+    ref = run("denoise_guided_filter", x, blobs.guided(radius, 1e-3))
+    assert_f32_parity(spec, ref, max_abs=1e-5, what=f"spec vs reference guided r={radius}")
+
+
+@pytest.mark.parametrize("dtype", [np.float32, np.float16])
+@pytest.mark.parametrize("h,w,levels,lumas,chromas", [(96, 64, 5, 1.0, 1.0), (201, 300, 6, 1.0, 1.0),
+                                                      (17, 33, 3, 0.0, 2.0), (64, 96, 1, 1.0, 0.5)])
+def test_atrous_matches_oracle(cuda_device, dtype, h, w, levels, lumas, chromas):
+    sigma = 0.03
+    x = frame(h, w, sigma, 7 * h + w, dtype)
+    got = run("denoise_wavelet_atrous_spec", x, blobs.atrous(levels, sigma, lumas, chromas))
+    want = S.atrous_spec(x.astype(np.float64), levels, sigma, lumas, chromas)
+    check(got, want, dtype, f"a-trous L={levels} {w}x{h} {np.dtype(dtype).name}")
+    np.testing.assert_array_equal(got[..., 3], x[..., 3])
+
+
+def test_atrous_zero_levels_copies(cuda_device):
+    x = frame(40, 50, 0.03, 1, np.float16)
+    got = run("denoise_wavelet_atrous_spec", x, blobs.atrous(0, 0.03))
+    np.testing.assert_array_equal(got.view(np.uint16), x.view(np.uint16))
+
+
+def test_spec_filters_refuse_out_of_range(cuda_device):
+    x = frame(16, 16, 0.03, 1, np.float32)
+    out = np.zeros_like(x)
+    assert call_filter("denoise_guided_filter_spec", [x], [out], blobs.guided(17, 1e-3)) != 0
+    assert call_filter("denoise_guided_filter_spec", [x], [out], blobs.guided(0, 1e-3)) != 0
+    assert call_filter("denoise_guided_filter_spec", [x], [out], blobs.guided(4, 0.0)) != 0
+    assert call_filter("denoise_wavelet_atrous_spec", [x], [out], blobs.atrous(7, 0.03)) != 0
+    assert call_filter("denoise_wavelet_atrous_spec", [x], [out], blobs.atrous(5, -1.0)) != 0
