@@ -128,7 +128,8 @@ class ChainConfig(C.Structure):
                 ("plain_f32", C.c_int32), ("use_graph", C.c_int32), ("denoise_mode", C.c_int32),
                 ("bm3d_spec", Bm3dSpecParams), ("surrogate_blob", C.c_void_p), ("surrogate_blob_size", C.c_size_t),
                 ("noise_a", C.c_float), ("noise_b", C.c_float), ("stop_after", C.c_int32),
-                ("spot_tiles", C.c_int32), ("spot_min_psnr_db", C.c_float), ("quad_bayer", C.c_int32)]
+                ("spot_tiles", C.c_int32), ("spot_min_psnr_db", C.c_float), ("quad_bayer", C.c_int32),
+                ("guided_spec", C.c_int32), ("atrous_levels", C.c_int32), ("atrous_luma_strength", C.c_float)]
 
 
 MAIN_ENTRY = C.CFUNCTYPE(C.c_int, C.c_char_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p)

@@ -88,6 +88,9 @@ class ChainConfig:
     quad_bayer: bool = False       # raw input is a Sony Quad-Bayer mosaic, remosaiced first
     spot_tiles: int = 16           # surrogate spot check: BM3D on this many 256x256 tiles per frame
     spot_min_psnr_db: float = 40.0  # ... and BM3D for the whole frame when a tile is below this
+    guided_spec: bool = False      # guided filter with the true (2r+1)^2 box (radius 1..16)
+    atrous_levels: int = 0         # > 0: a-trous wavelet denoiser with that many levels instead of the 2x2 Haar
+    atrous_luma_strength: float = 1.0
 
     # ------------------------------------------------------------ workloads
     @classmethod
@@ -243,6 +246,9 @@ class ChainConfig:
         cfg.spot_tiles = int(self.spot_tiles)
         cfg.spot_min_psnr_db = float(self.spot_min_psnr_db)
         cfg.quad_bayer = int(self.quad_bayer)
+        cfg.guided_spec = int(self.guided_spec)
+        cfg.atrous_levels = int(self.atrous_levels)
+        cfg.atrous_luma_strength = float(self.atrous_luma_strength)
         return cfg, keep
 
 

@@ -24,6 +24,7 @@
 #include "filters_impl.h"
 #include "kernels.h"
 #include "bm3d_spec.h"
+#include "spec_denoise.h"
 #include "surrogate.h"
 #include "demosaic.cuh"
 #include "nodes.cuh"
@@ -425,6 +426,11 @@ struct cpipe_cuda_chain {
     void* d_tile_scratch = nullptr;
     float* d_tile_mse = nullptr;          // per-tile partial sums of squared differences
     int* d_gate = nullptr;                // 1: fall back to BM3D for this frame
+    // spec-mode stages between the denoiser and denoise_tone (0: none)
+    bool spec_stages = false;
+    bool guided_spec = false;
+    AtrousPlan atrous{};
+    void* d_atrous = nullptr;
     SpotStats* d_stats = nullptr;
     // The tiles' BM3D runs on a second stream beside the network (both read
     // only the denoiser's input), forked after K2 and joined before the MSE.
@@ -558,11 +564,39 @@ int launch_chain(cpipe_cuda_chain* c, const void* d_raw, size_t raw_pitch, void*
         if (e != cudaSuccess) return cuda_status(e, "chain denoise");
         k2_out = dn_out;
     }
-    if (ev) cudaEventRecord(ev[3], st);
     if (c->stop_after == 2) {
+        if (ev) cudaEventRecord(ev[3], st);
         if (ev) cudaEventRecord(ev[4], st);
         return cuda_status(cudaGetLastError(), "chain launch");
     }
+    if (c->spec_stages) {
+        // bm3d (mode 0: the reference's 2x2 blend, here as its own kernel) ->
+        // guided -> wavelet, ping-ponging between the two scratch frames; the
+        // tone kernel then runs filmic and the LUT (its blend at strength 0 is
+        // the identity on these non-negative values)
+        auto other = [&](const Img& cur) { return cur.data == mid0.data ? mid1 : mid0; };
+        Img x = k2_out;
+        cudaError_t e = cudaSuccess;
+        if (c->denoise_mode == 0) {
+            const Img y = other(x);
+            e = launch_bm3d_parity(x, y, c->f16, c->cfg.bm3d_sigma, st);
+            x = y;
+        }
+        if (e == cudaSuccess && c->cfg.guided_radius > 0) {
+            const Img y = other(x);
+            e = c->guided_spec ? guided_spec_run(x, y, c->f16, c->cfg.guided_radius, c->cfg.guided_eps, st)
+                               : launch_guided(x, y, c->f16, c->cfg.guided_radius, c->cfg.guided_eps, st);
+            x = y;
+        }
+        if (e == cudaSuccess && c->atrous.levels > 0) {
+            const Img y = other(x);
+            e = atrous_run(c->atrous, x, y, c->f16, c->d_atrous, st);
+            x = y;
+        }
+        if (e != cudaSuccess) return cuda_status(e, "chain spec stages");
+        k2_out = x;
+    }
+    if (ev) cudaEventRecord(ev[3], st);
     const dim3 gc((unsigned)((w + kCTW - 1) / kCTW), (unsigned)((h + kCTH - 1) / kCTH));
 #define K3(TT, F, R)                                                                                       \
     denoise_tone_kernel<TT, F, R><<<gc, 256, denoise_tone_smem<TT, F, R>(), st>>>(k2_out, out, c->tone);
@@ -723,6 +757,25 @@ cpipe_cuda_chain* cpipe_cuda_chain_create(const cpipe_cuda_chain_config* cfg, in
     // is 3x3 for radius <= 1 and 5x5 above (guided_filter_generator.cpp:66-70).
     c->radius = cfg->guided_radius <= 0 ? 0 : (cfg->guided_radius == 1 ? 1 : 2);
     c->tone.has_wavelet = cfg->wavelet_strength >= 0.0F;
+    // spec-mode guided / a-trous: run as their own stages ahead of the tone kernel
+    if (cfg->guided_spec && (cfg->guided_radius < 1 || cfg->guided_radius > kGuidedSpecMaxRadius))
+        return fail(CPIPE_BAD_INDEX, c);
+    if (cfg->atrous_levels < 0 || cfg->atrous_levels > kAtrousMaxLevels) return fail(CPIPE_BAD_INDEX, c);
+    c->guided_spec = cfg->guided_spec != 0;
+    c->spec_stages = c->guided_spec || cfg->atrous_levels > 0;
+    if (c->spec_stages) {
+        if (c->guided_spec && guided_spec_setup() != cudaSuccess) return fail(CPIPE_INTERNAL_ERROR, c);
+        if (cfg->atrous_levels > 0) {
+            const cpipe_AtrousWaveletParams ap{cfg->atrous_levels, cfg->bm3d_sigma, cfg->atrous_luma_strength,
+                                               cfg->wavelet_strength >= 0.0F ? cfg->wavelet_strength : 1.0F};
+            if ((st = atrous_plan(&ap, w, h, &c->atrous)) != CPIPE_OK) return fail(st, c);
+            if (cudaMalloc(&c->d_atrous, c->atrous.bytes) != cudaSuccess) return fail(CPIPE_OOM, c);
+            if (atrous_setup() != cudaSuccess) return fail(CPIPE_INTERNAL_ERROR, c);
+            c->tone.has_wavelet = 0;
+        }
+        if (c->denoise_mode == 0) c->tone.bm3d_strength = 0.0F;
+        c->radius = 0;
+    }
     c->tone.eps = cfg->guided_eps;
     c->tone.wavelet_th = 0.035F * cfg->wavelet_strength;
     c->tone.filmic = cpb_filmic_dev(&cfg->filmic);
@@ -760,6 +813,7 @@ void cpipe_cuda_chain_destroy(cpipe_cuda_chain* c) {
     cudaFree(c->d_tile_mse);
     cudaFree(c->d_gate);
     cudaFree(c->d_stats);
+    cudaFree(c->d_atrous);
     if (c->spot_fork) cudaEventDestroy(c->spot_fork);
     if (c->spot_join) cudaEventDestroy(c->spot_join);
     if (c->spot_stream) cudaStreamDestroy(c->spot_stream);
@@ -1200,7 +1254,7 @@ cpipe_cuda_batch* cpipe_cuda_batch_create(const cpipe_cuda_chain_config* cfgs, s
     std::vector<int> prefix(3 * (n + 1), 0);
     for (size_t i = 0; i < n; ++i) {
         cpipe_cuda_chain_config c = cfgs[i];
-        if (c.plain_f32 || c.denoise_mode != 0 || c.stop_after != 0) {
+        if (c.plain_f32 || c.denoise_mode != 0 || c.stop_after != 0 || c.guided_spec || c.atrous_levels) {
             set_error("batch: %s", "frames run the parity chain (binary16, the reference's denoise.bm3d)");
             return fail(CPIPE_UNSUPPORTED, b);
         }

@@ -340,32 +340,34 @@ int node_colormatrix(Ctx& c) {
     return c.step("color_matrix");
 }
 
-// denoise/bm3d.cpp:21-105: sigma from "sigma", else "sigma_override", else the
+// denoise/bm3d.cpp:21-55: sigma from "sigma", else "sigma_override", else the
 // NoiseProfile variance at signal 0.25, else 0.03.
+float noise_sigma(Ctx& c) {
+    double v;
+    if (c.get_double("sigma", &v)) return std::clamp((float)v, 0.0F, 0.2F);
+    if (c.get_double("sigma_override", &v)) return std::clamp((float)v, 0.0F, 0.2F);
+    float sigma = 0.03F;
+    const cpipe_metadata_t* m = c.metadata(c.in(0));
+    cpipe_calibration_view cal;
+    size_t n = 0;
+    if (m && calibration(c, m, &cal) && cal.get_noise_profile && cal.get_noise_profile(m, 0, &n, nullptr, nullptr) == CPIPE_OK && n) {
+        std::vector<float> beta(n), lambda(n);
+        if (cal.get_noise_profile(m, n, &n, beta.data(), lambda.data()) == CPIPE_OK) {
+            double var = 0.0;
+            for (size_t i = 0; i < n; ++i) var += std::max(0.0F, beta[i] + (lambda[i] * 0.25F));
+            var /= (double)n;
+            sigma = (float)std::sqrt(var);
+        }
+    }
+    return sigma;
+}
+
+// denoise/bm3d.cpp:21-105
 int node_bm3d(Ctx& c) {
     int st = check_rgba(c);
     if (st != CPIPE_OK) return st;
     double v;
-    float sigma;
-    if (c.get_double("sigma", &v)) {
-        sigma = std::clamp((float)v, 0.0F, 0.2F);
-    } else if (c.get_double("sigma_override", &v)) {
-        sigma = std::clamp((float)v, 0.0F, 0.2F);
-    } else {
-        sigma = 0.03F;
-        const cpipe_metadata_t* m = c.metadata(c.in(0));
-        cpipe_calibration_view cal;
-        size_t n = 0;
-        if (m && calibration(c, m, &cal) && cal.get_noise_profile && cal.get_noise_profile(m, 0, &n, nullptr, nullptr) == CPIPE_OK && n) {
-            std::vector<float> beta(n), lambda(n);
-            if (cal.get_noise_profile(m, n, &n, beta.data(), lambda.data()) == CPIPE_OK) {
-                double var = 0.0;
-                for (size_t i = 0; i < n; ++i) var += std::max(0.0F, beta[i] + (lambda[i] * 0.25F));
-                var /= (double)n;
-                sigma = (float)std::sqrt(var);
-            }
-        }
-    }
+    const float sigma = noise_sigma(c);
     std::string algorithm = "box2x2";
     c.get_string("algorithm", &algorithm);
     if (algorithm == "bm3d") {
@@ -386,8 +388,17 @@ int node_bm3d(Ctx& c) {
 int node_guided(Ctx& c) {
     int st = check_rgba(c);
     if (st != CPIPE_OK) return st;
-    const cpipe_GuidedFilterParams p{c.clamped_int("radius", 1, 1, 32), c.clamped_float("eps", 0.015F, 0.00001F, 0.1F)};
-    if ((st = c.submit("denoise_guided_filter", &p, sizeof(p))) != CPIPE_OK) return st;
+    std::string algorithm = "reference";
+    c.get_string("algorithm", &algorithm);
+    if (algorithm != "reference" && algorithm != "spec") return CPIPE_BAD_INDEX;
+    // Extension: "spec" boxes with the true (2r+1)^2 window (radius 1..16,
+    // aot_id denoise_guided_filter_spec); "reference" (default) is the
+    // reference's computation, 3x3 or 5x5 whatever the radius.
+    const bool spec = algorithm == "spec";
+    const cpipe_GuidedFilterParams p{c.clamped_int("radius", 1, 1, spec ? 16 : 32),
+                                     c.clamped_float("eps", 0.015F, 0.00001F, 0.1F)};
+    if ((st = c.submit(spec ? "denoise_guided_filter_spec" : "denoise_guided_filter", &p, sizeof(p))) != CPIPE_OK)
+        return st;
     return c.step("denoise.guided_filter");
 }
 
@@ -395,6 +406,19 @@ int node_guided(Ctx& c) {
 int node_wavelet(Ctx& c) {
     int st = check_rgba(c);
     if (st != CPIPE_OK) return st;
+    std::string algorithm = "haar";
+    c.get_string("algorithm", &algorithm);
+    if (algorithm == "atrous") {
+        // Extension: the multi-level a-trous form (aot_id
+        // denoise_wavelet_atrous_spec); "haar" (default) is the reference's
+        // single 2x2 level on chroma.  Noise sigma as the bm3d node finds it.
+        const cpipe_AtrousWaveletParams ap{c.clamped_int("levels", 5, 0, 6), noise_sigma(c),
+                                           c.clamped_float("luma_strength", 1.0F, 0.0F, 2.0F),
+                                           c.clamped_float("chroma_strength", 1.0F, 0.0F, 2.0F)};
+        if ((st = c.submit("denoise_wavelet_atrous_spec", &ap, sizeof(ap))) != CPIPE_OK) return st;
+        return c.step("denoise.wavelet_bayes_shrink");
+    }
+    if (algorithm != "haar") return CPIPE_BAD_INDEX;
     const cpipe_WaveletBayesShrinkParams p{c.clamped_float("chroma_strength", 1.0F, 0.0F, 2.0F)};
     if ((st = c.submit("denoise_wavelet_bayes_shrink", &p, sizeof(p))) != CPIPE_OK) return st;
     return c.step("denoise.wavelet_bayes_shrink");
@@ -550,11 +574,16 @@ const char kBm3d[] = MANIFEST("com.cpipe.denoise.bm3d", "BM3D Denoise", "denoise
     "scene_linear_rec2020", "scene_linear_rec2020", "true", "\"bm3d_parity_kernel\",\"bm3d_match_kernel\",\"bm3d_filter_kernel\"");
 const char kGuided[] = MANIFEST("com.cpipe.denoise.guided_filter", "Guided Filter Denoise", "denoise",
     RGBA_IN("rgb", "\"requires_steps_applied\":[\"color_matrix\"]"), RGBA_OUT("rgb", "denoise.guided_filter", ""),
-    NUM("radius", "1", "32", "1") "," NUM("eps", "1e-05", "0.1", "0.015"), "scene_linear_rec2020",
-    "scene_linear_rec2020", "true", "\"guided_kernel\"");
+    NUM("radius", "1", "32", "1") "," NUM("eps", "1e-05", "0.1", "0.015") ","
+    "{\"name\":\"algorithm\",\"type\":\"enum\",\"values\":[\"reference\",\"spec\"],\"default\":\"reference\"}",
+    "scene_linear_rec2020", "scene_linear_rec2020", "true", "\"guided_kernel\",\"guided_spec_kernel\"");
 const char kWavelet[] = MANIFEST("com.cpipe.denoise.wavelet_bayes_shrink", "Wavelet BayesShrink Denoise", "denoise",
     RGBA_IN("rgb", "\"requires_steps_applied\":[\"color_matrix\"]"), RGBA_OUT("rgb", "denoise.wavelet_bayes_shrink", ""),
-    NUM("chroma_strength", "0", "2", "1"), "scene_linear_rec2020", "scene_linear_rec2020", "true", "\"wavelet_kernel\"");
+    NUM("chroma_strength", "0", "2", "1") ","
+    "{\"name\":\"algorithm\",\"type\":\"enum\",\"values\":[\"haar\",\"atrous\"],\"default\":\"haar\"},"
+    NUM("levels", "0", "6", "5") "," NUM("luma_strength", "0", "2", "1") ","
+    "{\"name\":\"sigma\",\"type\":\"number\",\"range\":{\"min\":0,\"max\":0.2}}",
+    "scene_linear_rec2020", "scene_linear_rec2020", "true", "\"wavelet_kernel\",\"atrous_level_kernel\"");
 const char kOpcode3[] = MANIFEST("com.cpipe.lens.dng_opcode_list_3", "DNG OpcodeList3", "lens",
     PORT("scene_rgb", "in", "\"rgba\"", "\"f16\",\"f32\"", "\"requires_blobs\":[\"com.cpipe.dng.opcode_list_3_bytes\"]"),
     PORT("corrected_rgb", "out", "\"rgba\"", "\"f16\",\"f32\"", "\"inherits_from\":\"scene_rgb\",\"sets_steps_applied\":[\"opcode_list_3\"]"),

@@ -243,6 +243,16 @@ typedef struct {
      * starts with demosaic.quad_bayer_remosaic to an RGGB Bayer frame (then
      * `black.cfa_pattern` must be RGGB). */
     int32_t quad_bayer;
+    /* Spec-mode denoisers ahead of the tone stage (extensions; 0 = the
+     * reference's computation): guided_spec = 1 boxes with the true
+     * (2 guided_radius + 1)^2 window (guided_radius 1..16; filter
+     * denoise_guided_filter_spec); atrous_levels 1..6 replaces the wavelet
+     * node's 2x2 Haar by the a-trous form with that many levels (filter
+     * denoise_wavelet_atrous_spec; noise sigma bm3d_sigma, chroma strength
+     * wavelet_strength when >= 0 else 1, luma strength atrous_luma_strength). */
+    int32_t guided_spec;
+    int32_t atrous_levels;
+    float atrous_luma_strength;
 } cpipe_cuda_chain_config;
 
 typedef struct cpipe_cuda_chain cpipe_cuda_chain;

@@ -64,8 +64,8 @@ EXPECTED_NODES = {
     # sigma, sigma_override as the reference; algorithm and stages select the
     # two-stage BM3D extension (default "box2x2" is the reference computation).
     "com.cpipe.denoise.bm3d": ("rgb", "rgb", ["sigma", "sigma_override", "algorithm", "stages"]),
-    "com.cpipe.denoise.guided_filter": ("rgb", "rgb", ["radius", "eps"]),
-    "com.cpipe.denoise.wavelet_bayes_shrink": ("rgb", "rgb", ["chroma_strength"]),
+    "com.cpipe.denoise.guided_filter": ("rgb", "rgb", ["radius", "eps", "algorithm"]),
+    "com.cpipe.denoise.wavelet_bayes_shrink": ("rgb", "rgb", ["chroma_strength", "algorithm", "levels", "luma_strength", "sigma"]),
     "com.cpipe.lens.dng_opcode_list_3": ("scene_rgb", "corrected_rgb", []),
     "com.cpipe.color.3d_lut": ("rgb", "rgb", ["lut_path", "interpolation"]),
     "com.cpipe.tone.filmic_rgb": ("rgb", "rgb", ["ev", "contrast", "saturation", "highlights", "shadows"]),

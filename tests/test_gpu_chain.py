@@ -48,8 +48,16 @@ def run_nodes_on_gpu(host, cfg, raw):
               ("com.cpipe.denoise.bm3d", F16, {"algorithm": "bm3d", "stages": cfg.bm3d_stages}
                if cfg.denoise == "bm3d" else {})]
     if cfg.guided_radius > 0:
-        steps.append(("com.cpipe.denoise.guided_filter", F16, {"radius": cfg.guided_radius, "eps": cfg.guided_eps}))
-    if cfg.wavelet_strength >= 0:
+        gp = {"radius": cfg.guided_radius, "eps": cfg.guided_eps}
+        if cfg.guided_spec:
+            gp["algorithm"] = "spec"
+        steps.append(("com.cpipe.denoise.guided_filter", F16, gp))
+    if cfg.atrous_levels > 0:
+        steps.append(("com.cpipe.denoise.wavelet_bayes_shrink", F16,
+                      {"algorithm": "atrous", "levels": cfg.atrous_levels, "sigma": cfg.bm3d_sigma,
+                       "luma_strength": cfg.atrous_luma_strength,
+                       "chroma_strength": cfg.wavelet_strength if cfg.wavelet_strength >= 0 else 1.0}))
+    elif cfg.wavelet_strength >= 0:
         steps.append(("com.cpipe.denoise.wavelet_bayes_shrink", F16, {"chroma_strength": cfg.wavelet_strength}))
     steps.append(("com.cpipe.tone.filmic_rgb", F16, {}))
     tmp = None
@@ -250,3 +258,33 @@ def test_run_host_frames_matches_run_host(cuda_device, mode):
             np.testing.assert_allclose(got[k].astype(np.float32), want[k].astype(np.float32), rtol=2e-3, atol=2e-3,
                                        err_msg=f"frame {k}")
     chain.close()
+
+
+@pytest.mark.parametrize("kw", [dict(guided_spec=True, atrous_levels=5),
+                                dict(guided_spec=True, guided_radius=3, atrous_levels=0, wavelet_strength=1.0),
+                                dict(guided_spec=False, atrous_levels=4, denoise="bm3d")])
+def test_chain_spec_denoisers_equal_nodes(host, kw):
+    """The chain with the spec-mode guided filter and/or the a-trous wavelet
+    stages returns, bit for bit, what the nodes with algorithm = "spec" /
+    "atrous" return one by one (the stages run as their own kernels between
+    the denoiser and the tone kernel)."""
+    base = dict(width=160, height=112)
+    base.update(kw)
+    cfg = ChainConfig.full_12mp(**base)
+    raw = cfg.make_raw()
+    chain = Chain(cfg)
+    got = chain.run_host(raw)
+    chain.close()
+    want = run_nodes_on_gpu(host, cfg, raw)
+    if cfg.denoise == "bm3d":  # BM3D's aggregation order on the GPU is not fixed
+        p = psnr(got[..., :3].astype(np.float64), want[..., :3].astype(np.float64))
+        assert p >= 60.0, p
+    else:
+        np.testing.assert_array_equal(got.view(np.uint16), want.view(np.uint16))
+
+
+def test_chain_spec_stage_refusals(cuda_device):
+    with pytest.raises(Exception):
+        Chain(ChainConfig.full_12mp(width=64, height=64, guided_spec=True, guided_radius=17))
+    with pytest.raises(Exception):
+        Chain(ChainConfig.full_12mp(width=64, height=64, atrous_levels=7))

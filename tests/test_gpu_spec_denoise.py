@@ -78,3 +78,28 @@ def test_spec_filters_refuse_out_of_range(cuda_device):
     assert call_filter("denoise_guided_filter_spec", [x], [out], blobs.guided(4, 0.0)) != 0
     assert call_filter("denoise_wavelet_atrous_spec", [x], [out], blobs.atrous(7, 0.03)) != 0
     assert call_filter("denoise_wavelet_atrous_spec", [x], [out], blobs.atrous(5, -1.0)) != 0
+
+
+def test_spec_nodes(host):
+    """com.cpipe.denoise.guided_filter with algorithm = "spec" and
+    com.cpipe.denoise.wavelet_bayes_shrink with algorithm = "atrous" submit the
+    spec filters (the a-trous noise sigma from the NoiseProfile, as the bm3d
+    node finds it: sqrt(beta + 0.25 lambda))."""
+    from cpipe_b200 import _abi as A
+    x = frame(48, 64, 0.03, 12, np.float16)
+    F16 = A.FMT_R16G16B16A16_SFLOAT
+    src = host.buffer(F16, x.shape[1], x.shape[0]).upload(x)
+    src.set_metadata(cs_role="scene_linear_rec2020", applied_steps=["color_matrix"], noise_profile=[(1e-5, 1e-3)])
+    out = host.buffer(F16, x.shape[1], x.shape[0])
+    st = host.run_node("com.cpipe.denoise.guided_filter", [src], [out], {"algorithm": "spec", "radius": 8, "eps": 1e-3})
+    assert st == 0, host.last_error()
+    want = S.guided_spec(x.astype(np.float64), 8, float(np.float32(1e-3)))
+    assert_f16_parity(out.download(), want, what="guided spec node")
+    assert out.has_step("denoise.guided_filter")
+    st = host.run_node("com.cpipe.denoise.wavelet_bayes_shrink", [src], [out], {"algorithm": "atrous", "levels": 4})
+    assert st == 0, host.last_error()
+    sigma = float(np.float32(np.sqrt(np.float32(1e-5) + np.float32(1e-3) * np.float32(0.25))))
+    want = S.atrous_spec(x.astype(np.float64), 4, sigma)
+    assert_f16_parity(out.download(), want, what="a-trous node")
+    assert host.run_node("com.cpipe.denoise.wavelet_bayes_shrink", [src], [out], {"algorithm": "nope"}) == A.BAD_INDEX
+    assert host.run_node("com.cpipe.denoise.guided_filter", [src], [out], {"algorithm": "nope"}) == A.BAD_INDEX
