@@ -13,6 +13,8 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -124,9 +126,40 @@ int Call::bind(halide_buffer_t* hb, Kind kind, bool is_output, Bound* out) {
     return CPIPE_OK;
 }
 
+// The filters' per-call scratch comes from a device memory pool of the
+// library's own that keeps what it has reserved (release threshold: never),
+// so a call does not map fresh device memory after every synchronisation;
+// cpipe_cuda_trim_scratch returns it.  One pool per device, made on first use.
+static cudaError_t scratch_pool(cudaMemPool_t* out) {
+    static std::mutex mu;
+    static std::map<int, cudaMemPool_t> pools;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(mu);
+    auto it = pools.find(dev);
+    if (it != pools.end()) {
+        *out = it->second;
+        return cudaSuccess;
+    }
+    cudaMemPoolProps props{};
+    props.allocType = cudaMemAllocationTypePinned;
+    props.location.type = cudaMemLocationTypeDevice;
+    props.location.id = dev;
+    cudaMemPool_t pool;
+    if ((e = cudaMemPoolCreate(&pool, &props)) != cudaSuccess) return e;
+    uint64_t keep = UINT64_MAX;
+    if ((e = cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep)) != cudaSuccess) return e;
+    pools[dev] = pool;
+    *out = pool;
+    return cudaSuccess;
+}
+
 int Call::alloc(size_t bytes, void** out) {
     void* d = nullptr;
-    const cudaError_t e = cudaMallocAsync(&d, bytes < 256 ? 256 : bytes, stream);
+    cudaMemPool_t pool;
+    cudaError_t e = scratch_pool(&pool);
+    if (e == cudaSuccess) e = cudaMallocFromPoolAsync(&d, bytes < 256 ? 256 : bytes, pool, stream);
     if (e != cudaSuccess) {
         cudaGetLastError();
         std::snprintf(g_err, sizeof(g_err), "device allocation of %zu bytes failed: %s", bytes, cudaGetErrorString(e));
@@ -220,6 +253,13 @@ int cpipe_cuda_set_stream(void* stream) {
 void* cpipe_cuda_get_stream(void) { return g_stream; }
 const char* cpipe_cuda_last_error(void) { return g_err; }
 int cpipe_cuda_synchronize(void) { return cuda_status(cudaStreamSynchronize(g_stream), "synchronize"); }
+int cpipe_cuda_trim_scratch(void) {
+    cudaMemPool_t pool;
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = scratch_pool(&pool);
+    if (e == cudaSuccess) e = cudaMemPoolTrimTo(pool, 0);
+    return cuda_status(e, "trim scratch");
+}
 int cpipe_cuda_device_count(void) {
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess) {

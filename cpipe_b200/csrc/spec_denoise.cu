@@ -34,11 +34,12 @@
 //                        variance does not cancel), a and b on the tile plus r,
 //                        separable box sums of a and b, the output.
 //   atrous_prep_kernel   RGBA -> Y, Co, Cg planes (FP32).
-//   atrous_level_kernel  one level for all channels: a 64x32 tile; the
-//                        horizontal pass of the rows the tile needs (halo
-//                        2 * 2^j) into shared memory, the vertical pass from
-//                        there; writes c_{j+1} and w_{j+1} and the tile's sum
-//                        of w^2 per channel.
+//   atrous_level_kernel  one level for all channels: a 64x32 tile; per
+//                        channel the input rows with a 2 * 2^j halo both ways
+//                        staged in shared memory (one coalesced pass), the
+//                        horizontal pass into a second buffer, the vertical
+//                        pass from there; writes c_{j+1} and w_{j+1} and the
+//                        tile's sum of w^2 per channel.
 //   atrous_thresh_kernel per (level, channel): the tiles' sums added in a fixed
 //                        order (FP64), the BayesShrink threshold.
 //   atrous_recon_kernel  shrink, sum, inverse colour transform.
@@ -58,7 +59,6 @@ namespace {
 
 // ------------------------------------------------------------------ guided
 constexpr int kGsTW = 32, kGsTH = 32, kGsThreads = 256;
-constexpr int kGsPer = kGsTW * kGsTH / kGsThreads;  // outputs per thread
 
 __host__ __device__ inline size_t gs_floats(int R) {
     const size_t IW = kGsTW + 4 * R, IH = kGsTH + 4 * R, AW = kGsTW + 2 * R, AH = kGsTH + 2 * R;
@@ -86,73 +86,121 @@ __global__ void __launch_bounds__(kGsThreads) guided_spec_kernel(Img in, Img out
         s_v[2 * IW * IH + i] = v.b;
     }
     __syncthreads();
-    float res[kGsPer][3];
+    // Box sums along rows or columns: each item is a run of up to kGsSeg
+    // consecutive outputs, its first window summed directly and the rest slid
+    // (one add and one subtract per output; the slide restarts every run).
+    constexpr int kGsSeg = 8;
+    static_assert(kGsTW * (kGsTH / kGsSeg) <= kGsThreads && kGsTW % kGsSeg == 0 && kGsTH % kGsSeg == 0, "runs");
+    float res[kGsSeg][3];
+#pragma unroll
     for (int c = 0; c < 3; ++c) {
         const float* v = s_v + c * IW * IH;
         const float k = v[(2 * R + kGsTH / 2) * IW + 2 * R + kGsTW / 2];
-        for (int i = threadIdx.x; i < IH * AW; i += blockDim.x) {
-            const int y = i / AW, x = i - y * AW;
-            const float* row = v + y * IW + x;
+        const int rseg = (AW + kGsSeg - 1) / kGsSeg;
+        for (int it = threadIdx.x; it < IH * rseg; it += blockDim.x) {  // rows of v: (v - k), (v - k)^2
+            const int y = it / rseg, x0s = (it - y * rseg) * kGsSeg, n = min(kGsSeg, AW - x0s);
+            const float* row = v + y * IW + x0s;
             float s1 = 0.0F, s2 = 0.0F;
             for (int d = 0; d < D; ++d) {
                 const float t = row[d] - k;
                 s1 = s1 + t;
                 s2 = s2 + t * t;
             }
-            s_r1[i] = s1;
-            s_r2[i] = s2;
+            s_r1[y * AW + x0s] = s1;
+            s_r2[y * AW + x0s] = s2;
+            for (int i = 1; i < n; ++i) {
+                const float ti = row[i + D - 1] - k, to = row[i - 1] - k;
+                s1 = (s1 + ti) - to;
+                s2 = (s2 + ti * ti) - to * to;
+                s_r1[y * AW + x0s + i] = s1;
+                s_r2[y * AW + x0s + i] = s2;
+            }
         }
         __syncthreads();
-        for (int i = threadIdx.x; i < AH * AW; i += blockDim.x) {
-            const int y = i / AW, x = i - y * AW;
+        const int cseg = (AH + kGsSeg - 1) / kGsSeg;
+        for (int it = threadIdx.x; it < AW * cseg; it += blockDim.x) {  // columns -> a, b
+            const int x = it % AW, y0s = (it / AW) * kGsSeg, n = min(kGsSeg, AH - y0s);
             float s1 = 0.0F, s2 = 0.0F;
             for (int d = 0; d < D; ++d) {
-                s1 = s1 + s_r1[(y + d) * AW + x];
-                s2 = s2 + s_r2[(y + d) * AW + x];
+                s1 = s1 + s_r1[(y0s + d) * AW + x];
+                s2 = s2 + s_r2[(y0s + d) * AW + x];
             }
-            const float mk = s1 / N, corr = s2 / N;
-            const float var = max0(corr - mk * mk);
-            const float m = mk + k;
-            const float a = var / (var + eps);
-            s_a[i] = a;
-            s_b[i] = m - a * m;
+            for (int i = 0; i < n; ++i) {
+                if (i > 0) {
+                    s1 = (s1 + s_r1[(y0s + i + D - 1) * AW + x]) - s_r1[(y0s + i - 1) * AW + x];
+                    s2 = (s2 + s_r2[(y0s + i + D - 1) * AW + x]) - s_r2[(y0s + i - 1) * AW + x];
+                }
+                const float mk = s1 / N, corr = s2 / N;
+                const float var = max0(corr - mk * mk);
+                const float m = mk + k;
+                const float a = var / (var + eps);
+                s_a[(y0s + i) * AW + x] = a;
+                s_b[(y0s + i) * AW + x] = m - a * m;
+            }
         }
         __syncthreads();
-        for (int i = threadIdx.x; i < AH * kGsTW; i += blockDim.x) {
-            const int y = i / kGsTW, x = i - y * kGsTW;
+        const int tseg = kGsTW / kGsSeg;
+        for (int it = threadIdx.x; it < AH * tseg; it += blockDim.x) {  // rows of a, b
+            const int y = it / tseg, x0s = (it - y * tseg) * kGsSeg;
+            const float* ra = s_a + y * AW + x0s;
+            const float* rb = s_b + y * AW + x0s;
             float sa = 0.0F, sb = 0.0F;
             for (int d = 0; d < D; ++d) {
-                sa = sa + s_a[y * AW + x + d];
-                sb = sb + s_b[y * AW + x + d];
+                sa = sa + ra[d];
+                sb = sb + rb[d];
             }
-            s_ra[i] = sa;
-            s_rb[i] = sb;
+            s_ra[y * kGsTW + x0s] = sa;
+            s_rb[y * kGsTW + x0s] = sb;
+            for (int i = 1; i < kGsSeg; ++i) {
+                sa = (sa + ra[i + D - 1]) - ra[i - 1];
+                sb = (sb + rb[i + D - 1]) - rb[i - 1];
+                s_ra[y * kGsTW + x0s + i] = sa;
+                s_rb[y * kGsTW + x0s + i] = sb;
+            }
         }
         __syncthreads();
+        // columns of the row-summed a, b -> the output: thread t < kGsTW * kGsTH / kGsSeg
+        // owns the run of rows 8 (t / kGsTW).. of column t % kGsTW, kept in registers
+        if ((int)threadIdx.x < kGsTW * (kGsTH / kGsSeg)) {
+            const int it = threadIdx.x;
+            const int x = it % kGsTW, y0s = (it / kGsTW) * kGsSeg;
+            float sa = 0.0F, sb = 0.0F;
+            for (int d = 0; d < D; ++d) {
+                sa = sa + s_ra[(y0s + d) * kGsTW + x];
+                sb = sb + s_rb[(y0s + d) * kGsTW + x];
+            }
 #pragma unroll
-        for (int q = 0; q < kGsPer; ++q) {
-            const int j = threadIdx.x + q * kGsThreads, y = j / kGsTW, x = j - y * kGsTW;
-            float sa = 0.0F, sb = 0.0F;
-            for (int d = 0; d < D; ++d) {
-                sa = sa + s_ra[(y + d) * kGsTW + x];
-                sb = sb + s_rb[(y + d) * kGsTW + x];
+            for (int i = 0; i < kGsSeg; ++i) {
+                if (i > 0) {
+                    sa = (sa + s_ra[(y0s + i + D - 1) * kGsTW + x]) - s_ra[(y0s + i - 1) * kGsTW + x];
+                    sb = (sb + s_rb[(y0s + i + D - 1) * kGsTW + x]) - s_rb[(y0s + i - 1) * kGsTW + x];
+                }
+                const int y = y0s + i;
+                res[i][c] = max0((sa / N) * v[(y + 2 * R) * IW + x + 2 * R] + (sb / N));
             }
-            res[q][c] = max0((sa / N) * v[(y + 2 * R) * IW + x + 2 * R] + (sb / N));
         }
         __syncthreads();
     }
+    if ((int)threadIdx.x < kGsTW * (kGsTH / kGsSeg)) {
+        const int x = x0 + (int)threadIdx.x % kGsTW, yb = y0 + ((int)threadIdx.x / kGsTW) * kGsSeg;
 #pragma unroll
-    for (int q = 0; q < kGsPer; ++q) {
-        const int j = threadIdx.x + q * kGsThreads, y = y0 + j / kGsTW, x = x0 + j % kGsTW;
-        if (x < out.w && y < out.h)
-            store_rgb_keep_alpha(px<T>(out, x, y), Rgba{res[q][0], res[q][1], res[q][2], 0.0F}, px<const T>(in, x, y));
+        for (int i = 0; i < kGsSeg; ++i) {
+            const int y = yb + i;
+            if (x < out.w && y < out.h)
+                store_rgb_keep_alpha(px<T>(out, x, y), Rgba{res[i][0], res[i][1], res[i][2], 0.0F}, px<const T>(in, x, y));
+        }
     }
 }
 
 // ----------------------------------------------------------------- a-trous
 constexpr int kAtTW = 64, kAtTH = 32, kAtThreads = 256;
 
-__host__ __device__ inline size_t at_smem(int s) { return sizeof(float) * 3 * (size_t)(kAtTH + 4 * s) * kAtTW; }
+// per channel: the input rows of the tile with a 2s halo both ways, then the
+// horizontally filtered rows
+__host__ __device__ inline size_t at_smem(int s) {
+    const size_t hr = kAtTH + 4 * s;
+    return sizeof(float) * (hr * (kAtTW + 4 * s) + hr * kAtTW);
+}
 
 template <class T>
 __global__ void atrous_prep_kernel(Img in, float* __restrict__ c0, long long npx) {
@@ -172,30 +220,39 @@ __device__ __forceinline__ float b3(float a, float b, float c, float d, float e)
 __global__ void __launch_bounds__(kAtThreads) atrous_level_kernel(const float* __restrict__ cin, float* __restrict__ cout,
                                                                   float* __restrict__ wout, float* __restrict__ part,
                                                                   int w, int h, long long npx, int s) {
-    extern __shared__ float sm[];  // [3][kAtTH + 4s][kAtTW]: rows filtered horizontally
-    const int x0 = blockIdx.x * kAtTW, y0 = blockIdx.y * kAtTH, HR = kAtTH + 4 * s;
-    for (int i = threadIdx.x; i < 3 * HR * kAtTW; i += blockDim.x) {
-        const int c = i / (HR * kAtTW), rem = i - c * HR * kAtTW;
-        const int r = rem / kAtTW, xx = rem - r * kAtTW;
-        const int y = clampi(y0 - 2 * s + r, 0, h - 1), x = min(x0 + xx, w - 1);
-        const float* row = cin + c * npx + (long long)y * w;
-        sm[i] = b3(row[clampi(x - 2 * s, 0, w - 1)], row[clampi(x - s, 0, w - 1)], row[x], row[clampi(x + s, 0, w - 1)],
-                   row[clampi(x + 2 * s, 0, w - 1)]);
-    }
-    __syncthreads();
+    extern __shared__ float sm[];
+    const int x0 = blockIdx.x * kAtTW, y0 = blockIdx.y * kAtTH, HR = kAtTH + 4 * s, IWd = kAtTW + 4 * s;
+    float* s_in = sm;             // [HR][IWd]: rows y0-2s.., columns x0-2s.. (clamped)
+    float* s_h = sm + HR * IWd;   // [HR][kAtTW]: filtered along rows
     float acc[3] = {0.0F, 0.0F, 0.0F};
-    for (int i = threadIdx.x; i < 3 * kAtTH * kAtTW; i += blockDim.x) {
-        const int c = i / (kAtTH * kAtTW), rem = i - c * kAtTH * kAtTW;
-        const int r = rem / kAtTW, xx = rem - r * kAtTW;
-        const int x = x0 + xx, y = y0 + r;
-        if (x >= w || y >= h) continue;
-        const float* col = sm + c * HR * kAtTW + (r + 2 * s) * kAtTW + xx;
-        const float v = b3(col[-2 * s * kAtTW], col[-s * kAtTW], col[0], col[s * kAtTW], col[2 * s * kAtTW]);
-        const long long o = c * npx + (long long)y * w + x;
-        const float d = cin[o] - v;
-        cout[o] = v;
-        wout[o] = d;
-        acc[c] += d * d;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const float* plane = cin + c * npx;
+        for (int i = threadIdx.x; i < HR * IWd; i += blockDim.x) {
+            const int r = i / IWd, xx = i - r * IWd;
+            const int y = clampi(y0 - 2 * s + r, 0, h - 1), x = clampi(x0 - 2 * s + xx, 0, w - 1);
+            s_in[i] = plane[(long long)y * w + x];
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < HR * kAtTW; i += blockDim.x) {
+            const int r = i / kAtTW, xx = i - r * kAtTW;
+            const float* row = s_in + r * IWd + xx + 2 * s;
+            s_h[i] = b3(row[-2 * s], row[-s], row[0], row[s], row[2 * s]);
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < kAtTH * kAtTW; i += blockDim.x) {
+            const int r = i / kAtTW, xx = i - r * kAtTW;
+            const int x = x0 + xx, y = y0 + r;
+            if (x >= w || y >= h) continue;
+            const float* col = s_h + (r + 2 * s) * kAtTW + xx;
+            const float v = b3(col[-2 * s * kAtTW], col[-s * kAtTW], col[0], col[s * kAtTW], col[2 * s * kAtTW]);
+            const long long o = c * npx + (long long)y * w + x;
+            const float d = s_in[(r + 2 * s) * IWd + xx + 2 * s] - v;
+            cout[o] = v;
+            wout[o] = d;
+            acc[c] += d * d;
+        }
+        __syncthreads();
     }
     __shared__ float red[kAtThreads / 32][3];
 #pragma unroll

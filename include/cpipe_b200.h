@@ -49,6 +49,11 @@ extern "C" {
 int cpipe_cuda_set_stream(void* cuda_stream);
 void* cpipe_cuda_get_stream(void);
 int cpipe_cuda_synchronize(void);
+/* The filters draw their per-call device scratch from a memory pool of the
+ * library's own, one per device, which keeps what it has reserved between
+ * calls; this waits for the device and returns that memory.  (No reference
+ * counterpart: the reference's filters run on the CPU.) */
+int cpipe_cuda_trim_scratch(void);
 const char* cpipe_cuda_last_error(void);
 int cpipe_cuda_device_count(void);
 

@@ -103,3 +103,17 @@ def test_spec_nodes(host):
     assert_f16_parity(out.download(), want, what="a-trous node")
     assert host.run_node("com.cpipe.denoise.wavelet_bayes_shrink", [src], [out], {"algorithm": "nope"}) == A.BAD_INDEX
     assert host.run_node("com.cpipe.denoise.guided_filter", [src], [out], {"algorithm": "nope"}) == A.BAD_INDEX
+
+
+def test_scratch_pool_is_reused_and_trimmed(cuda_device):
+    """Filters with scratch (here the a-trous form, ~100 B/px) draw it from the
+    library's pool: repeated calls give the same result, and trimming the pool
+    between calls changes nothing but the memory held."""
+    from cpipe_b200 import _abi as A
+    x = frame(96, 128, 0.03, 3, np.float32)
+    first = run("denoise_wavelet_atrous_spec", x, blobs.atrous(5, 0.03))
+    again = run("denoise_wavelet_atrous_spec", x, blobs.atrous(5, 0.03))
+    assert A.lib().cpipe_cuda_trim_scratch() == 0
+    third = run("denoise_wavelet_atrous_spec", x, blobs.atrous(5, 0.03))
+    np.testing.assert_array_equal(first, again)
+    np.testing.assert_array_equal(first, third)
