@@ -320,7 +320,8 @@ class Chain:
 
 def _main():
     """Run the 12 MP chain a few times on the GPU (used for profiler captures):
-    python -m cpipe_b200.chain [--frames N] [--width W --height H] [--demosaic rcd|amaze|bilinear]"""
+    python -m cpipe_b200.chain [--frames N] [--width W --height H] [--demosaic rcd|amaze|bilinear]
+                               [--denoise box2x2|bm3d|surrogate] [--guided-spec] [--atrous-levels L]"""
     import argparse
     ap = argparse.ArgumentParser()
     ap.add_argument("--frames", type=int, default=3)
@@ -328,6 +329,8 @@ def _main():
     ap.add_argument("--height", type=int, default=3024)
     ap.add_argument("--demosaic", default="rcd")
     ap.add_argument("--denoise", default="box2x2", choices=["box2x2", "bm3d", "surrogate"])
+    ap.add_argument("--guided-spec", action="store_true", help="guided filter with the true (2r+1)^2 box")
+    ap.add_argument("--atrous-levels", type=int, default=0, help="a-trous wavelet stages instead of the 2x2 Haar")
     args = ap.parse_args()
     L = A.lib()
     assert L.cpipe_cuda_device_count() > 0, "no CUDA device"
@@ -336,7 +339,8 @@ def _main():
         from .surrogate import load_weights
         blob = load_weights()
     cfg = ChainConfig.full_12mp(width=args.width, height=args.height, demosaic=args.demosaic, use_graph=False,
-                                denoise=args.denoise, surrogate_blob=blob)
+                                denoise=args.denoise, surrogate_blob=blob, guided_spec=args.guided_spec,
+                                atrous_levels=args.atrous_levels)
     raw = cfg.make_raw()
     chain = Chain(cfg)
     d_raw, d_out = C.c_void_p(), C.c_void_p()

@@ -60,30 +60,35 @@ namespace {
 // ------------------------------------------------------------------ guided
 constexpr int kGsTW = 32, kGsTH = 32, kGsThreads = 256;
 
+// Row-major shared buffers use odd pitches: the row passes give consecutive
+// threads consecutive rows, which then fall in different banks.
+__host__ __device__ inline int odd(int v) { return v | 1; }
 __host__ __device__ inline size_t gs_floats(int R) {
-    const size_t IW = kGsTW + 4 * R, IH = kGsTH + 4 * R, AW = kGsTW + 2 * R, AH = kGsTH + 2 * R;
-    return 3 * IW * IH + 2 * AW * IH + 2 * AW * AH + 2 * (size_t)kGsTW * AH;
+    const size_t IW = odd(kGsTW + 4 * R), IH = kGsTH + 4 * R, AW = odd(kGsTW + 2 * R), AH = kGsTH + 2 * R;
+    return 3 * IW * IH + 2 * AW * IH + 2 * AW * AH + 2 * (size_t)odd(kGsTW) * AH;
 }
 
 template <class T>
 __global__ void __launch_bounds__(kGsThreads) guided_spec_kernel(Img in, Img out, int R, float eps) {
     extern __shared__ float sm[];
-    const int IW = kGsTW + 4 * R, IH = kGsTH + 4 * R, AW = kGsTW + 2 * R, AH = kGsTH + 2 * R, D = 2 * R + 1;
+    // extents (IWn x IH input, AWn x AH for a / b) and odd row pitches
+    const int IWn = kGsTW + 4 * R, IH = kGsTH + 4 * R, AWn = kGsTW + 2 * R, AH = kGsTH + 2 * R, D = 2 * R + 1;
+    const int IW = odd(IWn), AW = odd(AWn), TP = odd(kGsTW);
     const float N = (float)(D * D);
     float* s_v = sm;                  // [3][IH][IW] clamped input
     float* s_r1 = s_v + 3 * IW * IH;  // [IH][AW] row sums of v - k
     float* s_r2 = s_r1 + IH * AW;     // [IH][AW] row sums of (v - k)^2
     float* s_a = s_r2 + IH * AW;      // [AH][AW]
     float* s_b = s_a + AH * AW;
-    float* s_ra = s_b + AH * AW;      // [AH][TW] row sums of a
-    float* s_rb = s_ra + AH * kGsTW;
+    float* s_ra = s_b + AH * AW;      // [AH][TP] row sums of a
+    float* s_rb = s_ra + AH * TP;
     const int x0 = blockIdx.x * kGsTW, y0 = blockIdx.y * kGsTH;
-    for (int i = threadIdx.x; i < IW * IH; i += blockDim.x) {
-        const int ty = i / IW, tx = i - ty * IW;
+    for (int i = threadIdx.x; i < IWn * IH; i += blockDim.x) {
+        const int ty = i / IWn, tx = i - ty * IWn;
         const Rgba v = load_clamped<T>(in, x0 - 2 * R + tx, y0 - 2 * R + ty);
-        s_v[i] = v.r;
-        s_v[IW * IH + i] = v.g;
-        s_v[2 * IW * IH + i] = v.b;
+        s_v[ty * IW + tx] = v.r;
+        s_v[IW * IH + ty * IW + tx] = v.g;
+        s_v[2 * IW * IH + ty * IW + tx] = v.b;
     }
     __syncthreads();
     // Box sums along rows or columns: each item is a run of up to kGsSeg
@@ -96,9 +101,9 @@ __global__ void __launch_bounds__(kGsThreads) guided_spec_kernel(Img in, Img out
     for (int c = 0; c < 3; ++c) {
         const float* v = s_v + c * IW * IH;
         const float k = v[(2 * R + kGsTH / 2) * IW + 2 * R + kGsTW / 2];
-        const int rseg = (AW + kGsSeg - 1) / kGsSeg;
+        const int rseg = (AWn + kGsSeg - 1) / kGsSeg;
         for (int it = threadIdx.x; it < IH * rseg; it += blockDim.x) {  // rows of v: (v - k), (v - k)^2
-            const int y = it / rseg, x0s = (it - y * rseg) * kGsSeg, n = min(kGsSeg, AW - x0s);
+            const int y = it % IH, x0s = (it / IH) * kGsSeg, n = min(kGsSeg, AWn - x0s);
             const float* row = v + y * IW + x0s;
             float s1 = 0.0F, s2 = 0.0F;
             for (int d = 0; d < D; ++d) {
@@ -118,8 +123,8 @@ __global__ void __launch_bounds__(kGsThreads) guided_spec_kernel(Img in, Img out
         }
         __syncthreads();
         const int cseg = (AH + kGsSeg - 1) / kGsSeg;
-        for (int it = threadIdx.x; it < AW * cseg; it += blockDim.x) {  // columns -> a, b
-            const int x = it % AW, y0s = (it / AW) * kGsSeg, n = min(kGsSeg, AH - y0s);
+        for (int it = threadIdx.x; it < AWn * cseg; it += blockDim.x) {  // columns -> a, b
+            const int x = it % AWn, y0s = (it / AWn) * kGsSeg, n = min(kGsSeg, AH - y0s);
             float s1 = 0.0F, s2 = 0.0F;
             for (int d = 0; d < D; ++d) {
                 s1 = s1 + s_r1[(y0s + d) * AW + x];
@@ -141,7 +146,7 @@ __global__ void __launch_bounds__(kGsThreads) guided_spec_kernel(Img in, Img out
         __syncthreads();
         const int tseg = kGsTW / kGsSeg;
         for (int it = threadIdx.x; it < AH * tseg; it += blockDim.x) {  // rows of a, b
-            const int y = it / tseg, x0s = (it - y * tseg) * kGsSeg;
+            const int y = it % AH, x0s = (it / AH) * kGsSeg;
             const float* ra = s_a + y * AW + x0s;
             const float* rb = s_b + y * AW + x0s;
             float sa = 0.0F, sb = 0.0F;
@@ -149,13 +154,13 @@ __global__ void __launch_bounds__(kGsThreads) guided_spec_kernel(Img in, Img out
                 sa = sa + ra[d];
                 sb = sb + rb[d];
             }
-            s_ra[y * kGsTW + x0s] = sa;
-            s_rb[y * kGsTW + x0s] = sb;
+            s_ra[y * TP + x0s] = sa;
+            s_rb[y * TP + x0s] = sb;
             for (int i = 1; i < kGsSeg; ++i) {
                 sa = (sa + ra[i + D - 1]) - ra[i - 1];
                 sb = (sb + rb[i + D - 1]) - rb[i - 1];
-                s_ra[y * kGsTW + x0s + i] = sa;
-                s_rb[y * kGsTW + x0s + i] = sb;
+                s_ra[y * TP + x0s + i] = sa;
+                s_rb[y * TP + x0s + i] = sb;
             }
         }
         __syncthreads();
@@ -166,14 +171,14 @@ __global__ void __launch_bounds__(kGsThreads) guided_spec_kernel(Img in, Img out
             const int x = it % kGsTW, y0s = (it / kGsTW) * kGsSeg;
             float sa = 0.0F, sb = 0.0F;
             for (int d = 0; d < D; ++d) {
-                sa = sa + s_ra[(y0s + d) * kGsTW + x];
-                sb = sb + s_rb[(y0s + d) * kGsTW + x];
+                sa = sa + s_ra[(y0s + d) * TP + x];
+                sb = sb + s_rb[(y0s + d) * TP + x];
             }
 #pragma unroll
             for (int i = 0; i < kGsSeg; ++i) {
                 if (i > 0) {
-                    sa = (sa + s_ra[(y0s + i + D - 1) * kGsTW + x]) - s_ra[(y0s + i - 1) * kGsTW + x];
-                    sb = (sb + s_rb[(y0s + i + D - 1) * kGsTW + x]) - s_rb[(y0s + i - 1) * kGsTW + x];
+                    sa = (sa + s_ra[(y0s + i + D - 1) * TP + x]) - s_ra[(y0s + i - 1) * TP + x];
+                    sb = (sb + s_rb[(y0s + i + D - 1) * TP + x]) - s_rb[(y0s + i - 1) * TP + x];
                 }
                 const int y = y0s + i;
                 res[i][c] = max0((sa / N) * v[(y + 2 * R) * IW + x + 2 * R] + (sb / N));
@@ -221,7 +226,8 @@ __global__ void __launch_bounds__(kAtThreads) atrous_level_kernel(const float* _
                                                                   float* __restrict__ wout, float* __restrict__ part,
                                                                   int w, int h, long long npx, int s) {
     extern __shared__ float sm[];
-    const int x0 = blockIdx.x * kAtTW, y0 = blockIdx.y * kAtTH, HR = kAtTH + 4 * s, IWd = kAtTW + 4 * s;
+    const int TH = kAtTH;
+    const int x0 = blockIdx.x * kAtTW, y0 = blockIdx.y * TH, HR = TH + 4 * s, IWd = kAtTW + 4 * s;
     float* s_in = sm;             // [HR][IWd]: rows y0-2s.., columns x0-2s.. (clamped)
     float* s_h = sm + HR * IWd;   // [HR][kAtTW]: filtered along rows
     float acc[3] = {0.0F, 0.0F, 0.0F};
@@ -240,7 +246,7 @@ __global__ void __launch_bounds__(kAtThreads) atrous_level_kernel(const float* _
             s_h[i] = b3(row[-2 * s], row[-s], row[0], row[s], row[2 * s]);
         }
         __syncthreads();
-        for (int i = threadIdx.x; i < kAtTH * kAtTW; i += blockDim.x) {
+        for (int i = threadIdx.x; i < TH * kAtTW; i += blockDim.x) {
             const int r = i / kAtTW, xx = i - r * kAtTW;
             const int x = x0 + xx, y = y0 + r;
             if (x >= w || y >= h) continue;
@@ -275,13 +281,18 @@ struct AtrousThrArgs {
     float strength[3];
 };
 
-// block (level, channel): the tiles' sums of w^2 in a fixed order -> threshold
-__global__ void __launch_bounds__(256) atrous_thresh_kernel(const float* __restrict__ part, int nblocks, long long npx,
+// block (level, channel): the tiles' sums of w^2 in a fixed order -> threshold;
+// level j's sums start at part + j * stride (3 per tile), nb[j] tiles
+struct AtrousTiles {
+    int nb[kAtrousMaxLevels];
+    int stride;
+};
+__global__ void __launch_bounds__(256) atrous_thresh_kernel(const float* __restrict__ part, AtrousTiles tl, long long npx,
                                                             AtrousThrArgs a, float* __restrict__ thr) {
-    const int j = blockIdx.x / 3, c = blockIdx.x % 3;
+    const int j = blockIdx.x / 3, c = blockIdx.x % 3, nblocks = tl.nb[j];
     __shared__ double red[256];
     double s = 0.0;
-    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) s += (double)part[((size_t)j * nblocks + b) * 3 + c];
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) s += (double)part[(size_t)j * tl.stride + (size_t)b * 3 + c];
     red[threadIdx.x] = s;
     __syncthreads();
     for (int k = 128; k > 0; k >>= 1) {
@@ -423,17 +434,20 @@ cudaError_t atrous_run(const AtrousPlan& p, const Img& in, const Img& out, bool 
     const dim3 pg((unsigned)((p.w + 255) / 256), (unsigned)p.h);
     if (f16) atrous_prep_kernel<__half><<<pg, 256, 0, st>>>(in, c[0], npx);
     else atrous_prep_kernel<float><<<pg, 256, 0, st>>>(in, c[0], npx);
-    const dim3 lg((unsigned)p.gx, (unsigned)p.gy);
+    AtrousTiles tl{};
+    tl.stride = p.gx * p.gy * 3;
     for (int j = 0; j < p.levels; ++j) {
         const int s = 1 << j;
+        const dim3 lg((unsigned)p.gx, (unsigned)p.gy);
+        tl.nb[j] = (int)(lg.x * lg.y);
         atrous_level_kernel<<<lg, kAtThreads, at_smem(s), st>>>(c[j & 1], c[(j + 1) & 1], wv + (size_t)j * 3 * npx,
-                                                               part + (size_t)j * p.gx * p.gy * 3, p.w, p.h, npx, s);
+                                                               part + (size_t)j * tl.stride, p.w, p.h, npx, s);
     }
     AtrousThrArgs ta{};
     for (int j = 0; j < p.levels; ++j)
         for (int k = 0; k < 3; ++k) ta.noise[j][k] = p.noise[j][k];
     for (int k = 0; k < 3; ++k) ta.strength[k] = p.strength[k];
-    atrous_thresh_kernel<<<p.levels * 3, 256, 0, st>>>(part, p.gx * p.gy, npx, ta, thr);
+    atrous_thresh_kernel<<<p.levels * 3, 256, 0, st>>>(part, tl, npx, ta, thr);
     if (f16) atrous_recon_kernel<__half><<<pg, 256, 0, st>>>(in, out, c[p.levels & 1], wv, thr, p.levels, npx);
     else atrous_recon_kernel<float><<<pg, 256, 0, st>>>(in, out, c[p.levels & 1], wv, thr, p.levels, npx);
     return cudaGetLastError();
