@@ -328,6 +328,7 @@ def b200_arm(args):
     from cpipe_b200 import _abi as A
     from cpipe_b200 import surrogate as S
     from cpipe_b200.chain import Chain, ChainConfig
+    from cpipe_b200.roofline import node_roofline
     L = A.lib()
     assert L.cpipe_cuda_set_device(local) == 0, "no CUDA device"
 
@@ -502,6 +503,10 @@ def b200_arm(args):
     if rank == 0 and world == 1 and not args.no_extra:
         line["batched_form"] = batched_form()
         line["spec_form"] = spec_form(peak_gbs)
+        line["node_roofline"] = {"peak_gbs": peak_gbs, "peak_kind": gbs_kind,
+                                 "note": "each node's filter alone, 12 MP device buffers, bytes = its input and "
+                                         "output once in the reference's formats",
+                                 "nodes": node_roofline(w, h, peak_gbs=peak_gbs)}
         line["qbc_50mp"] = qbc_50mp(weights)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         sample = ChainConfig.full_12mp(width=2016, height=1512, name="sample_2016x1512")

@@ -125,18 +125,6 @@ struct ToneGeom {
     static constexpr size_t bytes() { return sizeof(float) * (size_t)(3 * CP * CH + 2 * 3 * AB + 3 * kCTW * kCTH); }
 };
 
-// Sum of a D x D window (rows k..k+D-1 of `win`) in row-major order.
-template <int D, int ROWS>
-__device__ __forceinline__ float box_chain(const float (&win)[ROWS][D], int k) {
-    float s = win[k][0];
-#pragma unroll
-    for (int dy = 0; dy < D; ++dy)
-#pragma unroll
-        for (int dx = 0; dx < D; ++dx)
-            if (dy != 0 || dx != 0) s = s + win[k + dy][dx];
-    return s;
-}
-
 template <class T>
 __device__ __forceinline__ void load_pair(const Img& in, int x, int y, Rgba* a, Rgba* b);
 // Two adjacent RGBA16F pixels; one 16-byte load when the pair is 16-byte

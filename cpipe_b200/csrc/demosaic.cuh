@@ -8,7 +8,7 @@
 
 namespace cpb {
 
-constexpr int kDmTW = 64, kDmTH = 16, kDmHalo = 3;
+constexpr int kDmTW = 64, kDmTH = 16, kDmHalo = 3, kDmThreads = 256;
 constexpr int kDmIW = kDmTW + 2 * kDmHalo, kDmIH = kDmTH + 2 * kDmHalo;
 constexpr int kDmGW = kDmTW + 2, kDmGH = kDmTH + 2;
 
@@ -29,9 +29,20 @@ __device__ __forceinline__ void demosaic_tile_at(const Loader& load, int w, int 
     __shared__ float s_in[kDmIH * kDmIW];
     __shared__ float s_g[kDmGH * kDmGW];
     __shared__ float s_q[kDmGH * kDmGW];
-    for (int i = threadIdx.x; i < kDmIH * kDmIW; i += blockDim.x) {
+    // Every caller launches kDmThreads threads per block; a thread's tile loads
+    // are all issued before its first shared-memory store.
+    constexpr int kLoads = (kDmIH * kDmIW + kDmThreads - 1) / kDmThreads;
+    float v[kLoads];
+#pragma unroll
+    for (int k = 0; k < kLoads; ++k) {
+        const int i = threadIdx.x + kDmThreads * k;
         const int ty = i / kDmIW, tx = i - ty * kDmIW;
-        s_in[i] = load(clampi(x0 - kDmHalo + tx, 0, w - 1), clampi(y0 - kDmHalo + ty, 0, h - 1));
+        if (i < kDmIH * kDmIW) v[k] = load(clampi(x0 - kDmHalo + tx, 0, w - 1), clampi(y0 - kDmHalo + ty, 0, h - 1));
+    }
+#pragma unroll
+    for (int k = 0; k < kLoads; ++k) {
+        const int i = threadIdx.x + kDmThreads * k;
+        if (i < kDmIH * kDmIW) s_in[i] = v[k];
     }
     __syncthreads();
     if (ALGO != 0) {

@@ -31,51 +31,87 @@ __global__ void __launch_bounds__(kPtThreads) raw_point_kernel(Img in, Img out, 
     op(in, out, x0, y);
 }
 
-struct R16ToF32 {
-    __device__ void operator()(const Img& in, const Img& out, int x0, int y) const {
-        const uint16_t* s = px<const uint16_t>(in, x0, y);
-        float* d = px<float>(out, x0, y);
-        for (int i = 0; i < 4 && x0 + i < in.w; ++i) d[i] = (float)s[i];
+// Bayer-plane point ops with vector access: each thread handles N consecutive
+// pixels of one row (N = 16 for u16 input, 8 for f32: 32 bytes read per
+// thread), loading and storing in 16-byte pieces when the segment is whole,
+// unit-strided and aligned; other segments (row tails, strided or unaligned
+// buffers) take the per-pixel path.  Op maps (input value, x, y) -> float.
+__device__ __forceinline__ bool al16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
+
+template <class TI, class Op>
+__device__ __forceinline__ void raw_vec_row(const Img& in, const Img& out, const Op& op) {
+    constexpr int N = 32 / (int)sizeof(TI);
+    const int y = blockIdx.y;
+    const int x0 = (blockIdx.x * kPtThreads + threadIdx.x) * N;
+    if (x0 >= in.w) return;
+    const TI* s = px<const TI>(in, x0, y);
+    float* d = px<float>(out, x0, y);
+    if (x0 + N <= in.w && in.pix_stride == 1 && out.pix_stride == 1 && al16(s) && al16(d)) {
+        alignas(16) TI v[N];
+        alignas(16) float o[N];
+#pragma unroll
+        for (int i = 0; i < 2; ++i) reinterpret_cast<uint4*>(v)[i] = __ldcs(reinterpret_cast<const uint4*>(s) + i);
+#pragma unroll
+        for (int i = 0; i < N; ++i) o[i] = op(v[i], x0 + i, y);
+#pragma unroll
+        for (int i = 0; i < N / 4; ++i) __stcs(reinterpret_cast<float4*>(d) + i, reinterpret_cast<const float4*>(o)[i]);
+        return;
     }
+    for (int i = 0; i < N && x0 + i < in.w; ++i)
+        *px<float>(out, x0 + i, y) = op(*px<const TI>(in, x0 + i, y), x0 + i, y);
+}
+template <class TI, class Op>
+__global__ void __launch_bounds__(kPtThreads) raw_vec_kernel(Img in, Img out, Op op) {
+    raw_vec_row<TI>(in, out, op);
+}
+
+struct R16ToF32 {
+    __device__ float operator()(uint16_t v, int, int) const { return (float)v; }
 };
 struct Linearize {
     const uint16_t* table;
     int last;
-    __device__ void operator()(const Img& in, const Img& out, int x0, int y) const {
-        const uint16_t* s = px<const uint16_t>(in, x0, y);
-        float* d = px<float>(out, x0, y);
-        for (int i = 0; i < 4 && x0 + i < in.w; ++i) {
-            const int v = s[i];
-            d[i] = (float)__ldg(table + (v < last ? v : last));
-        }
-    }
+    __device__ float operator()(uint16_t v, int, int) const { return (float)__ldg(table + (v < last ? v : last)); }
 };
+// Linearize with the table copied to shared memory first (tables of up to
+// kLinSmemMax entries, which covers every 10..14-bit sensor): the per-pixel
+// lookups then read shared memory instead of gathering through L1.
+constexpr int kLinSmemMax = 16384;
+struct LinearizeShared {
+    const uint16_t* table;  // shared memory
+    int last;
+    __device__ float operator()(uint16_t v, int, int) const { return (float)table[v < last ? v : last]; }
+};
+__global__ void __launch_bounds__(kPtThreads) linearize_smem_kernel(Img in, Img out, const uint16_t* table, int n) {
+    extern __shared__ __align__(16) uint16_t s_tab[];
+    for (int i = threadIdx.x; i < n; i += kPtThreads) s_tab[i] = __ldg(table + i);
+    __syncthreads();
+    raw_vec_row<uint16_t>(in, out, LinearizeShared{s_tab, n - 1});
+}
 struct Blacklevel {
     BlackDev p;
-    __device__ void operator()(const Img& in, const Img& out, int x0, int y) const {
-        const float* s = px<const float>(in, x0, y);
-        float* d = px<float>(out, x0, y);
-        if (x0 + 4 <= in.w && ((reinterpret_cast<uintptr_t>(s) | reinterpret_cast<uintptr_t>(d)) & 15) == 0) {
-            const float4 v = *reinterpret_cast<const float4*>(s);
-            *reinterpret_cast<float4*>(d) =
-                make_float4(blacklevel_px(v.x, x0, y, p), blacklevel_px(v.y, x0 + 1, y, p),
-                            blacklevel_px(v.z, x0 + 2, y, p), blacklevel_px(v.w, x0 + 3, y, p));
-            return;
-        }
-        for (int i = 0; i < 4 && x0 + i < in.w; ++i) d[i] = blacklevel_px(s[i], x0 + i, y, p);
-    }
+    __device__ float operator()(float v, int x, int y) const { return blacklevel_px(v, x, y, p); }
 };
-struct GainMap {
-    GainMapDev g;
-    __device__ void operator()(const Img& in, const Img& out, int x0, int y) const {
-        const float* s = px<const float>(in, x0, y);
-        float* d = px<float>(out, x0, y);
-        for (int i = 0; i < 4 && x0 + i < in.w; ++i) {
-            const int m = gain_map_index(x0 + i, y, g);
-            d[i] = s[i] * gain_px(m, x0 + i, y, g);
-        }
+// GainMap: lanes take interleaved pixels (x0 + lane + 32 j) so that a warp's
+// per-column axis samples (12 bytes each) and its pixels are read as
+// contiguous runs; 8 pixels per thread.
+constexpr int kGmPx = 8;
+__global__ void __launch_bounds__(kPtThreads) gainmap_kernel(Img in, Img out, GainMapDev g) {
+    const int y = blockIdx.y;
+    const int lane = threadIdx.x & 31;
+    const int x0 = (blockIdx.x * kPtThreads + (threadIdx.x & ~31)) * kGmPx + lane;
+    float v[kGmPx];
+#pragma unroll
+    for (int j = 0; j < kGmPx; ++j) {
+        const int x = x0 + 32 * j;
+        v[j] = x < in.w ? __ldcs(px<const float>(in, x, y)) : 0.0F;
     }
-};
+#pragma unroll
+    for (int j = 0; j < kGmPx; ++j) {
+        const int x = x0 + 32 * j;
+        if (x < in.w) __stcs(px<float>(out, x, y), v[j] * gain_px(gain_map_index(x, y, g), x, y, g));
+    }
+}
 
 // Plain copy of one row segment, any element size (used by the pass-through cases).
 __global__ void copy_rows_kernel(const char* src, long long src_pitch, char* dst, long long dst_pitch,
@@ -103,44 +139,88 @@ __global__ void __launch_bounds__(256) demosaic_kernel(Img in, Img out, Cfa cfa)
 }
 
 // ---------------------------------------------------------------- QBC remosaic
-// demosaic_quad_bayer_remosaic_generator.cpp:17-58, integer arithmetic.  Tile
-// with halo 3 (5x5 gather of pixels whose gradients reach one further).
+// demosaic_quad_bayer_remosaic_generator.cpp:17-58, integer arithmetic.  A tap
+// (dx, dy) of output (x, y) reads source s = (clamp(x+dx), clamp(y+dy)); its
+// weight is 65536 / (64 + G(s) + 16 (|dx| + |dy|)), G(s) the source's clamped
+// horizontal plus vertical gradient, when the source's colour is the output's
+// Bayer target, else 0.  The weight depends on the tap only through the
+// source and the distance class d = |dx| + |dy| (0..4), so each tile first
+// computes, for every cell of its halo-2 ring, the clamped source's value,
+// colour and five class weights (5 divisions per cell instead of 25 per
+// output), addressed by the cell's unclamped position: the 25-tap sum then
+// reads cells with fixed offsets and no clamps.  Tile 64x16, input halo 3.
 constexpr int kQbTW = 64, kQbTH = 16, kQbHalo = 3;
 constexpr int kQbIW = kQbTW + 2 * kQbHalo, kQbIH = kQbTH + 2 * kQbHalo;
+constexpr int kQbCW = kQbTW + 4, kQbCH = kQbTH + 4;  // cells: tile + halo 2
 __device__ __forceinline__ int qbc_color(int x, int y) {
     const int mx = ((x % 4) + 4) % 4, my = ((y % 4) + 4) % 4;
     return (my < 2 && mx < 2) ? 0 : ((my >= 2 && mx >= 2) ? 2 : 1);
 }
+// floor(65536 / p) for 64 <= p < 2^18, by reciprocal estimate and one
+// remainder correction (division by multiplication with an approximate
+// reciprocal, Warren, Hacker's Delight 2nd ed., ch. 10).  rcp.approx has
+// relative error <= 2^-23, so 65536 * rcp(p) is within 1024 * 2^-22 < 1 of
+// the true quotient q <= 1024: the truncated estimate is q or one off either
+// way, and the sign of the remainder 65536 - q0 p picks the exact floor.
+__device__ __forceinline__ int div65536(int p) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"((float)p));
+    int q = (int)(65536.0F * r);
+    const int rem = 65536 - q * p;
+    q += rem < 0 ? -1 : (rem >= p ? 1 : 0);
+    return q;
+}
 __global__ void __launch_bounds__(256) qbc_kernel(Img in, Img out) {
     __shared__ int s[kQbIH * kQbIW];
+    __shared__ uint32_t s_vc[kQbCH * kQbCW];        // value | colour << 16
+    __shared__ uint16_t s_cw[5][kQbCH * kQbCW];     // class weights, d = 0..4
     const int x0 = blockIdx.x * kQbTW, y0 = blockIdx.y * kQbTH;
-    for (int i = threadIdx.x; i < kQbIH * kQbIW; i += blockDim.x) {
+    constexpr int kLoads = (kQbIH * kQbIW + 255) / 256;  // issued together (256-thread blocks)
+    int v[kLoads];
+#pragma unroll
+    for (int k = 0; k < kLoads; ++k) {
+        const int i = threadIdx.x + 256 * k;
         const int ty = i / kQbIW, tx = i - ty * kQbIW;
-        s[i] = *px<const uint16_t>(in, clampi(x0 - kQbHalo + tx, 0, in.w - 1), clampi(y0 - kQbHalo + ty, 0, in.h - 1));
+        if (i < kQbIH * kQbIW)
+            v[k] = *px<const uint16_t>(in, clampi(x0 - kQbHalo + tx, 0, in.w - 1), clampi(y0 - kQbHalo + ty, 0, in.h - 1));
+    }
+#pragma unroll
+    for (int k = 0; k < kLoads; ++k) {
+        const int i = threadIdx.x + 256 * k;
+        if (i < kQbIH * kQbIW) s[i] = v[k];
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < kQbCH * kQbCW; i += blockDim.x) {
+        const int cy = i / kQbCW, cx = i - cy * kQbCW;
+        const int sx = clampi(x0 - 2 + cx, 0, in.w - 1), sy = clampi(y0 - 2 + cy, 0, in.h - 1);
+        // tile coordinates of the source and of its clamped neighbours (all inside the halo-3 tile)
+        const int lx = sx - (x0 - kQbHalo), ly = sy - (y0 - kQbHalo);
+        const int lxm = clampi(sx - 1, 0, in.w - 1) - (x0 - kQbHalo), lxp = clampi(sx + 1, 0, in.w - 1) - (x0 - kQbHalo);
+        const int lym = clampi(sy - 1, 0, in.h - 1) - (y0 - kQbHalo), lyp = clampi(sy + 1, 0, in.h - 1) - (y0 - kQbHalo);
+        const int g = abs(s[ly * kQbIW + lxm] - s[ly * kQbIW + lxp]) + abs(s[lym * kQbIW + lx] - s[lyp * kQbIW + lx]);
+        s_vc[i] = (uint32_t)s[ly * kQbIW + lx] | ((uint32_t)qbc_color(sx, sy) << 16);
+#pragma unroll
+        for (int d = 0; d < 5; ++d) {
+            const int cw = div65536(64 + g + 16 * d);
+            s_cw[d][i] = (uint16_t)(cw < 1 ? 1 : cw);
+        }
     }
     __syncthreads();
     for (int i = threadIdx.x; i < kQbTH * kQbTW; i += blockDim.x) {
         const int ty = i / kQbTW, tx = i - ty * kQbTW;
         const int x = x0 + tx, y = y0 + ty;
         if (x >= out.w || y >= out.h) continue;
-        const int target = ((y & 1) == 0 && (x & 1) == 0) ? 0 : (((y & 1) != 0 && (x & 1) != 0) ? 2 : 1);
+        const uint32_t target = ((y & 1) == 0 && (x & 1) == 0) ? 0U : (((y & 1) != 0 && (x & 1) != 0) ? 2U : 1U);
+        const int c0 = (ty + 2) * kQbCW + (tx + 2);
         uint32_t ws = 0, wsum = 0;
 #pragma unroll
         for (int dy = -2; dy <= 2; ++dy) {
 #pragma unroll
             for (int dx = -2; dx <= 2; ++dx) {
-                const int sx = clampi(x + dx, 0, in.w - 1), sy = clampi(y + dy, 0, in.h - 1);
-                // tile coordinates of (sx, sy); clamped neighbours of sx stay inside the halo
-                const int lx = sx - (x0 - kQbHalo), ly = sy - (y0 - kQbHalo);
-                const int lxm = clampi(sx - 1, 0, in.w - 1) - (x0 - kQbHalo), lxp = clampi(sx + 1, 0, in.w - 1) - (x0 - kQbHalo);
-                const int lym = clampi(sy - 1, 0, in.h - 1) - (y0 - kQbHalo), lyp = clampi(sy + 1, 0, in.h - 1) - (y0 - kQbHalo);
-                const int gx = abs(s[ly * kQbIW + lxm] - s[ly * kQbIW + lxp]);
-                const int gy = abs(s[lym * kQbIW + lx] - s[lyp * kQbIW + lx]);
-                const int pen = 64 + gx + gy + ((abs(dx) + abs(dy)) * 16);
-                int cw = 65536 / pen;
-                cw = cw < 1 ? 1 : cw;
-                const uint32_t wt = qbc_color(sx, sy) == target ? (uint32_t)cw : 0U;
-                ws += wt * (uint32_t)s[ly * kQbIW + lx];
+                const int c = c0 + dy * kQbCW + dx;
+                const uint32_t vc = s_vc[c];
+                const uint32_t wt = (vc >> 16) == target ? (uint32_t)s_cw[abs(dx) + abs(dy)][c] : 0U;
+                ws += wt * (vc & 0xFFFFU);
                 wsum += wt;
             }
         }
@@ -149,14 +229,31 @@ __global__ void __launch_bounds__(256) qbc_kernel(Img in, Img out) {
 }
 
 // ------------------------------------------------------------ RGBA point ops
+// RGBA point ops: each thread handles 32 bytes of one row (4 RGBA16F or 2
+// RGBA32F pixels) with 16-byte loads and stores when the segment is whole,
+// 4-channel interleaved and aligned; other segments go pixel by pixel.
 template <class T, class Op>
 __global__ void __launch_bounds__(kPtThreads) rgba_point_kernel(Img in, Img out, Op op) {
+    constexpr int N = 32 / (4 * (int)sizeof(T));
     const int y = blockIdx.y;
-    const int x = blockIdx.x * kPtThreads + threadIdx.x;
-    if (x >= in.w) return;
-    const T* s = px<const T>(in, x, y);
-    op(s, px<T>(out, x, y));
+    const int x0 = (blockIdx.x * kPtThreads + threadIdx.x) * N;
+    if (x0 >= in.w) return;
+    const T* s = px<const T>(in, x0, y);
+    T* d = px<T>(out, x0, y);
+    if (x0 + N <= in.w && in.pix_stride == 4 && out.pix_stride == 4 && al16(s) && al16(d)) {
+        alignas(16) T v[4 * N];
+        alignas(16) T o[4 * N];
+#pragma unroll
+        for (int i = 0; i < 2; ++i) reinterpret_cast<uint4*>(v)[i] = __ldcs(reinterpret_cast<const uint4*>(s) + i);
+#pragma unroll
+        for (int i = 0; i < N; ++i) op(v + 4 * i, o + 4 * i);
+#pragma unroll
+        for (int i = 0; i < 2; ++i) __stcs(reinterpret_cast<uint4*>(d) + i, reinterpret_cast<const uint4*>(o)[i]);
+        return;
+    }
+    for (int i = 0; i < N && x0 + i < in.w; ++i) op(px<const T>(in, x0 + i, y), px<T>(out, x0 + i, y));
 }
+inline dim3 rgba_grid(int w, int h, bool f16) { return row_grid(w, h, f16 ? 4 : 2); }
 
 template <bool F16>
 struct RgbaRound {
@@ -246,73 +343,121 @@ __global__ void __launch_bounds__(256) wavelet_kernel(Img in, Img out, float th)
 }
 
 // ------------------------------------------------------------ guided filter
-// guided_filter_generator.cpp:45-85.  R = 1 (3x3 box) or 2 (5x5 box).  The
-// tile holds the clamped input with halo 2R; a and b are evaluated for the tile
-// plus halo R at unclamped coordinates (their inner reads are clamped), then
-// boxed again.  Sums keep the generator's row-major, left-associated order.
-constexpr int kGfTW = 32, kGfTH = 16;
+// guided_filter_generator.cpp:45-85, box 3x3 (R = 1, radius <= 1) or 5x5
+// (R = 2).  Tile kGfTW x kGfTH; s_v holds the clamped input at coordinates
+// [x0-2R, x0+TW+2R), s_a / s_b the a, b planes at the unclamped coordinates
+// [x0-R, x0+TW+R) (their windows read the clamped input), then
+// out = max(mean(a) v + mean(b), 0).  Box sums keep the generator's row-major
+// left-associated order: a thread loads one (kGfG + 2R) x D window into
+// registers and produces kGfG vertically adjacent sums from it, so each
+// value (and its square) is read and formed once per thread, not per sum.
+constexpr int kGfTW = 64, kGfTH = 16, kGfG = 4;
+template <int R>
+struct GuidedGeom {
+    static constexpr int H = 2 * R, D = 2 * R + 1;
+    static constexpr int IW = kGfTW + 2 * H, IH = kGfTH + 2 * H, IP = IW + 1;
+    static constexpr int AW = kGfTW + 2 * R, AH = kGfTH + 2 * R, AP = AW + 1;
+    static constexpr size_t bytes() { return sizeof(float) * (size_t)(3 * IP * IH + 2 * 3 * AP * AH); }
+};
 template <class T, bool F16, int R>
 __global__ void __launch_bounds__(256) guided_kernel(Img in, Img out, float eps) {
-    constexpr int IW = kGfTW + 4 * R, IH = kGfTH + 4 * R;
-    constexpr int AW = kGfTW + 2 * R, AH = kGfTH + 2 * R;
-    __shared__ float s_v[3][IH * IW];
-    __shared__ float s_a[3][AH * AW];
-    __shared__ float s_b[3][AH * AW];
+    using G = GuidedGeom<R>;
+    constexpr int H = G::H, D = G::D, IW = G::IW, IH = G::IH, IP = G::IP, AW = G::AW, AH = G::AH, AP = G::AP;
+    extern __shared__ __align__(16) float smem_f[];
+    float* s_v = smem_f;               // [3][IH][IP]
+    float* s_a = s_v + 3 * IP * IH;    // [3][AH][AP]
+    float* s_b = s_a + 3 * AP * AH;
     const int x0 = blockIdx.x * kGfTW, y0 = blockIdx.y * kGfTH;
-    for (int i = threadIdx.x; i < IH * IW; i += blockDim.x) {
+    // all of a thread's tile loads are issued before the first store (256-thread blocks)
+    constexpr int kLoads = (IH * IW + 255) / 256;
+    Rgba v[kLoads];
+#pragma unroll
+    for (int k = 0; k < kLoads; ++k) {
+        const int i = threadIdx.x + 256 * k;
         const int ty = i / IW, tx = i - ty * IW;
-        const Rgba v = load_clamped<T>(in, x0 - 2 * R + tx, y0 - 2 * R + ty);
-        s_v[0][i] = v.r;
-        s_v[1][i] = v.g;
-        s_v[2][i] = v.b;
+        if (i < IH * IW) v[k] = load_clamped<T>(in, x0 - H + tx, y0 - H + ty);
     }
-    __syncthreads();
-    constexpr float N = (float)((2 * R + 1) * (2 * R + 1));
-    for (int i = threadIdx.x; i < 3 * AH * AW; i += blockDim.x) {
-        const int c = i / (AH * AW);
-        const int j = i - c * AH * AW;
-        const int ty = j / AW, tx = j - ty * AW;
-        // centre of this a/b sample in s_v coordinates
-        const float* v = s_v[c] + (ty + R) * IW + (tx + R);
-        float sm = 0.0F, sq = 0.0F;
-        bool first = true;
 #pragma unroll
-        for (int dy = -R; dy <= R; ++dy)
-#pragma unroll
-            for (int dx = -R; dx <= R; ++dx) {
-                const float t = v[dy * IW + dx];
-                if (R == 1 && first) { sm = t; sq = t * t; first = false; }
-                else { sm = sm + t; sq = sq + (t * t); }
-            }
-        const float m = sm / N, corr = sq / N;
-        const float var = max0(corr - (m * m));
-        const float a = var / (var + eps);
-        s_a[c][j] = a;
-        s_b[c][j] = m - (a * m);
-    }
-    __syncthreads();
-    for (int i = threadIdx.x; i < kGfTH * kGfTW; i += blockDim.x) {
-        const int ty = i / kGfTW, tx = i - ty * kGfTW;
-        const int x = x0 + tx, y = y0 + ty;
-        if (x >= out.w || y >= out.h) continue;
-        const Rgba src = load_rgba(px<const T>(in, x, y));
-        float o[3];
-        for (int c = 0; c < 3; ++c) {
-            const float* A = s_a[c] + (ty + R) * AW + (tx + R);
-            const float* B = s_b[c] + (ty + R) * AW + (tx + R);
-            float sa = 0.0F, sb = 0.0F;
-            bool first = true;
-#pragma unroll
-            for (int dy = -R; dy <= R; ++dy)
-#pragma unroll
-                for (int dx = -R; dx <= R; ++dx) {
-                    if (R == 1 && first) { sa = A[dy * AW + dx]; sb = B[dy * AW + dx]; first = false; }
-                    else { sa = sa + A[dy * AW + dx]; sb = sb + B[dy * AW + dx]; }
-                }
-            const float v = s_v[c][(ty + 2 * R) * IW + (tx + 2 * R)];
-            o[c] = max0(((sa / N) * v) + (sb / N));
+    for (int k = 0; k < kLoads; ++k) {
+        const int i = threadIdx.x + 256 * k;
+        const int ty = i / IW, tx = i - ty * IW;
+        if (i < IH * IW) {
+            s_v[ty * IP + tx] = v[k].r;
+            s_v[IP * IH + ty * IP + tx] = v[k].g;
+            s_v[2 * IP * IH + ty * IP + tx] = v[k].b;
         }
-        store_rgba(px<T>(out, x, y), Rgba{o[0], o[1], o[2], src.a});
+    }
+    __syncthreads();
+    constexpr float N = (float)(D * D);
+    constexpr int AG = (AH + kGfG - 1) / kGfG;
+    for (int item = threadIdx.x; item < 3 * AW * AG; item += blockDim.x) {
+        const int c = item / (AW * AG);
+        const int rem = item - c * AW * AG;
+        const int g = rem / AW, tx = rem - g * AW;
+        const int ty0 = g * kGfG;
+        const float* V = s_v + c * IP * IH + ty0 * IP + tx;  // window origin of a/b sample (ty0, tx)
+        float win[kGfG + 2 * R][D], sq[kGfG + 2 * R][D];
+#pragma unroll
+        for (int r = 0; r < kGfG + 2 * R; ++r)
+#pragma unroll
+            for (int dx = 0; dx < D; ++dx) {
+                win[r][dx] = (ty0 + r < IH) ? V[r * IP + dx] : 0.0F;
+                sq[r][dx] = win[r][dx] * win[r][dx];
+            }
+#pragma unroll
+        for (int k = 0; k < kGfG; ++k) {
+            if (ty0 + k >= AH) break;
+            const float m = box_chain<D>(win, k) / N, corr = box_chain<D>(sq, k) / N;
+            const float var = max0(corr - (m * m));
+            const float a = var / (var + eps);
+            const int j = c * AP * AH + (ty0 + k) * AP + tx;
+            s_a[j] = a;
+            s_b[j] = m - (a * m);
+        }
+    }
+    __syncthreads();
+    constexpr int TG = kGfTH / kGfG;
+    for (int item = threadIdx.x; item < kGfTW * TG; item += blockDim.x) {
+        const int g = item / kGfTW, tx = item - g * kGfTW;
+        const int ty0 = g * kGfG;
+        float o[3][kGfG];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            float sa[kGfG], sb[kGfG];
+            {
+                float win[kGfG + 2 * R][D];
+                const float* A = s_a + c * AP * AH + ty0 * AP + tx;
+#pragma unroll
+                for (int r = 0; r < kGfG + 2 * R; ++r)
+#pragma unroll
+                    for (int dx = 0; dx < D; ++dx) win[r][dx] = A[r * AP + dx];
+#pragma unroll
+                for (int k = 0; k < kGfG; ++k) sa[k] = box_chain<D>(win, k);
+            }
+            {
+                float win[kGfG + 2 * R][D];
+                const float* B = s_b + c * AP * AH + ty0 * AP + tx;
+#pragma unroll
+                for (int r = 0; r < kGfG + 2 * R; ++r)
+#pragma unroll
+                    for (int dx = 0; dx < D; ++dx) win[r][dx] = B[r * AP + dx];
+#pragma unroll
+                for (int k = 0; k < kGfG; ++k) sb[k] = box_chain<D>(win, k);
+            }
+#pragma unroll
+            for (int k = 0; k < kGfG; ++k) {
+                const float v = s_v[c * IP * IH + (ty0 + k + H) * IP + (tx + H)];
+                o[c][k] = max0(((sa[k] / N) * v) + (sb[k] / N));
+            }
+        }
+        const int x = x0 + tx;
+#pragma unroll
+        for (int k = 0; k < kGfG; ++k) {
+            const int y = y0 + ty0 + k;
+            if (x >= out.w || y >= out.h) continue;
+            const Rgba src = load_rgba(px<const T>(in, x, y));
+            store_rgba(px<T>(out, x, y), Rgba{o[0][k], o[1][k], o[2][k], src.a});
+        }
     }
 }
 
@@ -417,19 +562,22 @@ __global__ void __launch_bounds__(256) trim_kernel(Img in, Img out, uint32_t top
 
 // ============================================================ host launchers
 cudaError_t launch_r16u_to_f32(const Img& in, const Img& out, cudaStream_t st) {
-    raw_point_kernel<<<row_grid(in.w, in.h, 4), kPtThreads, 0, st>>>(in, out, R16ToF32{});
+    raw_vec_kernel<uint16_t><<<row_grid(in.w, in.h, 16), kPtThreads, 0, st>>>(in, out, R16ToF32{});
     return cudaGetLastError();
 }
 cudaError_t launch_linearize(const Img& in, const Img& out, const uint16_t* d_table, int n, cudaStream_t st) {
-    raw_point_kernel<<<row_grid(in.w, in.h, 4), kPtThreads, 0, st>>>(in, out, Linearize{d_table, n - 1});
+    if (n > 0 && n <= kLinSmemMax)
+        linearize_smem_kernel<<<row_grid(in.w, in.h, 16), kPtThreads, (size_t)n * sizeof(uint16_t), st>>>(in, out, d_table, n);
+    else
+        raw_vec_kernel<uint16_t><<<row_grid(in.w, in.h, 16), kPtThreads, 0, st>>>(in, out, Linearize{d_table, n - 1});
     return cudaGetLastError();
 }
 cudaError_t launch_blacklevel(const Img& in, const Img& out, const BlackDev& p, cudaStream_t st) {
-    raw_point_kernel<<<row_grid(in.w, in.h, 4), kPtThreads, 0, st>>>(in, out, Blacklevel{p});
+    raw_vec_kernel<float><<<row_grid(in.w, in.h, 8), kPtThreads, 0, st>>>(in, out, Blacklevel{p});
     return cudaGetLastError();
 }
 cudaError_t launch_gainmap(const Img& in, const Img& out, const GainMapDev& g, cudaStream_t st) {
-    raw_point_kernel<<<row_grid(in.w, in.h, 4), kPtThreads, 0, st>>>(in, out, GainMap{g});
+    gainmap_kernel<<<row_grid(in.w, in.h, kGmPx), kPtThreads, 0, st>>>(in, out, g);
     return cudaGetLastError();
 }
 cudaError_t launch_copy(const void* src, long long src_pitch, void* dst, long long dst_pitch, long long row_bytes,
@@ -468,13 +616,13 @@ cudaError_t launch_rgba16f_to_unorm(const Img& in, const Img& out, int bits8, cu
     if (F16) { KERNEL_F16; } else { KERNEL_F32; }
 
 cudaError_t launch_wb(const Img& in, const Img& out, bool f16, const float n[3], cudaStream_t st) {
-    const dim3 g = row_grid(in.w, in.h, 1);
+    const dim3 g = rgba_grid(in.w, in.h, f16);
     RGBA_DISPATCH(f16, (rgba_point_kernel<__half><<<g, kPtThreads, 0, st>>>(in, out, WbOp<__half>{{n[0], n[1], n[2]}})),
                   (rgba_point_kernel<float><<<g, kPtThreads, 0, st>>>(in, out, WbOp<float>{{n[0], n[1], n[2]}})));
     return cudaGetLastError();
 }
 cudaError_t launch_colormatrix(const Img& in, const Img& out, bool f16, const float t[9], cudaStream_t st) {
-    const dim3 g = row_grid(in.w, in.h, 1);
+    const dim3 g = rgba_grid(in.w, in.h, f16);
     CmOp<__half> oh;
     CmOp<float> of;
     for (int i = 0; i < 9; ++i) oh.t[i] = of.t[i] = t[i];
@@ -483,13 +631,13 @@ cudaError_t launch_colormatrix(const Img& in, const Img& out, bool f16, const fl
     return cudaGetLastError();
 }
 cudaError_t launch_filmic(const Img& in, const Img& out, bool f16, const FilmicDev& p, cudaStream_t st) {
-    const dim3 g = row_grid(in.w, in.h, 1);
+    const dim3 g = rgba_grid(in.w, in.h, f16);
     RGBA_DISPATCH(f16, (rgba_point_kernel<__half><<<g, kPtThreads, 0, st>>>(in, out, FilmicOp<__half>{p})),
                   (rgba_point_kernel<float><<<g, kPtThreads, 0, st>>>(in, out, FilmicOp<float>{p})));
     return cudaGetLastError();
 }
 cudaError_t launch_lut3d(const Img& in, const Img& out, bool f16, const float4* d_lut, int S, int interp, cudaStream_t st) {
-    const dim3 g = row_grid(in.w, in.h, 1);
+    const dim3 g = rgba_grid(in.w, in.h, f16);
     RGBA_DISPATCH(f16, (rgba_point_kernel<__half><<<g, kPtThreads, 0, st>>>(in, out, LutOp<__half>{d_lut, S, interp})),
                   (rgba_point_kernel<float><<<g, kPtThreads, 0, st>>>(in, out, LutOp<float>{d_lut, S, interp})));
     return cudaGetLastError();
@@ -509,16 +657,19 @@ cudaError_t launch_wavelet(const Img& in, const Img& out, bool f16, float streng
                   (wavelet_kernel<float><<<g, 256, 0, st>>>(in, out, th)));
     return cudaGetLastError();
 }
-cudaError_t launch_guided(const Img& in, const Img& out, bool f16, int radius, float eps, cudaStream_t st) {
+template <class T, bool F16, int R>
+cudaError_t guided_launch(const Img& in, const Img& out, float eps, cudaStream_t st) {
+    static const cudaError_t attr = cudaFuncSetAttribute(guided_kernel<T, F16, R>,
+                                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                         (int)GuidedGeom<R>::bytes());
+    if (attr != cudaSuccess) return attr;
     const dim3 g((unsigned)((in.w + kGfTW - 1) / kGfTW), (unsigned)((in.h + kGfTH - 1) / kGfTH));
-    if (radius <= 1) {
-        RGBA_DISPATCH(f16, (guided_kernel<__half, true, 1><<<g, 256, 0, st>>>(in, out, eps)),
-                      (guided_kernel<float, false, 1><<<g, 256, 0, st>>>(in, out, eps)));
-    } else {
-        RGBA_DISPATCH(f16, (guided_kernel<__half, true, 2><<<g, 256, 0, st>>>(in, out, eps)),
-                      (guided_kernel<float, false, 2><<<g, 256, 0, st>>>(in, out, eps)));
-    }
+    guided_kernel<T, F16, R><<<g, 256, GuidedGeom<R>::bytes(), st>>>(in, out, eps);
     return cudaGetLastError();
+}
+cudaError_t launch_guided(const Img& in, const Img& out, bool f16, int radius, float eps, cudaStream_t st) {
+    if (radius <= 1) return f16 ? guided_launch<__half, true, 1>(in, out, eps, st) : guided_launch<float, false, 1>(in, out, eps, st);
+    return f16 ? guided_launch<__half, true, 2>(in, out, eps, st) : guided_launch<float, false, 2>(in, out, eps, st);
 }
 cudaError_t launch_warp(const Img& in, const Img& out, bool f16, const WarpDev& w, cudaStream_t st) {
     const dim3 g((unsigned)((out.w + 127) / 128), (unsigned)out.h);

@@ -372,4 +372,17 @@ __device__ __forceinline__ Rgba warp_px(const Img& in, const WarpDev& w, int x, 
     return v;
 }
 
+// Guided-filter box sum: the D x D window of rows k..k+D-1 of `win`, added in
+// the generator's row-major left-associated order (guided_filter_generator.cpp:60-76).
+template <int D, int ROWS>
+__device__ __forceinline__ float box_chain(const float (&win)[ROWS][D], int k) {
+    float s = win[k][0];
+#pragma unroll
+    for (int dy = 0; dy < D; ++dy)
+#pragma unroll
+        for (int dx = 0; dx < D; ++dx)
+            if (dy != 0 || dx != 0) s = s + win[k + dy][dx];
+    return s;
+}
+
 }  // namespace cpb
