@@ -214,18 +214,19 @@ __device__ __forceinline__ void denoise_tone_tile(const Img& in, const Img& out,
             const int g = rem / AW, tx = rem - g * AW;
             const int ty0 = g * kCG;
             const float* V = s_bm + c * CP * CH + ty0 * CP + tx;  // window origin of output (ty0, tx)
-            float win[kCG + 2 * R][D], sq[kCG + 2 * R][D];
+            float2 win[kCG + 2 * R][D];  // (value, value^2)
 #pragma unroll
             for (int r = 0; r < kCG + 2 * R; ++r)
 #pragma unroll
                 for (int dx = 0; dx < D; ++dx) {
-                    win[r][dx] = (ty0 + r < CH) ? V[r * CP + dx] : 0.0F;
-                    sq[r][dx] = win[r][dx] * win[r][dx];
+                    const float t = (ty0 + r < CH) ? V[r * CP + dx] : 0.0F;
+                    win[r][dx] = make_float2(t, t * t);
                 }
 #pragma unroll
             for (int k = 0; k < kCG; ++k) {
                 if (ty0 + k >= AH) break;
-                const float m = box_chain<D>(win, k) / N, corr = box_chain<D>(sq, k) / N;
+                const float2 sums = box_chain2<D>(win, k);
+                const float m = sums.x / N, corr = sums.y / N;
                 const float var = max0(corr - (m * m));
                 const float a = var / (var + p.eps);
                 const int j = c * AB + (ty0 + k) * AP + tx;
@@ -241,32 +242,19 @@ __device__ __forceinline__ void denoise_tone_tile(const Img& in, const Img& out,
             const int rem = item - c * kCTW * TG;
             const int g = rem / kCTW, tx = rem - g * kCTW;
             const int ty0 = g * kCG;
-            float sa[kCG], sb[kCG];
-            {
-                float win[kCG + 2 * R][D];
-                const float* A = s_a + c * AB + ty0 * AP + tx;
+            float2 win[kCG + 2 * R][D];  // (a, b)
+            const float* A = s_a + c * AB + ty0 * AP + tx;
+            const float* B = s_b + c * AB + ty0 * AP + tx;
 #pragma unroll
-                for (int r = 0; r < kCG + 2 * R; ++r)
+            for (int r = 0; r < kCG + 2 * R; ++r)
 #pragma unroll
-                    for (int dx = 0; dx < D; ++dx) win[r][dx] = A[r * AP + dx];
-#pragma unroll
-                for (int k = 0; k < kCG; ++k) sa[k] = box_chain<D>(win, k);
-            }
-            {
-                float win[kCG + 2 * R][D];
-                const float* B = s_b + c * AB + ty0 * AP + tx;
-#pragma unroll
-                for (int r = 0; r < kCG + 2 * R; ++r)
-#pragma unroll
-                    for (int dx = 0; dx < D; ++dx) win[r][dx] = B[r * AP + dx];
-#pragma unroll
-                for (int k = 0; k < kCG; ++k) sb[k] = box_chain<D>(win, k);
-            }
+                for (int dx = 0; dx < D; ++dx) win[r][dx] = make_float2(A[r * AP + dx], B[r * AP + dx]);
 #pragma unroll
             for (int k = 0; k < kCG; ++k) {
                 const int ty = ty0 + k;
+                const float2 sab = box_chain2<D>(win, k);
                 const float v = s_bm[c * CP * CH + (ty + H) * CP + (tx + H)];
-                s_gf[c * kCTW * kCTH + ty * kCTW + tx] = rnd<F16>(max0(((sa[k] / N) * v) + (sb[k] / N)));
+                s_gf[c * kCTW * kCTH + ty * kCTW + tx] = rnd<F16>(max0(((sab.x / N) * v) + (sab.y / N)));
             }
         }
     }
@@ -645,7 +633,9 @@ cpipe_cuda_chain* cpipe_cuda_chain_create(const cpipe_cuda_chain_config* cfg, in
         if (st != CPIPE_OK) return fail(st, c);
         c->tone.has_lut = 1;
     }
-    const size_t total = lut_off + cells.size() * sizeof(float4);
+    // per-grid-row gain table after the LUT, filled on the device below
+    const size_t hrows_off = (lut_off + cells.size() * sizeof(float4) + 15) & ~size_t(15);
+    const size_t total = hrows_off + (c->raw.has_gain ? gainmap_hrows_bytes(c->raw.gain, w) : 0);
     if (total) {
         if (cudaMalloc(&c->d_tables, total) != cudaSuccess) return fail(CPIPE_OOM, c);
         std::vector<char> host(total, 0);
@@ -653,7 +643,13 @@ cpipe_cuda_chain* cpipe_cuda_chain_create(const cpipe_cuda_chain_config* cfg, in
         if (!cells.empty()) std::memcpy(host.data() + lut_off, cells.data(), cells.size() * sizeof(float4));
         if (cudaMemcpy(c->d_tables, host.data(), total, cudaMemcpyHostToDevice) != cudaSuccess)
             return fail(CPIPE_INTERNAL_ERROR, c);
-        if (c->raw.has_gain) cpb_gainmap_bind(&c->raw.gain, static_cast<const char*>(c->d_tables), offsets);
+        if (c->raw.has_gain) {
+            cpb_gainmap_bind(&c->raw.gain, static_cast<const char*>(c->d_tables), offsets);
+            if (launch_gainmap_hrows(&c->raw.gain, static_cast<char*>(c->d_tables) + hrows_off, w, nullptr) !=
+                    cudaSuccess ||
+                cudaStreamSynchronize(nullptr) != cudaSuccess)
+                return fail(CPIPE_INTERNAL_ERROR, c);
+        }
         if (c->tone.has_lut) c->tone.lut = reinterpret_cast<const float4*>(static_cast<char*>(c->d_tables) + lut_off);
     }
     // OpcodeList3

@@ -208,6 +208,88 @@ Call::~Call() {
     for (void* p : scratch) cudaFreeAsync(p, stream);
 }
 
+// Device copies of prepared filter tables (linearization tables, GainMap
+// gain / axis / grid-row tables, 3D LUT cells), keyed by the exact parameter
+// blob and the frame extent: a pipeline that calls a filter with the same
+// parameters frame after frame prepares and uploads its tables once.  A small
+// least-recently-used set per process (each entry records its device).  The
+// caller holds the TableLock from lookup until its kernels are launched, so no
+// entry is released under a launch; an evicted entry is freed after a device
+// synchronisation.  cpipe_cuda_trim_scratch releases every entry.
+namespace {
+std::mutex g_tab_mu;
+std::vector<TableEntry> g_tabs;
+uint64_t g_tab_clock = 0;
+constexpr size_t kTableEntries = 8;
+}  // namespace
+
+TableLock::TableLock() : lock(g_tab_mu) {}
+
+const TableEntry* table_find(int kind, int w, int h, const void* key, size_t key_bytes) {
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) return nullptr;
+    for (TableEntry& e : g_tabs) {
+        if (e.dev == dev && e.kind == kind && e.w == w && e.h == h && e.key.size() == key_bytes &&
+            std::memcmp(e.key.data(), key, key_bytes) == 0) {
+            e.used = ++g_tab_clock;
+            return &e;
+        }
+    }
+    return nullptr;
+}
+
+int table_add(int kind, int w, int h, const void* key, size_t key_bytes, const void* host, size_t host_bytes,
+              size_t device_bytes, TableEntry** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return cuda_status(e, "table cache");
+    if (g_tabs.size() >= kTableEntries) {
+        size_t lru = 0;
+        for (size_t i = 1; i < g_tabs.size(); ++i)
+            if (g_tabs[i].used < g_tabs[lru].used) lru = i;
+        if ((e = cudaSetDevice(g_tabs[lru].dev)) == cudaSuccess && (e = cudaDeviceSynchronize()) == cudaSuccess)
+            e = cudaFree(g_tabs[lru].d);
+        cudaSetDevice(dev);
+        if (e != cudaSuccess) return cuda_status(e, "table cache eviction");
+        g_tabs.erase(g_tabs.begin() + (long)lru);
+    }
+    TableEntry t;
+    t.dev = dev;
+    t.kind = kind;
+    t.w = w;
+    t.h = h;
+    t.key.assign(static_cast<const unsigned char*>(key), static_cast<const unsigned char*>(key) + key_bytes);
+    if (cudaMalloc(&t.d, device_bytes < 256 ? 256 : device_bytes) != cudaSuccess) {
+        cudaGetLastError();
+        std::snprintf(g_err, sizeof(g_err), "device allocation of %zu bytes failed", device_bytes);
+        return CPIPE_OOM;
+    }
+    if ((e = cudaMemcpy(t.d, host, host_bytes, cudaMemcpyHostToDevice)) != cudaSuccess) {
+        cudaFree(t.d);
+        return cuda_status(e, "table upload");
+    }
+    t.used = ++g_tab_clock;
+    g_tabs.push_back(std::move(t));
+    *out = &g_tabs.back();
+    return CPIPE_OK;
+}
+
+static cudaError_t table_release_all() {
+    std::lock_guard<std::mutex> lock(g_tab_mu);
+    cudaError_t first = cudaSuccess;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    for (TableEntry& t : g_tabs) {
+        cudaError_t e = cudaSetDevice(t.dev);
+        if (e == cudaSuccess) e = cudaDeviceSynchronize();
+        if (e == cudaSuccess) e = cudaFree(t.d);
+        if (first == cudaSuccess) first = e;
+    }
+    cudaSetDevice(cur);
+    g_tabs.clear();
+    return first;
+}
+
 bool device_ready() {
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
@@ -255,7 +337,8 @@ const char* cpipe_cuda_last_error(void) { return g_err; }
 int cpipe_cuda_synchronize(void) { return cuda_status(cudaStreamSynchronize(g_stream), "synchronize"); }
 int cpipe_cuda_trim_scratch(void) {
     cudaMemPool_t pool;
-    cudaError_t e = cudaDeviceSynchronize();
+    cudaError_t e = table_release_all();
+    if (e == cudaSuccess) e = cudaDeviceSynchronize();
     if (e == cudaSuccess) e = scratch_pool(&pool);
     if (e == cudaSuccess) e = cudaMemPoolTrimTo(pool, 0);
     return cuda_status(e, "trim scratch");
@@ -325,11 +408,18 @@ int cpipe_cuda_linearize_dng_lut(halide_buffer_t* const* inputs, size_t n_in, ha
     BIND(0, inputs, Kind::BayerU16, false, in);
     BIND(0, outputs, Kind::BayerF32, true, out);
     REQUIRE_SAME_EXTENT(in, out);
-    void* d_table = nullptr;
-    int st = call.upload(static_cast<const char*>(blob) + sizeof(*hd), hd->table_size * sizeof(uint16_t), &d_table);
-    if (st != CPIPE_OK) return call.finish(st);
+    const size_t tbytes = hd->table_size * sizeof(uint16_t);
+    const char* table = static_cast<const char*>(blob) + sizeof(*hd);
+    TableLock lock;
+    const TableEntry* t = table_find(kTabLinearize, 0, 0, table, tbytes);
+    if (t == nullptr) {
+        TableEntry* added = nullptr;
+        const int st = table_add(kTabLinearize, 0, 0, table, tbytes, table, tbytes, tbytes, &added);
+        if (st != CPIPE_OK) return call.finish(st);
+        t = added;
+    }
     return call.finish(cuda_status(
-        launch_linearize(in.img, out.img, static_cast<const uint16_t*>(d_table), (int)hd->table_size, call.stream),
+        launch_linearize(in.img, out.img, static_cast<const uint16_t*>(t->d), (int)hd->table_size, call.stream),
         "linearize"));
 }
 
@@ -421,6 +511,7 @@ int cpb_gainmap_prepare(const void* blob, size_t blob_size, int w, int h, std::v
         std::memcpy(table->data() + off, gains + (size_t)maps[i].gain_offset * sizeof(float), n);
         off += (n + 15) & ~size_t(15);
         g->points_h[i] = (int)maps[i].map_points_h;
+        g->points_v[i] = (int)maps[i].map_points_v;
     }
     for (uint32_t i = 0; i < hd->map_count; ++i) {
         offsets[1][i] = off;
@@ -457,15 +548,29 @@ int cpipe_cuda_lens_shading_gainmap(halide_buffer_t* const* inputs, size_t n_in,
     BIND(0, inputs, Kind::BayerF32, false, in);
     BIND(0, outputs, Kind::BayerF32, true, out);
     REQUIRE_SAME_EXTENT(in, out);
-    std::vector<char> table;
-    GainMapDev g{};
-    size_t offsets[3][4] = {};
-    int st = cpb_gainmap_prepare(blob, blob_size, in.img.w, in.img.h, &table, &g, offsets);
-    if (st != CPIPE_OK) return call.finish(st);
-    void* d_table = nullptr;
-    st = call.upload(table.data(), table.size(), &d_table);
-    if (st != CPIPE_OK) return call.finish(st);
-    cpb_gainmap_bind(&g, static_cast<const char*>(d_table), offsets);
+    TableLock lock;
+    const TableEntry* t = table_find(kTabGainMap, in.img.w, in.img.h, blob, blob_size);
+    if (t == nullptr) {
+        std::vector<char> table;
+        GainMapDev g{};
+        size_t offsets[3][4] = {};
+        int st = cpb_gainmap_prepare(blob, blob_size, in.img.w, in.img.h, &table, &g, offsets);
+        if (st != CPIPE_OK) return call.finish(st);
+        const size_t hoff = (table.size() + 15) & ~size_t(15);
+        TableEntry* added = nullptr;
+        st = table_add(kTabGainMap, in.img.w, in.img.h, blob, blob_size, table.data(), table.size(),
+                       hoff + gainmap_hrows_bytes(g, in.img.w), &added);
+        if (st != CPIPE_OK) return call.finish(st);
+        cpb_gainmap_bind(&g, static_cast<const char*>(added->d), offsets);
+        cudaError_t e = launch_gainmap_hrows(&g, static_cast<char*>(added->d) + hoff, in.img.w, call.stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(call.stream);
+        if (e != cudaSuccess) return call.finish(cuda_status(e, "gainmap rows"));
+        added->meta.resize(sizeof(g));
+        std::memcpy(added->meta.data(), &g, sizeof(g));
+        t = added;
+    }
+    GainMapDev g;
+    std::memcpy(&g, t->meta.data(), sizeof(g));
     return call.finish(cuda_status(launch_gainmap(in.img, out.img, g, call.stream), "gainmap"));
 }
 
@@ -684,20 +789,34 @@ int cpb_lut_prepare(const void* blob, size_t blob_size, std::vector<float4>* cel
 int cpipe_cuda_color_3d_lut(halide_buffer_t* const* inputs, size_t n_in, halide_buffer_t* const* outputs,
                             size_t n_out, const void* blob, size_t blob_size) {
     CHECK_ARITY(1, 1);
+    if (blob == nullptr) return CPIPE_BAD_INDEX;
+    TableLock lock;
+    const TableEntry* t = table_find(kTabLut, 0, 0, blob, blob_size);
     std::vector<float4> cells;
-    int S = 0, interp = 0;
-    const int pst = cpb_lut_prepare(blob, blob_size, &cells, &S, &interp);
-    if (pst != CPIPE_OK) return pst;
+    int lut_si[2] = {0, 0};  // size, interpolation
+    if (t == nullptr) {
+        const int pst = cpb_lut_prepare(blob, blob_size, &cells, &lut_si[0], &lut_si[1]);
+        if (pst != CPIPE_OK) return pst;
+    } else {
+        std::memcpy(lut_si, t->meta.data(), sizeof(lut_si));
+    }
     if (!device_ready()) return CPIPE_INTERNAL_ERROR;
     Call call;
     Bound in, out;
     int st = rgba_pair(call, inputs, outputs, &in, &out);
     if (st != CPIPE_OK) return call.finish(st);
-    void* d_lut = nullptr;
-    st = call.upload(cells.data(), cells.size() * sizeof(float4), &d_lut);
-    if (st != CPIPE_OK) return call.finish(st);
-    return call.finish(cuda_status(
-        launch_lut3d(in.img, out.img, in.elem == 2, static_cast<const float4*>(d_lut), S, interp, call.stream), "lut"));
+    if (t == nullptr) {
+        TableEntry* added = nullptr;
+        const size_t bytes = cells.size() * sizeof(float4);
+        if ((st = table_add(kTabLut, 0, 0, blob, blob_size, cells.data(), bytes, bytes, &added)) != CPIPE_OK)
+            return call.finish(st);
+        added->meta.resize(sizeof(lut_si));
+        std::memcpy(added->meta.data(), lut_si, sizeof(lut_si));
+        t = added;
+    }
+    return call.finish(cuda_status(launch_lut3d(in.img, out.img, in.elem == 2, static_cast<const float4*>(t->d),
+                                                lut_si[0], lut_si[1], call.stream),
+                                   "lut"));
 }
 
 // ----------------------------------------------------------------- a16 filmic

@@ -4,6 +4,8 @@
 
 #include <cuda_runtime.h>
 
+#include <cstdint>
+#include <mutex>
 #include <vector>
 
 #include "../../include/cpipe_b200.h"
@@ -35,6 +37,29 @@ struct Call {
     int upload(const void* host, size_t bytes, void** out);
     int finish(int status);
 };
+
+// Prepared-table cache (filters.cu): a device copy of a filter's prepared
+// tables keyed by (kind, frame extent, parameter blob bytes).  Hold a
+// TableLock from table_find / table_add until the kernels that read the entry
+// are launched.
+enum TableKind { kTabLinearize = 1, kTabGainMap = 2, kTabLut = 3 };
+struct TableEntry {
+    int dev = 0, kind = 0, w = 0, h = 0;
+    std::vector<unsigned char> key;
+    void* d = nullptr;
+    std::vector<unsigned char> meta;  // kind-specific host values (GainMapDev, LUT size / interpolation)
+    uint64_t used = 0;
+};
+struct TableLock {
+    std::unique_lock<std::mutex> lock;
+    TableLock();
+};
+const TableEntry* table_find(int kind, int w, int h, const void* key, size_t key_bytes);
+// Copies host_bytes of `host` into a new device entry of device_bytes (which
+// may leave room for tables filled on the device), evicting the least recently
+// used entry when the set is full.
+int table_add(int kind, int w, int h, const void* key, size_t key_bytes, const void* host, size_t host_bytes,
+              size_t device_bytes, TableEntry** out);
 
 struct Opcode3View {
     uint32_t count = 0;

@@ -17,6 +17,11 @@ struct VignetteParams {
 cudaError_t launch_r16u_to_f32(const Img& in, const Img& out, cudaStream_t st);
 cudaError_t launch_linearize(const Img& in, const Img& out, const uint16_t* d_table, int n, cudaStream_t st);
 cudaError_t launch_blacklevel(const Img& in, const Img& out, const BlackDev& p, cudaStream_t st);
+// Device bytes of the per-grid-row table of g at image width w; fill it
+// (sets g->hrow / g->hw to point into d_hrows) before launch_gainmap or any
+// kernel that evaluates gain_px.
+size_t gainmap_hrows_bytes(const GainMapDev& g, int w);
+cudaError_t launch_gainmap_hrows(GainMapDev* g, void* d_hrows, int w, cudaStream_t st);
 cudaError_t launch_gainmap(const Img& in, const Img& out, const GainMapDev& g, cudaStream_t st);
 cudaError_t launch_copy(const void* src, long long src_pitch, void* dst, long long dst_pitch, long long row_bytes,
                         int rows, cudaStream_t st);

@@ -39,9 +39,8 @@ __global__ void __launch_bounds__(kPtThreads) raw_point_kernel(Img in, Img out, 
 __device__ __forceinline__ bool al16(const void* p) { return (reinterpret_cast<uintptr_t>(p) & 15) == 0; }
 
 template <class TI, class Op>
-__device__ __forceinline__ void raw_vec_row(const Img& in, const Img& out, const Op& op) {
+__device__ __forceinline__ void raw_vec_row(const Img& in, const Img& out, const Op& op, int y) {
     constexpr int N = 32 / (int)sizeof(TI);
-    const int y = blockIdx.y;
     const int x0 = (blockIdx.x * kPtThreads + threadIdx.x) * N;
     if (x0 >= in.w) return;
     const TI* s = px<const TI>(in, x0, y);
@@ -62,7 +61,7 @@ __device__ __forceinline__ void raw_vec_row(const Img& in, const Img& out, const
 }
 template <class TI, class Op>
 __global__ void __launch_bounds__(kPtThreads) raw_vec_kernel(Img in, Img out, Op op) {
-    raw_vec_row<TI>(in, out, op);
+    raw_vec_row<TI>(in, out, op, (int)blockIdx.y);
 }
 
 struct R16ToF32 {
@@ -82,20 +81,59 @@ struct LinearizeShared {
     int last;
     __device__ float operator()(uint16_t v, int, int) const { return (float)table[v < last ? v : last]; }
 };
+// Each block covers rows blockIdx.y, blockIdx.y + gridDim.y, ... so that the
+// table is copied once per block, not once per row.
+constexpr int kLinRowBlocks = 148 * 8;
 __global__ void __launch_bounds__(kPtThreads) linearize_smem_kernel(Img in, Img out, const uint16_t* table, int n) {
     extern __shared__ __align__(16) uint16_t s_tab[];
     for (int i = threadIdx.x; i < n; i += kPtThreads) s_tab[i] = __ldg(table + i);
     __syncthreads();
-    raw_vec_row<uint16_t>(in, out, LinearizeShared{s_tab, n - 1});
+    const LinearizeShared op{s_tab, n - 1};
+    for (int y = blockIdx.y; y < in.h; y += gridDim.y) raw_vec_row<uint16_t>(in, out, op, y);
 }
 struct Blacklevel {
     BlackDev p;
     __device__ float operator()(float v, int x, int y) const { return blacklevel_px(v, x, y, p); }
 };
+// hrow[m][r * hw + x] = gain_hrow(m, r, x) for every map, grid row and column.
+__global__ void __launch_bounds__(kPtThreads) gainmap_hrows_kernel(GainMapDev g) {
+    const int m = blockIdx.z, r = blockIdx.y;
+    const int x = blockIdx.x * kPtThreads + threadIdx.x;
+    if (m >= g.map_count || r >= g.points_v[m] || x >= g.hw) return;
+    const_cast<float*>(g.hrow[m])[(size_t)r * g.hw + x] = gain_hrow(m, r, x, g);
+}
+
+// One map for every plane (the common case): 8 consecutive pixels per thread
+// with 16-byte loads of the pixels and of both grid-row tables, and 16-byte
+// stores; whole, unit-strided, aligned segments only (others per pixel).
+constexpr int kGmPx = 8;
+__global__ void __launch_bounds__(kPtThreads) gainmap_one_map_kernel(Img in, Img out, GainMapDev g) {
+    const int y = blockIdx.y;
+    const int x0 = (blockIdx.x * kPtThreads + threadIdx.x) * kGmPx;
+    if (x0 >= in.w) return;
+    const AxisSample sy = g.rows[0][y];
+    const float* hl = g.hrow[0] + (size_t)sy.low * g.hw + x0;
+    const float* hh = g.hrow[0] + (size_t)sy.high * g.hw + x0;
+    const float* s = px<const float>(in, x0, y);
+    float* d = px<float>(out, x0, y);
+    if (x0 + kGmPx <= in.w && in.pix_stride == 1 && out.pix_stride == 1 && al16(s) && al16(d) && al16(hl) && al16(hh)) {
+#pragma unroll
+        for (int i = 0; i < kGmPx / 4; ++i) {
+            const float4 v = __ldcs(reinterpret_cast<const float4*>(s) + i);
+            const float4 a = __ldg(reinterpret_cast<const float4*>(hl) + i), b = __ldg(reinterpret_cast<const float4*>(hh) + i);
+            __stcs(reinterpret_cast<float4*>(d) + i,
+                   make_float4(v.x * lerpf(a.x, b.x, sy.weight), v.y * lerpf(a.y, b.y, sy.weight),
+                               v.z * lerpf(a.z, b.z, sy.weight), v.w * lerpf(a.w, b.w, sy.weight)));
+        }
+        return;
+    }
+    for (int i = 0; i < kGmPx && x0 + i < in.w; ++i)
+        *px<float>(out, x0 + i, y) = *px<const float>(in, x0 + i, y) * lerpf(__ldg(hl + i), __ldg(hh + i), sy.weight);
+}
+
 // GainMap: lanes take interleaved pixels (x0 + lane + 32 j) so that a warp's
 // per-column axis samples (12 bytes each) and its pixels are read as
-// contiguous runs; 8 pixels per thread.
-constexpr int kGmPx = 8;
+// contiguous runs; 8 pixels per thread (maps per plane).
 __global__ void __launch_bounds__(kPtThreads) gainmap_kernel(Img in, Img out, GainMapDev g) {
     const int y = blockIdx.y;
     const int lane = threadIdx.x & 31;
@@ -360,7 +398,7 @@ struct GuidedGeom {
     static constexpr size_t bytes() { return sizeof(float) * (size_t)(3 * IP * IH + 2 * 3 * AP * AH); }
 };
 template <class T, bool F16, int R>
-__global__ void __launch_bounds__(256) guided_kernel(Img in, Img out, float eps) {
+__global__ void __launch_bounds__(256, 3) guided_kernel(Img in, Img out, float eps) {
     using G = GuidedGeom<R>;
     constexpr int H = G::H, D = G::D, IW = G::IW, IH = G::IH, IP = G::IP, AW = G::AW, AH = G::AH, AP = G::AP;
     extern __shared__ __align__(16) float smem_f[];
@@ -396,18 +434,19 @@ __global__ void __launch_bounds__(256) guided_kernel(Img in, Img out, float eps)
         const int g = rem / AW, tx = rem - g * AW;
         const int ty0 = g * kGfG;
         const float* V = s_v + c * IP * IH + ty0 * IP + tx;  // window origin of a/b sample (ty0, tx)
-        float win[kGfG + 2 * R][D], sq[kGfG + 2 * R][D];
+        float2 win[kGfG + 2 * R][D];  // (value, value^2)
 #pragma unroll
         for (int r = 0; r < kGfG + 2 * R; ++r)
 #pragma unroll
             for (int dx = 0; dx < D; ++dx) {
-                win[r][dx] = (ty0 + r < IH) ? V[r * IP + dx] : 0.0F;
-                sq[r][dx] = win[r][dx] * win[r][dx];
+                const float t = (ty0 + r < IH) ? V[r * IP + dx] : 0.0F;
+                win[r][dx] = make_float2(t, t * t);
             }
 #pragma unroll
         for (int k = 0; k < kGfG; ++k) {
             if (ty0 + k >= AH) break;
-            const float m = box_chain<D>(win, k) / N, corr = box_chain<D>(sq, k) / N;
+            const float2 sums = box_chain2<D>(win, k);
+            const float m = sums.x / N, corr = sums.y / N;
             const float var = max0(corr - (m * m));
             const float a = var / (var + eps);
             const int j = c * AP * AH + (ty0 + k) * AP + tx;
@@ -423,31 +462,18 @@ __global__ void __launch_bounds__(256) guided_kernel(Img in, Img out, float eps)
         float o[3][kGfG];
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
-            float sa[kGfG], sb[kGfG];
-            {
-                float win[kGfG + 2 * R][D];
-                const float* A = s_a + c * AP * AH + ty0 * AP + tx;
+            float2 win[kGfG + 2 * R][D];  // (a, b)
+            const float* A = s_a + c * AP * AH + ty0 * AP + tx;
+            const float* B = s_b + c * AP * AH + ty0 * AP + tx;
 #pragma unroll
-                for (int r = 0; r < kGfG + 2 * R; ++r)
+            for (int r = 0; r < kGfG + 2 * R; ++r)
 #pragma unroll
-                    for (int dx = 0; dx < D; ++dx) win[r][dx] = A[r * AP + dx];
-#pragma unroll
-                for (int k = 0; k < kGfG; ++k) sa[k] = box_chain<D>(win, k);
-            }
-            {
-                float win[kGfG + 2 * R][D];
-                const float* B = s_b + c * AP * AH + ty0 * AP + tx;
-#pragma unroll
-                for (int r = 0; r < kGfG + 2 * R; ++r)
-#pragma unroll
-                    for (int dx = 0; dx < D; ++dx) win[r][dx] = B[r * AP + dx];
-#pragma unroll
-                for (int k = 0; k < kGfG; ++k) sb[k] = box_chain<D>(win, k);
-            }
+                for (int dx = 0; dx < D; ++dx) win[r][dx] = make_float2(A[r * AP + dx], B[r * AP + dx]);
 #pragma unroll
             for (int k = 0; k < kGfG; ++k) {
+                const float2 sab = box_chain2<D>(win, k);
                 const float v = s_v[c * IP * IH + (ty0 + k + H) * IP + (tx + H)];
-                o[c][k] = max0(((sa[k] / N) * v) + (sb[k] / N));
+                o[c][k] = max0(((sab.x / N) * v) + (sab.y / N));
             }
         }
         const int x = x0 + tx;
@@ -567,7 +593,8 @@ cudaError_t launch_r16u_to_f32(const Img& in, const Img& out, cudaStream_t st) {
 }
 cudaError_t launch_linearize(const Img& in, const Img& out, const uint16_t* d_table, int n, cudaStream_t st) {
     if (n > 0 && n <= kLinSmemMax)
-        linearize_smem_kernel<<<row_grid(in.w, in.h, 16), kPtThreads, (size_t)n * sizeof(uint16_t), st>>>(in, out, d_table, n);
+        linearize_smem_kernel<<<dim3(row_grid(in.w, in.h, 16).x, (unsigned)(in.h < kLinRowBlocks ? in.h : kLinRowBlocks)),
+                                kPtThreads, (size_t)n * sizeof(uint16_t), st>>>(in, out, d_table, n);
     else
         raw_vec_kernel<uint16_t><<<row_grid(in.w, in.h, 16), kPtThreads, 0, st>>>(in, out, Linearize{d_table, n - 1});
     return cudaGetLastError();
@@ -576,7 +603,29 @@ cudaError_t launch_blacklevel(const Img& in, const Img& out, const BlackDev& p, 
     raw_vec_kernel<float><<<row_grid(in.w, in.h, 8), kPtThreads, 0, st>>>(in, out, Blacklevel{p});
     return cudaGetLastError();
 }
+size_t gainmap_hrows_bytes(const GainMapDev& g, int w) {
+    size_t n = 0;
+    for (int m = 0; m < g.map_count; ++m) n += (((size_t)g.points_v[m] * w * sizeof(float)) + 15) & ~size_t(15);
+    return n;
+}
+cudaError_t launch_gainmap_hrows(GainMapDev* g, void* d_hrows, int w, cudaStream_t st) {
+    char* p = static_cast<char*>(d_hrows);
+    int pv = 1;
+    for (int m = 0; m < g->map_count; ++m) {
+        g->hrow[m] = reinterpret_cast<const float*>(p);
+        p += (((size_t)g->points_v[m] * w * sizeof(float)) + 15) & ~size_t(15);
+        pv = g->points_v[m] > pv ? g->points_v[m] : pv;
+    }
+    g->hw = w;
+    const dim3 grid((unsigned)((w + kPtThreads - 1) / kPtThreads), (unsigned)pv, (unsigned)g->map_count);
+    gainmap_hrows_kernel<<<grid, kPtThreads, 0, st>>>(*g);
+    return cudaGetLastError();
+}
 cudaError_t launch_gainmap(const Img& in, const Img& out, const GainMapDev& g, cudaStream_t st) {
+    if (g.map_count == 1) {
+        gainmap_one_map_kernel<<<row_grid(in.w, in.h, kGmPx), kPtThreads, 0, st>>>(in, out, g);
+        return cudaGetLastError();
+    }
     gainmap_kernel<<<row_grid(in.w, in.h, kGmPx), kPtThreads, 0, st>>>(in, out, g);
     return cudaGetLastError();
 }
@@ -659,9 +708,15 @@ cudaError_t launch_wavelet(const Img& in, const Img& out, bool f16, float streng
 }
 template <class T, bool F16, int R>
 cudaError_t guided_launch(const Img& in, const Img& out, float eps, cudaStream_t st) {
-    static const cudaError_t attr = cudaFuncSetAttribute(guided_kernel<T, F16, R>,
-                                                         cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                                         (int)GuidedGeom<R>::bytes());
+    // the whole carveout as shared memory, so that 3 blocks fit per SM
+    static const cudaError_t attr = [] {
+        cudaError_t e = cudaFuncSetAttribute(guided_kernel<T, F16, R>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)GuidedGeom<R>::bytes());
+        if (e == cudaSuccess)
+            e = cudaFuncSetAttribute(guided_kernel<T, F16, R>, cudaFuncAttributePreferredSharedMemoryCarveout,
+                                     (int)cudaSharedmemCarveoutMaxShared);
+        return e;
+    }();
     if (attr != cudaSuccess) return attr;
     const dim3 g((unsigned)((in.w + kGfTW - 1) / kGfTW), (unsigned)((in.h + kGfTH - 1) / kGfTH));
     guided_kernel<T, F16, R><<<g, 256, GuidedGeom<R>::bytes(), st>>>(in, out, eps);

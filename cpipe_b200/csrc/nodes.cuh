@@ -32,9 +32,13 @@ struct GainMapDev {
     int qbc;                   // 4x4 CFA repeat: plane from (y%4)/2, (x%4)/2
     int plane_to_map[4];       // -1 when no map covers that plane
     const float* gains[4];     // per map, row-major map_points_v x map_points_h
-    int points_h[4];
+    int points_h[4], points_v[4];
     const AxisSample* cols[4]; // per map, w entries
     const AxisSample* rows[4]; // per map, h entries
+    // per map, points_v x hw: the horizontal interpolation of each grid row at
+    // every image column (gainmap_hrows_kernel), shared by all image rows
+    const float* hrow[4];
+    int hw;
 };
 __device__ __forceinline__ float lerpf(float a, float b, float t) { return a + ((b - a) * t); }
 __device__ __forceinline__ int gain_map_index(int x, int y, const GainMapDev& g) {
@@ -43,14 +47,20 @@ __device__ __forceinline__ int gain_map_index(int x, int y, const GainMapDev& g)
     if (g.qbc) plane = (((y % 4) / 2) * 2) + ((x % 4) / 2);
     return g.plane_to_map[plane];
 }
+// The reference's bilinear gain (shading_gainmap_dispatch.cpp:38-72):
+// lerp(lerp(g00, g10, wx), lerp(g01, g11, wx), wy).  The inner lerps depend
+// on the grid row and the column only, so they are evaluated once per (grid
+// row, column) into hrow (gain_hrow, same operands and order) and the pixel
+// reads the two it needs.
+__device__ __forceinline__ float gain_hrow(int m, int r, int x, const GainMapDev& g) {
+    const AxisSample sx = g.cols[m][x];
+    const float* gm = g.gains[m] + r * g.points_h[m];
+    return lerpf(__ldg(gm + sx.low), __ldg(gm + sx.high), sx.weight);
+}
 __device__ __forceinline__ float gain_px(int m, int x, int y, const GainMapDev& g) {
     const AxisSample sy = g.rows[m][y];
-    const AxisSample sx = g.cols[m][x];
-    const float* gm = g.gains[m];
-    const int rs = g.points_h[m];
-    const float g00 = __ldg(gm + sy.low * rs + sx.low), g10 = __ldg(gm + sy.low * rs + sx.high);
-    const float g01 = __ldg(gm + sy.high * rs + sx.low), g11 = __ldg(gm + sy.high * rs + sx.high);
-    return lerpf(lerpf(g00, g10, sx.weight), lerpf(g01, g11, sx.weight), sy.weight);
+    const float* h = g.hrow[m];
+    return lerpf(__ldg(h + (size_t)sy.low * g.hw + x), __ldg(h + (size_t)sy.high * g.hw + x), sy.weight);
 }
 
 // ----------------------------------------------------------------- demosaic
@@ -382,6 +392,18 @@ __device__ __forceinline__ float box_chain(const float (&win)[ROWS][D], int k) {
 #pragma unroll
         for (int dx = 0; dx < D; ++dx)
             if (dy != 0 || dx != 0) s = s + win[k + dy][dx];
+    return s;
+}
+// Two box sums in the same order at once, one per float2 component, with the
+// sm_100 packed add (each component rounds exactly as __fadd_rn).
+template <int D, int ROWS>
+__device__ __forceinline__ float2 box_chain2(const float2 (&win)[ROWS][D], int k) {
+    float2 s = win[k][0];
+#pragma unroll
+    for (int dy = 0; dy < D; ++dy)
+#pragma unroll
+        for (int dx = 0; dx < D; ++dx)
+            if (dy != 0 || dx != 0) s = __fadd2_rn(s, win[k + dy][dx]);
     return s;
 }
 

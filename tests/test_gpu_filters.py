@@ -222,3 +222,31 @@ def test_device_buffers_in_place(cuda_device, host):
     assert st == 0
     assert _abi.lib().cpipe_cuda_synchronize() == 0
     assert_f16_parity(dst.download(), oracle.guided(x.astype(np.float32), 8, 1e-3, True), what="device guided")
+
+
+def test_prepared_table_cache(cuda_device):
+    """Linearize, GainMap and LUT tables are cached per (blob bytes, frame
+    extent): alternating blobs, more distinct blobs than the cache holds (so
+    entries are evicted), the same GainMap blob at two frame sizes and a trim
+    in between must all give each blob's own result."""
+    r = np.random.default_rng(70)
+    lib = _abi.lib()
+    raw = r.integers(0, 4096, size=(37, 53), dtype=np.uint16)
+    tables = [np.sort(r.integers(0, 65535, size=4096)).astype(np.uint16) for _ in range(11)]
+    for rep in range(2):
+        for i in (0, 1, 0) + tuple(range(11)) + (3,):
+            out = run("linearize_dng_lut", [raw], [np.zeros(raw.shape, np.float32)], blobs.linearize(tables[i]))
+            np.testing.assert_array_equal(out, oracle.linearize(raw, tables[i])[1])
+        assert lib.cpipe_cuda_trim_scratch() == 0
+    gm = blobs.gainmap_dispatch([dict(points_v=5, points_h=7, spacing_v=9.0, spacing_h=11.0,
+                                      gains=r.uniform(1.0, 1.8, 35))])
+    for h, w in ((40, 64), (33, 90), (40, 64)):
+        x = bayer(71, h, w)
+        out = run("lens_shading_gainmap", [x], [np.zeros_like(x)], gm)
+        np.testing.assert_array_equal(out, oracle.gainmap(x, gm)[1])
+    S = 9
+    x = rgba(72, 21, 19, -0.1, 1.1)
+    luts = [r.uniform(0.0, 1.0, size=(S, S, S, 3)).astype(np.float32) for _ in range(3)]
+    for i in (0, 1, 2, 1, 0):
+        out = run("color_3d_lut", [x], [np.zeros_like(x)], blobs.lut3d(S, luts[i], 0))
+        assert_f16_parity(out, oracle.lut3d(x.astype(np.float32), luts[i], S, 0, True), what=f"lut {i}")
