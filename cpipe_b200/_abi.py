@@ -118,6 +118,19 @@ class FilmicRgbParams(C.Structure):
     _fields_ = [(n, C.c_float) for n in ("ev", "contrast", "saturation", "highlights", "shadows")]
 
 
+class EdgeAwareUsmParams(C.Structure):
+    """cpipe_EdgeAwareUsmParams (aot_id sharpen_edge_aware_usm)."""
+    _fields_ = [("strength", C.c_float), ("radius", C.c_int32), ("threshold", C.c_float)]
+
+
+class DisplayParams(C.Structure):
+    """cpipe_DisplayParams (aot_id cpipe_scene_linear_to_display): target 0 sRGB, 1 BT2020-PQ."""
+    _fields_ = [("target", C.c_uint32)]
+
+
+DISPLAY_SRGB, DISPLAY_BT2020_PQ = 0, 1
+
+
 class ChainConfig(C.Structure):
     _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("black", BlacklevelParams),
                 ("gainmap_blob", C.c_void_p), ("gainmap_blob_size", C.c_size_t), ("demosaic", C.c_int32),
@@ -162,7 +175,8 @@ EXPORTS = [
     "cpipe_cuda_denoise_guided_filter_spec", "cpipe_cuda_denoise_wavelet_atrous_spec",
     "cpipe_cuda_denoise_guided_filter",
     "cpipe_cuda_denoise_wavelet_bayes_shrink", "cpipe_cuda_lens_dng_opcode_list_3", "cpipe_cuda_color_3d_lut",
-    "cpipe_cuda_tone_filmic_rgb", "cpipe_cuda_copy", "cpipe_cuda_filters", "cpipe_cuda_find_filter",
+    "cpipe_cuda_tone_filmic_rgb", "cpipe_cuda_sharpen_edge_aware_usm", "cpipe_cuda_scene_linear_to_display",
+    "cpipe_cuda_copy", "cpipe_cuda_filters", "cpipe_cuda_find_filter",
     "cpipe_cuda_color_3d_lut_noalloc",
     "cpipe_b200_node_descs", "cpipe_b200_find_node",
     "cpipe_cuda_scene_raw", "cpipe_cuda_scene_raw_cfa", "cpipe_surrogate_blob_size", "cpipe_surrogate_create", "cpipe_surrogate_destroy", "cpipe_surrogate_export",

@@ -79,6 +79,16 @@ def filmic(ev=0.0, contrast=1.0, saturation=1.0, highlights=1.0, shadows=1.0):
     return raw(A.FilmicRgbParams(ev, contrast, saturation, highlights, shadows))
 
 
+def usm(strength=0.75, radius=1, threshold=0.0):
+    """cpipe_EdgeAwareUsmParams for sharpen_edge_aware_usm."""
+    return raw(A.EdgeAwareUsmParams(float(strength), int(radius), float(threshold)))
+
+
+def display(target="sRGB"):
+    """cpipe_DisplayParams for cpipe_scene_linear_to_display ("sRGB" or "BT2020-PQ")."""
+    return raw(A.DisplayParams({"sRGB": A.DISPLAY_SRGB, "BT2020-PQ": A.DISPLAY_BT2020_PQ}[target]))
+
+
 def linearize(table):
     t = np.ascontiguousarray(table, dtype=np.uint16)
     return struct.pack("<I", t.size) + t.tobytes()

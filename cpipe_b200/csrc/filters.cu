@@ -843,6 +843,45 @@ int cpipe_cuda_tone_filmic_rgb(halide_buffer_t* const* inputs, size_t n_in, hali
     return call.finish(cuda_status(launch_filmic(in.img, out.img, in.elem == 2, f, call.stream), "filmic"));
 }
 
+// --------------------------------------------------- sharpen.edge_aware_usm
+// edge_aware_usm_dispatch.cpp:18-31 (blob EdgeAwareUsmParams, 12 bytes).
+int cpipe_cuda_sharpen_edge_aware_usm(halide_buffer_t* const* inputs, size_t n_in, halide_buffer_t* const* outputs,
+                                      size_t n_out, const void* blob, size_t blob_size) {
+    CHECK_ARITY(1, 1);
+    if (blob == nullptr || blob_size < sizeof(cpipe_EdgeAwareUsmParams)) return CPIPE_BAD_INDEX;
+    if (!device_ready()) return CPIPE_INTERNAL_ERROR;
+    Call call;
+    Bound in, out;
+    const int st = rgba_pair(call, inputs, outputs, &in, &out);
+    if (st != CPIPE_OK) return call.finish(st);
+    cpipe_EdgeAwareUsmParams p;
+    std::memcpy(&p, blob, sizeof(p));
+    return call.finish(cuda_status(
+        launch_usm(in.img, out.img, in.elem == 2, p.strength, p.radius, p.threshold, call.stream), "usm"));
+}
+
+// -------------------------------------------- color.scene_linear_to_display
+// RGBA16F in; RGBA8 unorm out (sRGB) or RGBA16 unorm (BT2020-PQ, 10-bit codes
+// in the top bits), as the reference's write_ocio_output (HostContext.cpp:155-185).
+int cpipe_cuda_scene_linear_to_display(halide_buffer_t* const* inputs, size_t n_in, halide_buffer_t* const* outputs,
+                                       size_t n_out, const void* blob, size_t blob_size) {
+    CHECK_ARITY(1, 1);
+    if (blob == nullptr || blob_size < sizeof(cpipe_DisplayParams)) return CPIPE_BAD_INDEX;
+    cpipe_DisplayParams p;
+    std::memcpy(&p, blob, sizeof(p));
+    if (p.target != CPIPE_DISPLAY_SRGB && p.target != CPIPE_DISPLAY_BT2020_PQ) {
+        set_error("scene_linear_to_display: %s", "target must be 0 (sRGB) or 1 (BT2020-PQ)");
+        return CPIPE_UNSUPPORTED;
+    }
+    if (!device_ready()) return CPIPE_INTERNAL_ERROR;
+    Call call;
+    BIND(0, inputs, Kind::Rgba, false, in);
+    if (in.elem != 2) return call.finish(CPIPE_BAD_PRECISION);
+    BIND(0, outputs, p.target == CPIPE_DISPLAY_SRGB ? Kind::RgbaU8 : Kind::RgbaU16, true, out);
+    REQUIRE_SAME_EXTENT(in, out);
+    return call.finish(cuda_status(launch_display(in.img, out.img, p.target, call.stream), "display"));
+}
+
 // ------------------------------------------------------------ a14 OpcodeList3
 // dng_opcode_list_3_dispatch.cpp:254-398.  Records run in order, each from the
 // previous result; two device scratch images ping-pong between them.
@@ -1051,6 +1090,8 @@ static const cpipe_cuda_filter_desc kFilters[] = {
     {"lens_dng_opcode_list_3", (void*)&cpipe_cuda_lens_dng_opcode_list_3, 1},
     {"color_3d_lut", (void*)&cpipe_cuda_color_3d_lut, 1},
     {"tone_filmic_rgb", (void*)&cpipe_cuda_tone_filmic_rgb, 1},
+    {"sharpen_edge_aware_usm", (void*)&cpipe_cuda_sharpen_edge_aware_usm, 1},
+    {"cpipe_scene_linear_to_display", (void*)&cpipe_cuda_scene_linear_to_display, 1},
     {"cpipe_copy", (void*)&cpipe_cuda_copy, 1},
 };
 

@@ -32,6 +32,9 @@ cudaError_t launch_rgba16f_to_unorm(const Img& in, const Img& out, int bits8, cu
 cudaError_t launch_wb(const Img& in, const Img& out, bool f16, const float n[3], cudaStream_t st);
 cudaError_t launch_colormatrix(const Img& in, const Img& out, bool f16, const float t[9], cudaStream_t st);
 cudaError_t launch_filmic(const Img& in, const Img& out, bool f16, const FilmicDev& p, cudaStream_t st);
+cudaError_t launch_usm(const Img& in, const Img& out, bool f16, float strength, int radius, float threshold,
+                       cudaStream_t st);
+cudaError_t launch_display(const Img& in, const Img& out, unsigned target, cudaStream_t st);
 cudaError_t launch_lut3d(const Img& in, const Img& out, bool f16, const float4* d_lut, int S, int interp,
                          cudaStream_t st);
 cudaError_t launch_bm3d_parity(const Img& in, const Img& out, bool f16, float sigma, cudaStream_t st);

@@ -4,8 +4,10 @@
 // are HBM-bandwidth kernels: coalesced vector loads along rows, grids sized to
 // the image (at 12 MP every launch covers >= 148 SMs many times over), and
 // shared-memory halo tiles for the stencil nodes.
+#include <cmath>
 #include <type_traits>
 
+#include "../../include/cpipe_b200_params.h"
 #include "demosaic.cuh"
 #include "kernels.h"
 #include "nodes.cuh"
@@ -487,6 +489,190 @@ __global__ void __launch_bounds__(256, 3) guided_kernel(Img in, Img out, float e
     }
 }
 
+// ------------------------------------------------- sharpen.edge_aware_usm
+// edge_aware_usm_generator.cpp:11-75: blur = mean3x3 (R = 1: the explicit
+// 9-term left-associated sum, :11-17) or mean5x5 (R = 2: 0 + the 25 terms in
+// row-major order, :19-27) of the clamped input; mask = v - blur;
+// RGB = max(0, |mask| >= threshold ? v + strength * mask : v); alpha = v.
+// Tile 64 x TH with halo R in shared memory (three planes); a thread loads one
+// (G + 2R) x D window per channel into registers and produces the G
+// vertically adjacent outputs of one column (64x16 tiles, G = 4; a 64x32 tile
+// with G = 8 measured no faster: the kernel is issue-bound by the exact-order
+// sums and the IEEE division per channel).
+constexpr int kUsmTW = 64, kUsmTH = 16, kUsmG = 4;
+template <int D, int ROWS>
+__device__ __forceinline__ float usm_box(const float (&win)[ROWS][D], int k) {
+    float s = D == 3 ? win[k][0] : 0.0F + win[k][0];
+#pragma unroll
+    for (int dy = 0; dy < D; ++dy)
+#pragma unroll
+        for (int dx = 0; dx < D; ++dx)
+            if (dy != 0 || dx != 0) s = s + win[k + dy][dx];
+    return s;
+}
+template <class T, int R, int TH, int G>
+__global__ void __launch_bounds__(256) usm_kernel(Img in, Img out, float strength, float threshold) {
+    static_assert(kUsmTW * TH == 256 * G, "one column of G rows per thread");
+    constexpr int D = 2 * R + 1, IW = kUsmTW + 2 * R, IH = TH + 2 * R, IP = IW + 1;
+    __shared__ float s_v[3][IH * IP];
+    const int x0 = blockIdx.x * kUsmTW, y0 = blockIdx.y * TH;
+    constexpr int kLoads = (IH * IW + 255) / 256;  // issued together (256-thread blocks)
+    Rgba v[kLoads];
+#pragma unroll
+    for (int k = 0; k < kLoads; ++k) {
+        const int i = threadIdx.x + 256 * k;
+        const int ty = i / IW, tx = i - ty * IW;
+        if (i < IH * IW) v[k] = load_clamped<T>(in, x0 - R + tx, y0 - R + ty);
+    }
+#pragma unroll
+    for (int k = 0; k < kLoads; ++k) {
+        const int i = threadIdx.x + 256 * k;
+        const int ty = i / IW, tx = i - ty * IW;
+        if (i < IH * IW) {
+            s_v[0][ty * IP + tx] = v[k].r;
+            s_v[1][ty * IP + tx] = v[k].g;
+            s_v[2][ty * IP + tx] = v[k].b;
+        }
+    }
+    __syncthreads();
+    const int tx = threadIdx.x & (kUsmTW - 1), ty0 = (threadIdx.x / kUsmTW) * G;
+    constexpr float N = (float)(D * D);
+    float o[3][G];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        float win[G + 2 * R][D];
+        const float* V = s_v[c] + ty0 * IP + tx;
+#pragma unroll
+        for (int r = 0; r < G + 2 * R; ++r)
+#pragma unroll
+            for (int dx = 0; dx < D; ++dx) win[r][dx] = V[r * IP + dx];
+#pragma unroll
+        for (int k = 0; k < G; ++k) {
+            const float blur = usm_box<D>(win, k) / N;
+            const float val = win[k + R][R];
+            const float mask = val - blur;
+            const float sh = fabsf(mask) >= threshold ? val + (strength * mask) : val;
+            o[c][k] = max0(sh);
+        }
+    }
+    const int x = x0 + tx;
+#pragma unroll
+    for (int k = 0; k < G; ++k) {
+        const int y = y0 + ty0 + k;
+        if (x >= out.w || y >= out.h) continue;
+        const Rgba src = load_rgba(px<const T>(in, x, y));
+        store_rgba(px<T>(out, x, y), Rgba{o[0][k], o[1][k], o[2][k], src.a});
+    }
+}
+
+// -------------------------------------------- color.scene_linear_to_display
+// The reference node runs the OCIO processor of its config
+// (share/cpipe/ocio/v0.2/config.ocio:57-79) on the host.  Restated from
+// OpenColorIO's published transform definitions:
+//  sRGB  : MatrixTransform (Rec.2020 -> Rec.709 primaries) on RGB, then the
+//          inverse ExponentWithLinearTransform (gamma 2.4, offset 0.055:
+//          e = L <= Lb ? L / slope : 1.055 L^(1/2.4) - 0.055), then
+//          RangeTransform [0, 1] (a clamp); alpha untouched.
+//  PQ    : RangeTransform [0, 1], then FixedFunction LIN_TO_PQ (SMPTE ST 2084,
+//          linear 1.0 = 100 cd/m^2); alpha untouched.
+// Quantisation as HostContext.cpp:91-99: round-half-away(clamp(v, 0, 1) * 255)
+// for R8G8B8A8_UNORM, and round(clamp(v, 0, 1) * 1023) << 6 for the 10-bit
+// R16G16B16A16_UNORM output.  Each thread converts 4 pixels of a row.
+struct DisplayDev {
+    float m[9];
+    float lin_break, inv_slope;  // moncurve: linear breakpoint, 1 / slope
+};
+// x^e for x > 0 as exp2(e log2 x) with the PTX approximate base-2 log and exp
+// (lg2.approx / ex2.approx, documented errors of order 2^-22): relative error
+// below 1e-5 even after PQ's exponent of 78.8, far under the half code value
+// (2e-3 of the range at 8 bits, 5e-4 at 10) that decides the output code.
+__device__ __forceinline__ float pow_pos(float x, float e) {
+    float l, r;
+    asm("lg2.approx.ftz.f32 %0, %1;" : "=f"(l) : "f"(x));
+    asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(e * l));
+    return r;
+}
+__device__ __forceinline__ float srgb_encode(float l, const DisplayDev& d) {
+    return l <= d.lin_break ? l * d.inv_slope : (1.055F * pow_pos(l, 1.0F / 2.4F)) - 0.055F;
+}
+__device__ __forceinline__ float pq_encode(float v) {
+    constexpr float m1 = 2610.0F / 16384.0F, m2 = 2523.0F / 4096.0F * 128.0F;
+    constexpr float c2 = 2413.0F / 4096.0F * 32.0F, c3 = 2392.0F / 4096.0F * 32.0F, c1 = c3 - c2 + 1.0F;
+    const float l = clampf(v, 0.0F, 1.0F) * 0.01F;
+    const float y = l > 0.0F ? pow_pos(l, m1) : 0.0F;
+    return pow_pos(__fdividef(c1 + (c2 * y), 1.0F + (c3 * y)), m2);
+}
+__device__ __forceinline__ float unorm_round(float v, float scale) { return roundf(clampf(v, 0.0F, 1.0F) * scale); }
+template <unsigned TARGET>
+__device__ __forceinline__ void display_px(Rgba v, const DisplayDev& d, float o[4]) {
+    if (TARGET == CPIPE_DISPLAY_SRGB) {
+        const float r = ((d.m[0] * v.r) + (d.m[1] * v.g)) + (d.m[2] * v.b);
+        const float g = ((d.m[3] * v.r) + (d.m[4] * v.g)) + (d.m[5] * v.b);
+        const float b = ((d.m[6] * v.r) + (d.m[7] * v.g)) + (d.m[8] * v.b);
+        o[0] = unorm_round(srgb_encode(r, d), 255.0F);
+        o[1] = unorm_round(srgb_encode(g, d), 255.0F);
+        o[2] = unorm_round(srgb_encode(b, d), 255.0F);
+        o[3] = unorm_round(v.a, 255.0F);
+    } else {
+        o[0] = unorm_round(pq_encode(v.r), 1023.0F);
+        o[1] = unorm_round(pq_encode(v.g), 1023.0F);
+        o[2] = unorm_round(pq_encode(v.b), 1023.0F);
+        o[3] = unorm_round(v.a, 1023.0F);
+    }
+}
+template <unsigned TARGET>
+__device__ __forceinline__ void display_store(const Img& out, int x, int y, const float o[4]) {
+    if (TARGET == CPIPE_DISPLAY_SRGB)
+        *reinterpret_cast<uchar4*>(px<uint8_t>(out, x, y)) =
+            make_uchar4((unsigned char)o[0], (unsigned char)o[1], (unsigned char)o[2], (unsigned char)o[3]);
+    else
+        *reinterpret_cast<ushort4*>(px<uint16_t>(out, x, y)) =
+            make_ushort4((unsigned short)((unsigned)o[0] << 6), (unsigned short)((unsigned)o[1] << 6),
+                          (unsigned short)((unsigned)o[2] << 6), (unsigned short)((unsigned)o[3] << 6));
+}
+template <unsigned TARGET>
+__global__ void __launch_bounds__(kPtThreads) display_kernel(Img in, Img out, DisplayDev d) {
+    const int y = blockIdx.y;
+    const int x0 = (blockIdx.x * kPtThreads + threadIdx.x) * 4;
+    if (x0 >= in.w) return;
+    const __half* s = px<const __half>(in, x0, y);
+    const bool whole = x0 + 4 <= in.w && in.pix_stride == 4 && out.pix_stride == 4 && al16(s) &&
+                       (TARGET == CPIPE_DISPLAY_SRGB ? al16(px<uint8_t>(out, x0, y)) : al16(px<uint16_t>(out, x0, y)));
+    if (!whole) {
+        for (int i = 0; i < 4 && x0 + i < in.w; ++i) {
+            float o[4];
+            display_px<TARGET>(load_rgba(px<const __half>(in, x0 + i, y)), d, o);
+            display_store<TARGET>(out, x0 + i, y, o);
+        }
+        return;
+    }
+    alignas(16) __half v[16];
+#pragma unroll
+    for (int i = 0; i < 2; ++i) reinterpret_cast<uint4*>(v)[i] = __ldcs(reinterpret_cast<const uint4*>(s) + i);
+    float o[4][4];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) display_px<TARGET>(load_rgba(v + 4 * i), d, o[i]);
+    if (TARGET == CPIPE_DISPLAY_SRGB) {
+        uint4 q;
+        uint32_t* w = reinterpret_cast<uint32_t*>(&q);
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+            w[i] = (uint32_t)o[i][0] | ((uint32_t)o[i][1] << 8) | ((uint32_t)o[i][2] << 16) | ((uint32_t)o[i][3] << 24);
+        __stcs(reinterpret_cast<uint4*>(px<uint8_t>(out, x0, y)), q);
+    } else {
+        uint4 q[2];
+        uint32_t* w = reinterpret_cast<uint32_t*>(q);
+#pragma unroll
+        for (int i = 0; i < 4; ++i) {
+            w[2 * i] = ((uint32_t)o[i][0] << 6) | ((uint32_t)o[i][1] << 22);
+            w[2 * i + 1] = ((uint32_t)o[i][2] << 6) | ((uint32_t)o[i][3] << 22);
+        }
+        uint4* dq = reinterpret_cast<uint4*>(px<uint16_t>(out, x0, y));
+        __stcs(dq, q[0]);
+        __stcs(dq + 1, q[1]);
+    }
+}
+
 // --------------------------------------------------------------- OpcodeList3
 template <class T, bool F16>
 __global__ void __launch_bounds__(128) warp_kernel(Img in, Img out, WarpDev w) {
@@ -725,6 +911,35 @@ cudaError_t guided_launch(const Img& in, const Img& out, float eps, cudaStream_t
 cudaError_t launch_guided(const Img& in, const Img& out, bool f16, int radius, float eps, cudaStream_t st) {
     if (radius <= 1) return f16 ? guided_launch<__half, true, 1>(in, out, eps, st) : guided_launch<float, false, 1>(in, out, eps, st);
     return f16 ? guided_launch<__half, true, 2>(in, out, eps, st) : guided_launch<float, false, 2>(in, out, eps, st);
+}
+cudaError_t launch_usm(const Img& in, const Img& out, bool f16, float strength, int radius, float threshold,
+                       cudaStream_t st) {
+    const dim3 g((unsigned)((in.w + kUsmTW - 1) / kUsmTW), (unsigned)((in.h + kUsmTH - 1) / kUsmTH));
+    if (radius <= 1) {
+        RGBA_DISPATCH(f16, (usm_kernel<__half, 1, kUsmTH, kUsmG><<<g, 256, 0, st>>>(in, out, strength, threshold)),
+                      (usm_kernel<float, 1, kUsmTH, kUsmG><<<g, 256, 0, st>>>(in, out, strength, threshold)));
+    } else {
+        RGBA_DISPATCH(f16, (usm_kernel<__half, 2, kUsmTH, kUsmG><<<g, 256, 0, st>>>(in, out, strength, threshold)),
+                      (usm_kernel<float, 2, kUsmTH, kUsmG><<<g, 256, 0, st>>>(in, out, strength, threshold)));
+    }
+    return cudaGetLastError();
+}
+cudaError_t launch_display(const Img& in, const Img& out, unsigned target, cudaStream_t st) {
+    // Rec.2020 -> Rec.709 matrix of the config's output_srgb colour space
+    static const float kM[9] = {1.6604910F, -0.5876411F, -0.0728499F, -0.1245505F, 1.1328999F,
+                                -0.0083494F, -0.0181508F, -0.1005789F, 1.1187297F};
+    DisplayDev d;
+    for (int i = 0; i < 9; ++i) d.m[i] = kM[i];
+    // moncurve with gamma g, offset o: encoded breakpoint eb = o / (g - 1), linear
+    // breakpoint Lb = (o g / ((g - 1)(1 + o)))^g, slope = Lb / eb (continuous)
+    const double gm = 2.4, off = 0.055;
+    const double eb = off / (gm - 1.0), lb = std::pow(off * gm / ((gm - 1.0) * (1.0 + off)), gm);
+    d.lin_break = (float)lb;
+    d.inv_slope = (float)(eb / lb);
+    const dim3 g = row_grid(in.w, in.h, 4);
+    if (target == CPIPE_DISPLAY_SRGB) display_kernel<CPIPE_DISPLAY_SRGB><<<g, kPtThreads, 0, st>>>(in, out, d);
+    else display_kernel<CPIPE_DISPLAY_BT2020_PQ><<<g, kPtThreads, 0, st>>>(in, out, d);
+    return cudaGetLastError();
 }
 cudaError_t launch_warp(const Img& in, const Img& out, bool f16, const WarpDev& w, cudaStream_t st) {
     const dim3 g((unsigned)((out.w + 127) / 128), (unsigned)out.h);

@@ -12,6 +12,7 @@
 // "process" -> run, "destroy" -> free.  No C++ exception crosses main_entry.
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -476,6 +477,77 @@ int node_filmic(Ctx& c) {
     return c.step("tone.filmic_rgb");
 }
 
+// sharpen/edge_aware_usm.cpp:29-50: parameters clamped as the reference node
+// does; the filter checks the buffers.
+int node_usm(Ctx& c) {
+    const cpipe_EdgeAwareUsmParams p{c.clamped_float("strength", 0.75F, 0.0F, 2.0F), c.clamped_int("radius", 1, 1, 32),
+                                     c.clamped_float("threshold", 0.0F, 0.0F, 0.1F)};
+    const int st = c.submit("sharpen_edge_aware_usm", &p, sizeof(p));
+    if (st != CPIPE_OK) return st;
+    return c.step("sharpen.edge_aware_usm");
+}
+
+// color/scene_linear_to_display.cpp:31-127: target -> output format and role,
+// buffer / metadata checks with the reference's codes, then the encode.  The
+// encode goes to this library's CUDA filter; a host that does not route
+// "cpipe_scene_linear_to_display" (CPIPE_UNSUPPORTED) gets the reference's own
+// path, its OCIO processor through the host suites.
+int node_display(Ctx& c) {
+    std::string target;
+    if (!c.get_string("target", &target)) return CPIPE_NEED_PARAM;
+    uint32_t code = 0;
+    int want = 0;
+    const char* dst = nullptr;
+    if (target == "sRGB") {
+        code = CPIPE_DISPLAY_SRGB;
+        want = CPIPE_FMT_R8G8B8A8_UNORM;
+        dst = "output_srgb";
+    } else if (target == "BT2020-PQ") {
+        code = CPIPE_DISPLAY_BT2020_PQ;
+        want = CPIPE_FMT_R16G16B16A16_UNORM;
+        dst = "output_pq_rec2020";
+    } else if (target == "DisplayP3" || target == "BT2020-HLG") {
+        c.msg = "display target reserved for v1.1";
+        return CPIPE_UNSUPPORTED;
+    } else {
+        c.msg = "unknown display target";
+        return CPIPE_NEED_PARAM;
+    }
+    int a = 0, b = 0;
+    int st = c.format(c.in(0), &a);
+    if (st == CPIPE_OK) st = c.format(c.out(0), &b);
+    if (st != CPIPE_OK) return st;
+    if (a != CPIPE_FMT_R16G16B16A16_SFLOAT || b != want) {
+        c.msg = "scene_linear_to_display format mismatch";
+        return CPIPE_BAD_PRECISION;
+    }
+    uint32_t w0, h0, w1, h1;
+    if ((st = c.dims(c.in(0), &w0, &h0)) != CPIPE_OK || (st = c.dims(c.out(0), &w1, &h1)) != CPIPE_OK) return st;
+    if (w0 != w1 || h0 != h1) return CPIPE_BAD_INDEX;
+    const cpipe_metadata_t* m = c.metadata(c.in(0));
+    const char* role = nullptr;
+    if (!m || c.meta->get_cs_role(m, &role) != CPIPE_OK || !role || std::strcmp(role, "scene_linear_rec2020") != 0) {
+        c.msg = "scene_linear_to_display needs Rec2020 scene linear";
+        return CPIPE_NEED_METADATA;
+    }
+    const cpipe_DisplayParams p{code};
+    st = c.submit("cpipe_scene_linear_to_display", &p, sizeof(p));
+    if (st == CPIPE_UNSUPPORTED) {
+        const char* env = std::getenv("CPIPE_OCIO_CONFIG");
+        const char* config = env && env[0] ? env : "share/cpipe/ocio/v0.2/config.ocio";
+        cpipe_ocio_processor_t* proc =
+            c.host->get_ocio_processor ? c.host->get_ocio_processor(c.host, config, "scene_linear_rec2020", dst) : nullptr;
+        if (proc == nullptr || c.compute->submit_ocio_processor == nullptr) {
+            c.msg = "scene_linear_to_display OCIO processor unavailable";
+            return CPIPE_FAILED;
+        }
+        st = c.compute->submit_ocio_processor(c.pc->compute, proc, c.in(0), c.out(0));
+    }
+    if (st != CPIPE_OK) return st;
+    if ((st = c.mb->set_cs_role(c.builder(), dst)) != CPIPE_OK) return st;
+    return c.step("color.scene_linear_to_display");
+}
+
 // ------------------------------------------------------------- dispatching
 using NodeFn = int (*)(Ctx&);
 
@@ -597,6 +669,17 @@ const char kFilmic[] = MANIFEST("com.cpipe.tone.filmic_rgb", "Filmic RGB Tone", 
     NUM("highlights", "0", "2", "1") "," NUM("shadows", "0", "2", "1"),
     "scene_linear_rec2020", "scene_linear_rec2020", "true", "\"rgba_point<filmic>\"");
 
+const char kUsm[] = MANIFEST("com.cpipe.sharpen.edge_aware_usm", "Edge-aware USM", "sharpen",
+    PORT("rgb", "in", "\"rgba\"", "\"f16\",\"f32\"", "\"requires_steps_applied\":[\"color.3d_lut\"]"),
+    PORT("rgb", "out", "\"rgba\"", "\"f16\",\"f32\"", "\"inherits_from\":\"rgb\",\"sets_steps_applied\":[\"sharpen.edge_aware_usm\"]"),
+    NUM("strength", "0", "2", "0.75") "," NUM("radius", "1", "32", "1") "," NUM("threshold", "0", "0.1", "0"),
+    "scene_linear_rec2020", "scene_linear_rec2020", "true", "\"usm_kernel\"");
+const char kDisplay[] = MANIFEST("com.cpipe.color.scene_linear_to_display", "Scene Linear to Display", "color",
+    PORT("rgb", "in", "\"rgba\"", "\"f16\"", ""),
+    PORT("display", "out", "\"rgba\"", "\"u8\",\"u16\"", "\"inherits_from\":\"rgb\",\"sets_steps_applied\":[\"color.scene_linear_to_display\"]"),
+    "{\"name\":\"target\",\"type\":\"enum\",\"enum_values\":[\"sRGB\",\"BT2020-PQ\",\"DisplayP3\",\"BT2020-HLG\"],\"default\":\"sRGB\"}",
+    "scene_linear_rec2020", "any", "true", "\"display_kernel\"");
+
 }  // namespace
 
 // Descriptors in the reference registry section (section.hpp:7, registry.hpp:24-31).
@@ -620,6 +703,8 @@ CPIPE_B200_REGISTER(cpipe_b200_desc_wavelet, "com.cpipe.denoise.wavelet_bayes_sh
 CPIPE_B200_REGISTER(cpipe_b200_desc_opcode3, "com.cpipe.lens.dng_opcode_list_3", kOpcode3, node_opcode3)
 CPIPE_B200_REGISTER(cpipe_b200_desc_lut, "com.cpipe.color.3d_lut", kLut, node_lut3d)
 CPIPE_B200_REGISTER(cpipe_b200_desc_filmic, "com.cpipe.tone.filmic_rgb", kFilmic, node_filmic)
+CPIPE_B200_REGISTER(cpipe_b200_desc_usm, "com.cpipe.sharpen.edge_aware_usm", kUsm, node_usm)
+CPIPE_B200_REGISTER(cpipe_b200_desc_display, "com.cpipe.color.scene_linear_to_display", kDisplay, node_display)
 
 extern "C" {
 extern const cpipe_plugin_desc_t __start_cpipe_registry[];

@@ -39,7 +39,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 # "issue" -- the reference's per-pixel arithmetic (RCD/AMaZE ratios, the QBC
 # 25-tap integer weights, the guided filter's exact-order box sums, the warp's
 # float-float coordinates and bicubic taps, filmic's log per channel) sets the
-# floor; "gather" -- 3D LUT cell reads through L1/L2.
+# floor (the PQ encode: two powf per channel); "gather" -- 3D LUT cell reads
+# through L1/L2.
 NODES = [
     ("a1 precision_convert", "precision_convert_r16u_to_f32", "u16", "f32", 6, None, "hbm"),
     ("a2 linearize", "linearize_dng_lut", "u16", "f32", 6, "linearize", "hbm"),
@@ -57,6 +58,9 @@ NODES = [
     ("a14 OpcodeList3 warp", "lens_dng_opcode_list_3", "rgba", "rgba", 16, "opcode3", "issue"),
     ("a15 3D LUT", "color_3d_lut", "rgba", "rgba", 16, "lut", "gather"),
     ("a16 filmic", "tone_filmic_rgb", "rgba", "rgba", 16, "filmic", "issue"),
+    ("sharpen.edge_aware_usm (3x3)", "sharpen_edge_aware_usm", "rgba", "rgba", 16, "usm", "hbm"),
+    ("scene_linear_to_display sRGB", "cpipe_scene_linear_to_display", "rgba", "rgba8", 12, "display_srgb", "hbm"),
+    ("scene_linear_to_display PQ", "cpipe_scene_linear_to_display", "rgba", "rgba16u", 16, "display_pq", "issue"),
 ]
 
 
@@ -75,6 +79,8 @@ def node_roofline(width=4032, height=3024, reps=10, peak_gbs=None):
     cfg = ChainConfig.full_12mp(width=width, height=height)
     b = cfg.blobs()
     b["linearize"] = B.linearize(np.arange(1 << cfg.bits, dtype=np.uint16))
+    b["usm"] = B.usm()
+    b["display_srgb"], b["display_pq"] = B.display("sRGB"), B.display("BT2020-PQ")
     raw = cfg.make_raw()
     frames = {"u16": raw, "f32raw": raw.astype(np.float32),
               "f32": np.clip((raw.astype(np.float32) - cfg.black) / (cfg.white - cfg.black), 0.0, 1.0),
@@ -88,7 +94,8 @@ def node_roofline(width=4032, height=3024, reps=10, peak_gbs=None):
         keep.append(p)
     outs = {}
     for kind, (shape, dtype) in {"f32": ((height, width), np.float32), "u16": ((height, width), np.uint16),
-                                 "rgba": ((height, width, 4), np.float16)}.items():
+                                 "rgba": ((height, width, 4), np.float16), "rgba8": ((height, width, 4), np.uint8),
+                                 "rgba16u": ((height, width, 4), np.uint16)}.items():
         p = C.c_void_p()
         assert L.cpipe_cuda_device_alloc(int(np.prod(shape)) * np.dtype(dtype).itemsize, C.byref(p)) == 0
         outs[kind] = DeviceImage(p.value, shape, dtype)

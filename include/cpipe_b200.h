@@ -100,6 +100,15 @@ CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_denoise_wavelet_atrous_spec);
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_lens_dng_opcode_list_3);     /* dng_opcode_list_3_dispatch.cpp:333-398 */
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_color_3d_lut);               /* lut3d_dispatch.cpp:20-60 */
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_tone_filmic_rgb);            /* filmic_rgb_dispatch.cpp:22-36 */
+CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_sharpen_edge_aware_usm);     /* edge_aware_usm_dispatch.cpp:18-31 */
+/* Scene-linear Rec.2020 to display encode (aot_id "cpipe_scene_linear_to_display",
+ * blob cpipe_DisplayParams; RGBA16F in, RGBA8 unorm out for sRGB, RGBA16
+ * unorm with 10-bit codes in the top bits for BT2020-PQ).  Replaces the OCIO
+ * CPU processor the reference node runs through its host
+ * (scene_linear_to_display.cpp:114-121, HostContext.cpp:956-983, the
+ * transforms of share/cpipe/ocio/v0.2/config.ocio); no reference filter
+ * counterpart. */
+CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_scene_linear_to_display);
 /* Device copy for pass-through cases (aot_id "cpipe_copy"); replaces the lock_cpu
  * memcpy of e.g. shading_gainmap.cpp:50-75.  No reference filter counterpart. */
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_copy);

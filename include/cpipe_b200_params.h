@@ -170,6 +170,22 @@ typedef struct {
     float shadows;
 } cpipe_FilmicRgbParams;
 
+/* sharpen.edge_aware_usm (nodes/sharpen/edge_aware_usm_dispatch.cpp:12-16). */
+typedef struct {
+    float strength;    /* 0..2 (node default 0.75) */
+    int32_t radius;    /* <= 1: 3x3 mean, else 5x5 mean */
+    float threshold;   /* |v - blur| below this leaves v unchanged */
+} cpipe_EdgeAwareUsmParams;
+
+/* color.scene_linear_to_display (nodes/color/scene_linear_to_display.cpp:31-50):
+ * target 0 = "sRGB" (R8G8B8A8_UNORM output), 1 = "BT2020-PQ"
+ * (R16G16B16A16_UNORM output, 10-bit codes in the top bits). */
+typedef struct {
+    uint32_t target;
+} cpipe_DisplayParams;
+#define CPIPE_DISPLAY_SRGB 0U
+#define CPIPE_DISPLAY_BT2020_PQ 1U
+
 /* Two-stage colour BM3D ("spec mode"; aot_id denoise_bm3d_spec).  The
  * reference's denoise.bm3d node computes a 2x2 box blend
  * (nodes/denoise/bm3d_step1_generator.cpp:33-61); this is the published
@@ -227,6 +243,8 @@ CPIPE_STATIC_ASSERT(sizeof(cpipe_Lut3dParamHeader) == 12, "Lut3dParamHeader layo
 CPIPE_STATIC_ASSERT(sizeof(cpipe_Bm3dSpecParams) == 40, "Bm3dSpecParams layout");
 CPIPE_STATIC_ASSERT(sizeof(cpipe_SurrogateHeader) == 32, "SurrogateHeader layout");
 CPIPE_STATIC_ASSERT(sizeof(cpipe_AtrousWaveletParams) == 16, "AtrousWaveletParams layout");
+CPIPE_STATIC_ASSERT(sizeof(cpipe_EdgeAwareUsmParams) == 12, "EdgeAwareUsmParams layout");
+CPIPE_STATIC_ASSERT(sizeof(cpipe_DisplayParams) == 4, "DisplayParams layout");
 
 #ifdef __cplusplus
 } /* extern "C" */

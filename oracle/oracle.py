@@ -188,6 +188,14 @@ def guided(x, radius, eps, f16=True):
     return out
 
 
+def usm(x, strength=0.75, radius=1, threshold=0.0, f16=True):
+    x = _f32(x)
+    out = np.empty_like(x)
+    lib().oracle_usm(_p(x), _p(out), x.shape[1], x.shape[0], C.c_float(strength), int(radius), C.c_float(threshold),
+                     int(f16))
+    return out
+
+
 def wavelet(x, strength, f16=True):
     x = _f32(x)
     out = np.empty_like(x)

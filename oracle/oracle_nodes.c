@@ -290,6 +290,48 @@ static inline float rs(const rgba_t* im, int x, int y, int c) {
     return im->p[4 * ((long)clampi(y, 0, im->h - 1) * im->w + clampi(x, 0, im->w - 1)) + c];
 }
 
+/* ---- sharpen.edge_aware_usm (src/cpipe/nodes/sharpen/edge_aware_usm_generator.cpp:11-75) ----
+ * blur = mean3x3 (radius <= 1, explicit 9-term left-associated sum) or mean5x5
+ * (0 + the 25 terms in row-major order), both over the clamped input;
+ * mask = v - blur; RGB = max(0, |mask| >= threshold ? v + strength * mask : v);
+ * alpha = v. */
+void oracle_usm(const float* in, float* out, int w, int h, float strength, int radius, float threshold, int f16) {
+    rgba_t I = {in, w, h};
+#pragma omp parallel for schedule(static)
+    for (int y = 0; y < h; ++y) {
+        for (int x = 0; x < w; ++x) {
+            for (int c = 0; c < 4; ++c) {
+                const float v = rs(&I, x, y, c);
+                float o = v;
+                if (c != 3) {
+                    float blur;
+                    if (radius <= 1) {
+                        float s = rs(&I, x - 1, y - 1, c);
+                        s = s + rs(&I, x, y - 1, c);
+                        s = s + rs(&I, x + 1, y - 1, c);
+                        s = s + rs(&I, x - 1, y, c);
+                        s = s + rs(&I, x, y, c);
+                        s = s + rs(&I, x + 1, y, c);
+                        s = s + rs(&I, x - 1, y + 1, c);
+                        s = s + rs(&I, x, y + 1, c);
+                        s = s + rs(&I, x + 1, y + 1, c);
+                        blur = s / 9.0F;
+                    } else {
+                        float s = 0.0F;
+                        for (int dy = -2; dy <= 2; ++dy)
+                            for (int dx = -2; dx <= 2; ++dx) s += rs(&I, x + dx, y + dy, c);
+                        blur = s / 25.0F;
+                    }
+                    const float mask = v - blur;
+                    const float sh = fabsf(mask) >= threshold ? v + (strength * mask) : v;
+                    o = maxf(0.0F, sh);
+                }
+                out[4 * ((long)y * w + x) + c] = rnd(o, f16);
+            }
+        }
+    }
+}
+
 /* ---- a9: white balance pixel op (wb/wb_dual_illuminant_dispatch.cpp:16-48) ---- */
 void oracle_wb(const float* in, float* out, int w, int h, const cpipe_WbParams* p, int f16) {
     for (long i = 0; i < (long)w * h; ++i) {

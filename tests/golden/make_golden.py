@@ -24,7 +24,7 @@ FIXTURES = [
     "linearize.dng_lut", "blacklevel.dng_levels", "lens.shading_gainmap", "demosaic.bilinear",
     "demosaic.rcd", "demosaic.amaze", "demosaic.quad_bayer_remosaic", "lens.dng_opcode_list_3",
     "wb.dual_illuminant", "colormatrix.dng_to_working", "denoise.bm3d", "denoise.guided_filter",
-    "denoise.wavelet_bayes_shrink", "tone.filmic_rgb", "color.3d_lut",
+    "denoise.wavelet_bayes_shrink", "tone.filmic_rgb", "color.3d_lut", "sharpen.edge_aware_usm",
 ]
 
 
