@@ -142,7 +142,9 @@ class ChainConfig(C.Structure):
                 ("bm3d_spec", Bm3dSpecParams), ("surrogate_blob", C.c_void_p), ("surrogate_blob_size", C.c_size_t),
                 ("noise_a", C.c_float), ("noise_b", C.c_float), ("stop_after", C.c_int32),
                 ("spot_tiles", C.c_int32), ("spot_min_psnr_db", C.c_float), ("quad_bayer", C.c_int32),
-                ("guided_spec", C.c_int32), ("atrous_levels", C.c_int32), ("atrous_luma_strength", C.c_float)]
+                ("guided_spec", C.c_int32), ("atrous_levels", C.c_int32), ("atrous_luma_strength", C.c_float),
+                ("sharpen", C.c_int32), ("sharpen_strength", C.c_float), ("sharpen_radius", C.c_int32),
+                ("sharpen_threshold", C.c_float), ("display", C.c_int32)]
 
 
 MAIN_ENTRY = C.CFUNCTYPE(C.c_int, C.c_char_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p)

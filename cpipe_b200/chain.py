@@ -91,6 +91,13 @@ class ChainConfig:
     guided_spec: bool = False      # guided filter with the true (2r+1)^2 box (radius 1..16)
     atrous_levels: int = 0         # > 0: a-trous wavelet denoiser with that many levels instead of the 2x2 Haar
     atrous_luma_strength: float = 1.0
+    # finishing stages after the LUT (the reference's example pipeline continues
+    # with them): sharpen.edge_aware_usm, then the display encode
+    sharpen: bool = False
+    sharpen_strength: float = 0.75
+    sharpen_radius: int = 1
+    sharpen_threshold: float = 0.0
+    display: str = ""              # "" (RGBA16F output) | "sRGB" (RGBA8) | "BT2020-PQ" (RGBA16 unorm)
 
     # ------------------------------------------------------------ workloads
     @classmethod
@@ -249,6 +256,11 @@ class ChainConfig:
         cfg.guided_spec = int(self.guided_spec)
         cfg.atrous_levels = int(self.atrous_levels)
         cfg.atrous_luma_strength = float(self.atrous_luma_strength)
+        cfg.sharpen = int(self.sharpen)
+        cfg.sharpen_strength = float(self.sharpen_strength)
+        cfg.sharpen_radius = int(self.sharpen_radius)
+        cfg.sharpen_threshold = float(self.sharpen_threshold)
+        cfg.display = {"": 0, "sRGB": 1, "BT2020-PQ": 2}[self.display]
         return cfg, keep
 
 
@@ -263,7 +275,8 @@ class Chain:
         del keep  # the library copies what it keeps
         if not self._h:
             raise CpipeError(st.value, "chain_create " + A.lib().cpipe_cuda_last_error().decode())
-        self.out_dtype = np.float32 if config.plain_f32 else np.float16
+        self.out_dtype = {"sRGB": np.uint8, "BT2020-PQ": np.uint16}.get(
+            config.display, np.float32 if config.plain_f32 else np.float16)
         self.out_shape = (config.height, config.width, 4)
 
     def close(self):

@@ -402,6 +402,9 @@ struct cpipe_cuda_chain {
     void* d_tile_scratch = nullptr;
     float* d_tile_mse = nullptr;          // per-tile partial sums of squared differences
     int* d_gate = nullptr;                // 1: fall back to BM3D for this frame
+    // finishing stages after denoise_tone: sharpen.edge_aware_usm, display encode
+    bool sharpen = false;
+    unsigned display = 0;  // 0 none, 1 sRGB, 2 BT2020-PQ
     // spec-mode stages between the denoiser and denoise_tone (0: none)
     bool spec_stages = false;
     bool guided_spec = false;
@@ -466,7 +469,8 @@ int launch_chain(cpipe_cuda_chain* c, const void* d_raw, size_t raw_pitch, void*
     }
     const Img mid0{c->d_mid[0], w, h, (long long)w * 4, 4};
     const Img mid1{c->d_mid[1], w, h, (long long)w * 4, 4};
-    const Img out{d_out, w, h, (long long)(out_pitch ? out_pitch / elem : (size_t)w * 4), 4};
+    const int out_elem = c->display == 1 ? 1 : (c->display == 2 ? 2 : elem);
+    const Img out{d_out, w, h, (long long)(out_pitch ? out_pitch / out_elem : (size_t)w * 4), 4};
     const dim3 ga((unsigned)((w + kDmTW - 1) / kDmTW), (unsigned)((h + kDmTH - 1) / kDmTH));
 #define K1(A)                                                                                        \
     if (c->f16) raw_to_rgba_kernel<A, __half><<<ga, 256, 0, st>>>(raw, mid0, c->raw);                \
@@ -573,15 +577,30 @@ int launch_chain(cpipe_cuda_chain* c, const void* d_raw, size_t raw_pitch, void*
         k2_out = x;
     }
     if (ev) cudaEventRecord(ev[3], st);
+    // with finishing stages the tone kernel writes a scratch frame they read
+    const bool finish = c->sharpen || c->display != 0;
+    const Img k3_out = !finish ? out : (k2_out.data == mid0.data ? mid1 : mid0);
     const dim3 gc((unsigned)((w + kCTW - 1) / kCTW), (unsigned)((h + kCTH - 1) / kCTH));
 #define K3(TT, F, R)                                                                                       \
-    denoise_tone_kernel<TT, F, R><<<gc, 256, denoise_tone_smem<TT, F, R>(), st>>>(k2_out, out, c->tone);
+    denoise_tone_kernel<TT, F, R><<<gc, 256, denoise_tone_smem<TT, F, R>(), st>>>(k2_out, k3_out, c->tone);
     if (c->f16) {
         if (c->radius == 0) { K3(__half, true, 0) } else if (c->radius == 1) { K3(__half, true, 1) } else { K3(__half, true, 2) }
     } else {
         if (c->radius == 0) { K3(float, false, 0) } else if (c->radius == 1) { K3(float, false, 1) } else { K3(float, false, 2) }
     }
 #undef K3
+    if (finish) {
+        const cpipe_cuda_chain_config& f = c->cfg;
+        cudaError_t e;
+        if (c->sharpen && c->display)
+            e = launch_usm_display(k3_out, out, f.sharpen_strength, f.sharpen_radius, f.sharpen_threshold,
+                                   c->display - 1, st);
+        else if (c->sharpen)
+            e = launch_usm(k3_out, out, true, f.sharpen_strength, f.sharpen_radius, f.sharpen_threshold, st);
+        else
+            e = launch_display(k3_out, out, c->display - 1, st);
+        if (e != cudaSuccess) return cuda_status(e, "chain finishing stages");
+    }
     if (ev) cudaEventRecord(ev[4], st);
     return cuda_status(cudaGetLastError(), "chain launch");
 }
@@ -765,8 +784,21 @@ cpipe_cuda_chain* cpipe_cuda_chain_create(const cpipe_cuda_chain_config* cfg, in
     c->tone.filmic = cpb_filmic_dev(&cfg->filmic);
     // scratch frames
     c->frame_bytes = (size_t)w * h * 4 * (c->f16 ? 2 : 4);
+    // finishing stages (sharpen.edge_aware_usm, display encode): f16 form, whole chain
+    if (cfg->sharpen || cfg->display) {
+        if (cfg->display < 0 || cfg->display > 2 || cfg->stop_after != 0) return fail(CPIPE_BAD_INDEX, c);
+        if (!c->f16) return fail(CPIPE_BAD_PRECISION, c);
+        c->sharpen = cfg->sharpen != 0;
+        c->display = (unsigned)cfg->display;
+        // the node's parameter clamps (edge_aware_usm.cpp:38-41)
+        c->cfg.sharpen_strength = std::clamp(cfg->sharpen_strength, 0.0F, 2.0F);
+        c->cfg.sharpen_radius = std::clamp(cfg->sharpen_radius, 1, 32);
+        c->cfg.sharpen_threshold = std::clamp(cfg->sharpen_threshold, 0.0F, 0.1F);
+        if (c->display) c->frame_bytes = (size_t)w * h * 4 * (c->display == 1 ? 1 : 2);
+    }
+    const size_t mid_bytes = (size_t)w * h * 4 * (c->f16 ? 2 : 4);  // RGBA working frames
     for (void*& p : c->d_mid)
-        if (cudaMalloc(&p, c->frame_bytes) != cudaSuccess) return fail(CPIPE_OOM, c);
+        if (cudaMalloc(&p, mid_bytes) != cudaSuccess) return fail(CPIPE_OOM, c);
     cudaError_t e = cudaSuccess;
     if (c->f16) e = c->radius == 0 ? allow_smem<__half, true, 0>() : c->radius == 1 ? allow_smem<__half, true, 1>() : allow_smem<__half, true, 2>();
     else e = c->radius == 0 ? allow_smem<float, false, 0>() : c->radius == 1 ? allow_smem<float, false, 1>() : allow_smem<float, false, 2>();
@@ -1238,7 +1270,8 @@ cpipe_cuda_batch* cpipe_cuda_batch_create(const cpipe_cuda_chain_config* cfgs, s
     std::vector<int> prefix(3 * (n + 1), 0);
     for (size_t i = 0; i < n; ++i) {
         cpipe_cuda_chain_config c = cfgs[i];
-        if (c.plain_f32 || c.denoise_mode != 0 || c.stop_after != 0 || c.guided_spec || c.atrous_levels) {
+        if (c.plain_f32 || c.denoise_mode != 0 || c.stop_after != 0 || c.guided_spec || c.atrous_levels || c.sharpen ||
+            c.display) {
             set_error("batch: %s", "frames run the parity chain (binary16, the reference's denoise.bm3d)");
             return fail(CPIPE_UNSUPPORTED, b);
         }

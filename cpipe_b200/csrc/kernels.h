@@ -35,6 +35,10 @@ cudaError_t launch_filmic(const Img& in, const Img& out, bool f16, const FilmicD
 cudaError_t launch_usm(const Img& in, const Img& out, bool f16, float strength, int radius, float threshold,
                        cudaStream_t st);
 cudaError_t launch_display(const Img& in, const Img& out, unsigned target, cudaStream_t st);
+// sharpen.edge_aware_usm on an RGBA16F frame, its f16-rounded result encoded
+// for display (target CPIPE_DISPLAY_SRGB / _BT2020_PQ) in the same kernel.
+cudaError_t launch_usm_display(const Img& in, const Img& out, float strength, int radius, float threshold,
+                               unsigned target, cudaStream_t st);
 cudaError_t launch_lut3d(const Img& in, const Img& out, bool f16, const float4* d_lut, int S, int interp,
                          cudaStream_t st);
 cudaError_t launch_bm3d_parity(const Img& in, const Img& out, bool f16, float sigma, cudaStream_t st);

@@ -5,6 +5,7 @@
 // the image (at 12 MP every launch covers >= 148 SMs many times over), and
 // shared-memory halo tiles for the stencil nodes.
 #include <cmath>
+#include <cstring>
 #include <type_traits>
 
 #include "../../include/cpipe_b200_params.h"
@@ -489,82 +490,6 @@ __global__ void __launch_bounds__(256, 3) guided_kernel(Img in, Img out, float e
     }
 }
 
-// ------------------------------------------------- sharpen.edge_aware_usm
-// edge_aware_usm_generator.cpp:11-75: blur = mean3x3 (R = 1: the explicit
-// 9-term left-associated sum, :11-17) or mean5x5 (R = 2: 0 + the 25 terms in
-// row-major order, :19-27) of the clamped input; mask = v - blur;
-// RGB = max(0, |mask| >= threshold ? v + strength * mask : v); alpha = v.
-// Tile 64 x TH with halo R in shared memory (three planes); a thread loads one
-// (G + 2R) x D window per channel into registers and produces the G
-// vertically adjacent outputs of one column (64x16 tiles, G = 4; a 64x32 tile
-// with G = 8 measured no faster: the kernel is issue-bound by the exact-order
-// sums and the IEEE division per channel).
-constexpr int kUsmTW = 64, kUsmTH = 16, kUsmG = 4;
-template <int D, int ROWS>
-__device__ __forceinline__ float usm_box(const float (&win)[ROWS][D], int k) {
-    float s = D == 3 ? win[k][0] : 0.0F + win[k][0];
-#pragma unroll
-    for (int dy = 0; dy < D; ++dy)
-#pragma unroll
-        for (int dx = 0; dx < D; ++dx)
-            if (dy != 0 || dx != 0) s = s + win[k + dy][dx];
-    return s;
-}
-template <class T, int R, int TH, int G>
-__global__ void __launch_bounds__(256) usm_kernel(Img in, Img out, float strength, float threshold) {
-    static_assert(kUsmTW * TH == 256 * G, "one column of G rows per thread");
-    constexpr int D = 2 * R + 1, IW = kUsmTW + 2 * R, IH = TH + 2 * R, IP = IW + 1;
-    __shared__ float s_v[3][IH * IP];
-    const int x0 = blockIdx.x * kUsmTW, y0 = blockIdx.y * TH;
-    constexpr int kLoads = (IH * IW + 255) / 256;  // issued together (256-thread blocks)
-    Rgba v[kLoads];
-#pragma unroll
-    for (int k = 0; k < kLoads; ++k) {
-        const int i = threadIdx.x + 256 * k;
-        const int ty = i / IW, tx = i - ty * IW;
-        if (i < IH * IW) v[k] = load_clamped<T>(in, x0 - R + tx, y0 - R + ty);
-    }
-#pragma unroll
-    for (int k = 0; k < kLoads; ++k) {
-        const int i = threadIdx.x + 256 * k;
-        const int ty = i / IW, tx = i - ty * IW;
-        if (i < IH * IW) {
-            s_v[0][ty * IP + tx] = v[k].r;
-            s_v[1][ty * IP + tx] = v[k].g;
-            s_v[2][ty * IP + tx] = v[k].b;
-        }
-    }
-    __syncthreads();
-    const int tx = threadIdx.x & (kUsmTW - 1), ty0 = (threadIdx.x / kUsmTW) * G;
-    constexpr float N = (float)(D * D);
-    float o[3][G];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        float win[G + 2 * R][D];
-        const float* V = s_v[c] + ty0 * IP + tx;
-#pragma unroll
-        for (int r = 0; r < G + 2 * R; ++r)
-#pragma unroll
-            for (int dx = 0; dx < D; ++dx) win[r][dx] = V[r * IP + dx];
-#pragma unroll
-        for (int k = 0; k < G; ++k) {
-            const float blur = usm_box<D>(win, k) / N;
-            const float val = win[k + R][R];
-            const float mask = val - blur;
-            const float sh = fabsf(mask) >= threshold ? val + (strength * mask) : val;
-            o[c][k] = max0(sh);
-        }
-    }
-    const int x = x0 + tx;
-#pragma unroll
-    for (int k = 0; k < G; ++k) {
-        const int y = y0 + ty0 + k;
-        if (x >= out.w || y >= out.h) continue;
-        const Rgba src = load_rgba(px<const T>(in, x, y));
-        store_rgba(px<T>(out, x, y), Rgba{o[0][k], o[1][k], o[2][k], src.a});
-    }
-}
-
 // -------------------------------------------- color.scene_linear_to_display
 // The reference node runs the OCIO processor of its config
 // (share/cpipe/ocio/v0.2/config.ocio:57-79) on the host.  Restated from
@@ -630,6 +555,91 @@ __device__ __forceinline__ void display_store(const Img& out, int x, int y, cons
             make_ushort4((unsigned short)((unsigned)o[0] << 6), (unsigned short)((unsigned)o[1] << 6),
                           (unsigned short)((unsigned)o[2] << 6), (unsigned short)((unsigned)o[3] << 6));
 }
+// ------------------------------------------------- sharpen.edge_aware_usm
+// edge_aware_usm_generator.cpp:11-75: blur = mean3x3 (R = 1: the explicit
+// 9-term left-associated sum, :11-17) or mean5x5 (R = 2: 0 + the 25 terms in
+// row-major order, :19-27) of the clamped input; mask = v - blur;
+// RGB = max(0, |mask| >= threshold ? v + strength * mask : v); alpha = v.
+// Tile 64 x TH with halo R in shared memory (three planes); a thread loads one
+// (G + 2R) x D window per channel into registers and produces the G
+// vertically adjacent outputs of one column (64x16 tiles, G = 4; a 64x32 tile
+// with G = 8 measured no faster: the kernel is issue-bound by the exact-order
+// sums and the IEEE division per channel).
+constexpr int kUsmTW = 64, kUsmTH = 16, kUsmG = 4;
+template <int D, int ROWS>
+__device__ __forceinline__ float usm_box(const float (&win)[ROWS][D], int k) {
+    float s = D == 3 ? win[k][0] : 0.0F + win[k][0];
+#pragma unroll
+    for (int dy = 0; dy < D; ++dy)
+#pragma unroll
+        for (int dx = 0; dx < D; ++dx)
+            if (dy != 0 || dx != 0) s = s + win[k + dy][dx];
+    return s;
+}
+// DISP 0: RGBA output of the input's type; 1 / 2: the f16-rounded result is
+// display-encoded (sRGB / BT2020-PQ) into an RGBA8 / RGBA16 unorm output.
+template <class T, int R, int TH, int G, int DISP>
+__global__ void __launch_bounds__(256) usm_kernel(Img in, Img out, float strength, float threshold, DisplayDev dd) {
+    static_assert(kUsmTW * TH == 256 * G, "one column of G rows per thread");
+    constexpr int D = 2 * R + 1, IW = kUsmTW + 2 * R, IH = TH + 2 * R, IP = IW + 1;
+    __shared__ float s_v[3][IH * IP];
+    const int x0 = blockIdx.x * kUsmTW, y0 = blockIdx.y * TH;
+    constexpr int kLoads = (IH * IW + 255) / 256;  // issued together (256-thread blocks)
+    Rgba v[kLoads];
+#pragma unroll
+    for (int k = 0; k < kLoads; ++k) {
+        const int i = threadIdx.x + 256 * k;
+        const int ty = i / IW, tx = i - ty * IW;
+        if (i < IH * IW) v[k] = load_clamped<T>(in, x0 - R + tx, y0 - R + ty);
+    }
+#pragma unroll
+    for (int k = 0; k < kLoads; ++k) {
+        const int i = threadIdx.x + 256 * k;
+        const int ty = i / IW, tx = i - ty * IW;
+        if (i < IH * IW) {
+            s_v[0][ty * IP + tx] = v[k].r;
+            s_v[1][ty * IP + tx] = v[k].g;
+            s_v[2][ty * IP + tx] = v[k].b;
+        }
+    }
+    __syncthreads();
+    const int tx = threadIdx.x & (kUsmTW - 1), ty0 = (threadIdx.x / kUsmTW) * G;
+    constexpr float N = (float)(D * D);
+    float o[3][G];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        float win[G + 2 * R][D];
+        const float* V = s_v[c] + ty0 * IP + tx;
+#pragma unroll
+        for (int r = 0; r < G + 2 * R; ++r)
+#pragma unroll
+            for (int dx = 0; dx < D; ++dx) win[r][dx] = V[r * IP + dx];
+#pragma unroll
+        for (int k = 0; k < G; ++k) {
+            const float blur = usm_box<D>(win, k) / N;
+            const float val = win[k + R][R];
+            const float mask = val - blur;
+            const float sh = fabsf(mask) >= threshold ? val + (strength * mask) : val;
+            o[c][k] = max0(sh);
+        }
+    }
+    const int x = x0 + tx;
+#pragma unroll
+    for (int k = 0; k < G; ++k) {
+        const int y = y0 + ty0 + k;
+        if (x >= out.w || y >= out.h) continue;
+        const Rgba src = load_rgba(px<const T>(in, x, y));
+        if constexpr (DISP == 0) {
+            store_rgba(px<T>(out, x, y), Rgba{o[0][k], o[1][k], o[2][k], src.a});
+        } else {
+            constexpr unsigned kTarget = (unsigned)(DISP - 1);
+            float q[4];
+            display_px<kTarget>(Rgba{h16(o[0][k]), h16(o[1][k]), h16(o[2][k]), src.a}, dd, q);
+            display_store<kTarget>(out, x, y, q);
+        }
+    }
+}
+
 template <unsigned TARGET>
 __global__ void __launch_bounds__(kPtThreads) display_kernel(Img in, Img out, DisplayDev d) {
     const int y = blockIdx.y;
@@ -912,19 +922,7 @@ cudaError_t launch_guided(const Img& in, const Img& out, bool f16, int radius, f
     if (radius <= 1) return f16 ? guided_launch<__half, true, 1>(in, out, eps, st) : guided_launch<float, false, 1>(in, out, eps, st);
     return f16 ? guided_launch<__half, true, 2>(in, out, eps, st) : guided_launch<float, false, 2>(in, out, eps, st);
 }
-cudaError_t launch_usm(const Img& in, const Img& out, bool f16, float strength, int radius, float threshold,
-                       cudaStream_t st) {
-    const dim3 g((unsigned)((in.w + kUsmTW - 1) / kUsmTW), (unsigned)((in.h + kUsmTH - 1) / kUsmTH));
-    if (radius <= 1) {
-        RGBA_DISPATCH(f16, (usm_kernel<__half, 1, kUsmTH, kUsmG><<<g, 256, 0, st>>>(in, out, strength, threshold)),
-                      (usm_kernel<float, 1, kUsmTH, kUsmG><<<g, 256, 0, st>>>(in, out, strength, threshold)));
-    } else {
-        RGBA_DISPATCH(f16, (usm_kernel<__half, 2, kUsmTH, kUsmG><<<g, 256, 0, st>>>(in, out, strength, threshold)),
-                      (usm_kernel<float, 2, kUsmTH, kUsmG><<<g, 256, 0, st>>>(in, out, strength, threshold)));
-    }
-    return cudaGetLastError();
-}
-cudaError_t launch_display(const Img& in, const Img& out, unsigned target, cudaStream_t st) {
+static DisplayDev display_dev() {
     // Rec.2020 -> Rec.709 matrix of the config's output_srgb colour space
     static const float kM[9] = {1.6604910F, -0.5876411F, -0.0728499F, -0.1245505F, 1.1328999F,
                                 -0.0083494F, -0.0181508F, -0.1005789F, 1.1187297F};
@@ -936,6 +934,35 @@ cudaError_t launch_display(const Img& in, const Img& out, unsigned target, cudaS
     const double eb = off / (gm - 1.0), lb = std::pow(off * gm / ((gm - 1.0) * (1.0 + off)), gm);
     d.lin_break = (float)lb;
     d.inv_slope = (float)(eb / lb);
+    return d;
+}
+cudaError_t launch_usm(const Img& in, const Img& out, bool f16, float strength, int radius, float threshold,
+                       cudaStream_t st) {
+    const dim3 g((unsigned)((in.w + kUsmTW - 1) / kUsmTW), (unsigned)((in.h + kUsmTH - 1) / kUsmTH));
+    if (radius <= 1) {
+        RGBA_DISPATCH(f16, (usm_kernel<__half, 1, kUsmTH, kUsmG, 0><<<g, 256, 0, st>>>(in, out, strength, threshold, DisplayDev{})),
+                      (usm_kernel<float, 1, kUsmTH, kUsmG, 0><<<g, 256, 0, st>>>(in, out, strength, threshold, DisplayDev{})));
+    } else {
+        RGBA_DISPATCH(f16, (usm_kernel<__half, 2, kUsmTH, kUsmG, 0><<<g, 256, 0, st>>>(in, out, strength, threshold, DisplayDev{})),
+                      (usm_kernel<float, 2, kUsmTH, kUsmG, 0><<<g, 256, 0, st>>>(in, out, strength, threshold, DisplayDev{})));
+    }
+    return cudaGetLastError();
+}
+cudaError_t launch_usm_display(const Img& in, const Img& out, float strength, int radius, float threshold,
+                               unsigned target, cudaStream_t st) {
+    const dim3 g((unsigned)((in.w + kUsmTW - 1) / kUsmTW), (unsigned)((in.h + kUsmTH - 1) / kUsmTH));
+    const DisplayDev dd = display_dev();
+#define USMD(R, D) usm_kernel<__half, R, kUsmTH, kUsmG, D><<<g, 256, 0, st>>>(in, out, strength, threshold, dd)
+    if (target == CPIPE_DISPLAY_SRGB) {
+        if (radius <= 1) USMD(1, 1); else USMD(2, 1);
+    } else {
+        if (radius <= 1) USMD(1, 2); else USMD(2, 2);
+    }
+#undef USMD
+    return cudaGetLastError();
+}
+cudaError_t launch_display(const Img& in, const Img& out, unsigned target, cudaStream_t st) {
+    const DisplayDev d = display_dev();
     const dim3 g = row_grid(in.w, in.h, 4);
     if (target == CPIPE_DISPLAY_SRGB) display_kernel<CPIPE_DISPLAY_SRGB><<<g, kPtThreads, 0, st>>>(in, out, d);
     else display_kernel<CPIPE_DISPLAY_BT2020_PQ><<<g, kPtThreads, 0, st>>>(in, out, d);

@@ -267,6 +267,18 @@ typedef struct {
     int32_t guided_spec;
     int32_t atrous_levels;
     float atrous_luma_strength;
+    /* Finishing stages after the LUT, as the reference's example pipeline
+     * continues (sharpen, display): sharpen = 1 runs sharpen.edge_aware_usm
+     * (sharpen_strength / _radius / _threshold as that node's params);
+     * display 1 = sRGB (RGBA8 unorm output, 4 bytes per pixel), 2 = BT2020-PQ
+     * (RGBA16 unorm output, 10-bit codes in the top bits), 0 = none (RGBA16F
+     * output).  Both need the f16 form and stop_after 0; with both, one kernel
+     * sharpens and encodes. */
+    int32_t sharpen;
+    float sharpen_strength;
+    int32_t sharpen_radius;
+    float sharpen_threshold;
+    int32_t display;
 } cpipe_cuda_chain_config;
 
 typedef struct cpipe_cuda_chain cpipe_cuda_chain;

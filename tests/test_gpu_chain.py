@@ -66,6 +66,14 @@ def run_nodes_on_gpu(host, cfg, raw):
         tmp.close()
         BL.write_cube(tmp.name, 33, b["lut_values"])
         steps.append(("com.cpipe.color.3d_lut", F16, {"lut_path": tmp.name}))
+    if cfg.sharpen:
+        steps.append(("com.cpipe.sharpen.edge_aware_usm", F16, {"strength": cfg.sharpen_strength,
+                                                              "radius": cfg.sharpen_radius,
+                                                              "threshold": cfg.sharpen_threshold}))
+    if cfg.display:
+        steps.append(("com.cpipe.color.scene_linear_to_display",
+                      A.FMT_R8G8B8A8_UNORM if cfg.display == "sRGB" else A.FMT_R16G16B16A16_UNORM,
+                      {"target": cfg.display}))
     try:
         for node_id, fmt, params in steps:
             nxt = host.buffer(fmt, w, h)
@@ -288,3 +296,27 @@ def test_chain_spec_stage_refusals(cuda_device):
         Chain(ChainConfig.full_12mp(width=64, height=64, guided_spec=True, guided_radius=17))
     with pytest.raises(Exception):
         Chain(ChainConfig.full_12mp(width=64, height=64, atrous_levels=7))
+
+
+@pytest.mark.parametrize("kw", [dict(sharpen=True), dict(display="sRGB"), dict(sharpen=True, display="sRGB"),
+                                dict(sharpen=True, sharpen_radius=2, sharpen_strength=1.4, sharpen_threshold=0.01,
+                                     display="BT2020-PQ")])
+def test_chain_finishing_stages_equal_nodes(host, kw):
+    """sharpen.edge_aware_usm and the display encode as the chain's last stages
+    (one fused kernel when both run) return, bit for bit, what the two nodes
+    return after the LUT node."""
+    cfg = ChainConfig.full_12mp(width=160, height=112, **kw)
+    raw = cfg.make_raw()
+    chain = Chain(cfg)
+    got = chain.run_host(raw)
+    chain.close()
+    want = run_nodes_on_gpu(host, cfg, raw)
+    assert got.dtype == want.dtype and got.shape == want.shape
+    np.testing.assert_array_equal(got.view(np.uint8), want.view(np.uint8))
+
+
+def test_chain_finishing_stage_refusals(cuda_device):
+    with pytest.raises(Exception):
+        Chain(ChainConfig.full_12mp(width=64, height=64, display="sRGB", plain_f32=True))
+    with pytest.raises(Exception):
+        Chain(ChainConfig.full_12mp(width=64, height=64, sharpen=True, stop_after=1))
