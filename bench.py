@@ -270,6 +270,46 @@ def spec_form(peak_gbs):
     return out
 
 
+def finishing_stages():
+    """The 12 MP chain (reference computation in the BM3D slot) with the
+    finishing stages the reference's example pipeline runs after the LUT:
+    sharpen.edge_aware_usm and the display encode, fused in one kernel
+    (sRGB: RGBA8 output; BT2020-PQ: RGBA16 unorm output); CUDA events around
+    10 frames on a device-resident raw frame after 3."""
+    from cpipe_b200 import _abi as A
+    from cpipe_b200.chain import Chain, ChainConfig
+    L = A.lib()
+    e0, e1 = C.c_void_p(), C.c_void_p()
+    L.cpipe_cuda_event_create(C.byref(e0))
+    L.cpipe_cuda_event_create(C.byref(e1))
+    out = {}
+    for name, kw in (("chain_ms", {}), ("chain_sharpen_srgb_ms", dict(sharpen=True, display="sRGB")),
+                     ("chain_sharpen_pq_ms", dict(sharpen=True, display="BT2020-PQ"))):
+        cfg = ChainConfig.full_12mp(**kw)
+        raw = cfg.make_raw()
+        ch = Chain(cfg)
+        d_raw, d_out = C.c_void_p(), C.c_void_p()
+        assert L.cpipe_cuda_device_alloc(raw.nbytes, C.byref(d_raw)) == 0
+        assert L.cpipe_cuda_device_alloc(L.cpipe_cuda_chain_output_bytes(ch._h), C.byref(d_out)) == 0
+        assert L.cpipe_cuda_memcpy_h2d(d_raw, raw.ctypes.data, raw.nbytes) == 0
+        for _ in range(3):
+            ch.run(d_raw.value, d_out.value)
+        L.cpipe_cuda_event_record(e0, None)
+        for _ in range(10):
+            ch.run(d_raw.value, d_out.value)
+        L.cpipe_cuda_event_record(e1, None)
+        assert L.cpipe_cuda_synchronize() == 0
+        ms = C.c_float()
+        L.cpipe_cuda_event_elapsed_ms(e0, e1, C.byref(ms))
+        out[name] = round(ms.value / 10, 4)
+        ch.close()
+        L.cpipe_cuda_device_free(d_raw)
+        L.cpipe_cuda_device_free(d_out)
+    out["note"] = ("full 12 MP chain with the reference's denoise.bm3d computation; sharpen r=1 strength 0.75 "
+                   "fused with the display encode after the LUT")
+    return out
+
+
 def batched_form():
     """The 64-frame uneven batch (cpipe_b200.batch): aggregate MP/s of one launch
     per stage over all frames, per-frame latency alone."""
@@ -503,6 +543,7 @@ def b200_arm(args):
     if rank == 0 and world == 1 and not args.no_extra:
         line["batched_form"] = batched_form()
         line["spec_form"] = spec_form(peak_gbs)
+        line["finishing_stages"] = finishing_stages()
         line["node_roofline"] = {"peak_gbs": peak_gbs, "peak_kind": gbs_kind,
                                  "note": "each node's filter alone, 12 MP device buffers, bytes = its input and "
                                          "output once in the reference's formats",

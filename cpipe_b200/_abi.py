@@ -118,6 +118,16 @@ class FilmicRgbParams(C.Structure):
     _fields_ = [(n, C.c_float) for n in ("ev", "contrast", "saturation", "highlights", "shadows")]
 
 
+class AcesFilmicParams(C.Structure):
+    """cpipe_AcesFilmicParams (aot_id tone_aces_filmic)."""
+    _fields_ = [("enabled", C.c_int32)]
+
+
+class ReinhardParams(C.Structure):
+    """cpipe_ReinhardParams (aot_id tone_reinhard)."""
+    _fields_ = [("white_point", C.c_float)]
+
+
 class EdgeAwareUsmParams(C.Structure):
     """cpipe_EdgeAwareUsmParams (aot_id sharpen_edge_aware_usm)."""
     _fields_ = [("strength", C.c_float), ("radius", C.c_int32), ("threshold", C.c_float)]
@@ -177,7 +187,8 @@ EXPORTS = [
     "cpipe_cuda_denoise_guided_filter_spec", "cpipe_cuda_denoise_wavelet_atrous_spec",
     "cpipe_cuda_denoise_guided_filter",
     "cpipe_cuda_denoise_wavelet_bayes_shrink", "cpipe_cuda_lens_dng_opcode_list_3", "cpipe_cuda_color_3d_lut",
-    "cpipe_cuda_tone_filmic_rgb", "cpipe_cuda_sharpen_edge_aware_usm", "cpipe_cuda_scene_linear_to_display",
+    "cpipe_cuda_tone_filmic_rgb", "cpipe_cuda_tone_aces_filmic", "cpipe_cuda_tone_reinhard",
+    "cpipe_cuda_sharpen_edge_aware_usm", "cpipe_cuda_scene_linear_to_display",
     "cpipe_cuda_copy", "cpipe_cuda_filters", "cpipe_cuda_find_filter",
     "cpipe_cuda_color_3d_lut_noalloc",
     "cpipe_b200_node_descs", "cpipe_b200_find_node",

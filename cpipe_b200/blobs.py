@@ -79,6 +79,16 @@ def filmic(ev=0.0, contrast=1.0, saturation=1.0, highlights=1.0, shadows=1.0):
     return raw(A.FilmicRgbParams(ev, contrast, saturation, highlights, shadows))
 
 
+def aces(enabled=True):
+    """cpipe_AcesFilmicParams for tone_aces_filmic."""
+    return raw(A.AcesFilmicParams(1 if enabled else 0))
+
+
+def reinhard(white_point=1000000.0):
+    """cpipe_ReinhardParams for tone_reinhard (1e6: the node's value when its param is unset)."""
+    return raw(A.ReinhardParams(float(white_point)))
+
+
 def usm(strength=0.75, radius=1, threshold=0.0):
     """cpipe_EdgeAwareUsmParams for sharpen_edge_aware_usm."""
     return raw(A.EdgeAwareUsmParams(float(strength), int(radius), float(threshold)))

@@ -843,6 +843,36 @@ int cpipe_cuda_tone_filmic_rgb(halide_buffer_t* const* inputs, size_t n_in, hali
     return call.finish(cuda_status(launch_filmic(in.img, out.img, in.elem == 2, f, call.stream), "filmic"));
 }
 
+// ------------------------------------------------ tone.aces_filmic / reinhard
+// aces_filmic_dispatch.cpp:17-31, reinhard_dispatch.cpp:16-29 (4-byte blobs).
+int cpipe_cuda_tone_aces_filmic(halide_buffer_t* const* inputs, size_t n_in, halide_buffer_t* const* outputs,
+                                size_t n_out, const void* blob, size_t blob_size) {
+    CHECK_ARITY(1, 1);
+    if (blob == nullptr || blob_size < sizeof(cpipe_AcesFilmicParams)) return CPIPE_BAD_INDEX;
+    if (!device_ready()) return CPIPE_INTERNAL_ERROR;
+    Call call;
+    Bound in, out;
+    const int st = rgba_pair(call, inputs, outputs, &in, &out);
+    if (st != CPIPE_OK) return call.finish(st);
+    cpipe_AcesFilmicParams p;
+    std::memcpy(&p, blob, sizeof(p));
+    return call.finish(cuda_status(launch_aces(in.img, out.img, in.elem == 2, p.enabled, call.stream), "aces"));
+}
+int cpipe_cuda_tone_reinhard(halide_buffer_t* const* inputs, size_t n_in, halide_buffer_t* const* outputs,
+                             size_t n_out, const void* blob, size_t blob_size) {
+    CHECK_ARITY(1, 1);
+    if (blob == nullptr || blob_size < sizeof(cpipe_ReinhardParams)) return CPIPE_BAD_INDEX;
+    if (!device_ready()) return CPIPE_INTERNAL_ERROR;
+    Call call;
+    Bound in, out;
+    const int st = rgba_pair(call, inputs, outputs, &in, &out);
+    if (st != CPIPE_OK) return call.finish(st);
+    cpipe_ReinhardParams p;
+    std::memcpy(&p, blob, sizeof(p));
+    return call.finish(
+        cuda_status(launch_reinhard(in.img, out.img, in.elem == 2, p.white_point, call.stream), "reinhard"));
+}
+
 // --------------------------------------------------- sharpen.edge_aware_usm
 // edge_aware_usm_dispatch.cpp:18-31 (blob EdgeAwareUsmParams, 12 bytes).
 int cpipe_cuda_sharpen_edge_aware_usm(halide_buffer_t* const* inputs, size_t n_in, halide_buffer_t* const* outputs,
@@ -1090,6 +1120,8 @@ static const cpipe_cuda_filter_desc kFilters[] = {
     {"lens_dng_opcode_list_3", (void*)&cpipe_cuda_lens_dng_opcode_list_3, 1},
     {"color_3d_lut", (void*)&cpipe_cuda_color_3d_lut, 1},
     {"tone_filmic_rgb", (void*)&cpipe_cuda_tone_filmic_rgb, 1},
+    {"tone_aces_filmic", (void*)&cpipe_cuda_tone_aces_filmic, 1},
+    {"tone_reinhard", (void*)&cpipe_cuda_tone_reinhard, 1},
     {"sharpen_edge_aware_usm", (void*)&cpipe_cuda_sharpen_edge_aware_usm, 1},
     {"cpipe_scene_linear_to_display", (void*)&cpipe_cuda_scene_linear_to_display, 1},
     {"cpipe_copy", (void*)&cpipe_cuda_copy, 1},

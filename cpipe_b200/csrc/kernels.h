@@ -32,6 +32,8 @@ cudaError_t launch_rgba16f_to_unorm(const Img& in, const Img& out, int bits8, cu
 cudaError_t launch_wb(const Img& in, const Img& out, bool f16, const float n[3], cudaStream_t st);
 cudaError_t launch_colormatrix(const Img& in, const Img& out, bool f16, const float t[9], cudaStream_t st);
 cudaError_t launch_filmic(const Img& in, const Img& out, bool f16, const FilmicDev& p, cudaStream_t st);
+cudaError_t launch_aces(const Img& in, const Img& out, bool f16, int enabled, cudaStream_t st);
+cudaError_t launch_reinhard(const Img& in, const Img& out, bool f16, float white_point, cudaStream_t st);
 cudaError_t launch_usm(const Img& in, const Img& out, bool f16, float strength, int radius, float threshold,
                        cudaStream_t st);
 cudaError_t launch_display(const Img& in, const Img& out, unsigned target, cudaStream_t st);

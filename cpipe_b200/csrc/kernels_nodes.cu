@@ -322,6 +322,35 @@ struct LutOp {
     int S, interp;
     __device__ void operator()(const T* s, T* d) const { store_rgb_keep_alpha(d, lut_px(load_rgba(s), lut, S, interp), s); }
 };
+// tone.aces_filmic (aces_filmic_generator.cpp:22-52): the Narkowicz 2016 fit
+// per RGB channel, alpha passes; enabled == 0 passes every channel.
+__device__ __forceinline__ float aces_fit(float v) {
+    v = max0(v);
+    return clampf((v * ((2.51F * v) + 0.03F)) / ((v * ((2.43F * v) + 0.59F)) + 0.14F), 0.0F, 1.0F);
+}
+template <class T>
+struct AcesOp {
+    int enabled;
+    __device__ void operator()(const T* s, T* d) const {
+        const Rgba v = load_rgba(s);
+        const Rgba o = enabled ? Rgba{aces_fit(v.r), aces_fit(v.g), aces_fit(v.b), v.a} : v;
+        store_rgb_keep_alpha(d, o, s);
+    }
+};
+// tone.reinhard (reinhard_generator.cpp:20-48): clamp(v (1 + v / wp^2) / (1 + v), 0, 1),
+// v = max(0, x), per RGB channel; alpha passes.
+__device__ __forceinline__ float reinhard_px(float x, float wp2) {
+    const float v = max0(x);
+    return clampf((v * (1.0F + (v / wp2))) / (1.0F + v), 0.0F, 1.0F);
+}
+template <class T>
+struct ReinhardOp {
+    float wp2;
+    __device__ void operator()(const T* s, T* d) const {
+        const Rgba v = load_rgba(s);
+        store_rgb_keep_alpha(d, Rgba{reinhard_px(v.r, wp2), reinhard_px(v.g, wp2), reinhard_px(v.b, wp2), v.a}, s);
+    }
+};
 // f32 -> RGBA f16 (precision_convert_generator.cpp:48-56): grey replicated, alpha 1.
 struct F32ToRgba16f {
     __device__ void operator()(const Img& in, const Img& out, int x0, int y) const {
@@ -935,6 +964,19 @@ static DisplayDev display_dev() {
     d.lin_break = (float)lb;
     d.inv_slope = (float)(eb / lb);
     return d;
+}
+cudaError_t launch_aces(const Img& in, const Img& out, bool f16, int enabled, cudaStream_t st) {
+    const dim3 g = rgba_grid(in.w, in.h, f16);
+    RGBA_DISPATCH(f16, (rgba_point_kernel<__half><<<g, kPtThreads, 0, st>>>(in, out, AcesOp<__half>{enabled})),
+                  (rgba_point_kernel<float><<<g, kPtThreads, 0, st>>>(in, out, AcesOp<float>{enabled})));
+    return cudaGetLastError();
+}
+cudaError_t launch_reinhard(const Img& in, const Img& out, bool f16, float white_point, cudaStream_t st) {
+    const float wp2 = white_point * white_point;
+    const dim3 g = rgba_grid(in.w, in.h, f16);
+    RGBA_DISPATCH(f16, (rgba_point_kernel<__half><<<g, kPtThreads, 0, st>>>(in, out, ReinhardOp<__half>{wp2})),
+                  (rgba_point_kernel<float><<<g, kPtThreads, 0, st>>>(in, out, ReinhardOp<float>{wp2})));
+    return cudaGetLastError();
 }
 cudaError_t launch_usm(const Img& in, const Img& out, bool f16, float strength, int radius, float threshold,
                        cudaStream_t st) {

@@ -83,6 +83,12 @@ struct Ctx {
         return std::clamp((float)double_or(key, fb), lo, hi);
     }
     int clamped_int(const char* key, int fb, int lo, int hi) const { return std::clamp((int)double_or(key, fb), lo, hi); }
+    // ParamUtils.hpp:37-50: the fallback when the suite or the key is missing
+    bool bool_or(const char* key, bool fallback) const {
+        int v = 0;
+        if (!param || !param->get_bool || !props || param->get_bool(props, key, &v) != CPIPE_OK) return fallback;
+        return v != 0;
+    }
     bool get_string(const char* key, std::string* s) const {
         const char* v = nullptr;
         if (!param || !param->get_enum || !props || param->get_enum(props, key, &v) != CPIPE_OK || !v) return false;
@@ -477,6 +483,23 @@ int node_filmic(Ctx& c) {
     return c.step("tone.filmic_rgb");
 }
 
+// tone/aces_filmic.cpp:28-46
+int node_aces(Ctx& c) {
+    const cpipe_AcesFilmicParams p{c.bool_or("toggle", true) ? 1 : 0};
+    const int st = c.submit("tone_aces_filmic", &p, sizeof(p));
+    if (st != CPIPE_OK) return st;
+    return c.step("tone.aces_filmic");
+}
+
+// tone/reinhard.cpp:28-47: white_point unset (-1) -> 1e6, else clamped to 0.1..10
+int node_reinhard(Ctx& c) {
+    const float wp = (float)c.double_or("white_point", -1.0);
+    const cpipe_ReinhardParams p{wp < 0.0F ? 1000000.0F : std::clamp(wp, 0.1F, 10.0F)};
+    const int st = c.submit("tone_reinhard", &p, sizeof(p));
+    if (st != CPIPE_OK) return st;
+    return c.step("tone.reinhard");
+}
+
 // sharpen/edge_aware_usm.cpp:29-50: parameters clamped as the reference node
 // does; the filter checks the buffers.
 int node_usm(Ctx& c) {
@@ -669,6 +692,14 @@ const char kFilmic[] = MANIFEST("com.cpipe.tone.filmic_rgb", "Filmic RGB Tone", 
     NUM("highlights", "0", "2", "1") "," NUM("shadows", "0", "2", "1"),
     "scene_linear_rec2020", "scene_linear_rec2020", "true", "\"rgba_point<filmic>\"");
 
+const char kAces[] = MANIFEST("com.cpipe.tone.aces_filmic", "ACES Filmic Tone", "tone",
+    RGBA_IN("rgb", "\"requires_steps_applied\":[\"denoise.wavelet_bayes_shrink\"]"), RGBA_OUT("rgb", "tone.aces_filmic", ""),
+    "{\"name\":\"toggle\",\"type\":\"bool\",\"default\":true}",
+    "scene_linear_rec2020", "scene_linear_rec2020", "true", "\"rgba_point<aces>\"");
+const char kReinhard[] = MANIFEST("com.cpipe.tone.reinhard", "Reinhard Tone", "tone",
+    RGBA_IN("rgb", "\"requires_steps_applied\":[\"denoise.wavelet_bayes_shrink\"]"), RGBA_OUT("rgb", "tone.reinhard", ""),
+    NUM("white_point", "0.1", "10", "10"),
+    "scene_linear_rec2020", "scene_linear_rec2020", "true", "\"rgba_point<reinhard>\"");
 const char kUsm[] = MANIFEST("com.cpipe.sharpen.edge_aware_usm", "Edge-aware USM", "sharpen",
     PORT("rgb", "in", "\"rgba\"", "\"f16\",\"f32\"", "\"requires_steps_applied\":[\"color.3d_lut\"]"),
     PORT("rgb", "out", "\"rgba\"", "\"f16\",\"f32\"", "\"inherits_from\":\"rgb\",\"sets_steps_applied\":[\"sharpen.edge_aware_usm\"]"),
@@ -703,6 +734,8 @@ CPIPE_B200_REGISTER(cpipe_b200_desc_wavelet, "com.cpipe.denoise.wavelet_bayes_sh
 CPIPE_B200_REGISTER(cpipe_b200_desc_opcode3, "com.cpipe.lens.dng_opcode_list_3", kOpcode3, node_opcode3)
 CPIPE_B200_REGISTER(cpipe_b200_desc_lut, "com.cpipe.color.3d_lut", kLut, node_lut3d)
 CPIPE_B200_REGISTER(cpipe_b200_desc_filmic, "com.cpipe.tone.filmic_rgb", kFilmic, node_filmic)
+CPIPE_B200_REGISTER(cpipe_b200_desc_aces, "com.cpipe.tone.aces_filmic", kAces, node_aces)
+CPIPE_B200_REGISTER(cpipe_b200_desc_reinhard, "com.cpipe.tone.reinhard", kReinhard, node_reinhard)
 CPIPE_B200_REGISTER(cpipe_b200_desc_usm, "com.cpipe.sharpen.edge_aware_usm", kUsm, node_usm)
 CPIPE_B200_REGISTER(cpipe_b200_desc_display, "com.cpipe.color.scene_linear_to_display", kDisplay, node_display)
 

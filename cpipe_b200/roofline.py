@@ -58,6 +58,8 @@ NODES = [
     ("a14 OpcodeList3 warp", "lens_dng_opcode_list_3", "rgba", "rgba", 16, "opcode3", "issue"),
     ("a15 3D LUT", "color_3d_lut", "rgba", "rgba", 16, "lut", "gather"),
     ("a16 filmic", "tone_filmic_rgb", "rgba", "rgba", 16, "filmic", "issue"),
+    ("tone.aces_filmic", "tone_aces_filmic", "rgba", "rgba", 16, "aces", "hbm"),
+    ("tone.reinhard", "tone_reinhard", "rgba", "rgba", 16, "reinhard", "hbm"),
     ("sharpen.edge_aware_usm (3x3)", "sharpen_edge_aware_usm", "rgba", "rgba", 16, "usm", "hbm"),
     ("scene_linear_to_display sRGB", "cpipe_scene_linear_to_display", "rgba", "rgba8", 12, "display_srgb", "hbm"),
     ("scene_linear_to_display PQ", "cpipe_scene_linear_to_display", "rgba", "rgba16u", 16, "display_pq", "issue"),
@@ -80,6 +82,7 @@ def node_roofline(width=4032, height=3024, reps=10, peak_gbs=None):
     b = cfg.blobs()
     b["linearize"] = B.linearize(np.arange(1 << cfg.bits, dtype=np.uint16))
     b["usm"] = B.usm()
+    b["aces"], b["reinhard"] = B.aces(), B.reinhard()
     b["display_srgb"], b["display_pq"] = B.display("sRGB"), B.display("BT2020-PQ")
     raw = cfg.make_raw()
     frames = {"u16": raw, "f32raw": raw.astype(np.float32),

@@ -100,6 +100,8 @@ CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_denoise_wavelet_atrous_spec);
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_lens_dng_opcode_list_3);     /* dng_opcode_list_3_dispatch.cpp:333-398 */
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_color_3d_lut);               /* lut3d_dispatch.cpp:20-60 */
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_tone_filmic_rgb);            /* filmic_rgb_dispatch.cpp:22-36 */
+CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_tone_aces_filmic);           /* aces_filmic_dispatch.cpp:17-31 */
+CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_tone_reinhard);              /* reinhard_dispatch.cpp:16-29 */
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_sharpen_edge_aware_usm);     /* edge_aware_usm_dispatch.cpp:18-31 */
 /* Scene-linear Rec.2020 to display encode (aot_id "cpipe_scene_linear_to_display",
  * blob cpipe_DisplayParams; RGBA16F in, RGBA8 unorm out for sRGB, RGBA16

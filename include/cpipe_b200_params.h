@@ -170,6 +170,16 @@ typedef struct {
     float shadows;
 } cpipe_FilmicRgbParams;
 
+/* tone.aces_filmic (nodes/tone/aces_filmic_dispatch.cpp:13-15). */
+typedef struct {
+    int32_t enabled;   /* 0: pass-through */
+} cpipe_AcesFilmicParams;
+
+/* tone.reinhard (nodes/tone/reinhard_dispatch.cpp:12-14). */
+typedef struct {
+    float white_point; /* the node sends 1e6 when its param is unset, else clamp(0.1, 10) */
+} cpipe_ReinhardParams;
+
 /* sharpen.edge_aware_usm (nodes/sharpen/edge_aware_usm_dispatch.cpp:12-16). */
 typedef struct {
     float strength;    /* 0..2 (node default 0.75) */
@@ -244,6 +254,8 @@ CPIPE_STATIC_ASSERT(sizeof(cpipe_Bm3dSpecParams) == 40, "Bm3dSpecParams layout")
 CPIPE_STATIC_ASSERT(sizeof(cpipe_SurrogateHeader) == 32, "SurrogateHeader layout");
 CPIPE_STATIC_ASSERT(sizeof(cpipe_AtrousWaveletParams) == 16, "AtrousWaveletParams layout");
 CPIPE_STATIC_ASSERT(sizeof(cpipe_EdgeAwareUsmParams) == 12, "EdgeAwareUsmParams layout");
+CPIPE_STATIC_ASSERT(sizeof(cpipe_AcesFilmicParams) == 4, "AcesFilmicParams layout");
+CPIPE_STATIC_ASSERT(sizeof(cpipe_ReinhardParams) == 4, "ReinhardParams layout");
 CPIPE_STATIC_ASSERT(sizeof(cpipe_DisplayParams) == 4, "DisplayParams layout");
 
 #ifdef __cplusplus

@@ -188,6 +188,20 @@ def guided(x, radius, eps, f16=True):
     return out
 
 
+def aces(x, enabled=True, f16=True):
+    x = _f32(x)
+    out = np.empty_like(x)
+    lib().oracle_aces(_p(x), _p(out), x.shape[1], x.shape[0], int(bool(enabled)), int(f16))
+    return out
+
+
+def reinhard(x, white_point=1000000.0, f16=True):
+    x = _f32(x)
+    out = np.empty_like(x)
+    lib().oracle_reinhard(_p(x), _p(out), x.shape[1], x.shape[0], C.c_float(white_point), int(f16))
+    return out
+
+
 def usm(x, strength=0.75, radius=1, threshold=0.0, f16=True):
     x = _f32(x)
     out = np.empty_like(x)

@@ -290,6 +290,35 @@ static inline float rs(const rgba_t* im, int x, int y, int c) {
     return im->p[4 * ((long)clampi(y, 0, im->h - 1) * im->w + clampi(x, 0, im->w - 1)) + c];
 }
 
+/* ---- tone.aces_filmic (src/cpipe/nodes/tone/aces_filmic_generator.cpp:22-52) and
+ * tone.reinhard (reinhard_generator.cpp:20-48): per RGB channel, alpha passes. */
+static float aces_fit(float v) {
+    v = maxf(0.0F, v);
+    return clampf((v * ((2.51F * v) + 0.03F)) / ((v * ((2.43F * v) + 0.59F)) + 0.14F), 0.0F, 1.0F);
+}
+void oracle_aces(const float* in, float* out, int w, int h, int enabled, int f16) {
+    const long n = (long)w * h;
+    for (long i = 0; i < n; ++i)
+        for (int c = 0; c < 4; ++c) {
+            const float v = in[4 * i + c];
+            out[4 * i + c] = rnd(c == 3 || enabled == 0 ? v : aces_fit(v), f16);
+        }
+}
+void oracle_reinhard(const float* in, float* out, int w, int h, float white_point, int f16) {
+    const long n = (long)w * h;
+    const float wp2 = white_point * white_point;
+    for (long i = 0; i < n; ++i)
+        for (int c = 0; c < 4; ++c) {
+            const float x = in[4 * i + c];
+            float o = x;
+            if (c != 3) {
+                const float v = maxf(0.0F, x);
+                o = clampf((v * (1.0F + (v / wp2))) / (1.0F + v), 0.0F, 1.0F);
+            }
+            out[4 * i + c] = rnd(o, f16);
+        }
+}
+
 /* ---- sharpen.edge_aware_usm (src/cpipe/nodes/sharpen/edge_aware_usm_generator.cpp:11-75) ----
  * blur = mean3x3 (radius <= 1, explicit 9-term left-associated sum) or mean5x5
  * (0 + the 25 terms in row-major order), both over the clamped input;

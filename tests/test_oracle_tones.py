@@ -1,0 +1,20 @@
+"""CPU checks of the tone.aces_filmic and tone.reinhard oracles against the
+reference's golden fixtures (written by its own golden generator)."""
+import numpy as np
+import oracle
+from conftest import golden
+
+
+def test_aces_oracle_matches_reference_golden():
+    g = golden("tone.aces_filmic")
+    x = g["input"].astype(np.float16).astype(np.float32)
+    np.testing.assert_array_equal(oracle.aces(x, True), g["output"])
+    np.testing.assert_array_equal(oracle.aces(x, False), x)  # toggle off passes every channel
+
+
+def test_reinhard_oracle_matches_reference_golden():
+    g = golden("tone.reinhard")
+    x = g["input"].astype(np.float16).astype(np.float32)
+    np.testing.assert_array_equal(oracle.reinhard(x, 1000000.0), g["output"])
+    y = oracle.reinhard(x, 0.1)  # a low white point saturates early
+    assert (y[..., :3] >= oracle.reinhard(x, 1000000.0)[..., :3]).all() and (y <= 1.0).all()
