@@ -118,6 +118,11 @@ class FilmicRgbParams(C.Structure):
     _fields_ = [(n, C.c_float) for n in ("ev", "contrast", "saturation", "highlights", "shadows")]
 
 
+class GreyworldParams(C.Structure):
+    """cpipe_GreyworldParams (aot_id cpipe_wb_greyworld_auto): host address of a float[3] for the neutral."""
+    _fields_ = [("neutral_out", C.c_uint64)]
+
+
 class AcesFilmicParams(C.Structure):
     """cpipe_AcesFilmicParams (aot_id tone_aces_filmic)."""
     _fields_ = [("enabled", C.c_int32)]
@@ -188,6 +193,7 @@ EXPORTS = [
     "cpipe_cuda_denoise_guided_filter",
     "cpipe_cuda_denoise_wavelet_bayes_shrink", "cpipe_cuda_lens_dng_opcode_list_3", "cpipe_cuda_color_3d_lut",
     "cpipe_cuda_tone_filmic_rgb", "cpipe_cuda_tone_aces_filmic", "cpipe_cuda_tone_reinhard",
+    "cpipe_cuda_wb_greyworld_auto",
     "cpipe_cuda_sharpen_edge_aware_usm", "cpipe_cuda_scene_linear_to_display",
     "cpipe_cuda_copy", "cpipe_cuda_filters", "cpipe_cuda_find_filter",
     "cpipe_cuda_color_3d_lut_noalloc",

@@ -843,6 +843,51 @@ int cpipe_cuda_tone_filmic_rgb(halide_buffer_t* const* inputs, size_t n_in, hali
     return call.finish(cuda_status(launch_filmic(in.img, out.img, in.elem == 2, f, call.stream), "filmic"));
 }
 
+// ------------------------------------------------------- wb.greyworld_auto
+// greyworld_auto.cpp:44-77 on the GPU: exact channel sums (greyworld_sum_kernel
+// block totals added here in 128-bit integers, then rounded to double once),
+// the neutral (R/G, 1, B/G) rounded to float as the reference does, v / neutral.
+int cpipe_cuda_wb_greyworld_auto(halide_buffer_t* const* inputs, size_t n_in, halide_buffer_t* const* outputs,
+                                 size_t n_out, const void* blob, size_t blob_size) {
+    CHECK_ARITY(1, 1);
+    if (blob == nullptr || blob_size < sizeof(cpipe_GreyworldParams)) return CPIPE_BAD_INDEX;
+    cpipe_GreyworldParams p;
+    std::memcpy(&p, blob, sizeof(p));
+    if (!device_ready()) return CPIPE_INTERNAL_ERROR;
+    Call call;
+    Bound in, out;
+    int st = rgba_pair(call, inputs, outputs, &in, &out);
+    if (st != CPIPE_OK) return call.finish(st);
+    if (in.elem != 2) return call.finish(CPIPE_BAD_PRECISION);
+    void* d_partial = nullptr;
+    if ((st = call.alloc(sizeof(long long) * 4 * kGreyworldBlocks, &d_partial)) != CPIPE_OK) return call.finish(st);
+    std::vector<long long> part(4 * kGreyworldBlocks);
+    cudaError_t e = launch_greyworld_sums(in.img, static_cast<long long*>(d_partial), kGreyworldBlocks, call.stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(part.data(), d_partial, part.size() * sizeof(long long), cudaMemcpyDeviceToHost,
+                            call.stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(call.stream);
+    if (e != cudaSuccess) return call.finish(cuda_status(e, "greyworld sums"));
+    __int128 t[3] = {0, 0, 0};
+    long long bad = 0;
+    for (int b = 0; b < kGreyworldBlocks; ++b) {
+        for (int k = 0; k < 3; ++k) t[k] += part[4 * b + k];
+        bad |= part[4 * b + 3];
+    }
+    double sums[3];
+    for (int k = 0; k < 3; ++k) sums[k] = std::ldexp((double)t[k], -24);
+    for (double v : sums)
+        if (bad || !(v > 0.0)) {
+            set_error("wb_greyworld_auto: %s", "invalid channel mean");
+            return call.finish(CPIPE_NEED_METADATA);
+        }
+    const float n[3] = {(float)(sums[0] / sums[1]), 1.0F, (float)(sums[2] / sums[1])};
+    if ((e = launch_greyworld_apply(in.img, out.img, n, call.stream)) != cudaSuccess)
+        return call.finish(cuda_status(e, "greyworld apply"));
+    if (p.neutral_out) std::memcpy(reinterpret_cast<void*>((uintptr_t)p.neutral_out), n, sizeof(n));
+    return call.finish(CPIPE_OK);
+}
+
 // ------------------------------------------------ tone.aces_filmic / reinhard
 // aces_filmic_dispatch.cpp:17-31, reinhard_dispatch.cpp:16-29 (4-byte blobs).
 int cpipe_cuda_tone_aces_filmic(halide_buffer_t* const* inputs, size_t n_in, halide_buffer_t* const* outputs,
@@ -1120,6 +1165,7 @@ static const cpipe_cuda_filter_desc kFilters[] = {
     {"lens_dng_opcode_list_3", (void*)&cpipe_cuda_lens_dng_opcode_list_3, 1},
     {"color_3d_lut", (void*)&cpipe_cuda_color_3d_lut, 1},
     {"tone_filmic_rgb", (void*)&cpipe_cuda_tone_filmic_rgb, 1},
+    {"cpipe_wb_greyworld_auto", (void*)&cpipe_cuda_wb_greyworld_auto, 1},
     {"tone_aces_filmic", (void*)&cpipe_cuda_tone_aces_filmic, 1},
     {"tone_reinhard", (void*)&cpipe_cuda_tone_reinhard, 1},
     {"sharpen_edge_aware_usm", (void*)&cpipe_cuda_sharpen_edge_aware_usm, 1},

@@ -32,6 +32,11 @@ cudaError_t launch_rgba16f_to_unorm(const Img& in, const Img& out, int bits8, cu
 cudaError_t launch_wb(const Img& in, const Img& out, bool f16, const float n[3], cudaStream_t st);
 cudaError_t launch_colormatrix(const Img& in, const Img& out, bool f16, const float t[9], cudaStream_t st);
 cudaError_t launch_filmic(const Img& in, const Img& out, bool f16, const FilmicDev& p, cudaStream_t st);
+// wb.greyworld_auto: per-block exact sums (d_partial: blocks x 4 int64, see
+// greyworld_sum_kernel), then v / n per RGB channel of an RGBA16F frame.
+constexpr int kGreyworldBlocks = 148 * 4;
+cudaError_t launch_greyworld_sums(const Img& in, long long* d_partial, int blocks, cudaStream_t st);
+cudaError_t launch_greyworld_apply(const Img& in, const Img& out, const float n[3], cudaStream_t st);
 cudaError_t launch_aces(const Img& in, const Img& out, bool f16, int enabled, cudaStream_t st);
 cudaError_t launch_reinhard(const Img& in, const Img& out, bool f16, float white_point, cudaStream_t st);
 cudaError_t launch_usm(const Img& in, const Img& out, bool f16, float strength, int radius, float threshold,

@@ -322,6 +322,16 @@ struct LutOp {
     int S, interp;
     __device__ void operator()(const T* s, T* d) const { store_rgb_keep_alpha(d, lut_px(load_rgba(s), lut, S, interp), s); }
 };
+// wb.greyworld_auto apply: v / neutral per RGB channel, alpha bits copied
+// (greyworld_auto.cpp:66-77).
+template <class T>
+struct GreyOp {
+    float n[3];
+    __device__ void operator()(const T* s, T* d) const {
+        const Rgba v = load_rgba(s);
+        store_rgb_keep_alpha(d, Rgba{v.r / n[0], v.g / n[1], v.b / n[2], v.a}, s);
+    }
+};
 // tone.aces_filmic (aces_filmic_generator.cpp:22-52): the Narkowicz 2016 fit
 // per RGB channel, alpha passes; enabled == 0 passes every channel.
 __device__ __forceinline__ float aces_fit(float v) {
@@ -584,6 +594,58 @@ __device__ __forceinline__ void display_store(const Img& out, int x, int y, cons
             make_ushort4((unsigned short)((unsigned)o[0] << 6), (unsigned short)((unsigned)o[1] << 6),
                           (unsigned short)((unsigned)o[2] << 6), (unsigned short)((unsigned)o[3] << 6));
 }
+// ------------------------------------------------------ wb.greyworld_auto
+// Estimate: per-channel sums of the RGB values of an RGBA16F frame.  Every
+// binary16 value is an integer multiple of 2^-24, below 2^41 of those units
+// in magnitude, so a block adds its pixels as int64 integers (exact, in any
+// order) over a fixed range of rows and the host adds the block totals in
+// 128-bit integers: the sum is exact and rounded to double once, whatever the
+// order the blocks ran in.  partial[b] = {sum R, sum G, sum B, non-finite seen}.
+__device__ __forceinline__ long long h16_units(unsigned h, int* nonfinite) {
+    const int e = (int)((h >> 10) & 31U), m = (int)(h & 1023U);
+    if (e == 31) {
+        *nonfinite = 1;
+        return 0;
+    }
+    const long long mag = e == 0 ? (long long)m : ((long long)(1024 + m) << (e - 1));
+    return (h & 0x8000U) ? -mag : mag;
+}
+__global__ void __launch_bounds__(256) greyworld_sum_kernel(Img in, long long* partial) {
+    const int rows = (in.h + (int)gridDim.x - 1) / (int)gridDim.x;
+    const int y0 = (int)blockIdx.x * rows, y1 = min(in.h, y0 + rows);
+    long long s0 = 0, s1 = 0, s2 = 0;
+    int bad = 0;
+    for (int y = y0; y < y1; ++y)
+        for (int x = threadIdx.x; x < in.w; x += blockDim.x) {
+            const uint2 u = *reinterpret_cast<const uint2*>(px<const __half>(in, x, y));
+            s0 += h16_units(u.x & 0xFFFFU, &bad);
+            s1 += h16_units(u.x >> 16, &bad);
+            s2 += h16_units(u.y & 0xFFFFU, &bad);
+        }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        s0 += __shfl_down_sync(0xFFFFFFFFU, s0, off);
+        s1 += __shfl_down_sync(0xFFFFFFFFU, s1, off);
+        s2 += __shfl_down_sync(0xFFFFFFFFU, s2, off);
+        bad |= __shfl_down_sync(0xFFFFFFFFU, bad, off);
+    }
+    __shared__ long long sh[8][4];
+    const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        sh[wid][0] = s0;
+        sh[wid][1] = s1;
+        sh[wid][2] = s2;
+        sh[wid][3] = bad;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        long long t[4] = {0, 0, 0, 0};
+        for (int w = 0; w < (int)(blockDim.x >> 5); ++w)
+            for (int k = 0; k < 4; ++k) t[k] = k < 3 ? t[k] + sh[w][k] : (t[k] | sh[w][k]);
+        for (int k = 0; k < 4; ++k) partial[4 * blockIdx.x + k] = t[k];
+    }
+}
+
 // ------------------------------------------------- sharpen.edge_aware_usm
 // edge_aware_usm_generator.cpp:11-75: blur = mean3x3 (R = 1: the explicit
 // 9-term left-associated sum, :11-17) or mean5x5 (R = 2: 0 + the 25 terms in
@@ -964,6 +1026,15 @@ static DisplayDev display_dev() {
     d.lin_break = (float)lb;
     d.inv_slope = (float)(eb / lb);
     return d;
+}
+cudaError_t launch_greyworld_sums(const Img& in, long long* d_partial, int blocks, cudaStream_t st) {
+    greyworld_sum_kernel<<<(unsigned)blocks, 256, 0, st>>>(in, d_partial);
+    return cudaGetLastError();
+}
+cudaError_t launch_greyworld_apply(const Img& in, const Img& out, const float n[3], cudaStream_t st) {
+    const dim3 g = rgba_grid(in.w, in.h, true);
+    rgba_point_kernel<__half><<<g, kPtThreads, 0, st>>>(in, out, GreyOp<__half>{{n[0], n[1], n[2]}});
+    return cudaGetLastError();
 }
 cudaError_t launch_aces(const Img& in, const Img& out, bool f16, int enabled, cudaStream_t st) {
     const dim3 g = rgba_grid(in.w, in.h, f16);

@@ -288,6 +288,19 @@ int node_qbc(Ctx& c) {
 }
 
 // wb_dual_illuminant.cpp:299-403
+// WbMetadata.hpp:265-306 (interpolate_calibration) through the host preparation.
+int wb_calibrate(const cpipe_calibration_view& cal, const Vec3& neutral, cpipe_WbParams* p, double* cct) {
+    Mat3 cm1, cm2, fm1, fm2;
+    std::memcpy(cm1.data(), cal.color_matrix1, sizeof(cm1));
+    std::memcpy(cm2.data(), cal.color_matrix2, sizeof(cm2));
+    std::memcpy(fm1.data(), cal.forward_matrix1, sizeof(fm1));
+    std::memcpy(fm2.data(), cal.forward_matrix2, sizeof(fm2));
+    const bool has_fm = cal.has_forward_matrix1 && cal.has_forward_matrix2;
+    return cpb::prep::wb_prepare(neutral, cal.has_color_matrix1 ? &cm1 : nullptr, cal.has_color_matrix2 ? &cm2 : nullptr,
+                                 has_fm ? &fm1 : nullptr, has_fm ? &fm2 : nullptr, cal.calibration_illuminant1,
+                                 cal.calibration_illuminant2, p, cct);
+}
+int emit_wb_blobs(Ctx& c, const Vec3& neutral, const cpipe_WbParams& p, double cct);
 int node_wb(Ctx& c) {
     int st = check_rgba(c);
     if (st != CPIPE_OK) return st;
@@ -296,20 +309,87 @@ int node_wb(Ctx& c) {
     cpipe_capture_view cap;
     cpipe_calibration_view cal;
     if (c.meta->get_capture(m, &cap) != CPIPE_OK || !calibration(c, m, &cal)) return CPIPE_NEED_METADATA;
-    Mat3 cm1, cm2, fm1, fm2;
-    std::memcpy(cm1.data(), cal.color_matrix1, sizeof(cm1));
-    std::memcpy(cm2.data(), cal.color_matrix2, sizeof(cm2));
-    std::memcpy(fm1.data(), cal.forward_matrix1, sizeof(fm1));
-    std::memcpy(fm2.data(), cal.forward_matrix2, sizeof(fm2));
     const Vec3 neutral{cap.as_shot_neutral[0], cap.as_shot_neutral[1], cap.as_shot_neutral[2]};
     cpipe_WbParams p{};
     double cct = 0.0;
-    const bool has_fm = cal.has_forward_matrix1 && cal.has_forward_matrix2;
-    st = cpb::prep::wb_prepare(neutral, cal.has_color_matrix1 ? &cm1 : nullptr, cal.has_color_matrix2 ? &cm2 : nullptr,
-                               has_fm ? &fm1 : nullptr, has_fm ? &fm2 : nullptr, cal.calibration_illuminant1,
-                               cal.calibration_illuminant2, &p, &cct);
-    if (st != CPIPE_OK) return st;
+    if ((st = wb_calibrate(cal, neutral, &p, &cct)) != CPIPE_OK) return st;
     if ((st = c.submit("wb_dual_illuminant", &p, sizeof(p))) != CPIPE_OK) return st;
+    if ((st = emit_wb_blobs(c, neutral, p, cct)) != CPIPE_OK) return st;
+    return c.step("white_balance");
+}
+
+// wb/greyworld_auto.cpp:80-166: checks, the grey-world estimate and apply (on
+// the GPU through "cpipe_wb_greyworld_auto"; on a host that does not route it,
+// the reference's own loops through lock_cpu), then the same calibration and
+// metadata as the dual-illuminant node with the estimated neutral.
+static int greyworld_cpu(Ctx& c, uint32_t w, uint32_t h, float n[3]) {
+    void* src = nullptr;
+    void* dst = nullptr;
+    int st = c.buf->lock_cpu(const_cast<cpipe_buffer_t*>(c.in(0)), CPIPE_CPU_ACCESS_READ, &src);
+    if (st != CPIPE_OK) return st;
+    if ((st = c.buf->lock_cpu(c.out(0), CPIPE_CPU_ACCESS_WRITE, &dst)) != CPIPE_OK) {
+        c.buf->unlock_cpu(const_cast<cpipe_buffer_t*>(c.in(0)));
+        return st;
+    }
+    const auto* in = static_cast<const _Float16*>(src);
+    auto* out = static_cast<_Float16*>(dst);
+    const size_t count = (size_t)w * h;
+    double sums[3] = {0.0, 0.0, 0.0};
+    for (size_t i = 0; i < count; ++i)
+        for (int k = 0; k < 3; ++k) sums[k] += (double)(float)in[4 * i + k];
+    bool valid = true;
+    for (double v : sums) valid = valid && std::isfinite(v) && v > 0.0;
+    if (valid) {
+        n[0] = (float)(sums[0] / sums[1]);
+        n[1] = 1.0F;
+        n[2] = (float)(sums[2] / sums[1]);
+        for (size_t i = 0; i < count; ++i) {
+            for (int k = 0; k < 3; ++k) out[4 * i + k] = (_Float16)((float)in[4 * i + k] / n[k]);
+            out[4 * i + 3] = in[4 * i + 3];
+        }
+    }
+    const int s1 = c.buf->unlock_cpu(c.out(0));
+    const int s2 = c.buf->unlock_cpu(const_cast<cpipe_buffer_t*>(c.in(0)));
+    if (s1 != CPIPE_OK) return s1;
+    if (s2 != CPIPE_OK) return s2;
+    if (!valid) {
+        c.msg = "wb.greyworld invalid channel mean";
+        return CPIPE_NEED_METADATA;
+    }
+    return c.buf->flush_cpu_writes(c.out(0));
+}
+int node_greyworld(Ctx& c) {
+    int a = 0, b = 0;
+    int st = c.format(c.in(0), &a);
+    if (st == CPIPE_OK) st = c.format(c.out(0), &b);
+    if (st != CPIPE_OK) return st;
+    if (a != CPIPE_FMT_R16G16B16A16_SFLOAT || b != CPIPE_FMT_R16G16B16A16_SFLOAT) {
+        c.msg = "wb.greyworld format mismatch";
+        return CPIPE_BAD_PRECISION;
+    }
+    uint32_t w, h;
+    if ((st = c.dims(c.in(0), &w, &h)) != CPIPE_OK) return st;
+    const cpipe_metadata_t* m = c.metadata(c.in(0));
+    if (!m) return CPIPE_NEED_METADATA;
+    cpipe_calibration_view cal;
+    if (!calibration(c, m, &cal)) return CPIPE_NEED_METADATA;
+    float n[3] = {1.0F, 1.0F, 1.0F};
+    const cpipe_GreyworldParams gp{(uint64_t)(uintptr_t)n};
+    st = c.submit("cpipe_wb_greyworld_auto", &gp, sizeof(gp));
+    if (st == CPIPE_UNSUPPORTED) st = greyworld_cpu(c, w, h, n);
+    if (st != CPIPE_OK) return st;
+    const Vec3 neutral{n[0], n[1], n[2]};
+    cpipe_WbParams p{};
+    double cct = 0.0;
+    if ((st = wb_calibrate(cal, neutral, &p, &cct)) != CPIPE_OK) return st;
+    if ((st = c.mb->set_as_shot_neutral(c.builder(), n)) != CPIPE_OK) return st;
+    if ((st = emit_wb_blobs(c, neutral, p, cct)) != CPIPE_OK) return st;
+    return c.step("white_balance");
+}
+
+// WbMetadata.hpp:308-327: the four white-balance blobs.
+int emit_wb_blobs(Ctx& c, const Vec3& neutral, const cpipe_WbParams& p, double cct) {
+    int st;
     const float diag[3] = {1.0F / neutral[0], 1.0F / neutral[1], 1.0F / neutral[2]};
     const float cct_f = (float)cct;
     if ((st = c.mb->set_blob(c.builder(), "com.cpipe.wb.camera_diag_f32", diag, sizeof(diag))) != CPIPE_OK) return st;
@@ -319,7 +399,7 @@ int node_wb(Ctx& c) {
     if ((st = c.mb->set_blob(c.builder(), "com.cpipe.wb.dual_illuminant_weight_f32", &p.dual_illuminant_weight,
                              sizeof(float))) != CPIPE_OK)
         return st;
-    return c.step("white_balance");
+    return CPIPE_OK;
 }
 
 // colormatrix_dng_to_working.cpp:99-140
@@ -692,6 +772,10 @@ const char kFilmic[] = MANIFEST("com.cpipe.tone.filmic_rgb", "Filmic RGB Tone", 
     NUM("highlights", "0", "2", "1") "," NUM("shadows", "0", "2", "1"),
     "scene_linear_rec2020", "scene_linear_rec2020", "true", "\"rgba_point<filmic>\"");
 
+const char kGreyworld[] = MANIFEST("com.cpipe.wb.greyworld_auto", "Grey-world Auto WB", "wb",
+    PORT("rgb", "in", "\"rgba\"", "\"f16\"", "\"requires_steps_applied\":[\"demosaic\"],\"requires_fields\":[\"calibration.color_matrix1\",\"calibration.color_matrix2\",\"calibration.calibration_illuminant1\",\"calibration.calibration_illuminant2\"]"),
+    PORT("rgb", "out", "\"rgba\"", "\"f16\"", "\"inherits_from\":\"rgb\",\"sets_steps_applied\":[\"white_balance\"],\"writes_fields\":[\"capture.as_shot_neutral\"]"),
+    "", "raw_camera", "raw_camera", "true", "\"greyworld_sum_kernel\",\"rgba_point<greyworld>\"");
 const char kAces[] = MANIFEST("com.cpipe.tone.aces_filmic", "ACES Filmic Tone", "tone",
     RGBA_IN("rgb", "\"requires_steps_applied\":[\"denoise.wavelet_bayes_shrink\"]"), RGBA_OUT("rgb", "tone.aces_filmic", ""),
     "{\"name\":\"toggle\",\"type\":\"bool\",\"default\":true}",
@@ -734,6 +818,7 @@ CPIPE_B200_REGISTER(cpipe_b200_desc_wavelet, "com.cpipe.denoise.wavelet_bayes_sh
 CPIPE_B200_REGISTER(cpipe_b200_desc_opcode3, "com.cpipe.lens.dng_opcode_list_3", kOpcode3, node_opcode3)
 CPIPE_B200_REGISTER(cpipe_b200_desc_lut, "com.cpipe.color.3d_lut", kLut, node_lut3d)
 CPIPE_B200_REGISTER(cpipe_b200_desc_filmic, "com.cpipe.tone.filmic_rgb", kFilmic, node_filmic)
+CPIPE_B200_REGISTER(cpipe_b200_desc_greyworld, "com.cpipe.wb.greyworld_auto", kGreyworld, node_greyworld)
 CPIPE_B200_REGISTER(cpipe_b200_desc_aces, "com.cpipe.tone.aces_filmic", kAces, node_aces)
 CPIPE_B200_REGISTER(cpipe_b200_desc_reinhard, "com.cpipe.tone.reinhard", kReinhard, node_reinhard)
 CPIPE_B200_REGISTER(cpipe_b200_desc_usm, "com.cpipe.sharpen.edge_aware_usm", kUsm, node_usm)

@@ -58,6 +58,7 @@ NODES = [
     ("a14 OpcodeList3 warp", "lens_dng_opcode_list_3", "rgba", "rgba", 16, "opcode3", "issue"),
     ("a15 3D LUT", "color_3d_lut", "rgba", "rgba", 16, "lut", "gather"),
     ("a16 filmic", "tone_filmic_rgb", "rgba", "rgba", 16, "filmic", "issue"),
+    ("wb.greyworld_auto (sum + apply)", "cpipe_wb_greyworld_auto", "rgba", "rgba", 16, "greyworld", "hbm"),
     ("tone.aces_filmic", "tone_aces_filmic", "rgba", "rgba", 16, "aces", "hbm"),
     ("tone.reinhard", "tone_reinhard", "rgba", "rgba", 16, "reinhard", "hbm"),
     ("sharpen.edge_aware_usm (3x3)", "sharpen_edge_aware_usm", "rgba", "rgba", 16, "usm", "hbm"),
@@ -83,6 +84,7 @@ def node_roofline(width=4032, height=3024, reps=10, peak_gbs=None):
     b["linearize"] = B.linearize(np.arange(1 << cfg.bits, dtype=np.uint16))
     b["usm"] = B.usm()
     b["aces"], b["reinhard"] = B.aces(), B.reinhard()
+    b["greyworld"] = bytes(A.GreyworldParams(0))
     b["display_srgb"], b["display_pq"] = B.display("sRGB"), B.display("BT2020-PQ")
     raw = cfg.make_raw()
     frames = {"u16": raw, "f32raw": raw.astype(np.float32),

@@ -100,6 +100,13 @@ CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_denoise_wavelet_atrous_spec);
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_lens_dng_opcode_list_3);     /* dng_opcode_list_3_dispatch.cpp:333-398 */
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_color_3d_lut);               /* lut3d_dispatch.cpp:20-60 */
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_tone_filmic_rgb);            /* filmic_rgb_dispatch.cpp:22-36 */
+/* wb.greyworld_auto (aot_id "cpipe_wb_greyworld_auto", blob
+ * cpipe_GreyworldParams; RGBA16F in and out): the grey-world neutral from
+ * exact per-channel sums of the frame, then v / neutral per RGB channel.
+ * Replaces the CPU loops of the reference node (greyworld_auto.cpp:44-77);
+ * no reference filter counterpart.  CPIPE_NEED_METADATA when a channel sum is
+ * not positive or a value is not finite, as the reference node. */
+CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_wb_greyworld_auto);
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_tone_aces_filmic);           /* aces_filmic_dispatch.cpp:17-31 */
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_tone_reinhard);              /* reinhard_dispatch.cpp:16-29 */
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_sharpen_edge_aware_usm);     /* edge_aware_usm_dispatch.cpp:18-31 */

@@ -170,6 +170,13 @@ typedef struct {
     float shadows;
 } cpipe_FilmicRgbParams;
 
+/* wb.greyworld_auto on the GPU (aot_id "cpipe_wb_greyworld_auto").
+ * neutral_out: host address of a float[3] that receives the estimated neutral
+ * (R/G, 1, B/G) the node then writes into the metadata. */
+typedef struct {
+    uint64_t neutral_out;
+} cpipe_GreyworldParams;
+
 /* tone.aces_filmic (nodes/tone/aces_filmic_dispatch.cpp:13-15). */
 typedef struct {
     int32_t enabled;   /* 0: pass-through */
@@ -255,6 +262,7 @@ CPIPE_STATIC_ASSERT(sizeof(cpipe_SurrogateHeader) == 32, "SurrogateHeader layout
 CPIPE_STATIC_ASSERT(sizeof(cpipe_AtrousWaveletParams) == 16, "AtrousWaveletParams layout");
 CPIPE_STATIC_ASSERT(sizeof(cpipe_EdgeAwareUsmParams) == 12, "EdgeAwareUsmParams layout");
 CPIPE_STATIC_ASSERT(sizeof(cpipe_AcesFilmicParams) == 4, "AcesFilmicParams layout");
+CPIPE_STATIC_ASSERT(sizeof(cpipe_GreyworldParams) == 8, "GreyworldParams layout");
 CPIPE_STATIC_ASSERT(sizeof(cpipe_ReinhardParams) == 4, "ReinhardParams layout");
 CPIPE_STATIC_ASSERT(sizeof(cpipe_DisplayParams) == 4, "DisplayParams layout");
 

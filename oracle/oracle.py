@@ -296,3 +296,22 @@ def ref_wb_interpolate(neutral, cm1, cm2, fm1=None, fm2=None, illum1=17, illum2=
                                     F9(*fm1) if fm1 is not None else None, F9(*fm2) if fm2 is not None else None,
                                     C.c_uint(illum1), C.c_uint(illum2), out, C.byref(cct), C.byref(wgt))
     return st, list(out), cct.value, wgt.value
+
+
+def greyworld(x):
+    """wb.greyworld_auto (src/cpipe/nodes/wb/greyworld_auto.cpp:44-77): the
+    neutral (R/G, 1, B/G) from the channel sums and v / neutral per RGB channel
+    in float, rounded to binary16; alpha passes.  The sums are exact and
+    rounded once (math.fsum): the reference adds sequentially in double, which
+    is exact for the fixture's few values.  Returns (neutral, out) or
+    (None, None) when a sum is not finite or not positive."""
+    import math
+    x = np.asarray(x, np.float16).astype(np.float32)
+    sums = [math.fsum(x[..., c].astype(np.float64).ravel().tolist()) for c in range(3)]
+    if any(not math.isfinite(v) or v <= 0.0 for v in sums):
+        return None, None
+    n = np.array([sums[0] / sums[1], 1.0, sums[2] / sums[1]], np.float32)
+    out = x.copy()
+    for c in range(3):
+        out[..., c] = (x[..., c] / n[c]).astype(np.float16).astype(np.float32)
+    return n, out

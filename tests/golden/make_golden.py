@@ -25,7 +25,7 @@ FIXTURES = [
     "demosaic.rcd", "demosaic.amaze", "demosaic.quad_bayer_remosaic", "lens.dng_opcode_list_3",
     "wb.dual_illuminant", "colormatrix.dng_to_working", "denoise.bm3d", "denoise.guided_filter",
     "denoise.wavelet_bayes_shrink", "tone.filmic_rgb", "color.3d_lut", "sharpen.edge_aware_usm",
-    "tone.aces_filmic", "tone.reinhard",
+    "tone.aces_filmic", "tone.reinhard", "wb.greyworld_auto",
 ]
 
 

@@ -69,6 +69,7 @@ EXPECTED_NODES = {
     "com.cpipe.lens.dng_opcode_list_3": ("scene_rgb", "corrected_rgb", []),
     "com.cpipe.color.3d_lut": ("rgb", "rgb", ["lut_path", "interpolation"]),
     "com.cpipe.tone.filmic_rgb": ("rgb", "rgb", ["ev", "contrast", "saturation", "highlights", "shadows"]),
+    "com.cpipe.wb.greyworld_auto": ("rgb", "rgb", []),
     "com.cpipe.tone.aces_filmic": ("rgb", "rgb", ["toggle"]),
     "com.cpipe.tone.reinhard": ("rgb", "rgb", ["white_point"]),
     "com.cpipe.sharpen.edge_aware_usm": ("rgb", "rgb", ["strength", "radius", "threshold"]),

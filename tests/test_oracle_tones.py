@@ -18,3 +18,11 @@ def test_reinhard_oracle_matches_reference_golden():
     np.testing.assert_array_equal(oracle.reinhard(x, 1000000.0), g["output"])
     y = oracle.reinhard(x, 0.1)  # a low white point saturates early
     assert (y[..., :3] >= oracle.reinhard(x, 1000000.0)[..., :3]).all() and (y <= 1.0).all()
+
+
+def test_greyworld_oracle_matches_reference_golden():
+    g = golden("wb.greyworld_auto")
+    n, out = oracle.greyworld(g["input"])
+    np.testing.assert_array_equal(out, g["output"])
+    assert n[1] == 1.0
+    assert oracle.greyworld(np.zeros((2, 2, 4), np.float32)) == (None, None)
