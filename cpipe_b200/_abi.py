@@ -123,6 +123,12 @@ class GreyworldParams(C.Structure):
     _fields_ = [("neutral_out", C.c_uint64)]
 
 
+class MertensLocalParams(C.Structure):
+    """cpipe_MertensLocalParams (aot_id tone_mertens_local)."""
+    _fields_ = [("weight_contrast", C.c_float), ("weight_saturation", C.c_float),
+                ("weight_well_exposedness", C.c_float)]
+
+
 class AcesFilmicParams(C.Structure):
     """cpipe_AcesFilmicParams (aot_id tone_aces_filmic)."""
     _fields_ = [("enabled", C.c_int32)]
@@ -193,7 +199,7 @@ EXPORTS = [
     "cpipe_cuda_denoise_guided_filter",
     "cpipe_cuda_denoise_wavelet_bayes_shrink", "cpipe_cuda_lens_dng_opcode_list_3", "cpipe_cuda_color_3d_lut",
     "cpipe_cuda_tone_filmic_rgb", "cpipe_cuda_tone_aces_filmic", "cpipe_cuda_tone_reinhard",
-    "cpipe_cuda_wb_greyworld_auto",
+    "cpipe_cuda_wb_greyworld_auto", "cpipe_cuda_tone_mertens_local",
     "cpipe_cuda_sharpen_edge_aware_usm", "cpipe_cuda_scene_linear_to_display",
     "cpipe_cuda_copy", "cpipe_cuda_filters", "cpipe_cuda_find_filter",
     "cpipe_cuda_color_3d_lut_noalloc",

@@ -79,6 +79,11 @@ def filmic(ev=0.0, contrast=1.0, saturation=1.0, highlights=1.0, shadows=1.0):
     return raw(A.FilmicRgbParams(ev, contrast, saturation, highlights, shadows))
 
 
+def mertens(weight_contrast=0.0, weight_saturation=1.0, weight_well_exposedness=1.0):
+    """cpipe_MertensLocalParams for tone_mertens_local."""
+    return raw(A.MertensLocalParams(float(weight_contrast), float(weight_saturation), float(weight_well_exposedness)))
+
+
 def aces(enabled=True):
     """cpipe_AcesFilmicParams for tone_aces_filmic."""
     return raw(A.AcesFilmicParams(1 if enabled else 0))

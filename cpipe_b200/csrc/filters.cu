@@ -888,6 +888,30 @@ int cpipe_cuda_wb_greyworld_auto(halide_buffer_t* const* inputs, size_t n_in, ha
     return call.finish(CPIPE_OK);
 }
 
+// ------------------------------------------------------ tone.mertens_local
+// mertens_local_dispatch.cpp:18-37: inputs under, normal, over (RGBA16F, one extent).
+int cpipe_cuda_tone_mertens_local(halide_buffer_t* const* inputs, size_t n_in, halide_buffer_t* const* outputs,
+                                  size_t n_out, const void* blob, size_t blob_size) {
+    CHECK_ARITY(3, 1);
+    if (inputs[1] == nullptr || inputs[2] == nullptr) return CPIPE_BAD_INDEX;
+    if (blob == nullptr || blob_size < sizeof(cpipe_MertensLocalParams)) return CPIPE_BAD_INDEX;
+    cpipe_MertensLocalParams p;
+    std::memcpy(&p, blob, sizeof(p));
+    if (!device_ready()) return CPIPE_INTERNAL_ERROR;
+    Call call;
+    BIND(0, inputs, Kind::Rgba, false, under);
+    BIND(1, inputs, Kind::Rgba, false, normal);
+    BIND(2, inputs, Kind::Rgba, false, over);
+    BIND(0, outputs, Kind::Rgba, true, out);
+    if (under.elem != 2 || normal.elem != 2 || over.elem != 2 || out.elem != 2) return call.finish(CPIPE_BAD_PRECISION);
+    REQUIRE_SAME_EXTENT(under, out);
+    REQUIRE_SAME_EXTENT(normal, out);
+    REQUIRE_SAME_EXTENT(over, out);
+    return call.finish(cuda_status(launch_mertens(under.img, normal.img, over.img, out.img, p.weight_contrast,
+                                                  p.weight_saturation, p.weight_well_exposedness, call.stream),
+                                   "mertens"));
+}
+
 // ------------------------------------------------ tone.aces_filmic / reinhard
 // aces_filmic_dispatch.cpp:17-31, reinhard_dispatch.cpp:16-29 (4-byte blobs).
 int cpipe_cuda_tone_aces_filmic(halide_buffer_t* const* inputs, size_t n_in, halide_buffer_t* const* outputs,
@@ -1166,6 +1190,7 @@ static const cpipe_cuda_filter_desc kFilters[] = {
     {"color_3d_lut", (void*)&cpipe_cuda_color_3d_lut, 1},
     {"tone_filmic_rgb", (void*)&cpipe_cuda_tone_filmic_rgb, 1},
     {"cpipe_wb_greyworld_auto", (void*)&cpipe_cuda_wb_greyworld_auto, 1},
+    {"tone_mertens_local", (void*)&cpipe_cuda_tone_mertens_local, 1},
     {"tone_aces_filmic", (void*)&cpipe_cuda_tone_aces_filmic, 1},
     {"tone_reinhard", (void*)&cpipe_cuda_tone_reinhard, 1},
     {"sharpen_edge_aware_usm", (void*)&cpipe_cuda_sharpen_edge_aware_usm, 1},

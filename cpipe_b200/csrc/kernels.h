@@ -37,6 +37,8 @@ cudaError_t launch_filmic(const Img& in, const Img& out, bool f16, const FilmicD
 constexpr int kGreyworldBlocks = 148 * 4;
 cudaError_t launch_greyworld_sums(const Img& in, long long* d_partial, int blocks, cudaStream_t st);
 cudaError_t launch_greyworld_apply(const Img& in, const Img& out, const float n[3], cudaStream_t st);
+cudaError_t launch_mertens(const Img& under, const Img& normal, const Img& over, const Img& out, float wc, float ws,
+                           float we, cudaStream_t st);
 cudaError_t launch_aces(const Img& in, const Img& out, bool f16, int enabled, cudaStream_t st);
 cudaError_t launch_reinhard(const Img& in, const Img& out, bool f16, float white_point, cudaStream_t st);
 cudaError_t launch_usm(const Img& in, const Img& out, bool f16, float strength, int radius, float threshold,

@@ -594,6 +594,47 @@ __device__ __forceinline__ void display_store(const Img& out, int x, int y, cons
             make_ushort4((unsigned short)((unsigned)o[0] << 6), (unsigned short)((unsigned)o[1] << 6),
                           (unsigned short)((unsigned)o[2] << 6), (unsigned short)((unsigned)o[3] << 6));
 }
+// ------------------------------------------------------ tone.mertens_local
+// mertens_local_generator.cpp:22-115: per pixel, a weight per exposure from
+// its contrast (|luma - 0.5|), saturation (RGB spread around the luma) and
+// well-exposedness (Gaussian around 0.5 per channel, sigma 0.2), each raised
+// to its parameter (1 / the plain factor at the defaults), then the weighted
+// mean of the three exposures, clamped to [0, 1]; alpha from the normal frame.
+struct MertensDev {
+    float wc, ws, we;
+};
+__device__ __forceinline__ float mertens_cew(float v) {
+    constexpr float k = 2.0F * 0.20F * 0.20F;
+    const float d = v - 0.5F;
+    return expf(-(d * d) / k);
+}
+__device__ __forceinline__ float mertens_weight(const Rgba& f, const MertensDev& p) {
+    const float red = max0(f.r), green = max0(f.g), blue = max0(f.b);
+    const float mean = ((f.r + f.g) + f.b) / 3.0F;
+    const float sat = sqrtf(((((red - mean) * (red - mean)) + ((green - mean) * (green - mean))) +
+                             ((blue - mean) * (blue - mean))) / 3.0F +
+                            0.0001F);
+    const float well = (mertens_cew(red) * mertens_cew(green)) * mertens_cew(blue);
+    const float contrast = fabsf(mean - 0.5F);
+    const float cf = p.wc == 0.0F ? 1.0F : powf(contrast + 0.01F, p.wc);
+    const float sf = p.ws == 1.0F ? sat + 0.01F : powf(sat + 0.01F, p.ws);
+    const float ef = p.we == 1.0F ? well : powf(well + 0.0001F, p.we);
+    return (cf * sf) * ef;
+}
+__global__ void __launch_bounds__(kPtThreads) mertens_kernel(Img under, Img normal, Img over, Img out, MertensDev p) {
+    const int y = blockIdx.y, x = blockIdx.x * kPtThreads + threadIdx.x;
+    if (x >= out.w) return;
+    const Rgba u = load_rgba(px<const __half>(under, x, y)), n = load_rgba(px<const __half>(normal, x, y));
+    const Rgba o = load_rgba(px<const __half>(over, x, y));
+    const float wu = mertens_weight(u, p), wn = mertens_weight(n, p), wo = mertens_weight(o, p);
+    const float total = maxf((wu + wn) + wo, 0.000001F);
+    const float r = clampf((((wu * u.r) + (wn * n.r)) + (wo * o.r)) / total, 0.0F, 1.0F);
+    const float g = clampf((((wu * u.g) + (wn * n.g)) + (wo * o.g)) / total, 0.0F, 1.0F);
+    const float b = clampf((((wu * u.b) + (wn * n.b)) + (wo * o.b)) / total, 0.0F, 1.0F);
+    const __half* ns = px<const __half>(normal, x, y);
+    store_rgb_keep_alpha(px<__half>(out, x, y), Rgba{r, g, b, n.a}, ns);
+}
+
 // ------------------------------------------------------ wb.greyworld_auto
 // Estimate: per-channel sums of the RGB values of an RGBA16F frame.  Every
 // binary16 value is an integer multiple of 2^-24, below 2^41 of those units
@@ -1026,6 +1067,11 @@ static DisplayDev display_dev() {
     d.lin_break = (float)lb;
     d.inv_slope = (float)(eb / lb);
     return d;
+}
+cudaError_t launch_mertens(const Img& under, const Img& normal, const Img& over, const Img& out, float wc, float ws,
+                           float we, cudaStream_t st) {
+    mertens_kernel<<<row_grid(out.w, out.h, 1), kPtThreads, 0, st>>>(under, normal, over, out, MertensDev{wc, ws, we});
+    return cudaGetLastError();
 }
 cudaError_t launch_greyworld_sums(const Img& in, long long* d_partial, int blocks, cudaStream_t st) {
     greyworld_sum_kernel<<<(unsigned)blocks, 256, 0, st>>>(in, d_partial);

@@ -124,9 +124,14 @@ struct Ctx {
     int step(const char* s) { return mb->add_applied_step(builder(), s); }
 };
 
-bool one_to_one(const cpipe_process_ctx* pc) {
-    return pc && pc->n_in == 1 && pc->n_out == 1 && pc->inputs && pc->outputs && pc->inputs[0] && pc->outputs[0] &&
-           pc->out_metadata && pc->out_metadata[0];
+// nin inputs and one output, all present, with an output metadata builder.
+bool n_to_one(const cpipe_process_ctx* pc, size_t nin) {
+    if (!pc || pc->n_in != nin || pc->n_out != 1 || !pc->inputs || !pc->outputs || !pc->outputs[0] ||
+        !pc->out_metadata || !pc->out_metadata[0])
+        return false;
+    for (size_t i = 0; i < nin; ++i)
+        if (!pc->inputs[i]) return false;
+    return true;
 }
 
 int check_formats(Ctx& c, int fin, int fout) {
@@ -563,6 +568,29 @@ int node_filmic(Ctx& c) {
     return c.step("tone.filmic_rgb");
 }
 
+// tone/mertens_local.cpp:20-101: output and the three inputs RGBA16F with one
+// extent, parameters clamped, then the fusion; the step name is the reference's.
+int node_mertens(Ctx& c) {
+    int f = 0;
+    int st = c.format(c.out(0), &f);
+    if (st != CPIPE_OK) return st;
+    if (f != CPIPE_FMT_R16G16B16A16_SFLOAT) return CPIPE_BAD_PRECISION;
+    uint32_t w, h;
+    if ((st = c.dims(c.out(0), &w, &h)) != CPIPE_OK) return st;
+    for (size_t i = 0; i < 3; ++i) {
+        if ((st = c.format(c.in(i), &f)) != CPIPE_OK) return st;
+        if (f != CPIPE_FMT_R16G16B16A16_SFLOAT) return CPIPE_BAD_PRECISION;
+        uint32_t wi, hi;
+        if ((st = c.dims(c.in(i), &wi, &hi)) != CPIPE_OK) return st;
+        if (wi != w || hi != h) return CPIPE_BAD_INDEX;
+    }
+    const cpipe_MertensLocalParams p{c.clamped_float("weight_contrast", 0.0F, 0.0F, 2.0F),
+                                     c.clamped_float("weight_saturation", 1.0F, 0.0F, 2.0F),
+                                     c.clamped_float("weight_well_exposedness", 1.0F, 0.0F, 2.0F)};
+    if ((st = c.submit("tone_mertens_local", &p, sizeof(p))) != CPIPE_OK) return st;
+    return c.step("tone_mertens_local");
+}
+
 // tone/aces_filmic.cpp:28-46
 int node_aces(Ctx& c) {
     const cpipe_AcesFilmicParams p{c.bool_or("toggle", true) ? 1 : 0};
@@ -654,7 +682,7 @@ int node_display(Ctx& c) {
 // ------------------------------------------------------------- dispatching
 using NodeFn = int (*)(Ctx&);
 
-template <NodeFn F>
+template <NodeFn F, size_t NIN = 1>
 int main_entry(const char* action, cpipe_host_t* host, cpipe_node_t* node, cpipe_props_t* params, void* in_ctx,
                void* out_ctx) {
     (void)node;
@@ -674,7 +702,7 @@ int main_entry(const char* action, cpipe_host_t* host, cpipe_node_t* node, cpipe
         if (!std::strcmp(action, CPIPE_ACTION_PROCESS)) {
             if (host == nullptr || host->get_suite == nullptr) return CPIPE_BAD_INDEX;
             auto* pc = static_cast<cpipe_process_ctx*>(in_ctx);
-            if (!one_to_one(pc)) return CPIPE_BAD_INDEX;
+            if (!n_to_one(pc, NIN)) return CPIPE_BAD_INDEX;
             Ctx c{host, nullptr, nullptr, nullptr, nullptr, nullptr, params, pc, {}};
             if (!c.init()) return CPIPE_BAD_INDEX;
             const int st = F(c);
@@ -776,6 +804,13 @@ const char kGreyworld[] = MANIFEST("com.cpipe.wb.greyworld_auto", "Grey-world Au
     PORT("rgb", "in", "\"rgba\"", "\"f16\"", "\"requires_steps_applied\":[\"demosaic\"],\"requires_fields\":[\"calibration.color_matrix1\",\"calibration.color_matrix2\",\"calibration.calibration_illuminant1\",\"calibration.calibration_illuminant2\"]"),
     PORT("rgb", "out", "\"rgba\"", "\"f16\"", "\"inherits_from\":\"rgb\",\"sets_steps_applied\":[\"white_balance\"],\"writes_fields\":[\"capture.as_shot_neutral\"]"),
     "", "raw_camera", "raw_camera", "true", "\"greyworld_sum_kernel\",\"rgba_point<greyworld>\"");
+#define MERTENS_IN(name) PORT(name, "in", "\"rgba\"", "\"f16\"", "\"requires_steps_applied\":[\"denoise.wavelet_bayes_shrink\"]")
+const char kMertens[] = MANIFEST("com.cpipe.tone.mertens_local", "Mertens Exposure Fusion", "tone",
+    MERTENS_IN("under") "," MERTENS_IN("normal") "," MERTENS_IN("over"),
+    PORT("rgb", "out", "\"rgba\"", "\"f16\"", "\"inherits_from\":\"normal\",\"sets_steps_applied\":[\"tone_mertens_local\"]"),
+    NUM("weight_contrast", "0", "2", "0") "," NUM("weight_saturation", "0", "2", "1") ","
+    NUM("weight_well_exposedness", "0", "2", "1"),
+    "scene_linear_rec2020", "scene_linear_rec2020", "true", "\"mertens_kernel\"");
 const char kAces[] = MANIFEST("com.cpipe.tone.aces_filmic", "ACES Filmic Tone", "tone",
     RGBA_IN("rgb", "\"requires_steps_applied\":[\"denoise.wavelet_bayes_shrink\"]"), RGBA_OUT("rgb", "tone.aces_filmic", ""),
     "{\"name\":\"toggle\",\"type\":\"bool\",\"default\":true}",
@@ -819,6 +854,10 @@ CPIPE_B200_REGISTER(cpipe_b200_desc_opcode3, "com.cpipe.lens.dng_opcode_list_3",
 CPIPE_B200_REGISTER(cpipe_b200_desc_lut, "com.cpipe.color.3d_lut", kLut, node_lut3d)
 CPIPE_B200_REGISTER(cpipe_b200_desc_filmic, "com.cpipe.tone.filmic_rgb", kFilmic, node_filmic)
 CPIPE_B200_REGISTER(cpipe_b200_desc_greyworld, "com.cpipe.wb.greyworld_auto", kGreyworld, node_greyworld)
+#define CPIPE_B200_REGISTER_N(sym, id, manifest, fn, nin)                                       \
+    __attribute__((used, section("cpipe_registry"), aligned(8))) const cpipe_plugin_desc_t sym = \
+        {CPIPE_ABI_MAJOR, CPIPE_ABI_MINOR, id, "1.0.0", manifest, &main_entry<fn, nin>};
+CPIPE_B200_REGISTER_N(cpipe_b200_desc_mertens, "com.cpipe.tone.mertens_local", kMertens, node_mertens, 3)
 CPIPE_B200_REGISTER(cpipe_b200_desc_aces, "com.cpipe.tone.aces_filmic", kAces, node_aces)
 CPIPE_B200_REGISTER(cpipe_b200_desc_reinhard, "com.cpipe.tone.reinhard", kReinhard, node_reinhard)
 CPIPE_B200_REGISTER(cpipe_b200_desc_usm, "com.cpipe.sharpen.edge_aware_usm", kUsm, node_usm)

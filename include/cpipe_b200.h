@@ -109,6 +109,8 @@ CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_tone_filmic_rgb);            /* filmic_rgb_di
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_wb_greyworld_auto);
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_tone_aces_filmic);           /* aces_filmic_dispatch.cpp:17-31 */
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_tone_reinhard);              /* reinhard_dispatch.cpp:16-29 */
+/* Three inputs (under, normal, over), one output. */
+CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_tone_mertens_local);         /* mertens_local_dispatch.cpp:18-37 */
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_sharpen_edge_aware_usm);     /* edge_aware_usm_dispatch.cpp:18-31 */
 /* Scene-linear Rec.2020 to display encode (aot_id "cpipe_scene_linear_to_display",
  * blob cpipe_DisplayParams; RGBA16F in, RGBA8 unorm out for sRGB, RGBA16

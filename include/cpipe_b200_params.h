@@ -177,6 +177,13 @@ typedef struct {
     uint64_t neutral_out;
 } cpipe_GreyworldParams;
 
+/* tone.mertens_local (nodes/tone/mertens_local_dispatch.cpp:12-16). */
+typedef struct {
+    float weight_contrast;          /* 0..2 (node default 0) */
+    float weight_saturation;        /* 0..2 (1) */
+    float weight_well_exposedness;  /* 0..2 (1) */
+} cpipe_MertensLocalParams;
+
 /* tone.aces_filmic (nodes/tone/aces_filmic_dispatch.cpp:13-15). */
 typedef struct {
     int32_t enabled;   /* 0: pass-through */
@@ -262,6 +269,7 @@ CPIPE_STATIC_ASSERT(sizeof(cpipe_SurrogateHeader) == 32, "SurrogateHeader layout
 CPIPE_STATIC_ASSERT(sizeof(cpipe_AtrousWaveletParams) == 16, "AtrousWaveletParams layout");
 CPIPE_STATIC_ASSERT(sizeof(cpipe_EdgeAwareUsmParams) == 12, "EdgeAwareUsmParams layout");
 CPIPE_STATIC_ASSERT(sizeof(cpipe_AcesFilmicParams) == 4, "AcesFilmicParams layout");
+CPIPE_STATIC_ASSERT(sizeof(cpipe_MertensLocalParams) == 12, "MertensLocalParams layout");
 CPIPE_STATIC_ASSERT(sizeof(cpipe_GreyworldParams) == 8, "GreyworldParams layout");
 CPIPE_STATIC_ASSERT(sizeof(cpipe_ReinhardParams) == 4, "ReinhardParams layout");
 CPIPE_STATIC_ASSERT(sizeof(cpipe_DisplayParams) == 4, "DisplayParams layout");

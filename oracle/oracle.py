@@ -188,6 +188,14 @@ def guided(x, radius, eps, f16=True):
     return out
 
 
+def mertens(under, normal, over, wc=0.0, ws=1.0, we=1.0, f16=True):
+    u, n, o = _f32(under), _f32(normal), _f32(over)
+    out = np.empty_like(n)
+    lib().oracle_mertens(_p(u), _p(n), _p(o), _p(out), n.shape[1], n.shape[0], C.c_float(wc), C.c_float(ws),
+                         C.c_float(we), int(f16))
+    return out
+
+
 def aces(x, enabled=True, f16=True):
     x = _f32(x)
     out = np.empty_like(x)

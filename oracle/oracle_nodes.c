@@ -319,6 +319,40 @@ void oracle_reinhard(const float* in, float* out, int w, int h, float white_poin
         }
 }
 
+/* ---- tone.mertens_local (src/cpipe/nodes/tone/mertens_local_generator.cpp:22-115):
+ * the Halide generator's expression order, libm exp / sqrt / pow. */
+static float mertens_cew(float v) {
+    const float k = 2.0F * 0.20F * 0.20F;
+    const float d = v - 0.5F;
+    return expf(-(d * d) / k);
+}
+static float mertens_w(const float* f, float wc, float ws, float we) {
+    const float red = maxf(0.0F, f[0]), green = maxf(0.0F, f[1]), blue = maxf(0.0F, f[2]);
+    const float mean = ((f[0] + f[1]) + f[2]) / 3.0F;
+    const float sat = sqrtf(((((red - mean) * (red - mean)) + ((green - mean) * (green - mean))) +
+                             ((blue - mean) * (blue - mean))) / 3.0F + 0.0001F);
+    const float well = (mertens_cew(red) * mertens_cew(green)) * mertens_cew(blue);
+    const float contrast = fabsf(mean - 0.5F);
+    const float cf = wc == 0.0F ? 1.0F : powf(contrast + 0.01F, wc);
+    const float sf = ws == 1.0F ? sat + 0.01F : powf(sat + 0.01F, ws);
+    const float ef = we == 1.0F ? well : powf(well + 0.0001F, we);
+    return (cf * sf) * ef;
+}
+void oracle_mertens(const float* u, const float* n, const float* o, float* out, int w, int h, float wc, float ws,
+                    float we, int f16) {
+    const long count = (long)w * h;
+    for (long i = 0; i < count; ++i) {
+        const float* U = u + 4 * i;
+        const float* N = n + 4 * i;
+        const float* O = o + 4 * i;
+        const float wu = mertens_w(U, wc, ws, we), wn = mertens_w(N, wc, ws, we), wo = mertens_w(O, wc, ws, we);
+        const float total = maxf((wu + wn) + wo, 0.000001F);
+        for (int c = 0; c < 3; ++c)
+            out[4 * i + c] = rnd(clampf((((wu * U[c]) + (wn * N[c])) + (wo * O[c])) / total, 0.0F, 1.0F), f16);
+        out[4 * i + 3] = rnd(N[3], f16);
+    }
+}
+
 /* ---- sharpen.edge_aware_usm (src/cpipe/nodes/sharpen/edge_aware_usm_generator.cpp:11-75) ----
  * blur = mean3x3 (radius <= 1, explicit 9-term left-associated sum) or mean5x5
  * (0 + the 25 terms in row-major order), both over the clamped input;

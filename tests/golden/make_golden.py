@@ -25,7 +25,7 @@ FIXTURES = [
     "demosaic.rcd", "demosaic.amaze", "demosaic.quad_bayer_remosaic", "lens.dng_opcode_list_3",
     "wb.dual_illuminant", "colormatrix.dng_to_working", "denoise.bm3d", "denoise.guided_filter",
     "denoise.wavelet_bayes_shrink", "tone.filmic_rgb", "color.3d_lut", "sharpen.edge_aware_usm",
-    "tone.aces_filmic", "tone.reinhard", "wb.greyworld_auto",
+    "tone.aces_filmic", "tone.reinhard", "wb.greyworld_auto", "tone.mertens_local",
 ]
 
 
@@ -61,6 +61,12 @@ def main():
         subprocess.check_call([gen, out_root])
         for name in FIXTURES:
             d = os.path.join(out_root, name)
+            if name == "tone.mertens_local":  # an exposure stack: under / normal / over in
+                arrays = {k: read_raw(os.path.join(d, k + ".exr")) for k in ("under", "normal", "over")}
+                arrays["output"] = read_raw(os.path.join(d, "out.exr"))
+                np.savez(os.path.join(HERE, name + ".npz"), **arrays)
+                print("wrote", name, arrays["normal"].shape, arrays["output"].shape)
+                continue
             arrays = {"input": read_raw(os.path.join(d, "in.exr")),
                       "output": read_raw(os.path.join(d, "out.exr"))}
             if name == "color.3d_lut":

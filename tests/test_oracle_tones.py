@@ -26,3 +26,13 @@ def test_greyworld_oracle_matches_reference_golden():
     np.testing.assert_array_equal(out, g["output"])
     assert n[1] == 1.0
     assert oracle.greyworld(np.zeros((2, 2, 4), np.float32)) == (None, None)
+
+
+def test_mertens_oracle_matches_reference_golden():
+    """The golden generator multiplies the three weight factors in another
+    association than the Halide generator the oracle follows: within one f16 ulp."""
+    from parity import assert_f16_parity
+    g = golden("tone.mertens_local")
+    u, n, o = (g[k].astype(np.float16).astype(np.float32) for k in ("under", "normal", "over"))
+    out = oracle.mertens(u, n, o)
+    assert_f16_parity(out, g["output"], what="mertens golden")
