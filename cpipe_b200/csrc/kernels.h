@@ -34,7 +34,7 @@ cudaError_t launch_colormatrix(const Img& in, const Img& out, bool f16, const fl
 cudaError_t launch_filmic(const Img& in, const Img& out, bool f16, const FilmicDev& p, cudaStream_t st);
 // wb.greyworld_auto: per-block exact sums (d_partial: blocks x 4 int64, see
 // greyworld_sum_kernel), then v / n per RGB channel of an RGBA16F frame.
-constexpr int kGreyworldBlocks = 148 * 4;
+constexpr int kGreyworldBlocks = 148 * 8;
 cudaError_t launch_greyworld_sums(const Img& in, long long* d_partial, int blocks, cudaStream_t st);
 cudaError_t launch_greyworld_apply(const Img& in, const Img& out, const float n[3], cudaStream_t st);
 cudaError_t launch_mertens(const Img& under, const Img& normal, const Img& over, const Img& out, float wc, float ws,

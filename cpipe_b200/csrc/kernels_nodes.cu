@@ -656,13 +656,24 @@ __global__ void __launch_bounds__(256) greyworld_sum_kernel(Img in, long long* p
     const int y0 = (int)blockIdx.x * rows, y1 = min(in.h, y0 + rows);
     long long s0 = 0, s1 = 0, s2 = 0;
     int bad = 0;
-    for (int y = y0; y < y1; ++y)
-        for (int x = threadIdx.x; x < in.w; x += blockDim.x) {
+    for (int y = y0; y < y1; ++y) {
+        // pixel pairs as 16-byte loads (cached: the apply pass reads the frame again)
+        const __half* row = px<const __half>(in, 0, y);
+        const int pairs = in.pix_stride == 4 && al16(row) ? in.w / 2 : 0;
+#pragma unroll 4
+        for (int j = threadIdx.x; j < pairs; j += blockDim.x) {
+            const uint4 u = __ldg(reinterpret_cast<const uint4*>(row) + j);
+            s0 += h16_units(u.x & 0xFFFFU, &bad) + h16_units(u.z & 0xFFFFU, &bad);
+            s1 += h16_units(u.x >> 16, &bad) + h16_units(u.z >> 16, &bad);
+            s2 += h16_units(u.y & 0xFFFFU, &bad) + h16_units(u.w & 0xFFFFU, &bad);
+        }
+        for (int x = 2 * pairs + threadIdx.x; x < in.w; x += blockDim.x) {
             const uint2 u = *reinterpret_cast<const uint2*>(px<const __half>(in, x, y));
             s0 += h16_units(u.x & 0xFFFFU, &bad);
             s1 += h16_units(u.x >> 16, &bad);
             s2 += h16_units(u.y & 0xFFFFU, &bad);
         }
+    }
 #pragma unroll
     for (int off = 16; off > 0; off >>= 1) {
         s0 += __shfl_down_sync(0xFFFFFFFFU, s0, off);
