@@ -165,7 +165,8 @@ class ChainConfig(C.Structure):
                 ("spot_tiles", C.c_int32), ("spot_min_psnr_db", C.c_float), ("quad_bayer", C.c_int32),
                 ("guided_spec", C.c_int32), ("atrous_levels", C.c_int32), ("atrous_luma_strength", C.c_float),
                 ("sharpen", C.c_int32), ("sharpen_strength", C.c_float), ("sharpen_radius", C.c_int32),
-                ("sharpen_threshold", C.c_float), ("display", C.c_int32)]
+                ("sharpen_threshold", C.c_float), ("display", C.c_int32), ("tone", C.c_int32),
+                ("reinhard_white_point", C.c_float)]
 
 
 MAIN_ENTRY = C.CFUNCTYPE(C.c_int, C.c_char_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p, C.c_void_p)

@@ -98,6 +98,8 @@ class ChainConfig:
     sharpen_radius: int = 1
     sharpen_threshold: float = 0.0
     display: str = ""              # "" (RGBA16F output) | "sRGB" (RGBA8) | "BT2020-PQ" (RGBA16 unorm)
+    tone: str = "filmic"           # tone stage: filmic | aces | reinhard
+    reinhard_white_point: float = -1.0  # < 0: the reinhard node's unset value
 
     # ------------------------------------------------------------ workloads
     @classmethod
@@ -261,6 +263,8 @@ class ChainConfig:
         cfg.sharpen_radius = int(self.sharpen_radius)
         cfg.sharpen_threshold = float(self.sharpen_threshold)
         cfg.display = {"": 0, "sRGB": 1, "BT2020-PQ": 2}[self.display]
+        cfg.tone = {"filmic": 0, "aces": 1, "reinhard": 2}[self.tone]
+        cfg.reinhard_white_point = float(self.reinhard_white_point)
         return cfg, keep
 
 

@@ -108,6 +108,8 @@ struct ToneParams {
     float eps;
     float wavelet_th;
     FilmicDev filmic;
+    int tone_op;        // 0 tone.filmic_rgb, 1 tone.aces_filmic, 2 tone.reinhard
+    float reinhard_wp2; // white point squared (tone_op 2)
     const float4* lut;
     int lut_size, lut_interp;
     int has_lut;
@@ -281,7 +283,9 @@ __device__ __forceinline__ void denoise_tone_tile(const Img& in, const Img& out,
             v = wavelet_px(q, v, ox, oy, p.wavelet_th);
             v = Rgba{rnd<F16>(v.r), rnd<F16>(v.g), rnd<F16>(v.b), rnd<F16>(v.a)};
         }
-        v = filmic_px(v, p.filmic);
+        if (p.tone_op == 0) v = filmic_px(v, p.filmic);
+        else if (p.tone_op == 1) v = Rgba{aces_fit(v.r), aces_fit(v.g), aces_fit(v.b), v.a};
+        else v = Rgba{reinhard_px(v.r, p.reinhard_wp2), reinhard_px(v.g, p.reinhard_wp2), reinhard_px(v.b, p.reinhard_wp2), v.a};
         if (p.has_lut) {
             v = Rgba{rnd<F16>(v.r), rnd<F16>(v.g), rnd<F16>(v.b), v.a};
             v = lut_px(v, p.lut, p.lut_size, p.lut_interp);
@@ -782,6 +786,15 @@ cpipe_cuda_chain* cpipe_cuda_chain_create(const cpipe_cuda_chain_config* cfg, in
     c->tone.eps = cfg->guided_eps;
     c->tone.wavelet_th = 0.035F * cfg->wavelet_strength;
     c->tone.filmic = cpb_filmic_dev(&cfg->filmic);
+    // tone stage: filmic (default), or tone.aces_filmic / tone.reinhard with the
+    // reference nodes' parameter handling (Reinhard: unset -> 1e6, else 0.1..10)
+    if (cfg->tone < 0 || cfg->tone > 2) return fail(CPIPE_BAD_INDEX, c);
+    c->tone.tone_op = cfg->tone;
+    {
+        const float wp = cfg->reinhard_white_point < 0.0F ? 1000000.0F
+                                                           : std::clamp(cfg->reinhard_white_point, 0.1F, 10.0F);
+        c->tone.reinhard_wp2 = wp * wp;
+    }
     // scratch frames
     c->frame_bytes = (size_t)w * h * 4 * (c->f16 ? 2 : 4);
     // finishing stages (sharpen.edge_aware_usm, display encode): f16 form, whole chain

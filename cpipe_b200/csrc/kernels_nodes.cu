@@ -334,10 +334,6 @@ struct GreyOp {
 };
 // tone.aces_filmic (aces_filmic_generator.cpp:22-52): the Narkowicz 2016 fit
 // per RGB channel, alpha passes; enabled == 0 passes every channel.
-__device__ __forceinline__ float aces_fit(float v) {
-    v = max0(v);
-    return clampf((v * ((2.51F * v) + 0.03F)) / ((v * ((2.43F * v) + 0.59F)) + 0.14F), 0.0F, 1.0F);
-}
 template <class T>
 struct AcesOp {
     int enabled;
@@ -347,12 +343,7 @@ struct AcesOp {
         store_rgb_keep_alpha(d, o, s);
     }
 };
-// tone.reinhard (reinhard_generator.cpp:20-48): clamp(v (1 + v / wp^2) / (1 + v), 0, 1),
-// v = max(0, x), per RGB channel; alpha passes.
-__device__ __forceinline__ float reinhard_px(float x, float wp2) {
-    const float v = max0(x);
-    return clampf((v * (1.0F + (v / wp2))) / (1.0F + v), 0.0F, 1.0F);
-}
+// tone.reinhard (reinhard_generator.cpp:20-48): reinhard_px per RGB channel; alpha passes.
 template <class T>
 struct ReinhardOp {
     float wp2;

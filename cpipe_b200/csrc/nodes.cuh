@@ -142,6 +142,17 @@ __device__ __forceinline__ Rgba filmic_px(Rgba v, const FilmicDev& p) {
                 clampf(luma + ((t2 - luma) * p.saturation), 0.0F, 1.0F), v.a};
 }
 
+// tone.aces_filmic (aces_filmic_generator.cpp:22-31): the Narkowicz 2016 fit.
+__device__ __forceinline__ float aces_fit(float v) {
+    v = max0(v);
+    return clampf((v * ((2.51F * v) + 0.03F)) / ((v * ((2.43F * v) + 0.59F)) + 0.14F), 0.0F, 1.0F);
+}
+// tone.reinhard (reinhard_generator.cpp:22-28): clamp(v (1 + v / wp^2) / (1 + v), 0, 1), v = max(0, x).
+__device__ __forceinline__ float reinhard_px(float x, float wp2) {
+    const float v = max0(x);
+    return clampf((v * (1.0F + (v / wp2))) / (1.0F + v), 0.0F, 1.0F);
+}
+
 // lut3d_generator.cpp:49-138.  The LUT is stored as float4 (r,g,b,0) per cell,
 // cell index ((r*S + g)*S + b), blue fastest (reference color/lut3d_generator.cpp:83-86).
 __device__ __forceinline__ float add_delta(float base, float from, float to, float w) {

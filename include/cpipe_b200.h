@@ -290,6 +290,11 @@ typedef struct {
     int32_t sharpen_radius;
     float sharpen_threshold;
     int32_t display;
+    /* Tone node in the tone stage: 0 = tone.filmic_rgb (`filmic` params),
+     * 1 = tone.aces_filmic, 2 = tone.reinhard (reinhard_white_point < 0: the
+     * node's unset value 1e6; else clamped to 0.1..10). */
+    int32_t tone;
+    float reinhard_white_point;
 } cpipe_cuda_chain_config;
 
 typedef struct cpipe_cuda_chain cpipe_cuda_chain;

@@ -59,7 +59,13 @@ def run_nodes_on_gpu(host, cfg, raw):
                        "chroma_strength": cfg.wavelet_strength if cfg.wavelet_strength >= 0 else 1.0}))
     elif cfg.wavelet_strength >= 0:
         steps.append(("com.cpipe.denoise.wavelet_bayes_shrink", F16, {"chroma_strength": cfg.wavelet_strength}))
-    steps.append(("com.cpipe.tone.filmic_rgb", F16, {}))
+    if cfg.tone == "aces":
+        steps.append(("com.cpipe.tone.aces_filmic", F16, {}))
+    elif cfg.tone == "reinhard":
+        steps.append(("com.cpipe.tone.reinhard", F16, {} if cfg.reinhard_white_point < 0 else
+                      {"white_point": cfg.reinhard_white_point}))
+    else:
+        steps.append(("com.cpipe.tone.filmic_rgb", F16, {}))
     tmp = None
     if "lut" in b:
         tmp = tempfile.NamedTemporaryFile(suffix=".cube", delete=False)
@@ -320,3 +326,17 @@ def test_chain_finishing_stage_refusals(cuda_device):
         Chain(ChainConfig.full_12mp(width=64, height=64, display="sRGB", plain_f32=True))
     with pytest.raises(Exception):
         Chain(ChainConfig.full_12mp(width=64, height=64, sharpen=True, stop_after=1))
+
+
+@pytest.mark.parametrize("kw", [dict(tone="aces"), dict(tone="reinhard"), dict(tone="reinhard", reinhard_white_point=2.5),
+                                dict(tone="aces", sharpen=True, display="sRGB")])
+def test_chain_tone_choice_equals_nodes(host, kw):
+    """The tone stage with tone.aces_filmic or tone.reinhard in place of filmic
+    returns, bit for bit, what those nodes return in the node-by-node chain."""
+    cfg = ChainConfig.full_12mp(width=160, height=112, **kw)
+    raw = cfg.make_raw()
+    chain = Chain(cfg)
+    got = chain.run_host(raw)
+    chain.close()
+    want = run_nodes_on_gpu(host, cfg, raw)
+    np.testing.assert_array_equal(got.view(np.uint8), want.view(np.uint8))
