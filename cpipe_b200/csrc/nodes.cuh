@@ -361,6 +361,17 @@ __device__ __forceinline__ Rgba warp_sample(const Img& in, const WarpDev& w, con
     const int ix = ff_floor(sx), iy = ff_floor(sy);
     const float tx = ff_frac(sx, ix), ty = ff_frac(sy, iy);
     Rgba rows[4];
+    if (ix >= 1 && ix + 2 < in.w && iy >= 1 && iy + 2 < in.h) {
+        // the 4x4 footprint lies inside the frame: the same taps without clamping
+        const T* base = px<const T>(in, ix - 1, iy - 1);
+        const long long ps = in.pix_stride;
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+            const T* row = base + (long long)r * in.row_stride;
+            rows[r] = cubic4(load_rgba(row), load_rgba(row + ps), load_rgba(row + 2 * ps), load_rgba(row + 3 * ps), tx);
+        }
+        return cubic4(rows[0], rows[1], rows[2], rows[3], ty);
+    }
 #pragma unroll
     for (int r = 0; r < 4; ++r) {
         const int yy = iy + r - 1;
