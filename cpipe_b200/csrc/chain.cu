@@ -63,12 +63,38 @@ struct ColorParams {
     float cm[9];
 };
 
-template <class T, bool F16, bool WARP>
+// A single warp's bicubic taps for every output pixel, computed once when the
+// chain is made (warp_taps_kernel; the same warp_tap as the inline path):
+// ixy = ix | iy << 16, tx, ty; n = w * h entries each.
+struct WarpTaps {
+    const uint32_t* ixy;
+    const float* tx;
+    const float* ty;
+};
+__global__ void __launch_bounds__(256) warp_taps_kernel(int w, int h, WarpDev wd, uint32_t* ixy, float* tx, float* ty) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
+    if (x >= w || y >= h) return;
+    const WarpTap t = warp_tap_px(wd, x, y);
+    const size_t i = (size_t)y * w + x;
+    ixy[i] = (uint32_t)t.ix | ((uint32_t)t.iy << 16);
+    tx[i] = t.tx;
+    ty[i] = t.ty;
+}
+
+// WARP 0: no warp; 1: the warp evaluated per pixel; 2: read from the tap table.
+template <class T, bool F16, int WARP>
 __device__ __forceinline__ void warp_wb_cm_px(const Img& in, const Img& out, const WarpDev& w, const ColorParams& cp,
-                                              int x, int y) {
+                                              int x, int y, const WarpTaps& taps = WarpTaps{}) {
     Rgba v;
-    if (WARP) {
-        const Rgba wv = warp_px<T>(in, w, x, y);
+    if (WARP != 0) {
+        Rgba wv;
+        if (WARP == 2) {
+            const size_t i = (size_t)y * out.w + x;
+            const uint32_t p = __ldg(taps.ixy + i);
+            wv = bicubic_at<T>(in, WarpTap{(int)(p & 0xFFFFU), (int)(p >> 16), __ldg(taps.tx + i), __ldg(taps.ty + i)});
+        } else {
+            wv = warp_px<T>(in, w, x, y);
+        }
         v = Rgba{rnd<F16>(wv.r), rnd<F16>(wv.g), rnd<F16>(wv.b), rnd<F16>(wv.a)};
     } else {
         v = load_rgba(px<const T>(in, x, y));
@@ -79,11 +105,11 @@ __device__ __forceinline__ void warp_wb_cm_px(const Img& in, const Img& out, con
     store_rgba(px<T>(out, x, y), Rgba{c.r, c.g, c.b, v.a});
 }
 
-template <class T, bool F16, bool WARP>
-__global__ void __launch_bounds__(128) warp_wb_cm_kernel(Img in, Img out, WarpDev w, ColorParams cp) {
+template <class T, bool F16, int WARP>
+__global__ void __launch_bounds__(128) warp_wb_cm_kernel(Img in, Img out, WarpDev w, ColorParams cp, WarpTaps taps) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     if (x >= out.w) return;
-    warp_wb_cm_px<T, F16, WARP>(in, out, w, cp, x, y);
+    warp_wb_cm_px<T, F16, WARP>(in, out, w, cp, x, y, taps);
 }
 
 // ------------------------------------------------------------------ K3
@@ -384,6 +410,10 @@ struct cpipe_cuda_chain {
     ToneParams tone{};
     WarpDev warp{};
     int warp_mode = 0;  // 0 none, 1 fused single warp, 2 general OpcodeList3 list
+    // single warp with one coefficient set: its per-pixel bicubic taps (WarpTaps)
+    uint32_t* d_taps_ixy = nullptr;
+    float* d_taps_tx = nullptr;
+    float* d_taps_ty = nullptr;
     std::vector<unsigned char> opcode3_blob;
     Opcode3View opcode3{};
     int radius = 2;
@@ -495,12 +525,16 @@ int launch_chain(cpipe_cuda_chain* c, const void* d_raw, size_t raw_pitch, void*
     }
     const dim3 gb((unsigned)((w + 127) / 128), (unsigned)h);
     Img k2_out = c->stop_after == 1 ? out : (c->warp_mode == 2) ? mid0 : mid1;
-    if (c->warp_mode == 1) {
-        if (c->f16) warp_wb_cm_kernel<__half, true, true><<<gb, 128, 0, st>>>(k2_in, k2_out, c->warp, c->color);
-        else warp_wb_cm_kernel<float, false, true><<<gb, 128, 0, st>>>(k2_in, k2_out, c->warp, c->color);
+    const WarpTaps taps{c->d_taps_ixy, c->d_taps_tx, c->d_taps_ty};
+    if (c->warp_mode == 1 && c->d_taps_ixy) {
+        if (c->f16) warp_wb_cm_kernel<__half, true, 2><<<gb, 128, 0, st>>>(k2_in, k2_out, c->warp, c->color, taps);
+        else warp_wb_cm_kernel<float, false, 2><<<gb, 128, 0, st>>>(k2_in, k2_out, c->warp, c->color, taps);
+    } else if (c->warp_mode == 1) {
+        if (c->f16) warp_wb_cm_kernel<__half, true, 1><<<gb, 128, 0, st>>>(k2_in, k2_out, c->warp, c->color, taps);
+        else warp_wb_cm_kernel<float, false, 1><<<gb, 128, 0, st>>>(k2_in, k2_out, c->warp, c->color, taps);
     } else {
-        if (c->f16) warp_wb_cm_kernel<__half, true, false><<<gb, 128, 0, st>>>(k2_in, k2_out, c->warp, c->color);
-        else warp_wb_cm_kernel<float, false, false><<<gb, 128, 0, st>>>(k2_in, k2_out, c->warp, c->color);
+        if (c->f16) warp_wb_cm_kernel<__half, true, 0><<<gb, 128, 0, st>>>(k2_in, k2_out, c->warp, c->color, taps);
+        else warp_wb_cm_kernel<float, false, 0><<<gb, 128, 0, st>>>(k2_in, k2_out, c->warp, c->color, taps);
     }
     if (ev) cudaEventRecord(ev[2], st);
     if (c->stop_after == 1) {
@@ -697,6 +731,19 @@ cpipe_cuda_chain* cpipe_cuda_chain_create(const cpipe_cuda_chain_config* cfg, in
         }
         if (applied == 1 && warps == 1) c->warp_mode = cpb_warp_dev(warp_rec, w, h, &c->warp) == CPIPE_OK ? 1 : 0;
         else if (applied > 0) c->warp_mode = 2;
+        // the frame geometry is fixed per chain: a single warp's taps are
+        // computed once here and read by K2 (12 bytes per pixel)
+        if (c->warp_mode == 1 && c->warp.count == 1 && w <= 65535 && h <= 65535) {
+            const size_t n = (size_t)w * h;
+            if (cudaMalloc(&c->d_taps_ixy, n * sizeof(uint32_t)) != cudaSuccess ||
+                cudaMalloc(&c->d_taps_tx, n * sizeof(float)) != cudaSuccess ||
+                cudaMalloc(&c->d_taps_ty, n * sizeof(float)) != cudaSuccess)
+                return fail(CPIPE_OOM, c);
+            const dim3 g((unsigned)((w + 255) / 256), (unsigned)h);
+            warp_taps_kernel<<<g, 256>>>(w, h, c->warp, c->d_taps_ixy, c->d_taps_tx, c->d_taps_ty);
+            if (cudaGetLastError() != cudaSuccess || cudaStreamSynchronize(nullptr) != cudaSuccess)
+                return fail(CPIPE_INTERNAL_ERROR, c);
+        }
     }
     // colour, denoise, tone
     std::memcpy(c->color.neutral, cfg->as_shot_neutral, sizeof(c->color.neutral));
@@ -833,6 +880,9 @@ void cpipe_cuda_chain_destroy(cpipe_cuda_chain* c) {
     if (c->s_h2d) cudaStreamDestroy(c->s_h2d);
     if (c->s_d2h) cudaStreamDestroy(c->s_d2h);
     cudaFree(c->d_tables);
+    cudaFree(c->d_taps_ixy);
+    cudaFree(c->d_taps_tx);
+    cudaFree(c->d_taps_ty);
     cudaFree(c->d_denoise);
     cudaFree(c->d_bayer);
     cudaFree(c->d_ab);

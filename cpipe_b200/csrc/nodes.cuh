@@ -351,15 +351,26 @@ __device__ __forceinline__ ff ff_clamp0(ff v, float maxv) {
     return v;
 }
 
-template <class T>
-__device__ __forceinline__ Rgba warp_sample(const Img& in, const WarpDev& w, const WarpCoefDev& k, float x, float y,
-                                            ff X, ff Y, ff q, ff r2) {
+// Bicubic source position of an output pixel: the 4x4 footprint's origin + 1
+// and the two fractions.
+struct WarpTap {
+    int ix, iy;
+    float tx, ty;
+};
+__device__ __forceinline__ WarpTap warp_tap(const WarpDev& w, const WarpCoefDev& k, float x, float y, ff X, ff Y, ff q,
+                                            ff r2) {
     ff sx, sy;
     warp_src(k, x, y, X, Y, q, r2, &sx, &sy);
     sx = ff_clamp0(sx, w.xmax);
     sy = ff_clamp0(sy, w.ymax);
     const int ix = ff_floor(sx), iy = ff_floor(sy);
-    const float tx = ff_frac(sx, ix), ty = ff_frac(sy, iy);
+    return WarpTap{ix, iy, ff_frac(sx, ix), ff_frac(sy, iy)};
+}
+// Catmull-Rom sample (all four channels) at a tap, clamped reads (sample_bicubic :55-73).
+template <class T>
+__device__ __forceinline__ Rgba bicubic_at(const Img& in, const WarpTap& t) {
+    const int ix = t.ix, iy = t.iy;
+    const float tx = t.tx, ty = t.ty;
     Rgba rows[4];
     if (ix >= 1 && ix + 2 < in.w && iy >= 1 && iy + 2 < in.h) {
         // the 4x4 footprint lies inside the frame: the same taps without clamping
@@ -379,6 +390,19 @@ __device__ __forceinline__ Rgba warp_sample(const Img& in, const WarpDev& w, con
                          load_clamped<T>(in, ix + 2, yy), tx);
     }
     return cubic4(rows[0], rows[1], rows[2], rows[3], ty);
+}
+template <class T>
+__device__ __forceinline__ Rgba warp_sample(const Img& in, const WarpDev& w, const WarpCoefDev& k, float x, float y,
+                                            ff X, ff Y, ff q, ff r2) {
+    return bicubic_at<T>(in, warp_tap(w, k, x, y, X, Y, q, r2));
+}
+// The tap of output pixel (x, y) for coefficient set 0 (the whole pixel when count == 1).
+__device__ __forceinline__ WarpTap warp_tap_px(const WarpDev& w, int x, int y) {
+    const float fx = (float)x, fy = (float)y;
+    const ff X = ff_add_f(ff_neg(w.cx), fx), Y = ff_add_f(ff_neg(w.cy), fy);
+    const ff q = ff_add(ff_mul(X, X), ff_mul(Y, Y));
+    const ff r2 = ff_mul(q, w.inv_m2);
+    return warp_tap(w, w.k[0], fx, fy, X, Y, q, r2);
 }
 
 // Warp output pixel (x, y), all channels (channel c uses coefficient set min(c, count-1)).
