@@ -38,9 +38,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 # bound: "hbm" -- a point or small-stencil node whose floor is its bytes;
 # "issue" -- the reference's per-pixel arithmetic (RCD/AMaZE ratios, the QBC
 # 25-tap integer weights, the guided filter's exact-order box sums, the warp's
-# float-float coordinates and bicubic taps, filmic's log per channel) sets the
-# floor (the PQ encode: two powf per channel); "gather" -- 3D LUT cell reads
-# through L1/L2.
+# float-float coordinates and bicubic taps, filmic's log per channel, USM's
+# exact-order sums and divisions, the PQ encode's two powers per channel) sets
+# the floor; "gather" -- 3D LUT cell reads through L1/L2.
 NODES = [
     ("a1 precision_convert", "precision_convert_r16u_to_f32", "u16", "f32", 6, None, "hbm"),
     ("a2 linearize", "linearize_dng_lut", "u16", "f32", 6, "linearize", "hbm"),
@@ -61,7 +61,7 @@ NODES = [
     ("wb.greyworld_auto (sum + apply)", "cpipe_wb_greyworld_auto", "rgba", "rgba", 16, "greyworld", "hbm"),
     ("tone.aces_filmic", "tone_aces_filmic", "rgba", "rgba", 16, "aces", "hbm"),
     ("tone.reinhard", "tone_reinhard", "rgba", "rgba", 16, "reinhard", "hbm"),
-    ("sharpen.edge_aware_usm (3x3)", "sharpen_edge_aware_usm", "rgba", "rgba", 16, "usm", "hbm"),
+    ("sharpen.edge_aware_usm (3x3)", "sharpen_edge_aware_usm", "rgba", "rgba", 16, "usm", "issue"),
     ("scene_linear_to_display sRGB", "cpipe_scene_linear_to_display", "rgba", "rgba8", 12, "display_srgb", "hbm"),
     ("scene_linear_to_display PQ", "cpipe_scene_linear_to_display", "rgba", "rgba16u", 16, "display_pq", "issue"),
 ]
