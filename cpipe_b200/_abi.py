@@ -200,7 +200,7 @@ EXPORTS = [
     "cpipe_cuda_denoise_guided_filter",
     "cpipe_cuda_denoise_wavelet_bayes_shrink", "cpipe_cuda_lens_dng_opcode_list_3", "cpipe_cuda_color_3d_lut",
     "cpipe_cuda_tone_filmic_rgb", "cpipe_cuda_tone_aces_filmic", "cpipe_cuda_tone_reinhard",
-    "cpipe_cuda_wb_greyworld_auto", "cpipe_cuda_tone_mertens_local",
+    "cpipe_cuda_wb_greyworld_auto", "cpipe_cuda_tone_mertens_local", "cpipe_cuda_selftest_const_division",
     "cpipe_cuda_sharpen_edge_aware_usm", "cpipe_cuda_scene_linear_to_display",
     "cpipe_cuda_copy", "cpipe_cuda_filters", "cpipe_cuda_find_filter",
     "cpipe_cuda_color_3d_lut_noalloc",
@@ -279,6 +279,7 @@ def lib():
         "cpipe_b200_load_lut": (i32, [cp, C.POINTER(u32), vp, sz]),
         "cpipe_cuda_chain_create": (vp, [C.POINTER(ChainConfig), C.POINTER(i32)]),
         "cpipe_cuda_chain_destroy": (None, [vp]), "cpipe_cuda_chain_output_bytes": (sz, [vp]),
+        "cpipe_cuda_selftest_const_division": (i32, [C.c_float, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
         "cpipe_cuda_chain_run": (i32, [vp, vp, vp, vp]), "cpipe_cuda_chain_run_host": (i32, [vp, vp, vp, vp]),
         "cpipe_cuda_chain_run_host_frames": (i32, [vp, vp, vp, i32, vp]),
         "cpipe_cuda_pinned_alloc": (i32, [sz, C.POINTER(vp)]), "cpipe_cuda_pinned_free": (None, [vp]),

@@ -225,6 +225,7 @@ __device__ __forceinline__ void denoise_tone_tile(const Img& in, const Img& out,
     }
     __syncthreads();
     constexpr float N = (float)(D * D);
+    const ConstDiv cN{N, (float)(1.0 / (double)(D * D))};  // IEEE x / N (const_div)
     if (R == 0) {  // no guided node: the wavelet reads the BM3D output
         for (int i = threadIdx.x; i < 3 * kCTW * kCTH; i += blockDim.x) {
             const int c = i / (kCTW * kCTH);
@@ -254,7 +255,7 @@ __device__ __forceinline__ void denoise_tone_tile(const Img& in, const Img& out,
             for (int k = 0; k < kCG; ++k) {
                 if (ty0 + k >= AH) break;
                 const float2 sums = box_chain2<D>(win, k);
-                const float m = sums.x / N, corr = sums.y / N;
+                const float m = const_div(sums.x, cN), corr = const_div(sums.y, cN);
                 const float var = max0(corr - (m * m));
                 const float a = var / (var + p.eps);
                 const int j = c * AB + (ty0 + k) * AP + tx;
@@ -282,7 +283,7 @@ __device__ __forceinline__ void denoise_tone_tile(const Img& in, const Img& out,
                 const int ty = ty0 + k;
                 const float2 sab = box_chain2<D>(win, k);
                 const float v = s_bm[c * CP * CH + (ty + H) * CP + (tx + H)];
-                s_gf[c * kCTW * kCTH + ty * kCTW + tx] = rnd<F16>(max0(((sab.x / N) * v) + (sab.y / N)));
+                s_gf[c * kCTW * kCTH + ty * kCTW + tx] = rnd<F16>(max0((const_div(sab.x, cN) * v) + const_div(sab.y, cN)));
             }
         }
     }

@@ -460,6 +460,7 @@ __global__ void __launch_bounds__(256, 3) guided_kernel(Img in, Img out, float e
     }
     __syncthreads();
     constexpr float N = (float)(D * D);
+    const ConstDiv cN{N, (float)(1.0 / (double)(D * D))};  // IEEE x / N (const_div)
     constexpr int AG = (AH + kGfG - 1) / kGfG;
     for (int item = threadIdx.x; item < 3 * AW * AG; item += blockDim.x) {
         const int c = item / (AW * AG);
@@ -479,7 +480,7 @@ __global__ void __launch_bounds__(256, 3) guided_kernel(Img in, Img out, float e
         for (int k = 0; k < kGfG; ++k) {
             if (ty0 + k >= AH) break;
             const float2 sums = box_chain2<D>(win, k);
-            const float m = sums.x / N, corr = sums.y / N;
+            const float m = const_div(sums.x, cN), corr = const_div(sums.y, cN);
             const float var = max0(corr - (m * m));
             const float a = var / (var + eps);
             const int j = c * AP * AH + (ty0 + k) * AP + tx;
@@ -506,7 +507,7 @@ __global__ void __launch_bounds__(256, 3) guided_kernel(Img in, Img out, float e
             for (int k = 0; k < kGfG; ++k) {
                 const float2 sab = box_chain2<D>(win, k);
                 const float v = s_v[c * IP * IH + (ty0 + k + H) * IP + (tx + H)];
-                o[c][k] = max0(((sab.x / N) * v) + (sab.y / N));
+                o[c][k] = max0((const_div(sab.x, cN) * v) + const_div(sab.y, cN));
             }
         }
         const int x = x0 + tx;
@@ -739,6 +740,7 @@ __global__ void __launch_bounds__(256) usm_kernel(Img in, Img out, float strengt
     __syncthreads();
     const int tx = threadIdx.x & (kUsmTW - 1), ty0 = (threadIdx.x / kUsmTW) * G;
     constexpr float N = (float)(D * D);
+    const ConstDiv cN{N, (float)(1.0 / (double)(D * D))};  // IEEE x / N (const_div)
     float o[3][G];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -750,7 +752,7 @@ __global__ void __launch_bounds__(256) usm_kernel(Img in, Img out, float strengt
             for (int dx = 0; dx < D; ++dx) win[r][dx] = V[r * IP + dx];
 #pragma unroll
         for (int k = 0; k < G; ++k) {
-            const float blur = usm_box<D>(win, k) / N;
+            const float blur = const_div(usm_box<D>(win, k), cN);
             const float val = win[k + R][R];
             const float mask = val - blur;
             const float sh = fabsf(mask) >= threshold ? val + (strength * mask) : val;

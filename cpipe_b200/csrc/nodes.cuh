@@ -116,6 +116,28 @@ __device__ __forceinline__ Rgba cm_px(Rgba v, const float t[9]) {
                 t[6] * v.r + t[7] * v.g + t[8] * v.b, v.a};
 }
 
+// x / d for a divisor fixed per launch, by Markstein's method (P. Markstein,
+// "Computation of elementary functions on the IBM RISC System/6000
+// processor", IBM J. Res. Dev. 34(1), 1990): with inv = RN(1/d), q0 = RN(x inv),
+// the exact remainder r = x - q0 d (one FMA) and q = RN(q0 + r inv) (one FMA).
+// Used only where |x| lies in [2^-90, 2^126] (ConstDiv::ok); the library's
+// self-test (cpipe_cuda_selftest_const_division) compares it with IEEE
+// division on every binary32 in that range for each divisor the kernels use
+// (the box sizes 9 and 25).
+struct ConstDiv {
+    float d, inv;  // inv = 1/d rounded to nearest (computed on the host in double)
+};
+__device__ __forceinline__ bool const_div_ok(float x) {
+    const float a = fabsf(x);
+    return a >= 0x1p-90F && a <= 0x1p126F;
+}
+__device__ __forceinline__ float const_div(float x, const ConstDiv& c) {
+    if (!const_div_ok(x)) return x / c.d;
+    const float q0 = __fmul_rn(x, c.inv);
+    const float r = __fmaf_rn(-q0, c.d, x);
+    return __fmaf_rn(r, c.inv, q0);
+}
+
 // filmic_rgb_generator.cpp:22-36,57-70.  exposure = pow(2, ev) and
 // inv_contrast = 1/contrast are computed once per launch on the host with the
 // same float operations; log_white = log(109) is the generator's constant.

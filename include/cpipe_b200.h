@@ -388,6 +388,12 @@ int cpipe_cuda_batch_autotune(cpipe_cuda_batch* batch, const void* const* d_raw,
 /* Frame i's single-frame chain (the same node parameters; for per-frame runs). */
 cpipe_cuda_chain* cpipe_cuda_batch_frame_chain(cpipe_cuda_batch* batch, size_t i);
 
+/* Self-test of the division by a fixed divisor the kernels use in place of
+ * IEEE division (Markstein's method, nodes.cuh const_div): compares it with
+ * IEEE division on every binary32 in its range for `divisor`; no reference
+ * counterpart. */
+int cpipe_cuda_selftest_const_division(float divisor, uint64_t* mismatches, uint64_t* checked);
+
 /* Device memory, streams and events for callers without their own CUDA runtime. */
 int cpipe_cuda_set_device(int device);
 int cpipe_cuda_device_alloc(size_t bytes, void** out);
