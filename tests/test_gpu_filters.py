@@ -250,3 +250,40 @@ def test_prepared_table_cache(cuda_device):
     for i in (0, 1, 2, 1, 0):
         out = run("color_3d_lut", [x], [np.zeros_like(x)], blobs.lut3d(S, luts[i], 0))
         assert_f16_parity(out, oracle.lut3d(x.astype(np.float32), luts[i], S, 0, True), what=f"lut {i}")
+
+
+def test_prepared_table_cache_concurrent_callers(cuda_device):
+    """Two host threads call the LUT and linearize filters at once with their
+    own tables (more distinct blobs than the cache holds): each result must be
+    its own table's."""
+    import threading
+    r = np.random.default_rng(71)
+    S = 9
+    x = rgba(73, 17, 23, -0.1, 1.1)
+    raw = r.integers(0, 4096, size=(19, 21), dtype=np.uint16)
+    jobs = []
+    for t in range(2):
+        luts = [r.uniform(0.0, 1.0, size=(S, S, S, 3)).astype(np.float32) for _ in range(5)]
+        tables = [np.sort(r.integers(0, 65535, size=4096)).astype(np.uint16) for _ in range(5)]
+        jobs.append((luts, tables))
+    errors = []
+
+    def worker(luts, tables):
+        try:
+            for rep in range(4):
+                for i in range(5):
+                    out = np.zeros_like(x)
+                    assert call_filter("color_3d_lut", [x], [out], blobs.lut3d(S, luts[i], 0)) == 0, last_error()
+                    assert_f16_parity(out, oracle.lut3d(x.astype(np.float32), luts[i], S, 0, True), what="lut")
+                    lin = np.zeros(raw.shape, np.float32)
+                    assert call_filter("linearize_dng_lut", [raw], [lin], blobs.linearize(tables[i])) == 0
+                    np.testing.assert_array_equal(lin, oracle.linearize(raw, tables[i])[1])
+        except Exception as e:  # reported below
+            errors.append(e)
+
+    threads = [threading.Thread(target=worker, args=job) for job in jobs]
+    for th in threads:
+        th.start()
+    for th in threads:
+        th.join()
+    assert not errors, errors
