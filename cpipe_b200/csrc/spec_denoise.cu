@@ -34,12 +34,12 @@
 //                        variance does not cancel), a and b on the tile plus r,
 //                        separable box sums of a and b, the output.
 //   atrous_prep_kernel   RGBA -> Y, Co, Cg planes (FP32).
-//   atrous_level_kernel  one level for all channels: a 64x32 tile; per
-//                        channel the input rows with a 2 * 2^j halo both ways
-//                        staged in shared memory (one coalesced pass), the
-//                        horizontal pass into a second buffer, the vertical
-//                        pass from there; writes c_{j+1} and w_{j+1} and the
-//                        tile's sum of w^2 per channel.
+//   atrous_h_kernel      one level's horizontal B3 pass of all three planes
+//                        into a scratch plane set (taps 2^j apart, clamped).
+//   atrous_v_kernel      per 64x32 tile: the vertical pass from the scratch
+//                        planes, c_{j+1} and w_{j+1}, the tile's sum of w^2
+//                        per channel (no halo staging: the taps come through
+//                        L1 / L2).
 //   atrous_thresh_kernel per (level, channel): the tiles' sums added in a fixed
 //                        order (FP64), the BayesShrink threshold.
 //   atrous_recon_kernel  shrink, sum, inverse colour transform.
@@ -200,13 +200,6 @@ __global__ void __launch_bounds__(kGsThreads) guided_spec_kernel(Img in, Img out
 // ----------------------------------------------------------------- a-trous
 constexpr int kAtTW = 64, kAtTH = 32, kAtThreads = 256;
 
-// per channel: the input rows of the tile with a 2s halo both ways, then the
-// horizontally filtered rows
-__host__ __device__ inline size_t at_smem(int s) {
-    const size_t hr = kAtTH + 4 * s;
-    return sizeof(float) * (hr * (kAtTW + 4 * s) + hr * kAtTW);
-}
-
 template <class T>
 __global__ void atrous_prep_kernel(Img in, float* __restrict__ c0, long long npx) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
@@ -222,43 +215,43 @@ __device__ __forceinline__ float b3(float a, float b, float c, float d, float e)
     return 0.0625F * (a + e) + 0.25F * (b + d) + 0.375F * c;
 }
 
-__global__ void __launch_bounds__(kAtThreads) atrous_level_kernel(const float* __restrict__ cin, float* __restrict__ cout,
-                                                                  float* __restrict__ wout, float* __restrict__ part,
-                                                                  int w, int h, long long npx, int s) {
-    extern __shared__ float sm[];
-    const int TH = kAtTH;
-    const int x0 = blockIdx.x * kAtTW, y0 = blockIdx.y * TH, HR = TH + 4 * s, IWd = kAtTW + 4 * s;
-    float* s_in = sm;             // [HR][IWd]: rows y0-2s.., columns x0-2s.. (clamped)
-    float* s_h = sm + HR * IWd;   // [HR][kAtTW]: filtered along rows
+// One level in two passes over frame-wide planes (no halo staging): the
+// horizontal B3 pass of each channel's rows into tmp, then, per 64x32 tile,
+// the vertical pass, c_{j+1}, w_{j+1} = c_j - c_{j+1} and the tile's sum of
+// w^2 per channel.  Taps clamp at the frame edges; the pixel-to-thread mapping
+// of the vertical pass fixes the order of each tile's sum.
+__global__ void __launch_bounds__(kAtThreads) atrous_h_kernel(const float* __restrict__ cin, float* __restrict__ tmp,
+                                                              int w, long long npx, int s) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, c = blockIdx.z;
+    if (x >= w) return;
+    const float* row = cin + c * npx + (long long)y * w;
+    tmp[c * npx + (long long)y * w + x] = b3(__ldg(row + clampi(x - 2 * s, 0, w - 1)), __ldg(row + clampi(x - s, 0, w - 1)),
+                                             __ldg(row + x), __ldg(row + clampi(x + s, 0, w - 1)),
+                                             __ldg(row + clampi(x + 2 * s, 0, w - 1)));
+}
+__global__ void __launch_bounds__(kAtThreads) atrous_v_kernel(const float* __restrict__ cin, const float* __restrict__ tmp,
+                                                              float* __restrict__ cout, float* __restrict__ wout,
+                                                              float* __restrict__ part, int w, int h, long long npx,
+                                                              int s) {
+    const int x0 = blockIdx.x * kAtTW, y0 = blockIdx.y * kAtTH;
     float acc[3] = {0.0F, 0.0F, 0.0F};
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        const float* plane = cin + c * npx;
-        for (int i = threadIdx.x; i < HR * IWd; i += blockDim.x) {
-            const int r = i / IWd, xx = i - r * IWd;
-            const int y = clampi(y0 - 2 * s + r, 0, h - 1), x = clampi(x0 - 2 * s + xx, 0, w - 1);
-            s_in[i] = plane[(long long)y * w + x];
-        }
-        __syncthreads();
-        for (int i = threadIdx.x; i < HR * kAtTW; i += blockDim.x) {
-            const int r = i / kAtTW, xx = i - r * kAtTW;
-            const float* row = s_in + r * IWd + xx + 2 * s;
-            s_h[i] = b3(row[-2 * s], row[-s], row[0], row[s], row[2 * s]);
-        }
-        __syncthreads();
-        for (int i = threadIdx.x; i < TH * kAtTW; i += blockDim.x) {
+        const float* t = tmp + c * npx;
+        for (int i = threadIdx.x; i < kAtTH * kAtTW; i += kAtThreads) {
             const int r = i / kAtTW, xx = i - r * kAtTW;
             const int x = x0 + xx, y = y0 + r;
             if (x >= w || y >= h) continue;
-            const float* col = s_h + (r + 2 * s) * kAtTW + xx;
-            const float v = b3(col[-2 * s * kAtTW], col[-s * kAtTW], col[0], col[s * kAtTW], col[2 * s * kAtTW]);
+            const float v = b3(__ldg(t + (long long)clampi(y - 2 * s, 0, h - 1) * w + x),
+                               __ldg(t + (long long)clampi(y - s, 0, h - 1) * w + x), __ldg(t + (long long)y * w + x),
+                               __ldg(t + (long long)clampi(y + s, 0, h - 1) * w + x),
+                               __ldg(t + (long long)clampi(y + 2 * s, 0, h - 1) * w + x));
             const long long o = c * npx + (long long)y * w + x;
-            const float d = s_in[(r + 2 * s) * IWd + xx + 2 * s] - v;
+            const float d = __ldg(cin + o) - v;
             cout[o] = v;
             wout[o] = d;
             acc[c] += d * d;
         }
-        __syncthreads();
     }
     __shared__ float red[kAtThreads / 32][3];
 #pragma unroll
@@ -404,6 +397,8 @@ int atrous_plan(const cpipe_AtrousWaveletParams* p, int w, int h, AtrousPlan* ou
     o = align256(o + plane3);
     q.off_c1 = o;
     o = align256(o + plane3);
+    q.off_tmp = o;
+    o = align256(o + plane3);
     q.off_w = o;
     o = align256(o + (size_t)q.levels * plane3);
     q.off_part = o;
@@ -414,10 +409,7 @@ int atrous_plan(const cpipe_AtrousWaveletParams* p, int w, int h, AtrousPlan* ou
     return CPIPE_OK;
 }
 
-cudaError_t atrous_setup() {
-    return cudaFuncSetAttribute(atrous_level_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)at_smem(1 << (kAtrousMaxLevels - 1)));
-}
+cudaError_t atrous_setup() { return cudaSuccess; }  // the two-pass level kernels use no dynamic shared memory
 
 cudaError_t atrous_run(const AtrousPlan& p, const Img& in, const Img& out, bool f16, void* scratch, cudaStream_t st) {
     if (p.copy) {
@@ -428,6 +420,7 @@ cudaError_t atrous_run(const AtrousPlan& p, const Img& in, const Img& out, bool 
     char* base = static_cast<char*>(scratch);
     float* c[2] = {reinterpret_cast<float*>(base + p.off_c0), reinterpret_cast<float*>(base + p.off_c1)};
     float* wv = reinterpret_cast<float*>(base + p.off_w);
+    float* tmp = reinterpret_cast<float*>(base + p.off_tmp);
     float* part = reinterpret_cast<float*>(base + p.off_part);
     float* thr = reinterpret_cast<float*>(base + p.off_thr);
     const long long npx = (long long)p.w * p.h;
@@ -440,8 +433,10 @@ cudaError_t atrous_run(const AtrousPlan& p, const Img& in, const Img& out, bool 
         const int s = 1 << j;
         const dim3 lg((unsigned)p.gx, (unsigned)p.gy);
         tl.nb[j] = (int)(lg.x * lg.y);
-        atrous_level_kernel<<<lg, kAtThreads, at_smem(s), st>>>(c[j & 1], c[(j + 1) & 1], wv + (size_t)j * 3 * npx,
-                                                               part + (size_t)j * tl.stride, p.w, p.h, npx, s);
+        const dim3 hg((unsigned)((p.w + kAtThreads - 1) / kAtThreads), (unsigned)p.h, 3);
+        atrous_h_kernel<<<hg, kAtThreads, 0, st>>>(c[j & 1], tmp, p.w, npx, s);
+        atrous_v_kernel<<<lg, kAtThreads, 0, st>>>(c[j & 1], tmp, c[(j + 1) & 1], wv + (size_t)j * 3 * npx,
+                                                   part + (size_t)j * tl.stride, p.w, p.h, npx, s);
     }
     AtrousThrArgs ta{};
     for (int j = 0; j < p.levels; ++j)
