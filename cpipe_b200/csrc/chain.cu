@@ -445,6 +445,7 @@ struct cpipe_cuda_chain {
     bool guided_spec = false;
     AtrousPlan atrous{};
     void* d_atrous = nullptr;
+    void* d_gspec = nullptr;  // spec guided filter's planes
     SpotStats* d_stats = nullptr;
     // The tiles' BM3D runs on a second stream beside the network (both read
     // only the denoiser's input), forked after K2 and joined before the MSE.
@@ -603,7 +604,7 @@ int launch_chain(cpipe_cuda_chain* c, const void* d_raw, size_t raw_pitch, void*
         }
         if (e == cudaSuccess && c->cfg.guided_radius > 0) {
             const Img y = other(x);
-            e = c->guided_spec ? guided_spec_run(x, y, c->f16, c->cfg.guided_radius, c->cfg.guided_eps, st)
+            e = c->guided_spec ? guided_spec_run(x, y, c->f16, c->cfg.guided_radius, c->cfg.guided_eps, c->d_gspec, st)
                                : launch_guided(x, y, c->f16, c->cfg.guided_radius, c->cfg.guided_eps, st);
             x = y;
         }
@@ -820,6 +821,9 @@ cpipe_cuda_chain* cpipe_cuda_chain_create(const cpipe_cuda_chain_config* cfg, in
     c->spec_stages = c->guided_spec || cfg->atrous_levels > 0;
     if (c->spec_stages) {
         if (c->guided_spec && guided_spec_setup() != cudaSuccess) return fail(CPIPE_INTERNAL_ERROR, c);
+        if (c->guided_spec &&
+            cudaMalloc(&c->d_gspec, guided_spec_scratch_bytes(w, h, cfg->guided_radius)) != cudaSuccess)
+            return fail(CPIPE_OOM, c);
         if (cfg->atrous_levels > 0) {
             const cpipe_AtrousWaveletParams ap{cfg->atrous_levels, cfg->bm3d_sigma, cfg->atrous_luma_strength,
                                                cfg->wavelet_strength >= 0.0F ? cfg->wavelet_strength : 1.0F};
@@ -881,6 +885,7 @@ void cpipe_cuda_chain_destroy(cpipe_cuda_chain* c) {
     if (c->s_h2d) cudaStreamDestroy(c->s_h2d);
     if (c->s_d2h) cudaStreamDestroy(c->s_d2h);
     cudaFree(c->d_tables);
+    cudaFree(c->d_gspec);
     cudaFree(c->d_taps_ixy);
     cudaFree(c->d_taps_tx);
     cudaFree(c->d_taps_ty);

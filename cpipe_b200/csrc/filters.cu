@@ -715,10 +715,13 @@ int cpipe_cuda_denoise_guided_filter_spec(halide_buffer_t* const* inputs, size_t
     if (setup != cudaSuccess) return cuda_status(setup, "guided_filter_spec setup");
     Call call;
     Bound in, out;
-    const int st = rgba_pair(call, inputs, outputs, &in, &out);
+    int st = rgba_pair(call, inputs, outputs, &in, &out);
     if (st != CPIPE_OK) return call.finish(st);
-    return call.finish(
-        cuda_status(guided_spec_run(in.img, out.img, in.elem == 2, prm.radius, prm.eps, call.stream), "guided_spec"));
+    void* scratch = nullptr;
+    if ((st = call.alloc(guided_spec_scratch_bytes(in.img.w, in.img.h, prm.radius), &scratch)) != CPIPE_OK)
+        return call.finish(st);
+    return call.finish(cuda_status(
+        guided_spec_run(in.img, out.img, in.elem == 2, prm.radius, prm.eps, scratch, call.stream), "guided_spec"));
 }
 int cpipe_cuda_denoise_wavelet_atrous_spec(halide_buffer_t* const* inputs, size_t n_in,
                                            halide_buffer_t* const* outputs, size_t n_out, const void* blob,

@@ -27,12 +27,10 @@
 //          alpha copied.
 //
 // Kernels
-//   guided_spec_kernel   32x32 output tile, the clamped input with a 2r halo
-//                        for all three channels in shared memory; per channel
-//                        separable box sums (rows, then columns) of v - k and
-//                        (v - k)^2 (k: the tile's centre sample, so the
-//                        variance does not cancel), a and b on the tile plus r,
-//                        separable box sums of a and b, the output.
+//   gsp_rows / ab / ab_rows / out   the guided filter as four separable
+//                        passes over frame-wide planes (row passes staged in
+//                        shared memory, column passes with running FP64 sums;
+//                        v^2 sums and the variance in FP64), see below.
 //   atrous_prep_kernel   RGBA -> Y, Co, Cg planes (FP32).
 //   atrous_h_kernel      one level's horizontal B3 pass of all three planes
 //                        into a scratch plane set (taps 2^j apart, clamped).
@@ -49,6 +47,7 @@
 
 #include <algorithm>
 #include <cmath>
+#include <type_traits>
 #include <vector>
 
 #include "../../include/cpipe_node_abi.h"
@@ -58,141 +57,150 @@ namespace cpb {
 namespace {
 
 // ------------------------------------------------------------------ guided
-constexpr int kGsTW = 32, kGsTH = 32, kGsThreads = 256;
-
-// Row-major shared buffers use odd pitches: the row passes give consecutive
-// threads consecutive rows, which then fall in different banks.
-__host__ __device__ inline int odd(int v) { return v | 1; }
-__host__ __device__ inline size_t gs_floats(int R) {
-    const size_t IW = odd(kGsTW + 4 * R), IH = kGsTH + 4 * R, AW = odd(kGsTW + 2 * R), AH = kGsTH + 2 * R;
-    return 3 * IW * IH + 2 * AW * IH + 2 * AW * AH + 2 * (size_t)odd(kGsTW) * AH;
+// Four separable passes over frame-wide planes, per RGB channel (blockIdx.z):
+//   rows   S1, S2 = sums of v and v^2 (S2 in FP64) over the D = 2R+1 columns
+//          around xa in [-R, w+R), on rows yr in [-2R, h+2R) of the clamped
+//          image; the row segment is staged in shared memory;
+//   cols   running FP64 sums of S1, S2 down the D rows around ya in [-R, h+R):
+//          m = S1/N, corr = S2/N, var = max(corr - m^2, 0) in FP64 (so no
+//          shift is needed against cancellation), a = var / (var + eps),
+//          b = m - a m;
+//   rows   sums of a and b over the D columns around x in [0, w);
+//   cols   running sums down the D rows around y: mean_a, mean_b,
+//          out = max(mean_a v + mean_b, 0), alpha copied.
+// a and b live on the extended domain [-R, w+R) x [-R, h+R), as the filter's
+// definition evaluates them at positions outside the image.
+constexpr int kGsThreads = 256, kGsSeg = 32;  // column passes: rows per thread
+struct GsPlanes {
+    int w, h, R, Wa, Ha, Hr;
+    float* s1;   // [3][Hr][Wa]
+    double* s2;  // [3][Hr][Wa]
+    float* a;    // [3][Ha][Wa]
+    float* b;
+    float* sa;   // [3][Ha][w]
+    float* sb;
+};
+GsPlanes gs_planes(int w, int h, int R, void* scratch) {
+    GsPlanes p{w, h, R, w + 2 * R, h + 2 * R, h + 4 * R, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
+    char* c = static_cast<char*>(scratch);
+    const size_t nr = 3 * (size_t)p.Hr * p.Wa, na = 3 * (size_t)p.Ha * p.Wa, ns = 3 * (size_t)p.Ha * w;
+    p.s2 = reinterpret_cast<double*>(c);
+    c += nr * sizeof(double);
+    p.s1 = reinterpret_cast<float*>(c);
+    c += nr * sizeof(float);
+    p.a = reinterpret_cast<float*>(c);
+    c += na * sizeof(float);
+    p.b = reinterpret_cast<float*>(c);
+    c += na * sizeof(float);
+    p.sa = reinterpret_cast<float*>(c);
+    c += ns * sizeof(float);
+    p.sb = reinterpret_cast<float*>(c);
+    return p;
 }
-
+// pass 1: block = 256 consecutive xa of one row yi and channel c
 template <class T>
-__global__ void __launch_bounds__(kGsThreads) guided_spec_kernel(Img in, Img out, int R, float eps) {
-    extern __shared__ float sm[];
-    // extents (IWn x IH input, AWn x AH for a / b) and odd row pitches
-    const int IWn = kGsTW + 4 * R, IH = kGsTH + 4 * R, AWn = kGsTW + 2 * R, AH = kGsTH + 2 * R, D = 2 * R + 1;
-    const int IW = odd(IWn), AW = odd(AWn), TP = odd(kGsTW);
-    const float N = (float)(D * D);
-    float* s_v = sm;                  // [3][IH][IW] clamped input
-    float* s_r1 = s_v + 3 * IW * IH;  // [IH][AW] row sums of v - k
-    float* s_r2 = s_r1 + IH * AW;     // [IH][AW] row sums of (v - k)^2
-    float* s_a = s_r2 + IH * AW;      // [AH][AW]
-    float* s_b = s_a + AH * AW;
-    float* s_ra = s_b + AH * AW;      // [AH][TP] row sums of a
-    float* s_rb = s_ra + AH * TP;
-    const int x0 = blockIdx.x * kGsTW, y0 = blockIdx.y * kGsTH;
-    for (int i = threadIdx.x; i < IWn * IH; i += blockDim.x) {
-        const int ty = i / IWn, tx = i - ty * IWn;
-        const Rgba v = load_clamped<T>(in, x0 - 2 * R + tx, y0 - 2 * R + ty);
-        s_v[ty * IW + tx] = v.r;
-        s_v[IW * IH + ty * IW + tx] = v.g;
-        s_v[2 * IW * IH + ty * IW + tx] = v.b;
+__global__ void __launch_bounds__(kGsThreads) gsp_rows_kernel(Img in, GsPlanes p) {
+    __shared__ float s_row[kGsThreads + 2 * kGuidedSpecMaxRadius];
+    const int xb = blockIdx.x * kGsThreads, yi = blockIdx.y, c = blockIdx.z, R = p.R;
+    const int y = clampi(yi - 2 * R, 0, in.h - 1);
+    for (int i = threadIdx.x; i < kGsThreads + 2 * R; i += kGsThreads) {
+        const int x = clampi(xb + i - 2 * R, 0, in.w - 1);  // xa = xb + i - R, its box from xa - R
+        s_row[i] = (float)px<const T>(in, x, y)[c];
     }
     __syncthreads();
-    // Box sums along rows or columns: each item is a run of up to kGsSeg
-    // consecutive outputs, its first window summed directly and the rest slid
-    // (one add and one subtract per output; the slide restarts every run).
-    constexpr int kGsSeg = 8;
-    static_assert(kGsTW * (kGsTH / kGsSeg) <= kGsThreads && kGsTW % kGsSeg == 0 && kGsTH % kGsSeg == 0, "runs");
-    float res[kGsSeg][3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        const float* v = s_v + c * IW * IH;
-        const float k = v[(2 * R + kGsTH / 2) * IW + 2 * R + kGsTW / 2];
-        const int rseg = (AWn + kGsSeg - 1) / kGsSeg;
-        for (int it = threadIdx.x; it < IH * rseg; it += blockDim.x) {  // rows of v: (v - k), (v - k)^2
-            const int y = it % IH, x0s = (it / IH) * kGsSeg, n = min(kGsSeg, AWn - x0s);
-            const float* row = v + y * IW + x0s;
-            float s1 = 0.0F, s2 = 0.0F;
-            for (int d = 0; d < D; ++d) {
-                const float t = row[d] - k;
-                s1 = s1 + t;
-                s2 = s2 + t * t;
-            }
-            s_r1[y * AW + x0s] = s1;
-            s_r2[y * AW + x0s] = s2;
-            for (int i = 1; i < n; ++i) {
-                const float ti = row[i + D - 1] - k, to = row[i - 1] - k;
-                s1 = (s1 + ti) - to;
-                s2 = (s2 + ti * ti) - to * to;
-                s_r1[y * AW + x0s + i] = s1;
-                s_r2[y * AW + x0s + i] = s2;
-            }
-        }
-        __syncthreads();
-        const int cseg = (AH + kGsSeg - 1) / kGsSeg;
-        for (int it = threadIdx.x; it < AWn * cseg; it += blockDim.x) {  // columns -> a, b
-            const int x = it % AWn, y0s = (it / AWn) * kGsSeg, n = min(kGsSeg, AH - y0s);
-            float s1 = 0.0F, s2 = 0.0F;
-            for (int d = 0; d < D; ++d) {
-                s1 = s1 + s_r1[(y0s + d) * AW + x];
-                s2 = s2 + s_r2[(y0s + d) * AW + x];
-            }
-            for (int i = 0; i < n; ++i) {
-                if (i > 0) {
-                    s1 = (s1 + s_r1[(y0s + i + D - 1) * AW + x]) - s_r1[(y0s + i - 1) * AW + x];
-                    s2 = (s2 + s_r2[(y0s + i + D - 1) * AW + x]) - s_r2[(y0s + i - 1) * AW + x];
-                }
-                const float mk = s1 / N, corr = s2 / N;
-                const float var = max0(corr - mk * mk);
-                const float m = mk + k;
-                const float a = var / (var + eps);
-                s_a[(y0s + i) * AW + x] = a;
-                s_b[(y0s + i) * AW + x] = m - a * m;
-            }
-        }
-        __syncthreads();
-        const int tseg = kGsTW / kGsSeg;
-        for (int it = threadIdx.x; it < AH * tseg; it += blockDim.x) {  // rows of a, b
-            const int y = it % AH, x0s = (it / AH) * kGsSeg;
-            const float* ra = s_a + y * AW + x0s;
-            const float* rb = s_b + y * AW + x0s;
-            float sa = 0.0F, sb = 0.0F;
-            for (int d = 0; d < D; ++d) {
-                sa = sa + ra[d];
-                sb = sb + rb[d];
-            }
-            s_ra[y * TP + x0s] = sa;
-            s_rb[y * TP + x0s] = sb;
-            for (int i = 1; i < kGsSeg; ++i) {
-                sa = (sa + ra[i + D - 1]) - ra[i - 1];
-                sb = (sb + rb[i + D - 1]) - rb[i - 1];
-                s_ra[y * TP + x0s + i] = sa;
-                s_rb[y * TP + x0s + i] = sb;
-            }
-        }
-        __syncthreads();
-        // columns of the row-summed a, b -> the output: thread t < kGsTW * kGsTH / kGsSeg
-        // owns the run of rows 8 (t / kGsTW).. of column t % kGsTW, kept in registers
-        if ((int)threadIdx.x < kGsTW * (kGsTH / kGsSeg)) {
-            const int it = threadIdx.x;
-            const int x = it % kGsTW, y0s = (it / kGsTW) * kGsSeg;
-            float sa = 0.0F, sb = 0.0F;
-            for (int d = 0; d < D; ++d) {
-                sa = sa + s_ra[(y0s + d) * TP + x];
-                sb = sb + s_rb[(y0s + d) * TP + x];
-            }
-#pragma unroll
-            for (int i = 0; i < kGsSeg; ++i) {
-                if (i > 0) {
-                    sa = (sa + s_ra[(y0s + i + D - 1) * TP + x]) - s_ra[(y0s + i - 1) * TP + x];
-                    sb = (sb + s_rb[(y0s + i + D - 1) * TP + x]) - s_rb[(y0s + i - 1) * TP + x];
-                }
-                const int y = y0s + i;
-                res[i][c] = max0((sa / N) * v[(y + 2 * R) * IW + x + 2 * R] + (sb / N));
-            }
-        }
-        __syncthreads();
+    const int xi = xb + threadIdx.x;
+    if (xi >= p.Wa) return;
+    float s = 0.0F;
+    double q = 0.0;
+    for (int dx = 0; dx <= 2 * R; ++dx) {
+        const float v = s_row[threadIdx.x + dx];
+        s += v;
+        // a binary16 value squares exactly in binary32 (11-bit significand)
+        q += std::is_same<T, __half>::value ? (double)(v * v) : (double)v * (double)v;
     }
-    if ((int)threadIdx.x < kGsTW * (kGsTH / kGsSeg)) {
-        const int x = x0 + (int)threadIdx.x % kGsTW, yb = y0 + ((int)threadIdx.x / kGsTW) * kGsSeg;
-#pragma unroll
-        for (int i = 0; i < kGsSeg; ++i) {
-            const int y = yb + i;
-            if (x < out.w && y < out.h)
-                store_rgb_keep_alpha(px<T>(out, x, y), Rgba{res[i][0], res[i][1], res[i][2], 0.0F}, px<const T>(in, x, y));
+    const size_t o = ((size_t)c * p.Hr + yi) * p.Wa + xi;
+    p.s1[o] = s;
+    p.s2[o] = q;
+}
+// pass 2: a thread walks kGsSeg rows of one column with running sums
+__global__ void __launch_bounds__(kGsThreads) gsp_ab_kernel(GsPlanes p, float eps) {
+    const int xi = blockIdx.x * blockDim.x + threadIdx.x, y0 = blockIdx.y * kGsSeg, c = blockIdx.z;
+    if (xi >= p.Wa || y0 >= p.Ha) return;
+    const int D = 2 * p.R + 1, y1 = min(p.Ha, y0 + kGsSeg);
+    const double invN = 1.0 / ((double)D * D);
+    const float* s1 = p.s1 + (size_t)c * p.Hr * p.Wa + xi;
+    const double* s2 = p.s2 + (size_t)c * p.Hr * p.Wa + xi;
+    double sm = 0.0, sq = 0.0;
+    for (int r = y0; r < y0 + D - 1; ++r) {  // S rows ya_i .. ya_i + 2R belong to output row ya_i
+        sm += (double)s1[(size_t)r * p.Wa];
+        sq += s2[(size_t)r * p.Wa];
+    }
+    for (int yi = y0; yi < y1; ++yi) {
+        const size_t add = (size_t)(yi + D - 1) * p.Wa;
+        sm += (double)s1[add];
+        sq += s2[add];
+        const double m = sm * invN, var = fmax(sq * invN - m * m, 0.0);
+        const float vf = (float)var, mf = (float)m;
+        const float a = vf / (vf + eps);  // in [0, 1]: binary32 is ample
+        const size_t o = ((size_t)c * p.Ha + yi) * p.Wa + xi;
+        p.a[o] = a;
+        p.b[o] = mf - a * mf;
+        const size_t sub = (size_t)yi * p.Wa;
+        sm -= (double)s1[sub];
+        sq -= s2[sub];
+    }
+}
+// pass 3: block = 256 consecutive x of one extended row yi and channel c
+__global__ void __launch_bounds__(kGsThreads) gsp_ab_rows_kernel(GsPlanes p) {
+    __shared__ float s_a[kGsThreads + 2 * kGuidedSpecMaxRadius], s_b[kGsThreads + 2 * kGuidedSpecMaxRadius];
+    const int xb = blockIdx.x * kGsThreads, yi = blockIdx.y, c = blockIdx.z, R = p.R;
+    const size_t row = ((size_t)c * p.Ha + yi) * p.Wa;
+    for (int i = threadIdx.x; i < kGsThreads + 2 * R; i += kGsThreads) {
+        const int xa = min(xb + i, p.Wa - 1);  // xa index x + dx (x - R + dx in image coordinates)
+        s_a[i] = p.a[row + xa];
+        s_b[i] = p.b[row + xa];
+    }
+    __syncthreads();
+    const int x = xb + threadIdx.x;
+    if (x >= p.w) return;
+    float sa = 0.0F, sb = 0.0F;
+    for (int dx = 0; dx <= 2 * R; ++dx) {
+        sa += s_a[threadIdx.x + dx];
+        sb += s_b[threadIdx.x + dx];
+    }
+    const size_t o = ((size_t)c * p.Ha + yi) * p.w + x;
+    p.sa[o] = sa;
+    p.sb[o] = sb;
+}
+// pass 4: a thread walks kGsSeg output rows of one column, all three channels
+template <class T>
+__global__ void __launch_bounds__(kGsThreads) gsp_out_kernel(Img in, Img out, GsPlanes p) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y0 = blockIdx.y * kGsSeg;
+    if (x >= p.w || y0 >= p.h) return;
+    const int D = 2 * p.R + 1, y1 = min(p.h, y0 + kGsSeg);
+    const float N = (float)(D * D);
+    double sa[3] = {0.0, 0.0, 0.0}, sb[3] = {0.0, 0.0, 0.0};
+    const size_t plane = (size_t)p.Ha * p.w;
+    for (int r = y0; r < y0 + D - 1; ++r)
+        for (int c = 0; c < 3; ++c) {
+            sa[c] += (double)p.sa[c * plane + (size_t)r * p.w + x];
+            sb[c] += (double)p.sb[c * plane + (size_t)r * p.w + x];
+        }
+    for (int y = y0; y < y1; ++y) {
+        const size_t add = (size_t)(y + D - 1) * p.w + x, sub = (size_t)y * p.w + x;
+        for (int c = 0; c < 3; ++c) {
+            sa[c] += (double)p.sa[c * plane + add];
+            sb[c] += (double)p.sb[c * plane + add];
+        }
+        const Rgba v = load_rgba(px<const T>(in, x, y));
+        const float ma[3] = {(float)sa[0] / N, (float)sa[1] / N, (float)sa[2] / N};
+        const float mb[3] = {(float)sb[0] / N, (float)sb[1] / N, (float)sb[2] / N};
+        store_rgb_keep_alpha(px<T>(out, x, y),
+                             Rgba{max0(ma[0] * v.r + mb[0]), max0(ma[1] * v.g + mb[1]), max0(ma[2] * v.b + mb[2]), 0.0F},
+                             px<const T>(in, x, y));
+        for (int c = 0; c < 3; ++c) {
+            sa[c] -= (double)p.sa[c * plane + sub];
+            sb[c] -= (double)p.sb[c * plane + sub];
         }
     }
 }
@@ -327,20 +335,25 @@ size_t align256(size_t v) { return (v + 255U) & ~(size_t)255U; }
 
 }  // namespace
 
-cudaError_t guided_spec_setup() {
-    const int bytes = (int)(gs_floats(kGuidedSpecMaxRadius) * sizeof(float));
-    cudaError_t e = cudaFuncSetAttribute(guided_spec_kernel<__half>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    if (e == cudaSuccess)
-        e = cudaFuncSetAttribute(guided_spec_kernel<float>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    return e;
+cudaError_t guided_spec_setup() { return cudaSuccess; }  // the pass kernels use no dynamic shared memory
+
+size_t guided_spec_scratch_bytes(int w, int h, int radius) {
+    const size_t Wa = (size_t)w + 2 * radius, Ha = (size_t)h + 2 * radius, Hr = (size_t)h + 4 * radius;
+    return 3 * (Hr * Wa * (sizeof(double) + sizeof(float)) + 2 * Ha * Wa * sizeof(float) + 2 * Ha * (size_t)w * sizeof(float));
 }
 
-cudaError_t guided_spec_run(const Img& in, const Img& out, bool f16, int radius, float eps, cudaStream_t st) {
+cudaError_t guided_spec_run(const Img& in, const Img& out, bool f16, int radius, float eps, void* scratch,
+                            cudaStream_t st) {
     if (radius < 1 || radius > kGuidedSpecMaxRadius) return cudaErrorInvalidValue;
-    const dim3 grid((unsigned)((in.w + kGsTW - 1) / kGsTW), (unsigned)((in.h + kGsTH - 1) / kGsTH));
-    const size_t bytes = gs_floats(radius) * sizeof(float);
-    if (f16) guided_spec_kernel<__half><<<grid, kGsThreads, bytes, st>>>(in, out, radius, eps);
-    else guided_spec_kernel<float><<<grid, kGsThreads, bytes, st>>>(in, out, radius, eps);
+    const GsPlanes p = gs_planes(in.w, in.h, radius, scratch);
+    const unsigned ga = (unsigned)((p.Wa + kGsThreads - 1) / kGsThreads), gw = (unsigned)((in.w + kGsThreads - 1) / kGsThreads);
+    if (f16) gsp_rows_kernel<__half><<<dim3(ga, (unsigned)p.Hr, 3), kGsThreads, 0, st>>>(in, p);
+    else gsp_rows_kernel<float><<<dim3(ga, (unsigned)p.Hr, 3), kGsThreads, 0, st>>>(in, p);
+    gsp_ab_kernel<<<dim3(ga, (unsigned)((p.Ha + kGsSeg - 1) / kGsSeg), 3), kGsThreads, 0, st>>>(p, eps);
+    gsp_ab_rows_kernel<<<dim3(gw, (unsigned)p.Ha, 3), kGsThreads, 0, st>>>(p);
+    const dim3 go(gw, (unsigned)((in.h + kGsSeg - 1) / kGsSeg));
+    if (f16) gsp_out_kernel<__half><<<go, kGsThreads, 0, st>>>(in, out, p);
+    else gsp_out_kernel<float><<<go, kGsThreads, 0, st>>>(in, out, p);
     return cudaGetLastError();
 }
 

@@ -14,9 +14,12 @@ constexpr int kGuidedSpecMaxRadius = 16;
 constexpr int kAtrousMaxLevels = 6;
 
 // Guided filter with a true (2r+1)^2 box, r in 1..kGuidedSpecMaxRadius; RGBA
-// in and out (binary16 when f16, else float32), alpha copied.  No scratch.
+// in and out (binary16 when f16, else float32), alpha copied.  scratch:
+// guided_spec_scratch_bytes(w, h, r) of device memory, 8-byte aligned.
 cudaError_t guided_spec_setup();
-cudaError_t guided_spec_run(const Img& in, const Img& out, bool f16, int radius, float eps, cudaStream_t stream);
+size_t guided_spec_scratch_bytes(int w, int h, int radius);
+cudaError_t guided_spec_run(const Img& in, const Img& out, bool f16, int radius, float eps, void* scratch,
+                            cudaStream_t stream);
 
 struct AtrousPlan {
     int w = 0, h = 0, levels = 0;
