@@ -310,6 +310,64 @@ def finishing_stages():
     return out
 
 
+def dng_ingest(peak_gbs):
+    """DNG ingest of a 4032x3024 frame: the strip unpack alone from a
+    device-resident strip (16-bit words; 12-bit packed), bytes = strip read +
+    plane written once; and cpipe_cuda_dng_decode from the file image in
+    pageable host memory (parse, strip upload, unpack).  CUDA events around 20
+    calls after 3; the 16-bit strip and plane (48 MB) stay in L2 only partly."""
+    import numpy as np
+    from cpipe_b200 import _abi as A
+    from cpipe_b200.dng_synth import SHORT, build_dng
+    L = A.lib()
+    L.cpipe_cuda_set_stream(None)
+    w, h = 4032, 3024
+    rng = np.random.default_rng(4032)
+    e0, e1 = C.c_void_p(), C.c_void_p()
+    L.cpipe_cuda_event_create(C.byref(e0))
+    L.cpipe_cuda_event_create(C.byref(e1))
+    out = {"frame": f"{w}x{h}"}
+    d_raw = C.c_void_p()
+    assert L.cpipe_cuda_device_alloc(w * h * 2, C.byref(d_raw)) == 0
+
+    def timed(fn, n=20):
+        for _ in range(3):
+            assert fn() == 0
+        L.cpipe_cuda_event_record(e0, None)
+        for _ in range(n):
+            fn()
+        L.cpipe_cuda_event_record(e1, None)
+        assert L.cpipe_cuda_synchronize() == 0
+        ms = C.c_float()
+        L.cpipe_cuda_event_elapsed_ms(e0, e1, C.byref(ms))
+        return ms.value / n
+
+    for bits in (16, 12):
+        x = rng.integers(0, 1 << bits, (h, w), dtype=np.uint32).astype(np.uint16)
+        if bits == 16:
+            strip = x.astype("<u2").tobytes()
+        else:
+            rows = np.empty((h, w, bits), np.uint8)
+            for i in range(bits):
+                rows[..., i] = (x >> (bits - 1 - i)) & 1
+            strip = np.packbits(rows.reshape(h, w * bits), axis=1).tobytes()
+        d_strip = C.c_void_p()
+        assert L.cpipe_cuda_device_alloc(len(strip), C.byref(d_strip)) == 0
+        assert L.cpipe_cuda_memcpy_h2d(d_strip, strip, len(strip)) == 0
+        ms = timed(lambda: L.cpipe_cuda_dng_unpack(d_strip, len(strip), w, h, bits, d_raw))
+        gbs = (len(strip) + w * h * 2) / (ms * 1e-3) / 1e9
+        data = build_dng(width=w, height=h, strip=strip, overrides={258: (SHORT, [bits])})
+        e2e = timed(lambda: L.cpipe_cuda_dng_decode(data, len(data), d_raw, w * h * 2, None), n=10)
+        out[f"bits{bits}"] = {"unpack_ms": round(ms, 4), "achieved_gbs": round(gbs, 1),
+                              "frac": round(gbs / peak_gbs, 4), "decode_from_host_ms": round(e2e, 3),
+                              "file_bytes": len(data)}
+        L.cpipe_cuda_device_free(d_strip)
+    L.cpipe_cuda_device_free(d_raw)
+    out["note"] = ("decode_from_host_ms includes the pageable host-to-device copy of the strip, "
+                   "which bounds it; the unpack is the kernel's share")
+    return out
+
+
 def batched_form():
     """The 64-frame uneven batch (cpipe_b200.batch): aggregate MP/s of one launch
     per stage over all frames, per-frame latency alone."""
@@ -544,6 +602,7 @@ def b200_arm(args):
         line["batched_form"] = batched_form()
         line["spec_form"] = spec_form(peak_gbs)
         line["finishing_stages"] = finishing_stages()
+        line["dng_ingest"] = dng_ingest(peak_gbs)
         line["node_roofline"] = {"peak_gbs": peak_gbs, "peak_kind": gbs_kind,
                                  "note": "each node's filter alone, 12 MP device buffers, bytes = its input and "
                                          "output once in the reference's formats",

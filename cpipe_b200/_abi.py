@@ -152,6 +152,23 @@ class DisplayParams(C.Structure):
 DISPLAY_SRGB, DISPLAY_BT2020_PQ = 0, 1
 
 
+class DngInfo(C.Structure):
+    """include/cpipe_b200_dng.h cpipe_DngInfo."""
+    _fields_ = [("width", C.c_uint32), ("height", C.c_uint32), ("bits_per_sample", C.c_uint32),
+                ("compression", C.c_uint32), ("strip_offset", C.c_uint32), ("strip_byte_count", C.c_uint32),
+                ("orientation", C.c_uint32), ("cfa_repeat", C.c_uint32 * 2), ("cfa_pattern", C.c_uint8 * 16),
+                ("black_level", C.c_float * 4), ("white_level", C.c_uint32),
+                ("calibration_illuminant", C.c_uint32 * 2), ("has_matrix", C.c_uint32 * 4),
+                ("matrix", (C.c_float * 9) * 4), ("as_shot_neutral", C.c_float * 3),
+                ("has_active_area", C.c_uint32), ("active_area", C.c_uint32 * 4), ("iso", C.c_int32),
+                ("exposure_time_ns", C.c_int64), ("lens_aperture", C.c_float),
+                ("lens_focal_length_mm", C.c_float), ("linearization_offset", C.c_uint32),
+                ("linearization_count", C.c_uint32), ("opcode_list_offset", C.c_uint32 * 3),
+                ("opcode_list_bytes", C.c_uint32 * 3), ("exif_offset", C.c_uint32), ("exif_bytes", C.c_uint32),
+                ("xmp_offset", C.c_uint32), ("xmp_bytes", C.c_uint32), ("icc_offset", C.c_uint32),
+                ("icc_bytes", C.c_uint32), ("make", C.c_char * 64), ("model", C.c_char * 64)]
+
+
 class ChainConfig(C.Structure):
     _fields_ = [("width", C.c_int32), ("height", C.c_int32), ("black", BlacklevelParams),
                 ("gainmap_blob", C.c_void_p), ("gainmap_blob_size", C.c_size_t), ("demosaic", C.c_int32),
@@ -204,6 +221,7 @@ EXPORTS = [
     "cpipe_cuda_sharpen_edge_aware_usm", "cpipe_cuda_scene_linear_to_display",
     "cpipe_cuda_copy", "cpipe_cuda_filters", "cpipe_cuda_find_filter",
     "cpipe_cuda_color_3d_lut_noalloc",
+    "cpipe_dng_parse", "cpipe_cuda_dng_decode", "cpipe_cuda_dng_unpack",
     "cpipe_b200_node_descs", "cpipe_b200_find_node",
     "cpipe_cuda_scene_raw", "cpipe_cuda_scene_raw_cfa", "cpipe_surrogate_blob_size", "cpipe_surrogate_create", "cpipe_surrogate_destroy", "cpipe_surrogate_export",
     "cpipe_surrogate_denoise", "cpipe_surrogate_set_engine", "cpipe_surrogate_check", "cpipe_surrogate_profile", "cpipe_surrogate_train_step", "cpipe_surrogate_gradients",
@@ -280,6 +298,9 @@ def lib():
         "cpipe_cuda_chain_create": (vp, [C.POINTER(ChainConfig), C.POINTER(i32)]),
         "cpipe_cuda_chain_destroy": (None, [vp]), "cpipe_cuda_chain_output_bytes": (sz, [vp]),
         "cpipe_cuda_selftest_const_division": (i32, [C.c_float, C.POINTER(C.c_uint64), C.POINTER(C.c_uint64)]),
+        "cpipe_dng_parse": (i32, [vp, sz, C.POINTER(DngInfo)]),
+        "cpipe_cuda_dng_decode": (i32, [vp, sz, vp, sz, C.POINTER(DngInfo)]),
+        "cpipe_cuda_dng_unpack": (i32, [vp, sz, u32, u32, u32, vp]),
         "cpipe_cuda_chain_run": (i32, [vp, vp, vp, vp]), "cpipe_cuda_chain_run_host": (i32, [vp, vp, vp, vp]),
         "cpipe_cuda_chain_run_host_frames": (i32, [vp, vp, vp, i32, vp]),
         "cpipe_cuda_pinned_alloc": (i32, [sz, C.POINTER(vp)]), "cpipe_cuda_pinned_free": (None, [vp]),

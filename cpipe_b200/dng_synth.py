@@ -1,0 +1,125 @@
+"""Synthetic little-endian DNG files (seeded test and benchmark frames).
+
+The tag set and values follow the reference's own synthetic fixture
+(tests/unit/dng_test_fixture.hpp:199-300 in the reference: a 4x3 RGGB RAW16
+frame with pixels 64 + 9 i, ISO 400, 1/125 s, f/1.7, 4.3 mm, linearization
+table {0, 128, 1024, 4095}, black levels 64..67, white 4095, identity matrices,
+AsShotNeutral {1, 2, 3}, illuminants 21 / 17, a full active area), so the
+expectations of tests/unit/test_dng_reader.cpp apply to these files.  Layout:
+header, IFD0 at offset 8 (entries sorted by tag), then the value sections.
+"""
+import struct
+
+import numpy as np
+
+BYTE, ASCII, SHORT, LONG, RATIONAL, UNDEFINED, SRATIONAL = 1, 2, 3, 4, 5, 7, 10
+
+
+def _vals(typ, values):
+    if typ in (BYTE, UNDEFINED):
+        return bytes(values)
+    if typ == ASCII:
+        return values.encode("latin-1") + b"\0"
+    if typ == SHORT:
+        return struct.pack("<%dH" % len(values), *values)
+    if typ == LONG:
+        return struct.pack("<%dI" % len(values), *values)
+    if typ == RATIONAL:
+        return b"".join(struct.pack("<II", n, d) for n, d in values)
+    if typ == SRATIONAL:
+        return b"".join(struct.pack("<ii", n, d) for n, d in values)
+    raise ValueError(typ)
+
+
+def default_pixels(w, h):
+    return np.array([(64 + 9 * i) & 0xFFFF for i in range(w * h)], np.uint16).reshape(h, w)
+
+
+def build_dng(width=4, height=3, pixels=None, strip=None, bits=16, cfa_repeat=(2, 2), cfa_pattern=(0, 1, 1, 2),
+              include_cfa=True, include_opcode_lists=True, include_sidecars=True, strip_byte_count=None,
+              overrides=None, drop=()):
+    """bytes of a DNG.  `strip` (bytes) replaces the RAW16 little-endian words
+    of `pixels`; `overrides` maps tag -> (type, values); `drop` lists tags to
+    leave out."""
+    if strip is None:
+        px = default_pixels(width, height) if pixels is None else np.asarray(pixels, np.uint16)
+        strip = px.astype("<u2").tobytes()
+    ident = [(1, 1), (0, 1), (0, 1), (0, 1), (1, 1), (0, 1), (0, 1), (0, 1), (1, 1)]
+    tags = {
+        256: (LONG, [width]), 257: (LONG, [height]), 258: (SHORT, [bits]), 259: (SHORT, [1]),
+        262: (SHORT, [32803]), 271: (ASCII, "GoogleTest"), 272: (ASCII, "Pixel8UT"),
+        273: (LONG, None),  # strip offset, filled in below
+        274: (SHORT, [1]), 277: (SHORT, [1]), 278: (LONG, [height]),
+        279: (LONG, [len(strip) if strip_byte_count is None else strip_byte_count]),
+        33434: (RATIONAL, [(1, 125)]), 33437: (RATIONAL, [(17, 10)]),
+        34665: (LONG, None),  # Exif IFD offset
+        34855: (SHORT, [400]), 37386: (RATIONAL, [(43, 10)]),
+        50706: (BYTE, [1, 4, 0, 0]), 50707: (BYTE, [1, 4, 0, 0]), 50708: (ASCII, "cpipe unit camera"),
+        50712: (SHORT, [0, 128, 1024, 4095]),
+        50714: (RATIONAL, [(64, 1), (65, 1), (66, 1), (67, 1)]), 50717: (LONG, [4095]),
+        50721: (SRATIONAL, ident), 50722: (SRATIONAL, ident),
+        50728: (RATIONAL, [(1, 1), (2, 1), (3, 1)]), 50778: (SHORT, [21]), 50779: (SHORT, [17]),
+        50829: (LONG, [0, 0, height, width]), 50964: (SRATIONAL, ident), 50965: (SRATIONAL, ident),
+    }
+    if include_sidecars:
+        tags[700] = (BYTE, list(b"<x:xmpmeta>unit</x:xmpmeta>\0"))
+        tags[34675] = (UNDEFINED, [1, 2, 3, 4])
+    if include_cfa:
+        tags[33421] = (SHORT, list(cfa_repeat))
+        tags[33422] = (BYTE, list(cfa_pattern))
+    if include_opcode_lists:
+        for tag in (51008, 51009, 51022):
+            tags[tag] = (UNDEFINED, [0, 0, 0, 0, 0, 0, 0, 0])  # big-endian opcode count 0 + padding
+    for t, v in (overrides or {}).items():
+        tags[t] = v
+    for t in drop:
+        tags.pop(t, None)
+
+    n = len(tags)
+    data_start = 8 + 2 + 12 * n + 4
+    sections = bytearray()
+    exif = struct.pack("<H", 0) + struct.pack("<I", 0)  # an empty Exif IFD: 0 entries, no next IFD
+    entries = []
+    for tag in sorted(tags):
+        typ, values = tags[tag]
+        if tag == 273:
+            raw = None
+        elif tag == 34665:
+            raw = None
+        else:
+            raw = _vals(typ, values)
+        count = 1 if raw is None else (len(raw) // {BYTE: 1, ASCII: 1, UNDEFINED: 1, SHORT: 2, LONG: 4,
+                                                      RATIONAL: 8, SRATIONAL: 8}[typ])
+        entries.append([tag, typ, count, raw])
+    # Place out-of-line values, then the Exif IFD, then the strip (16-byte aligned).
+    for e in entries:
+        if e[3] is not None and len(e[3]) > 4:
+            while (data_start + len(sections)) % 2:
+                sections.append(0)
+            off = data_start + len(sections)
+            sections += e[3]
+            e.append(off)
+    while (data_start + len(sections)) % 2:
+        sections.append(0)
+    exif_off = data_start + len(sections)
+    sections += exif
+    while (data_start + len(sections)) % 16:
+        sections.append(0)
+    strip_off = data_start + len(sections)
+    sections += strip
+
+    out = bytearray(b"II" + struct.pack("<HI", 42, 8) + struct.pack("<H", n))
+    for e in entries:
+        tag, typ, count, raw = e[:4]
+        if tag == 273:
+            field = struct.pack("<I", strip_off)
+        elif tag == 34665:
+            field = struct.pack("<I", exif_off)
+        elif len(raw) <= 4:
+            field = raw + b"\0" * (4 - len(raw))
+        else:
+            field = struct.pack("<I", e[4])
+        out += struct.pack("<HHI", tag, typ, count) + field
+    out += struct.pack("<I", 0)
+    assert len(out) == data_start
+    return bytes(out + sections)

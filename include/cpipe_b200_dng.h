@@ -1,0 +1,85 @@
+/* DNG ingest: host TIFF/DNG tag parse and GPU unpack of the CFA strip into an
+ * R16_UINT plane in device memory.
+ *
+ * Replaces the reference's ingest pair:
+ *   - cpipe::ingest::dng_opcode::OpcodeListParser::parse
+ *     (src/cpipe/ingest/dng_opcode/OpcodeListParser.cpp:330-515), whose
+ *     ParsedDngMetadata (include/cpipe/ingest/dng_opcode/OpcodeList.hpp:15-40)
+ *     cpipe_DngInfo flattens into plain fields and file byte ranges;
+ *   - cpipe::ingest::dng::DngReader::read
+ *     (src/cpipe/ingest/dng/DngReader.cpp:190-232), which the
+ *     com.cpipe.builtin.dng_input node calls
+ *     (src/cpipe/nodes/dng_input/dng_input.cpp:27-38).
+ *
+ * Status codes are the reference's cpipe_status_t values (cpipe_node_abi.h).
+ * The message of the last failure is read with cpipe_cuda_last_error(). */
+#ifndef CPIPE_B200_DNG_H
+#define CPIPE_B200_DNG_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct cpipe_DngInfo {
+    uint32_t width, height;            /* ImageWidth / ImageLength */
+    uint32_t bits_per_sample;          /* BitsPerSample (1..16) */
+    uint32_t compression;              /* Compression (1 = none; 1 when the tag is absent) */
+    uint32_t strip_offset;             /* first StripOffsets value */
+    uint32_t strip_byte_count;         /* first StripByteCounts value */
+    uint32_t orientation;              /* Orientation; 0 when the tag is absent */
+    uint32_t cfa_repeat[2];            /* CFARepeatPatternDim (2x2 or 4x4) */
+    uint8_t cfa_pattern[16];           /* CFAPattern, row-major, repeat[0] * repeat[1] entries */
+    float black_level[4];              /* first four BlackLevel values, 0 past the tag's count */
+    uint32_t white_level;              /* WhiteLevel (SHORT / LONG); 0 when absent */
+    uint32_t calibration_illuminant[2];
+    uint32_t has_matrix[4];            /* ColorMatrix1, ColorMatrix2, ForwardMatrix1, ForwardMatrix2 present */
+    float matrix[4][9];                /* in the same order, row-major, 0 past the tag's count */
+    float as_shot_neutral[3];
+    uint32_t has_active_area;
+    uint32_t active_area[4];           /* x, y, width, height (from the tag's top, left, bottom, right) */
+    int32_t iso;                       /* ISOSpeedRatings (IFD0, then the Exif IFD) */
+    int64_t exposure_time_ns;          /* ExposureTime * 1e9 in binary32, truncated */
+    float lens_aperture, lens_focal_length_mm;
+    /* Byte ranges of variable-length values inside the file (offset, bytes);
+     * bytes = 0 when the tag is absent.  linearization holds SHORT entries. */
+    uint32_t linearization_offset, linearization_count;
+    uint32_t opcode_list_offset[3], opcode_list_bytes[3];
+    uint32_t exif_offset, exif_bytes;  /* the Exif IFD's entry table (2 + 12 n + 4 bytes) */
+    uint32_t xmp_offset, xmp_bytes, icc_offset, icc_bytes;
+    char make[64], model[64];          /* NUL-terminated, truncated to 63 characters */
+} cpipe_DngInfo;
+
+/* Parse IFD0 of a little-endian DNG held in host memory.  CPIPE_OK, or
+ * CPIPE_FAILED (bad header, bad IFD table, missing raw fields), or
+ * CPIPE_UNSUPPORTED (not a single-plane CFA, CFA repeat other than 2x2 / 4x4,
+ * missing CFA pattern), exactly as OpcodeListParser::parse decides.  Host only:
+ * needs no GPU. */
+int cpipe_dng_parse(const uint8_t* file, size_t file_bytes, cpipe_DngInfo* info);
+
+/* DngReader::read over a file image in host memory: parse (CPIPE_UNSUPPORTED
+ * becomes CPIPE_FAILED, as the reader maps it), copy the raw strip to the
+ * device and unpack it into `d_raw` (width x height R16_UINT, row pitch width,
+ * at least width * height * 2 bytes) on the library's current stream.
+ * Uncompressed strips only; a compressed raw (lossless JPEG) returns
+ * CPIPE_UNSUPPORTED.  `info` may be NULL. */
+int cpipe_cuda_dng_decode(const uint8_t* file, size_t file_bytes, uint16_t* d_raw, size_t raw_bytes,
+                          cpipe_DngInfo* info);
+
+/* The unpack alone, from a strip already in device memory (16-byte aligned):
+ *   bits == 16, or strip_bytes >= width * height * 2: little-endian 16-bit
+ *     words, the first min(strip_bytes, width * height * 2) bytes copied and
+ *     the rest of the plane zero (DngReader.cpp:145-164);
+ *   bits 1..15 otherwise: samples packed most-significant bit first, each row
+ *     starting on a byte boundary (DNG 1.4 uncompressed layout); bits past the
+ *     strip read as zero. */
+int cpipe_cuda_dng_unpack(const uint8_t* d_strip, size_t strip_bytes, uint32_t width, uint32_t height,
+                          uint32_t bits, uint16_t* d_raw);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif

@@ -23,7 +23,7 @@ def declared_functions():
         src = open(os.path.join(INCLUDE, f)).read()
         src = re.sub(r"/\*.*?\*/", "", src, flags=re.S)
         src = re.sub(r"#define[^\n]*(\\\n[^\n]*)*", "", src)
-        names |= set(re.findall(r"\b(cpipe_(?:cuda|b200|surrogate)_\w+)\s*\(", src))
+        names |= set(re.findall(r"\b(cpipe_(?:cuda|b200|surrogate|dng)_\w+)\s*\(", src))
         names |= set(re.findall(r"CPIPE_CUDA_PARAM_FILTER\((\w+)\)", open(os.path.join(INCLUDE, f)).read()))
     return names - {"cpipe_cuda_filter_desc", "name"}
 
