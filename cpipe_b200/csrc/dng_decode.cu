@@ -39,7 +39,10 @@ __global__ void __launch_bounds__(kUnpackThreads) dng_words_kernel(const uint8_t
 // boundaries.  Thread (y, g) writes samples [8 g, 8 g + 8) of row y, which
 // start at bit 8 g * bits = byte g * bits of the row: no group straddles a
 // byte it shares with another group.  Bytes at or past `avail` read as zero.
-template <int kBits>
+// kWords: the group's bytes come in as aligned 32-bit words (the strip is
+// 4-byte aligned), funnel-shifted to the group's first byte; otherwise byte
+// by byte.
+template <int kBits, bool kWords>
 __global__ void __launch_bounds__(kUnpackThreads) dng_packed_kernel(const uint8_t* __restrict__ strip, uint64_t avail,
                                                                     uint32_t w, uint32_t h, uint64_t row_bytes,
                                                                     uint16_t* __restrict__ out, bool vec_store) {
@@ -52,12 +55,36 @@ __global__ void __launch_bounds__(kUnpackThreads) dng_packed_kernel(const uint8_
         const uint64_t base = (uint64_t)y * row_bytes + (uint64_t)g * kBits;
         // Up to 8 * 16 = 128 bits: hi holds the first 64, lo the rest.
         uint64_t hi = 0, lo = 0;
+        if constexpr (kWords) {
+            constexpr int kAligned = (kBits + 3) / 4;  // little-endian words from `base`
+            const uint64_t start = base & ~3ull;
+            const uint32_t sh = 8u * (uint32_t)(base & 3);
+            uint32_t raw[kAligned + 1];
 #pragma unroll
-        for (int k = 0; k < kBits; ++k) {
-            const uint64_t b = base + k;
-            const uint64_t v = b < avail ? (uint64_t)__ldg(strip + b) : 0ull;
-            if (k < 8) hi |= v << ((56 - 8 * k) & 63);
-            else lo |= v << ((120 - 8 * k) & 63);
+            for (int i = 0; i <= kAligned; ++i) {
+                const uint64_t a = start + 4ull * i;
+                if (a + 4 <= avail) {
+                    raw[i] = __ldg(reinterpret_cast<const uint32_t*>(strip + a));
+                } else {
+                    uint32_t v = 0;
+                    for (int k = 0; k < 4; ++k)
+                        if (a + k < avail) v |= (uint32_t)__ldg(strip + a + k) << (8 * k);
+                    raw[i] = v;
+                }
+            }
+            uint32_t wd[4] = {0, 0, 0, 0};  // bytes base .. base + 15, big-endian per word
+#pragma unroll
+            for (int i = 0; i < kAligned; ++i) wd[i] = __byte_perm(__funnelshift_r(raw[i], raw[i + 1], sh), 0, 0x0123);
+            hi = ((uint64_t)wd[0] << 32) | wd[1];
+            lo = ((uint64_t)wd[2] << 32) | wd[3];
+        } else {
+#pragma unroll
+            for (int k = 0; k < kBits; ++k) {
+                const uint64_t b = base + k;
+                const uint64_t v = b < avail ? (uint64_t)__ldg(strip + b) : 0ull;
+                if (k < 8) hi |= v << ((56 - 8 * k) & 63);
+                else lo |= v << ((120 - 8 * k) & 63);
+            }
         }
         uint16_t s[8];
 #pragma unroll
@@ -103,7 +130,10 @@ template <int kBits>
 void launch_packed(const uint8_t* strip, uint64_t avail, uint32_t w, uint32_t h, uint64_t row_bytes, uint16_t* out,
                    bool vec, cudaStream_t st) {
     const uint64_t units = (uint64_t)((w + 7) / 8) * h;
-    dng_packed_kernel<kBits><<<grid_for(units), kUnpackThreads, 0, st>>>(strip, avail, w, h, row_bytes, out, vec);
+    if ((uintptr_t)strip % 4 == 0)
+        dng_packed_kernel<kBits, true><<<grid_for(units), kUnpackThreads, 0, st>>>(strip, avail, w, h, row_bytes, out, vec);
+    else
+        dng_packed_kernel<kBits, false><<<grid_for(units), kUnpackThreads, 0, st>>>(strip, avail, w, h, row_bytes, out, vec);
 }
 
 int unpack(const uint8_t* d_strip, uint64_t strip_bytes, uint32_t w, uint32_t h, uint32_t bits, uint16_t* d_raw,

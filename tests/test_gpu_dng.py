@@ -108,14 +108,19 @@ def test_12mp_round_trip(bits):
     assert (host[w * h:] == 0xBEEF).all()  # nothing written past the plane
 
 
-def test_unpack_from_device_strip():
-    w, h, bits = 4032, 3024, 12
-    x = np.random.default_rng(9).integers(0, 4096, (h, w), dtype=np.uint32).astype(np.uint16)
-    strip = torch.from_numpy(np.frombuffer(od.pack(x, bits), np.uint8).copy()).cuda()
+@pytest.mark.parametrize("w,h,bits", [(4032, 3024, 12), (1001, 7, 10), (333, 5, 14), (64, 3, 7)])
+@pytest.mark.parametrize("strip_offset", [0, 1, 3])
+def test_unpack_from_device_strip(w, h, bits, strip_offset):
+    """Aligned strips take the word-load path, misaligned ones the byte path; both exact."""
+    x = np.random.default_rng(9 + bits).integers(0, 1 << bits, (h, w), dtype=np.uint32).astype(np.uint16)
+    packed = od.pack(x, bits)
+    buf = torch.zeros(len(packed) + 16, dtype=torch.uint8, device="cuda")
+    buf[strip_offset:strip_offset + len(packed)] = torch.from_numpy(np.frombuffer(packed, np.uint8).copy()).cuda()
     out = torch.empty((h, w), dtype=torch.uint16, device="cuda")
     L = _abi.lib()
     L.cpipe_cuda_set_stream(C.c_void_p(torch.cuda.current_stream().cuda_stream))
-    rc = L.cpipe_cuda_dng_unpack(C.c_void_p(strip.data_ptr()), strip.numel(), w, h, bits, C.c_void_p(out.data_ptr()))
+    rc = L.cpipe_cuda_dng_unpack(C.c_void_p(buf.data_ptr() + strip_offset), len(packed), w, h, bits,
+                                 C.c_void_p(out.data_ptr()))
     torch.cuda.synchronize()
     assert rc == _abi.OK
     assert np.array_equal(out.cpu().view(torch.int16).numpy().view(np.uint16), x)
