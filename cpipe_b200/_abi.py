@@ -205,7 +205,7 @@ PLAIN_FILTER = C.CFUNCTYPE(C.c_int, C.POINTER(HalideBuffer), C.POINTER(HalideBuf
 # Every extern "C" symbol declared in include/cpipe_b200.h.
 EXPORTS = [
     "cpipe_cuda_set_stream", "cpipe_cuda_get_stream", "cpipe_cuda_synchronize", "cpipe_cuda_last_error",
-    "cpipe_cuda_trim_scratch",
+    "cpipe_cuda_trim_scratch", "cpipe_cuda_memory_stats",
     "cpipe_cuda_device_count",
     "cpipe_cuda_precision_convert_r16u_to_f32", "cpipe_cuda_precision_convert_f32_to_rgba16f",
     "cpipe_cuda_precision_convert_rgba16f_to_rgba8", "cpipe_cuda_precision_convert_rgba16f_to_rgba16u",
@@ -264,7 +264,8 @@ def lib():
     vp, sz, i32, u32, cp = C.c_void_p, C.c_size_t, C.c_int, C.c_uint32, C.c_char_p
     sigs = {
         "cpipe_cuda_set_stream": (i32, [vp]), "cpipe_cuda_get_stream": (vp, []),
-        "cpipe_cuda_synchronize": (i32, []), "cpipe_cuda_trim_scratch": (i32, []), "cpipe_cuda_last_error": (cp, []), "cpipe_cuda_device_count": (i32, []),
+        "cpipe_cuda_synchronize": (i32, []), "cpipe_cuda_trim_scratch": (i32, []),
+        "cpipe_cuda_memory_stats": (i32, [vp, vp, vp, vp]), "cpipe_cuda_last_error": (cp, []), "cpipe_cuda_device_count": (i32, []),
         "cpipe_cuda_filters": (C.POINTER(FilterDesc), [C.POINTER(sz)]),
         "cpipe_cuda_find_filter": (C.POINTER(FilterDesc), [cp]),
         "cpipe_b200_node_descs": (C.POINTER(PluginDesc), [C.POINTER(sz)]),

@@ -138,6 +138,10 @@ void launch_packed(const uint8_t* strip, uint64_t avail, uint32_t w, uint32_t h,
 
 int unpack(const uint8_t* d_strip, uint64_t strip_bytes, uint32_t w, uint32_t h, uint32_t bits, uint16_t* d_raw,
            cudaStream_t st) {
+    if (bits < 1 || bits > 16) {
+        set_error("%s", "BitsPerSample outside 1..16");
+        return CPIPE_UNSUPPORTED;
+    }
     const uint64_t plane = (uint64_t)w * h * 2;
     if (bits == 16 || strip_bytes >= plane) {
         const uint64_t copy = strip_bytes < plane ? strip_bytes : plane;

@@ -6,6 +6,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
+#include <vector>
 
 #include "../../include/cpipe_b200_dng.h"
 #include "../../include/cpipe_node_abi.h"
@@ -88,11 +89,10 @@ uint32_t rd16(const uint8_t* p) { return (uint32_t)p[0] | ((uint32_t)p[1] << 8);
 uint32_t rd32(const uint8_t* p) { return rd16(p) | (rd16(p + 2) << 16); }
 
 struct Ifd {
-    Entry e[256];
-    uint64_t pos[256];  // file offset of each entry
-    int n = 0;
+    std::vector<Entry> e;
+    std::vector<uint64_t> pos;  // file offset of each entry
     const Entry* find(uint16_t tag, uint64_t* where = nullptr) const {
-        for (int i = 0; i < n; ++i)
+        for (size_t i = 0; i < e.size(); ++i)
             if (e[i].tag == tag) {
                 if (where) *where = pos[i];
                 return &e[i];
@@ -101,25 +101,26 @@ struct Ifd {
     }
 };
 
-// Reads the entry table at `off`.  Tags past the 256th are not kept: none of
-// the tags read here sit that deep in a real IFD0, and a table of more entries
-// still passes the same bounds check as the reference's.
+// Reads the whole entry table at `off` (up to 65535 entries, as the count field
+// allows); find() returns the first entry of a tag, as a linear search over the
+// table does.
 bool read_ifd(const Tiff& t, uint64_t off, Ifd* out) {
     if (off + 2 > t.n) return false;
     const uint32_t count = t.u16(off);
     if (off + 2 + (uint64_t)count * 12 > t.n) return false;
-    out->n = 0;
+    out->e.clear();
+    out->pos.clear();
+    out->e.reserve(count);
+    out->pos.reserve(count);
     for (uint32_t i = 0; i < count && i < (uint32_t)kMaxEntries; ++i) {
         const uint64_t o = off + 2 + (uint64_t)i * 12;
-        // First occurrence wins, as in a linear search over all entries.
-        if (out->n == 256) break;
         Entry e;
         e.tag = (uint16_t)t.u16(o);
         e.type = (uint16_t)t.u16(o + 2);
         e.count = t.u32(o + 4);
         e.value = t.u32(o + 8);
-        out->pos[out->n] = o;
-        out->e[out->n++] = e;
+        out->pos.push_back(o);
+        out->e.push_back(e);
     }
     return true;
 }

@@ -343,6 +343,25 @@ int cpipe_cuda_trim_scratch(void) {
     if (e == cudaSuccess) e = cudaMemPoolTrimTo(pool, 0);
     return cuda_status(e, "trim scratch");
 }
+int cpipe_cuda_memory_stats(uint64_t* scratch_reserved, uint64_t* scratch_used, uint64_t* device_free,
+                            uint64_t* prepared_tables) {
+    cudaMemPool_t pool;
+    cudaError_t e = scratch_pool(&pool);
+    uint64_t reserved = 0, used = 0;
+    size_t free_b = 0, total_b = 0;
+    if (e == cudaSuccess) e = cudaMemPoolGetAttribute(pool, cudaMemPoolAttrReservedMemCurrent, &reserved);
+    if (e == cudaSuccess) e = cudaMemPoolGetAttribute(pool, cudaMemPoolAttrUsedMemCurrent, &used);
+    if (e == cudaSuccess) e = cudaMemGetInfo(&free_b, &total_b);
+    if (e != cudaSuccess) return cuda_status(e, "memory stats");
+    if (scratch_reserved) *scratch_reserved = reserved;
+    if (scratch_used) *scratch_used = used;
+    if (device_free) *device_free = free_b;
+    if (prepared_tables) {
+        std::lock_guard<std::mutex> lock(g_tab_mu);
+        *prepared_tables = g_tabs.size();
+    }
+    return CPIPE_OK;
+}
 int cpipe_cuda_device_count(void) {
     int n = 0;
     if (cudaGetDeviceCount(&n) != cudaSuccess) {

@@ -24,7 +24,15 @@
 //    CPIPE_UNSUPPORTED;
 //  * the first call on each device resolves the array's device address
 //    (cudaGetSymbolAddress, with that device current); make that first call
-//    before any stream capture on that device.
+//    before any stream capture on that device;
+//  * the LUT is copied from the caller's blob with cudaMemcpyAsync on the
+//    call's stream.  From ordinary (pageable) host memory the CUDA runtime
+//    waits for the work already queued on that stream before it copies, so the
+//    call returns only once that earlier work has finished.  A blob in
+//    page-locked memory (cudaHostAlloc / cudaHostRegister) is copied without
+//    that wait; it must then stay unchanged until the stream reaches the copy;
+//  * frames of any height are covered: the grid is at most 65535 rows high and
+//    each block row steps through the frame's rows.
 #include <cstring>
 #include <mutex>
 
@@ -74,12 +82,13 @@ struct LutRgbCells {
 
 template <class T>
 __global__ void __launch_bounds__(256) lut_rgb_kernel(cpb::Img in, cpb::Img out, const float* lut, int S, int interp) {
-    const int y = blockIdx.y;
     const int x = blockIdx.x * blockDim.x + threadIdx.x;
     if (x >= in.w) return;
-    const T* s = cpb::px<const T>(in, x, y);
-    cpb::store_rgb_keep_alpha(cpb::px<T>(out, x, y), cpb::lut_px_cells(cpb::load_rgba(s), LutRgbCells{lut}, S, interp),
-                              s);
+    for (int y = blockIdx.y; y < in.h; y += gridDim.y) {
+        const T* s = cpb::px<const T>(in, x, y);
+        cpb::store_rgb_keep_alpha(cpb::px<T>(out, x, y),
+                                  cpb::lut_px_cells(cpb::load_rgba(s), LutRgbCells{lut}, S, interp), s);
+    }
 }
 
 // A device RGBA buffer as an Img (no staging: host buffers are refused).
@@ -136,7 +145,7 @@ extern "C" int cpipe_cuda_color_3d_lut_noalloc(halide_buffer_t* const* inputs, s
     st = cpb::cuda_status(cudaMemcpyAsync(scratch, values, floats * sizeof(float), cudaMemcpyHostToDevice, stream),
                           "LUT upload");
     if (st != CPIPE_OK) return st;
-    const dim3 grid((unsigned)((in.w + 255) / 256), (unsigned)in.h);
+    const dim3 grid((unsigned)((in.w + 255) / 256), (unsigned)(in.h < 65535 ? in.h : 65535));
     const int interp = hd.interpolation == 1U ? 1 : 0;
     if (ein == 2) lut_rgb_kernel<__half><<<grid, 256, 0, stream>>>(in, out, scratch, (int)hd.size, interp);
     else lut_rgb_kernel<float><<<grid, 256, 0, stream>>>(in, out, scratch, (int)hd.size, interp);

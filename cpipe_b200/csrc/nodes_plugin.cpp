@@ -323,46 +323,11 @@ int node_wb(Ctx& c) {
     return c.step("white_balance");
 }
 
-// wb/greyworld_auto.cpp:80-166: checks, the grey-world estimate and apply (on
-// the GPU through "cpipe_wb_greyworld_auto"; on a host that does not route it,
-// the reference's own loops through lock_cpu), then the same calibration and
-// metadata as the dual-illuminant node with the estimated neutral.
-static int greyworld_cpu(Ctx& c, uint32_t w, uint32_t h, float n[3]) {
-    void* src = nullptr;
-    void* dst = nullptr;
-    int st = c.buf->lock_cpu(const_cast<cpipe_buffer_t*>(c.in(0)), CPIPE_CPU_ACCESS_READ, &src);
-    if (st != CPIPE_OK) return st;
-    if ((st = c.buf->lock_cpu(c.out(0), CPIPE_CPU_ACCESS_WRITE, &dst)) != CPIPE_OK) {
-        c.buf->unlock_cpu(const_cast<cpipe_buffer_t*>(c.in(0)));
-        return st;
-    }
-    const auto* in = static_cast<const _Float16*>(src);
-    auto* out = static_cast<_Float16*>(dst);
-    const size_t count = (size_t)w * h;
-    double sums[3] = {0.0, 0.0, 0.0};
-    for (size_t i = 0; i < count; ++i)
-        for (int k = 0; k < 3; ++k) sums[k] += (double)(float)in[4 * i + k];
-    bool valid = true;
-    for (double v : sums) valid = valid && std::isfinite(v) && v > 0.0;
-    if (valid) {
-        n[0] = (float)(sums[0] / sums[1]);
-        n[1] = 1.0F;
-        n[2] = (float)(sums[2] / sums[1]);
-        for (size_t i = 0; i < count; ++i) {
-            for (int k = 0; k < 3; ++k) out[4 * i + k] = (_Float16)((float)in[4 * i + k] / n[k]);
-            out[4 * i + 3] = in[4 * i + 3];
-        }
-    }
-    const int s1 = c.buf->unlock_cpu(c.out(0));
-    const int s2 = c.buf->unlock_cpu(const_cast<cpipe_buffer_t*>(c.in(0)));
-    if (s1 != CPIPE_OK) return s1;
-    if (s2 != CPIPE_OK) return s2;
-    if (!valid) {
-        c.msg = "wb.greyworld invalid channel mean";
-        return CPIPE_NEED_METADATA;
-    }
-    return c.buf->flush_cpu_writes(c.out(0));
-}
+// wb/greyworld_auto.cpp:80-166: checks, the grey-world estimate and apply on
+// the GPU through "cpipe_wb_greyworld_auto", then the same calibration and
+// metadata as the dual-illuminant node with the estimated neutral.  A host that
+// does not route that aot_id gets CPIPE_UNSUPPORTED, as for every other node of
+// this library: there is no CPU path.
 int node_greyworld(Ctx& c) {
     int a = 0, b = 0;
     int st = c.format(c.in(0), &a);
@@ -374,6 +339,8 @@ int node_greyworld(Ctx& c) {
     }
     uint32_t w, h;
     if ((st = c.dims(c.in(0), &w, &h)) != CPIPE_OK) return st;
+    (void)w;
+    (void)h;
     const cpipe_metadata_t* m = c.metadata(c.in(0));
     if (!m) return CPIPE_NEED_METADATA;
     cpipe_calibration_view cal;
@@ -381,7 +348,7 @@ int node_greyworld(Ctx& c) {
     float n[3] = {1.0F, 1.0F, 1.0F};
     const cpipe_GreyworldParams gp{(uint64_t)(uintptr_t)n};
     st = c.submit("cpipe_wb_greyworld_auto", &gp, sizeof(gp));
-    if (st == CPIPE_UNSUPPORTED) st = greyworld_cpu(c, w, h, n);
+    if (st == CPIPE_UNSUPPORTED && c.msg.empty()) c.msg = "wb.greyworld_auto needs the CUDA filter cpipe_wb_greyworld_auto";
     if (st != CPIPE_OK) return st;
     const Vec3 neutral{n[0], n[1], n[2]};
     cpipe_WbParams p{};
@@ -663,17 +630,8 @@ int node_display(Ctx& c) {
     }
     const cpipe_DisplayParams p{code};
     st = c.submit("cpipe_scene_linear_to_display", &p, sizeof(p));
-    if (st == CPIPE_UNSUPPORTED) {
-        const char* env = std::getenv("CPIPE_OCIO_CONFIG");
-        const char* config = env && env[0] ? env : "share/cpipe/ocio/v0.2/config.ocio";
-        cpipe_ocio_processor_t* proc =
-            c.host->get_ocio_processor ? c.host->get_ocio_processor(c.host, config, "scene_linear_rec2020", dst) : nullptr;
-        if (proc == nullptr || c.compute->submit_ocio_processor == nullptr) {
-            c.msg = "scene_linear_to_display OCIO processor unavailable";
-            return CPIPE_FAILED;
-        }
-        st = c.compute->submit_ocio_processor(c.pc->compute, proc, c.in(0), c.out(0));
-    }
+    if (st == CPIPE_UNSUPPORTED && c.msg.empty())
+        c.msg = "scene_linear_to_display needs the CUDA filter cpipe_scene_linear_to_display";
     if (st != CPIPE_OK) return st;
     if ((st = c.mb->set_cs_role(c.builder(), dst)) != CPIPE_OK) return st;
     return c.step("color.scene_linear_to_display");

@@ -54,6 +54,13 @@ int cpipe_cuda_synchronize(void);
  * calls; this waits for the device and returns that memory.  (No reference
  * counterpart: the reference's filters run on the CPU.) */
 int cpipe_cuda_trim_scratch(void);
+/* Memory figures of the current device, for callers that budget device memory:
+ * bytes the scratch pool above has reserved and has handed out, the device's
+ * free bytes (cudaMemGetInfo), and the number of prepared tables (linearize,
+ * GainMap, LUT) the library keeps.  Any pointer may be NULL.  (No reference
+ * counterpart.) */
+int cpipe_cuda_memory_stats(uint64_t* scratch_reserved, uint64_t* scratch_used, uint64_t* device_free,
+                            uint64_t* prepared_tables);
 const char* cpipe_cuda_last_error(void);
 int cpipe_cuda_device_count(void);
 
@@ -134,7 +141,12 @@ CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_copy);
  * output must be device buffers (host buffers: CPIPE_UNSUPPORTED), and calls
  * that overlap on the GPU race on that one array (calls in order on one stream
  * are safe).  The first call on a device looks up the array's device address;
- * make it before any stream capture on that device. */
+ * make it before any stream capture on that device.  The LUT is copied from the
+ * blob with cudaMemcpyAsync on the call's stream: from pageable host memory
+ * that copy first waits for the work already queued on the stream, so the call
+ * returns only after it; a page-locked blob avoids the wait and must stay
+ * unchanged until the stream reaches the copy.  Frames of any height are
+ * covered (the grid's rows step through the frame). */
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_color_3d_lut_noalloc);
 
 /* Registration table: entry is a HalideParamFilterEntry when takes_params != 0,

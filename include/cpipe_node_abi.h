@@ -1,3 +1,6 @@
+// SPDX-License-Identifier: Apache-2.0
+// Copyright (c) 2026 cpipe contributors
+// (upstream notice of include/cpipe/sdk/cpipe_node.h, whose interface this header restates)
 /* cpipe plugin C ABI, version 0.4 -- restated for the B200 node library.
  *
  * The node library must be binary-compatible with hosts written against the

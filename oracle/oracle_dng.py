@@ -13,11 +13,14 @@ read()   follows cpipe::ingest::dng::DngReader::read (src/cpipe/ingest/dng/
          The reference first tries LibRaw (vcpkg dependency `libraw`, absent from
          the reference tree); for strips shorter than a 16-bit plane with
          BitsPerSample < 16 this restatement unpacks the DNG 1.4 uncompressed
-         packing (samples most-significant bit first, rows on byte boundaries),
-         which is what LibRaw reads there.  Parity for those packed depths is
-         pinned only by pack -> unpack round trips; the 16-bit path and the
-         parse are pinned by the reference's own unit-test expectations
-         (tests/unit/test_dng_reader.cpp).
+         packing (samples most-significant bit first, rows on byte boundaries).
+         Both paths return the stored samples as they are: they equal the
+         reference's single-strip fallback, not necessarily LibRaw, whose DNG
+         loaders are understood (not checked here: its source is absent) to map
+         samples through the file's LinearizationTable when one is present.
+         Parity for the packed depths is pinned only by pack -> unpack round
+         trips; the 16-bit path and the parse are pinned by the reference's own
+         unit-test expectations (tests/unit/test_dng_reader.cpp).
 """
 import struct
 

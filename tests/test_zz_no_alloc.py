@@ -8,7 +8,8 @@ array inside the library.  This test calls it through the C ABI twice in a row,
 with different LUTs (the second call must not see the first call's LUT), and
 checks each result against the regular cpipe_cuda_color_3d_lut on the same
 device buffers, within the f16 tolerance the other parity tests use.  It also
-checks the documented refusals: LUTs above 65 per edge and host buffers.
+checks that warm calls leave the device's memory figures unchanged, and the
+documented refusals: LUTs above 65 per edge and host buffers.
 
 The file name sorts last so that a run stopping at the first failure has run
 every other test before this one.
@@ -75,6 +76,33 @@ def test_noalloc_lut_matches_regular_filter_twice(cuda_device):
         assert np.array_equal(out.view(np.uint16), want.view(np.uint16))
         for f in (src, ref, got):
             f.free()
+
+
+def memory_stats():
+    vals = [C.c_uint64() for _ in range(4)]
+    assert A.lib().cpipe_cuda_memory_stats(*[C.byref(v) for v in vals]) == 0, last_error()
+    return tuple(v.value for v in vals)
+
+
+def test_noalloc_lut_allocates_nothing(cuda_device):
+    """Its defining property: once the device is warm, calls change neither
+    the library's scratch pool, nor its prepared-table cache, nor the device's
+    free memory."""
+    x = frame(4, 301, 257)
+    src, dst = DeviceFrame(x), DeviceFrame(np.zeros_like(x))
+    blob = blobs.lut3d(33, lut_values(33, 7), 0)
+    assert call_entry("cpipe_cuda_color_3d_lut_noalloc", [src.image()], [dst.image()], blob) == 0, last_error()
+    assert A.lib().cpipe_cuda_synchronize() == 0
+    before = memory_stats()
+    for k in range(2):
+        blob = blobs.lut3d(17 + 16 * k, lut_values(17 + 16 * k, 8 + k), k)
+        assert call_entry("cpipe_cuda_color_3d_lut_noalloc", [src.image()], [dst.image()], blob) == 0, last_error()
+    assert A.lib().cpipe_cuda_synchronize() == 0
+    after = memory_stats()
+    names = ("scratch reserved", "scratch used", "device free", "prepared tables")
+    assert before == after, {n: (b, a) for n, b, a in zip(names, before, after) if b != a}
+    src.free()
+    dst.free()
 
 
 def test_noalloc_lut_refusals(cuda_device):
