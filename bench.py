@@ -46,14 +46,27 @@ def measured_peak_gbs():
         return 6650.0, "fallback"
 
 
-def traffic_per_launch(kernel):
-    """DRAM bytes per launch from the committed ncu summary, or None."""
+def chain_profile(kernel, key="dram_bytes_per_launch"):
+    """A per-launch figure of a chain kernel (DRAM bytes, or warp instructions
+    with key="warp_inst_per_launch") from the committed ncu summary, or None."""
     path = os.path.join(ROOT, "profiles", "traffic_full_chain_12mp.json")
     try:
         with open(path) as f:
-            return json.load(f)["dram_bytes_per_launch"].get(kernel)
+            return json.load(f)[key].get(kernel)
     except Exception:
         return None
+
+
+def traffic_per_launch(kernel):
+    return chain_profile(kernel)
+
+
+def issue_frac(warp_inst, ms, sm_mhz, sms=148):
+    """Warp instructions per launch over the SMs' issue capacity in the launch's
+    time (4 schedulers per SM, one warp instruction per clock each)."""
+    if not warp_inst or not sm_mhz or ms <= 0:
+        return None
+    return round(warp_inst / (sms * 4 * sm_mhz * 1e6 * ms * 1e-3), 4)
 
 
 class ClockSampler:
@@ -105,19 +118,81 @@ class ClockSampler:
                 "reasons": reasons, "samples": len(rows)}
 
 
-def cpu_chain_ms(cfg_small, scale, repeats=1):
-    """Time the CPU chain (oracle restatement of the reference nodes) on a
-    sample frame; returns ms per 12 MP frame (area-scaled) and the sample."""
+def host_cpu():
+    """CPU model, logical CPUs, and the CPUs this process may run on."""
+    model = "unknown"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    usable = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    return {"model": model, "nproc": os.cpu_count(), "usable": usable}
+
+
+def reference_cpu_chain(cfg):
+    """The reference's CPU chain for `cfg` (oracle/chain_oracle.run_reference_chain:
+    the reference's own plain-C++ filters from oracle/_ref, single-threaded as
+    the reference runs them; C restatements of its Halide nodes with OpenMP over
+    rows on every usable CPU).  Its blobs come from oracle/oracle_blobs, so the
+    product library is never loaded.  Returns (run, threads, label)."""
+    threads = host_cpu()["usable"]
+    os.environ["OMP_NUM_THREADS"] = str(threads)
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
-    from chain_oracle import run_chain_oracle
-    raw = cfg_small.make_raw()
-    b = cfg_small.blobs()
-    times = []
-    for _ in range(repeats):
+    import oracle
+    import oracle_blobs
+    from chain_oracle import run_reference_chain
+    if oracle.ref_lib() is None:
+        raise RuntimeError("the reference build oracle/_ref is absent")
+    blobs = oracle_blobs.chain_blobs(cfg)
+    raw = cfg.make_raw()
+
+    def run():
         t0 = time.perf_counter()
-        run_chain_oracle(cfg_small, raw, blobs=b)
-        times.append(time.perf_counter() - t0)
-    return 1000.0 * min(times) * scale
+        run_reference_chain(cfg, raw, blobs)
+        return 1000.0 * (time.perf_counter() - t0)
+    label = (f"full {cfg.width}x{cfg.height} frame per step through the reference's CPU chain: its plain-C++ "
+             "filters (blacklevel, GainMap, OpcodeList3 warp, WB, colormatrix) compiled from its source, "
+             "single-threaded as the reference runs them; C restatements of its Halide nodes (convert, RCD, "
+             "denoise.bm3d, guided, wavelet, filmic, 3D LUT; Halide is not buildable here), OpenMP over rows "
+             f"on {threads} threads")
+    return run, threads, label
+
+
+def bm3d_cpu_crop(n=768):
+    """The two-stage BM3D FP64 oracle (oracle_bm3d.c, OpenMP) on an n x n crop
+    of a seeded noisy RGBA16F frame: the CPU anchor of the BM3D chain."""
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+    from cpipe_b200.scene import scene_rgb
+    rng = np.random.default_rng(0x5EED0002)
+    x = np.ones((n, n, 4), np.float32)
+    x[..., :3] = scene_rgb(n, n, 0x5EED0002) + rng.normal(0.0, 0.032, (n, n, 3))
+    x = x.astype(np.float16).astype(np.float32)
+    from cpipe_b200 import blobs as B  # ctypes struct layout only; the library is not loaded
+    blob = B.bm3d_spec(0.032)
+    t0 = time.perf_counter()
+    oracle.bm3d_spec(x, blob)
+    ms = 1000.0 * (time.perf_counter() - t0)
+    return {"crop": f"{n}x{n}", "crop_ms": round(ms, 1), "mp_per_s": round(n * n / 1e6 / (ms * 1e-3), 4),
+            "threads": int(os.environ.get("OMP_NUM_THREADS", host_cpu()["usable"])), "kind": "port",
+            "note": "FP64 oracle of the two-stage BM3D (8x8 blocks, 16-block groups, 39x39 search, step 3) on a "
+                    "crop, not a 12 MP frame"}
+
+
+def workload_config(cfg, world):
+    """The `config` object both arms print (the reference arm computes the same
+    chain with the reference's own denoise.bm3d in the denoiser slot)."""
+    return {"workload": cfg.name, "frame": f"{cfg.width}x{cfg.height} RGGB 10-bit",
+            "nodes": ["precision_convert", "blacklevel", "gainmap 17x13", "demosaic.rcd", "opcode_list_3 warp",
+                      "wb.dual_illuminant", "colormatrix", "denoiser", "guided r8 (5x5 box, as the reference)",
+                      "wavelet (2x2 Haar, as the reference)", "filmic", "3d_lut 33^3"],
+            "l2": "inputs larger than L2: ring of 8 raw frames (195 MB) and 2 output frames",
+            "parallelism": f"replicas x{world}"}
 
 
 # ------------------------------------------------------------ rank helpers
@@ -147,28 +222,34 @@ def whole_job_ms_per_frame(max_ms, steps, world):
 
 
 def reference_arm(args):
-    rank = int(os.environ.get("RANK", "0"))
+    rank, world, _ = rank_env(args.gpus)
     if rank != 0:
         return 0
     from cpipe_b200.chain import ChainConfig
-    cores = os.cpu_count()
-    os.environ.setdefault("OMP_NUM_THREADS", str(cores))
-    full = ChainConfig.full_12mp()
-    sample = ChainConfig.full_12mp(width=1008, height=756, name="sample_1008x756")
-    scale = (full.width * full.height) / (sample.width * sample.height)
+    cfg = ChainConfig.full_12mp()
+    cpu = host_cpu()
+    try:
+        run, threads, label = reference_cpu_chain(cfg)
+    except Exception as e:  # noqa: BLE001
+        print(json.dumps({"impl": "reference", "unavailable": f"reference CPU chain: {e}"}), flush=True)
+        return 0
     for _ in range(args.warmup):
-        cpu_chain_ms(sample, scale)
-    vals = [cpu_chain_ms(sample, scale) for _ in range(args.steps)]
-    v = statistics.median(vals)
+        run()
+    t0 = time.perf_counter()
+    steps = [run() for _ in range(args.steps)]
+    total_ms = 1000.0 * (time.perf_counter() - t0)
+    v = total_ms / args.steps
     line = {"impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "ms/frame", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(v, 3), "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Philox scene)",
-            "config": {"workload": full.name, "sample": sample.name},
-            "cpu_baseline": {"value": round(v, 3), "unit": "ms/frame", "cores": cores, "kind": "port",
-                             "sample": f"one {sample.width}x{sample.height} frame of the same chain per step, "
-                                       f"scaled x{scale:.0f} by area; C restatement of the reference nodes "
-                                       "(plain-C++ filters single-threaded as in the reference, Halide "
-                                       "restatements OpenMP over rows)"},
+            "config": workload_config(cfg, world),
+            "denoiser_slot": "denoise.bm3d as the reference computes it: a 2x2 box blend (the reference has no "
+                             "block-matching BM3D and no learned denoiser)",
+            "step_ms": {"min": round(min(steps), 1), "median": round(statistics.median(steps), 1),
+                        "max": round(max(steps), 1)},
+            "cpu": cpu,
+            "cpu_baseline": {"value": round(v, 3), "unit": "ms/frame", "cores": threads, "kind": "reference",
+                             "sample": label},
             "e2e": {"value": round(v, 3), "unit": "ms/frame", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
     return 0
@@ -268,6 +349,55 @@ def spec_form(peak_gbs):
     L.cpipe_cuda_device_free(d_raw)
     L.cpipe_cuda_device_free(d_out)
     return out
+
+
+def config1_chain(peak_gbs):
+    """The plain chain at its configured size (2016x1512 RGGB 12-bit, black 64,
+    WB (2, 1, 1.6), RCD, camera matrix, denoise.bm3d with sigma from the noise
+    model, wavelet, filmic, identity+gamma 33^3 LUT): CUDA events around 50
+    frames after 5, inputs rotating through 8 raw frames and 4 outputs (147 MB,
+    more than L2); bytes = the raw frame read and the RGBA16F frame written once
+    (10 B/px)."""
+    import numpy as np
+    from cpipe_b200 import _abi as A
+    from cpipe_b200.chain import Chain, ChainConfig
+    L = A.lib()
+    cfg = ChainConfig.small_frame()
+    w, h = cfg.width, cfg.height
+    base = cfg.make_raw()
+    d_raw, d_out = [], []
+    for k in range(8):
+        fr = np.ascontiguousarray(np.roll(base, (2 * k, 4 * k), axis=(0, 1)))
+        p = C.c_void_p()
+        assert L.cpipe_cuda_device_alloc(fr.nbytes, C.byref(p)) == 0
+        assert L.cpipe_cuda_memcpy_h2d(p, fr.ctypes.data, fr.nbytes) == 0
+        d_raw.append(p)
+    for _ in range(4):
+        p = C.c_void_p()
+        assert L.cpipe_cuda_device_alloc(w * h * 8, C.byref(p)) == 0
+        d_out.append(p)
+    ch = Chain(cfg)
+    e0, e1 = C.c_void_p(), C.c_void_p()
+    L.cpipe_cuda_event_create(C.byref(e0))
+    L.cpipe_cuda_event_create(C.byref(e1))
+    for i in range(5):
+        ch.run(d_raw[i % 8].value, d_out[i % 4].value)
+    n = 50
+    L.cpipe_cuda_event_record(e0, None)
+    for i in range(n):
+        ch.run(d_raw[i % 8].value, d_out[i % 4].value)
+    L.cpipe_cuda_event_record(e1, None)
+    assert L.cpipe_cuda_synchronize() == 0
+    ms = C.c_float()
+    L.cpipe_cuda_event_elapsed_ms(e0, e1, C.byref(ms))
+    t = ms.value / n
+    ch.close()
+    for p in d_raw + d_out:
+        L.cpipe_cuda_device_free(p)
+    gbs = 10.0 * w * h / (t * 1e-3) / 1e9
+    return {"workload": cfg.name, "frame": f"{w}x{h} RGGB 12-bit", "ms_per_frame": round(t, 4),
+            "mp_per_s": round(w * h / 1e6 / (t * 1e-3), 1), "bytes_per_px": 10, "achieved_gbs": round(gbs, 1),
+            "frac": round(gbs / peak_gbs, 4)}
 
 
 def finishing_stages():
@@ -567,24 +697,24 @@ def b200_arm(args):
     hidden_flop = HIDDEN_FLOP_PER_PX * w * h
     achieved_tf = hidden_flop / (hidden_ms * 1e-3) / 1e12
     peak_gbs, gbs_kind = measured_peak_gbs()
-    hbm = {k: {"ms": round(stages[k], 4),
-               "achieved_gbs": round(BYTES_PER_PX[k] * w * h / (stages[k] * 1e-3) / 1e9, 1),
-               "frac": round(BYTES_PER_PX[k] * w * h / (stages[k] * 1e-3) / 1e9 / peak_gbs, 4),
-               "traffic": traffic_per_launch(k)} for k in BYTES_PER_PX}
+    hbm = {k: {"ms": round(ref_stages[k], 4),
+               "achieved_gbs": round(BYTES_PER_PX[k] * w * h / (ref_stages[k] * 1e-3) / 1e9, 1),
+               "frac": round(BYTES_PER_PX[k] * w * h / (ref_stages[k] * 1e-3) / 1e9 / peak_gbs, 4),
+               "traffic": traffic_per_launch(k),
+               "warp_inst": chain_profile(k, "warp_inst_per_launch"),
+               "issue_frac": issue_frac(chain_profile(k, "warp_inst_per_launch"), ref_stages[k],
+                                        clk.get("sm_mhz"))} for k in BYTES_PER_PX}
     line = {
         "metric": METRIC, "value": round(value, 4), "unit": "ms/frame", "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": round(total_ms / args.steps, 4), "higher_is_better": False,
         "scaling": "weak", "vs_baseline": None, "dtype": "bf16", "data": "synthetic (seeded Philox scene)",
-        "config": {"workload": cfg.name, "frame": f"{w}x{h} RGGB 10-bit",
-                   "denoiser": "learned surrogate: 8 3x3 conv layers, 32 channels, BF16, FP32 accumulation; "
-                               "per frame BM3D spot check on 16 256x256 tiles, BM3D fallback below 40 dB",
-                   "compared_with": "the same chain with two-stage BM3D (8x8 blocks, 16-block groups, 39x39 "
-                                    "search, step 3, hard threshold + Wiener), FP32",
-                   "nodes": ["precision_convert", "blacklevel", "gainmap 17x13", "demosaic.rcd",
-                             "opcode_list_3 warp", "wb.dual_illuminant", "colormatrix", "denoiser", "guided r8",
-                             "wavelet", "filmic", "3d_lut 33^3"],
-                   "l2": "inputs larger than L2: ring of 8 raw frames (195 MB) and 2 output frames",
-                   "parallelism": f"replicas x{world}"},
+        "config": workload_config(cfg, world),
+        "denoiser_slot": {"denoiser": "learned surrogate: 8 3x3 conv layers, 32 channels, BF16, FP32 accumulation; "
+                                      "per frame BM3D spot check on 16 256x256 tiles, BM3D fallback below 40 dB",
+                          "compared_with": "the same chain with two-stage BM3D (8x8 blocks, 16-block groups, 39x39 "
+                                           "search, step 3, hard threshold + Wiener); group transforms on the "
+                                           "tensor cores (mma.sync) with hi/lo-split FP16 operands and FP32 "
+                                           "accumulation, matching and aggregation in FP32"},
         "per_stage_ms": {k: round(v, 4) for k, v in stages.items()},
         "bm3d_chain": {"ms_per_frame": round(bm3d_value, 3), "frames": bm3d_frames,
                        "per_stage_ms": {k: round(v, 4) for k, v in bm3d_stages.items()}},
@@ -602,7 +732,10 @@ def b200_arm(args):
                      "achieved": round(achieved_tf, 1), "peak": peak_tf, "peak_kind": peak_kind,
                      "unit": "TFLOP/s", "frac": round(achieved_tf / peak_tf, 4),
                      "algorithmic_flop": hidden_flop, "traffic": traffic_surrogate_hidden(w * h)},
-        "hbm_roofline": {"peak_gbs": peak_gbs, "peak_kind": gbs_kind, "kernels": hbm},
+        "hbm_roofline": {"peak_gbs": peak_gbs, "peak_kind": gbs_kind, "kernels": hbm,
+                         "note": "chain kernels of the reference-computation chain (CUDA events); warp_inst from "
+                                 "the committed ncu summary; issue_frac = warp_inst / (148 SMs x 4 x median SM "
+                                 "clock x time)"},
         "e2e": {"value": round(whole_job_ms_per_frame(e2e_ms, e2e_steps, world), 4), "unit": "ms/frame",
                 "h2d_bytes_per_step": raw_bytes, "d2h_bytes_per_step": out_bytes,
                 "api": "cpipe_cuda_chain_run_host_frames (copies overlapped with the neighbouring frames)",
@@ -614,6 +747,7 @@ def b200_arm(args):
         line["batched_form"] = batched_form()
         line["spec_form"] = spec_form(peak_gbs)
         line["finishing_stages"] = finishing_stages()
+        line["config1_chain"] = config1_chain(peak_gbs)
         line["dng_ingest"] = dng_ingest(peak_gbs)
         line["node_roofline"] = {"peak_gbs": peak_gbs, "peak_kind": gbs_kind,
                                  "note": "each node's filter alone, 12 MP device buffers, bytes = its input and "
@@ -621,15 +755,12 @@ def b200_arm(args):
                                  "nodes": node_roofline(w, h, peak_gbs=peak_gbs)}
         line["qbc_50mp"] = qbc_50mp(weights)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        sample = ChainConfig.full_12mp(width=2016, height=1512, name="sample_2016x1512")
-        scale = (w * h) / (sample.width * sample.height)
-        os.environ.setdefault("OMP_NUM_THREADS", str(os.cpu_count()))
-        v = cpu_chain_ms(sample, scale)
-        line["cpu_baseline"] = {"value": round(v, 1), "unit": "ms/frame", "cores": os.cpu_count(), "kind": "port",
-                                "sample": "one 2016x1512 frame of the reference's chain (denoise.bm3d as the "
-                                          "reference computes it), scaled x4 by area; C restatement of the "
-                                          "reference nodes (plain-C++ filters single-threaded as in the "
-                                          "reference, Halide restatements OpenMP over rows)"}
+        run, threads, label = reference_cpu_chain(ChainConfig.full_12mp())
+        v = run()
+        line["cpu_baseline"] = {"value": round(v, 1), "unit": "ms/frame", "cores": threads, "kind": "reference",
+                                "sample": "one " + label[len("full "):].replace(" per step", "", 1),
+                                "cpu": host_cpu()}
+        line["cpu_baseline_bm3d"] = bm3d_cpu_crop()
     for c in (chain, bm3d_chain, ref_chain):
         c.close()
     if rank == 0:

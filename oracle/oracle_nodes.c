@@ -465,9 +465,23 @@ static void gf_ab(const rgba_t* I, int x, int y, int c, int r, float eps, float*
     *a = var / (var + eps);
     *b = m - (*a * m);
 }
+/* The generator inlines a and b at every use (25 or 9 evaluations per output);
+ * here each is evaluated once per position of the extended domain
+ * [-r, w + r) x [-r, h + r) that the output boxes read, on the same clamped
+ * input, so the box sums add the same floats in the same order. */
 void oracle_guided(const float* in, float* out, int w, int h, int radius, float eps, int f16) {
     rgba_t I = {in, w, h};
     const int r = radius <= 1 ? 1 : 2;
+    const long ew = w + 2 * r, eh = h + 2 * r;
+    float* ab = (float*)malloc(sizeof(float) * 6 * (size_t)ew * (size_t)eh);
+    if (ab == NULL) return;
+#pragma omp parallel for schedule(static)
+    for (long yy = 0; yy < eh; ++yy)
+        for (long xx = 0; xx < ew; ++xx)
+            for (int c = 0; c < 3; ++c) {
+                float* d = ab + 6 * (yy * ew + xx) + 2 * c;
+                gf_ab(&I, (int)xx - r, (int)yy - r, c, r, eps, &d[0], &d[1]);
+            }
 #pragma omp parallel for schedule(static)
     for (int y = 0; y < h; ++y) {
         for (int x = 0; x < w; ++x) {
@@ -477,33 +491,29 @@ void oracle_guided(const float* in, float* out, int w, int h, int radius, float 
                 if (c == 3) {
                     o = v;
                 } else {
-                    float sa = 0.0F, sb = 0.0F, a, b;
-                    if (r == 1) {
-                        float av[9], bv[9];
-                        int k = 0;
-                        for (int dy = -1; dy <= 1; ++dy)
-                            for (int dx = -1; dx <= 1; ++dx, ++k) gf_ab(&I, x + dx, y + dy, c, r, eps, &av[k], &bv[k]);
-                        sa = av[0];
-                        sb = bv[0];
-                        for (int i = 1; i < 9; ++i) { sa = sa + av[i]; sb = sb + bv[i]; }
-                        sa = sa / 9.0F;
-                        sb = sb / 9.0F;
-                    } else {
-                        for (int dy = -2; dy <= 2; ++dy)
-                            for (int dx = -2; dx <= 2; ++dx) {
-                                gf_ab(&I, x + dx, y + dy, c, r, eps, &a, &b);
-                                sa += a;
-                                sb += b;
+                    float sa = 0.0F, sb = 0.0F;
+                    int first = 1;
+                    for (int dy = -r; dy <= r; ++dy)
+                        for (int dx = -r; dx <= r; ++dx) {
+                            const float* d = ab + 6 * ((long)(y + dy + r) * ew + (x + dx + r)) + 2 * c;
+                            if (r == 1 && first) {
+                                sa = d[0];
+                                sb = d[1];
+                                first = 0;
+                            } else {
+                                sa = sa + d[0];
+                                sb = sb + d[1];
                             }
-                        sa = sa / 25.0F;
-                        sb = sb / 25.0F;
-                    }
+                        }
+                    sa = r == 1 ? sa / 9.0F : sa / 25.0F;
+                    sb = r == 1 ? sb / 9.0F : sb / 25.0F;
                     o = maxf(0.0F, (sa * v) + sb);
                 }
                 out[4 * ((long)y * w + x) + c] = rnd(o, f16);
             }
         }
     }
+    free(ab);
 }
 
 /* ---- a13: wavelet Bayes shrink (denoise/wavelet_bayes_shrink_generator.cpp:9-31,57-86) ---- */

@@ -340,3 +340,43 @@ def test_chain_tone_choice_equals_nodes(host, kw):
     chain.close()
     want = run_nodes_on_gpu(host, cfg, raw)
     np.testing.assert_array_equal(got.view(np.uint8), want.view(np.uint8))
+
+
+def test_config1_small_frame_as_configured(cuda_device, host):
+    """The plain chain at its configured size: 2016x1512 RGGB 12-bit (black 64,
+    white 4095, a=1e-3, b=1e-5), WB gains (2, 1, 1.6), RCD, the camera matrix
+    to Rec.2020, denoise.bm3d with sigma from the noise model, filmic and the
+    identity+gamma 33^3 LUT; no GainMap, warp or guided filter (the wavelet
+    node stays, as the reference loader requires it upstream of filmic).
+    The fused chain equals the nodes run one by one bit for bit, and the CPU
+    oracle within the RGBA16F tolerance; with the reference's own plain-C++
+    filters in the chain (oracle/_ref) the CPU result is the same floats."""
+    import oracle_blobs
+    from chain_oracle import run_reference_chain
+    cfg = ChainConfig.small_frame()
+    assert (cfg.width, cfg.height, cfg.bits, cfg.black, cfg.white) == (2016, 1512, 12, 64.0, 4095)
+    assert not cfg.gainmap and cfg.warp is None and cfg.guided_radius == 0 and cfg.lut == "identity_gamma"
+    raw = cfg.make_raw()
+    chain = Chain(cfg)
+    got = chain.run_host(raw)
+    chain.close()
+    nodes = run_nodes_on_gpu(host, cfg, raw)
+    assert f16_ulp_distance(got, nodes).max() == 0, "fused differs from node-by-node"
+    want = run_chain_oracle(cfg, raw)
+    assert_f16_parity(got, want, what="config 1 chain vs oracle")
+    import oracle as O
+    if O.ref_lib() is not None:
+        ref = run_reference_chain(cfg, raw, oracle_blobs.chain_blobs(cfg))
+        np.testing.assert_array_equal(ref.view(np.uint32), want.view(np.uint32))
+
+
+def test_config1_small_frame_plain_f32(cuda_device):
+    """Config 1 in the FP32 plain form (RGBA f32 between the nodes): max-abs
+    <= 1e-4 and PSNR >= 60 dB against the FP32 oracle chain."""
+    cfg = ChainConfig.small_frame(plain_f32=True)
+    raw = cfg.make_raw()
+    chain = Chain(cfg)
+    got = chain.run_host(raw)
+    chain.close()
+    assert got.dtype == np.float32
+    assert_f32_parity(got, run_chain_oracle(cfg, raw), what="config 1 chain f32")
