@@ -211,7 +211,8 @@ EXPORTS = [
     "cpipe_cuda_precision_convert_rgba16f_to_rgba8", "cpipe_cuda_precision_convert_rgba16f_to_rgba16u",
     "cpipe_cuda_demosaic_quad_bayer_remosaic", "cpipe_cuda_linearize_dng_lut", "cpipe_cuda_blacklevel_dng_levels",
     "cpipe_cuda_lens_shading_gainmap", "cpipe_cuda_demosaic_bilinear", "cpipe_cuda_demosaic_rcd",
-    "cpipe_cuda_demosaic_amaze", "cpipe_cuda_wb_dual_illuminant", "cpipe_cuda_colormatrix_dng_to_working",
+    "cpipe_cuda_demosaic_amaze", "cpipe_cuda_demosaic_rcd_full", "cpipe_cuda_demosaic_amaze_full",
+    "cpipe_cuda_wb_dual_illuminant", "cpipe_cuda_colormatrix_dng_to_working",
     "cpipe_cuda_denoise_bm3d_step1", "cpipe_cuda_denoise_bm3d_step2", "cpipe_cuda_denoise_bm3d_spec",
     "cpipe_cuda_denoise_guided_filter_spec", "cpipe_cuda_denoise_wavelet_atrous_spec",
     "cpipe_cuda_denoise_guided_filter",

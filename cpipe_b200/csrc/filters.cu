@@ -620,6 +620,43 @@ int cpipe_cuda_demosaic_amaze(halide_buffer_t* const* i, size_t ni, halide_buffe
     return demosaic_filter(2, i, ni, o, no, b, bs);
 }
 
+// Full-form RCD / AMaZE (no reference filter: the reference's nodes compute the
+// reduced stencils above).  Bayer patterns with the two greens on a diagonal.
+static int demosaic_full_filter(int algo, halide_buffer_t* const* inputs, size_t n_in, halide_buffer_t* const* outputs,
+                                size_t n_out, const void* blob, size_t blob_size) {
+    CHECK_ARITY(1, 1);
+    if (blob == nullptr || blob_size < sizeof(cpipe_DemosaicParams)) return CPIPE_BAD_INDEX;
+    const auto* p = static_cast<const cpipe_DemosaicParams*>(blob);
+    const int cfa[4] = {p->cfa_pattern[0], p->cfa_pattern[1], p->cfa_pattern[2], p->cfa_pattern[3]};
+    const bool bayer = ((cfa[0] == 1 && cfa[3] == 1 && cfa[1] + cfa[2] == 2 && cfa[1] != 1) ||
+                        (cfa[1] == 1 && cfa[2] == 1 && cfa[0] + cfa[3] == 2 && cfa[0] != 1));
+    if (!bayer) {
+        set_error("%s", "full-form demosaic needs a 2x2 Bayer pattern (RGGB, BGGR, GRBG, GBRG)");
+        return CPIPE_UNSUPPORTED;
+    }
+    if (!device_ready()) return CPIPE_INTERNAL_ERROR;
+    Call call;
+    BIND(0, inputs, Kind::BayerF32, false, in);
+    BIND(0, outputs, Kind::Rgba, true, out);
+    REQUIRE_SAME_EXTENT(in, out);
+    void* scratch = nullptr;
+    const size_t bytes = demosaic_full_scratch_bytes(algo, in.img.w, in.img.h);
+    if (bytes) {
+        const int st = call.alloc(bytes, &scratch);
+        if (st != CPIPE_OK) return call.finish(st);
+    }
+    return call.finish(cuda_status(launch_demosaic_full(algo, in.img, out.img, out.elem == 2, cfa, scratch, call.stream),
+                                   "demosaic full"));
+}
+int cpipe_cuda_demosaic_rcd_full(halide_buffer_t* const* i, size_t ni, halide_buffer_t* const* o, size_t no,
+                                 const void* b, size_t bs) {
+    return demosaic_full_filter(1, i, ni, o, no, b, bs);
+}
+int cpipe_cuda_demosaic_amaze_full(halide_buffer_t* const* i, size_t ni, halide_buffer_t* const* o, size_t no,
+                                   const void* b, size_t bs) {
+    return demosaic_full_filter(2, i, ni, o, no, b, bs);
+}
+
 // ------------------------------------------------------------ a8 QBC remosaic
 int cpipe_cuda_demosaic_quad_bayer_remosaic(halide_buffer_t* input, halide_buffer_t* output) {
     if (!device_ready()) return CPIPE_INTERNAL_ERROR;
@@ -1199,6 +1236,8 @@ static const cpipe_cuda_filter_desc kFilters[] = {
     {"demosaic_bilinear", (void*)&cpipe_cuda_demosaic_bilinear, 1},
     {"demosaic_rcd", (void*)&cpipe_cuda_demosaic_rcd, 1},
     {"demosaic_amaze", (void*)&cpipe_cuda_demosaic_amaze, 1},
+    {"demosaic_rcd_full", (void*)&cpipe_cuda_demosaic_rcd_full, 1},
+    {"demosaic_amaze_full", (void*)&cpipe_cuda_demosaic_amaze_full, 1},
     {"wb_dual_illuminant", (void*)&cpipe_cuda_wb_dual_illuminant, 1},
     {"colormatrix_dng_to_working", (void*)&cpipe_cuda_colormatrix_dng_to_working, 1},
     {"denoise_bm3d_step1", (void*)&cpipe_cuda_denoise_bm3d_step1, 1},

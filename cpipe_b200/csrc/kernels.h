@@ -27,6 +27,11 @@ cudaError_t launch_copy(const void* src, long long src_pitch, void* dst, long lo
                         int rows, cudaStream_t st);
 cudaError_t launch_demosaic(int algo, const Img& in, const Img& out, bool out_f16, const int cfa[4], cudaStream_t st);
 cudaError_t launch_qbc_remosaic(const Img& in, const Img& out, cudaStream_t st);
+// Full-form RCD (algo 1) and AMaZE (algo 2) demosaics (demosaic_full.cu); AMaZE
+// needs demosaic_full_scratch_bytes(2, w, h) of device scratch (RCD none).
+size_t demosaic_full_scratch_bytes(int algo, int w, int h);
+cudaError_t launch_demosaic_full(int algo, const Img& in, const Img& out, bool out_f16, const int cfa[4], void* scratch,
+                                 cudaStream_t st);
 cudaError_t launch_f32_to_rgba16f(const Img& in, const Img& out, cudaStream_t st);
 cudaError_t launch_rgba16f_to_unorm(const Img& in, const Img& out, int bits8, cudaStream_t st);
 cudaError_t launch_wb(const Img& in, const Img& out, bool f16, const float n[3], cudaStream_t st);

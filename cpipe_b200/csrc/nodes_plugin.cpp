@@ -263,9 +263,14 @@ int node_demosaic(Ctx& c, const char* aot) {
         for (const auto& p : kSupported) ok = ok || std::memcmp(p, cal.cfa_pattern, 4) == 0;
     }
     if (!ok) return CPIPE_UNSUPPORTED;
+    std::string algorithm = "reference";
+    c.get_string("algorithm", &algorithm);
+    std::string id = aot;
+    if (algorithm == "full" && id != "demosaic_bilinear") id += "_full";
+    else if (algorithm != "reference") return CPIPE_BAD_INDEX;
     cpipe_DemosaicParams p{};
     std::memcpy(p.cfa_pattern, cal.cfa_pattern, 4);
-    int st = c.submit(aot, &p, sizeof(p));
+    int st = c.submit(id.c_str(), &p, sizeof(p));
     if (st != CPIPE_OK) return st;
     if ((st = c.mb->clear_cfa(c.builder())) != CPIPE_OK) return st;
     return c.step("demosaic");
@@ -708,13 +713,16 @@ const char kGainmap[] = MANIFEST("com.cpipe.lens.shading_gainmap", "Lens Shading
     PORT("linear_bayer", "in", "\"r\"", "\"f32\"", "\"requires_fields\":[\"calibration.cfa\"],\"requires_blobs\":[\"com.cpipe.dng.opcode_list_2_bytes\"]"),
     PORT("corrected_bayer", "out", "\"r\"", "\"f32\"", "\"inherits_from\":\"linear_bayer\",\"sets_steps_applied\":[\"lens_shading_gainmap\"]"),
     "", "raw_camera", "raw_camera", "false", "\"raw_point<gainmap>\"");
-#define DEMOSAIC_MANIFEST(id, label, k) MANIFEST(id, label, "raw",                                                   \
+#define DEMOSAIC_MANIFEST(id, label, params, k) MANIFEST(id, label, "raw",                                           \
     PORT("bayer", "in", "\"r\"", "\"f32\"", "\"requires_steps_applied\":[\"black_white_scaling\"],\"requires_fields\":[\"calibration.cfa\"]"), \
     PORT("rgba", "out", "\"rgba\"", "\"f16\",\"f32\"", "\"inherits_from\":\"bayer\",\"clears_fields\":[\"calibration.cfa\"],\"sets_steps_applied\":[\"demosaic\"]"), \
-    "", "raw_camera", "raw_camera", "false", k)
-const char kRcd[] = DEMOSAIC_MANIFEST("com.cpipe.demosaic.rcd", "RCD Demosaic", "\"demosaic_kernel<rcd>\"");
-const char kAmaze[] = DEMOSAIC_MANIFEST("com.cpipe.demosaic.amaze", "AMaZE Demosaic", "\"demosaic_kernel<amaze>\"");
-const char kBilinear[] = DEMOSAIC_MANIFEST("com.cpipe.demosaic.bilinear", "Bilinear Demosaic", "\"demosaic_kernel<bilinear>\"");
+    params, "raw_camera", "raw_camera", "false", k)
+#define DEMOSAIC_ALGORITHM "{\"name\":\"algorithm\",\"type\":\"enum\",\"values\":[\"reference\",\"full\"],\"default\":\"reference\"}"
+const char kRcd[] = DEMOSAIC_MANIFEST("com.cpipe.demosaic.rcd", "RCD Demosaic", DEMOSAIC_ALGORITHM,
+                                      "\"demosaic_kernel<rcd>\",\"rcd_full_kernel\"");
+const char kAmaze[] = DEMOSAIC_MANIFEST("com.cpipe.demosaic.amaze", "AMaZE Demosaic", DEMOSAIC_ALGORITHM,
+                                        "\"demosaic_kernel<amaze>\",\"amaze_cd_kernel\",\"amaze_green_kernel\",\"amaze_out_kernel\"");
+const char kBilinear[] = DEMOSAIC_MANIFEST("com.cpipe.demosaic.bilinear", "Bilinear Demosaic", "", "\"demosaic_kernel<bilinear>\"");
 const char kQbc[] = MANIFEST("com.cpipe.demosaic.quad_bayer_remosaic", "Quad Bayer Remosaic", "raw",
     PORT("qbc", "in", "\"r\"", "\"u16\"", "\"requires_fields\":[\"calibration.cfa\"]"),
     PORT("bayer", "out", "\"r\"", "\"u16\"", "\"inherits_from\":\"qbc\",\"writes_fields\":[\"calibration.cfa\"],\"sets_steps_applied\":[\"quad_bayer_remosaic\"]"),

@@ -39,8 +39,8 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 # "issue" -- the reference's per-pixel arithmetic (RCD/AMaZE ratios, the QBC
 # 25-tap integer weights, the guided filter's exact-order box sums, the warp's
 # float-float coordinates and bicubic taps, filmic's log per channel, USM's
-# exact-order sums and divisions, the PQ encode's two powers per channel) sets
-# the floor; "gather" -- 3D LUT cell reads through L1/L2.
+# exact-order sums and divisions, the PQ encode's two powers per channel, the
+# full-form RCD / AMaZE stages) sets the floor; "gather" -- 3D LUT cell reads through L1/L2.
 NODES = [
     ("a1 precision_convert", "precision_convert_r16u_to_f32", "u16", "f32", 6, None, "hbm"),
     ("a2 linearize", "linearize_dng_lut", "u16", "f32", 6, "linearize", "hbm"),
@@ -49,6 +49,8 @@ NODES = [
     ("a5 demosaic RCD", "demosaic_rcd", "f32", "rgba", 12, "demosaic", "issue"),
     ("a6 demosaic AMaZE", "demosaic_amaze", "f32", "rgba", 12, "demosaic", "issue"),
     ("a7 demosaic bilinear", "demosaic_bilinear", "f32", "rgba", 12, "demosaic", "hbm"),
+    ("a5 demosaic RCD (full form)", "demosaic_rcd_full", "f32", "rgba", 12, "demosaic", "issue"),
+    ("a6 demosaic AMaZE (full form)", "demosaic_amaze_full", "f32", "rgba", 12, "demosaic", "issue"),
     ("a8 QBC remosaic", "demosaic_quad_bayer_remosaic", "u16", "u16", 4, None, "issue"),
     ("a9 WB", "wb_dual_illuminant", "rgba", "rgba", 16, "wb", "hbm"),
     ("a10 colormatrix", "colormatrix_dng_to_working", "rgba", "rgba", 16, "colormatrix", "hbm"),

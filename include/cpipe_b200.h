@@ -81,7 +81,16 @@ CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_blacklevel_dng_levels);      /* blacklevel_dn
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_lens_shading_gainmap);       /* shading_gainmap_dispatch.cpp:73-133 */
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_demosaic_bilinear);          /* demosaic_bilinear_dispatch.cpp */
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_demosaic_rcd);               /* demosaic_rcd_dispatch.cpp:19-38 */
-CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_demosaic_amaze);             /* demosaic_amaze_dispatch.cpp */
+CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_demosaic_amaze);
+/* Full-form RCD and AMaZE (aot_ids "demosaic_rcd_full", "demosaic_amaze_full";
+ * node parameter algorithm = "full" of com.cpipe.demosaic.rcd / .amaze): the
+ * published algorithms the reference's reduced 5x5 stencils are named after
+ * (demosaic_rcd_generator.cpp:8-77, demosaic_amaze_generator.cpp:8-79 are the
+ * nodes they stand beside; no reference filter counterpart).  Same buffers and
+ * blob as the reference demosaic filters; 2x2 Bayer patterns only
+ * (otherwise CPIPE_UNSUPPORTED). */
+CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_demosaic_rcd_full);
+CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_demosaic_amaze_full);             /* demosaic_amaze_dispatch.cpp */
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_wb_dual_illuminant);         /* wb_dual_illuminant_dispatch.cpp:16-48 */
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_colormatrix_dng_to_working); /* colormatrix_dng_to_working_dispatch.cpp:17-62 */
 CPIPE_CUDA_PARAM_FILTER(cpipe_cuda_denoise_bm3d_step1);         /* bm3d_dispatch.cpp:19-30 */

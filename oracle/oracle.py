@@ -116,6 +116,28 @@ def demosaic(algo, x, cfa4, f16=True):
     return out
 
 
+def demosaic_full(algo, x, cfa4, prec="f32"):
+    """Full-form RCD ('rcd') or AMaZE ('amaze') of oracle_demosaic_full.c.
+    x: HxW float32 normalised mosaic.  prec 'f32': the kernels' binary32
+    arithmetic; 'f64': the FP64 reference.  Returns HxWx3 float64 RGB."""
+    x = _f32(x)
+    h, w = x.shape
+    out = np.empty((h, w, 3), np.float64)
+    cfa = (C.c_uint8 * 4)(*cfa4)
+    st = lib().oracle_demosaic_full({"rcd": 1, "amaze": 2}[algo], {"f32": 0, "f64": 1}[prec], _p(x), w, h, cfa,
+                                    _p(out))
+    if st != 0:
+        raise MemoryError("oracle_demosaic_full")
+    return out
+
+
+def rgba_from_rgb(rgb, f16=True):
+    """HxWx3 -> HxWx4 float32 with alpha 1, rounded to binary16 when f16."""
+    out = np.ones(rgb.shape[:2] + (4,), np.float32)
+    out[..., :3] = np.asarray(rgb, np.float32)
+    return h16(out) if f16 else out
+
+
 def qbc_remosaic(raw):
     raw = np.ascontiguousarray(raw, dtype=np.uint16)
     out = np.empty_like(raw)

@@ -55,8 +55,8 @@ EXPECTED_NODES = {
     "com.cpipe.linearize.dng_lut": ("raw", "bayer", []),
     "com.cpipe.blacklevel.dng_levels": ("bayer", "bayer", []),
     "com.cpipe.lens.shading_gainmap": ("linear_bayer", "corrected_bayer", []),
-    "com.cpipe.demosaic.rcd": ("bayer", "rgba", []),
-    "com.cpipe.demosaic.amaze": ("bayer", "rgba", []),
+    "com.cpipe.demosaic.rcd": ("bayer", "rgba", ["algorithm"]),
+    "com.cpipe.demosaic.amaze": ("bayer", "rgba", ["algorithm"]),
     "com.cpipe.demosaic.bilinear": ("bayer", "rgba", []),
     "com.cpipe.demosaic.quad_bayer_remosaic": ("qbc", "bayer", []),
     "com.cpipe.wb.dual_illuminant": ("rgb", "rgb", []),
