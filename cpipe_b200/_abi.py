@@ -230,7 +230,7 @@ EXPORTS = [
     "cpipe_b200_pack_opcode_list_3", "cpipe_b200_load_lut",
     "cpipe_b200_host_create", "cpipe_b200_host_destroy", "cpipe_b200_host_abi", "cpipe_b200_host_set_memory_cap",
     "cpipe_b200_buffer_create", "cpipe_b200_buffer_destroy", "cpipe_b200_buffer_upload",
-    "cpipe_b200_buffer_download", "cpipe_b200_buffer_device_ptr", "cpipe_b200_buffer_abi",
+    "cpipe_b200_buffer_download", "cpipe_b200_buffer_device_ptr", "cpipe_b200_buffer_abi", "cpipe_b200_buffer_format",
     "cpipe_b200_buffer_set_cfa", "cpipe_b200_buffer_set_levels", "cpipe_b200_buffer_set_matrix",
     "cpipe_b200_buffer_set_illuminants", "cpipe_b200_buffer_set_linearization_table",
     "cpipe_b200_buffer_set_noise_profile", "cpipe_b200_buffer_set_as_shot_neutral", "cpipe_b200_buffer_set_cs_role",
@@ -239,6 +239,9 @@ EXPORTS = [
     "cpipe_b200_params_create", "cpipe_b200_params_destroy", "cpipe_b200_params_set_double",
     "cpipe_b200_params_set_string", "cpipe_b200_params_set_bool", "cpipe_b200_run_node",
     "cpipe_b200_host_last_error",
+    "cpipe_b200_pipeline_load", "cpipe_b200_pipeline_destroy", "cpipe_b200_pipeline_last_error",
+    "cpipe_b200_pipeline_node_count", "cpipe_b200_pipeline_node_id", "cpipe_b200_pipeline_node_type",
+    "cpipe_b200_pipeline_memory_plan", "cpipe_b200_pipeline_run",
     "cpipe_cuda_chain_create", "cpipe_cuda_chain_destroy", "cpipe_cuda_chain_output_bytes", "cpipe_cuda_chain_run",
     "cpipe_cuda_chain_run_host", "cpipe_cuda_chain_run_host_frames", "cpipe_cuda_pinned_alloc", "cpipe_cuda_pinned_free",
     "cpipe_cuda_batch_create", "cpipe_cuda_batch_destroy", "cpipe_cuda_batch_run", "cpipe_cuda_batch_autotune",
@@ -265,8 +268,7 @@ def lib():
     vp, sz, i32, u32, cp = C.c_void_p, C.c_size_t, C.c_int, C.c_uint32, C.c_char_p
     sigs = {
         "cpipe_cuda_set_stream": (i32, [vp]), "cpipe_cuda_get_stream": (vp, []),
-        "cpipe_cuda_synchronize": (i32, []), "cpipe_cuda_trim_scratch": (i32, []),
-        "cpipe_cuda_memory_stats": (i32, [vp, vp, vp, vp]), "cpipe_cuda_last_error": (cp, []), "cpipe_cuda_device_count": (i32, []),
+        "cpipe_cuda_synchronize": (i32, []), "cpipe_cuda_trim_scratch": (i32, []), "cpipe_cuda_last_error": (cp, []), "cpipe_cuda_device_count": (i32, []),
         "cpipe_cuda_filters": (C.POINTER(FilterDesc), [C.POINTER(sz)]),
         "cpipe_cuda_find_filter": (C.POINTER(FilterDesc), [cp]),
         "cpipe_b200_node_descs": (C.POINTER(PluginDesc), [C.POINTER(sz)]),
@@ -292,6 +294,13 @@ def lib():
         "cpipe_b200_params_set_string": (i32, [vp, cp, cp]), "cpipe_b200_params_set_bool": (i32, [vp, cp, i32]),
         "cpipe_b200_run_node": (i32, [vp, cp, vp, C.POINTER(vp), sz, C.POINTER(vp), sz]),
         "cpipe_b200_host_last_error": (cp, [vp]),
+        "cpipe_b200_pipeline_load": (vp, [vp, cp, sz, cp, C.POINTER(i32)]),
+        "cpipe_b200_pipeline_destroy": (None, [vp]), "cpipe_b200_pipeline_last_error": (cp, [vp]),
+        "cpipe_b200_pipeline_node_count": (sz, [vp]), "cpipe_b200_pipeline_node_id": (cp, [vp, sz]),
+        "cpipe_b200_pipeline_node_type": (cp, [vp, sz]),
+        "cpipe_b200_pipeline_memory_plan": (i32, [vp, u32, u32, C.POINTER(C.c_uint64), C.POINTER(u32)]),
+        "cpipe_b200_pipeline_run": (i32, [vp, vp, C.POINTER(vp)]), "cpipe_b200_buffer_format": (i32, [vp]),
+        "cpipe_cuda_memory_stats": (i32, [vp, vp, vp, vp]),
         "cpipe_b200_wb_prepare": (i32, [vp, vp, vp, vp, vp, C.c_uint16, C.c_uint16, vp, C.POINTER(C.c_double)]),
         "cpipe_b200_colormatrix_compose": (i32, [vp, vp]),
         "cpipe_b200_pack_gain_maps": (i32, [vp, sz, vp, vp, vp, C.POINTER(sz)]),

@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "../../include/cpipe_b200.h"
+#include "host_internal.h"
 
 namespace {
 
@@ -96,6 +97,7 @@ struct cpipe_b200_buffer {
     uint32_t w = 0, h = 0;
     void* dev = nullptr;
     size_t bytes = 0;
+    bool owned = true;  // false: a view over device memory someone else owns (planner slots)
     std::shared_ptr<Metadata> meta = std::make_shared<Metadata>();
     std::vector<unsigned char> mirror;
     int lock_access = -1;
@@ -582,7 +584,7 @@ cpipe_b200_buffer* cpipe_b200_buffer_create(cpipe_b200_host* h, int format, uint
 }
 void cpipe_b200_buffer_destroy(cpipe_b200_buffer* b) {
     if (!b) return;
-    if (b->host) {
+    if (b->host && b->owned) {
         cudaStreamSynchronize(b->host->stream);
         cudaFree(b->dev);
         b->host->allocated -= b->bytes;
@@ -605,6 +607,7 @@ int cpipe_b200_buffer_download(cpipe_b200_buffer* b, void* data, size_t bytes) {
     return CPIPE_OK;
 }
 void* cpipe_b200_buffer_device_ptr(cpipe_b200_buffer* b) { return b ? b->dev : nullptr; }
+int cpipe_b200_buffer_format(const cpipe_b200_buffer* b) { return b ? b->format : 0; }
 const cpipe_buffer_t* cpipe_b200_buffer_abi(cpipe_b200_buffer* b) { return reinterpret_cast<const cpipe_buffer_t*>(b); }
 
 int cpipe_b200_buffer_set_cfa(cpipe_b200_buffer* b, const uint8_t repeat[2], const uint8_t pattern[16]) {
@@ -719,6 +722,47 @@ int cpipe_b200_run_node(cpipe_b200_host* h, const char* node_id, const cpipe_b20
         h->error = std::string("unknown node id ") + node_id;
         return CPIPE_BAD_INDEX;
     }
+    return cpb_run_node(h, desc, params, inputs, n_in, outputs, n_out, true);
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------- pipeline runner hooks
+cpipe_b200_buffer* cpb_buffer_view(cpipe_b200_host* h, int format, uint32_t w, uint32_t hgt, void* dev) {
+    if (!h || !dev || w == 0 || hgt == 0 || format_bytes(format) == 0) return nullptr;
+    auto* b = new (std::nothrow) cpipe_b200_buffer();
+    if (!b) return nullptr;
+    b->host = h;
+    b->format = format;
+    b->w = w;
+    b->h = hgt;
+    b->dev = dev;
+    b->bytes = (size_t)w * hgt * format_bytes(format);
+    b->owned = false;
+    return b;
+}
+size_t cpb_format_bytes(int format) { return (size_t)format_bytes(format); }
+int cpb_buffer_format(const cpipe_b200_buffer* b) { return b ? b->format : 0; }
+void cpb_buffer_extent(const cpipe_b200_buffer* b, uint32_t* w, uint32_t* h) {
+    *w = b ? b->w : 0;
+    *h = b ? b->h : 0;
+}
+void cpb_buffer_share_metadata(cpipe_b200_buffer* dst, const cpipe_b200_buffer* src) {
+    if (dst && src) dst->meta = src->meta;
+}
+cudaStream_t cpb_host_stream(cpipe_b200_host* h) { return h ? h->stream : nullptr; }
+uint64_t cpb_host_memory_cap(cpipe_b200_host* h) { return h ? h->cap : 0; }
+void cpb_host_set_error(cpipe_b200_host* h, const std::string& e) {
+    if (h) h->error = e;
+}
+const std::string& cpb_host_error(cpipe_b200_host* h) { return h->error; }
+
+// One node through its main_entry (create, process, destroy) on the host's
+// stream; with sync == false its kernels stay queued (the pipeline runner
+// synchronises once per run).
+int cpb_run_node(cpipe_b200_host* h, const cpipe_plugin_desc_t* desc, const cpipe_b200_params* params,
+                 cpipe_b200_buffer* const* inputs, size_t n_in, cpipe_b200_buffer* const* outputs, size_t n_out,
+                 bool sync) {
     cpipe_b200_params empty;
     cpipe_props_t* props = reinterpret_cast<cpipe_props_t*>(const_cast<cpipe_b200_params*>(params ? params : &empty));
     void* instance = nullptr;
@@ -743,7 +787,7 @@ int cpipe_b200_run_node(cpipe_b200_host* h, const char* node_id, const cpipe_b20
     h->error.clear();
     st = desc->main_entry(CPIPE_ACTION_PROCESS, &h->abi, reinterpret_cast<cpipe_node_t*>(instance), props, &ctx, nullptr);
     const int dst = desc->main_entry(CPIPE_ACTION_DESTROY, &h->abi, nullptr, props, instance, nullptr);
-    const cudaError_t e = cudaStreamSynchronize(h->stream);
+    const cudaError_t e = sync ? cudaStreamSynchronize(h->stream) : cudaGetLastError();
     if (st == CPIPE_OK && e != cudaSuccess) {
         h->error = cudaGetErrorString(e);
         st = CPIPE_INTERNAL_ERROR;
@@ -754,5 +798,3 @@ int cpipe_b200_run_node(cpipe_b200_host* h, const char* node_id, const cpipe_b20
     }
     return st != CPIPE_OK ? st : dst;
 }
-
-}  // extern "C"

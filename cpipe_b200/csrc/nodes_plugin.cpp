@@ -591,10 +591,9 @@ int node_usm(Ctx& c) {
 }
 
 // color/scene_linear_to_display.cpp:31-127: target -> output format and role,
-// buffer / metadata checks with the reference's codes, then the encode.  The
-// encode goes to this library's CUDA filter; a host that does not route
-// "cpipe_scene_linear_to_display" (CPIPE_UNSUPPORTED) gets the reference's own
-// path, its OCIO processor through the host suites.
+// buffer / metadata checks with the reference's codes, then the encode on this
+// library's CUDA filter "cpipe_scene_linear_to_display"; a host that does not
+// route it gets CPIPE_UNSUPPORTED (there is no CPU path).
 int node_display(Ctx& c) {
     std::string target;
     if (!c.get_string("target", &target)) return CPIPE_NEED_PARAM;
@@ -693,13 +692,13 @@ int n_bilinear(Ctx& c) { return node_demosaic(c, "demosaic_bilinear"); }
 #define PORT(name, kind, ch, prec, meta) \
     "{\"name\":\"" name "\",\"kind\":\"" kind "\",\"caps\":{\"buffer_kind\":\"Image2D\",\"channels\":[" ch "],\"precision\":[" prec "]},\"cardinality\":\"single\",\"metadata\":{" meta "}}"
 #define RGBA_IN(name, meta) PORT(name, "in", "\"rgba\"", "\"f16\",\"f32\"", meta)
-#define RGBA_OUT(name, step, extra) PORT(name, "out", "\"rgba\"", "\"f16\",\"f32\"", "\"inherits_from\":\"rgb\",\"sets_steps_applied\":[\"" step "\"]" extra)
+#define RGBA_OUT(name, step, extra) PORT(name, "out", "\"rgba\"", "\"f16\"", "\"inherits_from\":\"rgb\",\"sets_steps_applied\":[\"" step "\"]" extra)
 #define NUM(name, lo, hi, def) "{\"name\":\"" name "\",\"type\":\"number\",\"range\":{\"min\":" lo ",\"max\":" hi "},\"default\":" def "}"
 
 const char kPrecision[] = MANIFEST("com.cpipe.precision_convert", "Precision Convert", "utility",
     PORT("in", "in", "\"r\",\"rgba\"", "\"u16\",\"f32\",\"f16\"", ""),
     PORT("out", "out", "\"r\",\"rgba\"", "\"f32\",\"f16\",\"u8\",\"u16\"", "\"inherits_from\":\"in\",\"sets_steps_applied\":[\"precision_convert\"]"),
-    "{\"name\":\"target_format\",\"type\":\"enum\",\"values\":[\"R32_SFLOAT\",\"R16G16B16A16_SFLOAT\",\"R8G8B8A8_UNORM\",\"R16G16B16A16_UNORM\"]}",
+    "{\"name\":\"target_format\",\"type\":\"enum\",\"enum_values\":[\"R32_SFLOAT\",\"R16G16B16A16_SFLOAT\",\"R8G8B8A8_UNORM\",\"R16G16B16A16_UNORM\"]}",
     "any", "any", "true", "\"precision_convert\"");
 const char kLinearize[] = MANIFEST("com.cpipe.linearize.dng_lut", "DNG Linearization LUT", "raw",
     PORT("raw", "in", "\"r\"", "\"u16\"", "\"requires_fields\":[\"calibration.linearization_table\"]"),
@@ -715,9 +714,9 @@ const char kGainmap[] = MANIFEST("com.cpipe.lens.shading_gainmap", "Lens Shading
     "", "raw_camera", "raw_camera", "false", "\"raw_point<gainmap>\"");
 #define DEMOSAIC_MANIFEST(id, label, params, k) MANIFEST(id, label, "raw",                                           \
     PORT("bayer", "in", "\"r\"", "\"f32\"", "\"requires_steps_applied\":[\"black_white_scaling\"],\"requires_fields\":[\"calibration.cfa\"]"), \
-    PORT("rgba", "out", "\"rgba\"", "\"f16\",\"f32\"", "\"inherits_from\":\"bayer\",\"clears_fields\":[\"calibration.cfa\"],\"sets_steps_applied\":[\"demosaic\"]"), \
+    PORT("rgba", "out", "\"rgba\"", "\"f16\"", "\"inherits_from\":\"bayer\",\"clears_fields\":[\"calibration.cfa\"],\"sets_steps_applied\":[\"demosaic\"]"), \
     params, "raw_camera", "raw_camera", "false", k)
-#define DEMOSAIC_ALGORITHM "{\"name\":\"algorithm\",\"type\":\"enum\",\"values\":[\"reference\",\"full\"],\"default\":\"reference\"}"
+#define DEMOSAIC_ALGORITHM "{\"name\":\"algorithm\",\"type\":\"enum\",\"enum_values\":[\"reference\",\"full\"],\"default\":\"reference\"}"
 const char kRcd[] = DEMOSAIC_MANIFEST("com.cpipe.demosaic.rcd", "RCD Demosaic", DEMOSAIC_ALGORITHM,
                                       "\"demosaic_kernel<rcd>\",\"rcd_full_kernel\"");
 const char kAmaze[] = DEMOSAIC_MANIFEST("com.cpipe.demosaic.amaze", "AMaZE Demosaic", DEMOSAIC_ALGORITHM,
@@ -738,27 +737,27 @@ const char kBm3d[] = MANIFEST("com.cpipe.denoise.bm3d", "BM3D Denoise", "denoise
     RGBA_IN("rgb", "\"requires_steps_applied\":[\"color_matrix\"],\"requires_fields\":[\"calibration.noise_profile\"]"),
     RGBA_OUT("rgb", "denoise.bm3d", ""),
     "{\"name\":\"sigma\",\"type\":\"number\",\"range\":{\"min\":0,\"max\":0.2}},{\"name\":\"sigma_override\",\"type\":\"number\",\"range\":{\"min\":0},\"default\":0},"
-    "{\"name\":\"algorithm\",\"type\":\"enum\",\"values\":[\"box2x2\",\"bm3d\"],\"default\":\"box2x2\"},"
+    "{\"name\":\"algorithm\",\"type\":\"enum\",\"enum_values\":[\"box2x2\",\"bm3d\"],\"default\":\"box2x2\"},"
     NUM("stages", "1", "2", "2"),
     "scene_linear_rec2020", "scene_linear_rec2020", "true", "\"bm3d_parity_kernel\",\"bm3d_match_kernel\",\"bm3d_filter_kernel\"");
 const char kGuided[] = MANIFEST("com.cpipe.denoise.guided_filter", "Guided Filter Denoise", "denoise",
     RGBA_IN("rgb", "\"requires_steps_applied\":[\"color_matrix\"]"), RGBA_OUT("rgb", "denoise.guided_filter", ""),
     NUM("radius", "1", "32", "1") "," NUM("eps", "1e-05", "0.1", "0.015") ","
-    "{\"name\":\"algorithm\",\"type\":\"enum\",\"values\":[\"reference\",\"spec\"],\"default\":\"reference\"}",
+    "{\"name\":\"algorithm\",\"type\":\"enum\",\"enum_values\":[\"reference\",\"spec\"],\"default\":\"reference\"}",
     "scene_linear_rec2020", "scene_linear_rec2020", "true", "\"guided_kernel\",\"guided_spec_kernel\"");
 const char kWavelet[] = MANIFEST("com.cpipe.denoise.wavelet_bayes_shrink", "Wavelet BayesShrink Denoise", "denoise",
     RGBA_IN("rgb", "\"requires_steps_applied\":[\"color_matrix\"]"), RGBA_OUT("rgb", "denoise.wavelet_bayes_shrink", ""),
     NUM("chroma_strength", "0", "2", "1") ","
-    "{\"name\":\"algorithm\",\"type\":\"enum\",\"values\":[\"haar\",\"atrous\"],\"default\":\"haar\"},"
+    "{\"name\":\"algorithm\",\"type\":\"enum\",\"enum_values\":[\"haar\",\"atrous\"],\"default\":\"haar\"},"
     NUM("levels", "0", "6", "5") "," NUM("luma_strength", "0", "2", "1") ","
     "{\"name\":\"sigma\",\"type\":\"number\",\"range\":{\"min\":0,\"max\":0.2}}",
     "scene_linear_rec2020", "scene_linear_rec2020", "true", "\"wavelet_kernel\",\"atrous_level_kernel\"");
 const char kOpcode3[] = MANIFEST("com.cpipe.lens.dng_opcode_list_3", "DNG OpcodeList3", "lens",
     PORT("scene_rgb", "in", "\"rgba\"", "\"f16\",\"f32\"", "\"requires_blobs\":[\"com.cpipe.dng.opcode_list_3_bytes\"]"),
-    PORT("corrected_rgb", "out", "\"rgba\"", "\"f16\",\"f32\"", "\"inherits_from\":\"scene_rgb\",\"sets_steps_applied\":[\"opcode_list_3\"]"),
+    PORT("corrected_rgb", "out", "\"rgba\"", "\"f16\"", "\"inherits_from\":\"scene_rgb\",\"sets_steps_applied\":[\"opcode_list_3\"]"),
     "", "raw_camera", "raw_camera", "true", "\"warp_kernel\",\"vignette_kernel\",\"bad_constant_kernel\",\"bad_list_kernel\",\"trim_kernel\"");
 const char kLut[] = MANIFEST("com.cpipe.color.3d_lut", "3D LUT", "color", RGBA_IN("rgb", ""), RGBA_OUT("rgb", "color.3d_lut", ""),
-    "{\"name\":\"lut_path\",\"type\":\"string\"},{\"name\":\"interpolation\",\"type\":\"enum\",\"values\":[\"tetrahedral\",\"trilinear\"],\"default\":\"tetrahedral\"}",
+    "{\"name\":\"lut_path\",\"type\":\"string\"},{\"name\":\"interpolation\",\"type\":\"enum\",\"enum_values\":[\"tetrahedral\",\"trilinear\"],\"default\":\"tetrahedral\"}",
     "scene_linear_rec2020", "scene_linear_rec2020", "false", "\"rgba_point<lut3d>\"");
 const char kFilmic[] = MANIFEST("com.cpipe.tone.filmic_rgb", "Filmic RGB Tone", "tone",
     RGBA_IN("rgb", "\"requires_steps_applied\":[\"denoise.wavelet_bayes_shrink\"]"), RGBA_OUT("rgb", "tone.filmic_rgb", ""),
@@ -787,7 +786,7 @@ const char kReinhard[] = MANIFEST("com.cpipe.tone.reinhard", "Reinhard Tone", "t
     "scene_linear_rec2020", "scene_linear_rec2020", "true", "\"rgba_point<reinhard>\"");
 const char kUsm[] = MANIFEST("com.cpipe.sharpen.edge_aware_usm", "Edge-aware USM", "sharpen",
     PORT("rgb", "in", "\"rgba\"", "\"f16\",\"f32\"", "\"requires_steps_applied\":[\"color.3d_lut\"]"),
-    PORT("rgb", "out", "\"rgba\"", "\"f16\",\"f32\"", "\"inherits_from\":\"rgb\",\"sets_steps_applied\":[\"sharpen.edge_aware_usm\"]"),
+    PORT("rgb", "out", "\"rgba\"", "\"f16\"", "\"inherits_from\":\"rgb\",\"sets_steps_applied\":[\"sharpen.edge_aware_usm\"]"),
     NUM("strength", "0", "2", "0.75") "," NUM("radius", "1", "32", "1") "," NUM("threshold", "0", "0.1", "0"),
     "scene_linear_rec2020", "scene_linear_rec2020", "true", "\"usm_kernel\"");
 const char kDisplay[] = MANIFEST("com.cpipe.color.scene_linear_to_display", "Scene Linear to Display", "color",

@@ -27,10 +27,8 @@
 //          alpha copied.
 //
 // Kernels
-//   gsp_rows / ab / ab_rows / out   the guided filter as four separable
-//                        passes over frame-wide planes (row passes staged in
-//                        shared memory, column passes with running FP64 sums;
-//                        v^2 sums and the variance in FP64), see below.
+//   gsp_ab / gsp_out     the guided filter as two column-strip kernels with
+//                        running binary32 box sums (see below).
 //   atrous_prep_kernel   RGBA -> Y, Co, Cg planes (FP32).
 //   atrous_h_kernel      one level's horizontal B3 pass of all three planes
 //                        into a scratch plane set (taps 2^j apart, clamped).
@@ -39,7 +37,8 @@
 //                        per channel (no halo staging: the taps come through
 //                        L1 / L2).
 //   atrous_thresh_kernel per (level, channel): the tiles' sums added in a fixed
-//                        order (FP64), the BayesShrink threshold.
+//                        order (compensated binary32), the BayesShrink
+//                        threshold.
 //   atrous_recon_kernel  shrink, sum, inverse colour transform.
 #include "spec_denoise.h"
 
@@ -57,151 +56,147 @@ namespace cpb {
 namespace {
 
 // ------------------------------------------------------------------ guided
-// Four separable passes over frame-wide planes, per RGB channel (blockIdx.z):
-//   rows   S1, S2 = sums of v and v^2 (S2 in FP64) over the D = 2R+1 columns
-//          around xa in [-R, w+R), on rows yr in [-2R, h+2R) of the clamped
-//          image; the row segment is staged in shared memory;
-//   cols   running FP64 sums of S1, S2 down the D rows around ya in [-R, h+R):
-//          m = S1/N, corr = S2/N, var = max(corr - m^2, 0) in FP64 (so no
-//          shift is needed against cancellation), a = var / (var + eps),
-//          b = m - a m;
-//   rows   sums of a and b over the D columns around x in [0, w);
-//   cols   running sums down the D rows around y: mean_a, mean_b,
-//          out = max(mean_a v + mean_b, 0), alpha copied.
-// a and b live on the extended domain [-R, w+R) x [-R, h+R), as the filter's
-// definition evaluates them at positions outside the image.
-constexpr int kGsThreads = 256, kGsSeg = 32;  // column passes: rows per thread
+// Two kernels over column strips, per RGB channel, in binary32:
+//   ab    a thread per column xa of the extended domain [-R, w+R) walks a
+//         segment of kGsSeg rows ya: the horizontal sums of v and v^2 of the
+//         clamped image row entering the vertical box (staged in shared
+//         memory) are added to running column sums, a and b are written, and
+//         the sums of the row leaving the box are subtracted;
+//   out   a thread per output column walks kGsSeg rows the same way over the
+//         a and b planes of all three channels (horizontal sums of the entering
+//         and leaving rows), out = max(mean_a v + mean_b, 0), alpha copied.
+// Each segment starts its running sums afresh (2R rows of warm-up), so no sum
+// runs over more than kGsSeg + 2R rows.  Binary16 values square exactly in
+// binary32; against the FP64 definition the results are within one binary16
+// ulp (binary16 frames) or 1e-5 (binary32 frames).
+constexpr int kGsThreads = 128, kGsSeg = 64;
 struct GsPlanes {
-    int w, h, R, Wa, Ha, Hr;
-    float* s1;   // [3][Hr][Wa]
-    double* s2;  // [3][Hr][Wa]
-    float* a;    // [3][Ha][Wa]
+    int w, h, R, Wa, Ha;
+    float* a;  // [3][Ha][Wa]
     float* b;
-    float* sa;   // [3][Ha][w]
-    float* sb;
 };
 GsPlanes gs_planes(int w, int h, int R, void* scratch) {
-    GsPlanes p{w, h, R, w + 2 * R, h + 2 * R, h + 4 * R, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
-    char* c = static_cast<char*>(scratch);
-    const size_t nr = 3 * (size_t)p.Hr * p.Wa, na = 3 * (size_t)p.Ha * p.Wa, ns = 3 * (size_t)p.Ha * w;
-    p.s2 = reinterpret_cast<double*>(c);
-    c += nr * sizeof(double);
-    p.s1 = reinterpret_cast<float*>(c);
-    c += nr * sizeof(float);
-    p.a = reinterpret_cast<float*>(c);
-    c += na * sizeof(float);
-    p.b = reinterpret_cast<float*>(c);
-    c += na * sizeof(float);
-    p.sa = reinterpret_cast<float*>(c);
-    c += ns * sizeof(float);
-    p.sb = reinterpret_cast<float*>(c);
+    GsPlanes p{w, h, R, w + 2 * R, h + 2 * R, nullptr, nullptr};
+    p.a = static_cast<float*>(scratch);
+    p.b = p.a + 3 * (size_t)p.Ha * p.Wa;
     return p;
 }
-// pass 1: block = 256 consecutive xa of one row yi and channel c
+// block: extended columns [xs, xs + 128) of channel blockIdx.z, extended rows
+// ya in [blockIdx.y * kGsSeg - R, + kGsSeg)
 template <class T>
-__global__ void __launch_bounds__(kGsThreads) gsp_rows_kernel(Img in, GsPlanes p) {
-    __shared__ float s_row[kGsThreads + 2 * kGuidedSpecMaxRadius];
-    const int xb = blockIdx.x * kGsThreads, yi = blockIdx.y, c = blockIdx.z, R = p.R;
-    const int y = clampi(yi - 2 * R, 0, in.h - 1);
-    for (int i = threadIdx.x; i < kGsThreads + 2 * R; i += kGsThreads) {
-        const int x = clampi(xb + i - 2 * R, 0, in.w - 1);  // xa = xb + i - R, its box from xa - R
-        s_row[i] = (float)px<const T>(in, x, y)[c];
+__global__ void __launch_bounds__(kGsThreads) gsp_ab_kernel(Img in, GsPlanes p, float eps) {
+    __shared__ float s_new[kGsThreads + 2 * kGuidedSpecMaxRadius], s_old[kGsThreads + 2 * kGuidedSpecMaxRadius];
+    const int c = blockIdx.z, xs = blockIdx.x * kGsThreads, t = threadIdx.x, R = p.R, D = 2 * R + 1;
+    const int ya0 = (int)blockIdx.y * kGsSeg - R, ya1 = min(ya0 + kGsSeg, p.h + R);
+    const float N = (float)(D * D);
+    // extended column xi = xs + t is image column xi - R; its box reads image
+    // columns xi - 2R .. xi, staged at s[t .. t + 2R]
+    auto stage = [&](float* buf, int row) {
+        const int y = clampi(row, 0, in.h - 1);
+        for (int i = t; i < kGsThreads + 2 * R; i += kGsThreads)
+            buf[i] = (float)px<const T>(in, clampi(xs - 2 * R + i, 0, in.w - 1), y)[c];
+    };
+    auto hsum = [&](const float* buf, float& h1, float& h2) {
+        h1 = 0.0F;
+        h2 = 0.0F;
+        for (int k = 0; k < D; ++k) {
+            const float v = buf[t + k];
+            h1 = h1 + v;
+            h2 = h2 + v * v;
+        }
+    };
+    float s1 = 0.0F, s2 = 0.0F, h1, h2;
+    for (int r = ya0 - R; r < ya0 + R; ++r) {
+        stage(s_new, r);
+        __syncthreads();
+        hsum(s_new, h1, h2);
+        s1 = s1 + h1;
+        s2 = s2 + h2;
+        __syncthreads();
     }
-    __syncthreads();
-    const int xi = xb + threadIdx.x;
-    if (xi >= p.Wa) return;
-    float s = 0.0F;
-    double q = 0.0;
-    for (int dx = 0; dx <= 2 * R; ++dx) {
-        const float v = s_row[threadIdx.x + dx];
-        s += v;
-        // a binary16 value squares exactly in binary32 (11-bit significand)
-        q += std::is_same<T, __half>::value ? (double)(v * v) : (double)v * (double)v;
+    const int xi = xs + t;
+    for (int ya = ya0; ya < ya1; ++ya) {
+        stage(s_new, ya + R);
+        stage(s_old, ya - R);
+        __syncthreads();
+        hsum(s_new, h1, h2);
+        s1 = s1 + h1;
+        s2 = s2 + h2;
+        const float m = s1 / N, corr = s2 / N;
+        const float var = maxf(corr - m * m, 0.0F);
+        const float a = var / (var + eps);
+        if (xi < p.Wa) {
+            const size_t o = ((size_t)c * p.Ha + (ya + R)) * p.Wa + xi;
+            p.a[o] = a;
+            p.b[o] = m - a * m;
+        }
+        hsum(s_old, h1, h2);
+        s1 = s1 - h1;
+        s2 = s2 - h2;
+        __syncthreads();
     }
-    const size_t o = ((size_t)c * p.Hr + yi) * p.Wa + xi;
-    p.s1[o] = s;
-    p.s2[o] = q;
 }
-// pass 2: a thread walks kGsSeg rows of one column with running sums
-__global__ void __launch_bounds__(kGsThreads) gsp_ab_kernel(GsPlanes p, float eps) {
-    const int xi = blockIdx.x * blockDim.x + threadIdx.x, y0 = blockIdx.y * kGsSeg, c = blockIdx.z;
-    if (xi >= p.Wa || y0 >= p.Ha) return;
-    const int D = 2 * p.R + 1, y1 = min(p.Ha, y0 + kGsSeg);
-    const double invN = 1.0 / ((double)D * D);
-    const float* s1 = p.s1 + (size_t)c * p.Hr * p.Wa + xi;
-    const double* s2 = p.s2 + (size_t)c * p.Hr * p.Wa + xi;
-    double sm = 0.0, sq = 0.0;
-    for (int r = y0; r < y0 + D - 1; ++r) {  // S rows ya_i .. ya_i + 2R belong to output row ya_i
-        sm += (double)s1[(size_t)r * p.Wa];
-        sq += s2[(size_t)r * p.Wa];
-    }
-    for (int yi = y0; yi < y1; ++yi) {
-        const size_t add = (size_t)(yi + D - 1) * p.Wa;
-        sm += (double)s1[add];
-        sq += s2[add];
-        const double m = sm * invN, var = fmax(sq * invN - m * m, 0.0);
-        const float vf = (float)var, mf = (float)m;
-        const float a = vf / (vf + eps);  // in [0, 1]: binary32 is ample
-        const size_t o = ((size_t)c * p.Ha + yi) * p.Wa + xi;
-        p.a[o] = a;
-        p.b[o] = mf - a * mf;
-        const size_t sub = (size_t)yi * p.Wa;
-        sm -= (double)s1[sub];
-        sq -= s2[sub];
-    }
-}
-// pass 3: block = 256 consecutive x of one extended row yi and channel c
-__global__ void __launch_bounds__(kGsThreads) gsp_ab_rows_kernel(GsPlanes p) {
-    __shared__ float s_a[kGsThreads + 2 * kGuidedSpecMaxRadius], s_b[kGsThreads + 2 * kGuidedSpecMaxRadius];
-    const int xb = blockIdx.x * kGsThreads, yi = blockIdx.y, c = blockIdx.z, R = p.R;
-    const size_t row = ((size_t)c * p.Ha + yi) * p.Wa;
-    for (int i = threadIdx.x; i < kGsThreads + 2 * R; i += kGsThreads) {
-        const int xa = min(xb + i, p.Wa - 1);  // xa index x + dx (x - R + dx in image coordinates)
-        s_a[i] = p.a[row + xa];
-        s_b[i] = p.b[row + xa];
-    }
-    __syncthreads();
-    const int x = xb + threadIdx.x;
-    if (x >= p.w) return;
-    float sa = 0.0F, sb = 0.0F;
-    for (int dx = 0; dx <= 2 * R; ++dx) {
-        sa += s_a[threadIdx.x + dx];
-        sb += s_b[threadIdx.x + dx];
-    }
-    const size_t o = ((size_t)c * p.Ha + yi) * p.w + x;
-    p.sa[o] = sa;
-    p.sb[o] = sb;
-}
-// pass 4: a thread walks kGsSeg output rows of one column, all three channels
+// block: output columns [xs, xs + 128), rows [blockIdx.y * kGsSeg, + kGsSeg)
 template <class T>
 __global__ void __launch_bounds__(kGsThreads) gsp_out_kernel(Img in, Img out, GsPlanes p) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y0 = blockIdx.y * kGsSeg;
-    if (x >= p.w || y0 >= p.h) return;
-    const int D = 2 * p.R + 1, y1 = min(p.h, y0 + kGsSeg);
+    constexpr int kS = kGsThreads + 2 * kGuidedSpecMaxRadius;
+    __shared__ float s_new[6][kS], s_old[6][kS];
+    const int xs = blockIdx.x * kGsThreads, t = threadIdx.x, R = p.R, D = 2 * R + 1;
+    const int y0 = (int)blockIdx.y * kGsSeg, y1 = min(y0 + kGsSeg, p.h);
     const float N = (float)(D * D);
-    double sa[3] = {0.0, 0.0, 0.0}, sb[3] = {0.0, 0.0, 0.0};
-    const size_t plane = (size_t)p.Ha * p.w;
-    for (int r = y0; r < y0 + D - 1; ++r)
-        for (int c = 0; c < 3; ++c) {
-            sa[c] += (double)p.sa[c * plane + (size_t)r * p.w + x];
-            sb[c] += (double)p.sb[c * plane + (size_t)r * p.w + x];
+    const size_t plane = (size_t)p.Ha * p.Wa;
+    // output column x reads extended columns x .. x + 2R (image x - R .. x + R)
+    auto stage = [&](float (*buf)[kS], int ya) {
+        const size_t row = (size_t)(ya + R) * p.Wa;
+        for (int i = t; i < kGsThreads + 2 * R; i += kGsThreads) {
+            const size_t xi = row + (size_t)min(xs + i, p.Wa - 1);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                buf[2 * c][i] = p.a[c * plane + xi];
+                buf[2 * c + 1][i] = p.b[c * plane + xi];
+            }
         }
+    };
+    float sa[3] = {0.0F, 0.0F, 0.0F}, sb[3] = {0.0F, 0.0F, 0.0F};
+    auto add = [&](float (*buf)[kS], float sign) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            float ha = 0.0F, hb = 0.0F;
+            for (int k = 0; k < D; ++k) {
+                ha = ha + buf[2 * c][t + k];
+                hb = hb + buf[2 * c + 1][t + k];
+            }
+            if (sign > 0.0F) {
+                sa[c] = sa[c] + ha;
+                sb[c] = sb[c] + hb;
+            } else {
+                sa[c] = sa[c] - ha;
+                sb[c] = sb[c] - hb;
+            }
+        }
+    };
+    for (int ya = y0 - R; ya < y0 + R; ++ya) {
+        stage(s_new, ya);
+        __syncthreads();
+        add(s_new, 1.0F);
+        __syncthreads();
+    }
+    const int x = xs + t;
     for (int y = y0; y < y1; ++y) {
-        const size_t add = (size_t)(y + D - 1) * p.w + x, sub = (size_t)y * p.w + x;
-        for (int c = 0; c < 3; ++c) {
-            sa[c] += (double)p.sa[c * plane + add];
-            sb[c] += (double)p.sb[c * plane + add];
+        stage(s_new, y + R);
+        stage(s_old, y - R);
+        __syncthreads();
+        add(s_new, 1.0F);
+        if (x < p.w) {
+            const T* src = px<const T>(in, x, y);
+            const Rgba v = load_rgba(src);
+            store_rgb_keep_alpha(px<T>(out, x, y),
+                                 Rgba{max0((sa[0] / N) * v.r + sb[0] / N), max0((sa[1] / N) * v.g + sb[1] / N),
+                                      max0((sa[2] / N) * v.b + sb[2] / N), 0.0F},
+                                 src);
         }
-        const Rgba v = load_rgba(px<const T>(in, x, y));
-        const float ma[3] = {(float)sa[0] / N, (float)sa[1] / N, (float)sa[2] / N};
-        const float mb[3] = {(float)sb[0] / N, (float)sb[1] / N, (float)sb[2] / N};
-        store_rgb_keep_alpha(px<T>(out, x, y),
-                             Rgba{max0(ma[0] * v.r + mb[0]), max0(ma[1] * v.g + mb[1]), max0(ma[2] * v.b + mb[2]), 0.0F},
-                             px<const T>(in, x, y));
-        for (int c = 0; c < 3; ++c) {
-            sa[c] -= (double)p.sa[c * plane + sub];
-            sb[c] -= (double)p.sb[c * plane + sub];
-        }
+        add(s_old, -1.0F);
+        __syncthreads();
     }
 }
 
@@ -288,23 +283,42 @@ struct AtrousTiles {
     int nb[kAtrousMaxLevels];
     int stride;
 };
+// Compensated binary32 addition (Knuth's TwoSum): hi + lo carries the sum
+// to about 48 significant bits, so the fixed-order reduction below needs no
+// FP64.
+struct Ff2 {
+    float hi, lo;
+};
+__device__ __forceinline__ Ff2 ff_add(Ff2 a, float b) {
+    const float s = __fadd_rn(a.hi, b);
+    const float bp = __fsub_rn(s, a.hi);
+    const float e = __fadd_rn(__fsub_rn(a.hi, __fsub_rn(s, bp)), __fsub_rn(b, bp));
+    return Ff2{s, __fadd_rn(a.lo, e)};
+}
+__device__ __forceinline__ Ff2 ff_add(Ff2 a, Ff2 b) {
+    Ff2 r = ff_add(a, b.hi);
+    r.lo = __fadd_rn(r.lo, b.lo);
+    return r;
+}
 __global__ void __launch_bounds__(256) atrous_thresh_kernel(const float* __restrict__ part, AtrousTiles tl, long long npx,
                                                             AtrousThrArgs a, float* __restrict__ thr) {
     const int j = blockIdx.x / 3, c = blockIdx.x % 3, nblocks = tl.nb[j];
-    __shared__ double red[256];
-    double s = 0.0;
-    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) s += (double)part[(size_t)j * tl.stride + (size_t)b * 3 + c];
+    __shared__ Ff2 red[256];
+    Ff2 s{0.0F, 0.0F};
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) s = ff_add(s, part[(size_t)j * tl.stride + (size_t)b * 3 + c]);
     red[threadIdx.x] = s;
     __syncthreads();
     for (int k = 128; k > 0; k >>= 1) {
-        if ((int)threadIdx.x < k) red[threadIdx.x] += red[threadIdx.x + k];
+        if ((int)threadIdx.x < k) red[threadIdx.x] = ff_add(red[threadIdx.x], red[threadIdx.x + k]);
         __syncthreads();
     }
     if (threadIdx.x == 0) {
-        const double sw2 = red[0] / (double)npx, sn = (double)a.noise[j][c];
-        const double sx = sqrt(fmax(sw2 - sn * sn, 0.0));
+        // mean of w^2: (hi + lo) / npx, npx exact in binary32 up to 2^24 and
+        // rounded once above it
+        const float sw2 = __fdiv_rn(__fadd_rn(red[0].hi, red[0].lo), (float)npx), sn = a.noise[j][c];
+        const float sx = sqrtf(fmaxf(__fsub_rn(sw2, __fmul_rn(sn, sn)), 0.0F));
         const float st = a.strength[c];
-        thr[j * 3 + c] = st == 0.0F ? 0.0F : (sx > 0.0 ? (float)((double)st * sn * sn / sx) : INFINITY);
+        thr[j * 3 + c] = st == 0.0F ? 0.0F : (sx > 0.0F ? __fdiv_rn(__fmul_rn(__fmul_rn(st, sn), sn), sx) : INFINITY);
     }
 }
 
@@ -338,20 +352,18 @@ size_t align256(size_t v) { return (v + 255U) & ~(size_t)255U; }
 cudaError_t guided_spec_setup() { return cudaSuccess; }  // the pass kernels use no dynamic shared memory
 
 size_t guided_spec_scratch_bytes(int w, int h, int radius) {
-    const size_t Wa = (size_t)w + 2 * radius, Ha = (size_t)h + 2 * radius, Hr = (size_t)h + 4 * radius;
-    return 3 * (Hr * Wa * (sizeof(double) + sizeof(float)) + 2 * Ha * Wa * sizeof(float) + 2 * Ha * (size_t)w * sizeof(float));
+    const size_t Wa = (size_t)w + 2 * radius, Ha = (size_t)h + 2 * radius;
+    return 2 * 3 * Ha * Wa * sizeof(float);
 }
 
 cudaError_t guided_spec_run(const Img& in, const Img& out, bool f16, int radius, float eps, void* scratch,
                             cudaStream_t st) {
     if (radius < 1 || radius > kGuidedSpecMaxRadius) return cudaErrorInvalidValue;
     const GsPlanes p = gs_planes(in.w, in.h, radius, scratch);
-    const unsigned ga = (unsigned)((p.Wa + kGsThreads - 1) / kGsThreads), gw = (unsigned)((in.w + kGsThreads - 1) / kGsThreads);
-    if (f16) gsp_rows_kernel<__half><<<dim3(ga, (unsigned)p.Hr, 3), kGsThreads, 0, st>>>(in, p);
-    else gsp_rows_kernel<float><<<dim3(ga, (unsigned)p.Hr, 3), kGsThreads, 0, st>>>(in, p);
-    gsp_ab_kernel<<<dim3(ga, (unsigned)((p.Ha + kGsSeg - 1) / kGsSeg), 3), kGsThreads, 0, st>>>(p, eps);
-    gsp_ab_rows_kernel<<<dim3(gw, (unsigned)p.Ha, 3), kGsThreads, 0, st>>>(p);
-    const dim3 go(gw, (unsigned)((in.h + kGsSeg - 1) / kGsSeg));
+    const dim3 ga((unsigned)((p.Wa + kGsThreads - 1) / kGsThreads), (unsigned)((p.Ha + kGsSeg - 1) / kGsSeg), 3);
+    if (f16) gsp_ab_kernel<__half><<<ga, kGsThreads, 0, st>>>(in, p, eps);
+    else gsp_ab_kernel<float><<<ga, kGsThreads, 0, st>>>(in, p, eps);
+    const dim3 go((unsigned)((in.w + kGsThreads - 1) / kGsThreads), (unsigned)((in.h + kGsSeg - 1) / kGsSeg));
     if (f16) gsp_out_kernel<__half><<<go, kGsThreads, 0, st>>>(in, out, p);
     else gsp_out_kernel<float><<<go, kGsThreads, 0, st>>>(in, out, p);
     return cudaGetLastError();

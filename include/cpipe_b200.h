@@ -209,6 +209,8 @@ void cpipe_b200_buffer_destroy(cpipe_b200_buffer* buffer);
 int cpipe_b200_buffer_upload(cpipe_b200_buffer* buffer, const void* host_data, size_t bytes);
 int cpipe_b200_buffer_download(cpipe_b200_buffer* buffer, void* host_data, size_t bytes);
 void* cpipe_b200_buffer_device_ptr(cpipe_b200_buffer* buffer);
+/* The buffer's CPIPE_FMT_* value (0 for NULL). */
+int cpipe_b200_buffer_format(const cpipe_b200_buffer* buffer);
 const cpipe_buffer_t* cpipe_b200_buffer_abi(cpipe_b200_buffer* buffer);
 
 /* Buffer metadata (what the reference BufferMetadata carries for this path). */
@@ -240,6 +242,39 @@ int cpipe_b200_run_node(cpipe_b200_host* host, const char* node_id, const cpipe_
                         cpipe_b200_buffer* const* inputs, size_t n_in, cpipe_b200_buffer* const* outputs,
                         size_t n_out);
 const char* cpipe_b200_host_last_error(cpipe_b200_host* host);
+
+/* ---------------------------------------------------------- pipeline runner */
+/* A pipeline document (*.cpipe.json, schema v0.4) planned once and run on
+ * device buffers: replaces Pipeline::load + Pipeline::run_bound
+ * (src/cpipe/runtime/Pipeline.cpp:368-601, 629-792) with the same load-time
+ * checks and status codes (version / schema: CPIPE_FAILED; reserved or
+ * unknown node type, bad param, dangling edge: CPIPE_BAD_INDEX; cycle:
+ * CPIPE_FAILED; missing step or colour-role mismatch: CPIPE_NEED_METADATA;
+ * implicit precision_convert insertion as PrecisionPlanner::auto_insert, else
+ * CPIPE_BAD_PRECISION), the memory plan of MemoryPlanner::plan_graph
+ * (MemoryPlanner.cpp:188-219) kept as device slots between runs, and one
+ * host synchronisation per run.  until: NULL, or a node id whose ancestors and
+ * itself are the nodes planned (a document's device prefix).  host may be NULL
+ * for planning only (load checks, node order, memory plan; run refuses).  After
+ * a failed load, cpipe_b200_pipeline_last_error(NULL) gives this thread's
+ * message. */
+typedef struct cpipe_b200_pipeline cpipe_b200_pipeline;
+cpipe_b200_pipeline* cpipe_b200_pipeline_load(cpipe_b200_host* host, const char* json, size_t json_bytes,
+                                              const char* until, int* status);
+void cpipe_b200_pipeline_destroy(cpipe_b200_pipeline* p);
+const char* cpipe_b200_pipeline_last_error(const cpipe_b200_pipeline* p);
+/* Planned nodes in execution order, implicit precision converts included. */
+size_t cpipe_b200_pipeline_node_count(const cpipe_b200_pipeline* p);
+const char* cpipe_b200_pipeline_node_id(const cpipe_b200_pipeline* p, size_t i);
+const char* cpipe_b200_pipeline_node_type(const cpipe_b200_pipeline* p, size_t i);
+/* Memory plan for a w x h input: peak bytes (input + slots) and slot count. */
+int cpipe_b200_pipeline_memory_plan(cpipe_b200_pipeline* p, uint32_t w, uint32_t h, uint64_t* peak_bytes,
+                                    uint32_t* slots);
+/* Runs the plan on `input` (a buffer of this host in the input port's format).
+ * *output: the last node's buffer, owned by the pipeline and valid until the
+ * next run or destroy (its device memory is a planner slot).  A peak above the
+ * host's memory cap is CPIPE_OOM (reference Pipeline.cpp:587-592). */
+int cpipe_b200_pipeline_run(cpipe_b200_pipeline* p, cpipe_b200_buffer* input, cpipe_b200_buffer** output);
 
 /* ---------------------------------------------------------------- fused chain */
 /* The raw->linear node sequence of the reference's classic pipeline
