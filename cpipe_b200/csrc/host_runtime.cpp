@@ -24,6 +24,7 @@
 #include <vector>
 
 #include "../../include/cpipe_b200.h"
+#include "../../include/cpipe_b200_dng.h"
 #include "host_internal.h"
 
 namespace {
@@ -751,6 +752,46 @@ void cpb_buffer_share_metadata(cpipe_b200_buffer* dst, const cpipe_b200_buffer* 
     if (dst && src) dst->meta = src->meta;
 }
 cudaStream_t cpb_host_stream(cpipe_b200_host* h) { return h ? h->stream : nullptr; }
+bool cpb_is_own_host(const cpipe_host_t* h) { return h && h->get_suite == &h_get_suite; }
+cudaStream_t cpb_abi_host_stream(cpipe_host_t* h) { return cpb_is_own_host(h) ? H(h)->stream : nullptr; }
+void* cpb_buffer_device(const cpipe_buffer_t* b) { return b ? B(b)->dev : nullptr; }
+// The DNG's calibration, capture and blobs as DngReader attaches them
+// (DngReader.cpp:214-230), written into one of this host's builders.
+int cpb_builder_set_dng(cpipe_metadata_builder_t* builder, const cpipe_DngInfo* info, const uint8_t* file,
+                        size_t file_bytes) {
+    if (!builder || !info || !file) return CPIPE_BAD_INDEX;
+    Metadata& m = BL(builder)->m;
+    m = Metadata{};
+    m.has_cfa = true;
+    m.cfa_repeat[0] = (uint8_t)info->cfa_repeat[0];
+    m.cfa_repeat[1] = (uint8_t)info->cfa_repeat[1];
+    std::memcpy(m.cfa_pattern, info->cfa_pattern, 16);
+    std::memcpy(m.black, info->black_level, sizeof(m.black));
+    m.white = info->white_level;
+    for (int k = 0; k < 4; ++k) {
+        if (!info->has_matrix[k]) continue;
+        std::array<float, 9> a;
+        std::memcpy(a.data(), info->matrix[k], sizeof(float) * 9);
+        m.m[k] = a;
+    }
+    m.illum1 = (uint16_t)info->calibration_illuminant[0];
+    m.illum2 = (uint16_t)info->calibration_illuminant[1];
+    std::memcpy(m.as_shot_neutral, info->as_shot_neutral, sizeof(m.as_shot_neutral));
+    m.cs_role = "raw_camera";
+    auto range = [&](uint32_t off, uint32_t n) -> const uint8_t* {
+        return (n && (uint64_t)off + n <= file_bytes) ? file + off : nullptr;
+    };
+    if (const uint8_t* p = range(info->linearization_offset, 2 * info->linearization_count)) {
+        m.lin_table.resize(info->linearization_count);
+        for (uint32_t i = 0; i < info->linearization_count; ++i) m.lin_table[i] = (uint16_t)(p[2 * i] | (p[2 * i + 1] << 8));
+    }
+    static const char* kOpcodeKeys[3] = {"com.cpipe.dng.opcode_list_1_bytes", "com.cpipe.dng.opcode_list_2_bytes",
+                                         "com.cpipe.dng.opcode_list_3_bytes"};
+    for (int k = 0; k < 3; ++k)
+        if (const uint8_t* p = range(info->opcode_list_offset[k], info->opcode_list_bytes[k]))
+            m.blobs[kOpcodeKeys[k]] = std::vector<unsigned char>(p, p + info->opcode_list_bytes[k]);
+    return CPIPE_OK;
+}
 uint64_t cpb_host_memory_cap(cpipe_b200_host* h) { return h ? h->cap : 0; }
 void cpb_host_set_error(cpipe_b200_host* h, const std::string& e) {
     if (h) h->error = e;

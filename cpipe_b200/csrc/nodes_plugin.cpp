@@ -12,12 +12,15 @@
 // "process" -> run, "destroy" -> free.  No C++ exception crosses main_entry.
 #include <algorithm>
 #include <cmath>
+#include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
 
 #include "../../include/cpipe_b200.h"
+#include "../../include/cpipe_b200_dng.h"
+#include "host_internal.h"
 #include "host_prep.h"
 
 namespace {
@@ -126,7 +129,7 @@ struct Ctx {
 
 // nin inputs and one output, all present, with an output metadata builder.
 bool n_to_one(const cpipe_process_ctx* pc, size_t nin) {
-    if (!pc || pc->n_in != nin || pc->n_out != 1 || !pc->inputs || !pc->outputs || !pc->outputs[0] ||
+    if (!pc || pc->n_in != nin || pc->n_out != 1 || (nin > 0 && !pc->inputs) || !pc->outputs || !pc->outputs[0] ||
         !pc->out_metadata || !pc->out_metadata[0])
         return false;
     for (size_t i = 0; i < nin; ++i)
@@ -676,6 +679,59 @@ int main_entry(const char* action, cpipe_host_t* host, cpipe_node_t* node, cpipe
         return CPIPE_INTERNAL_ERROR;
     }
 }
+// nodes/dng_input/dng_input.cpp:17-40: the file at param "path" through
+// DngReader::read.  The reference builtin replaces its output's buffer object
+// with the reader's; here the host allocates the output (an R16_UINT Image2D
+// of the file's extent, else CPIPE_BAD_INDEX), the strip is decoded on the GPU
+// straight into it, and the reader's metadata is attached through this
+// library's host runtime (another host: CPIPE_UNSUPPORTED).
+int node_dng_input(Ctx& c) {
+    std::string path;
+    if (!c.get_string("path", &path)) {
+        c.msg = "dng_input needs a path";
+        return CPIPE_NEED_PARAM;
+    }
+    if (!cpb_is_own_host(c.host)) {
+        c.msg = "dng_input writes device buffers of the cpipe_b200 host runtime";
+        return CPIPE_UNSUPPORTED;
+    }
+    std::vector<uint8_t> file;
+    {
+        FILE* f = std::fopen(path.c_str(), "rb");
+        if (!f) {
+            c.msg = "failed to open DNG";
+            return CPIPE_FAILED;
+        }
+        uint8_t chunk[1 << 16];
+        size_t n;
+        while ((n = std::fread(chunk, 1, sizeof(chunk), f)) > 0) file.insert(file.end(), chunk, chunk + n);
+        std::fclose(f);
+    }
+    cpipe_DngInfo info{};
+    int st = cpipe_dng_parse(file.data(), file.size(), &info);
+    if (st != CPIPE_OK) {
+        c.msg = cpipe_cuda_last_error();
+        return st == CPIPE_UNSUPPORTED ? CPIPE_FAILED : st;  // DngReader.cpp:192-195
+    }
+    int fmt = 0;
+    uint32_t w = 0, h = 0;
+    if ((st = c.format(c.out(0), &fmt)) != CPIPE_OK || (st = c.dims(c.out(0), &w, &h)) != CPIPE_OK) return st;
+    if (fmt != CPIPE_FMT_R16_UINT || w != info.width || h != info.height) {
+        c.msg = "dng_input output must be an R16_UINT image of the file's extent";
+        return CPIPE_BAD_INDEX;
+    }
+    void* prev = cpipe_cuda_get_stream();
+    cpipe_cuda_set_stream(cpb_abi_host_stream(c.host));
+    st = cpipe_cuda_dng_decode(file.data(), file.size(), static_cast<uint16_t*>(cpb_buffer_device(c.out(0))),
+                               (size_t)w * h * 2, &info);
+    cpipe_cuda_set_stream(prev);
+    if (st != CPIPE_OK) {
+        c.msg = cpipe_cuda_last_error();
+        return st;
+    }
+    return cpb_builder_set_dng(c.builder(), &info, file.data(), file.size());
+}
+
 int n_rcd(Ctx& c) { return node_demosaic(c, "demosaic_rcd"); }
 int n_amaze(Ctx& c) { return node_demosaic(c, "demosaic_amaze"); }
 int n_bilinear(Ctx& c) { return node_demosaic(c, "demosaic_bilinear"); }
@@ -721,6 +777,12 @@ const char kRcd[] = DEMOSAIC_MANIFEST("com.cpipe.demosaic.rcd", "RCD Demosaic", 
                                       "\"demosaic_kernel<rcd>\",\"rcd_full_kernel\"");
 const char kAmaze[] = DEMOSAIC_MANIFEST("com.cpipe.demosaic.amaze", "AMaZE Demosaic", DEMOSAIC_ALGORITHM,
                                         "\"demosaic_kernel<amaze>\",\"amaze_cd_kernel\",\"amaze_green_kernel\",\"amaze_out_kernel\"");
+const char kDngInput[] = "{\"$schema\":\"https://schemas.cpipe.dev/node/v0.2.json\",\"id\":\"com.cpipe.builtin.dng_input\","
+    "\"version\":\"1.0.0\",\"label\":\"DNG Input\",\"category\":\"builtin\",\"ports\":["
+    PORT("raw", "out", "\"r\"", "\"u16\"", "\"writes_fields\":[\"calibration\",\"capture\",\"cs_role\",\"ext_blobs\"]")
+    "],\"params\":[{\"name\":\"path\",\"type\":\"string\",\"required\":true}],"
+    "\"compute\":{\"device\":\"CUDA\",\"engine\":\"CUDA\",\"arch\":\"sm_100a\",\"kernels\":[\"dng_words_kernel\",\"dng_packed_kernel\"]},"
+    "\"color\":{\"input_role\":\"none\",\"output_role\":\"raw_camera\",\"respects_chromaticity\":false}}";
 const char kBilinear[] = DEMOSAIC_MANIFEST("com.cpipe.demosaic.bilinear", "Bilinear Demosaic", "", "\"demosaic_kernel<bilinear>\"");
 const char kQbc[] = MANIFEST("com.cpipe.demosaic.quad_bayer_remosaic", "Quad Bayer Remosaic", "raw",
     PORT("qbc", "in", "\"r\"", "\"u16\"", "\"requires_fields\":[\"calibration.cfa\"]"),
@@ -823,6 +885,7 @@ CPIPE_B200_REGISTER(cpipe_b200_desc_greyworld, "com.cpipe.wb.greyworld_auto", kG
     __attribute__((used, section("cpipe_registry"), aligned(8))) const cpipe_plugin_desc_t sym = \
         {CPIPE_ABI_MAJOR, CPIPE_ABI_MINOR, id, "1.0.0", manifest, &main_entry<fn, nin>};
 CPIPE_B200_REGISTER_N(cpipe_b200_desc_mertens, "com.cpipe.tone.mertens_local", kMertens, node_mertens, 3)
+CPIPE_B200_REGISTER_N(cpipe_b200_desc_dng_input, "com.cpipe.builtin.dng_input", kDngInput, node_dng_input, 0)
 CPIPE_B200_REGISTER(cpipe_b200_desc_aces, "com.cpipe.tone.aces_filmic", kAces, node_aces)
 CPIPE_B200_REGISTER(cpipe_b200_desc_reinhard, "com.cpipe.tone.reinhard", kReinhard, node_reinhard)
 CPIPE_B200_REGISTER(cpipe_b200_desc_usm, "com.cpipe.sharpen.edge_aware_usm", kUsm, node_usm)

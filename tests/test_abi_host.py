@@ -76,6 +76,7 @@ EXPECTED_NODES = {
     "com.cpipe.tone.reinhard": ("rgb", "rgb", ["white_point"]),
     "com.cpipe.sharpen.edge_aware_usm": ("rgb", "rgb", ["strength", "radius", "threshold"]),
     "com.cpipe.color.scene_linear_to_display": ("rgb", "display", ["target"]),
+    "com.cpipe.builtin.dng_input": ((), "raw", ["path"]),
 }
 
 
@@ -91,6 +92,11 @@ def test_registry_and_manifests():
         ins = [p["name"] for p in m["ports"] if p["kind"] == "in"]
         outs = [p["name"] for p in m["ports"] if p["kind"] == "out"]
         assert ins == (list(pin) if isinstance(pin, tuple) else [pin]) and outs == [pout], node_id
+        # the reference's output layouts need a single precision per output port
+        # (Pipeline.cpp:162-171), display excepted (it picks by its target)
+        out_prec = [p["caps"]["precision"] for p in m["ports"] if p["kind"] == "out"][0]
+        assert len(out_prec) == 1 or node_id in ("com.cpipe.precision_convert",
+                                                 "com.cpipe.color.scene_linear_to_display"), node_id
         assert [p["name"] for p in m["params"]] == params, node_id
         assert m["compute"]["device"] == "CUDA"
 

@@ -137,3 +137,38 @@ def test_error_statuses():
     assert rc == _abi.FAILED
     assert DngReader.read(build_dng(include_cfa=False)).status == _abi.FAILED
     assert DngReader.read("/nonexistent/frame.dng").status == _abi.FAILED
+
+
+def test_dng_input_node(host, tmp_path):
+    """com.cpipe.builtin.dng_input (dng_input.cpp:17-40): the file at "path"
+    decoded on the GPU into the host's R16_UINT output, the reader's metadata
+    attached; status codes for a missing path, a missing file and an output of
+    the wrong extent."""
+    import ctypes as C
+    from cpipe_b200 import _abi as A
+    from cpipe_b200.dng_synth import build_dng
+    rng = np.random.default_rng(11)
+    px = rng.integers(0, 4096, (48, 64)).astype(np.uint16)
+    path = tmp_path / "frame.dng"
+    path.write_bytes(build_dng(width=64, height=48, pixels=px))
+    out = host.buffer(A.FMT_R16_UINT, 64, 48)
+    st = host.run_node("com.cpipe.builtin.dng_input", [], [out], {"path": str(path)})
+    assert st == 0, host.last_error()
+    np.testing.assert_array_equal(out.download(), px)
+    L = A.lib()
+    assert L.cpipe_b200_buffer_cs_role(out._h).decode() == "raw_camera"
+    has, rep, pat = C.c_int(), (C.c_uint8 * 2)(), (C.c_uint8 * 16)()
+    assert L.cpipe_b200_buffer_get_cfa(out._h, C.byref(has), rep, pat) == 0
+    assert has.value == 1 and list(rep) == [2, 2] and list(pat)[:4] == [0, 1, 1, 2]
+    ptr, n = C.c_void_p(), C.c_size_t()
+    assert L.cpipe_b200_buffer_get_blob(out._h, b"com.cpipe.dng.opcode_list_2_bytes", C.byref(ptr), C.byref(n)) == 0
+    assert n.value == 8
+    # the decoded frame feeds the rest of the raw path: linearize -> black level
+    lin = host.buffer(A.FMT_R32_SFLOAT, 64, 48)
+    assert host.run_node("com.cpipe.linearize.dng_lut", [out], [lin]) == 0, host.last_error()
+    table = np.array([0, 128, 1024, 4095], np.float32)
+    np.testing.assert_array_equal(lin.download(), table[np.minimum(px, 3)])
+    assert host.run_node("com.cpipe.builtin.dng_input", [], [out], {}) == A.NEED_PARAM
+    assert host.run_node("com.cpipe.builtin.dng_input", [], [out], {"path": str(tmp_path / "none.dng")}) == A.FAILED
+    wrong = host.buffer(A.FMT_R16_UINT, 32, 48)
+    assert host.run_node("com.cpipe.builtin.dng_input", [], [wrong], {"path": str(path)}) == A.BAD_INDEX
