@@ -166,7 +166,10 @@ class DngInfo(C.Structure):
                 ("linearization_count", C.c_uint32), ("opcode_list_offset", C.c_uint32 * 3),
                 ("opcode_list_bytes", C.c_uint32 * 3), ("exif_offset", C.c_uint32), ("exif_bytes", C.c_uint32),
                 ("xmp_offset", C.c_uint32), ("xmp_bytes", C.c_uint32), ("icc_offset", C.c_uint32),
-                ("icc_bytes", C.c_uint32), ("make", C.c_char * 64), ("model", C.c_char * 64)]
+                ("icc_bytes", C.c_uint32), ("make", C.c_char * 64), ("model", C.c_char * 64),
+                ("seg_tiled", C.c_uint32), ("seg_width", C.c_uint32), ("seg_height", C.c_uint32),
+                ("seg_count", C.c_uint32), ("seg_offsets_pos", C.c_uint32), ("seg_offsets_type", C.c_uint32),
+                ("seg_counts_pos", C.c_uint32), ("seg_counts_type", C.c_uint32)]
 
 
 class ChainConfig(C.Structure):
@@ -222,7 +225,7 @@ EXPORTS = [
     "cpipe_cuda_sharpen_edge_aware_usm", "cpipe_cuda_scene_linear_to_display",
     "cpipe_cuda_copy", "cpipe_cuda_filters", "cpipe_cuda_find_filter",
     "cpipe_cuda_color_3d_lut_noalloc",
-    "cpipe_dng_parse", "cpipe_cuda_dng_decode", "cpipe_cuda_dng_unpack",
+    "cpipe_dng_parse", "cpipe_cuda_dng_decode", "cpipe_cuda_dng_unpack", "cpipe_cuda_lj92_decode",
     "cpipe_b200_node_descs", "cpipe_b200_find_node",
     "cpipe_cuda_scene_raw", "cpipe_cuda_scene_raw_cfa", "cpipe_surrogate_blob_size", "cpipe_surrogate_create", "cpipe_surrogate_destroy", "cpipe_surrogate_export",
     "cpipe_surrogate_denoise", "cpipe_surrogate_set_engine", "cpipe_surrogate_check", "cpipe_surrogate_profile", "cpipe_surrogate_train_step", "cpipe_surrogate_gradients",
@@ -312,6 +315,7 @@ def lib():
         "cpipe_dng_parse": (i32, [vp, sz, C.POINTER(DngInfo)]),
         "cpipe_cuda_dng_decode": (i32, [vp, sz, vp, sz, C.POINTER(DngInfo)]),
         "cpipe_cuda_dng_unpack": (i32, [vp, sz, u32, u32, u32, vp]),
+        "cpipe_cuda_lj92_decode": (i32, [vp, vp, u32, u32, u32, u32, u32, u32, vp]),
         "cpipe_cuda_chain_run": (i32, [vp, vp, vp, vp]), "cpipe_cuda_chain_run_host": (i32, [vp, vp, vp, vp]),
         "cpipe_cuda_chain_run_host_frames": (i32, [vp, vp, vp, i32, vp]),
         "cpipe_cuda_pinned_alloc": (i32, [sz, C.POINTER(vp)]), "cpipe_cuda_pinned_free": (None, [vp]),

@@ -9,6 +9,8 @@
 #include <cstdint>
 #include <cstring>
 
+#include <vector>
+
 #include "../../include/cpipe_b200_dng.h"
 #include "filters_impl.h"
 
@@ -189,8 +191,44 @@ extern "C" int cpipe_cuda_dng_decode(const uint8_t* file, size_t file_bytes, uin
     int st = cpipe_dng_parse(file, file_bytes, d);
     if (st == CPIPE_UNSUPPORTED) return CPIPE_FAILED;  // DngReader.cpp:192-195
     if (st != CPIPE_OK) return st;
+    if (d->compression == 7) {
+        // Lossless JPEG segments (the reference reader hands these to LibRaw).
+        const uint64_t plane7 = (uint64_t)d->width * d->height * 2;
+        if (d_raw == nullptr || raw_bytes < plane7) {
+            set_error("%s", "dng decode: output plane smaller than width * height * 2 bytes");
+            return CPIPE_BAD_INDEX;
+        }
+        if (d->seg_count == 0) {
+            set_error("%s", "compressed DNG without raw data segments");
+            return CPIPE_FAILED;
+        }
+        auto value = [&](uint32_t pos, uint32_t type, uint32_t i, uint64_t* v) {
+            const uint64_t sz = type == 3 ? 2 : 4, at = (uint64_t)pos + sz * i;
+            if (at + sz > file_bytes) return false;
+            const uint8_t* q = file + at;
+            *v = type == 3 ? (uint64_t)(q[0] | (q[1] << 8))
+                           : (uint64_t)q[0] | ((uint64_t)q[1] << 8) | ((uint64_t)q[2] << 16) | ((uint64_t)q[3] << 24);
+            return true;
+        };
+        std::vector<const uint8_t*> streams(d->seg_count);
+        std::vector<size_t> sizes(d->seg_count);
+        for (uint32_t i = 0; i < d->seg_count; ++i) {
+            uint64_t off = 0, cnt = 0;
+            if (!value(d->seg_offsets_pos, d->seg_offsets_type, i, &off) ||
+                !value(d->seg_counts_pos, d->seg_counts_type, i, &cnt) || off > file_bytes || cnt > file_bytes - off) {
+                set_error("%s", "compressed DNG segment lies outside the file");
+                return CPIPE_FAILED;
+            }
+            streams[i] = file + off;
+            sizes[i] = (size_t)cnt;
+        }
+        const uint32_t across = d->seg_tiled ? (d->width + d->seg_width - 1) / d->seg_width : 1;
+        st = lj92_decode(streams.data(), sizes.data(), d->seg_count, across, d->seg_width, d->seg_height, d->width,
+                         d->height, d_raw);
+        return st == CPIPE_UNSUPPORTED ? CPIPE_FAILED : st;
+    }
     if (d->compression != 1) {
-        set_error("%s", "compressed DNG raw (lossless JPEG) decode is not built");
+        set_error("%s", "DNG compression other than none (1) and lossless JPEG (7)");
         return CPIPE_UNSUPPORTED;
     }
     // The strip must lie inside the file (DngReader.cpp:151-154).

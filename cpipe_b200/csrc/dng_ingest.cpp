@@ -23,7 +23,8 @@ enum : uint16_t {
 enum : uint16_t {
     kTagWidth = 256, kTagLength = 257, kTagBits = 258, kTagCompression = 259, kTagPhotometric = 262,
     kTagMake = 271, kTagModel = 272, kTagStripOffsets = 273, kTagOrientation = 274, kTagSamples = 277,
-    kTagStripByteCounts = 279, kTagXmp = 700, kTagCfaRepeat = 33421, kTagCfaPattern = 33422,
+    kTagRowsPerStrip = 278, kTagStripByteCounts = 279, kTagTileWidth = 322, kTagTileLength = 323,
+    kTagTileOffsets = 324, kTagTileByteCounts = 325, kTagXmp = 700, kTagCfaRepeat = 33421, kTagCfaPattern = 33422,
     kTagExposure = 33434, kTagFNumber = 33437, kTagExifIfd = 34665, kTagIcc = 34675, kTagIso = 34855,
     kTagFocal = 37386, kTagLinearization = 50712, kTagBlack = 50714, kTagWhite = 50717,
     kTagColorMatrix1 = 50721, kTagColorMatrix2 = 50722, kTagAsShotNeutral = 50728,
@@ -325,6 +326,33 @@ extern "C" int cpipe_dng_parse(const uint8_t* file, size_t file_bytes, cpipe_Dng
     byte_range(t, ifd0, kTagOpcodeList1, &d.opcode_list_offset[0], &d.opcode_list_bytes[0]);
     byte_range(t, ifd0, kTagOpcodeList2, &d.opcode_list_offset[1], &d.opcode_list_bytes[1]);
     byte_range(t, ifd0, kTagOpcodeList3, &d.opcode_list_offset[2], &d.opcode_list_bytes[2]);
+    // raw data segments: tiles when present, else strips
+    auto array_at = [&](uint16_t tag, uint32_t* where, uint32_t* type, uint32_t* count) {
+        uint64_t p = 0;
+        const Entry* e = ifd0.find(tag, &p);
+        if (!e || (e->type != kShort && e->type != kLong)) return false;
+        const Span s = value_bytes(t, *e, p);
+        if (s.len == 0) return false;
+        *where = (uint32_t)s.file_offset;
+        *type = e->type;
+        *count = e->count;
+        return true;
+    };
+    uint32_t n_off = 0, n_cnt = 0;
+    if (array_at(kTagTileOffsets, &d.seg_offsets_pos, &d.seg_offsets_type, &n_off) &&
+        array_at(kTagTileByteCounts, &d.seg_counts_pos, &d.seg_counts_type, &n_cnt)) {
+        d.seg_tiled = 1;
+        d.seg_width = first_u32(t, ifd0, kTagTileWidth);
+        d.seg_height = first_u32(t, ifd0, kTagTileLength);
+    } else if (array_at(kTagStripOffsets, &d.seg_offsets_pos, &d.seg_offsets_type, &n_off) &&
+               array_at(kTagStripByteCounts, &d.seg_counts_pos, &d.seg_counts_type, &n_cnt)) {
+        bool has_rows = false;
+        const uint32_t rows = first_u32(t, ifd0, kTagRowsPerStrip, &has_rows);
+        d.seg_width = d.width;
+        d.seg_height = has_rows && rows > 0 && rows < d.height ? rows : d.height;
+    }
+    d.seg_count = n_off < n_cnt ? n_off : n_cnt;
+    if (d.seg_width == 0 || d.seg_height == 0) d.seg_count = 0;
 
     *info = d;
     if (d.width == 0 || d.height == 0 || d.bits_per_sample == 0 || d.bits_per_sample > 16 ||

@@ -74,6 +74,9 @@ cudaStream_t current_stream();
 int cuda_status(cudaError_t e, const char* where);
 bool device_ready();
 ff split(double v);
+// Lossless JPEG segments (lj92.cu; cpipe_cuda_lj92_decode's contract).
+int lj92_decode(const uint8_t* const* streams, const size_t* bytes, uint32_t count, uint32_t across, uint32_t seg_w,
+                uint32_t seg_h, uint32_t width, uint32_t height, uint16_t* d_raw);
 
 }  // namespace cpb
 

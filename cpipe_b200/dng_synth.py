@@ -37,10 +37,16 @@ def default_pixels(w, h):
 
 def build_dng(width=4, height=3, pixels=None, strip=None, bits=16, cfa_repeat=(2, 2), cfa_pattern=(0, 1, 1, 2),
               include_cfa=True, include_opcode_lists=True, include_sidecars=True, strip_byte_count=None,
-              overrides=None, drop=()):
+              overrides=None, drop=(), segments=None, tile=None, rows_per_strip=None, strip_tags=True):
     """bytes of a DNG.  `strip` (bytes) replaces the RAW16 little-endian words
     of `pixels`; `overrides` maps tag -> (type, values); `drop` lists tags to
-    leave out."""
+    leave out.  `segments` (list of bytes) makes a Compression 7 file: tiles of
+    `tile` = (width, length) when given (with StripOffsets / StripByteCounts
+    also pointing at the first tile when `strip_tags`), else strips of
+    `rows_per_strip` rows."""
+    if segments is not None:
+        return _build_segmented(width, height, segments, bits, tile, rows_per_strip, strip_tags, cfa_repeat,
+                                cfa_pattern, overrides, drop)
     if strip is None:
         px = default_pixels(width, height) if pixels is None else np.asarray(pixels, np.uint16)
         strip = px.astype("<u2").tobytes()
@@ -48,7 +54,7 @@ def build_dng(width=4, height=3, pixels=None, strip=None, bits=16, cfa_repeat=(2
     tags = {
         256: (LONG, [width]), 257: (LONG, [height]), 258: (SHORT, [bits]), 259: (SHORT, [1]),
         262: (SHORT, [32803]), 271: (ASCII, "GoogleTest"), 272: (ASCII, "Pixel8UT"),
-        273: (LONG, None),  # strip offset, filled in below
+        273: (LONG, None),  # strip offset, filled in below (or by _build_segmented)
         274: (SHORT, [1]), 277: (SHORT, [1]), 278: (LONG, [height]),
         279: (LONG, [len(strip) if strip_byte_count is None else strip_byte_count]),
         33434: (RATIONAL, [(1, 125)]), 33437: (RATIONAL, [(17, 10)]),
@@ -82,7 +88,7 @@ def build_dng(width=4, height=3, pixels=None, strip=None, bits=16, cfa_repeat=(2
     entries = []
     for tag in sorted(tags):
         typ, values = tags[tag]
-        if tag == 273:
+        if tag == 273 and values is None:
             raw = None
         elif tag == 34665:
             raw = None
@@ -111,7 +117,7 @@ def build_dng(width=4, height=3, pixels=None, strip=None, bits=16, cfa_repeat=(2
     out = bytearray(b"II" + struct.pack("<HI", 42, 8) + struct.pack("<H", n))
     for e in entries:
         tag, typ, count, raw = e[:4]
-        if tag == 273:
+        if tag == 273 and raw is None:
             field = struct.pack("<I", strip_off)
         elif tag == 34665:
             field = struct.pack("<I", exif_off)
@@ -123,3 +129,51 @@ def build_dng(width=4, height=3, pixels=None, strip=None, bits=16, cfa_repeat=(2
     out += struct.pack("<I", 0)
     assert len(out) == data_start
     return bytes(out + sections)
+
+
+def _build_segmented(width, height, segments, bits, tile, rows_per_strip, strip_tags, cfa_repeat, cfa_pattern,
+                     overrides, drop):
+    """A Compression 7 file: the base tag set with the data split into
+    segments, whose offset arrays are filled in once the data is placed."""
+    n = len(segments)
+    sizes = [len(x) for x in segments]
+    ov = {259: (SHORT, [7])}
+    if tile is not None:
+        ov.update({322: (LONG, [tile[0]]), 323: (LONG, [tile[1]]), 324: (LONG, [0] * n), 325: (LONG, sizes)})
+        if not strip_tags:
+            drop = tuple(drop) + (273, 279, 278)
+    else:
+        ov.update({273: (LONG, [0] * n), 278: (LONG, [rows_per_strip or height]), 279: (LONG, sizes)})
+    ov.update(overrides or {})
+    marker = b"SEGMENTDATA!"
+    base = build_dng(width, height, strip=marker, bits=bits, cfa_repeat=cfa_repeat, cfa_pattern=cfa_pattern,
+                     overrides=ov, drop=drop)
+    # the base file holds `marker` where the single strip would be: replace it
+    # by the segments (16-byte aligned each) and patch the offsets
+    at = base.index(marker)
+    out = bytearray(base[:at])
+    offsets = []
+    for seg in segments:
+        while len(out) % 16:
+            out.append(0)
+        offsets.append(len(out))
+        out += seg
+    ifd = struct.unpack_from("<I", out, 4)[0]
+    count = struct.unpack_from("<H", out, ifd)[0]
+    for k in range(count):
+        e = ifd + 2 + 12 * k
+        tag, typ, cnt = struct.unpack_from("<HHI", out, e)
+        if (tile is None and tag == 273) or (tile is not None and tag == 324):
+            vals = struct.pack("<%dI" % cnt, *offsets[:cnt])
+        elif tile is not None and tag == 273:
+            vals = struct.pack("<I", offsets[0])
+        elif tile is not None and tag == 279:
+            vals = struct.pack("<I", sizes[0])
+        else:
+            continue
+        if len(vals) <= 4:
+            out[e + 8:e + 12] = vals + b"\0" * (4 - len(vals))
+        else:
+            where = struct.unpack_from("<I", out, e + 8)[0]
+            out[where:where + len(vals)] = vals
+    return bytes(out)

@@ -50,6 +50,14 @@ typedef struct cpipe_DngInfo {
     uint32_t exif_offset, exif_bytes;  /* the Exif IFD's entry table (2 + 12 n + 4 bytes) */
     uint32_t xmp_offset, xmp_bytes, icc_offset, icc_bytes;
     char make[64], model[64];          /* NUL-terminated, truncated to 63 characters */
+    /* Raw data segments: the tiles (TileWidth / TileLength / TileOffsets /
+     * TileByteCounts) when the file has them, else the strips (RowsPerStrip,
+     * StripOffsets, StripByteCounts).  seg_width x seg_height per segment,
+     * seg_count segments in row-major order; the offset and byte-count arrays
+     * sit at the given file offsets with the given TIFF types (3 SHORT,
+     * 4 LONG).  A Compression 7 file has one lossless JPEG stream per segment. */
+    uint32_t seg_tiled, seg_width, seg_height, seg_count;
+    uint32_t seg_offsets_pos, seg_offsets_type, seg_counts_pos, seg_counts_type;
 } cpipe_DngInfo;
 
 /* Parse IFD0 of a little-endian DNG held in host memory.  CPIPE_OK, or
@@ -60,11 +68,14 @@ typedef struct cpipe_DngInfo {
 int cpipe_dng_parse(const uint8_t* file, size_t file_bytes, cpipe_DngInfo* info);
 
 /* DngReader::read over a file image in host memory: parse (CPIPE_UNSUPPORTED
- * becomes CPIPE_FAILED, as the reader maps it), copy the raw strip to the
- * device and unpack it into `d_raw` (width x height R16_UINT, row pitch width,
+ * becomes CPIPE_FAILED, as the reader maps it), copy the raw data to the
+ * device and decode it into `d_raw` (width x height R16_UINT, row pitch width,
  * at least width * height * 2 bytes) on the library's current stream.
- * Uncompressed strips only; a compressed raw (lossless JPEG) returns
- * CPIPE_UNSUPPORTED.  `info` may be NULL. */
+ * Compression 1: the uncompressed strip (cpipe_cuda_dng_unpack).  Compression
+ * 7: the lossless JPEG segments (tiles or strips) through
+ * cpipe_cuda_lj92_decode, where the reference reader calls LibRaw
+ * (DngReader.cpp:113-124); a stream that does not decode is CPIPE_FAILED.
+ * Other compressions: CPIPE_UNSUPPORTED.  `info` may be NULL. */
 int cpipe_cuda_dng_decode(const uint8_t* file, size_t file_bytes, uint16_t* d_raw, size_t raw_bytes,
                           cpipe_DngInfo* info);
 
@@ -77,6 +88,19 @@ int cpipe_cuda_dng_decode(const uint8_t* file, size_t file_bytes, uint16_t* d_ra
  *     strip read as zero. */
 int cpipe_cuda_dng_unpack(const uint8_t* d_strip, size_t strip_bytes, uint32_t width, uint32_t height,
                           uint32_t bits, uint16_t* d_raw);
+
+/* Lossless JPEG (ITU-T T.81 process 14; DNG Compression 7) segments held in
+ * host memory, decoded on the GPU into `d_raw` (width x height R16_UINT): one
+ * stream per segment, segments row-major, `across` per row, each
+ * seg_w x seg_h samples filled row after row from the JPEG lines (X * Nf
+ * samples each) and cropped at the image edges.  Headers are parsed on the
+ * host (SOF3, DHT, DRI, SOS; 1-4 components, predictors 1-7, restart
+ * intervals, point transform); one GPU thread decodes each segment.
+ * CPIPE_FAILED with a message when a header is malformed or a stream does not
+ * decode (it never reads past its segment).  No reference counterpart: the
+ * reference decodes these through LibRaw. */
+int cpipe_cuda_lj92_decode(const uint8_t* const* streams, const size_t* stream_bytes, uint32_t count, uint32_t across,
+                           uint32_t seg_w, uint32_t seg_h, uint32_t width, uint32_t height, uint16_t* d_raw);
 
 #ifdef __cplusplus
 }

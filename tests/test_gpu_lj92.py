@@ -1,0 +1,106 @@
+"""Lossless JPEG (DNG Compression 7) decoded on the GPU (cpipe_cuda_lj92_decode
+and the Compression 7 branch of cpipe_cuda_dng_decode) against the oracle
+codec: every predictor, 1/2/4 components, 8-16 bits, restart intervals, tiles
+cropped at the image edges, strip files, a 12 MP tiled frame; malformed
+streams fail with CPIPE_FAILED."""
+import ctypes as C
+
+import numpy as np
+import oracle_lj92 as L
+import pytest
+from cpipe_b200 import _abi as A
+from cpipe_b200.dng_synth import build_dng
+
+pytestmark = pytest.mark.gpu
+
+
+def smooth(h, w, bits, seed):
+    rng = np.random.default_rng(seed)
+    return (np.cumsum(rng.integers(-40, 41, (h, w)), 1) % (1 << bits)).astype(np.uint16)
+
+
+def gpu_decode(segs, across, sw, sh, w, h):
+    Lb = A.lib()
+    out = C.c_void_p()
+    assert Lb.cpipe_cuda_device_alloc(w * h * 2, C.byref(out)) == 0
+    keep = [C.create_string_buffer(s, len(s)) for s in segs]
+    ptrs = (C.c_void_p * len(segs))(*[C.addressof(k) for k in keep])
+    sizes = (C.c_size_t * len(segs))(*[len(s) for s in segs])
+    st = Lb.cpipe_cuda_lj92_decode(ptrs, sizes, len(segs), across, sw, sh, w, h, out)
+    img = np.zeros((h, w), np.uint16)
+    if st == 0:
+        assert Lb.cpipe_cuda_memcpy_d2h(img.ctypes.data, out, img.nbytes) == 0
+    Lb.cpipe_cuda_device_free(out)
+    return st, img
+
+
+def dng_decode(data, w, h):
+    Lb = A.lib()
+    out = C.c_void_p()
+    assert Lb.cpipe_cuda_device_alloc(w * h * 2, C.byref(out)) == 0
+    st = Lb.cpipe_cuda_dng_decode(data, len(data), out, w * h * 2, None)
+    img = np.zeros((h, w), np.uint16)
+    assert Lb.cpipe_cuda_synchronize() == 0
+    if st == 0:
+        assert Lb.cpipe_cuda_memcpy_d2h(img.ctypes.data, out, img.nbytes) == 0
+    Lb.cpipe_cuda_device_free(out)
+    return st, img
+
+
+@pytest.mark.parametrize("ps", range(1, 8))
+@pytest.mark.parametrize("nf,bits,restart", [(2, 12, 0), (1, 16, 0), (4, 10, 0), (2, 14, 7), (2, 8, 5)])
+def test_stream_matches_oracle(cuda_device, ps, nf, bits, restart):
+    img = np.vstack([smooth(16, 48, bits, ps), np.random.default_rng(ps).integers(0, 1 << bits, (8, 48))]).astype(np.uint16)
+    seg = L.encode(img, bits, ps, nf, restart)
+    want = L.decode(seg, 48, 24)
+    st, got = gpu_decode([seg], 1, 48, 24, 48, 24)
+    assert st == 0, A.lib().cpipe_cuda_last_error()
+    np.testing.assert_array_equal(got, want)
+    np.testing.assert_array_equal(got, img)
+
+
+@pytest.mark.parametrize("w,h,tw,th", [(100, 70, 32, 16), (64, 64, 64, 64), (257, 129, 128, 64), (33, 17, 16, 8)])
+def test_tiles_cropped(cuda_device, w, h, tw, th):
+    img = smooth(h, w, 12, w + h)
+    segs = L.encode_tiles(img, 12, tw, th)
+    st, got = gpu_decode(segs, (w + tw - 1) // tw, tw, th, w, h)
+    assert st == 0, A.lib().cpipe_cuda_last_error()
+    np.testing.assert_array_equal(got, img)
+
+
+def test_dng_files(cuda_device):
+    img = smooth(48, 70, 12, 3)
+    strips = build_dng(width=70, height=48, bits=12, rows_per_strip=16,
+                       segments=[L.encode(img[r:r + 16], 12, 6) for r in range(0, 48, 16)])
+    st, got = dng_decode(strips, 70, 48)
+    assert st == 0, A.lib().cpipe_cuda_last_error()
+    np.testing.assert_array_equal(got, img)
+    tiles = build_dng(width=70, height=48, bits=12, tile=(32, 16), segments=L.encode_tiles(img, 12, 32, 16))
+    st, got = dng_decode(tiles, 70, 48)
+    assert st == 0, A.lib().cpipe_cuda_last_error()
+    np.testing.assert_array_equal(got, img)
+
+
+def test_12mp_tiled_round_trip(cuda_device):
+    img = smooth(3024, 4032, 12, 12)
+    data = build_dng(width=4032, height=3024, bits=12, tile=(256, 256), segments=L.encode_tiles_fast(img, 12, 256, 256))
+    st, got = dng_decode(data, 4032, 3024)
+    assert st == 0, A.lib().cpipe_cuda_last_error()
+    np.testing.assert_array_equal(got, img)
+
+
+def test_malformed_streams_fail(cuda_device):
+    img = smooth(16, 32, 12, 9)
+    seg = bytearray(L.encode(img, 12, 1, 2))
+    sos = bytes(seg).index(b"\xff\xda")
+    start = sos + 2 + int.from_bytes(seg[sos + 2:sos + 4], "big")
+    # the all-ones code is never assigned: a run of stuffed 0xFF bytes cannot decode
+    bad = bytes(seg[:start]) + b"\xff\x00" * 64 + b"\xff\xd9"
+    assert gpu_decode([bad], 1, 32, 16, 32, 16)[0] == A.FAILED
+    assert gpu_decode([bytes(seg[:start - 3])], 1, 32, 16, 32, 16)[0] == A.FAILED  # scan header cut
+    assert gpu_decode([b"\x00\x01" + bytes(seg[2:])], 1, 32, 16, 32, 16)[0] == A.FAILED  # no SOI
+    rst = bytearray(L.encode(img, 12, 1, 2, restart=4))
+    k = bytes(rst).index(b"\xff\xd0")
+    assert gpu_decode([bytes(rst[:k] + rst[k + 2:])], 1, 32, 16, 32, 16)[0] == A.FAILED  # restart marker removed
+    # more samples than the segment holds
+    assert gpu_decode([bytes(seg)], 1, 16, 16, 16, 16)[0] == A.FAILED
