@@ -510,12 +510,18 @@ def dng_ingest(peak_gbs):
     return out
 
 
-def batched_form():
+def batched_form(weights):
     """The 64-frame uneven batch (cpipe_b200.batch): aggregate MP/s of one launch
-    per stage over all frames, per-frame latency alone."""
+    per stage over all frames, per-frame latency inside the batched launch and
+    alone; with the reference's 2x2 blend in the denoiser slot, and with the
+    network and its BM3D spot check there."""
     from cpipe_b200 import batch as B
     r = B.measure(64, 3)
     r.pop("sizes_mp", None)
+    s = B.measure(64, 2, denoise="surrogate", surrogate_blob=weights)
+    s.pop("sizes_mp", None)
+    s.pop("mix", None)
+    r["surrogate_denoiser"] = s
     return r
 
 
@@ -744,7 +750,7 @@ def b200_arm(args):
         "gpu_launches": 33 * args.steps,  # K1, K2, K3, 9 denoiser, 3 spot check, 2 x 9 BM3D (tiles; gated fallback)
     }
     if rank == 0 and world == 1 and not args.no_extra:
-        line["batched_form"] = batched_form()
+        line["batched_form"] = batched_form(weights)
         line["spec_form"] = spec_form(peak_gbs)
         line["finishing_stages"] = finishing_stages()
         line["config1_chain"] = config1_chain(peak_gbs)

@@ -248,7 +248,7 @@ EXPORTS = [
     "cpipe_cuda_chain_create", "cpipe_cuda_chain_destroy", "cpipe_cuda_chain_output_bytes", "cpipe_cuda_chain_run",
     "cpipe_cuda_chain_run_host", "cpipe_cuda_chain_run_host_frames", "cpipe_cuda_pinned_alloc", "cpipe_cuda_pinned_free",
     "cpipe_cuda_batch_create", "cpipe_cuda_batch_destroy", "cpipe_cuda_batch_run", "cpipe_cuda_batch_autotune",
-    "cpipe_cuda_batch_frame_chain", "cpipe_cuda_chain_set_profiling", "cpipe_cuda_chain_profile", "cpipe_cuda_chain_denoise_stats", "cpipe_cuda_set_device", "cpipe_cuda_device_alloc",
+    "cpipe_cuda_batch_frame_chain", "cpipe_cuda_batch_schedule", "cpipe_cuda_batch_frame_times", "cpipe_cuda_chain_set_profiling", "cpipe_cuda_chain_profile", "cpipe_cuda_chain_denoise_stats", "cpipe_cuda_set_device", "cpipe_cuda_device_alloc",
     "cpipe_cuda_device_free", "cpipe_cuda_memcpy_h2d", "cpipe_cuda_memcpy_d2h", "cpipe_cuda_memcpy_d2d_async", "cpipe_cuda_count_nonfinite",
     "cpipe_cuda_stream_create",
     "cpipe_cuda_stream_destroy", "cpipe_cuda_stream_synchronize", "cpipe_cuda_event_create",
@@ -323,6 +323,8 @@ def lib():
         "cpipe_cuda_batch_create": (vp, [vp, sz, C.POINTER(i32)]), "cpipe_cuda_batch_destroy": (None, [vp]),
         "cpipe_cuda_batch_run": (i32, [vp, vp, vp, vp]), "cpipe_cuda_batch_autotune": (i32, [vp, vp, vp, vp, vp]),
         "cpipe_cuda_batch_frame_chain": (vp, [vp, sz]),
+        "cpipe_cuda_batch_schedule": (i32, [vp, vp, C.POINTER(i32)]),
+        "cpipe_cuda_batch_frame_times": (i32, [vp, vp, vp, sz]),
         "cpipe_cuda_chain_profile": (i32, [vp, C.POINTER(C.c_double), C.POINTER(i32)]),
         "cpipe_cuda_chain_denoise_stats": (i32, [vp, C.POINTER(u32), C.POINTER(u32), C.POINTER(C.c_float)]),
         "cpipe_cuda_set_device": (i32, [i32]), "cpipe_cuda_device_alloc": (i32, [sz, C.POINTER(vp)]),

@@ -426,6 +426,7 @@ struct cpipe_cuda_chain {
     Bm3dPlan bm3d{};
     void* d_denoise = nullptr;            // scratch of the mode-1 denoiser
     SurrogateNet* sg = nullptr;           // mode-2 network
+    bool owns_sg = true, owns_denoise = true;  // false: a batch's shared network / BM3D scratch
     float* d_ab = nullptr;                // its noise model (a, b) on the device
     // mode-2 spot check
     int spot_tiles = 0, spot_edge = 0;
@@ -490,6 +491,47 @@ cudaEvent_t* profile_slot(cpipe_cuda_chain* c) {
     return &c->events[c->profiled++ * kProfileEvents];
 }
 
+// The denoiser between K2 and K3 (denoise_mode 1: two-stage BM3D; 2: the
+// network with its spot check: the tiles' BM3D forked onto the side stream,
+// joined before the MSE, and the full-frame BM3D gated on the device).
+int denoise_stage(cpipe_cuda_chain* c, const Img& k2_out, const Img& dn_out, cudaStream_t st) {
+    const int w = c->cfg.width, h = c->cfg.height;
+    const bool spot = c->denoise_mode == 2 && c->spot_tiles > 0;
+    cudaError_t e = cudaSuccess;
+    if (spot) {  // fork: gather + the tiles' BM3D on the side stream
+        const int E = c->spot_edge, n = c->spot_tiles;
+        const Img tin{c->d_tile_in, E, E * n, (long long)E * 4, 4};
+        const Img tref{c->d_tile_ref, E, E * n, (long long)E * 4, 4};
+        const dim3 gg((unsigned)((E + 127) / 128), (unsigned)E, (unsigned)n);
+        cudaStream_t ss = c->spot_stream;
+        e = cudaEventRecord(c->spot_fork, st);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(ss, c->spot_fork, 0);
+        if (e != cudaSuccess) return cuda_status(e, "chain spot fork");
+        if (c->f16) spot::gather_kernel<__half><<<gg, 128, 0, ss>>>(k2_out, static_cast<__half*>(c->d_tile_in), E, c->spot);
+        else spot::gather_kernel<float><<<gg, 128, 0, ss>>>(k2_out, static_cast<float*>(c->d_tile_in), E, c->spot);
+        e = bm3d_run(c->tile_plan, tin, tref, c->f16, c->d_tile_scratch, ss, false);
+        // the join is recorded even after a launch error, so the side stream never stays forked
+        const cudaError_t ej = cudaEventRecord(c->spot_join, ss);
+        if (e == cudaSuccess) e = ej;
+    }
+    if (e == cudaSuccess)
+        e = c->denoise_mode == 1 ? bm3d_run(c->bm3d, k2_out, dn_out, c->f16, c->d_denoise, st, false)
+                                 : surrogate_infer(c->sg, k2_out.data, dn_out.data, 1, h, w, c->f16, c->d_ab, st);
+    if (spot) {
+        const cudaError_t ew = cudaStreamWaitEvent(st, c->spot_join, 0);
+        if (e == cudaSuccess) e = ew;
+    }
+    if (e == cudaSuccess && spot) {
+        const int E = c->spot_edge, n = c->spot_tiles;
+        const dim3 gm((unsigned)((E + spot::kMseRows - 1) / spot::kMseRows), (unsigned)n);
+        if (c->f16) spot::mse_kernel<__half><<<gm, 256, 0, st>>>(dn_out, static_cast<const __half*>(c->d_tile_ref), E, c->spot, c->d_tile_mse);
+        else spot::mse_kernel<float><<<gm, 256, 0, st>>>(dn_out, static_cast<const float*>(c->d_tile_ref), E, c->spot, c->d_tile_mse);
+        spot::decide_kernel<<<1, 1, 0, st>>>(c->d_tile_mse, n, E, c->spot_mse_max, c->d_gate, c->d_stats);
+        e = bm3d_run(c->bm3d, k2_out, dn_out, c->f16, c->d_denoise, st, false, c->d_gate);
+    }
+    return e == cudaSuccess ? CPIPE_OK : cuda_status(e, "chain denoise");
+}
+
 int launch_chain(cpipe_cuda_chain* c, const void* d_raw, size_t raw_pitch, void* d_out, size_t out_pitch,
                  cudaStream_t st) {
     cudaEvent_t* ev = profile_slot(c);
@@ -546,42 +588,8 @@ int launch_chain(cpipe_cuda_chain* c, const void* d_raw, size_t raw_pitch, void*
     }
     if (c->denoise_mode != 0) {
         const Img dn_out = c->stop_after == 2 ? out : (k2_out.data == mid1.data) ? mid0 : mid1;
-        const bool spot = c->denoise_mode == 2 && c->spot_tiles > 0;
-        cudaError_t e = cudaSuccess;
-        if (spot) {  // fork: gather + the tiles' BM3D on the side stream
-            const int E = c->spot_edge, n = c->spot_tiles;
-            const Img tin{c->d_tile_in, E, E * n, (long long)E * 4, 4};
-            const Img tref{c->d_tile_ref, E, E * n, (long long)E * 4, 4};
-            const dim3 gg((unsigned)((E + 127) / 128), (unsigned)E, (unsigned)n);
-            cudaStream_t ss = c->spot_stream;
-            e = cudaEventRecord(c->spot_fork, st);
-            if (e == cudaSuccess) e = cudaStreamWaitEvent(ss, c->spot_fork, 0);
-            if (e != cudaSuccess) return cuda_status(e, "chain spot fork");
-            if (c->f16) spot::gather_kernel<__half><<<gg, 128, 0, ss>>>(k2_out, static_cast<__half*>(c->d_tile_in), E, c->spot);
-            else spot::gather_kernel<float><<<gg, 128, 0, ss>>>(k2_out, static_cast<float*>(c->d_tile_in), E, c->spot);
-            e = bm3d_run(c->tile_plan, tin, tref, c->f16, c->d_tile_scratch, ss, false);
-            // the join is recorded even after a launch error, so the side stream never stays forked
-            const cudaError_t ej = cudaEventRecord(c->spot_join, ss);
-            if (e == cudaSuccess) e = ej;
-        }
-        if (e == cudaSuccess)
-            e = c->denoise_mode == 1 ? bm3d_run(c->bm3d, k2_out, dn_out, c->f16, c->d_denoise, st, false)
-                                     : surrogate_infer(c->sg, k2_out.data, dn_out.data, 1, h, w, c->f16, c->d_ab, st);
-        if (spot) {
-            const cudaError_t ew = cudaStreamWaitEvent(st, c->spot_join, 0);
-            if (e == cudaSuccess) e = ew;
-        }
-        if (e == cudaSuccess && spot) {
-            const int E = c->spot_edge, n = c->spot_tiles;
-            {
-                const dim3 gm((unsigned)((E + spot::kMseRows - 1) / spot::kMseRows), (unsigned)n);
-                if (c->f16) spot::mse_kernel<__half><<<gm, 256, 0, st>>>(dn_out, static_cast<const __half*>(c->d_tile_ref), E, c->spot, c->d_tile_mse);
-                else spot::mse_kernel<float><<<gm, 256, 0, st>>>(dn_out, static_cast<const float*>(c->d_tile_ref), E, c->spot, c->d_tile_mse);
-                spot::decide_kernel<<<1, 1, 0, st>>>(c->d_tile_mse, n, E, c->spot_mse_max, c->d_gate, c->d_stats);
-                e = bm3d_run(c->bm3d, k2_out, dn_out, c->f16, c->d_denoise, st, false, c->d_gate);
-            }
-        }
-        if (e != cudaSuccess) return cuda_status(e, "chain denoise");
+        const int ds = denoise_stage(c, k2_out, dn_out, st);
+        if (ds != CPIPE_OK) return ds;
         k2_out = dn_out;
     }
     if (c->stop_after == 2) {
@@ -659,7 +667,20 @@ cudaError_t allow_smem() {
 
 extern "C" {
 
+// A batch's denoiser resources shared by its frames' chains (frames are
+// denoised one after another on one stream): the network, reserved for the
+// largest frame, and the full-frame BM3D scratch of the largest plan.
+struct ChainShared {
+    SurrogateNet* sg = nullptr;
+    void* d_denoise = nullptr;
+};
+static cpipe_cuda_chain* chain_create(const cpipe_cuda_chain_config* cfg, int* status, const ChainShared* shared);
+
 cpipe_cuda_chain* cpipe_cuda_chain_create(const cpipe_cuda_chain_config* cfg, int* status) {
+    return chain_create(cfg, status, nullptr);
+}
+
+static cpipe_cuda_chain* chain_create(const cpipe_cuda_chain_config* cfg, int* status, const ChainShared* shared) {
     auto fail = [&](int st, cpipe_cuda_chain* c) -> cpipe_cuda_chain* {
         if (status) *status = st;
         if (c) cpipe_cuda_chain_destroy(c);
@@ -758,13 +779,18 @@ cpipe_cuda_chain* cpipe_cuda_chain_create(const cpipe_cuda_chain_config* cfg, in
     if (c->stop_after < 0 || c->stop_after > 2 || (c->stop_after == 2 && c->denoise_mode == 0))
         return fail(CPIPE_UNSUPPORTED, c);
     if (c->denoise_mode == 2) {
-        c->sg = surrogate_new(cfg->surrogate_blob, cfg->surrogate_blob_size, &st);
+        if (shared) {
+            c->sg = shared->sg;
+            c->owns_sg = false;
+        } else {
+            c->sg = surrogate_new(cfg->surrogate_blob, cfg->surrogate_blob_size, &st);
+        }
         if (!c->sg) return fail(st, c);
         const float ab[2] = {cfg->noise_a, cfg->noise_b};
         if (cudaMalloc(&c->d_ab, sizeof(ab)) != cudaSuccess) return fail(CPIPE_OOM, c);
         if (cudaMemcpy(c->d_ab, ab, sizeof(ab), cudaMemcpyHostToDevice) != cudaSuccess)
             return fail(CPIPE_INTERNAL_ERROR, c);
-        if (surrogate_reserve(c->sg, (long long)w * h) != cudaSuccess) return fail(CPIPE_OOM, c);
+        if (!shared && surrogate_reserve(c->sg, (long long)w * h) != cudaSuccess) return fail(CPIPE_OOM, c);
         c->spot_tiles = cfg->spot_tiles < 0 ? 0 : (cfg->spot_tiles > 16 ? 16 : cfg->spot_tiles);
         if (c->spot_tiles > 0) {
             // stratified tiles: the centres of a 4x4 grid of cells, clamped inside the frame
@@ -783,7 +809,7 @@ cpipe_cuda_chain* cpipe_cuda_chain_create(const cpipe_cuda_chain_config* cfg, in
             const size_t tile_bytes = (size_t)E * E * c->spot_tiles * 4 * (c->f16 ? 2 : 4);
             if (cudaMalloc(&c->d_tile_in, tile_bytes) != cudaSuccess || cudaMalloc(&c->d_tile_ref, tile_bytes) != cudaSuccess ||
                 (!c->tile_plan.copy && cudaMalloc(&c->d_tile_scratch, c->tile_plan.bytes) != cudaSuccess) ||
-                (!c->bm3d.copy && cudaMalloc(&c->d_denoise, c->bm3d.bytes) != cudaSuccess) ||
+                (!c->bm3d.copy && !shared && cudaMalloc(&c->d_denoise, c->bm3d.bytes) != cudaSuccess) ||
                 cudaMalloc(&c->d_tile_mse, sizeof(float) * 16 * spot::kMseChunks) != cudaSuccess ||
                 cudaMalloc(&c->d_gate, sizeof(int)) != cudaSuccess || cudaMalloc(&c->d_stats, sizeof(SpotStats)) != cudaSuccess)
                 return fail(CPIPE_OOM, c);
@@ -806,8 +832,12 @@ cpipe_cuda_chain* cpipe_cuda_chain_create(const cpipe_cuda_chain_config* cfg, in
         cpipe_Bm3dSpecParams sp = cfg->bm3d_spec;
         if (!(sp.sigma > 0.0F)) sp.sigma = cfg->bm3d_sigma;
         if ((st = bm3d_plan(&sp, w, h, &c->bm3d)) != CPIPE_OK) return fail(st, c);
-        if (!c->bm3d.copy && cudaMalloc(&c->d_denoise, c->bm3d.bytes) != cudaSuccess) return fail(CPIPE_OOM, c);
+        if (!c->bm3d.copy && !shared && cudaMalloc(&c->d_denoise, c->bm3d.bytes) != cudaSuccess) return fail(CPIPE_OOM, c);
         if (cudaError_t e = bm3d_setup(c->bm3d); e != cudaSuccess) return fail(cuda_status(e, "bm3d setup"), c);
+    }
+    if (shared) {
+        c->d_denoise = shared->d_denoise;
+        c->owns_denoise = false;
     }
     // guided_radius 0 leaves the guided node out; otherwise the reference box
     // is 3x3 for radius <= 1 and 5x5 above (guided_filter_generator.cpp:66-70).
@@ -889,7 +919,7 @@ void cpipe_cuda_chain_destroy(cpipe_cuda_chain* c) {
     cudaFree(c->d_taps_ixy);
     cudaFree(c->d_taps_tx);
     cudaFree(c->d_taps_ty);
-    cudaFree(c->d_denoise);
+    if (c->owns_denoise) cudaFree(c->d_denoise);
     cudaFree(c->d_bayer);
     cudaFree(c->d_ab);
     cudaFree(c->d_tile_in);
@@ -902,7 +932,7 @@ void cpipe_cuda_chain_destroy(cpipe_cuda_chain* c) {
     if (c->spot_fork) cudaEventDestroy(c->spot_fork);
     if (c->spot_join) cudaEventDestroy(c->spot_join);
     if (c->spot_stream) cudaStreamDestroy(c->spot_stream);
-    surrogate_free(c->sg);
+    if (c->owns_sg) surrogate_free(c->sg);
     for (void* p : c->d_mid) cudaFree(p);
     for (void* p : c->d_io) cudaFree(p);
     delete c;
@@ -1160,13 +1190,28 @@ constexpr int kK2Rows = 8;  // stage-2 work item: 128 pixels x 8 rows
 
 struct Frame {
     Img bayer, mid0, mid1, out;  // bayer: the raw input, or its remosaic for Quad-Bayer frames
+    Img tone_in;                 // mid1, or the denoiser's output (mid0) when a denoiser runs between
     RawParams raw;
     WarpDev warp;
     ColorParams color;
     ToneParams tone;
     int t1x, t2x, t3x;  // work items per row, per stage
-    int pad;
+    int rows2;          // rows per stage-2 work item (autotuned)
 };
+
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// First node of a batch run: the start time and each frame's count of
+// stage-3 items still to finish.
+__global__ void batch_clock_kernel(const int* __restrict__ prefix3, int n, int* __restrict__ left,
+                                   unsigned long long* __restrict__ t0) {
+    for (int i = threadIdx.x; i < n; i += blockDim.x) left[i] = prefix3[i + 1] - prefix3[i];
+    if (threadIdx.x == 0) *t0 = global_ns();
+}
 
 __device__ __forceinline__ int find_frame(const int* prefix, int n, int t) {
     int lo = 0, hi = n - 1;
@@ -1220,16 +1265,19 @@ __global__ void __launch_bounds__(128) batch_color_kernel(const Frame* __restric
     int cur = -1;
     for (int t = blockIdx.x; t < s_prefix[n]; t += gridDim.x) {
         const int local = next_item(frames, s_prefix, n, t, &s_f, &cur);
-        const int x = (local % s_f.t2x) * 128 + (int)threadIdx.x, y0 = (local / s_f.t2x) * kK2Rows;
+        const int rows = s_f.rows2;
+        const int x = (local % s_f.t2x) * 128 + (int)threadIdx.x, y0 = (local / s_f.t2x) * rows;
         if (x < s_f.mid1.w)
-            for (int r = 0; r < kK2Rows && y0 + r < s_f.mid1.h; ++r)
+            for (int r = 0; r < rows && y0 + r < s_f.mid1.h; ++r)
                 warp_wb_cm_px<__half, true, WARP>(s_f.mid0, s_f.mid1, s_f.warp, s_f.color, x, y0 + r);
     }
 }
 
 template <int R>
 __global__ void __launch_bounds__(256, 3) batch_tone_kernel(const Frame* __restrict__ frames,
-                                                            const int* __restrict__ prefix, int n) {
+                                                            const int* __restrict__ prefix, int n,
+                                                            int* __restrict__ left,
+                                                            unsigned long long* __restrict__ done) {
     extern __shared__ __align__(16) float smem_f[];
     __shared__ int s_prefix[kMaxFrames + 1];
     __shared__ Frame s_f;
@@ -1238,9 +1286,14 @@ __global__ void __launch_bounds__(256, 3) batch_tone_kernel(const Frame* __restr
     int cur = -1;
     for (int t = blockIdx.x; t < s_prefix[n]; t += gridDim.x) {
         const int local = next_item(frames, s_prefix, n, t, &s_f, &cur);
-        denoise_tone_tile<__half, true, R>(s_f.mid1, s_f.out, s_f.tone, (local % s_f.t3x) * kCTW,
+        denoise_tone_tile<__half, true, R>(s_f.tone_in, s_f.out, s_f.tone, (local % s_f.t3x) * kCTW,
                                            (local / s_f.t3x) * kCTH, smem_f);
         __syncthreads();
+        // the frame's completion time: stamped by the CTA that finishes its last item
+        if (threadIdx.x == 0 && left != nullptr) {
+            __threadfence();
+            if (atomicSub(left + cur, 1) == 1) done[cur] = global_ns();
+        }
     }
 }
 
@@ -1255,6 +1308,13 @@ struct cpipe_cuda_batch {
     int n = 0, algo = 1, radius = 2;
     bool warp = false;
     int per_sm[3] = {2, 8, 3};  // persistent CTAs per SM for the three stages (autotuned)
+    int rows2 = cpb::batch::kK2Rows;  // rows per stage-2 work item (autotuned)
+    int denoise_mode = 0;             // 0: the reference's 2x2 blend in K3; 1 / 2: BM3D / the network between K2 and K3
+    std::vector<int> prefix;          // three arrays of n + 1 (host copy)
+    SurrogateNet* shared_sg = nullptr;  // denoiser resources shared by the frames' chains
+    void* shared_denoise = nullptr;
+    int* d_left = nullptr;            // per frame: stage-3 items not finished yet
+    unsigned long long* d_times = nullptr;  // [0]: start; [1 + i]: frame i's completion (globaltimer ns)
     cudaGraphExec_t graph = nullptr;
     std::vector<const void*> graph_in;
     std::vector<void*> graph_out;
@@ -1265,7 +1325,7 @@ namespace {
 
 using cpb::batch::Frame;
 
-int batch_launch_stage(cpipe_cuda_batch* b, int stage, cudaStream_t st) {
+int batch_launch_stage(cpipe_cuda_batch* b, int stage, cudaStream_t st, bool timed = false) {
     const int grid = kSmCount * b->per_sm[stage];
     const int* pf = b->d_prefix + stage * (b->n + 1);
     if (stage == 0) {
@@ -1276,12 +1336,15 @@ int batch_launch_stage(cpipe_cuda_batch* b, int stage, cudaStream_t st) {
         if (b->warp) cpb::batch::batch_color_kernel<true><<<grid, 128, 0, st>>>(b->d_frames, pf, b->n);
         else cpb::batch::batch_color_kernel<false><<<grid, 128, 0, st>>>(b->d_frames, pf, b->n);
     } else {
+        // completion stamps only in a full run (the autotuner times stages alone)
+        int* left = timed ? b->d_left : nullptr;
+        unsigned long long* done = b->d_times + 1;
         if (b->radius == 0)
-            cpb::batch::batch_tone_kernel<0><<<grid, 256, denoise_tone_smem<__half, true, 0>(), st>>>(b->d_frames, pf, b->n);
+            cpb::batch::batch_tone_kernel<0><<<grid, 256, denoise_tone_smem<__half, true, 0>(), st>>>(b->d_frames, pf, b->n, left, done);
         else if (b->radius == 1)
-            cpb::batch::batch_tone_kernel<1><<<grid, 256, denoise_tone_smem<__half, true, 1>(), st>>>(b->d_frames, pf, b->n);
+            cpb::batch::batch_tone_kernel<1><<<grid, 256, denoise_tone_smem<__half, true, 1>(), st>>>(b->d_frames, pf, b->n, left, done);
         else
-            cpb::batch::batch_tone_kernel<2><<<grid, 256, denoise_tone_smem<__half, true, 2>(), st>>>(b->d_frames, pf, b->n);
+            cpb::batch::batch_tone_kernel<2><<<grid, 256, denoise_tone_smem<__half, true, 2>(), st>>>(b->d_frames, pf, b->n, left, done);
     }
     return cuda_status(cudaGetLastError(), "batch stage");
 }
@@ -1296,11 +1359,36 @@ int batch_launch(cpipe_cuda_batch* b, cudaStream_t st) {
             if (e != cudaSuccess) return cuda_status(e, "batch remosaic");
         }
     }
+    cpb::batch::batch_clock_kernel<<<1, 64, 0, st>>>(b->d_prefix + 2 * (b->n + 1), b->n, b->d_left, b->d_times);
     for (int stage = 0; stage < 3; ++stage) {
-        const int s = batch_launch_stage(b, stage, st);
+        const int s = batch_launch_stage(b, stage, st, true);
         if (s != CPIPE_OK) return s;
+        if (stage == 1 && b->denoise_mode != 0) {
+            // the denoiser of every frame between its K2 and K3 (its chain's
+            // network, spot check and gated BM3D, or its BM3D)
+            for (int i = 0; i < b->n; ++i) {
+                const int ds = denoise_stage(b->chains[i], b->frames[i].mid1, b->frames[i].mid0, st);
+                if (ds != CPIPE_OK) return ds;
+            }
+        }
     }
     return CPIPE_OK;
+}
+
+// Stage prefixes for the current stage-2 rows per item; copied to the device.
+int batch_prefix(cpipe_cuda_batch* b) {
+    const int n = b->n;
+    b->prefix.assign(3 * (n + 1), 0);
+    for (int i = 0; i < n; ++i) {
+        cpb::batch::Frame& f = b->frames[i];
+        const int h = f.mid0.h;
+        f.rows2 = b->rows2;
+        b->prefix[0 * (n + 1) + i + 1] = b->prefix[0 * (n + 1) + i] + f.t1x * ((h + kDmTH - 1) / kDmTH);
+        b->prefix[1 * (n + 1) + i + 1] = b->prefix[1 * (n + 1) + i] + f.t2x * ((h + b->rows2 - 1) / b->rows2);
+        b->prefix[2 * (n + 1) + i + 1] = b->prefix[2 * (n + 1) + i] + f.t3x * ((h + kCTH - 1) / kCTH);
+    }
+    return cuda_status(cudaMemcpy(b->d_prefix, b->prefix.data(), sizeof(int) * b->prefix.size(), cudaMemcpyHostToDevice),
+                       "batch prefix");
 }
 
 template <int R>
@@ -1321,8 +1409,12 @@ void cpipe_cuda_batch_destroy(cpipe_cuda_batch* b) {
     if (!b) return;
     if (b->graph) cudaGraphExecDestroy(b->graph);
     for (cpipe_cuda_chain* c : b->chains) cpipe_cuda_chain_destroy(c);
+    surrogate_free(b->shared_sg);
+    cudaFree(b->shared_denoise);
     cudaFree(b->d_frames);
     cudaFree(b->d_prefix);
+    cudaFree(b->d_left);
+    cudaFree(b->d_times);
     delete b;
 }
 
@@ -1336,17 +1428,48 @@ cpipe_cuda_batch* cpipe_cuda_batch_create(const cpipe_cuda_chain_config* cfgs, s
     auto* b = new (std::nothrow) cpipe_cuda_batch();
     if (!b) return fail(CPIPE_OOM, nullptr);
     b->n = (int)n;
-    std::vector<int> prefix(3 * (n + 1), 0);
+    b->denoise_mode = cfgs[0].denoise_mode;
+    ChainShared shared{};
+    if (b->denoise_mode == 1 || b->denoise_mode == 2) {
+        // one network reserved for the largest frame and one BM3D scratch of
+        // the largest plan serve every frame (they are denoised in turn)
+        long long max_px = 0;
+        size_t max_bytes = 0;
+        for (size_t i = 0; i < n; ++i) {
+            const cpipe_cuda_chain_config& c = cfgs[i];
+            if (c.denoise_mode == 2 && (c.surrogate_blob_size != cfgs[0].surrogate_blob_size ||
+                                        (c.surrogate_blob != cfgs[0].surrogate_blob &&
+                                         std::memcmp(c.surrogate_blob, cfgs[0].surrogate_blob, c.surrogate_blob_size)))) {
+                set_error("batch: %s", "every frame needs the same network weights");
+                return fail(CPIPE_UNSUPPORTED, b);
+            }
+            max_px = std::max(max_px, (long long)c.width * c.height);
+            cpipe_Bm3dSpecParams sp = c.bm3d_spec;
+            if (!(sp.sigma > 0.0F)) sp.sigma = c.bm3d_sigma;
+            Bm3dPlan q;
+            if (bm3d_plan(&sp, c.width, c.height, &q) == CPIPE_OK && !q.copy) max_bytes = std::max(max_bytes, q.bytes);
+        }
+        if (b->denoise_mode == 2) {
+            int st = CPIPE_OK;
+            b->shared_sg = surrogate_new(cfgs[0].surrogate_blob, cfgs[0].surrogate_blob_size, &st);
+            if (!b->shared_sg) return fail(st, b);
+            if (surrogate_reserve(b->shared_sg, max_px) != cudaSuccess) return fail(CPIPE_OOM, b);
+        }
+        if (max_bytes && cudaMalloc(&b->shared_denoise, max_bytes) != cudaSuccess) return fail(CPIPE_OOM, b);
+        shared.sg = b->shared_sg;
+        shared.d_denoise = b->shared_denoise;
+    }
     for (size_t i = 0; i < n; ++i) {
         cpipe_cuda_chain_config c = cfgs[i];
-        if (c.plain_f32 || c.denoise_mode != 0 || c.stop_after != 0 || c.guided_spec || c.atrous_levels || c.sharpen ||
-            c.display) {
-            set_error("batch: %s", "frames run the parity chain (binary16, the reference's denoise.bm3d)");
+        if (c.plain_f32 || c.denoise_mode != b->denoise_mode || c.stop_after != 0 || c.guided_spec || c.atrous_levels ||
+            c.sharpen || c.display) {
+            set_error("batch: %s", "frames run the binary16 chain with one denoiser for all (the reference's "
+                                   "denoise.bm3d, two-stage BM3D or the network)");
             return fail(CPIPE_UNSUPPORTED, b);
         }
         c.use_graph = 0;
         int st = CPIPE_OK;
-        cpipe_cuda_chain* ch = cpipe_cuda_chain_create(&c, &st);
+        cpipe_cuda_chain* ch = chain_create(&c, &st, b->denoise_mode != 0 ? &shared : nullptr);
         if (!ch) return fail(st, b);
         b->chains.push_back(ch);
         if (i == 0) {
@@ -1362,6 +1485,7 @@ cpipe_cuda_batch* cpipe_cuda_batch_create(const cpipe_cuda_chain_config* cfgs, s
         Frame f{};
         f.mid0 = Img{ch->d_mid[0], w, h, (long long)w * 4, 4};
         f.mid1 = Img{ch->d_mid[1], w, h, (long long)w * 4, 4};
+        f.tone_in = b->denoise_mode != 0 ? f.mid0 : f.mid1;
         f.raw = ch->raw;
         f.warp = ch->warp;
         f.color = ch->color;
@@ -1370,15 +1494,13 @@ cpipe_cuda_batch* cpipe_cuda_batch_create(const cpipe_cuda_chain_config* cfgs, s
         f.t2x = (w + 127) / 128;
         f.t3x = (w + kCTW - 1) / kCTW;
         b->frames.push_back(f);
-        prefix[0 * (n + 1) + i + 1] = prefix[0 * (n + 1) + i] + f.t1x * ((h + kDmTH - 1) / kDmTH);
-        prefix[1 * (n + 1) + i + 1] = prefix[1 * (n + 1) + i] + f.t2x * ((h + cpb::batch::kK2Rows - 1) / cpb::batch::kK2Rows);
-        prefix[2 * (n + 1) + i + 1] = prefix[2 * (n + 1) + i] + f.t3x * ((h + kCTH - 1) / kCTH);
     }
     if (cudaMalloc(&b->d_frames, sizeof(Frame) * n) != cudaSuccess ||
-        cudaMalloc(&b->d_prefix, sizeof(int) * prefix.size()) != cudaSuccess)
+        cudaMalloc(&b->d_prefix, sizeof(int) * 3 * (n + 1)) != cudaSuccess ||
+        cudaMalloc(&b->d_left, sizeof(int) * n) != cudaSuccess ||
+        cudaMalloc(&b->d_times, sizeof(unsigned long long) * (n + 1)) != cudaSuccess)
         return fail(CPIPE_OOM, b);
-    if (cudaMemcpy(b->d_prefix, prefix.data(), sizeof(int) * prefix.size(), cudaMemcpyHostToDevice) != cudaSuccess)
-        return fail(CPIPE_INTERNAL_ERROR, b);
+    if (batch_prefix(b) != CPIPE_OK) return fail(CPIPE_INTERNAL_ERROR, b);
     cudaError_t e = b->radius == 0 ? allow_batch_smem<0>() : b->radius == 1 ? allow_batch_smem<1>() : allow_batch_smem<2>();
     if (e != cudaSuccess) return fail(cuda_status(e, "batch smem"), b);
     if (status) *status = CPIPE_OK;
@@ -1445,27 +1567,47 @@ int cpipe_cuda_batch_autotune(cpipe_cuda_batch* b, const void* const* d_raw, voi
     cudaEvent_t e0, e1;
     if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return CPIPE_INTERNAL_ERROR;
     s = batch_launch(b, st);  // fills every stage's input once
+    // stage 2 also picks its work-item shape: 128 pixels x rows2 rows
+    static const int rows_cand[4] = {4, 8, 16, 32};
     for (int stage = 0; stage < 3 && s == CPIPE_OK; ++stage) {
         float best = 1e30F;
-        int best_k = b->per_sm[stage];
-        for (int k : cand[stage]) {
-            b->per_sm[stage] = k;
-            float total = 0.0F;
-            for (int r = 0; r < 3 && s == CPIPE_OK; ++r) {
-                cudaEventRecord(e0, st);
-                s = batch_launch_stage(b, stage, st);
-                cudaEventRecord(e1, st);
-                if (cudaEventSynchronize(e1) != cudaSuccess) s = CPIPE_INTERNAL_ERROR;
-                float ms = 0.0F;
-                cudaEventElapsedTime(&ms, e0, e1);
-                if (r > 0) total += ms;  // the first run warms up
+        int best_k = b->per_sm[stage], best_rows = b->rows2;
+        for (int ri = 0; ri < (stage == 1 ? 4 : 1) && s == CPIPE_OK; ++ri) {
+            if (stage == 1) {
+                b->rows2 = rows_cand[ri];
+                s = batch_prefix(b);
+                if (s == CPIPE_OK)
+                    s = cuda_status(cudaMemcpy(b->d_frames, b->frames.data(), sizeof(Frame) * b->n, cudaMemcpyHostToDevice),
+                                    "batch descriptors");
             }
-            if (total < best) {
-                best = total;
-                best_k = k;
+            for (int k : cand[stage]) {
+                if (s != CPIPE_OK) break;
+                b->per_sm[stage] = k;
+                float total = 0.0F;
+                for (int r = 0; r < 3 && s == CPIPE_OK; ++r) {
+                    cudaEventRecord(e0, st);
+                    s = batch_launch_stage(b, stage, st);
+                    cudaEventRecord(e1, st);
+                    if (cudaEventSynchronize(e1) != cudaSuccess) s = CPIPE_INTERNAL_ERROR;
+                    float ms = 0.0F;
+                    cudaEventElapsedTime(&ms, e0, e1);
+                    if (r > 0) total += ms;  // the first run warms up
+                }
+                if (total < best) {
+                    best = total;
+                    best_k = k;
+                    best_rows = b->rows2;
+                }
             }
         }
         b->per_sm[stage] = best_k;
+        if (stage == 1 && s == CPIPE_OK) {
+            b->rows2 = best_rows;
+            s = batch_prefix(b);
+            if (s == CPIPE_OK)
+                s = cuda_status(cudaMemcpy(b->d_frames, b->frames.data(), sizeof(Frame) * b->n, cudaMemcpyHostToDevice),
+                                "batch descriptors");
+        }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -1476,6 +1618,26 @@ int cpipe_cuda_batch_autotune(cpipe_cuda_batch* b, const void* const* d_raw, voi
 
 cpipe_cuda_chain* cpipe_cuda_batch_frame_chain(cpipe_cuda_batch* b, size_t i) {
     return (b && i < b->chains.size()) ? b->chains[i] : nullptr;
+}
+
+int cpipe_cuda_batch_schedule(cpipe_cuda_batch* b, int per_sm[3], int* rows_per_item) {
+    if (!b) return CPIPE_BAD_INDEX;
+    if (per_sm)
+        for (int i = 0; i < 3; ++i) per_sm[i] = b->per_sm[i];
+    if (rows_per_item) *rows_per_item = b->rows2;
+    return CPIPE_OK;
+}
+
+int cpipe_cuda_batch_frame_times(cpipe_cuda_batch* b, void* stream, float* ms, size_t n) {
+    if (!b || !ms || n < (size_t)b->n) return CPIPE_BAD_INDEX;
+    std::vector<unsigned long long> t((size_t)b->n + 1);
+    const cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int s = cuda_status(cudaMemcpyAsync(t.data(), b->d_times, sizeof(unsigned long long) * t.size(),
+                                        cudaMemcpyDeviceToHost, st), "batch times");
+    if (s == CPIPE_OK) s = cuda_status(cudaStreamSynchronize(st), "batch times");
+    if (s != CPIPE_OK) return s;
+    for (int i = 0; i < b->n; ++i) ms[i] = t[i + 1] >= t[0] ? (float)((double)(t[i + 1] - t[0]) * 1e-6) : -1.0F;
+    return CPIPE_OK;
 }
 
 }  // extern "C"

@@ -523,6 +523,9 @@ static void free_acts(SurrogateNet* s) {
 static cudaError_t ensure_acts(SurrogateNet* s, long long px, bool training) {
     const long long need = training ? px : -px;  // training needs every activation and the gradients
     if (s->act_px == need) return cudaSuccess;
+    // inference keeps a larger allocation: the layer buffers are laid out by
+    // the call's pixel count inside it (frames of a batch share one network)
+    if (!training && s->act_px < 0 && -s->act_px >= px) return cudaSuccess;
     free_acts(s);
     const size_t a0 = (size_t)px * 8, hid = (size_t)px * kCh;
     const size_t acts = training ? a0 + 7 * hid : a0 + 2 * hid;
