@@ -14,7 +14,16 @@ constexpr int kDmGW = kDmTW + 2, kDmGH = kDmTH + 2;
 
 struct DmTap {
     const float* base;
-    __device__ __forceinline__ float operator()(int dx, int dy) const { return base[dy * kDmIW + dx]; }
+    int pitch;
+    __device__ __forceinline__ float operator()(int dx, int dy) const { return base[dy * pitch + dx]; }
+};
+
+// Staged halo: RCD / AMaZE read green / chroma at +-1 whose stencils reach
+// +-2 (halo 3); bilinear reads +-1 only (halo 1, a smaller tile to load).
+template <int ALGO>
+struct DmGeom {
+    static constexpr int kHalo = ALGO == 0 ? 1 : kDmHalo;
+    static constexpr int kIW = kDmTW + 2 * kHalo, kIH = kDmTH + 2 * kHalo;
 };
 
 // Tile of kDmTW x kDmTH outputs; shared memory holds the loaded input with a
@@ -26,29 +35,30 @@ struct DmTap {
 template <int ALGO, class TOut, class Loader>
 __device__ __forceinline__ void demosaic_tile_at(const Loader& load, int w, int h, const Img& out, const Cfa& cfa, int x0,
                                                  int y0) {
-    __shared__ float s_in[kDmIH * kDmIW];
-    __shared__ float s_g[kDmGH * kDmGW];
-    __shared__ float s_q[kDmGH * kDmGW];
+    constexpr int HL = DmGeom<ALGO>::kHalo, IW = DmGeom<ALGO>::kIW, IH = DmGeom<ALGO>::kIH;
+    __shared__ float s_in[IH * IW];
+    __shared__ float s_g[ALGO != 0 ? kDmGH * kDmGW : 1];
+    __shared__ float s_q[ALGO != 0 ? kDmGH * kDmGW : 1];
     // Every caller launches kDmThreads threads per block; a thread's tile loads
     // are all issued before its first shared-memory store.
-    constexpr int kLoads = (kDmIH * kDmIW + kDmThreads - 1) / kDmThreads;
+    constexpr int kLoads = (IH * IW + kDmThreads - 1) / kDmThreads;
     float v[kLoads];
 #pragma unroll
     for (int k = 0; k < kLoads; ++k) {
         const int i = threadIdx.x + kDmThreads * k;
-        const int ty = i / kDmIW, tx = i - ty * kDmIW;
-        if (i < kDmIH * kDmIW) v[k] = load(clampi(x0 - kDmHalo + tx, 0, w - 1), clampi(y0 - kDmHalo + ty, 0, h - 1));
+        const int ty = i / IW, tx = i - ty * IW;
+        if (i < IH * IW) v[k] = load(clampi(x0 - HL + tx, 0, w - 1), clampi(y0 - HL + ty, 0, h - 1));
     }
 #pragma unroll
     for (int k = 0; k < kLoads; ++k) {
         const int i = threadIdx.x + kDmThreads * k;
-        if (i < kDmIH * kDmIW) s_in[i] = v[k];
+        if (i < IH * IW) s_in[i] = v[k];
     }
     __syncthreads();
     if (ALGO != 0) {
         for (int i = threadIdx.x; i < kDmGH * kDmGW; i += blockDim.x) {
             const int ty = i / kDmGW, tx = i - ty * kDmGW;
-            const DmTap T{s_in + (ty + kDmHalo - 1) * kDmIW + (tx + kDmHalo - 1)};
+            const DmTap T{s_in + (ty + HL - 1) * IW + (tx + HL - 1), IW};
             const float g = ALGO == 1 ? rcd_green(T, x0 - 1 + tx, y0 - 1 + ty, cfa)
                                       : amaze_green(T, x0 - 1 + tx, y0 - 1 + ty, cfa);
             s_g[i] = g;
@@ -60,8 +70,8 @@ __device__ __forceinline__ void demosaic_tile_at(const Loader& load, int w, int 
         const int ty = i / kDmTW, tx = i - ty * kDmTW;
         const int x = x0 + tx, y = y0 + ty;
         if (x >= out.w || y >= out.h) continue;
-        const float* c = s_in + (ty + kDmHalo) * kDmIW + (tx + kDmHalo);
-        const DmTap T{c};
+        const float* c = s_in + (ty + HL) * IW + (tx + HL);
+        const DmTap T{c, IW};
         const float ctr = c[0];
         const int site = cfa.at(x, y);
         const bool red = site == 0, blue = site == 2;
