@@ -272,6 +272,70 @@ __global__ void __launch_bounds__(kAtThreads) atrous_v_kernel(const float* __res
     }
 }
 
+// One level in one pass per 64x32 tile for taps up to 16 apart: the tile's
+// rows [y0 - 2s, y0 + 32 + 2s) of c_j over columns [x0 - 2s, x0 + 64 + 2s)
+// (clamped) staged in shared memory, the horizontal B3 pass of those rows into
+// shared memory, then the vertical pass, c_{j+1}, w_{j+1} and the tile's sum of
+// w^2 per channel -- the same operands, taps and pixel-to-thread mapping as the
+// two-pass form above, so the same floats, without the frame-wide scratch
+// planes of the horizontal pass.
+constexpr int kAtFuseMaxStep = 16;
+size_t atrous_level_smem(int s) {
+    return ((size_t)(kAtTH + 4 * s) * (kAtTW + 4 * s) + (size_t)(kAtTH + 4 * s) * kAtTW) * sizeof(float);
+}
+__global__ void __launch_bounds__(kAtThreads) atrous_level_kernel(const float* __restrict__ cin, float* __restrict__ cout,
+                                                                  float* __restrict__ wout, float* __restrict__ part,
+                                                                  int w, int h, long long npx, int s) {
+    extern __shared__ float sm[];
+    const int x0 = blockIdx.x * kAtTW, y0 = blockIdx.y * kAtTH;
+    const int SR = kAtTH + 4 * s, SC = kAtTW + 4 * s;
+    float* st = sm;            // staged c_j: SR x SC
+    float* hp = sm + SR * SC;  // horizontal pass: SR x kAtTW
+    float acc[3] = {0.0F, 0.0F, 0.0F};
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const float* src = cin + c * npx;
+        __syncthreads();
+        for (int i = threadIdx.x; i < SR * SC; i += kAtThreads) {
+            const int r = i / SC, q = i - r * SC;
+            st[i] = __ldg(src + (long long)clampi(y0 - 2 * s + r, 0, h - 1) * w + clampi(x0 - 2 * s + q, 0, w - 1));
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < SR * kAtTW; i += kAtThreads) {
+            const int r = i / kAtTW, tx = i - r * kAtTW;
+            const float* row = st + r * SC + tx + 2 * s;
+            hp[i] = b3(row[-2 * s], row[-s], row[0], row[s], row[2 * s]);
+        }
+        __syncthreads();
+        for (int i = threadIdx.x; i < kAtTH * kAtTW; i += kAtThreads) {
+            const int r = i / kAtTW, xx = i - r * kAtTW;
+            const int x = x0 + xx, y = y0 + r;
+            if (x >= w || y >= h) continue;
+            const float* col = hp + (r + 2 * s) * kAtTW + xx;
+            const float v = b3(col[-2 * s * kAtTW], col[-s * kAtTW], col[0], col[s * kAtTW], col[2 * s * kAtTW]);
+            const long long o = c * npx + (long long)y * w + x;
+            const float d = st[(r + 2 * s) * SC + xx + 2 * s] - v;
+            cout[o] = v;
+            wout[o] = d;
+            acc[c] += d * d;
+        }
+    }
+    __shared__ float red[kAtThreads / 32][3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        float a = acc[c];
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) a += __shfl_xor_sync(0xFFFFFFFFU, a, off);
+        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5][c] = a;
+    }
+    __syncthreads();
+    if (threadIdx.x < 3) {
+        float a = 0.0F;
+        for (int k = 0; k < kAtThreads / 32; ++k) a += red[k][threadIdx.x];
+        part[(size_t)(blockIdx.y * gridDim.x + blockIdx.x) * 3 + threadIdx.x] = a;
+    }
+}
+
 struct AtrousThrArgs {
     float noise[kAtrousMaxLevels][3];
     float strength[3];
@@ -434,7 +498,10 @@ int atrous_plan(const cpipe_AtrousWaveletParams* p, int w, int h, AtrousPlan* ou
     return CPIPE_OK;
 }
 
-cudaError_t atrous_setup() { return cudaSuccess; }  // the two-pass level kernels use no dynamic shared memory
+cudaError_t atrous_setup() {
+    return cudaFuncSetAttribute(atrous_level_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)atrous_level_smem(kAtFuseMaxStep));
+}
 
 cudaError_t atrous_run(const AtrousPlan& p, const Img& in, const Img& out, bool f16, void* scratch, cudaStream_t st) {
     if (p.copy) {
@@ -458,6 +525,11 @@ cudaError_t atrous_run(const AtrousPlan& p, const Img& in, const Img& out, bool 
         const int s = 1 << j;
         const dim3 lg((unsigned)p.gx, (unsigned)p.gy);
         tl.nb[j] = (int)(lg.x * lg.y);
+        if (s <= kAtFuseMaxStep) {
+            atrous_level_kernel<<<lg, kAtThreads, atrous_level_smem(s), st>>>(
+                c[j & 1], c[(j + 1) & 1], wv + (size_t)j * 3 * npx, part + (size_t)j * tl.stride, p.w, p.h, npx, s);
+            continue;
+        }
         const dim3 hg((unsigned)((p.w + kAtThreads - 1) / kAtThreads), (unsigned)p.h, 3);
         atrous_h_kernel<<<hg, kAtThreads, 0, st>>>(c[j & 1], tmp, p.w, npx, s);
         atrous_v_kernel<<<lg, kAtThreads, 0, st>>>(c[j & 1], tmp, c[(j + 1) & 1], wv + (size_t)j * 3 * npx,
