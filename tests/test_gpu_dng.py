@@ -131,7 +131,11 @@ def test_error_statuses():
     data = build_dng()
     rc, _, host = decode(data, out_elems=11)  # one sample short
     assert rc == _abi.BAD_INDEX and (host == 0xBEEF).all()
+    # Compression 7 whose strip is not a lossless JPEG stream: the decode fails
     rc, _, _ = decode(build_dng(overrides={259: (SHORT, [7])}))
+    assert rc == _abi.FAILED and L.cpipe_cuda_last_error()
+    # any other compression (8 = Deflate) is left to the caller
+    rc, _, _ = decode(build_dng(overrides={259: (SHORT, [8])}))
     assert rc == _abi.UNSUPPORTED and b"lossless JPEG" in L.cpipe_cuda_last_error()
     rc, _, _ = decode(build_dng(strip_byte_count=10 ** 6))  # strip past the end of the file
     assert rc == _abi.FAILED
