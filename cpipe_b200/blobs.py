@@ -56,10 +56,12 @@ def bm3d_spec(sigma, lambda3d=2.7, tau_match1=2500.0, tau_match2=400.0, n2=16, n
               kaiser_beta=2.0, stages=2, transform="tensor"):
     """Two-stage BM3D parameters; defaults are the published values (8x8 blocks,
     16-block groups, 39x39 search, step 3, hard threshold then Wiener).
-    transform: "tensor" (FP16 hi/lo split on the tensor cores) or "fp32"."""
+    transform: "tensor" (FP16 hi/lo split on the tensor cores), "fp32", or
+    "tensor_fp16" (single FP16 products on the tensor cores: the screening
+    form the surrogate's spot check runs)."""
     return raw(A.Bm3dSpecParams(float(sigma), float(lambda3d), float(tau_match1), float(tau_match2), int(n2),
                                 int(ns), int(nstep), float(kaiser_beta), int(stages),
-                                {"tensor": 0, "fp32": 1}[transform]))
+                                {"tensor": 0, "fp32": 1, "tensor_fp16": 2}[transform]))
 
 
 def guided(radius, eps):

@@ -6,7 +6,7 @@ device; the filter runs in place on the library's stream and is timed with
 CUDA events over `reps` calls after three untimed ones.
 
     python -m cpipe_b200.bm3d [--width 4032] [--height 3024] [--stages 2]
-                              [--transform tensor|fp32] [--sigma 0.032] [--reps 5]
+                              [--transform tensor|fp32|tensor_fp16] [--sigma 0.032] [--reps 5]
 """
 import argparse
 import ctypes as C
@@ -63,7 +63,7 @@ def _main():
     ap.add_argument("--width", type=int, default=4032)
     ap.add_argument("--height", type=int, default=3024)
     ap.add_argument("--stages", type=int, default=2)
-    ap.add_argument("--transform", default="tensor", choices=("tensor", "fp32"))
+    ap.add_argument("--transform", default="tensor", choices=("tensor", "fp32", "tensor_fp16"))
     ap.add_argument("--sigma", type=float, default=0.032)
     ap.add_argument("--reps", type=int, default=5)
     a = ap.parse_args()

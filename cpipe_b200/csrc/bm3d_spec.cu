@@ -504,6 +504,33 @@ __device__ __forceinline__ void mma_split_t(float (&c)[4], const float (&r)[4], 
     mma1688(c, h0, h1, bl);
 }
 
+// Single FP16 products (transform 2, the screening form): A rounded once to
+// FP16, B = the DCT matrix's FP16 part, FP32 accumulation -- about 2^-11
+// relative per product instead of the split form's FP32-level accuracy.
+__device__ __forceinline__ uint32_t pack2(float x0, float x1) {
+    const __half2 h = __floats2half2_rn(x0, x1);
+    return *reinterpret_cast<const uint32_t*>(&h);
+}
+template <bool SPLIT>
+__device__ __forceinline__ void mma_prod(float (&c)[4], float a00, float a01, float a10, float a11, uint32_t bh,
+                                         uint32_t bl) {
+    if (SPLIT) {
+        mma_split(c, a00, a01, a10, a11, bh, bl);
+    } else {
+        c[0] = c[1] = c[2] = c[3] = 0.0F;
+        mma1688(c, pack2(a00, a01), pack2(a10, a11), bh);
+    }
+}
+template <bool SPLIT>
+__device__ __forceinline__ void mma_prod_t(float (&c)[4], const float (&r)[4], uint32_t bh, uint32_t bl) {
+    if (SPLIT) {
+        mma_split_t(c, r, bh, bl);
+    } else {
+        c[0] = c[1] = c[2] = c[3] = 0.0F;
+        mma1688(c, movtrans(pack2(r[0], r[1])), movtrans(pack2(r[2], r[3])), bh);
+    }
+}
+
 struct DctFrags {
     uint32_t fh, fl;  // B[k][n] = C[n][k] (k = 2q, 2q+1; n = g): products with C^T
     uint32_t ih, il;  // B[k][n] = C[k][n]: products with C
@@ -554,6 +581,7 @@ __device__ __forceinline__ float exp2i(int e) { return __int_as_float((127 + e) 
 // Forward 2D DCT and Haar of one group of N blocks read from `img` (row pitch P;
 // off[b]: block b's offset in the footprint plane).  H[t][e]: block 2t (e < 2) or 2t + 1 (e >= 2),
 // coefficient (v = g, u = 2q + (e & 1)).
+template <bool SPLIT>
 __device__ __forceinline__ void tc_forward(const float* img, int P, const int* off, int N, const DctFrags& d,
                                            float (&H)[8][4]) {
     const int lane = threadIdx.x & 31, g = lane >> 2, q = lane & 3;
@@ -570,8 +598,8 @@ __device__ __forceinline__ void tc_forward(const float* img, int P, const int* o
                 v[hh][1] = src[P];
             }
         float rc[4];
-        mma_split(rc, v[0][0], v[0][1], v[1][0], v[1][1], d.fh, d.fl);  // rows (block, x = g), columns v
-        mma_split_t(H[t], rc, d.fh, d.fl);                             // rows (block, v = g), columns u
+        mma_prod<SPLIT>(rc, v[0][0], v[0][1], v[1][0], v[1][1], d.fh, d.fl);  // rows (block, x = g), columns v
+        mma_prod_t<SPLIT>(H[t], rc, d.fh, d.fl);                             // rows (block, v = g), columns u
     }
     if (N > 1) haar_level<1>(H);
     if (N > 2) haar_level<2>(H);
@@ -580,6 +608,7 @@ __device__ __forceinline__ void tc_forward(const float* img, int P, const int* o
 }
 
 // Inverse Haar and 2D DCT: X[t][e] = block 2t (e < 2) or 2t + 1, pixel (x = g, y = 2q + (e & 1)).
+template <bool SPLIT>
 __device__ __forceinline__ void tc_inverse(float (&H)[8][4], int N, const DctFrags& d, float (&X)[8][4]) {
     if (N > 8) haar_level<8>(H);
     if (N > 4) haar_level<4>(H);
@@ -590,8 +619,8 @@ __device__ __forceinline__ void tc_inverse(float (&H)[8][4], int N, const DctFra
         X[t][0] = X[t][1] = X[t][2] = X[t][3] = 0.0F;
         if (2 * t >= N) continue;
         float rr[4];
-        mma_split(rr, H[t][0], H[t][1], H[t][2], H[t][3], d.ih, d.il);  // rows (block, v = g), columns x
-        mma_split_t(X[t], rr, d.ih, d.il);                             // rows (block, x = g), columns y
+        mma_prod<SPLIT>(rr, H[t][0], H[t][1], H[t][2], H[t][3], d.ih, d.il);  // rows (block, v = g), columns x
+        mma_prod_t<SPLIT>(X[t], rr, d.ih, d.il);                             // rows (block, x = g), columns y
     }
 }
 
@@ -623,7 +652,7 @@ __host__ __device__ constexpr int tc_stage_blocks(int stage) { return stage == 2
 //                weights are added at the block origins (a weight map, one
 //                atomic per block), and the separable Kaiser window is applied
 //                to that map at the flush.
-template <int STAGE>
+template <int STAGE, bool SPLIT>
 __global__ void __launch_bounds__(32 * kTcWarps, 3) bm3d_filter_tc_kernel(FilterArgs a) {
     constexpr int SB = tc_stage_blocks(STAGE);
     extern __shared__ __align__(16) float sm[];
@@ -694,7 +723,7 @@ __global__ void __launch_bounds__(32 * kTcWarps, 3) bm3d_filter_tc_kernel(Filter
         }
         __syncwarp();
         float H[8][4];
-        tc_forward(s_img, P, woff, N, dct, H);
+        tc_forward<SPLIT>(s_img, P, woff, N, dct, H);
         const int L = 31 - __clz(N);
         float wgt;
         if (STAGE == 1) {
@@ -716,7 +745,7 @@ __global__ void __launch_bounds__(32 * kTcWarps, 3) bm3d_filter_tc_kernel(Filter
             wgt = kept > 0U ? 1.0F / (float)kept : a.sigma2;
         } else {
             float B[8][4];
-            tc_forward(s_bas, P, woff, N, dct, B);
+            tc_forward<SPLIT>(s_bas, P, woff, N, dct, B);
             const float s0 = a.sigma2 * exp2i(L), sc0 = exp2i(-L);
             float sw2 = 0.0F;
 #pragma unroll
@@ -737,7 +766,7 @@ __global__ void __launch_bounds__(32 * kTcWarps, 3) bm3d_filter_tc_kernel(Filter
         }
         if (lane == 0) s_wgt[k] = wgt;
         float X[8][4];
-        tc_inverse(H, N, dct, X);
+        tc_inverse<SPLIT>(H, N, dct, X);
         // numerator: X -> staging [block][x][y], SB blocks per round -> one block's
         // 8x4 half per atomic instruction
         const float kw0 = wgt * kq0, kw1 = wgt * kq1;
@@ -894,7 +923,7 @@ int bm3d_plan(const cpipe_Bm3dSpecParams* p, int w, int h, Bm3dPlan* out, int ba
     if (!(p->tau_match2 >= 0.0F && p->tau_match2 <= 16000.0F)) return CPIPE_BAD_INDEX;
     if (p->stages != 1 && p->stages != 2) return CPIPE_BAD_INDEX;
     if (!(p->lambda3d >= 0.0F) || !(p->kaiser_beta >= 0.0F)) return CPIPE_BAD_INDEX;
-    if (p->transform != 0 && p->transform != 1) return CPIPE_BAD_INDEX;
+    if (p->transform < 0 || p->transform > 2) return CPIPE_BAD_INDEX;
     if (w <= 0 || h <= 0 || batch < 1 || w > 65535 || (long long)h * batch > 65535) return CPIPE_BAD_INDEX;
     Bm3dPlan& q = *out;
     q = Bm3dPlan{};
@@ -906,7 +935,8 @@ int bm3d_plan(const cpipe_Bm3dSpecParams* p, int w, int h, Bm3dPlan* out, int ba
     q.n2 = n2;
     q.nstep = p->nstep;
     q.stages = p->stages;
-    q.tensor = p->transform == 0;
+    q.tensor = p->transform != 1;
+    q.split = p->transform == 0;
     q.sigma = p->sigma;
     q.sigma2 = p->sigma * p->sigma;
     q.thr = p->lambda3d * p->sigma;
@@ -965,10 +995,10 @@ cudaError_t bm3d_setup(const Bm3dPlan& p) {
     if (p.tensor) {
         const size_t t1 = filter_tc_smem(p, 1), t2 = filter_tc_smem(p, 2);
         if (t2 > kSmemOptIn) return cudaErrorInvalidConfiguration;
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(bm3d_filter_tc_kernel<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t1);
-        if (e == cudaSuccess)
-            e = cudaFuncSetAttribute(bm3d_filter_tc_kernel<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t2);
+        const void* k1 = p.split ? (const void*)bm3d_filter_tc_kernel<1, true> : (const void*)bm3d_filter_tc_kernel<1, false>;
+        const void* k2 = p.split ? (const void*)bm3d_filter_tc_kernel<2, true> : (const void*)bm3d_filter_tc_kernel<2, false>;
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k1, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t1);
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(k2, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)t2);
     }
     return e;
 }
@@ -1034,8 +1064,13 @@ cudaError_t bm3d_run(const Bm3dPlan& p, const Img& in, const Img& out, bool f16,
         if (p.mwpr == kMatchWprStd) bm3d_match_kernel<kMatchWprStd><<<mgrid, kMatchTile * kMatchTile, ms, st>>>(ma);
         else bm3d_match_kernel<0><<<mgrid, kMatchTile * kMatchTile, ms, st>>>(ma);
         if (p.tensor) {
-            if (stage == 1) bm3d_filter_tc_kernel<1><<<tgrid, 32 * kTcWarps, ts1, st>>>(ta);
-            else bm3d_filter_tc_kernel<2><<<tgrid, 32 * kTcWarps, ts2, st>>>(ta);
+            if (p.split) {
+                if (stage == 1) bm3d_filter_tc_kernel<1, true><<<tgrid, 32 * kTcWarps, ts1, st>>>(ta);
+                else bm3d_filter_tc_kernel<2, true><<<tgrid, 32 * kTcWarps, ts2, st>>>(ta);
+            } else {
+                if (stage == 1) bm3d_filter_tc_kernel<1, false><<<tgrid, 32 * kTcWarps, ts1, st>>>(ta);
+                else bm3d_filter_tc_kernel<2, false><<<tgrid, 32 * kTcWarps, ts2, st>>>(ta);
+            }
         } else {
             for (int py = 0; py < p.phases; ++py)
                 for (int pxh = 0; pxh < p.phases; ++pxh) {

@@ -25,7 +25,8 @@ struct Bm3dPlan {
     int ntx = 0, nty = 0;  // filter tiles (8x8 reference blocks each)
     int mwin = 0, mwpr = 0;  // match tile region edge bound, words per smem row
     bool copy = false;       // image below 8x8 or sigma <= 0: output = input
-    bool tensor = true;      // transforms on the tensor cores (FP16 hi/lo split) or FP32 CUDA cores
+    bool tensor = true;      // transforms on the tensor cores or FP32 CUDA cores
+    bool split = true;       // tensor cores: FP16 hi/lo split products (else single FP16 products)
     size_t off_yuv = 0, off_basic = 0, off_acc = 0, off_q = 0, off_list = 0, off_cnt = 0, bytes = 0;
 };
 

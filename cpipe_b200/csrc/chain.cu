@@ -805,7 +805,12 @@ static cpipe_cuda_chain* chain_create(const cpipe_cuda_chain_config* cfg, int* s
             cpipe_Bm3dSpecParams sp = cfg->bm3d_spec;
             if (!(sp.sigma > 0.0F)) sp.sigma = cfg->bm3d_sigma;
             if ((st = bm3d_plan(&sp, w, h, &c->bm3d)) != CPIPE_OK) return fail(st, c);
-            if ((st = bm3d_plan(&sp, E, E, &c->tile_plan, c->spot_tiles)) != CPIPE_OK) return fail(st, c);
+            // the check screens the network's output against BM3D with single FP16
+            // transform products (2^-11 relative each, far below the decision
+            // margin); the fallback keeps the configured form
+            cpipe_Bm3dSpecParams spot_sp = sp;
+            if (spot_sp.transform == 0) spot_sp.transform = 2;
+            if ((st = bm3d_plan(&spot_sp, E, E, &c->tile_plan, c->spot_tiles)) != CPIPE_OK) return fail(st, c);
             const size_t tile_bytes = (size_t)E * E * c->spot_tiles * 4 * (c->f16 ? 2 : 4);
             if (cudaMalloc(&c->d_tile_in, tile_bytes) != cudaSuccess || cudaMalloc(&c->d_tile_ref, tile_bytes) != cudaSuccess ||
                 (!c->tile_plan.copy && cudaMalloc(&c->d_tile_scratch, c->tile_plan.bytes) != cudaSuccess) ||

@@ -27,19 +27,18 @@
 //          alpha copied.
 //
 // Kernels
-//   gsp_ab / gsp_out     the guided filter as two column-strip kernels with
-//                        running binary32 box sums (see below).
-//   atrous_prep_kernel   RGBA -> Y, Co, Cg planes (FP32).
-//   atrous_h_kernel      one level's horizontal B3 pass of all three planes
-//                        into a scratch plane set (taps 2^j apart, clamped).
-//   atrous_v_kernel      per 64x32 tile: the vertical pass from the scratch
-//                        planes, c_{j+1} and w_{j+1}, the tile's sum of w^2
-//                        per channel (no halo staging: the taps come through
-//                        L1 / L2).
+//   gsp_ab / gsp_out     the guided filter as two tile kernels with sliding
+//                        binary32 box sums along rows and columns (see below).
+//   atrous_level_kernel  per 256x8 tile, one level: the vertical B3 taps of
+//                        all three channels through L1 / L2 into shared
+//                        memory, the horizontal taps from there, c_{j+1}
+//                        written, the tile's sum of w_{j+1}^2 per channel; the
+//                        first level reads c_0 (Y, Co, Cg) from the input frame.
 //   atrous_thresh_kernel per (level, channel): the tiles' sums added in a fixed
 //                        order (compensated binary32), the BayesShrink
 //                        threshold.
-//   atrous_recon_kernel  shrink, sum, inverse colour transform.
+//   atrous_recon_kernel  c_0 from the input, the bands c_j - c_{j+1} from the
+//                        stored levels, shrink, sum, inverse colour transform.
 #include "spec_denoise.h"
 
 #include <math.h>
@@ -56,20 +55,29 @@ namespace cpb {
 namespace {
 
 // ------------------------------------------------------------------ guided
-// Two kernels over column strips, per RGB channel, in binary32:
-//   ab    a thread per column xa of the extended domain [-R, w+R) walks a
-//         segment of kGsSeg rows ya: the horizontal sums of v and v^2 of the
-//         clamped image row entering the vertical box (staged in shared
-//         memory) are added to running column sums, a and b are written, and
-//         the sums of the row leaving the box are subtracted;
-//   out   a thread per output column walks kGsSeg rows the same way over the
-//         a and b planes of all three channels (horizontal sums of the entering
-//         and leaving rows), out = max(mean_a v + mean_b, 0), alpha copied.
-// Each segment starts its running sums afresh (2R rows of warm-up), so no sum
-// runs over more than kGsSeg + 2R rows.  Binary16 values square exactly in
-// binary32; against the FP64 definition the results are within one binary16
-// ulp (binary16 frames) or 1e-5 (binary32 frames).
-constexpr int kGsThreads = 128, kGsSeg = 64;
+// Two tile kernels in binary32 with sliding box sums along both axes; the
+// paired sums (sum v, sum v^2) and (sum a, sum b) run as sm_100 packed adds.
+//   ab   per channel (grid z), a 64x32 tile of the extended domain
+//        [-R, w+R) x [-R, h+R): the clamped image tile with its 2R halo staged
+//        in shared memory; row sums of (v, v^2) over 2R+1 columns (one sliding
+//        window per 16 outputs, restarted at each window); column sums of
+//        those over 2R+1 rows (one window per 8 outputs); m = S/N, corr = Q/N
+//        (products with the binary32 reciprocal of N), var = max(corr - m^2, 0),
+//        a = var/(var+eps) (__fdividef: within 2 ulp), b = m - a m into the a
+//        and b planes (extended domain, row pitch w + 2R).
+//   out  per 64x32 output tile, the three channels in turn: the (a, b) pairs
+//        with their 2R halo staged and box-summed the same way; per pixel
+//        out = max(mean_a v + mean_b, 0) (means as products with 1/N) held in
+//        registers, then written with the input's alpha.
+// Each running sum adds at most 2R+1 + 2 * 15 terms, so binary16 frames stay
+// within one binary16 ulp of the FP64 definition and binary32 frames within
+// 1e-5.  Shared-memory pitches are odd (in elements of the stored type), so
+// the lanes of a warp (rows in the row pass, columns in the column pass) hit
+// distinct banks.
+constexpr int kGsTW = 64, kGsTH = 32, kGsRunX = 16, kGsRunY = 8, kGsThreads = 256;
+static_assert(kGsTW * (kGsTH / kGsRunY) == kGsThreads, "one column window per thread");
+static_assert((kGsTW / kGsRunX) * 64 == kGsThreads && kGsTH + 2 * kGuidedSpecMaxRadius <= 64,
+              "one row window per thread: the staged rows fit 64 lanes");
 struct GsPlanes {
     int w, h, R, Wa, Ha;
     float* a;  // [3][Ha][Wa]
@@ -81,181 +89,182 @@ GsPlanes gs_planes(int w, int h, int R, void* scratch) {
     p.b = p.a + 3 * (size_t)p.Ha * p.Wa;
     return p;
 }
-// block: extended columns [xs, xs + 128) of channel blockIdx.z, extended rows
-// ya in [blockIdx.y * kGsSeg - R, + kGsSeg)
+__host__ __device__ constexpr int gs_pitch(int R) { return (kGsTW + 2 * R) | 1; }  // staged pitch (elements)
+constexpr int kGsPH = kGsTW + 1;                                                  // row-sum pitch (float2)
+// ab: scalar staged tile + float2 row sums; out: float2 staged tile + float2 row sums
+__host__ __device__ constexpr size_t gs_ab_smem(int R) {
+    return (size_t)(kGsTH + 2 * R) * gs_pitch(R) * 4 + (size_t)(kGsTH + 2 * R) * kGsPH * 8;
+}
+__host__ __device__ constexpr size_t gs_out_smem(int R) {
+    return (size_t)(kGsTH + 2 * R) * gs_pitch(R) * 8 + (size_t)(kGsTH + 2 * R) * kGsPH * 8;
+}
+__device__ __forceinline__ float2 neg2(float2 v) { return make_float2(-v.x, -v.y); }
+
 template <class T>
 __global__ void __launch_bounds__(kGsThreads) gsp_ab_kernel(Img in, GsPlanes p, float eps) {
-    __shared__ float s_new[kGsThreads + 2 * kGuidedSpecMaxRadius], s_old[kGsThreads + 2 * kGuidedSpecMaxRadius];
-    const int c = blockIdx.z, xs = blockIdx.x * kGsThreads, t = threadIdx.x, R = p.R, D = 2 * R + 1;
-    const int ya0 = (int)blockIdx.y * kGsSeg - R, ya1 = min(ya0 + kGsSeg, p.h + R);
-    const float N = (float)(D * D);
-    // extended column xi = xs + t is image column xi - R; its box reads image
-    // columns xi - 2R .. xi, staged at s[t .. t + 2R]
-    auto stage = [&](float* buf, int row) {
-        const int y = clampi(row, 0, in.h - 1);
-        for (int i = t; i < kGsThreads + 2 * R; i += kGsThreads)
-            buf[i] = (float)px<const T>(in, clampi(xs - 2 * R + i, 0, in.w - 1), y)[c];
-    };
-    auto hsum = [&](const float* buf, float& h1, float& h2) {
-        h1 = 0.0F;
-        h2 = 0.0F;
-        for (int k = 0; k < D; ++k) {
-            const float v = buf[t + k];
-            h1 = h1 + v;
-            h2 = h2 + v * v;
-        }
-    };
-    float s1 = 0.0F, s2 = 0.0F, h1, h2;
-    for (int r = ya0 - R; r < ya0 + R; ++r) {
-        stage(s_new, r);
-        __syncthreads();
-        hsum(s_new, h1, h2);
-        s1 = s1 + h1;
-        s2 = s2 + h2;
-        __syncthreads();
+    extern __shared__ float4 gsm4[];
+    float* gsm = reinterpret_cast<float*>(gsm4);
+    const int R = p.R, D = 2 * R + 1, SR = kGsTH + 2 * R, SC = kGsTW + 2 * R, PV = gs_pitch(R);
+    float* sv = gsm;
+    float2* hs = reinterpret_cast<float2*>(gsm + ((SR * PV + 1) & ~1));
+    const int c = blockIdx.z, X0 = blockIdx.x * kGsTW, Y0 = blockIdx.y * kGsTH;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    // plane column X0 + q's box starts at image column X0 - 2R + q
+    for (int r = warp; r < SR; r += kGsThreads / 32) {
+        const T* row = px<const T>(in, 0, clampi(Y0 - 2 * R + r, 0, in.h - 1)) + c;
+        float* dst = sv + r * PV;
+#pragma unroll 3
+        for (int q = lane; q < SC; q += 32) dst[q] = (float)row[4 * clampi(X0 - 2 * R + q, 0, in.w - 1)];
     }
-    const int xi = xs + t;
-    for (int ya = ya0; ya < ya1; ++ya) {
-        stage(s_new, ya + R);
-        stage(s_old, ya - R);
-        __syncthreads();
-        hsum(s_new, h1, h2);
-        s1 = s1 + h1;
-        s2 = s2 + h2;
-        const float m = s1 / N, corr = s2 / N;
-        const float var = maxf(corr - m * m, 0.0F);
-        const float a = var / (var + eps);
-        if (xi < p.Wa) {
-            const size_t o = ((size_t)c * p.Ha + (ya + R)) * p.Wa + xi;
-            p.a[o] = a;
-            p.b[o] = m - a * m;
+    __syncthreads();
+    // row pass: one window per thread, rows on the lanes (SR <= 64 rows)
+    {
+        const int r = threadIdx.x & 63, x0 = (threadIdx.x >> 6) * kGsRunX;
+        if (r < SR) {
+        const float* row = sv + r * PV + x0;
+        float2 s = make_float2(0.0F, 0.0F);
+#pragma unroll 4
+        for (int k = 0; k < D; ++k) {
+            const float v = row[k];
+            s = __fadd2_rn(s, make_float2(v, v * v));
         }
-        hsum(s_old, h1, h2);
-        s1 = s1 - h1;
-        s2 = s2 - h2;
-        __syncthreads();
+        float2* o = hs + r * kGsPH + x0;
+        o[0] = s;
+#pragma unroll
+        for (int x = 1; x < kGsRunX; ++x) {
+            const float vi = row[x + D - 1], vo = row[x - 1];
+            s = __fadd2_rn(__fadd2_rn(s, make_float2(vi, vi * vi)), make_float2(-vo, -(vo * vo)));
+            o[x] = s;
+        }
+        }
+    }
+    __syncthreads();
+    const float invN = 1.0F / (float)(D * D);
+    const int x = threadIdx.x % kGsTW, y0 = (threadIdx.x / kGsTW) * kGsRunY;
+    const int xa = X0 + x;
+    float2 S = make_float2(0.0F, 0.0F);
+#pragma unroll 4
+    for (int k = 0; k < D; ++k) S = __fadd2_rn(S, hs[(y0 + k) * kGsPH + x]);
+    const size_t plane = (size_t)p.Ha * p.Wa;
+    // plane offsets fit 32 bits (Ha * Wa < 2^31 is checked on the host)
+    float* pa = p.a + (size_t)c * plane + (unsigned)((Y0 + y0) * p.Wa + xa);
+    float* pb = p.b + (size_t)c * plane + (unsigned)((Y0 + y0) * p.Wa + xa);
+    const float2* hin = hs + (y0 + D) * kGsPH + x;
+    const float2* hout = hs + y0 * kGsPH + x;
+    const int nrow = min(kGsRunY, p.Ha - (Y0 + y0));
+    const bool col = xa < p.Wa;
+#pragma unroll
+    for (int y = 0; y < kGsRunY; ++y) {
+        if (y > 0) S = __fadd2_rn(__fadd2_rn(S, hin[(y - 1) * kGsPH]), neg2(hout[(y - 1) * kGsPH]));
+        if (col && y < nrow) {
+            const float2 mc = __fmul2_rn(S, make_float2(invN, invN));  // (m, corr)
+            const float var = maxf(mc.y - mc.x * mc.x, 0.0F);
+            const float a = __fdividef(var, var + eps);
+            pa[y * p.Wa] = a;
+            pb[y * p.Wa] = mc.x - a * mc.x;
+        }
     }
 }
-// block: output columns [xs, xs + 128), rows [blockIdx.y * kGsSeg, + kGsSeg)
+
 template <class T>
 __global__ void __launch_bounds__(kGsThreads) gsp_out_kernel(Img in, Img out, GsPlanes p) {
-    constexpr int kS = kGsThreads + 2 * kGuidedSpecMaxRadius;
-    __shared__ float s_new[6][kS], s_old[6][kS];
-    const int xs = blockIdx.x * kGsThreads, t = threadIdx.x, R = p.R, D = 2 * R + 1;
-    const int y0 = (int)blockIdx.y * kGsSeg, y1 = min(y0 + kGsSeg, p.h);
-    const float N = (float)(D * D);
+    extern __shared__ float4 gsm4[];
+    const int R = p.R, D = 2 * R + 1, SR = kGsTH + 2 * R, SC = kGsTW + 2 * R, PV = gs_pitch(R);
+    float2* sab = reinterpret_cast<float2*>(gsm4);
+    float2* hs = sab + SR * PV;
+    const int X0 = blockIdx.x * kGsTW, Y0 = blockIdx.y * kGsTH;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const float invN = 1.0F / (float)(D * D);
     const size_t plane = (size_t)p.Ha * p.Wa;
-    // output column x reads extended columns x .. x + 2R (image x - R .. x + R)
-    auto stage = [&](float (*buf)[kS], int ya) {
-        const size_t row = (size_t)(ya + R) * p.Wa;
-        for (int i = t; i < kGsThreads + 2 * R; i += kGsThreads) {
-            const size_t xi = row + (size_t)min(xs + i, p.Wa - 1);
+    const int x = threadIdx.x % kGsTW, y0 = (threadIdx.x / kGsTW) * kGsRunY;
+    const int gx = X0 + x;
+    // the thread's eight input pixels (alpha and v), loaded once
+    Rgba vin[kGsRunY];
 #pragma unroll
-            for (int c = 0; c < 3; ++c) {
-                buf[2 * c][i] = p.a[c * plane + xi];
-                buf[2 * c + 1][i] = p.b[c * plane + xi];
-            }
-        }
-    };
-    float sa[3] = {0.0F, 0.0F, 0.0F}, sb[3] = {0.0F, 0.0F, 0.0F};
-    auto add = [&](float (*buf)[kS], float sign) {
-#pragma unroll
-        for (int c = 0; c < 3; ++c) {
-            float ha = 0.0F, hb = 0.0F;
-            for (int k = 0; k < D; ++k) {
-                ha = ha + buf[2 * c][t + k];
-                hb = hb + buf[2 * c + 1][t + k];
-            }
-            if (sign > 0.0F) {
-                sa[c] = sa[c] + ha;
-                sb[c] = sb[c] + hb;
-            } else {
-                sa[c] = sa[c] - ha;
-                sb[c] = sb[c] - hb;
-            }
-        }
-    };
-    for (int ya = y0 - R; ya < y0 + R; ++ya) {
-        stage(s_new, ya);
-        __syncthreads();
-        add(s_new, 1.0F);
-        __syncthreads();
+    for (int y = 0; y < kGsRunY; ++y) {
+        const int gy = Y0 + y0 + y;
+        vin[y] = (gx < p.w && gy < p.h) ? load_rgba(px<const T>(in, gx, gy)) : Rgba{0.0F, 0.0F, 0.0F, 0.0F};
     }
-    const int x = xs + t;
-    for (int y = y0; y < y1; ++y) {
-        stage(s_new, y + R);
-        stage(s_old, y - R);
-        __syncthreads();
-        add(s_new, 1.0F);
-        if (x < p.w) {
-            const T* src = px<const T>(in, x, y);
-            const Rgba v = load_rgba(src);
-            store_rgb_keep_alpha(px<T>(out, x, y),
-                                 Rgba{max0((sa[0] / N) * v.r + sb[0] / N), max0((sa[1] / N) * v.g + sb[1] / N),
-                                      max0((sa[2] / N) * v.b + sb[2] / N), 0.0F},
-                                 src);
+    float res[3][kGsRunY];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        // output x reads plane columns x .. x + 2R (extended x - R .. x + R)
+        const float* ca = p.a + (size_t)c * plane;
+        const float* cb = p.b + (size_t)c * plane;
+        for (int r = warp; r < SR; r += kGsThreads / 32) {
+            const unsigned ro = (unsigned)min(Y0 + r, p.Ha - 1) * (unsigned)p.Wa;
+            const float* ra = ca + ro;
+            const float* rb = cb + ro;
+            float2* dst = sab + r * PV;
+#pragma unroll 3
+            for (int q = lane; q < SC; q += 32) {
+                const int xq = min(X0 + q, p.Wa - 1);
+                dst[q] = make_float2(__ldg(ra + xq), __ldg(rb + xq));
+            }
         }
-        add(s_old, -1.0F);
         __syncthreads();
+        {
+            const int r = threadIdx.x & 63, x0 = (threadIdx.x >> 6) * kGsRunX;
+            if (r < SR) {
+            const float2* row = sab + r * PV + x0;
+            float2 s = make_float2(0.0F, 0.0F);
+#pragma unroll 4
+            for (int k = 0; k < D; ++k) s = __fadd2_rn(s, row[k]);
+            float2* o = hs + r * kGsPH + x0;
+            o[0] = s;
+#pragma unroll
+            for (int xx = 1; xx < kGsRunX; ++xx) {
+                s = __fadd2_rn(__fadd2_rn(s, row[xx + D - 1]), neg2(row[xx - 1]));
+                o[xx] = s;
+            }
+            }
+        }
+        __syncthreads();
+        float2 S = make_float2(0.0F, 0.0F);
+#pragma unroll 4
+        for (int k = 0; k < D; ++k) S = __fadd2_rn(S, hs[(y0 + k) * kGsPH + x]);
+        const float2* hin = hs + (y0 + D) * kGsPH + x;
+        const float2* hout = hs + y0 * kGsPH + x;
+#pragma unroll
+        for (int y = 0; y < kGsRunY; ++y) {
+            if (y > 0) S = __fadd2_rn(__fadd2_rn(S, hin[(y - 1) * kGsPH]), neg2(hout[(y - 1) * kGsPH]));
+            const float2 mab = __fmul2_rn(S, make_float2(invN, invN));  // (mean_a, mean_b)
+            const float v = c == 0 ? vin[y].r : (c == 1 ? vin[y].g : vin[y].b);
+            res[c][y] = max0(mab.x * v + mab.y);
+        }
+        __syncthreads();  // the next channel restages sab and hs
+    }
+    if (gx >= p.w) return;
+#pragma unroll
+    for (int y = 0; y < kGsRunY; ++y) {
+        const int gy = Y0 + y0 + y;
+        if (gy < p.h) store_rgb_keep_alpha(px<T>(out, gx, gy), Rgba{res[0][y], res[1][y], res[2][y], 0.0F},
+                                           px<const T>(in, gx, gy));
     }
 }
 
 // ----------------------------------------------------------------- a-trous
-constexpr int kAtTW = 64, kAtTH = 32, kAtThreads = 256;
+// Scratch holds c_1 .. c_L (three FP32 planes each); the bands are never
+// stored: w_{j+1} = c_j - c_{j+1} is formed again where it is needed (the
+// same binary32 subtraction of the same stored values), and c_0 comes from the
+// input frame each time (the same colour transform).
+constexpr int kAtTW = 256, kAtTH = 8, kAtThreads = 256;  // level tile and block
+static_assert(kAtTW == kAtThreads, "a tile row is one item per thread");
 
 template <class T>
-__global__ void atrous_prep_kernel(Img in, float* __restrict__ c0, long long npx) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
-    if (x >= in.w) return;
+__device__ __forceinline__ void atrous_c0(const Img& in, int x, int y, float& Y, float& Co, float& Cg) {
     const Rgba p = load_rgba(px<const T>(in, x, y));
-    const long long o = (long long)y * in.w + x;
-    c0[o] = (p.r + 2.0F * p.g + p.b) * 0.25F;
-    c0[npx + o] = p.r - p.b;
-    c0[2 * npx + o] = p.g - (p.r + p.b) * 0.5F;
+    Y = (p.r + 2.0F * p.g + p.b) * 0.25F;
+    Co = p.r - p.b;
+    Cg = p.g - (p.r + p.b) * 0.5F;
 }
 
 __device__ __forceinline__ float b3(float a, float b, float c, float d, float e) {
     return 0.0625F * (a + e) + 0.25F * (b + d) + 0.375F * c;
 }
 
-// One level in two passes over frame-wide planes (no halo staging): the
-// horizontal B3 pass of each channel's rows into tmp, then, per 64x32 tile,
-// the vertical pass, c_{j+1}, w_{j+1} = c_j - c_{j+1} and the tile's sum of
-// w^2 per channel.  Taps clamp at the frame edges; the pixel-to-thread mapping
-// of the vertical pass fixes the order of each tile's sum.
-__global__ void __launch_bounds__(kAtThreads) atrous_h_kernel(const float* __restrict__ cin, float* __restrict__ tmp,
-                                                              int w, long long npx, int s) {
-    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, c = blockIdx.z;
-    if (x >= w) return;
-    const float* row = cin + c * npx + (long long)y * w;
-    tmp[c * npx + (long long)y * w + x] = b3(__ldg(row + clampi(x - 2 * s, 0, w - 1)), __ldg(row + clampi(x - s, 0, w - 1)),
-                                             __ldg(row + x), __ldg(row + clampi(x + s, 0, w - 1)),
-                                             __ldg(row + clampi(x + 2 * s, 0, w - 1)));
-}
-__global__ void __launch_bounds__(kAtThreads) atrous_v_kernel(const float* __restrict__ cin, const float* __restrict__ tmp,
-                                                              float* __restrict__ cout, float* __restrict__ wout,
-                                                              float* __restrict__ part, int w, int h, long long npx,
-                                                              int s) {
-    const int x0 = blockIdx.x * kAtTW, y0 = blockIdx.y * kAtTH;
-    float acc[3] = {0.0F, 0.0F, 0.0F};
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        const float* t = tmp + c * npx;
-        for (int i = threadIdx.x; i < kAtTH * kAtTW; i += kAtThreads) {
-            const int r = i / kAtTW, xx = i - r * kAtTW;
-            const int x = x0 + xx, y = y0 + r;
-            if (x >= w || y >= h) continue;
-            const float v = b3(__ldg(t + (long long)clampi(y - 2 * s, 0, h - 1) * w + x),
-                               __ldg(t + (long long)clampi(y - s, 0, h - 1) * w + x), __ldg(t + (long long)y * w + x),
-                               __ldg(t + (long long)clampi(y + s, 0, h - 1) * w + x),
-                               __ldg(t + (long long)clampi(y + 2 * s, 0, h - 1) * w + x));
-            const long long o = c * npx + (long long)y * w + x;
-            const float d = __ldg(cin + o) - v;
-            cout[o] = v;
-            wout[o] = d;
-            acc[c] += d * d;
-        }
-    }
+// The tile's sums of w^2 per channel: warp shuffles, then the warps in order.
+__device__ __forceinline__ void atrous_tile_sums(const float (&acc)[3], float* __restrict__ part) {
     __shared__ float red[kAtThreads / 32][3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
@@ -272,68 +281,81 @@ __global__ void __launch_bounds__(kAtThreads) atrous_v_kernel(const float* __res
     }
 }
 
-// One level in one pass per 64x32 tile for taps up to 16 apart: the tile's
-// rows [y0 - 2s, y0 + 32 + 2s) of c_j over columns [x0 - 2s, x0 + 64 + 2s)
-// (clamped) staged in shared memory, the horizontal B3 pass of those rows into
-// shared memory, then the vertical pass, c_{j+1}, w_{j+1} and the tile's sum of
-// w^2 per channel -- the same operands, taps and pixel-to-thread mapping as the
-// two-pass form above, so the same floats, without the frame-wide scratch
-// planes of the horizontal pass.
-constexpr int kAtFuseMaxStep = 16;
-size_t atrous_level_smem(int s) {
-    return ((size_t)(kAtTH + 4 * s) * (kAtTW + 4 * s) + (size_t)(kAtTH + 4 * s) * kAtTW) * sizeof(float);
+// One level per 256x8 tile, for any tap distance s:
+//   vertical    for the tile's 8 rows and columns [x0 - 2s, x0 + 256 + 2s)
+//               (clamped), the B3 taps of rows y - 2s .. y + 2s (clamped) of
+//               all three channels, read through L1 / L2 (a warp reads 32
+//               consecutive columns of a row), into shared memory with the
+//               centre values of c_j;
+//   horizontal  the B3 taps of that row from shared memory: c_{j+1} written,
+//               w_{j+1} = c_j - c_{j+1}, the tile's sum of w_{j+1}^2 per
+//               channel.
+// FIRST (j = 0, taps 1 apart): the taps read the input frame and convert to
+// c_0 = (Y, Co, Cg).  The taps a row band needs lie within 4s rows, which stay
+// in L2 between neighbouring tiles, so DRAM reads each c_j about once.
+__host__ __device__ constexpr size_t atrous_level_floats(int s) {
+    return (size_t)3 * kAtTH * (kAtTW + 4 * s) + (size_t)3 * kAtTH * kAtTW;
 }
-__global__ void __launch_bounds__(kAtThreads) atrous_level_kernel(const float* __restrict__ cin, float* __restrict__ cout,
-                                                                  float* __restrict__ wout, float* __restrict__ part,
+template <class T, bool FIRST>
+__device__ __forceinline__ void atrous_tap(const Img& in, const float* __restrict__ cin, long long npx, int w, int x,
+                                           int y, float (&v)[3]) {
+    if (FIRST) {
+        atrous_c0<T>(in, x, y, v[0], v[1], v[2]);
+    } else {
+        const float* p = cin + (long long)y * w + x;
+        v[0] = __ldg(p);
+        v[1] = __ldg(p + npx);
+        v[2] = __ldg(p + 2 * npx);
+    }
+}
+template <class T, bool FIRST>
+__global__ void __launch_bounds__(kAtThreads) atrous_level_kernel(Img in, const float* __restrict__ cin,
+                                                                  float* __restrict__ cout, float* __restrict__ part,
                                                                   int w, int h, long long npx, int s) {
     extern __shared__ float sm[];
     const int x0 = blockIdx.x * kAtTW, y0 = blockIdx.y * kAtTH;
-    const int SR = kAtTH + 4 * s, SC = kAtTW + 4 * s;
-    float* st = sm;            // staged c_j: SR x SC
-    float* hp = sm + SR * SC;  // horizontal pass: SR x kAtTW
+    const int VW = kAtTW + 4 * s;
+    float* sv = sm;                          // [3][kAtTH][VW] vertical pass
+    float* sc = sm + 3 * kAtTH * VW;         // [3][kAtTH][kAtTW] centre values of c_j
+    // item i = r * VW + q, stepped by the block size without a division (VW > 256)
+    for (int i = threadIdx.x, r = 0, q = threadIdx.x; i < kAtTH * VW; i += kAtThreads) {
+        const int y = y0 + r, xq = x0 - 2 * s + q;
+        const int yc = min(y, h - 1), xc = clampi(xq, 0, w - 1);
+        float t[5][3];
+        atrous_tap<T, FIRST>(in, cin, npx, w, xc, clampi(yc - 2 * s, 0, h - 1), t[0]);
+        atrous_tap<T, FIRST>(in, cin, npx, w, xc, clampi(yc - s, 0, h - 1), t[1]);
+        atrous_tap<T, FIRST>(in, cin, npx, w, xc, yc, t[2]);
+        atrous_tap<T, FIRST>(in, cin, npx, w, xc, min(yc + s, h - 1), t[3]);
+        atrous_tap<T, FIRST>(in, cin, npx, w, xc, min(yc + 2 * s, h - 1), t[4]);
+#pragma unroll
+        for (int c = 0; c < 3; ++c) sv[(c * kAtTH + r) * VW + q] = b3(t[0][c], t[1][c], t[2][c], t[3][c], t[4][c]);
+        const int xx = q - 2 * s;
+        if (xx >= 0 && xx < kAtTW) {
+#pragma unroll
+            for (int c = 0; c < 3; ++c) sc[(c * kAtTH + r) * kAtTW + xx] = t[2][c];
+        }
+        q += kAtThreads;
+        if (q >= VW) {
+            q -= VW;
+            ++r;
+        }
+    }
+    __syncthreads();
     float acc[3] = {0.0F, 0.0F, 0.0F};
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        const float* src = cin + c * npx;
-        __syncthreads();
-        for (int i = threadIdx.x; i < SR * SC; i += kAtThreads) {
-            const int r = i / SC, q = i - r * SC;
-            st[i] = __ldg(src + (long long)clampi(y0 - 2 * s + r, 0, h - 1) * w + clampi(x0 - 2 * s + q, 0, w - 1));
-        }
-        __syncthreads();
-        for (int i = threadIdx.x; i < SR * kAtTW; i += kAtThreads) {
-            const int r = i / kAtTW, tx = i - r * kAtTW;
-            const float* row = st + r * SC + tx + 2 * s;
-            hp[i] = b3(row[-2 * s], row[-s], row[0], row[s], row[2 * s]);
-        }
-        __syncthreads();
         for (int i = threadIdx.x; i < kAtTH * kAtTW; i += kAtThreads) {
-            const int r = i / kAtTW, xx = i - r * kAtTW;
+            const int r = i / kAtTW, xx = i % kAtTW;  // powers of two
             const int x = x0 + xx, y = y0 + r;
             if (x >= w || y >= h) continue;
-            const float* col = hp + (r + 2 * s) * kAtTW + xx;
-            const float v = b3(col[-2 * s * kAtTW], col[-s * kAtTW], col[0], col[s * kAtTW], col[2 * s * kAtTW]);
-            const long long o = c * npx + (long long)y * w + x;
-            const float d = st[(r + 2 * s) * SC + xx + 2 * s] - v;
-            cout[o] = v;
-            wout[o] = d;
+            const float* row = sv + (c * kAtTH + r) * VW + xx + 2 * s;
+            const float v = b3(row[-2 * s], row[-s], row[0], row[s], row[2 * s]);
+            const float d = sc[(c * kAtTH + r) * kAtTW + xx] - v;
+            cout[c * npx + (long long)y * w + x] = v;
             acc[c] += d * d;
         }
     }
-    __shared__ float red[kAtThreads / 32][3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        float a = acc[c];
-#pragma unroll
-        for (int off = 16; off > 0; off >>= 1) a += __shfl_xor_sync(0xFFFFFFFFU, a, off);
-        if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5][c] = a;
-    }
-    __syncthreads();
-    if (threadIdx.x < 3) {
-        float a = 0.0F;
-        for (int k = 0; k < kAtThreads / 32; ++k) a += red[k][threadIdx.x];
-        part[(size_t)(blockIdx.y * gridDim.x + blockIdx.x) * 3 + threadIdx.x] = a;
-    }
+    atrous_tile_sums(acc, part);
 }
 
 struct AtrousThrArgs {
@@ -391,17 +413,28 @@ __device__ __forceinline__ float soft(float w, float t) {
     return m > 0.0F ? copysignf(m, w) : 0.0F;
 }
 
+// c = c_L + sum over j = L-1 .. 0 of soft(c_j - c_{j+1}, T_j), c_0 from the
+// input; inverse colour transform; alpha copied.  c_j (j >= 1) sits at
+// cl + (j - 1) * 3 * npx.
 template <class T>
-__global__ void atrous_recon_kernel(Img in, Img out, const float* __restrict__ cl, const float* __restrict__ wv,
-                                    const float* __restrict__ thr, int levels, long long npx) {
+__global__ void atrous_recon_kernel(Img in, Img out, const float* __restrict__ cl, const float* __restrict__ thr,
+                                    int levels, long long npx) {
     const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y;
     if (x >= in.w) return;
     const long long o = (long long)y * in.w + x;
+    float c0[3];
+    atrous_c0<T>(in, x, y, c0[0], c0[1], c0[2]);
     float v[3];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        float r = cl[c * npx + o];
-        for (int j = levels - 1; j >= 0; --j) r = r + soft(wv[((long long)j * 3 + c) * npx + o], thr[j * 3 + c]);
+        const float* p = cl + c * npx + o;
+        float hi = __ldg(p + (long long)(levels - 1) * 3 * npx);  // c_L
+        float r = hi;
+        for (int j = levels - 1; j >= 0; --j) {
+            const float lo = j == 0 ? c0[c] : __ldg(p + (long long)(j - 1) * 3 * npx);  // c_j
+            r = r + soft(lo - hi, thr[j * 3 + c]);
+            hi = lo;
+        }
         v[c] = r;
     }
     const float t = v[0] - 0.5F * v[2];
@@ -409,11 +442,74 @@ __global__ void atrous_recon_kernel(Img in, Img out, const float* __restrict__ c
                          px<const T>(in, x, y));
 }
 
+// The same per pixel for four pixels per thread (frames whose width is a
+// multiple of 4): 16-byte loads from each level plane.
+template <class T>
+__global__ void atrous_recon4_kernel(Img in, Img out, const float* __restrict__ cl, const float* __restrict__ thr,
+                                     int levels, long long npx) {
+    const int x = 4 * (blockIdx.x * blockDim.x + threadIdx.x), y = blockIdx.y;
+    if (x >= in.w) return;
+    const unsigned o = (unsigned)(y * in.w + x);
+    Rgba px4[4];
+    float c0[4][3];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        px4[i] = load_rgba(px<const T>(in, x + i, y));
+        c0[i][0] = (px4[i].r + 2.0F * px4[i].g + px4[i].b) * 0.25F;
+        c0[i][1] = px4[i].r - px4[i].b;
+        c0[i][2] = px4[i].g - (px4[i].r + px4[i].b) * 0.5F;
+    }
+    float v[4][3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        const float* p = cl + c * npx + o;
+        float4 hi4 = __ldg(reinterpret_cast<const float4*>(p + (long long)(levels - 1) * 3 * npx));  // c_L
+        float hi[4] = {hi4.x, hi4.y, hi4.z, hi4.w};
+        float r[4] = {hi4.x, hi4.y, hi4.z, hi4.w};
+        for (int j = levels - 1; j >= 0; --j) {
+            float lo[4];
+            if (j == 0) {
+#pragma unroll
+                for (int i = 0; i < 4; ++i) lo[i] = c0[i][c];
+            } else {
+                const float4 l4 = __ldg(reinterpret_cast<const float4*>(p + (long long)(j - 1) * 3 * npx));  // c_j
+                lo[0] = l4.x;
+                lo[1] = l4.y;
+                lo[2] = l4.z;
+                lo[3] = l4.w;
+            }
+            const float t = thr[j * 3 + c];
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                r[i] = r[i] + soft(lo[i] - hi[i], t);
+                hi[i] = lo[i];
+            }
+        }
+#pragma unroll
+        for (int i = 0; i < 4; ++i) v[i][c] = r[i];
+    }
+#pragma unroll
+    for (int i = 0; i < 4; ++i) {
+        const float t = v[i][0] - 0.5F * v[i][2];
+        store_rgb_keep_alpha(px<T>(out, x + i, y),
+                             Rgba{max0(t + 0.5F * v[i][1]), max0(t + v[i][2]), max0(t - 0.5F * v[i][1]), 0.0F},
+                             px<const T>(in, x + i, y));
+    }
+}
+
 size_t align256(size_t v) { return (v + 255U) & ~(size_t)255U; }
 
 }  // namespace
 
-cudaError_t guided_spec_setup() { return cudaSuccess; }  // the pass kernels use no dynamic shared memory
+cudaError_t guided_spec_setup() {
+    const int ab = (int)gs_ab_smem(kGuidedSpecMaxRadius), ob = (int)gs_out_smem(kGuidedSpecMaxRadius);
+    cudaError_t e = cudaSuccess;
+    for (const void* f : {(const void*)gsp_ab_kernel<__half>, (const void*)gsp_ab_kernel<float>})
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, ab);
+    for (const void* f : {(const void*)gsp_out_kernel<__half>, (const void*)gsp_out_kernel<float>})
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, ob);
+    return e;
+}
 
 size_t guided_spec_scratch_bytes(int w, int h, int radius) {
     const size_t Wa = (size_t)w + 2 * radius, Ha = (size_t)h + 2 * radius;
@@ -424,12 +520,14 @@ cudaError_t guided_spec_run(const Img& in, const Img& out, bool f16, int radius,
                             cudaStream_t st) {
     if (radius < 1 || radius > kGuidedSpecMaxRadius) return cudaErrorInvalidValue;
     const GsPlanes p = gs_planes(in.w, in.h, radius, scratch);
-    const dim3 ga((unsigned)((p.Wa + kGsThreads - 1) / kGsThreads), (unsigned)((p.Ha + kGsSeg - 1) / kGsSeg), 3);
-    if (f16) gsp_ab_kernel<__half><<<ga, kGsThreads, 0, st>>>(in, p, eps);
-    else gsp_ab_kernel<float><<<ga, kGsThreads, 0, st>>>(in, p, eps);
-    const dim3 go((unsigned)((in.w + kGsThreads - 1) / kGsThreads), (unsigned)((in.h + kGsSeg - 1) / kGsSeg));
-    if (f16) gsp_out_kernel<__half><<<go, kGsThreads, 0, st>>>(in, out, p);
-    else gsp_out_kernel<float><<<go, kGsThreads, 0, st>>>(in, out, p);
+    if ((size_t)p.Ha * p.Wa >= ((size_t)1 << 31)) return cudaErrorInvalidValue;  // 32-bit plane offsets
+    const dim3 ga((unsigned)((p.Wa + kGsTW - 1) / kGsTW), (unsigned)((p.Ha + kGsTH - 1) / kGsTH), 3);
+    const size_t sa = gs_ab_smem(radius), so = gs_out_smem(radius);
+    if (f16) gsp_ab_kernel<__half><<<ga, kGsThreads, sa, st>>>(in, p, eps);
+    else gsp_ab_kernel<float><<<ga, kGsThreads, sa, st>>>(in, p, eps);
+    const dim3 go((unsigned)((in.w + kGsTW - 1) / kGsTW), (unsigned)((in.h + kGsTH - 1) / kGsTH));
+    if (f16) gsp_out_kernel<__half><<<go, kGsThreads, so, st>>>(in, out, p);
+    else gsp_out_kernel<float><<<go, kGsThreads, so, st>>>(in, out, p);
     return cudaGetLastError();
 }
 
@@ -482,13 +580,7 @@ int atrous_plan(const cpipe_AtrousWaveletParams* p, int w, int h, AtrousPlan* ou
     q.gy = (h + kAtTH - 1) / kAtTH;
     const size_t npx = (size_t)w * h, plane3 = 3 * npx * sizeof(float);
     size_t o = 0;
-    q.off_c0 = o;
-    o = align256(o + plane3);
-    q.off_c1 = o;
-    o = align256(o + plane3);
-    q.off_tmp = o;
-    o = align256(o + plane3);
-    q.off_w = o;
+    q.off_c = o;  // c_1 .. c_L
     o = align256(o + (size_t)q.levels * plane3);
     q.off_part = o;
     o = align256(o + (size_t)q.levels * q.gx * q.gy * 3 * sizeof(float));
@@ -499,8 +591,12 @@ int atrous_plan(const cpipe_AtrousWaveletParams* p, int w, int h, AtrousPlan* ou
 }
 
 cudaError_t atrous_setup() {
-    return cudaFuncSetAttribute(atrous_level_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)atrous_level_smem(kAtFuseMaxStep));
+    const int bytes = (int)(atrous_level_floats(1 << (kAtrousMaxLevels - 1)) * sizeof(float));
+    cudaError_t e = cudaSuccess;
+    for (const void* f : {(const void*)atrous_level_kernel<__half, true>, (const void*)atrous_level_kernel<float, true>,
+                          (const void*)atrous_level_kernel<float, false>})
+        if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    return e;
 }
 
 cudaError_t atrous_run(const AtrousPlan& p, const Img& in, const Img& out, bool f16, void* scratch, cudaStream_t st) {
@@ -510,38 +606,43 @@ cudaError_t atrous_run(const AtrousPlan& p, const Img& in, const Img& out, bool 
                            in.h, st);
     }
     char* base = static_cast<char*>(scratch);
-    float* c[2] = {reinterpret_cast<float*>(base + p.off_c0), reinterpret_cast<float*>(base + p.off_c1)};
-    float* wv = reinterpret_cast<float*>(base + p.off_w);
-    float* tmp = reinterpret_cast<float*>(base + p.off_tmp);
+    const long long npx = (long long)p.w * p.h;
+    if (npx >= ((long long)1 << 31)) return cudaErrorInvalidValue;  // 32-bit plane offsets
+    float* cl = reinterpret_cast<float*>(base + p.off_c);  // c_{j+1} at cl + j * 3 * npx
     float* part = reinterpret_cast<float*>(base + p.off_part);
     float* thr = reinterpret_cast<float*>(base + p.off_thr);
-    const long long npx = (long long)p.w * p.h;
-    const dim3 pg((unsigned)((p.w + 255) / 256), (unsigned)p.h);
-    if (f16) atrous_prep_kernel<__half><<<pg, 256, 0, st>>>(in, c[0], npx);
-    else atrous_prep_kernel<float><<<pg, 256, 0, st>>>(in, c[0], npx);
     AtrousTiles tl{};
     tl.stride = p.gx * p.gy * 3;
+    const dim3 lg((unsigned)p.gx, (unsigned)p.gy);
     for (int j = 0; j < p.levels; ++j) {
         const int s = 1 << j;
-        const dim3 lg((unsigned)p.gx, (unsigned)p.gy);
         tl.nb[j] = (int)(lg.x * lg.y);
-        if (s <= kAtFuseMaxStep) {
-            atrous_level_kernel<<<lg, kAtThreads, atrous_level_smem(s), st>>>(
-                c[j & 1], c[(j + 1) & 1], wv + (size_t)j * 3 * npx, part + (size_t)j * tl.stride, p.w, p.h, npx, s);
-            continue;
+        float* cout = cl + (size_t)j * 3 * npx;
+        float* pj = part + (size_t)j * tl.stride;
+        const size_t sm = atrous_level_floats(s) * sizeof(float);
+        if (j == 0) {
+            if (f16) atrous_level_kernel<__half, true><<<lg, kAtThreads, sm, st>>>(in, nullptr, cout, pj, p.w, p.h, npx, s);
+            else atrous_level_kernel<float, true><<<lg, kAtThreads, sm, st>>>(in, nullptr, cout, pj, p.w, p.h, npx, s);
+        } else {
+            // past the first level the input frame is not read (T is immaterial)
+            atrous_level_kernel<float, false><<<lg, kAtThreads, sm, st>>>(in, cl + (size_t)(j - 1) * 3 * npx, cout, pj,
+                                                                         p.w, p.h, npx, s);
         }
-        const dim3 hg((unsigned)((p.w + kAtThreads - 1) / kAtThreads), (unsigned)p.h, 3);
-        atrous_h_kernel<<<hg, kAtThreads, 0, st>>>(c[j & 1], tmp, p.w, npx, s);
-        atrous_v_kernel<<<lg, kAtThreads, 0, st>>>(c[j & 1], tmp, c[(j + 1) & 1], wv + (size_t)j * 3 * npx,
-                                                   part + (size_t)j * tl.stride, p.w, p.h, npx, s);
     }
     AtrousThrArgs ta{};
     for (int j = 0; j < p.levels; ++j)
         for (int k = 0; k < 3; ++k) ta.noise[j][k] = p.noise[j][k];
     for (int k = 0; k < 3; ++k) ta.strength[k] = p.strength[k];
     atrous_thresh_kernel<<<p.levels * 3, 256, 0, st>>>(part, tl, npx, ta, thr);
-    if (f16) atrous_recon_kernel<__half><<<pg, 256, 0, st>>>(in, out, c[p.levels & 1], wv, thr, p.levels, npx);
-    else atrous_recon_kernel<float><<<pg, 256, 0, st>>>(in, out, c[p.levels & 1], wv, thr, p.levels, npx);
+    if (p.w % 4 == 0) {
+        const dim3 pg((unsigned)((p.w / 4 + 127) / 128), (unsigned)p.h);
+        if (f16) atrous_recon4_kernel<__half><<<pg, 128, 0, st>>>(in, out, cl, thr, p.levels, npx);
+        else atrous_recon4_kernel<float><<<pg, 128, 0, st>>>(in, out, cl, thr, p.levels, npx);
+    } else {
+        const dim3 pg((unsigned)((p.w + 255) / 256), (unsigned)p.h);
+        if (f16) atrous_recon_kernel<__half><<<pg, 256, 0, st>>>(in, out, cl, thr, p.levels, npx);
+        else atrous_recon_kernel<float><<<pg, 256, 0, st>>>(in, out, cl, thr, p.levels, npx);
+    }
     return cudaGetLastError();
 }
 

@@ -27,7 +27,7 @@ struct AtrousPlan {
     float noise[kAtrousMaxLevels][3] = {};  // band noise std per level and channel (Y, Co, Cg)
     float strength[3] = {};
     bool copy = false;           // levels 0: output = input
-    size_t off_c0 = 0, off_c1 = 0, off_tmp = 0, off_w = 0, off_part = 0, off_thr = 0, bytes = 0;
+    size_t off_c = 0, off_part = 0, off_thr = 0, bytes = 0;  // off_c: c_1 .. c_L (3 FP32 planes each)
 };
 
 // Validates the parameters (CPIPE_BAD_INDEX when out of range) and sizes the

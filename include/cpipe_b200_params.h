@@ -231,7 +231,10 @@ typedef struct {
     float kaiser_beta;  /* aggregation window parameter (2.0) */
     int32_t stages;     /* 1 = hard threshold only, 2 = hard threshold then Wiener */
     int32_t transform;  /* 0 = DCT/Haar on the tensor cores (FP16 hi/lo split products, FP32
-                           accumulation); 1 = FP32 on the CUDA cores.  Same definition. */
+                           accumulation); 1 = FP32 on the CUDA cores.  Same definition.
+                           2 = screening form: tensor cores with single FP16 products (about
+                           2^-11 relative per product), for checks that need BM3D's output
+                           to a few 1e-4 rather than to FP32 accuracy. */
 } cpipe_Bm3dSpecParams;
 
 /* Learned surrogate denoiser weights (no reference counterpart: the

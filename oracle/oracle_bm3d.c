@@ -320,7 +320,7 @@ static int check_params(const cpipe_Bm3dSpecParams* p) {
     if (!(p->tau_match1 >= 0.0f && p->tau_match1 <= 16000.0f)) return 0;
     if (!(p->tau_match2 >= 0.0f && p->tau_match2 <= 16000.0f)) return 0;
     if (p->stages != 1 && p->stages != 2) return 0;
-    if (p->transform != 0 && p->transform != 1) return 0;
+    if (p->transform < 0 || p->transform > 2) return 0; /* precision forms of the GPU path; one definition */
     if (!(p->lambda3d >= 0.0f) || !(p->kaiser_beta >= 0.0f)) return 0;
     return 1;
 }

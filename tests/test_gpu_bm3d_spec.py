@@ -149,3 +149,20 @@ def test_bm3d_precision_forms_against_fp64(cuda_device, h, w, sigma, kw):
             errs[form] = compare(got, want, f"{form} {np.dtype(dtype).name} {w}x{h} {kw}")
         if dtype == np.float32:
             assert errs["tensor"][0] <= 2e-3 and errs["fp32"][0] <= 1e-3
+
+
+@pytest.mark.parametrize("h,w,sigma", [(256, 256, 0.032), (96, 128, 0.03)])
+def test_bm3d_screening_form(cuda_device, h, w, sigma):
+    """The screening form (transform 2: single FP16 products on the tensor
+    cores), which the surrogate's spot check runs, against the FP64 oracle and
+    against the split form.  Its error is far below the spot check's 40 dB
+    decision margin: >= 50 dB against both (measured values printed)."""
+    clean = clean_rgb(h + 5 * w, h, w)
+    x = noisy_rgba(clean, sigma, h * w + 1, dtype=np.float16)
+    want = oracle.bm3d_spec(x.astype(np.float32), blobs.bm3d_spec(sigma))
+    fast = gpu_bm3d(x, blobs.bm3d_spec(sigma, transform="tensor_fp16")).astype(np.float64)[..., :3]
+    split = gpu_bm3d(x, blobs.bm3d_spec(sigma, transform="tensor")).astype(np.float64)[..., :3]
+    p_oracle, p_split = psnr(fast, np.asarray(want, np.float64)[..., :3]), psnr(fast, split)
+    print(f"screening form {w}x{h}: {p_oracle:.1f} dB against the oracle, {p_split:.1f} dB against the split form")
+    assert p_oracle >= 50.0 and p_split >= 50.0
+    np.testing.assert_array_equal(gpu_bm3d(x, blobs.bm3d_spec(sigma, transform="tensor_fp16"))[..., 3], x[..., 3])
