@@ -59,14 +59,15 @@ namespace {
 // paired sums (sum v, sum v^2) and (sum a, sum b) run as sm_100 packed adds.
 //   ab   per channel (grid z), a 64x32 tile of the extended domain
 //        [-R, w+R) x [-R, h+R): the clamped image tile with its 2R halo staged
-//        in shared memory; row sums of (v, v^2) over 2R+1 columns (one sliding
+//        in shared memory by asynchronous copies; row sums of (v, v^2) over 2R+1 columns (one sliding
 //        window per 16 outputs, restarted at each window); column sums of
 //        those over 2R+1 rows (one window per 8 outputs); m = S/N, corr = Q/N
 //        (products with the binary32 reciprocal of N), var = max(corr - m^2, 0),
 //        a = var/(var+eps) (__fdividef: within 2 ulp), b = m - a m into the a
 //        and b planes (extended domain, row pitch w + 2R).
 //   out  per 64x32 output tile, the three channels in turn: the (a, b) pairs
-//        with their 2R halo staged and box-summed the same way; per pixel
+//        with their 2R halo staged by asynchronous copies and box-summed the
+//        same way; per pixel
 //        out = max(mean_a v + mean_b, 0) (means as products with 1/N) held in
 //        registers, then written with the input's alpha.
 // Each running sum adds at most 2R+1 + 2 * 15 terms, so binary16 frames stay
@@ -99,6 +100,23 @@ __host__ __device__ constexpr size_t gs_out_smem(int R) {
     return (size_t)(kGsTH + 2 * R) * gs_pitch(R) * 8 + (size_t)(kGsTH + 2 * R) * kGsPH * 8;
 }
 __device__ __forceinline__ float2 neg2(float2 v) { return make_float2(-v.x, -v.y); }
+// 4-byte asynchronous global -> shared copies: a warp's whole staging is in
+// flight at once instead of one dependent load per iteration.
+__device__ __forceinline__ void gs_cp4(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"((unsigned)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void gs_cp_wait() { asm volatile("cp.async.commit_group;\ncp.async.wait_group 0;\n" ::: "memory"); }
+// A staged 32-bit word -> the channel's value: binary32 frames stage the value,
+// binary16 frames the word holding channels (c & ~1, c | 1).
+template <class T>
+__device__ __forceinline__ float gs_val(uint32_t word, int c);
+template <>
+__device__ __forceinline__ float gs_val<float>(uint32_t word, int) { return __uint_as_float(word); }
+template <>
+__device__ __forceinline__ float gs_val<__half>(uint32_t word, int c) {
+    return __half2float(__ushort_as_half((unsigned short)((c & 1) ? (word >> 16) : (word & 0xFFFFU))));
+}
 
 template <class T>
 __global__ void __launch_bounds__(kGsThreads) gsp_ab_kernel(Img in, GsPlanes p, float eps) {
@@ -110,29 +128,30 @@ __global__ void __launch_bounds__(kGsThreads) gsp_ab_kernel(Img in, GsPlanes p, 
     const int c = blockIdx.z, X0 = blockIdx.x * kGsTW, Y0 = blockIdx.y * kGsTH;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     // plane column X0 + q's box starts at image column X0 - 2R + q
+    const int cw = std::is_same<T, float>::value ? c : (c & ~1);  // element of the staged word
     for (int r = warp; r < SR; r += kGsThreads / 32) {
-        const T* row = px<const T>(in, 0, clampi(Y0 - 2 * R + r, 0, in.h - 1)) + c;
+        const T* row = px<const T>(in, 0, clampi(Y0 - 2 * R + r, 0, in.h - 1)) + cw;
         float* dst = sv + r * PV;
-#pragma unroll 3
-        for (int q = lane; q < SC; q += 32) dst[q] = (float)row[4 * clampi(X0 - 2 * R + q, 0, in.w - 1)];
+        for (int q = lane; q < SC; q += 32) gs_cp4(dst + q, row + 4 * clampi(X0 - 2 * R + q, 0, in.w - 1));
     }
+    gs_cp_wait();
     __syncthreads();
     // row pass: one window per thread, rows on the lanes (SR <= 64 rows)
     {
         const int r = threadIdx.x & 63, x0 = (threadIdx.x >> 6) * kGsRunX;
         if (r < SR) {
-        const float* row = sv + r * PV + x0;
+        const uint32_t* row = reinterpret_cast<const uint32_t*>(sv) + r * PV + x0;
         float2 s = make_float2(0.0F, 0.0F);
 #pragma unroll 4
         for (int k = 0; k < D; ++k) {
-            const float v = row[k];
+            const float v = gs_val<T>(row[k], c);
             s = __fadd2_rn(s, make_float2(v, v * v));
         }
         float2* o = hs + r * kGsPH + x0;
         o[0] = s;
 #pragma unroll
         for (int x = 1; x < kGsRunX; ++x) {
-            const float vi = row[x + D - 1], vo = row[x - 1];
+            const float vi = gs_val<T>(row[x + D - 1], c), vo = gs_val<T>(row[x - 1], c);
             s = __fadd2_rn(__fadd2_rn(s, make_float2(vi, vi * vi)), make_float2(-vo, -(vo * vo)));
             o[x] = s;
         }
@@ -178,6 +197,24 @@ __global__ void __launch_bounds__(kGsThreads) gsp_out_kernel(Img in, Img out, Gs
     const size_t plane = (size_t)p.Ha * p.Wa;
     const int x = threadIdx.x % kGsTW, y0 = (threadIdx.x / kGsTW) * kGsRunY;
     const int gx = X0 + x;
+    // output x reads plane columns x .. x + 2R (extended x - R .. x + R)
+    auto stage = [&](int c) {
+        const float* ca = p.a + (size_t)c * plane;
+        const float* cb = p.b + (size_t)c * plane;
+        for (int r = warp; r < SR; r += kGsThreads / 32) {
+            const unsigned ro = (unsigned)min(Y0 + r, p.Ha - 1) * (unsigned)p.Wa;
+            const float* ra = ca + ro;
+            const float* rb = cb + ro;
+            float2* dst = sab + r * PV;
+            for (int q = lane; q < SC; q += 32) {
+                const int xq = min(X0 + q, p.Wa - 1);
+                gs_cp4(&dst[q].x, ra + xq);
+                gs_cp4(&dst[q].y, rb + xq);
+            }
+        }
+        asm volatile("cp.async.commit_group;\n" ::: "memory");
+    };
+    stage(0);
     // the thread's eight input pixels (alpha and v), loaded once
     Rgba vin[kGsRunY];
 #pragma unroll
@@ -188,20 +225,8 @@ __global__ void __launch_bounds__(kGsThreads) gsp_out_kernel(Img in, Img out, Gs
     float res[3][kGsRunY];
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        // output x reads plane columns x .. x + 2R (extended x - R .. x + R)
-        const float* ca = p.a + (size_t)c * plane;
-        const float* cb = p.b + (size_t)c * plane;
-        for (int r = warp; r < SR; r += kGsThreads / 32) {
-            const unsigned ro = (unsigned)min(Y0 + r, p.Ha - 1) * (unsigned)p.Wa;
-            const float* ra = ca + ro;
-            const float* rb = cb + ro;
-            float2* dst = sab + r * PV;
-#pragma unroll 3
-            for (int q = lane; q < SC; q += 32) {
-                const int xq = min(X0 + q, p.Wa - 1);
-                dst[q] = make_float2(__ldg(ra + xq), __ldg(rb + xq));
-            }
-        }
+        if (c > 0) stage(c);  // the previous channel's passes are done with sab
+        asm volatile("cp.async.wait_group 0;\n" ::: "memory");
         __syncthreads();
         {
             const int r = threadIdx.x & 63, x0 = (threadIdx.x >> 6) * kGsRunX;
@@ -232,7 +257,7 @@ __global__ void __launch_bounds__(kGsThreads) gsp_out_kernel(Img in, Img out, Gs
             const float v = c == 0 ? vin[y].r : (c == 1 ? vin[y].g : vin[y].b);
             res[c][y] = max0(mab.x * v + mab.y);
         }
-        __syncthreads();  // the next channel restages sab and hs
+        __syncthreads();  // the next channel restages sab and rewrites hs
     }
     if (gx >= p.w) return;
 #pragma unroll
@@ -521,6 +546,10 @@ cudaError_t guided_spec_run(const Img& in, const Img& out, bool f16, int radius,
     if (radius < 1 || radius > kGuidedSpecMaxRadius) return cudaErrorInvalidValue;
     const GsPlanes p = gs_planes(in.w, in.h, radius, scratch);
     if ((size_t)p.Ha * p.Wa >= ((size_t)1 << 31)) return cudaErrorInvalidValue;  // 32-bit plane offsets
+    // the staging copies move aligned 32-bit words of interleaved RGBA pixels
+    const size_t elem = f16 ? 2 : 4;
+    if (in.pix_stride != 4 || (reinterpret_cast<uintptr_t>(in.data) & 3U) != 0 || (in.row_stride * elem) % 4 != 0)
+        return cudaErrorInvalidValue;
     const dim3 ga((unsigned)((p.Wa + kGsTW - 1) / kGsTW), (unsigned)((p.Ha + kGsTH - 1) / kGsTH), 3);
     const size_t sa = gs_ab_smem(radius), so = gs_out_smem(radius);
     if (f16) gsp_ab_kernel<__half><<<ga, kGsThreads, sa, st>>>(in, p, eps);
