@@ -29,11 +29,13 @@
 // Kernels
 //   gsp_ab / gsp_out     the guided filter as two tile kernels with sliding
 //                        binary32 box sums along rows and columns (see below).
-//   atrous_level_kernel  per 256x8 tile, one level: the vertical B3 taps of
-//                        all three channels through L1 / L2 into shared
-//                        memory, the horizontal taps from there, c_{j+1}
-//                        written, the tile's sum of w_{j+1}^2 per channel; the
-//                        first level reads c_0 (Y, Co, Cg) from the input frame.
+//   atrous_walk_kernel   one level: per block 256 columns and one residue class
+//                        of rows (y = phi + k 2^j), each thread walking its
+//                        column with the five vertical taps of each channel in
+//                        registers (one new row per step), the horizontal taps
+//                        through shared memory; c_{j+1} written, the block's
+//                        sum of w_{j+1}^2 per channel; the first level reads
+//                        c_0 (Y, Co, Cg) from the input frame.
 //   atrous_thresh_kernel per (level, channel): the tiles' sums added in a fixed
 //                        order (compensated binary32), the BayesShrink
 //                        threshold.
@@ -273,8 +275,7 @@ __global__ void __launch_bounds__(kGsThreads) gsp_out_kernel(Img in, Img out, Gs
 // stored: w_{j+1} = c_j - c_{j+1} is formed again where it is needed (the
 // same binary32 subtraction of the same stored values), and c_0 comes from the
 // input frame each time (the same colour transform).
-constexpr int kAtTW = 256, kAtTH = 8, kAtThreads = 256;  // level tile and block
-static_assert(kAtTW == kAtThreads, "a tile row is one item per thread");
+constexpr int kAtThreads = 256;  // level block: 256 columns
 
 template <class T>
 __device__ __forceinline__ void atrous_c0(const Img& in, int x, int y, float& Y, float& Co, float& Cg) {
@@ -306,21 +307,6 @@ __device__ __forceinline__ void atrous_tile_sums(const float (&acc)[3], float* _
     }
 }
 
-// One level per 256x8 tile, for any tap distance s:
-//   vertical    for the tile's 8 rows and columns [x0 - 2s, x0 + 256 + 2s)
-//               (clamped), the B3 taps of rows y - 2s .. y + 2s (clamped) of
-//               all three channels, read through L1 / L2 (a warp reads 32
-//               consecutive columns of a row), into shared memory with the
-//               centre values of c_j;
-//   horizontal  the B3 taps of that row from shared memory: c_{j+1} written,
-//               w_{j+1} = c_j - c_{j+1}, the tile's sum of w_{j+1}^2 per
-//               channel.
-// FIRST (j = 0, taps 1 apart): the taps read the input frame and convert to
-// c_0 = (Y, Co, Cg).  The taps a row band needs lie within 4s rows, which stay
-// in L2 between neighbouring tiles, so DRAM reads each c_j about once.
-__host__ __device__ constexpr size_t atrous_level_floats(int s) {
-    return (size_t)3 * kAtTH * (kAtTW + 4 * s) + (size_t)3 * kAtTH * kAtTW;
-}
 template <class T, bool FIRST>
 __device__ __forceinline__ void atrous_tap(const Img& in, const float* __restrict__ cin, long long npx, int w, int x,
                                            int y, float (&v)[3]) {
@@ -333,51 +319,60 @@ __device__ __forceinline__ void atrous_tap(const Img& in, const float* __restric
         v[2] = __ldg(p + 2 * npx);
     }
 }
+// One level as a polyphase walk: the taps of
+// output row y lie in rows y + m s, so the rows of one residue class phi
+// (y = phi + k s) form a dense 5-tap filter.  A block covers 256 columns
+// (256 - 4s outputs and their 2s halo each side); each thread keeps one
+// column's five vertical taps per channel in registers and walks kAtSeg steps
+// of one residue class, loading one new row per step; per step the block's
+// vertical results go through shared memory for the horizontal taps.  Every
+// c_j value is read about once (plus the 4s/(256 - 4s) column halo and the four
+// warm-up rows per walk).  Per output: the vertical B3 taps first, then the
+// horizontal ones, each b3(t[-2s], t[-s], t[0], t[s], t[2s]); the first level
+// (s = 1) reads c_0 = (Y, Co, Cg) from the input frame.
+constexpr int kAtSeg = 64;  // steps per walk
+__host__ __device__ constexpr int atrous_walk_cols(int s) { return kAtThreads - 4 * s; }
 template <class T, bool FIRST>
-__global__ void __launch_bounds__(kAtThreads) atrous_level_kernel(Img in, const float* __restrict__ cin,
-                                                                  float* __restrict__ cout, float* __restrict__ part,
-                                                                  int w, int h, long long npx, int s) {
-    extern __shared__ float sm[];
-    const int x0 = blockIdx.x * kAtTW, y0 = blockIdx.y * kAtTH;
-    const int VW = kAtTW + 4 * s;
-    float* sv = sm;                          // [3][kAtTH][VW] vertical pass
-    float* sc = sm + 3 * kAtTH * VW;         // [3][kAtTH][kAtTW] centre values of c_j
-    // item i = r * VW + q, stepped by the block size without a division (VW > 256)
-    for (int i = threadIdx.x, r = 0, q = threadIdx.x; i < kAtTH * VW; i += kAtThreads) {
-        const int y = y0 + r, xq = x0 - 2 * s + q;
-        const int yc = min(y, h - 1), xc = clampi(xq, 0, w - 1);
-        float t[5][3];
-        atrous_tap<T, FIRST>(in, cin, npx, w, xc, clampi(yc - 2 * s, 0, h - 1), t[0]);
-        atrous_tap<T, FIRST>(in, cin, npx, w, xc, clampi(yc - s, 0, h - 1), t[1]);
-        atrous_tap<T, FIRST>(in, cin, npx, w, xc, yc, t[2]);
-        atrous_tap<T, FIRST>(in, cin, npx, w, xc, min(yc + s, h - 1), t[3]);
-        atrous_tap<T, FIRST>(in, cin, npx, w, xc, min(yc + 2 * s, h - 1), t[4]);
-#pragma unroll
-        for (int c = 0; c < 3; ++c) sv[(c * kAtTH + r) * VW + q] = b3(t[0][c], t[1][c], t[2][c], t[3][c], t[4][c]);
-        const int xx = q - 2 * s;
-        if (xx >= 0 && xx < kAtTW) {
-#pragma unroll
-            for (int c = 0; c < 3; ++c) sc[(c * kAtTH + r) * kAtTW + xx] = t[2][c];
-        }
-        q += kAtThreads;
-        if (q >= VW) {
-            q -= VW;
-            ++r;
-        }
-    }
-    __syncthreads();
+__global__ void __launch_bounds__(kAtThreads) atrous_walk_kernel(Img in, const float* __restrict__ cin,
+                                                                 float* __restrict__ cout, float* __restrict__ part,
+                                                                 int w, int h, long long npx, int s) {
+    __shared__ float vrow[3][kAtThreads];
+    const int t = threadIdx.x, OW = atrous_walk_cols(s);
+    const int x0 = blockIdx.x * OW;                      // first output column
+    const int xc = clampi(x0 - 2 * s + t, 0, w - 1);      // this thread's (clamped) column
+    const int phi = blockIdx.y % s, k0 = (blockIdx.y / s) * kAtSeg;
+    // steps with phi + s k < h (block-uniform)
+    const int nk = phi < h ? min(kAtSeg, (h - 1 - phi) / s + 1 - k0) : 0;
     float acc[3] = {0.0F, 0.0F, 0.0F};
+    if (nk > 0) {
+        const int x = x0 + t - 2 * s;
+        const bool out = t >= 2 * s && t < 2 * s + OW && x < w;
+        float ring[5][3];  // c_j at rows y - 2s .. y + 2s (clamped) of this column
+        const int yb = phi + s * k0;
 #pragma unroll
-    for (int c = 0; c < 3; ++c) {
-        for (int i = threadIdx.x; i < kAtTH * kAtTW; i += kAtThreads) {
-            const int r = i / kAtTW, xx = i % kAtTW;  // powers of two
-            const int x = x0 + xx, y = y0 + r;
-            if (x >= w || y >= h) continue;
-            const float* row = sv + (c * kAtTH + r) * VW + xx + 2 * s;
-            const float v = b3(row[-2 * s], row[-s], row[0], row[s], row[2 * s]);
-            const float d = sc[(c * kAtTH + r) * kAtTW + xx] - v;
-            cout[c * npx + (long long)y * w + x] = v;
-            acc[c] += d * d;
+        for (int m = 0; m < 4; ++m) atrous_tap<T, FIRST>(in, cin, npx, w, xc, clampi(yb + (m - 2) * s, 0, h - 1), ring[m]);
+        for (int k = 0; k < nk; ++k) {
+            const int y = yb + s * k;
+            atrous_tap<T, FIRST>(in, cin, npx, w, xc, min(y + 2 * s, h - 1), ring[4]);
+#pragma unroll
+            for (int c = 0; c < 3; ++c) vrow[c][t] = b3(ring[0][c], ring[1][c], ring[2][c], ring[3][c], ring[4][c]);
+            __syncthreads();
+            if (out) {
+                float* dst = cout + (unsigned)(y * w + x);
+#pragma unroll
+                for (int c = 0; c < 3; ++c) {
+                    const float* v = vrow[c] + t;
+                    const float hv = b3(v[-2 * s], v[-s], v[0], v[s], v[2 * s]);
+                    const float d = ring[2][c] - hv;
+                    dst[c * npx] = hv;
+                    acc[c] += d * d;
+                }
+            }
+            __syncthreads();  // vrow is rewritten by the next step
+#pragma unroll
+            for (int m = 0; m < 4; ++m)
+#pragma unroll
+                for (int c = 0; c < 3; ++c) ring[m][c] = ring[m + 1][c];
         }
     }
     atrous_tile_sums(acc, part);
@@ -524,6 +519,12 @@ __global__ void atrous_recon4_kernel(Img in, Img out, const float* __restrict__ 
 
 size_t align256(size_t v) { return (v + 255U) & ~(size_t)255U; }
 
+dim3 atrous_walk_grid(int w, int h, int s) {
+    const int rows = (h + s - 1) / s;  // steps of the longest residue class
+    return dim3((unsigned)((w + atrous_walk_cols(s) - 1) / atrous_walk_cols(s)),
+                (unsigned)(s * ((rows + kAtSeg - 1) / kAtSeg)));
+}
+
 }  // namespace
 
 cudaError_t guided_spec_setup() {
@@ -605,28 +606,25 @@ int atrous_plan(const cpipe_AtrousWaveletParams* p, int w, int h, AtrousPlan* ou
     }
     q.strength[0] = p->luma_strength;
     q.strength[1] = q.strength[2] = p->chroma_strength;
-    q.gx = (w + kAtTW - 1) / kAtTW;
-    q.gy = (h + kAtTH - 1) / kAtTH;
     const size_t npx = (size_t)w * h, plane3 = 3 * npx * sizeof(float);
     size_t o = 0;
     q.off_c = o;  // c_1 .. c_L
     o = align256(o + (size_t)q.levels * plane3);
     q.off_part = o;
-    o = align256(o + (size_t)q.levels * q.gx * q.gy * 3 * sizeof(float));
+    size_t tiles = 0;
+    for (int j = 0; j < q.levels; ++j) {
+        const dim3 g = atrous_walk_grid(w, h, 1 << j);
+        tiles = std::max(tiles, (size_t)g.x * g.y);
+    }
+    q.tiles = (int)tiles;
+    o = align256(o + (size_t)q.levels * tiles * 3 * sizeof(float));
     q.off_thr = o;
     o = align256(o + (size_t)q.levels * 3 * sizeof(float));
     q.bytes = o;
     return CPIPE_OK;
 }
 
-cudaError_t atrous_setup() {
-    const int bytes = (int)(atrous_level_floats(1 << (kAtrousMaxLevels - 1)) * sizeof(float));
-    cudaError_t e = cudaSuccess;
-    for (const void* f : {(const void*)atrous_level_kernel<__half, true>, (const void*)atrous_level_kernel<float, true>,
-                          (const void*)atrous_level_kernel<float, false>})
-        if (e == cudaSuccess) e = cudaFuncSetAttribute(f, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
-    return e;
-}
+cudaError_t atrous_setup() { return cudaSuccess; }  // the level kernels use static shared memory only
 
 cudaError_t atrous_run(const AtrousPlan& p, const Img& in, const Img& out, bool f16, void* scratch, cudaStream_t st) {
     if (p.copy) {
@@ -641,21 +639,20 @@ cudaError_t atrous_run(const AtrousPlan& p, const Img& in, const Img& out, bool 
     float* part = reinterpret_cast<float*>(base + p.off_part);
     float* thr = reinterpret_cast<float*>(base + p.off_thr);
     AtrousTiles tl{};
-    tl.stride = p.gx * p.gy * 3;
-    const dim3 lg((unsigned)p.gx, (unsigned)p.gy);
+    tl.stride = p.tiles * 3;
     for (int j = 0; j < p.levels; ++j) {
         const int s = 1 << j;
-        tl.nb[j] = (int)(lg.x * lg.y);
         float* cout = cl + (size_t)j * 3 * npx;
         float* pj = part + (size_t)j * tl.stride;
-        const size_t sm = atrous_level_floats(s) * sizeof(float);
+        const dim3 wg = atrous_walk_grid(p.w, p.h, s);
+        tl.nb[j] = (int)(wg.x * wg.y);
         if (j == 0) {
-            if (f16) atrous_level_kernel<__half, true><<<lg, kAtThreads, sm, st>>>(in, nullptr, cout, pj, p.w, p.h, npx, s);
-            else atrous_level_kernel<float, true><<<lg, kAtThreads, sm, st>>>(in, nullptr, cout, pj, p.w, p.h, npx, s);
+            if (f16) atrous_walk_kernel<__half, true><<<wg, kAtThreads, 0, st>>>(in, nullptr, cout, pj, p.w, p.h, npx, s);
+            else atrous_walk_kernel<float, true><<<wg, kAtThreads, 0, st>>>(in, nullptr, cout, pj, p.w, p.h, npx, s);
         } else {
             // past the first level the input frame is not read (T is immaterial)
-            atrous_level_kernel<float, false><<<lg, kAtThreads, sm, st>>>(in, cl + (size_t)(j - 1) * 3 * npx, cout, pj,
-                                                                         p.w, p.h, npx, s);
+            atrous_walk_kernel<float, false><<<wg, kAtThreads, 0, st>>>(in, cl + (size_t)(j - 1) * 3 * npx, cout, pj,
+                                                                        p.w, p.h, npx, s);
         }
     }
     AtrousThrArgs ta{};

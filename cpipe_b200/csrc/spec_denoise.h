@@ -23,7 +23,7 @@ cudaError_t guided_spec_run(const Img& in, const Img& out, bool f16, int radius,
 
 struct AtrousPlan {
     int w = 0, h = 0, levels = 0;
-    int gx = 0, gy = 0;          // level-kernel grid (partial sums per CTA)
+    int tiles = 0;               // most partial-sum blocks of any level (one per level-kernel block)
     float noise[kAtrousMaxLevels][3] = {};  // band noise std per level and channel (Y, Co, Cg)
     float strength[3] = {};
     bool copy = false;           // levels 0: output = input
@@ -33,7 +33,7 @@ struct AtrousPlan {
 // Validates the parameters (CPIPE_BAD_INDEX when out of range) and sizes the
 // scratch buffer for a w x h frame.
 int atrous_plan(const cpipe_AtrousWaveletParams* p, int w, int h, AtrousPlan* out);
-// Sets the level kernel's shared-memory limit (host side; before a capture).
+// Kernel attributes (none needed at present; kept for callers that set up once before a capture).
 cudaError_t atrous_setup();
 // RGBA in -> RGBA out; scratch: plan.bytes of device memory, 256-byte aligned.
 cudaError_t atrous_run(const AtrousPlan& plan, const Img& in, const Img& out, bool f16, void* scratch,
