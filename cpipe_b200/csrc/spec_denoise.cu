@@ -307,6 +307,36 @@ __device__ __forceinline__ void atrous_tile_sums(const float (&acc)[3], float* _
     }
 }
 
+// One tap row's raw words for one column: the three level planes, or the
+// input pixel (converted to c_0 by value()).
+template <class T, bool FIRST>
+struct AtrousRaw {
+    float v[3];
+    __device__ __forceinline__ void fetch(const Img&, const float* __restrict__ cin, long long npx, int w, int x, int y) {
+        const float* p = cin + (unsigned)(y * w + x);
+        v[0] = __ldg(p);
+        v[1] = __ldg(p + npx);
+        v[2] = __ldg(p + 2 * npx);
+    }
+    __device__ __forceinline__ void value(float (&o)[3]) const {
+        o[0] = v[0];
+        o[1] = v[1];
+        o[2] = v[2];
+    }
+};
+template <class T>
+struct AtrousRaw<T, true> {
+    typename std::conditional<std::is_same<T, float>::value, float4, uint2>::type u;
+    __device__ __forceinline__ void fetch(const Img& in, const float*, long long, int, int x, int y) {
+        u = *reinterpret_cast<const decltype(u)*>(px<const T>(in, x, y));
+    }
+    __device__ __forceinline__ void value(float (&o)[3]) const {
+        const Rgba p = load_rgba(reinterpret_cast<const T*>(&u));
+        o[0] = (p.r + 2.0F * p.g + p.b) * 0.25F;
+        o[1] = p.r - p.b;
+        o[2] = p.g - (p.r + p.b) * 0.5F;
+    }
+};
 template <class T, bool FIRST>
 __device__ __forceinline__ void atrous_tap(const Img& in, const float* __restrict__ cin, long long npx, int w, int x,
                                            int y, float (&v)[3]) {
@@ -350,12 +380,15 @@ __global__ void __launch_bounds__(kAtThreads) atrous_walk_kernel(Img in, const f
         float ring[5][3];  // c_j at rows y - 2s .. y + 2s (clamped) of this column
         const int yb = phi + s * k0;
 #pragma unroll
-        for (int m = 0; m < 4; ++m) atrous_tap<T, FIRST>(in, cin, npx, w, xc, clampi(yb + (m - 2) * s, 0, h - 1), ring[m]);
+        for (int m = 0; m < 5; ++m) atrous_tap<T, FIRST>(in, cin, npx, w, xc, clampi(yb + (m - 2) * s, 0, h - 1), ring[m]);
         for (int k = 0; k < nk; ++k) {
             const int y = yb + s * k;
-            atrous_tap<T, FIRST>(in, cin, npx, w, xc, min(y + 2 * s, h - 1), ring[4]);
 #pragma unroll
             for (int c = 0; c < 3; ++c) vrow[c][t] = b3(ring[0][c], ring[1][c], ring[2][c], ring[3][c], ring[4][c]);
+            // the next step's new row, in flight across this step's barriers
+            // (raw words; converted after them)
+            AtrousRaw<T, FIRST> nxt;
+            nxt.fetch(in, cin, npx, w, xc, min(y + 3 * s, h - 1));
             __syncthreads();
             if (out) {
                 float* dst = cout + (unsigned)(y * w + x);
@@ -373,6 +406,7 @@ __global__ void __launch_bounds__(kAtThreads) atrous_walk_kernel(Img in, const f
             for (int m = 0; m < 4; ++m)
 #pragma unroll
                 for (int c = 0; c < 3; ++c) ring[m][c] = ring[m + 1][c];
+            nxt.value(ring[4]);
         }
     }
     atrous_tile_sums(acc, part);
