@@ -356,13 +356,14 @@ def spec_form(peak_gbs, weights):
     return out
 
 
-def config1_chain(peak_gbs):
+def config1_chain(peak_gbs, with_cpu=False):
     """The plain chain at its configured size (2016x1512 RGGB 12-bit, black 64,
     WB (2, 1, 1.6), RCD, camera matrix, denoise.bm3d with sigma from the noise
     model, wavelet, filmic, identity+gamma 33^3 LUT): CUDA events around 50
     frames after 5, inputs rotating through 8 raw frames and 4 outputs (147 MB,
     more than L2); bytes = the raw frame read and the RGBA16F frame written once
-    (10 B/px)."""
+    (10 B/px).  with_cpu: also the reference's CPU chain on the same frame
+    (cpu_reference_ms, on the host's cores)."""
     import numpy as np
     from cpipe_b200 import _abi as A
     from cpipe_b200.chain import Chain, ChainConfig
@@ -400,9 +401,16 @@ def config1_chain(peak_gbs):
     for p in d_raw + d_out:
         L.cpipe_cuda_device_free(p)
     gbs = 10.0 * w * h / (t * 1e-3) / 1e9
-    return {"workload": cfg.name, "frame": f"{w}x{h} RGGB 12-bit", "ms_per_frame": round(t, 4),
-            "mp_per_s": round(w * h / 1e6 / (t * 1e-3), 1), "bytes_per_px": 10, "achieved_gbs": round(gbs, 1),
-            "frac": round(gbs / peak_gbs, 4)}
+    out = {"workload": cfg.name, "frame": f"{w}x{h} RGGB 12-bit", "ms_per_frame": round(t, 4),
+           "mp_per_s": round(w * h / 1e6 / (t * 1e-3), 1), "bytes_per_px": 10, "achieved_gbs": round(gbs, 1),
+           "frac": round(gbs / peak_gbs, 4)}
+    if with_cpu:
+        # the reference's CPU chain on the same frame (one run after one untimed run)
+        run, threads, _ = reference_cpu_chain(cfg)
+        run()
+        out["cpu_reference_ms"] = round(run(), 1)
+        out["cpu_threads"] = threads
+    return out
 
 
 def finishing_stages():
@@ -758,7 +766,7 @@ def b200_arm(args):
         line["batched_form"] = batched_form(weights)
         line["spec_form"] = spec_form(peak_gbs, weights)
         line["finishing_stages"] = finishing_stages()
-        line["config1_chain"] = config1_chain(peak_gbs)
+        line["config1_chain"] = config1_chain(peak_gbs, with_cpu=not args.no_cpu_baseline)
         line["dng_ingest"] = dng_ingest(peak_gbs)
         line["node_roofline"] = {"peak_gbs": peak_gbs, "peak_kind": gbs_kind,
                                  "note": "each node's filter alone, 12 MP device buffers, bytes = its input and "
