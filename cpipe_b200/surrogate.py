@@ -18,10 +18,14 @@ activations, FP32 accumulation) that stands in for the two-stage BM3D
 No reference counterpart exists (the reference's AI denoise node is planned,
 docs/research/08-ai-isp-algorithms.md:37, but not implemented).
 
-    python -m cpipe_b200.surrogate train --pairs 80000 --steps 40000 --lr 1e-3 --out weights.cpsn
+    python -m cpipe_b200.surrogate train --pairs 80000 --steps 40000 --lr 1e-3 --out base.cpsn
+    python -m cpipe_b200.surrogate train --init base.cpsn --pairs 80000 --steps 20000 --lr 3e-4 \
+        --noise-a-max 0.015 --seed 7 --out weights.cpsn
 
-(the committed cpipe_b200/weights/surrogate_bm3d.cpsn was made by this command;
-its report is surrogate_bm3d.report.json beside it)
+(the committed cpipe_b200/weights/surrogate_bm3d.cpsn was made by these two
+commands: the second fine-tunes on noise up to a = 0.015, past the 0.01 top of
+the batched workload's mix; its report, with the base run's, is
+surrogate_bm3d.report.json beside it)
 """
 import argparse
 import ctypes as C
@@ -274,7 +278,7 @@ class PairGenerator:
         if st:
             raise CpipeError(st, "bm3d " + last_error())
 
-    def dataset(self, count, rng):
+    def dataset(self, count, rng, noise_a=NOISE_A):
         """count tiles in shuffled order: (noisy, target) DeviceArrays of
         [count][tile][tile][4] binary16 and the per-tile (a, b)."""
         tb = self.tile * self.tile * 8
@@ -284,7 +288,7 @@ class PairGenerator:
         k, f = 0, 0
         self.skipped = 0
         while k < count:
-            a = float(np.exp(rng.uniform(np.log(NOISE_A[0]), np.log(NOISE_A[1]))))
+            a = float(np.exp(rng.uniform(np.log(noise_a[0]), np.log(noise_a[1]))))
             b = float(np.exp(rng.uniform(np.log(NOISE_B[0]), np.log(NOISE_B[1]))))
             kind = self.kinds[int(rng.integers(len(self.kinds)))]
             bits = self.bits[int(rng.integers(len(self.bits)))]
@@ -346,12 +350,15 @@ def evaluate(sg, noisy, target, ab, first, count, tile=256, batch=16):
     return {k: float(np.mean(v)) for k, v in res.items()}
 
 
-def train(pairs=20000, steps=4000, batch=16, lr=5e-4, seed=1, tile=256, val=256, log=print, init=None):
-    """Generate `pairs` training tiles on the GPU and train; returns (blob, report)."""
+def train(pairs=20000, steps=4000, batch=16, lr=5e-4, seed=1, tile=256, val=256, log=print, init=None,
+          noise_a=NOISE_A):
+    """Generate `pairs` training tiles on the GPU and train; returns (blob, report).
+    init: a weights blob to start from; noise_a: the range of the noise
+    model's a the tiles are drawn from (log-uniform)."""
     rng = np.random.default_rng(seed)
     t0 = time.time()
     gen = PairGenerator(tile=tile)
-    noisy, target, ab = gen.dataset(pairs + val, rng)
+    noisy, target, ab = gen.dataset(pairs + val, rng, noise_a)
     gen.close()
     t_data = time.time() - t0
     skipped = gen.skipped
@@ -382,6 +389,7 @@ def train(pairs=20000, steps=4000, batch=16, lr=5e-4, seed=1, tile=256, val=256,
     log(f"after: {after}; training {t_train:.1f} s ({1000 * t_train / steps:.2f} ms/step)")
     blob = sg.export()
     report = dict(pairs=pairs, held_out=val, tile=tile, steps=steps, batch=batch, lr=lr, seed=seed,
+                  noise_a=list(noise_a), fine_tuned=init is not None,
                   skipped_frames=skipped, data_seconds=t_data, train_seconds=t_train, before=before, after=after, history=history)
     sg.close()
     for d in (noisy, target, bn, bt):
@@ -400,9 +408,14 @@ def _main():
     t.add_argument("--seed", type=int, default=1)
     t.add_argument("--out", default=DEFAULT_WEIGHTS)
     t.add_argument("--report", default=None)
+    t.add_argument("--init", default=None, help="start from these weights (fine-tuning) instead of a random init")
+    t.add_argument("--noise-a-max", type=float, default=NOISE_A[1],
+                   help="upper end of the training noise model's a (log-uniform from %g)" % NOISE_A[0])
     args = ap.parse_args()
     assert A.lib().cpipe_cuda_device_count() > 0, "no CUDA device"
-    blob, report = train(args.pairs, args.steps, args.batch, args.lr, args.seed)
+    init = load_weights(args.init) if args.init else None
+    blob, report = train(args.pairs, args.steps, args.batch, args.lr, args.seed, init=init,
+                         noise_a=(NOISE_A[0], args.noise_a_max))
     os.makedirs(os.path.dirname(os.path.abspath(args.out)), exist_ok=True)
     with open(args.out, "wb") as f:
         f.write(blob)
