@@ -188,7 +188,7 @@ __global__ void __launch_bounds__(kGsThreads) gsp_ab_kernel(Img in, GsPlanes p, 
 }
 
 template <class T>
-__global__ void __launch_bounds__(kGsThreads) gsp_out_kernel(Img in, Img out, GsPlanes p) {
+__global__ void __launch_bounds__(kGsThreads, 4) gsp_out_kernel(Img in, Img out, GsPlanes p) {
     extern __shared__ float4 gsm4[];
     const int R = p.R, D = 2 * R + 1, SR = kGsTH + 2 * R, SC = kGsTW + 2 * R, PV = gs_pitch(R);
     float2* sab = reinterpret_cast<float2*>(gsm4);
@@ -360,7 +360,7 @@ __device__ __forceinline__ void atrous_tap(const Img& in, const float* __restric
 // warm-up rows per walk).  Per output: the vertical B3 taps first, then the
 // horizontal ones, each b3(t[-2s], t[-s], t[0], t[s], t[2s]); the first level
 // (s = 1) reads c_0 = (Y, Co, Cg) from the input frame.
-constexpr int kAtSeg = 64;  // steps per walk
+constexpr int kAtSeg = 32;  // steps per walk
 __host__ __device__ constexpr int atrous_walk_cols(int s) { return kAtThreads - 4 * s; }
 template <class T, bool FIRST>
 __global__ void __launch_bounds__(kAtThreads) atrous_walk_kernel(Img in, const float* __restrict__ cin,
