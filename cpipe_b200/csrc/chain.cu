@@ -1198,6 +1198,7 @@ struct Frame {
     Img tone_in;                 // mid1, or the denoiser's output (mid0) when a denoiser runs between
     RawParams raw;
     WarpDev warp;
+    WarpTaps taps;      // the frame chain's per-pixel warp taps (null when it evaluates the warp per pixel)
     ColorParams color;
     ToneParams tone;
     int t1x, t2x, t3x;  // work items per row, per stage
@@ -1272,9 +1273,15 @@ __global__ void __launch_bounds__(128) batch_color_kernel(const Frame* __restric
         const int local = next_item(frames, s_prefix, n, t, &s_f, &cur);
         const int rows = s_f.rows2;
         const int x = (local % s_f.t2x) * 128 + (int)threadIdx.x, y0 = (local / s_f.t2x) * rows;
-        if (x < s_f.mid1.w)
-            for (int r = 0; r < rows && y0 + r < s_f.mid1.h; ++r)
-                warp_wb_cm_px<__half, true, WARP>(s_f.mid0, s_f.mid1, s_f.warp, s_f.color, x, y0 + r);
+        if (x < s_f.mid1.w) {
+            if (WARP && s_f.taps.ixy != nullptr) {  // the tap table, as the frame's own chain reads it
+                for (int r = 0; r < rows && y0 + r < s_f.mid1.h; ++r)
+                    warp_wb_cm_px<__half, true, 2>(s_f.mid0, s_f.mid1, s_f.warp, s_f.color, x, y0 + r, s_f.taps);
+            } else {
+                for (int r = 0; r < rows && y0 + r < s_f.mid1.h; ++r)
+                    warp_wb_cm_px<__half, true, WARP>(s_f.mid0, s_f.mid1, s_f.warp, s_f.color, x, y0 + r);
+            }
+        }
     }
 }
 
@@ -1493,6 +1500,7 @@ cpipe_cuda_batch* cpipe_cuda_batch_create(const cpipe_cuda_chain_config* cfgs, s
         f.tone_in = b->denoise_mode != 0 ? f.mid0 : f.mid1;
         f.raw = ch->raw;
         f.warp = ch->warp;
+        f.taps = WarpTaps{ch->d_taps_ixy, ch->d_taps_tx, ch->d_taps_ty};
         f.color = ch->color;
         f.tone = ch->tone;
         f.t1x = (w + kDmTW - 1) / kDmTW;
