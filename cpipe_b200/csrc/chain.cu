@@ -1338,7 +1338,9 @@ namespace {
 using cpb::batch::Frame;
 
 int batch_launch_stage(cpipe_cuda_batch* b, int stage, cudaStream_t st, bool timed = false) {
-    const int grid = kSmCount * b->per_sm[stage];
+    // per_sm 0: one work item per CTA (the queue's limit case: a grid of all items)
+    const int items = b->prefix[(size_t)stage * (b->n + 1) + b->n];
+    const int grid = b->per_sm[stage] > 0 ? kSmCount * b->per_sm[stage] : (items > 0 ? items : 1);
     const int* pf = b->d_prefix + stage * (b->n + 1);
     if (stage == 0) {
         if (b->algo == 0) cpb::batch::batch_raw_kernel<0><<<grid, 256, 0, st>>>(b->d_frames, pf, b->n);
@@ -1576,7 +1578,7 @@ int cpipe_cuda_batch_autotune(cpipe_cuda_batch* b, const void* const* d_raw, voi
     if (s != CPIPE_OK) return s;
     if (b->graph) cudaGraphExecDestroy(b->graph);
     b->graph = nullptr;
-    static const int cand[3][6] = {{1, 2, 3, 4, 6, 8}, {2, 4, 8, 12, 16, 24}, {1, 2, 3, 4, 6, 8}};
+    static const int cand[3][7] = {{1, 2, 3, 4, 6, 8, 0}, {2, 4, 8, 12, 16, 24, 0}, {1, 2, 3, 4, 6, 8, 0}};
     cudaEvent_t e0, e1;
     if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) return CPIPE_INTERNAL_ERROR;
     s = batch_launch(b, st);  // fills every stage's input once

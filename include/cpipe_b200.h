@@ -443,9 +443,9 @@ int cpipe_cuda_batch_autotune(cpipe_cuda_batch* batch, const void* const* d_raw,
                               int per_sm_out[3]);
 /* Frame i's single-frame chain (the same node parameters; for per-frame runs). */
 cpipe_cuda_chain* cpipe_cuda_batch_frame_chain(cpipe_cuda_batch* batch, size_t i);
-/* The schedule in use: persistent CTAs per SM of the three stages and the rows
- * of a stage-2 work item (128 pixels wide); both set by
- * cpipe_cuda_batch_autotune. */
+/* The schedule in use: persistent CTAs per SM of the three stages (0: one
+ * work item per CTA, a grid of all the stage's items) and the rows of a
+ * stage-2 work item (128 pixels wide); both set by cpipe_cuda_batch_autotune. */
 int cpipe_cuda_batch_schedule(cpipe_cuda_batch* batch, int per_sm[3], int* rows_per_item);
 /* Completion time of each frame in the last cpipe_cuda_batch_run on `stream`,
  * in ms after the run's first kernel started: the device clock is read when the
