@@ -674,8 +674,9 @@ __global__ void __launch_bounds__(32 * kTcWarps, 3) bm3d_filter_tc_kernel(Filter
     float* s_aux = s_img + (STAGE == 2 ? 2 : 1) * FP;  // staging buffers (stage 1: at the flush the row-filtered map)
     float* s_k = s_aux + (STAGE == 2 ? kTcWarps * SB * kStageStride : max(FP, kTcWarps * SB * kStageStride));
     float* s_k1 = s_k + 64;
-    float* s_wgt = s_k1 + 8;
-    uint32_t* s_list = reinterpret_cast<uint32_t*>((reinterpret_cast<uintptr_t>(s_wgt + 64) + 15) & ~(uintptr_t)15);
+    float* s_wgt = s_k1 + 8;  // one aggregation weight per reference block of the tile
+    uint32_t* s_list = reinterpret_cast<uint32_t*>((reinterpret_cast<uintptr_t>(s_wgt + kRefTile * kRefTile) + 15) &
+                                                   ~(uintptr_t)15);
     uint32_t* s_cnt = s_list + kRefTile * kRefTile * 16;
     int* s_off = reinterpret_cast<int*>(s_cnt + kRefTile * kRefTile);  // [warp][16] block offsets of the group
     const float* gz = a.noisy + (long long)c * a.npx;
@@ -907,7 +908,7 @@ size_t filter_tc_smem(const Bm3dPlan& p, int stage) {
     const size_t fp = (size_t)p.fw * tile_pitch(p.fw);
     const size_t stg = (size_t)kTcWarps * tc_stage_blocks(stage) * kStageStride;
     const size_t aux = stage == 2 ? stg : std::max(fp, stg);
-    const size_t floats = fp + (stage == 2 ? 2 : 1) * fp + aux + 64 + 8 + 64;
+    const size_t floats = fp + (stage == 2 ? 2 : 1) * fp + aux + 64 + 8 + kRefTile * kRefTile;  // + Kaiser, its 1D factor, weights
     return sizeof(float) * floats + 16 + sizeof(uint32_t) * kRefTile * kRefTile * 17 + sizeof(int) * kTcWarps * 16;
 }
 
