@@ -456,8 +456,9 @@ def finishing_stages():
 def dng_ingest(peak_gbs):
     """DNG ingest of a 4032x3024 frame: the strip unpack alone from a
     device-resident strip (16-bit words; 12-bit packed), bytes = strip read +
-    plane written once; and cpipe_cuda_dng_decode from the file image in
-    pageable host memory (parse, strip upload, unpack).  CUDA events around 20
+    plane written once; cpipe_cuda_dng_decode from the file image in
+    pageable host memory (parse, strip upload, unpack); and the same decode of
+    a lossless-JPEG (Compression 7) file of the benchmark frame's mosaic.  CUDA events around 20
     calls after 3, the unpack over four strip / plane sets in turn (192 MB for
     16-bit, more than L2)."""
     import numpy as np
@@ -516,10 +517,24 @@ def dng_ingest(peak_gbs):
                               "file_bytes": len(data)}
         for d in d_strips:
             L.cpipe_cuda_device_free(d)
+    # Compression 7: the 12 MP benchmark frame's mosaic (10-bit) as 256x256
+    # lossless-JPEG tiles (predictor 1, two components per JPEG line, as DNG
+    # writers store CFA data), decoded from the file image in host memory
+    from cpipe_b200.chain import ChainConfig
+    from cpipe_b200.dng_synth import lj92_tiles
+    raw = ChainConfig.full_12mp().make_raw()
+    data = build_dng(width=w, height=h, bits=10, tile=(256, 256), segments=lj92_tiles(raw, 10, 256, 256))
+    ms = timed(lambda: L.cpipe_cuda_dng_decode(data, len(data), d_raw, w * h * 2, None), n=10)
+    got = np.empty((h, w), np.uint16)
+    assert L.cpipe_cuda_memcpy_d2h(got.ctypes.data, d_raw, got.nbytes) == 0
+    out["lossless_jpeg"] = {"decode_from_host_ms": round(ms, 3), "mp_per_s": round(w * h / 1e6 / (ms * 1e-3), 1),
+                            "file_bytes": len(data), "tiles": "256x256 (192), predictor 1",
+                            "exact": bool(np.array_equal(got, raw))}
     for d in d_raws:
         L.cpipe_cuda_device_free(d)
     out["note"] = ("decode_from_host_ms includes the pageable host-to-device copy of the strip, "
-                   "which bounds it; the unpack is the kernel's share")
+                   "which bounds it; the unpack is the kernel's share; lossless_jpeg: one thread per tile "
+                   "decodes its Huffman stream")
     return out
 
 

@@ -177,3 +177,75 @@ def _build_segmented(width, height, segments, bits, tile, rows_per_strip, strip_
             where = struct.unpack_from("<I", out, e + 8)[0]
             out[where:where + len(vals)] = vals
     return bytes(out)
+
+
+# ------------------------------------------------------- lossless-JPEG segments
+# Code lengths of difference categories 0..16 for the writer below: a fixed,
+# prefix-free table (Kraft sum 0.875, so no code is all ones) that favours the
+# small categories of smooth raw data.  Decoders read it from the DHT segment.
+_LJ_LENGTHS = (2, 3, 3, 3, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15)
+
+
+def lj92_segment(samples, bits, components=2):
+    """One lossless-JPEG stream (ITU-T T.81 process 14, DNG Compression 7) for a
+    raster of uint16 samples laid out as JPEG lines of X * components samples:
+    predictor 1, no restart intervals, one fixed Huffman table.  For synthetic
+    benchmark and test files; `samples` is (rows, X * components)."""
+    a = np.asarray(samples, np.int64)
+    rows, cols = a.shape
+    X = cols // components
+    r = a.reshape(rows, X, components)
+    pred = np.empty_like(r)
+    pred[0, 0] = 1 << (bits - 1)
+    pred[0, 1:] = r[0, :-1]
+    pred[1:, 0] = r[:-1, 0]
+    pred[1:, 1:] = r[1:, :-1]
+    diff = (r - pred) & 0xFFFF
+    diff = np.where(diff > 0x8000, diff - 0x10000, diff).reshape(-1)
+    mag = np.abs(diff)
+    cat = np.where(mag == 0, 0, np.frexp(mag.astype(np.float64))[1]).astype(np.int64)
+    cat[mag == 32768] = 16
+    # canonical codes of the fixed lengths, symbols in (length, symbol) order
+    order = sorted(range(17), key=lambda s: (_LJ_LENGTHS[s], s))
+    code_of, code_len = np.zeros(17, np.int64), np.zeros(17, np.int64)
+    code, prev = 0, _LJ_LENGTHS[order[0]]
+    for sym in order:
+        code <<= _LJ_LENGTHS[sym] - prev
+        prev = _LJ_LENGTHS[sym]
+        code_of[sym], code_len[sym] = code, prev
+        code += 1
+    n_extra = np.where(cat < 16, cat, 0)
+    extra = np.where(diff >= 0, diff, diff + (1 << cat) - 1) & ((1 << n_extra) - 1)
+    # one field per sample: the category's code followed by its extra bits
+    field = (code_of[cat] << n_extra) | extra
+    flen = code_len[cat] + n_extra
+    end = np.cumsum(flen)
+    nbits = int(end[-1]) if end.size else 0
+    total = (nbits + 7) // 8 * 8
+    bitbuf = np.ones(total, np.uint8)  # the tail pads with one bits
+    start = end - flen
+    for k in range(int(flen.max()) if flen.size else 0):
+        sel = flen > k
+        bitbuf[start[sel] + k] = (field[sel] >> (flen[sel] - 1 - k)) & 1
+    data = np.packbits(bitbuf)
+    data = np.insert(data, np.nonzero(data == 0xFF)[0] + 1, 0)  # byte stuffing
+    counts = [0] * 16
+    for sym in range(17):
+        counts[_LJ_LENGTHS[sym] - 1] += 1
+    marker = lambda m, body: bytes((0xFF, m)) + struct.pack(">H", len(body) + 2) + body
+    dht = bytes([0x00]) + bytes(counts) + bytes(order)
+    sof = struct.pack(">BHHB", bits, rows, X, components) + b"".join(bytes((c + 1, 0x11, 0))
+                                                                     for c in range(components))
+    sos = bytes([components]) + b"".join(bytes((c + 1, 0x00)) for c in range(components)) + bytes((1, 0, 0))
+    return (b"\xff\xd8" + marker(0xC4, dht) + marker(0xC3, sof) + marker(0xDA, sos) + data.tobytes() + b"\xff\xd9")
+
+
+def lj92_tiles(img, bits, tile_w, tile_h, components=2):
+    """lj92_segment of every tile_w x tile_h tile of `img`, row-major, the edge
+    tiles padded by repeating the last row / column (DNG tiles are whole)."""
+    img = np.asarray(img, np.uint16)
+    h, w = img.shape
+    across, down = -(-w // tile_w), -(-h // tile_h)
+    pad = np.pad(img, ((0, down * tile_h - h), (0, across * tile_w - w)), mode="edge")
+    return [lj92_segment(pad[ty * tile_h:(ty + 1) * tile_h, tx * tile_w:(tx + 1) * tile_w], bits, components)
+            for ty in range(down) for tx in range(across)]

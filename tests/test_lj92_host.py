@@ -50,3 +50,18 @@ def test_parse_finds_segments():
                            segments=L.encode_tiles(img, 12, 32, 16))
     assert dng.parse(only_tiles)[0] == A.FAILED
     assert od.parse(only_tiles)[0] == A.FAILED
+
+
+def test_writer_segments_round_trip():
+    """The package's lossless-JPEG writer (dng_synth.lj92_segment, used for
+    benchmark files) decodes back exactly through the oracle decoder."""
+    import numpy as np
+    import oracle_lj92 as O
+    from cpipe_b200.dng_synth import lj92_segment
+    rng = np.random.default_rng(11)
+    for h, w, bits, nf in [(16, 32, 12, 2), (7, 10, 16, 2), (9, 9, 10, 1), (40, 64, 14, 2)]:
+        noise = rng.integers(0, 1 << bits, (h, w)).astype(np.uint16)
+        ramp = (np.add.outer(np.arange(h), 3 * np.arange(w)) % (1 << bits)).astype(np.uint16)
+        for img in (noise, ramp):
+            got = np.asarray(O.decode(lj92_segment(img, bits, nf), w, h)).reshape(h, w)
+            np.testing.assert_array_equal(got, img)
