@@ -226,6 +226,7 @@ EXPORTS = [
     "cpipe_cuda_copy", "cpipe_cuda_filters", "cpipe_cuda_find_filter",
     "cpipe_cuda_color_3d_lut_noalloc",
     "cpipe_dng_parse", "cpipe_cuda_dng_decode", "cpipe_cuda_dng_unpack", "cpipe_cuda_lj92_decode",
+    "cpipe_cuda_lj92_last_stats",
     "cpipe_b200_node_descs", "cpipe_b200_find_node",
     "cpipe_cuda_scene_raw", "cpipe_cuda_scene_raw_cfa", "cpipe_surrogate_blob_size", "cpipe_surrogate_create", "cpipe_surrogate_destroy", "cpipe_surrogate_export",
     "cpipe_surrogate_denoise", "cpipe_surrogate_set_engine", "cpipe_surrogate_check", "cpipe_surrogate_profile", "cpipe_surrogate_train_step", "cpipe_surrogate_gradients",
@@ -316,6 +317,7 @@ def lib():
         "cpipe_cuda_dng_decode": (i32, [vp, sz, vp, sz, C.POINTER(DngInfo)]),
         "cpipe_cuda_dng_unpack": (i32, [vp, sz, u32, u32, u32, vp]),
         "cpipe_cuda_lj92_decode": (i32, [vp, vp, u32, u32, u32, u32, u32, u32, vp]),
+        "cpipe_cuda_lj92_last_stats": (i32, [C.POINTER(C.c_uint64), u32]),
         "cpipe_cuda_chain_run": (i32, [vp, vp, vp, vp]), "cpipe_cuda_chain_run_host": (i32, [vp, vp, vp, vp]),
         "cpipe_cuda_chain_run_host_frames": (i32, [vp, vp, vp, i32, vp]),
         "cpipe_cuda_pinned_alloc": (i32, [sz, C.POINTER(vp)]), "cpipe_cuda_pinned_free": (None, [vp]),

@@ -8,6 +8,7 @@ AsShotNeutral {1, 2, 3}, illuminants 21 / 17, a full active area), so the
 expectations of tests/unit/test_dng_reader.cpp apply to these files.  Layout:
 header, IFD0 at offset 8 (entries sorted by tag), then the value sections.
 """
+import heapq
 import struct
 
 import numpy as np
@@ -186,11 +187,64 @@ def _build_segmented(width, height, segments, bits, tile, rows_per_strip, strip_
 _LJ_LENGTHS = (2, 3, 3, 3, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15)
 
 
-def lj92_segment(samples, bits, components=2):
+def _huffman_lengths(freq):
+    """Code lengths of at most 16 bits for the categories with freq > 0:
+    Huffman's construction over them plus one reserved, least frequent point
+    (so that no code is all ones), lengths over 16 folded back and the reserved
+    point then dropped from the longest length, as T.81 Annex K.2 describes."""
+    syms = [s for s in range(17) if freq[s] > 0] or [0]
+    heap = [(int(freq[s]), i, (s,)) for i, s in enumerate(syms)] + [(0, len(syms), (17,))]
+    heapq.heapify(heap)
+    depth = dict.fromkeys(list(syms) + [17], 0)
+    k = len(heap)
+    while len(heap) > 1:
+        fa, _, a = heapq.heappop(heap)
+        fb, _, b = heapq.heappop(heap)
+        for s in a + b:
+            depth[s] += 1
+        heapq.heappush(heap, (fa + fb, k, a + b))
+        k += 1
+    bits = [0] * 64
+    for d in depth.values():
+        bits[d] += 1
+    for i in range(63, 16, -1):
+        while bits[i] > 0:
+            j = i - 2
+            while bits[j] == 0:
+                j -= 1
+            bits[i] -= 2
+            bits[i - 1] += 1
+            bits[j + 1] += 2
+            bits[j] -= 1
+    longest = max(i for i in range(17) if bits[i])
+    bits[longest] -= 1
+    order = iter(sorted(syms, key=lambda s: (-int(freq[s]), s)))
+    return {next(order): n for n in range(1, 17) for _ in range(bits[n])}
+
+
+def _canonical_codes(lengths):
+    """(code, length) arrays over categories 0..16 and the DHT symbol order."""
+    order = sorted(lengths, key=lambda s: (lengths[s], s))
+    code_of, code_len = np.zeros(17, np.int64), np.zeros(17, np.int64)
+    code, prev = 0, lengths[order[0]]
+    for sym in order:
+        code <<= lengths[sym] - prev
+        prev = lengths[sym]
+        code_of[sym], code_len[sym] = code, prev
+        code += 1
+    counts = [0] * 16
+    for sym in order:
+        counts[lengths[sym] - 1] += 1
+    return code_of, code_len, bytes(counts) + bytes(order)
+
+
+def lj92_segment(samples, bits, components=2, tables="fixed"):
     """One lossless-JPEG stream (ITU-T T.81 process 14, DNG Compression 7) for a
     raster of uint16 samples laid out as JPEG lines of X * components samples:
-    predictor 1, no restart intervals, one fixed Huffman table.  For synthetic
-    benchmark and test files; `samples` is (rows, X * components)."""
+    predictor 1, no restart intervals.  tables="fixed": one fixed Huffman table
+    for every component; "per_component": an optimal table per component from
+    its own category counts, as DNG writers emit.  For synthetic benchmark and
+    test files; `samples` is (rows, X * components)."""
     a = np.asarray(samples, np.int64)
     rows, cols = a.shape
     X = cols // components
@@ -205,20 +259,22 @@ def lj92_segment(samples, bits, components=2):
     mag = np.abs(diff)
     cat = np.where(mag == 0, 0, np.frexp(mag.astype(np.float64))[1]).astype(np.int64)
     cat[mag == 32768] = 16
-    # canonical codes of the fixed lengths, symbols in (length, symbol) order
-    order = sorted(range(17), key=lambda s: (_LJ_LENGTHS[s], s))
-    code_of, code_len = np.zeros(17, np.int64), np.zeros(17, np.int64)
-    code, prev = 0, _LJ_LENGTHS[order[0]]
-    for sym in order:
-        code <<= _LJ_LENGTHS[sym] - prev
-        prev = _LJ_LENGTHS[sym]
-        code_of[sym], code_len[sym] = code, prev
-        code += 1
+    comp = np.arange(diff.size) % components
+    if tables == "fixed":
+        lengths = [dict(enumerate(_LJ_LENGTHS))]
+    elif tables == "per_component":
+        lengths = [_huffman_lengths(np.bincount(cat[comp == c], minlength=17)) for c in range(components)]
+    else:
+        raise ValueError("tables must be 'fixed' or 'per_component'")
+    made = [_canonical_codes(ln) for ln in lengths]
+    code_of = np.stack([m[0] for m in made])
+    code_len = np.stack([m[1] for m in made])
+    tsel = comp if len(made) > 1 else np.zeros_like(comp)
     n_extra = np.where(cat < 16, cat, 0)
     extra = np.where(diff >= 0, diff, diff + (1 << cat) - 1) & ((1 << n_extra) - 1)
     # one field per sample: the category's code followed by its extra bits
-    field = (code_of[cat] << n_extra) | extra
-    flen = code_len[cat] + n_extra
+    field = (code_of[tsel, cat] << n_extra) | extra
+    flen = code_len[tsel, cat] + n_extra
     end = np.cumsum(flen)
     nbits = int(end[-1]) if end.size else 0
     total = (nbits + 7) // 8 * 8
@@ -229,23 +285,21 @@ def lj92_segment(samples, bits, components=2):
         bitbuf[start[sel] + k] = (field[sel] >> (flen[sel] - 1 - k)) & 1
     data = np.packbits(bitbuf)
     data = np.insert(data, np.nonzero(data == 0xFF)[0] + 1, 0)  # byte stuffing
-    counts = [0] * 16
-    for sym in range(17):
-        counts[_LJ_LENGTHS[sym] - 1] += 1
     marker = lambda m, body: bytes((0xFF, m)) + struct.pack(">H", len(body) + 2) + body
-    dht = bytes([0x00]) + bytes(counts) + bytes(order)
+    dht = b"".join(bytes([t]) + m[2] for t, m in enumerate(made))
     sof = struct.pack(">BHHB", bits, rows, X, components) + b"".join(bytes((c + 1, 0x11, 0))
                                                                      for c in range(components))
-    sos = bytes([components]) + b"".join(bytes((c + 1, 0x00)) for c in range(components)) + bytes((1, 0, 0))
+    td = [c if len(made) > 1 else 0 for c in range(components)]
+    sos = bytes([components]) + b"".join(bytes((c + 1, td[c] << 4)) for c in range(components)) + bytes((1, 0, 0))
     return (b"\xff\xd8" + marker(0xC4, dht) + marker(0xC3, sof) + marker(0xDA, sos) + data.tobytes() + b"\xff\xd9")
 
 
-def lj92_tiles(img, bits, tile_w, tile_h, components=2):
+def lj92_tiles(img, bits, tile_w, tile_h, components=2, tables="fixed"):
     """lj92_segment of every tile_w x tile_h tile of `img`, row-major, the edge
     tiles padded by repeating the last row / column (DNG tiles are whole)."""
     img = np.asarray(img, np.uint16)
     h, w = img.shape
     across, down = -(-w // tile_w), -(-h // tile_h)
     pad = np.pad(img, ((0, down * tile_h - h), (0, across * tile_w - w)), mode="edge")
-    return [lj92_segment(pad[ty * tile_h:(ty + 1) * tile_h, tx * tile_w:(tx + 1) * tile_w], bits, components)
-            for ty in range(down) for tx in range(across)]
+    return [lj92_segment(pad[ty * tile_h:(ty + 1) * tile_h, tx * tile_w:(tx + 1) * tile_w], bits, components,
+                         tables) for ty in range(down) for tx in range(across)]

@@ -95,12 +95,25 @@ int cpipe_cuda_dng_unpack(const uint8_t* d_strip, size_t strip_bytes, uint32_t w
  * seg_w x seg_h samples filled row after row from the JPEG lines (X * Nf
  * samples each) and cropped at the image edges.  Headers are parsed on the
  * host (SOF3, DHT, DRI, SOS; 1-4 components, predictors 1-7, restart
- * intervals, point transform); one GPU thread decodes each segment.
+ * intervals, point transform).  Segments without restart intervals are
+ * decoded in parallel within each stream (1024-bit chunks decoded
+ * speculatively and chained by warps; predictor 1 reconstructed by prefix
+ * sums); segments with restart intervals by one GPU thread each.
  * CPIPE_FAILED with a message when a header is malformed or a stream does not
  * decode (it never reads past its segment).  No reference counterpart: the
  * reference decodes these through LibRaw. */
 int cpipe_cuda_lj92_decode(const uint8_t* const* streams, const size_t* stream_bytes, uint32_t count, uint32_t across,
                            uint32_t seg_w, uint32_t seg_h, uint32_t width, uint32_t height, uint16_t* d_raw);
+
+/* Figures of the process's last successful lossless-JPEG decode, the first
+ * min(count, 9) of: [0] stream chunks of the parallel path, [1] segments on
+ * the parallel path, [2] on the sequential path, [3] chunks the group walks
+ * decoded again (no speculative path started at the exact state), [4] groups
+ * whose entry the segment walks did not find, [5] chunks those walks decoded
+ * again, [6] chunks the write walks decoded again, [7] bits decoded again,
+ * [8] the longest such decode in bits.  CPIPE_BAD_INDEX when figures is NULL
+ * and count is not 0. */
+int cpipe_cuda_lj92_last_stats(uint64_t* figures, uint32_t count);
 
 #ifdef __cplusplus
 }

@@ -104,3 +104,102 @@ def test_malformed_streams_fail(cuda_device):
     assert gpu_decode([bytes(rst[:k] + rst[k + 2:])], 1, 32, 16, 32, 16)[0] == A.FAILED  # restart marker removed
     # more samples than the segment holds
     assert gpu_decode([bytes(seg)], 1, 16, 16, 16, 16)[0] == A.FAILED
+
+
+def _entropy_span(seg):
+    """(start, end) of the entropy-coded bytes of a one-scan stream."""
+    sos = bytes(seg).index(b"\xff\xda")
+    start = sos + 2 + int.from_bytes(seg[sos + 2:sos + 4], "big")
+    return start, len(seg) - 2  # EOI closes the stream
+
+
+def _stats():
+    """(chunks, chunks decoded again by the write walks, parallel segments,
+    sequential segments) of the last decode."""
+    f = (C.c_uint64 * 9)()
+    assert A.lib().cpipe_cuda_lj92_last_stats(f, 9) == 0
+    return f[0], f[6], f[1], f[2]
+
+
+@pytest.mark.parametrize("tables", ["fixed", "per_component"])
+def test_12mp_tiled_writer_tables(cuda_device, tables):
+    """The benchmark layout (256x256 tiles, two components per JPEG line),
+    with one table and with a table per component as DNG writers emit:
+    bit-exact, every segment on the parallel path, and speculative paths
+    that start at the true state of almost every chunk."""
+    from cpipe_b200.dng_synth import lj92_tiles
+    img = np.random.default_rng(7).integers(0, 1024, (3024, 4032)).astype(np.uint16)
+    img[:1500] = smooth(1500, 4032, 10, 8)
+    segs = lj92_tiles(img, 10, 256, 256, 2, tables)
+    st, got = gpu_decode(segs, 16, 256, 256, 4032, 3024)
+    assert st == 0, A.lib().cpipe_cuda_last_error()
+    np.testing.assert_array_equal(got, img)
+    chunks, redecodes, npar, nser = _stats()
+    assert (npar, nser) == (len(segs), 0)
+    assert chunks > 10000 and redecodes < (0.001 if tables == "fixed" else 0.05) * chunks
+
+
+@pytest.mark.parametrize("tables", ["fixed", "per_component"])
+def test_single_segment_frame(cuda_device, tables):
+    """A whole 12 MP frame in one stream (one strip): thousands of chunk
+    groups chained by one warp."""
+    from cpipe_b200.dng_synth import lj92_segment
+    rng = np.random.default_rng(12)
+    img = smooth(3024, 4032, 14, 5)
+    img[2000:] = rng.integers(0, 1 << 14, (1024, 4032))
+    seg = lj92_segment(img, 14, 2, tables)
+    st, got = gpu_decode([seg], 1, 4032, 3024, 4032, 3024)
+    assert st == 0, A.lib().cpipe_cuda_last_error()
+    np.testing.assert_array_equal(got, img)
+    assert _stats()[2] == 1
+
+
+@pytest.mark.parametrize("nf", [1, 2, 3, 4])
+@pytest.mark.parametrize("bits", [8, 12, 16])
+def test_components_and_depths_parallel(cuda_device, nf, bits):
+    """Per-component tables with 1-4 components and 8-16 bits, noisy enough
+    that the stream spans many chunks."""
+    from cpipe_b200.dng_synth import lj92_segment
+    rng = np.random.default_rng(nf * 100 + bits)
+    img = rng.integers(0, 1 << bits, (96, 120 * nf)).astype(np.uint16)
+    img[:40] = smooth(40, 120 * nf, bits, nf)
+    seg = lj92_segment(img, bits, nf, "per_component")
+    st, got = gpu_decode([seg], 1, 120 * nf, 96, 120 * nf, 96)
+    assert st == 0, A.lib().cpipe_cuda_last_error()
+    np.testing.assert_array_equal(got, img)
+
+
+def test_short_long_and_empty_streams(cuda_device):
+    """Streams that end early (zeros past the data, as a sequential decoder
+    reads), carry bytes after the last sample, or hold no data at all: the
+    same samples as the oracle decoder."""
+    img = np.random.default_rng(3).integers(0, 4096, (64, 128)).astype(np.uint16)
+    seg = bytes(L.encode(img, 12, 1, 2))
+    start, end = _entropy_span(seg)
+    cut = seg[:start + (end - start) // 2]
+    if cut.endswith(b"\xff"):
+        cut = cut[:-1]
+    cases = {
+        "short": cut + b"\xff\xd9",
+        "long": seg[:end] + bytes(range(1, 200)) + b"\xff\xd9",
+        "empty": seg[:start] + b"\xff\xd9",
+        "no_eoi": seg[:end],
+    }
+    for name, s in cases.items():
+        want = L.decode(s, 128, 64)
+        st, got = gpu_decode([s], 1, 128, 64, 128, 64)
+        assert st == 0, (name, A.lib().cpipe_cuda_last_error())
+        np.testing.assert_array_equal(got, want, err_msg=name)
+
+
+def test_invalid_code_mid_stream_fails(cuda_device):
+    """64 one bits in the middle of a long stream hold no code on any path:
+    the parallel decoder reports the segment as not decoding."""
+    img = smooth(512, 512, 12, 4)
+    seg = bytes(L.encode(img, 12, 1, 2))
+    start, end = _entropy_span(seg)
+    mid = start + (end - start) // 2
+    while seg[mid - 1] == 0xFF:
+        mid += 1
+    bad = seg[:mid] + b"\xff\x00" * 8 + seg[mid:]
+    assert gpu_decode([bad], 1, 512, 512, 512, 512)[0] == A.FAILED

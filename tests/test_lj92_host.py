@@ -59,9 +59,32 @@ def test_writer_segments_round_trip():
     import oracle_lj92 as O
     from cpipe_b200.dng_synth import lj92_segment
     rng = np.random.default_rng(11)
-    for h, w, bits, nf in [(16, 32, 12, 2), (7, 10, 16, 2), (9, 9, 10, 1), (40, 64, 14, 2)]:
+    for h, w, bits, nf in [(16, 32, 12, 2), (7, 10, 16, 2), (9, 9, 10, 1), (40, 64, 14, 2), (12, 24, 12, 4)]:
         noise = rng.integers(0, 1 << bits, (h, w)).astype(np.uint16)
         ramp = (np.add.outer(np.arange(h), 3 * np.arange(w)) % (1 << bits)).astype(np.uint16)
-        for img in (noise, ramp):
-            got = np.asarray(O.decode(lj92_segment(img, bits, nf), w, h)).reshape(h, w)
-            np.testing.assert_array_equal(got, img)
+        flat = np.full((h, w), 7, np.uint16)
+        for img in (noise, ramp, flat):
+            for tables in ("fixed", "per_component"):
+                got = np.asarray(O.decode(lj92_segment(img, bits, nf, tables), w, h)).reshape(h, w)
+                np.testing.assert_array_equal(got, img)
+
+
+def test_writer_per_component_tables_differ():
+    """Per-component tables come from each component's own statistics: a
+    noisy and a flat component get different code lengths, and the scan
+    selects table c for component c."""
+    import numpy as np
+    from cpipe_b200.dng_synth import lj92_segment
+    rng = np.random.default_rng(5)
+    img = np.zeros((32, 64), np.uint16)
+    img[:, 0::2] = rng.integers(0, 4096, (32, 32))
+    img[:, 1::2] = 100
+    seg = lj92_segment(img, 12, 2, "per_component")
+    dht = seg.index(b"\xff\xc4")
+    n = int.from_bytes(seg[dht + 2:dht + 4], "big")
+    body = seg[dht + 4:dht + 2 + n]
+    t0_total = sum(body[1:17])
+    t1 = body[17 + t0_total:]
+    assert body[0] == 0 and t1[0] == 1 and body[1:17] != t1[1:17]
+    sos = seg.index(b"\xff\xda")
+    assert seg[sos + 5:sos + 9] == bytes((1, 0x00, 2, 0x10))
