@@ -26,13 +26,15 @@
 //     is long because high-entropy data resynchronise slowly: with an optimal
 //     table for 10-bit noise the codes are 1-3 bits ahead of 9-10 raw bits, and
 //     a path one component off under different tables soon parts again;
-//  3. walks: a warp per group of 32 chunks chains the chunks from the leading
-//     candidate of its first chunk (lane j takes the path whose start is lane
-//     j-1's exit; a chunk with no matching candidate is decoded again from the
-//     exact state), then a warp per segment chains the groups from the
-//     stream's start (walking a group's chunks itself where the group's entry
-//     was not the true one), giving every group its exact entry state and
-//     first sample;
+//     Within a CTA each chunk also takes a path from every exit of the chunk
+//     before that starts none of its own, so only neighbouring failures miss;
+//  3. walks: a warp per group of 32 chunks chains the chunks from its first
+//     chunk's lead path and next-phase path (lane j takes the path whose start
+//     is lane j-1's exit; a chunk with no matching path is decoded again from
+//     the exact state), then a warp per segment chains the groups from the
+//     stream's start (walking a group's chunks itself where neither entry was
+//     the true one), giving every group its exact entry state and first
+//     sample;
 //  4. write: a warp per group chains its chunks once more from the exact entry,
 //     scans the counts, and every lane decodes its chunk from its exact start,
 //     storing each sample's difference (EXTEND, SSSS = 16 -> 32768); an invalid
@@ -68,6 +70,7 @@ constexpr uint32_t kChunkBits = 1024;   // bits of stream per chunk
 constexpr uint32_t kOverlapBits = 1536;  // bits decoded ahead of a chunk to synchronise
 constexpr int kChunksPerCta = 256;      // one chunk per thread; 8 groups of 32
 constexpr int kCands = 4;  // paths kept per chunk: lead, next phase, two from the exits of the chunk before
+constexpr int kGroupEntries = 2;  // group walks from a chunk group's lead path and its next-phase path
 constexpr int kStageWords = 8576;       // >= skewed words a CTA stages: (256 x 1024 + 1536 + 192) / 32 + 2 + skew
 constexpr int kScanBytes = 4096;        // unstuff block: 256 threads x 16 bytes
 constexpr uint64_t kMaxParallelBytes = 1ull << 27;
@@ -101,8 +104,8 @@ struct SegDev {
 struct LjCand {
     uint32_t s, e, n, meta;
 };
-// A path through a group of chunks from the leading candidate of its first
-// chunk (entry state, exit state, samples).
+// A path through a group of chunks from one of its first chunk's paths
+// (entry state, exit state, samples).
 struct LjGroup {
     uint32_t s, e, n, meta;
 };
@@ -268,7 +271,7 @@ __device__ __forceinline__ bool lj_skip(Bits& br, const uint16_t* lut, const LjT
 // state), then to the first at or after ce (the exit), counting samples.
 // SHARED: one table, the phase stays 0.
 template <bool STAGED, bool SHARED>
-__device__ __noinline__ LjCand lj_path_t(const LjCtx x, uint32_t pos, uint32_t ph, uint32_t cs, uint32_t ce) {
+__device__ __forceinline__ LjCand lj_path_t(const LjCtx& x, uint32_t pos, uint32_t ph, uint32_t cs, uint32_t ce) {
     LjBits<STAGED> br;
     x.open(br, pos);
     const LjTab* tab0 = x.tabs + lj_tid(x.tids, 0);
@@ -302,11 +305,25 @@ __device__ __forceinline__ LjCand lj_path(const LjCtx& x, uint32_t pos, uint32_t
     return x.shared ? lj_path_t<STAGED, true>(x, pos, 0, cs, ce) : lj_path_t<STAGED, false>(x, pos, ph, cs, ce);
 }
 
+// The lookahead tables of the segment's phases into shared memory, 16 bytes a
+// load with eight loads in flight per thread.
 __device__ __forceinline__ void stage_luts(uint16_t* lut, const LjTab* tabs, const SegDev& s) {
+    constexpr uint32_t kVec = kLut / 8;  // uint4 per table
     const uint32_t phases = s.shared ? 1u : s.nf;
-    for (uint32_t i = threadIdx.x; i < phases * kLut; i += blockDim.x) {
-        const uint32_t ph = i / kLut;
-        lut[i] = tabs[lj_tid(s.tids, ph)].lut[i % kLut];
+    uint4* dst = reinterpret_cast<uint4*>(lut);
+    for (uint32_t i0 = threadIdx.x; i0 < phases * kVec; i0 += 8 * blockDim.x) {
+        uint4 v[8];
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const uint32_t i = i0 + k * blockDim.x;
+            if (i < phases * kVec)
+                v[k] = __ldg(reinterpret_cast<const uint4*>(tabs[lj_tid(s.tids, i / kVec)].lut) + i % kVec);
+        }
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const uint32_t i = i0 + k * blockDim.x;
+            if (i < phases * kVec) dst[i] = v[k];
+        }
     }
 }
 
@@ -527,6 +544,24 @@ __global__ void __launch_bounds__(kChunksPerCta) lj_cand_kernel(const SegDev* __
                 else f0 = r;
             }
         }
+    // A second round over the paths the first one added, for runs of two
+    // chunks that did not synchronise.
+    __syncthreads();
+    first[2 * threadIdx.x] = f0;
+    first[2 * threadIdx.x + 1] = f1;
+    __syncthreads();
+    if (live && c > 0 && threadIdx.x > 0 && !(f1.meta & 16u))
+#pragma unroll
+        for (int j = 0; j < 2; ++j) {
+            const LjCand q = first[2 * (threadIdx.x - 1) + j];
+            const uint32_t ep = (q.meta >> 2) & 3u;
+            auto starts = [&](const LjCand& r) { return (r.meta & 16u) && r.s == q.e && (r.meta & 3u) == ep; };
+            if ((q.meta & 16u) && !(f1.meta & 16u) && !starts(p0) && !starts(p1) && !starts(f0)) {
+                const LjCand r = lj_path<true>(x, q.e, ep, cs, ce);
+                if (f0.meta & 16u) f1 = r;
+                else f0 = r;
+            }
+        }
     if (c >= s.nchunk) return;
     LjCand* out = cand + (size_t)(s.chunk0 + c) * kCands;
     out[0] = p0;
@@ -538,17 +573,18 @@ __global__ void __launch_bounds__(kChunksPerCta) lj_cand_kernel(const SegDev* __
 // Chains chunks gc0 .. gc0 + glive - 1 (lane j holds chunk gc0 + j's
 // candidates in c) from state (pos, ph), warp-collectively: lane j takes the
 // candidate that starts at lane j-1's exit, or decodes its chunk again from
-// that exact state.  On return (pos, ph) is the group's exit, `total` has
-// grown by its samples, and lane j holds its chunk's exact start and count.
+// that exact state (or, with give_up, the walk returns false there).  On
+// return (pos, ph) is the group's exit, `total` has grown by its samples, and
+// lane j holds its chunk's exact start and count.
 template <bool STAGED>
-__device__ void lj_walk(const LjCtx& x, const LjCand (&c)[kCands], uint32_t gc0, uint32_t glive, uint32_t& pos,
+__device__ bool lj_walk(const LjCtx& x, const LjCand (&c)[kCands], uint32_t gc0, uint32_t glive, uint32_t& pos,
                         uint32_t& ph, uint32_t& my_pos, uint32_t& my_ph, uint32_t& my_n, uint32_t& total,
-                        unsigned long long* stats, int which) {
+                        unsigned long long* stats, int which, bool give_up = false) {
     const uint32_t lane = threadIdx.x & 31;
     for (uint32_t j = 0; j < glive; ++j) {
         uint32_t e = 0, ep = 0, n = 0;
+        bool hit = false;
         if (lane == j) {
-            bool hit = false;
 #pragma unroll
             for (int k = 0; k < kCands; ++k)
                 if (!hit && (c[k].meta & 16u) && c[k].s == pos && (c[k].meta & 3u) == ph) {
@@ -557,7 +593,7 @@ __device__ void lj_walk(const LjCtx& x, const LjCand (&c)[kCands], uint32_t gc0,
                     ep = (c[k].meta >> 2) & 3u;
                     n = c[k].n;
                 }
-            if (!hit) {
+            if (!hit && !give_up) {
                 const uint32_t cc = gc0 + j;
                 const LjCand r = lj_path<STAGED>(x, pos, ph, x.cs(cc), x.ce(cc));
                 e = r.e;
@@ -571,10 +607,12 @@ __device__ void lj_walk(const LjCtx& x, const LjCand (&c)[kCands], uint32_t gc0,
             my_ph = ph;
             my_n = n;
         }
+        if (give_up && !__shfl_sync(0xFFFFFFFFu, hit, j)) return false;
         pos = __shfl_sync(0xFFFFFFFFu, e, j);
         ph = __shfl_sync(0xFFFFFFFFu, ep, j);
         total += __shfl_sync(0xFFFFFFFFu, n, j);
     }
+    return true;
 }
 
 __device__ __forceinline__ void load_cands(const LjCand* __restrict__ cand, const SegDev& s, uint32_t gc0,
@@ -589,10 +627,10 @@ __device__ __forceinline__ void load_cands(const LjCand* __restrict__ cand, cons
     }
 }
 
-// A warp per group of 32 chunks: the group's path from the leading candidate
-// of its first chunk.  When the true entry differs (another component phase,
-// or a chunk that did not synchronise) the segment walk chains that group's
-// chunks itself.
+// A warp per group of 32 chunks: the group's paths from the lead path of its
+// first chunk and from that path's next-phase start.  When the true entry is
+// neither (a chunk that did not synchronise) the segment walk chains that
+// group's chunks itself.
 __global__ void __launch_bounds__(kChunksPerCta) lj_group_kernel(const SegDev* __restrict__ segs,
                                                                  const CtaDesc* __restrict__ ctas,
                                                                  const LjTab* __restrict__ tabs,
@@ -601,7 +639,7 @@ __global__ void __launch_bounds__(kChunksPerCta) lj_group_kernel(const SegDev* _
                                                                  const LjCand* __restrict__ cand,
                                                                  LjGroup* __restrict__ groups,
                                                                  unsigned long long* stats) {
-    __shared__ uint16_t lut[4 * kLut];
+    __shared__ __align__(16) uint16_t lut[4 * kLut];
     const CtaDesc d = ctas[blockIdx.x];
     const SegDev s = segs[d.seg];
     stage_luts(lut, tabs, s);
@@ -609,22 +647,31 @@ __global__ void __launch_bounds__(kChunksPerCta) lj_group_kernel(const SegDev* _
     const LjCtx x = make_ctx(s, ubuf, ulen[d.seg], lut, tabs);
     const uint32_t gc0 = d.c0 + (threadIdx.x >> 5) * 32;
     if (gc0 >= s.nchunk) return;  // warp-uniform
-    LjGroup* out = groups + s.group0 + gc0 / 32;
+    LjGroup* out = groups + (size_t)(s.group0 + gc0 / 32) * kGroupEntries;
     const uint32_t lane = threadIdx.x & 31;
     if (gc0 > x.last) {
-        if (lane == 0) *out = LjGroup{0, 0, 0, 0};
+        if (lane < kGroupEntries) out[lane] = LjGroup{0, 0, 0, 0};
         return;
     }
     const uint32_t glive = min(32u, x.last + 1 - gc0);
     LjCand c[kCands];
     load_cands(cand, s, gc0, glive, c);
 #pragma unroll
-    const uint32_t meta = __shfl_sync(0xFFFFFFFFu, c[0].meta, 0);
-    uint32_t pos = __shfl_sync(0xFFFFFFFFu, c[0].s, 0), ph = meta & 3u;
-    const uint32_t s0 = pos, p0 = ph;
-    uint32_t mp = 0, mph = 0, mn = 0, total = 0;
-    lj_walk<false>(x, c, gc0, glive, pos, ph, mp, mph, mn, total, stats, kStatGroup);
-    if (lane == 0) *out = LjGroup{s0, pos, total, p0 | (ph << 2) | 16u};
+#pragma unroll
+    for (int k = 0; k < kGroupEntries; ++k) {
+        const uint32_t meta = __shfl_sync(0xFFFFFFFFu, c[k].meta, 0);
+        LjGroup g = {0, 0, 0, 0};
+        if (meta & 16u) {
+            uint32_t pos = __shfl_sync(0xFFFFFFFFu, c[k].s, 0), ph = meta & 3u;
+            const uint32_t s0 = pos, p0 = ph;
+            uint32_t mp = 0, mph = 0, mn = 0, total = 0;
+            // the lead path's walk decodes missing chunks again; the other
+            // phase's walk gives up at its first miss
+            if (lj_walk<false>(x, c, gc0, glive, pos, ph, mp, mph, mn, total, stats, kStatGroup, k > 0))
+                g = LjGroup{s0, pos, total, p0 | (ph << 2) | 16u};
+        }
+        if (lane == 0) out[k] = g;
+    }
 }
 
 // A warp per segment: chains the groups from the stream's start; gentry[g] =
@@ -634,7 +681,7 @@ __global__ void __launch_bounds__(32) lj_seg_kernel(const SegDev* __restrict__ s
                                                     const uint32_t* __restrict__ ulen, const LjCand* __restrict__ cand,
                                                     const LjGroup* __restrict__ groups, uint4* __restrict__ gentry,
                                                     unsigned long long* stats) {
-    __shared__ uint16_t lut[4 * kLut];
+    __shared__ __align__(16) uint16_t lut[4 * kLut];
     const uint32_t seg = par[blockIdx.x];
     const SegDev s = segs[seg];
     stage_luts(lut, tabs, s);
@@ -644,16 +691,22 @@ __global__ void __launch_bounds__(32) lj_seg_kernel(const SegDev* __restrict__ s
     const uint32_t ngl = x.last / 32 + 1;
     uint32_t pos = 0, ph = 0, off = 0;
     for (uint32_t gb = 0; gb < ngl; gb += 32) {
-        const LjGroup e = gb + lane < ngl ? groups[s.group0 + gb + lane] : LjGroup{0, 0, 0, 0};
+        LjGroup e[kGroupEntries];
+#pragma unroll
+        for (int k = 0; k < kGroupEntries; ++k)
+            e[k] = gb + lane < ngl ? groups[(size_t)(s.group0 + gb + lane) * kGroupEntries + k] : LjGroup{0, 0, 0, 0};
         const uint32_t nb = min(32u, ngl - gb);
         for (uint32_t j = 0; j < nb; ++j) {
             uint32_t hit = 0, ex = 0, exp = 0, n = 0;
-            if (lane == j && (e.meta & 16u) && e.s == pos && (e.meta & 3u) == ph) {
-                hit = 1;
-                ex = e.e;
-                exp = (e.meta >> 2) & 3u;
-                n = e.n;
-            }
+            if (lane == j)
+#pragma unroll
+                for (int k = 0; k < kGroupEntries; ++k)
+                    if (!hit && (e[k].meta & 16u) && e[k].s == pos && (e[k].meta & 3u) == ph) {
+                        hit = 1;
+                        ex = e[k].e;
+                        exp = (e[k].meta >> 2) & 3u;
+                        n = e[k].n;
+                    }
             if (lane == 0) gentry[s.group0 + gb + j] = make_uint4(pos, ph, off, 0);
             if (__shfl_sync(0xFFFFFFFFu, hit, j)) {
                 pos = __shfl_sync(0xFFFFFFFFu, ex, j);
@@ -1268,7 +1321,7 @@ int lj92_decode(const uint8_t* const* streams, const size_t* bytes, uint32_t cou
         if (st == CPIPE_OK) st = call.alloc(count * 4, &d_ulen);
         if (st == CPIPE_OK) st = call.alloc(ubytes, &d_ubuf);
         if (st == CPIPE_OK) st = call.alloc(chunks * kCands * sizeof(LjCand), &d_cand);
-        if (st == CPIPE_OK) st = call.alloc(groups * sizeof(LjGroup), &d_groups);
+        if (st == CPIPE_OK) st = call.alloc(groups * kGroupEntries * sizeof(LjGroup), &d_groups);
         if (st == CPIPE_OK) st = call.alloc(groups * sizeof(uint4), &d_gentry);
         if (st == CPIPE_OK) st = call.alloc(samples * 2, &d_dbuf);
         if (st == CPIPE_OK) st = call.alloc(nlines * 8, &d_cbuf);

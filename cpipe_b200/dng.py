@@ -101,3 +101,44 @@ class DngReader:
         if st != _abi.OK:
             return DngReadResult(st, message=L.cpipe_cuda_last_error().decode())
         return DngReadResult(_abi.OK, out, info_to_metadata(info, data))
+
+
+def _main():
+    """Times cpipe_cuda_dng_decode of a synthetic lossless-JPEG DNG: the 12 MP
+    benchmark frame's 10-bit mosaic in 256x256 tiles.
+
+        python -m cpipe_b200.dng --tables per_component --reps 5
+    """
+    import argparse
+    import time
+
+    import numpy as np
+
+    from .chain import ChainConfig
+    from .dng_synth import build_dng, lj92_tiles
+    ap = argparse.ArgumentParser(description=_main.__doc__.split("\n")[0])
+    ap.add_argument("--tables", choices=["per_component", "fixed"], default="per_component")
+    ap.add_argument("--tile", type=int, default=256)
+    ap.add_argument("--reps", type=int, default=5)
+    a = ap.parse_args()
+    L = _abi.lib()
+    raw = ChainConfig.full_12mp().make_raw()
+    h, w = raw.shape
+    data = build_dng(width=w, height=h, bits=10, tile=(a.tile, a.tile),
+                     segments=lj92_tiles(raw, 10, a.tile, a.tile, 2, a.tables))
+    out = torch.empty((h, w), dtype=torch.int16, device="cuda")
+    ms = []
+    for _ in range(a.reps):
+        t = time.perf_counter()
+        st = L.cpipe_cuda_dng_decode(data, len(data), C.c_void_p(out.data_ptr()), out.numel() * 2, None)
+        ms.append((time.perf_counter() - t) * 1e3)
+        assert st == 0, L.cpipe_cuda_last_error().decode()
+    fig = (C.c_uint64 * 9)()
+    L.cpipe_cuda_lj92_last_stats(fig, 9)
+    exact = bool(np.array_equal(out.cpu().numpy().view(np.uint16), raw))
+    print(f"lossless-JPEG DNG {w}x{h} ({len(data)} bytes, tables {a.tables}): best {min(ms):.3f} ms "
+          f"from host memory; exact {exact}; figures {list(fig)}")
+
+
+if __name__ == "__main__":
+    _main()
