@@ -3,6 +3,15 @@
 // (src/cpipe/ingest/dng_opcode/OpcodeListParser.cpp:330-515) decision for
 // decision: the same header check, the same IFD bounds, the same per-type value
 // reads (OpcodeListParser.cpp:84-278) and the same status for each rejection.
+//
+// One extension, for files the reference rejects: when IFD0 is not a
+// single-plane CFA image (a camera or converter DNG whose IFD0 is the preview),
+// the first SubIFD (tag 330) that is a full-resolution (NewSubFileType 0)
+// single-plane CFA image supplies the image tags -- size, depth, compression,
+// strips / tiles, CFA, black and white levels, linearization, active area,
+// opcode lists -- while the camera tags stay IFD0's (make, model, orientation,
+// illuminants, matrices, as-shot neutral, Exif, XMP, ICC), as the DNG
+// specification places them.
 #include <cstdint>
 #include <cstdio>
 #include <cstring>
@@ -22,9 +31,9 @@ enum : uint16_t {
 };
 enum : uint16_t {
     kTagWidth = 256, kTagLength = 257, kTagBits = 258, kTagCompression = 259, kTagPhotometric = 262,
-    kTagMake = 271, kTagModel = 272, kTagStripOffsets = 273, kTagOrientation = 274, kTagSamples = 277,
+    kTagNewSubFileType = 254, kTagMake = 271, kTagModel = 272, kTagStripOffsets = 273, kTagOrientation = 274, kTagSamples = 277,
     kTagRowsPerStrip = 278, kTagStripByteCounts = 279, kTagTileWidth = 322, kTagTileLength = 323,
-    kTagTileOffsets = 324, kTagTileByteCounts = 325, kTagXmp = 700, kTagCfaRepeat = 33421, kTagCfaPattern = 33422,
+    kTagTileOffsets = 324, kTagTileByteCounts = 325, kTagSubIfds = 330, kTagXmp = 700, kTagCfaRepeat = 33421, kTagCfaPattern = 33422,
     kTagExposure = 33434, kTagFNumber = 33437, kTagExifIfd = 34665, kTagIcc = 34675, kTagIso = 34855,
     kTagFocal = 37386, kTagLinearization = 50712, kTagBlack = 50714, kTagWhite = 50717,
     kTagColorMatrix1 = 50721, kTagColorMatrix2 = 50722, kTagAsShotNeutral = 50728,
@@ -226,30 +235,49 @@ extern "C" int cpipe_dng_parse(const uint8_t* file, size_t file_bytes, cpipe_Dng
     const Tiff t{file, (uint64_t)file_bytes};
     if (t.n < 8 || file[0] != 'I' || file[1] != 'I' || t.u16(2) != 42)
         return fail(CPIPE_FAILED, "unsupported DNG/TIFF header");
-    static thread_local Ifd ifd0, exif;
+    static thread_local Ifd ifd0, exif, sub;
     if (!read_ifd(t, t.u32(4), &ifd0)) return fail(CPIPE_FAILED, "invalid IFD table");
 
     bool found = false;
-    d.compression = first_u32(t, ifd0, kTagCompression, &found);
+    auto cfa_image = [&](const Ifd& ifd) {
+        uint32_t photometric = first_u32(t, ifd, kTagPhotometric, &found);
+        if (!found) photometric = kPhotometricCfa;
+        uint32_t samples = first_u32(t, ifd, kTagSamples, &found);
+        if (!found) samples = 1;
+        return photometric == kPhotometricCfa && samples == 1;
+    };
+    // the IFD that holds the raw image: IFD0, or (extension) a SubIFD
+    const Ifd* rif = &ifd0;
+    if (!cfa_image(ifd0)) {
+        uint64_t where = 0;
+        const Entry* subs = ifd0.find(kTagSubIfds, &where);
+        if (subs && (subs->type == kLong || subs->type == 13) && subs->count > 0) {
+            const uint64_t at = subs->count == 1 ? where + 8 : subs->value;
+            for (uint32_t k = 0; k < subs->count && k < 16 && at + 4 * (uint64_t)(k + 1) <= t.n; ++k) {
+                if (!read_ifd(t, t.u32(at + 4 * (uint64_t)k), &sub)) continue;
+                if (first_u32(t, sub, kTagNewSubFileType) == 0 && cfa_image(sub)) {
+                    rif = &sub;
+                    break;
+                }
+            }
+        }
+    }
+    const Ifd& raw = *rif;
+    d.compression = first_u32(t, raw, kTagCompression, &found);
     if (!found) d.compression = 1;
-    uint32_t photometric = first_u32(t, ifd0, kTagPhotometric, &found);
-    if (!found) photometric = kPhotometricCfa;
-    uint32_t samples = first_u32(t, ifd0, kTagSamples, &found);
-    if (!found) samples = 1;
     auto unsupported = [&](const char* m) {
         *info = d;
         return fail(CPIPE_UNSUPPORTED, m);
     };
-    if (photometric != kPhotometricCfa || samples != 1)
-        return unsupported("only single-plane Bayer CFA DNG is supported in P1");
+    if (!cfa_image(raw)) return unsupported("only single-plane Bayer CFA DNG is supported in P1");
 
-    d.width = first_u32(t, ifd0, kTagWidth);
-    d.height = first_u32(t, ifd0, kTagLength);
-    d.bits_per_sample = first_u32(t, ifd0, kTagBits);
-    d.strip_offset = first_u32(t, ifd0, kTagStripOffsets);
-    d.strip_byte_count = first_u32(t, ifd0, kTagStripByteCounts);
+    d.width = first_u32(t, raw, kTagWidth);
+    d.height = first_u32(t, raw, kTagLength);
+    d.bits_per_sample = first_u32(t, raw, kTagBits);
+    d.strip_offset = first_u32(t, raw, kTagStripOffsets);
+    d.strip_byte_count = first_u32(t, raw, kTagStripByteCounts);
     d.orientation = first_u32(t, ifd0, kTagOrientation) & 0xFFu;
-    d.white_level = first_u32(t, ifd0, kTagWhite);
+    d.white_level = first_u32(t, raw, kTagWhite);
     d.calibration_illuminant[0] = first_u32(t, ifd0, kTagIlluminant1) & 0xFFFFu;
     d.calibration_illuminant[1] = first_u32(t, ifd0, kTagIlluminant2) & 0xFFFFu;
     capture_tags(t, ifd0, &d);
@@ -259,7 +287,7 @@ extern "C" int cpipe_dng_parse(const uint8_t* file, size_t file_bytes, cpipe_Dng
     // CFA: a SHORT[2] repeat of 2x2 or 4x4, and a pattern of exactly that
     // many bytes (OpcodeListParser.cpp:413-446).
     uint64_t pos = 0;
-    const Entry* rep = ifd0.find(kTagCfaRepeat, &pos);
+    const Entry* rep = raw.find(kTagCfaRepeat, &pos);
     if (!rep) return unsupported("DNG is missing CFARepeatPatternDim");
     uint32_t r[4] = {0, 0, 0, 0};
     const int nr = rep->type == kShort ? u32_values(t, *rep, pos, r, 4) : 0;
@@ -267,7 +295,7 @@ extern "C" int cpipe_dng_parse(const uint8_t* file, size_t file_bytes, cpipe_Dng
         return unsupported("only 2x2 Bayer or 4x4 Quad Bayer DNG is supported");
     d.cfa_repeat[0] = r[0];
     d.cfa_repeat[1] = r[1];
-    const Entry* pat = ifd0.find(kTagCfaPattern, &pos);
+    const Entry* pat = raw.find(kTagCfaPattern, &pos);
     bool cfa_ok = false;
     if (pat) {
         const Span s = value_bytes(t, *pat, pos);
@@ -281,8 +309,8 @@ extern "C" int cpipe_dng_parse(const uint8_t* file, size_t file_bytes, cpipe_Dng
         return unsupported("DNG is missing a supported CFA pattern");
     }
 
-    float_values(t, ifd0, kTagBlack, d.black_level, 4);
-    const Entry* lin = ifd0.find(kTagLinearization, &pos);
+    float_values(t, raw, kTagBlack, d.black_level, 4);
+    const Entry* lin = raw.find(kTagLinearization, &pos);
     if (lin && lin->type == kShort) {
         const Span s = value_bytes(t, *lin, pos);
         if (s.len) {
@@ -297,7 +325,7 @@ extern "C" int cpipe_dng_parse(const uint8_t* file, size_t file_bytes, cpipe_Dng
         d.has_matrix[m] = has ? 1u : 0u;
     }
     float_values(t, ifd0, kTagAsShotNeutral, d.as_shot_neutral, 3);
-    const Entry* aa = ifd0.find(kTagActiveArea, &pos);
+    const Entry* aa = raw.find(kTagActiveArea, &pos);
     if (aa) {
         uint32_t v[5];
         const int n = u32_values(t, *aa, pos, v, 5);
@@ -323,13 +351,13 @@ extern "C" int cpipe_dng_parse(const uint8_t* file, size_t file_bytes, cpipe_Dng
     }
     byte_range(t, ifd0, kTagXmp, &d.xmp_offset, &d.xmp_bytes);
     byte_range(t, ifd0, kTagIcc, &d.icc_offset, &d.icc_bytes);
-    byte_range(t, ifd0, kTagOpcodeList1, &d.opcode_list_offset[0], &d.opcode_list_bytes[0]);
-    byte_range(t, ifd0, kTagOpcodeList2, &d.opcode_list_offset[1], &d.opcode_list_bytes[1]);
-    byte_range(t, ifd0, kTagOpcodeList3, &d.opcode_list_offset[2], &d.opcode_list_bytes[2]);
+    byte_range(t, raw, kTagOpcodeList1, &d.opcode_list_offset[0], &d.opcode_list_bytes[0]);
+    byte_range(t, raw, kTagOpcodeList2, &d.opcode_list_offset[1], &d.opcode_list_bytes[1]);
+    byte_range(t, raw, kTagOpcodeList3, &d.opcode_list_offset[2], &d.opcode_list_bytes[2]);
     // raw data segments: tiles when present, else strips
     auto array_at = [&](uint16_t tag, uint32_t* where, uint32_t* type, uint32_t* count) {
         uint64_t p = 0;
-        const Entry* e = ifd0.find(tag, &p);
+        const Entry* e = raw.find(tag, &p);
         if (!e || (e->type != kShort && e->type != kLong)) return false;
         const Span s = value_bytes(t, *e, p);
         if (s.len == 0) return false;
@@ -342,12 +370,12 @@ extern "C" int cpipe_dng_parse(const uint8_t* file, size_t file_bytes, cpipe_Dng
     if (array_at(kTagTileOffsets, &d.seg_offsets_pos, &d.seg_offsets_type, &n_off) &&
         array_at(kTagTileByteCounts, &d.seg_counts_pos, &d.seg_counts_type, &n_cnt)) {
         d.seg_tiled = 1;
-        d.seg_width = first_u32(t, ifd0, kTagTileWidth);
-        d.seg_height = first_u32(t, ifd0, kTagTileLength);
+        d.seg_width = first_u32(t, raw, kTagTileWidth);
+        d.seg_height = first_u32(t, raw, kTagTileLength);
     } else if (array_at(kTagStripOffsets, &d.seg_offsets_pos, &d.seg_offsets_type, &n_off) &&
                array_at(kTagStripByteCounts, &d.seg_counts_pos, &d.seg_counts_type, &n_cnt)) {
         bool has_rows = false;
-        const uint32_t rows = first_u32(t, ifd0, kTagRowsPerStrip, &has_rows);
+        const uint32_t rows = first_u32(t, raw, kTagRowsPerStrip, &has_rows);
         d.seg_width = d.width;
         d.seg_height = has_rows && rows > 0 && rows < d.height ? rows : d.height;
     }

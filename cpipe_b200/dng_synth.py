@@ -303,3 +303,52 @@ def lj92_tiles(img, bits, tile_w, tile_h, components=2, tables="fixed"):
     pad = np.pad(img, ((0, down * tile_h - h), (0, across * tile_w - w)), mode="edge")
     return [lj92_segment(pad[ty * tile_h:(ty + 1) * tile_h, tx * tile_w:(tx + 1) * tile_w], bits, components,
                          tables) for ty in range(down) for tx in range(across)]
+
+
+# Tags a DNG keeps in IFD0 when the raw image sits in a SubIFD: camera,
+# colour and capture metadata, Exif / XMP / ICC (DNG 1.4 specification).
+_CAMERA_TAGS = (271, 272, 274, 700, 33434, 33437, 34665, 34675, 34855, 37386, 50706, 50707, 50708, 50721, 50722,
+                50728, 50778, 50779, 50964, 50965)
+
+
+def subifd_dng(dng, thumb=(8, 6)):
+    """The DNG `dng` (raw image in IFD0, as build_dng writes it) rewritten in
+    the layout of camera and converter DNGs: IFD0 a small RGB preview
+    (NewSubFileType 1) carrying the camera tags and a SubIFDs tag, the raw
+    image's tags (NewSubFileType 0) in that SubIFD.  Data stay where they
+    were; the new IFDs and the preview strip are appended."""
+    b = bytearray(dng)
+    ifd0 = struct.unpack_from("<I", b, 4)[0]
+    n = struct.unpack_from("<H", b, ifd0)[0]
+    entries = [bytes(b[ifd0 + 2 + 12 * k: ifd0 + 14 + 12 * k]) for k in range(n)]
+    tag_of = lambda e: struct.unpack_from("<H", e)[0]
+    camera = [e for e in entries if tag_of(e) in _CAMERA_TAGS]
+    image = [e for e in entries if tag_of(e) not in _CAMERA_TAGS and tag_of(e) != 254]
+    image.append(struct.pack("<HHII", 254, LONG, 1, 0))
+
+    def append_ifd(ents):
+        while len(b) % 2:
+            b.append(0)
+        at = len(b)
+        ents = sorted(ents, key=tag_of)
+        b.extend(struct.pack("<H", len(ents)) + b"".join(ents) + struct.pack("<I", 0))
+        return at
+
+    raw_ifd = append_ifd(image)
+    tw, th = thumb
+    while len(b) % 2:
+        b.append(0)
+    bits_at = len(b)
+    b.extend(struct.pack("<HHH", 8, 8, 8))
+    strip_at = len(b)
+    b.extend(bytes((x * 37) & 0xFF for x in range(tw * th * 3)))
+    preview = camera + [
+        struct.pack("<HHII", 254, LONG, 1, 1), struct.pack("<HHII", 256, LONG, 1, tw),
+        struct.pack("<HHII", 257, LONG, 1, th), struct.pack("<HHII", 258, SHORT, 3, bits_at),
+        struct.pack("<HHIHH", 259, SHORT, 1, 1, 0), struct.pack("<HHIHH", 262, SHORT, 1, 2, 0),
+        struct.pack("<HHII", 273, LONG, 1, strip_at), struct.pack("<HHIHH", 277, SHORT, 1, 3, 0),
+        struct.pack("<HHII", 278, LONG, 1, th), struct.pack("<HHII", 279, LONG, 1, tw * th * 3),
+        struct.pack("<HHII", 330, LONG, 1, raw_ifd),
+    ]
+    struct.pack_into("<I", b, 4, append_ifd(preview))
+    return bytes(b)

@@ -6,7 +6,9 @@ library never loads it.
 parse()  follows cpipe::ingest::dng_opcode::OpcodeListParser::parse
          (src/cpipe/ingest/dng_opcode/OpcodeListParser.cpp:330-515) and its
          value readers (OpcodeListParser.cpp:84-278): little-endian TIFF only,
-         IFD0 plus the Exif IFD's capture tags.
+         IFD0 plus the Exif IFD's capture tags.  One extension for files the
+         reference rejects: when IFD0 is not a CFA image, the first
+         full-resolution CFA SubIFD supplies the image tags.
 read()   follows cpipe::ingest::dng::DngReader::read (src/cpipe/ingest/dng/
          DngReader.cpp:190-232) on its single-strip path (DngReader.cpp:145-164):
          copy min(width * height * 2, strip bytes) into a zeroed R16 plane.
@@ -137,15 +139,32 @@ def parse(b):
     ents = _entries(b, struct.unpack_from("<I", b, 4)[0])
     if ents is None:
         return FAILED, info
-    c = _first(b, ents, 259)
+
+    def cfa_image(e):
+        ph, spp = _first(b, e, 262), _first(b, e, 277)
+        return (32803 if ph is None else ph) == 32803 and (1 if spp is None else spp) == 1
+
+    # Extension beyond the reference (which reads IFD0 only and rejects these
+    # files): when IFD0 is not a CFA image, the first full-resolution CFA
+    # SubIFD supplies the image tags; camera tags stay IFD0's.
+    raw = ents
+    if not cfa_image(ents) and 330 in ents and ents[330][0] in (LONG, 13) and ents[330][1] > 0:
+        typ, cnt, val, pos = ents[330]
+        at = pos + 8 if cnt == 1 else val
+        for k in range(min(cnt, 16)):
+            if at + 4 * (k + 1) > len(b):
+                break
+            sub = _entries(b, struct.unpack_from("<I", b, at + 4 * k)[0])
+            if sub is not None and (_first(b, sub, 254) or 0) == 0 and cfa_image(sub):
+                raw = sub
+                break
+    c = _first(b, raw, 259)
     info["compression"] = 1 if c is None else c
-    ph = _first(b, ents, 262)
-    spp = _first(b, ents, 277)
-    if (32803 if ph is None else ph) != 32803 or (1 if spp is None else spp) != 1:
+    if not cfa_image(raw):
         return UNSUPPORTED, info
     for key, tag in (("width", 256), ("height", 257), ("bits_per_sample", 258), ("strip_offset", 273),
                      ("strip_byte_count", 279), ("white_level", 50717)):
-        v = _first(b, ents, tag)
+        v = _first(b, raw, tag)
         info[key] = 0 if v is None else v
     info["orientation"] = (_first(b, ents, 274) or 0) & 0xFF
     info["calibration_illuminant"] = [(_first(b, ents, 50778) or 0) & 0xFFFF, (_first(b, ents, 50779) or 0) & 0xFFFF]
@@ -155,21 +174,21 @@ def parse(b):
         if e is not None and e[0] == ASCII:
             d, _ = _data(b, e)
             info[key] = d.split(b"\0")[0][:63].decode("latin-1")
-    rep = ents.get(33421)
+    rep = raw.get(33421)
     if rep is None:
         return UNSUPPORTED, info
     r = _ints(b, rep) if rep[0] == SHORT else []
     if len(r) != 2 or r[0] != r[1] or r[0] not in (2, 4):
         return UNSUPPORTED, info
-    pat = ents.get(33422)
+    pat = raw.get(33422)
     d = _data(b, pat)[0] if pat is not None else b""
     if not (pat is not None and len(d) == r[0] * r[1] and len(d) <= 16):
         return UNSUPPORTED, info
     info["cfa_repeat"], info["cfa_pattern"] = r, list(d)
-    v = _floats(b, ents, 50714) or []
+    v = _floats(b, raw, 50714) or []
     for i in range(min(4, len(v))):
         info["black_level"][i] = float(v[i])
-    e = ents.get(50712)
+    e = raw.get(50712)
     if e is not None and e[0] == SHORT:
         info["linearization"] = _ints(b, e)
     for m, tag in enumerate((50721, 50722, 50964, 50965)):
@@ -181,7 +200,7 @@ def parse(b):
     v = _floats(b, ents, 50728) or []
     for i in range(min(3, len(v))):
         info["as_shot_neutral"][i] = float(v[i])
-    e = ents.get(50829)
+    e = raw.get(50829)
     if e is not None:
         v = _ints(b, e)
         if len(v) == 4 and v[2] >= v[0] and v[3] >= v[1]:
@@ -197,7 +216,7 @@ def parse(b):
             _capture(b, ex, info)
     for name, tag in (("xmp", 700), ("icc", 34675), ("opcode_list_1", 51008), ("opcode_list_2", 51009),
                       ("opcode_list_3", 51022)):
-        e = ents.get(tag)
+        e = (raw if tag > 50000 else ents).get(tag)
         if e is not None:
             d, off = _data(b, e)
             info["blobs"][name] = (off, len(d))

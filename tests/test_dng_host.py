@@ -160,3 +160,52 @@ def test_oracle_words_copy_semantics():
     assert short[:4].tolist() == x.ravel()[:4].tolist() and short[4] == (x.ravel()[4] & 0xFF)
     assert not short[5:].any()
     assert np.array_equal(od.unpack(full + b"\x01\x02", 4, 3, 12), x)  # >= a 16-bit plane: words
+
+
+def test_subifd_raw_layout():
+    """Camera / converter layout (IFD0 a preview, the raw in a SubIFD): the C
+    parser and the oracle take the image tags from the SubIFD and the camera
+    tags from IFD0, and agree with the same file in the reference's IFD0-only
+    layout on every field but the preview-dependent offsets of inline values."""
+    from cpipe_b200.dng_synth import lj92_tiles, subifd_dng
+    flat = build_dng(width=70, height=48, bits=12)
+    img = (np.arange(48 * 70).reshape(48, 70) * 7 % 4096).astype(np.uint16)
+    tiled = build_dng(width=70, height=48, bits=12, tile=(32, 16), segments=lj92_tiles(img, 12, 32, 16))
+    for base in (flat, tiled):
+        st0, info0 = parse(base)
+        assert st0 == od.OK
+        moved = subifd_dng(base)
+        st, info = check_same(moved)
+        assert st == od.OK
+        f0, f1 = c_fields(info0), c_fields(info)
+        assert f0 == f1
+        keys = ["seg_count", "seg_tiled", "seg_width", "seg_height", "linearization_offset", "exif_offset",
+                "xmp_offset"]
+        if base is tiled:  # out-of-line offset arrays stay put (a single strip's sits in its moved entry)
+            keys += ["seg_offsets_pos", "seg_counts_pos"]
+        for k in keys:
+            assert getattr(info0, k) == getattr(info, k), k
+        assert list(info0.opcode_list_offset) == list(info.opcode_list_offset)
+
+
+def test_subifd_only_for_cfa_full_resolution():
+    """IFD0 not a CFA image and no usable SubIFD: still UNSUPPORTED, as the
+    reference reports it; a reduced-resolution (NewSubFileType 1) SubIFD is
+    not taken."""
+    import struct
+    from cpipe_b200.dng_synth import subifd_dng
+    moved = bytearray(subifd_dng(build_dng(width=8, height=6)))
+    ifd0 = struct.unpack_from("<I", moved, 4)[0]
+    n = struct.unpack_from("<H", moved, ifd0)[0]
+    for k in range(n):
+        e = ifd0 + 2 + 12 * k
+        if struct.unpack_from("<H", moved, e)[0] == 330:
+            raw_ifd = struct.unpack_from("<I", moved, e + 8)[0]
+    m = struct.unpack_from("<H", moved, raw_ifd)[0]
+    for k in range(m):
+        e = raw_ifd + 2 + 12 * k
+        if struct.unpack_from("<H", moved, e)[0] == 254:
+            struct.pack_into("<I", moved, e + 8, 1)
+    assert check_same(bytes(moved))[0] == od.UNSUPPORTED
+    no_sub = build_dng(width=8, height=6, overrides={262: (SHORT, [2]), 277: (SHORT, [3])})
+    assert check_same(no_sub)[0] == od.UNSUPPORTED

@@ -203,3 +203,19 @@ def test_invalid_code_mid_stream_fails(cuda_device):
         mid += 1
     bad = seg[:mid] + b"\xff\x00" * 8 + seg[mid:]
     assert gpu_decode([bad], 1, 512, 512, 512, 512)[0] == A.FAILED
+
+
+def test_subifd_files(cuda_device):
+    """Camera / converter layout (IFD0 a preview, the raw in a SubIFD), with
+    an uncompressed strip and with lossless-JPEG tiles: the raw decodes."""
+    from cpipe_b200.dng_synth import lj92_tiles, subifd_dng
+    img = smooth(48, 70, 12, 21)
+    tiled = build_dng(width=70, height=48, bits=12, tile=(32, 16),
+                      segments=lj92_tiles(img, 12, 32, 16, 2, "per_component"))
+    st, got = dng_decode(subifd_dng(tiled), 70, 48)
+    assert st == 0, A.lib().cpipe_cuda_last_error()
+    np.testing.assert_array_equal(got, img)
+    flat = build_dng(width=70, height=48, pixels=img)
+    st, got = dng_decode(subifd_dng(flat), 70, 48)
+    assert st == 0, A.lib().cpipe_cuda_last_error()
+    np.testing.assert_array_equal(got, img)
