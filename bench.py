@@ -133,6 +133,9 @@ def host_cpu():
     return {"model": model, "nproc": os.cpu_count(), "usable": usable}
 
 
+REFERENCE_ARM_BUDGET_S = 150.0  # the whole --impl reference run: warm-up and timed steps
+
+
 def reference_cpu_chain(cfg):
     """The reference's CPU chain for `cfg` (oracle/chain_oracle.run_reference_chain:
     the reference's own plain-C++ filters from oracle/_ref, single-threaded as
@@ -228,17 +231,33 @@ def reference_arm(args):
     from cpipe_b200.chain import ChainConfig
     cfg = ChainConfig.full_12mp()
     cpu = host_cpu()
+    # Each step is a bounded sample: a full-width band of the frame whose rows
+    # are sized so that warm-up and timed steps together take about
+    # REFERENCE_ARM_BUDGET_S; the time scales to a whole frame by rows (the
+    # chain's work per pixel is the same across the frame).
     try:
-        run, threads, label = reference_cpu_chain(cfg)
+        probe_rows = 64
+        probe, _, _ = reference_cpu_chain(ChainConfig.full_12mp(height=probe_rows, name="band"))
+        probe()
+        per_row_ms = probe() / probe_rows
+        per_step_ms = 1000.0 * REFERENCE_ARM_BUDGET_S / max(1, args.steps + args.warmup)
+        rows = int(min(cfg.height, max(16, per_step_ms / per_row_ms)) // 16 * 16)
+        band = cfg if rows >= cfg.height else ChainConfig.full_12mp(height=rows, name=f"band_{cfg.width}x{rows}")
+        run, threads, label = reference_cpu_chain(band)
     except Exception as e:  # noqa: BLE001
         print(json.dumps({"impl": "reference", "unavailable": f"reference CPU chain: {e}"}), flush=True)
         return 0
+    if band is not cfg:
+        label = (f"a {band.width}x{band.height} band of the frame (of {cfg.height} rows) per step, sized so that "
+                 f"the run takes about {REFERENCE_ARM_BUDGET_S:.0f} s, step times scaled by {cfg.height}/"
+                 f"{band.height}: " + label.split(" frame per step ", 1)[-1])
+    scale = cfg.height / band.height
     for _ in range(args.warmup):
         run()
     t0 = time.perf_counter()
-    steps = [run() for _ in range(args.steps)]
+    steps = [run() * scale for _ in range(args.steps)]
     total_ms = 1000.0 * (time.perf_counter() - t0)
-    v = total_ms / args.steps
+    v = total_ms * scale / args.steps
     line = {"impl": "reference", "metric": METRIC, "value": round(v, 3), "unit": "ms/frame", "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(v, 3), "higher_is_better": False,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded Philox scene)",
