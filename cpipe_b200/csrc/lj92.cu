@@ -1348,13 +1348,11 @@ int lj92_decode(const uint8_t* const* streams, const size_t* bytes, uint32_t cou
                                                                   static_cast<const uint32_t*>(d_end),
                                                                   static_cast<const uint32_t*>(d_boff), ubuf, ulen);
         }
-        static const bool attrs = [] {
-            const int most = 4 * kLut * 2 + kStageWords * 4 + kChunksPerCta * 2 * (int)sizeof(LjCand);
-            return cudaFuncSetAttribute(lj_cand_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, most) ==
-                       cudaSuccess &&
-                   cudaFuncSetAttribute(lj_write_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, most) ==
-                       cudaSuccess;
-        }();
+        // per call: the attribute belongs to the current device
+        const int most = 4 * kLut * 2 + kStageWords * 4 + kChunksPerCta * 2 * (int)sizeof(LjCand);
+        const bool attrs =
+            cudaFuncSetAttribute(lj_cand_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, most) == cudaSuccess &&
+            cudaFuncSetAttribute(lj_write_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, most) == cudaSuccess;
         if (!attrs) {
             cudaGetLastError();
             set_error("%s", "lj92: shared memory attribute refused");
