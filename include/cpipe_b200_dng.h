@@ -63,8 +63,10 @@ typedef struct cpipe_DngInfo {
 /* Parse IFD0 of a little-endian DNG held in host memory.  CPIPE_OK, or
  * CPIPE_FAILED (bad header, bad IFD table, missing raw fields), or
  * CPIPE_UNSUPPORTED (not a single-plane CFA, CFA repeat other than 2x2 / 4x4,
- * missing CFA pattern), exactly as OpcodeListParser::parse decides.  Host only:
- * needs no GPU. */
+ * missing CFA pattern), exactly as OpcodeListParser::parse decides.  One
+ * extension for files that parse rejects: when IFD0 is not a single-plane CFA
+ * image (a preview), the first full-resolution single-plane CFA SubIFD
+ * supplies the image tags, IFD0 the camera tags.  Host only: needs no GPU. */
 int cpipe_dng_parse(const uint8_t* file, size_t file_bytes, cpipe_DngInfo* info);
 
 /* DngReader::read over a file image in host memory: parse (CPIPE_UNSUPPORTED
