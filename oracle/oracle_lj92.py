@@ -3,9 +3,11 @@
 TEST INFRASTRUCTURE: the encoder makes Compression 7 test files; the decoder
 is the checker of the GPU decode.  Neither is imported by the product.
 
-The reference decodes compressed DNGs through LibRaw (vcpkg dependency
-`libraw`, absent from the reference tree; DngReader.cpp:113-124), so this is a
-restatement of the published standard, not of a reference file:
+Parity unpinned: the reference decodes compressed DNGs through LibRaw (vcpkg
+dependency `libraw`, absent from the reference tree; DngReader.cpp:113-124)
+and holds no Compression 7 test files, so this is a restatement of the
+published standard, not of a reference file, checked by round trips against
+two encoders (this one and cpipe_b200.dng_synth.lj92_segment):
 
   * markers SOI, SOF3 (precision P, lines Y, samples per line X, Nf
     components, each H = V = 1), DHT (class 0 tables), SOS (Ns = Nf, table
