@@ -21,13 +21,13 @@
 //     that path first reaches a sample boundary inside the chunk (its start
 //     state: bit position and component phase), where it leaves the chunk and
 //     how many samples lie between; with different tables per component, also
-//     the paths from that start in the other phases.  Huffman codes
-//     resynchronise, so one of these is almost always the true path.  The lead
-//     is long because high-entropy data resynchronise slowly: with an optimal
-//     table for 10-bit noise the codes are 1-3 bits ahead of 9-10 raw bits, and
-//     a path one component off under different tables soon parts again;
-//     Within a CTA each chunk also takes a path from every exit of the chunk
-//     before that starts none of its own, so only neighbouring failures miss;
+//     the path from that start one phase on.  Huffman codes resynchronise, so
+//     one of these is almost always the true path.  The lead is long because
+//     high-entropy data resynchronise slowly: with an optimal table for 10-bit
+//     noise the codes are 1-3 bits ahead of 9-10 raw bits, and a path one
+//     component off under different tables soon parts again.  Within a CTA, in
+//     two rounds, each chunk also takes a path from every exit of the chunk
+//     before that starts none of its own, so only runs of failures miss;
 //  3. walks: a warp per group of 32 chunks chains the chunks from its first
 //     chunk's lead path and next-phase path (lane j takes the path whose start
 //     is lane j-1's exit; a chunk with no matching path is decoded again from
